@@ -1,0 +1,511 @@
+"""ctypes binding of libab2 (include/ab2.h, include/ab2_problems.h).
+
+This is the Python face of the C ABI, shaped like Alien's algebra/solver API
+(SimpleCSRInternalLinearAlgebra method names, the krylov example's solver and
+preconditioner options, SolverStatus).  It loads ``alien_b200/lib/libab2.so``
+and nothing else: when the library is missing the import fails loudly -- there
+is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(os.environ.get("AB2_LIB", Path(__file__).resolve().parent / "lib" / "libab2.so"))
+
+AB2_OK = 0
+AB2_ERR_CUDA = -1
+AB2_ERR_OOM = -2
+AB2_ERR_BREAKDOWN = -3
+AB2_ERR_NOT_CONVERGED = -4
+AB2_ERR_TIMEOUT = -5
+AB2_ERR_BAD_ARG = -6
+AB2_ERR_UNSUPPORTED = -7
+
+FMT_CSR, FMT_ELL, FMT_F32 = 1, 2, 4
+SPMV_AUTO, SPMV_CSR_SCALAR, SPMV_CSR_STAGED, SPMV_ELL = 0, 1, 2, 3
+SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
+PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3}
+BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho"}
+
+
+class AB2Error(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libab2 error {code}: {msg}")
+        self.code = code
+
+
+class MatrixInfo(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("ell_stored", C.c_longlong), ("ell_slice", C.c_int),
+                ("formats", C.c_int), ("device_bytes", C.c_longlong)]
+
+
+class PrecondOptions(C.Structure):
+    _fields_ = [("kind", C.c_int), ("poly_factor", C.c_double), ("poly_order", C.c_int),
+                ("poly_factor_max_iter", C.c_int)]
+
+
+class PrecondInfo(C.Structure):
+    _fields_ = [("kind", C.c_int), ("cheb_alpha", C.c_double), ("cheb_beta", C.c_double),
+                ("ilu_levels_lower", C.c_int), ("ilu_levels_upper", C.c_int)]
+
+
+class SolverOptions(C.Structure):
+    _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
+                ("poly_factor", C.c_double), ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int),
+                ("spmv_variant", C.c_int), ("use_graph", C.c_int)]
+
+
+class Status(C.Structure):
+    _fields_ = [("succeeded", C.c_int), ("iterations", C.c_int), ("error", C.c_int), ("breakdown", C.c_int),
+                ("residual", C.c_double), ("true_residual", C.c_double), ("nrm2_b", C.c_double),
+                ("setup_ms", C.c_double), ("solve_ms", C.c_double)]
+
+
+class Problem(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("row_ptr", C.POINTER(C.c_int)), ("cols", C.POINTER(C.c_int)), ("vals", C.POINTER(C.c_double)),
+                ("x_true", C.POINTER(C.c_double)), ("b", C.POINTER(C.c_double)),
+                ("log10_k", C.POINTER(C.c_double))]
+
+
+_P = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+
+# name -> (restype, argtypes); the full list of entry points in include/*.h
+SIGNATURES: dict[str, tuple] = {
+    "ab2_context_create": (_I, [_I, C.POINTER(_P)]),
+    "ab2_context_destroy": (_I, [_P]),
+    "ab2_last_error_message": (C.c_char_p, [_P]),
+    "ab2_context_stream": (_I, [_P, C.POINTER(_P)]),
+    "ab2_synchronize": (_I, [_P]),
+    "ab2_context_launch_count": (_I, [_P, C.POINTER(C.c_longlong)]),
+    "ab2_matrix_create_csr": (_I, [_P, _I, _IP, _IP, _DP, _I, C.POINTER(_P)]),
+    "ab2_matrix_update_values": (_I, [_P, _P, _DP]),
+    "ab2_matrix_destroy": (_I, [_P]),
+    "ab2_matrix_get_info": (_I, [_P, C.POINTER(MatrixInfo)]),
+    "ab2_vector_create": (_I, [_P, _I, C.POINTER(_P)]),
+    "ab2_vector_destroy": (_I, [_P]),
+    "ab2_vector_size": (_I, [_P, _IP]),
+    "ab2_vector_upload": (_I, [_P, _P, _DP]),
+    "ab2_vector_download": (_I, [_P, _P, _DP]),
+    "ab2_vector_device_ptr": (_I, [_P, C.POINTER(_P)]),
+    "ab2_mult": (_I, [_P, _P, _P, _P]),
+    "ab2_mult_variant": (_I, [_P, _P, _P, _P, _I]),
+    "ab2_add_lmult": (_I, [_P, _D, _P, _P, _P]),
+    "ab2_add_umult": (_I, [_P, _D, _P, _P, _P]),
+    "ab2_compute_inv_diag": (_I, [_P, _P, _P]),
+    "ab2_mult_inv_diag": (_I, [_P, _P, _P]),
+    "ab2_axpy": (_I, [_P, _D, _P, _P]),
+    "ab2_aypx": (_I, [_P, _D, _P, _P]),
+    "ab2_copy": (_I, [_P, _P, _P]),
+    "ab2_scal": (_I, [_P, _D, _P]),
+    "ab2_pointwise_mult": (_I, [_P, _P, _P, _P]),
+    "ab2_assign": (_I, [_P, _P, _D]),
+    "ab2_diagonal": (_I, [_P, _P, _P]),
+    "ab2_reciprocal": (_I, [_P, _P]),
+    "ab2_dot": (_I, [_P, _P, _P, _DP]),
+    "ab2_norm0": (_I, [_P, _P, _DP]),
+    "ab2_norm1": (_I, [_P, _P, _DP]),
+    "ab2_norm2": (_I, [_P, _P, _DP]),
+    "ab2_scalar_create": (_I, [_P, C.POINTER(_P)]),
+    "ab2_scalar_destroy": (_I, [_P]),
+    "ab2_dot_async": (_I, [_P, _P, _P, _P]),
+    "ab2_scalar_get": (_I, [_P, _P, _DP]),
+    "ab2_precond_create": (_I, [_P, _P, C.POINTER(PrecondOptions), C.POINTER(_P)]),
+    "ab2_precond_apply": (_I, [_P, _P, _P, _P]),
+    "ab2_precond_destroy": (_I, [_P]),
+    "ab2_precond_get_info": (_I, [_P, C.POINTER(PrecondInfo)]),
+    "ab2_precond_ilu0_values": (_I, [_P, _P, _DP]),
+    "ab2_solver_options_default": (None, [C.POINTER(SolverOptions)]),
+    "ab2_solver_create": (_I, [_P, _P, C.POINTER(SolverOptions), C.POINTER(_P)]),
+    "ab2_solver_solve": (_I, [_P, _P, _P, C.POINTER(Status)]),
+    "ab2_solver_history": (_I, [_P, _DP, _I, _IP]),
+    "ab2_solver_destroy": (_I, [_P]),
+    "ab2_problem_poisson": (_I, [_I, _I, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
+    "ab2_problem_diffusion": (_I, [_I, _I, _I, _D, _D, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
+    "ab2_problem_convdiff": (_I, [_I, _I, _I, _D, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
+    "ab2_problem_destroy": (_I, [C.POINTER(Problem)]),
+    "ab2_rng_u64": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
+    "ab2_rng_uniform": (_D, [C.c_uint64, C.c_uint64, C.c_uint64]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded libab2 (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"libab2 not built: {LIB_PATH} is missing (run python -m alien_b200.build)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_DP)
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(_IP)
+
+
+# ---------------------------------------------------------------------------- handles
+class Context:
+    """One CUDA device + stream (ab2_context)."""
+
+    def __init__(self, device: int = 0):
+        h = _P()
+        rc = lib().ab2_context_create(device, C.byref(h))
+        if rc != AB2_OK:
+            raise AB2Error(rc, "ab2_context_create failed")
+        self.h = h
+
+    def check(self, rc: int, what: str = ""):
+        if rc != AB2_OK:
+            msg = lib().ab2_last_error_message(self.h) or b""
+            raise AB2Error(rc, f"{what}: {msg.decode(errors='replace')}")
+        return rc
+
+    def close(self):
+        if self.h:
+            lib().ab2_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self):
+        self.check(lib().ab2_synchronize(self.h), "synchronize")
+
+    @property
+    def stream(self) -> int:
+        s = _P()
+        self.check(lib().ab2_context_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    @property
+    def launches(self) -> int:
+        c = C.c_longlong()
+        self.check(lib().ab2_context_launch_count(self.h, C.byref(c)))
+        return c.value
+
+    # -- objects
+    def matrix(self, row_ptr, cols, vals, formats: int = FMT_CSR | FMT_ELL) -> "Matrix":
+        return Matrix(self, row_ptr, cols, vals, formats)
+
+    def vector(self, n_or_array) -> "Vector":
+        if np.isscalar(n_or_array):
+            return Vector(self, int(n_or_array))
+        a = np.ascontiguousarray(n_or_array, dtype=np.float64)
+        v = Vector(self, a.size)
+        v.upload(a)
+        return v
+
+    # -- algebra (IInternalLinearAlgebra method names)
+    def mult(self, A, x, y, variant: int = SPMV_AUTO):
+        self.check(lib().ab2_mult_variant(self.h, A.h, x.h, y.h, variant), "mult")
+
+    def addLMult(self, alpha, A, x, y):
+        self.check(lib().ab2_add_lmult(self.h, alpha, A.h, x.h, y.h), "addLMult")
+
+    def addUMult(self, alpha, A, x, y):
+        self.check(lib().ab2_add_umult(self.h, alpha, A.h, x.h, y.h), "addUMult")
+
+    def computeInvDiag(self, A, d):
+        self.check(lib().ab2_compute_inv_diag(self.h, A.h, d.h), "computeInvDiag")
+
+    def multInvDiag(self, A, y):
+        self.check(lib().ab2_mult_inv_diag(self.h, A.h, y.h), "multInvDiag")
+
+    def diagonal(self, A, d):
+        self.check(lib().ab2_diagonal(self.h, A.h, d.h), "diagonal")
+
+    def axpy(self, alpha, x, y):
+        self.check(lib().ab2_axpy(self.h, alpha, x.h, y.h), "axpy")
+
+    def aypx(self, alpha, y, x):
+        self.check(lib().ab2_aypx(self.h, alpha, y.h, x.h), "aypx")
+
+    def copy(self, x, y):
+        self.check(lib().ab2_copy(self.h, x.h, y.h), "copy")
+
+    def scal(self, alpha, x):
+        self.check(lib().ab2_scal(self.h, alpha, x.h), "scal")
+
+    def pointwiseMult(self, x, y, w):
+        self.check(lib().ab2_pointwise_mult(self.h, x.h, y.h, w.h), "pointwiseMult")
+
+    def assign(self, x, alpha):
+        self.check(lib().ab2_assign(self.h, x.h, alpha), "assign")
+
+    def reciprocal(self, x):
+        self.check(lib().ab2_reciprocal(self.h, x.h), "reciprocal")
+
+    def dot(self, x, y) -> float:
+        r = C.c_double()
+        self.check(lib().ab2_dot(self.h, x.h, y.h, C.byref(r)), "dot")
+        return r.value
+
+    def norm0(self, x) -> float:
+        r = C.c_double()
+        self.check(lib().ab2_norm0(self.h, x.h, C.byref(r)), "norm0")
+        return r.value
+
+    def norm1(self, x) -> float:
+        r = C.c_double()
+        self.check(lib().ab2_norm1(self.h, x.h, C.byref(r)), "norm1")
+        return r.value
+
+    def norm2(self, x) -> float:
+        r = C.c_double()
+        self.check(lib().ab2_norm2(self.h, x.h, C.byref(r)), "norm2")
+        return r.value
+
+
+class Matrix:
+    def __init__(self, ctx: Context, row_ptr, cols, vals, formats: int):
+        self.ctx = ctx
+        self.row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        self.cols = np.ascontiguousarray(cols, dtype=np.int32)
+        self.vals = np.ascontiguousarray(vals, dtype=np.float64)
+        self.n = self.row_ptr.size - 1
+        h = _P()
+        ctx.check(lib().ab2_matrix_create_csr(ctx.h, self.n, _ip(self.row_ptr), _ip(self.cols), _dp(self.vals),
+                                              formats, C.byref(h)), "matrix_create_csr")
+        self.h = h
+
+    def update_values(self, vals):
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        self.ctx.check(lib().ab2_matrix_update_values(self.ctx.h, self.h, _dp(v)), "update_values")
+        self.vals = v
+
+    @property
+    def info(self) -> MatrixInfo:
+        i = MatrixInfo()
+        self.ctx.check(lib().ab2_matrix_get_info(self.h, C.byref(i)))
+        return i
+
+    def close(self):
+        if self.h:
+            lib().ab2_matrix_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Vector:
+    def __init__(self, ctx: Context, n: int):
+        self.ctx = ctx
+        self.n = n
+        h = _P()
+        ctx.check(lib().ab2_vector_create(ctx.h, n, C.byref(h)), "vector_create")
+        self.h = h
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.size == self.n
+        self.ctx.check(lib().ab2_vector_upload(self.ctx.h, self.h, _dp(a)), "upload")
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.float64)
+        self.ctx.check(lib().ab2_vector_download(self.ctx.h, self.h, _dp(out)), "download")
+        return out
+
+    @property
+    def device_ptr(self) -> int:
+        p = _P()
+        self.ctx.check(lib().ab2_vector_device_ptr(self.h, C.byref(p)))
+        return p.value or 0
+
+    def close(self):
+        if self.h:
+            lib().ab2_vector_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Precond:
+    def __init__(self, ctx: Context, A: Matrix, kind: str = "diag", poly_factor: float = 0.0, poly_order: int = 3,
+                 poly_factor_max_iter: int = 10):
+        self.ctx, self.A = ctx, A
+        o = PrecondOptions(PRECOND[kind], poly_factor, poly_order, poly_factor_max_iter)
+        h = _P()
+        ctx.check(lib().ab2_precond_create(ctx.h, A.h, C.byref(o), C.byref(h)), "precond_create")
+        self.h = h
+
+    def apply(self, x: Vector, y: Vector):
+        self.ctx.check(lib().ab2_precond_apply(self.ctx.h, self.h, x.h, y.h), "precond_apply")
+
+    @property
+    def info(self) -> PrecondInfo:
+        i = PrecondInfo()
+        self.ctx.check(lib().ab2_precond_get_info(self.h, C.byref(i)))
+        return i
+
+    def ilu0_values(self) -> np.ndarray:
+        out = np.empty(self.A.cols.size, dtype=np.float64)
+        self.ctx.check(lib().ab2_precond_ilu0_values(self.ctx.h, self.h, _dp(out)), "ilu0_values")
+        return out
+
+    def close(self):
+        if self.h:
+            lib().ab2_precond_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class SolveResult:
+    succeeded: bool
+    iterations: int
+    error: int
+    breakdown: str | None
+    residual: float
+    true_residual: float
+    nrm2_b: float
+    setup_ms: float
+    solve_ms: float
+
+
+def solver_options(solver="cg", precond="diag", tol=1e-8, max_iter=1000, poly_factor=0.0, poly_order=3,
+                   poly_factor_max_iter=10, spmv_variant=SPMV_AUTO, use_graph=True) -> SolverOptions:
+    o = SolverOptions()
+    lib().ab2_solver_options_default(C.byref(o))
+    o.solver = SOLVER[solver]
+    o.precond = PRECOND[precond]
+    o.tol = tol
+    o.max_iter = max_iter
+    o.poly_factor = poly_factor
+    o.poly_order = poly_order
+    o.poly_factor_max_iter = poly_factor_max_iter
+    o.spmv_variant = spmv_variant
+    o.use_graph = 1 if use_graph else 0
+    return o
+
+
+class Solver:
+    """ab2_solver: preconditioner set-up at construction, device-resident loop in solve()."""
+
+    def __init__(self, ctx: Context, A: Matrix, **opts):
+        self.ctx, self.A = ctx, A
+        self.opts = solver_options(**opts)
+        h = _P()
+        ctx.check(lib().ab2_solver_create(ctx.h, A.h, C.byref(self.opts), C.byref(h)), "solver_create")
+        self.h = h
+
+    def solve(self, b: Vector, x: Vector) -> SolveResult:
+        st = Status()
+        self.ctx.check(lib().ab2_solver_solve(self.h, b.h, x.h, C.byref(st)), "solve")
+        return SolveResult(bool(st.succeeded), st.iterations, st.error, BREAKDOWN.get(st.breakdown), st.residual,
+                           st.true_residual, st.nrm2_b, st.setup_ms, st.solve_ms)
+
+    def history(self) -> np.ndarray:
+        n = C.c_int()
+        lib().ab2_solver_history(self.h, None, 0, C.byref(n))
+        out = np.empty(max(n.value, 0), dtype=np.float64)
+        if n.value:
+            self.ctx.check(lib().ab2_solver_history(self.h, _dp(out), n.value, C.byref(n)), "history")
+        return out
+
+    def close(self):
+        if self.h:
+            lib().ab2_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------- problems
+@dataclass
+class CsrProblem:
+    n: int
+    row_ptr: np.ndarray
+    cols: np.ndarray
+    vals: np.ndarray
+    x_true: np.ndarray
+    b: np.ndarray
+    log10_k: np.ndarray | None
+    shape: tuple
+
+    @property
+    def nnz(self) -> int:
+        return int(self.row_ptr[-1])
+
+
+def _take(p) -> CsrProblem:
+    P = p.contents
+    n, nnz = P.n, P.nnz
+
+    def arr(ptr, count, dt):
+        return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+    out = CsrProblem(n, arr(P.row_ptr, n + 1, np.int32), arr(P.cols, nnz, np.int32), arr(P.vals, nnz, np.float64),
+                     arr(P.x_true, n, np.float64), arr(P.b, n, np.float64),
+                     arr(P.log10_k, n, np.float64) if bool(P.log10_k) else None, (P.nx, P.ny, P.nz))
+    lib().ab2_problem_destroy(p)
+    return out
+
+
+def poisson(nx, ny=None, nz=None, seed=0) -> CsrProblem:
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    p = C.POINTER(Problem)()
+    rc = lib().ab2_problem_poisson(nx, ny, nz, seed, C.byref(p))
+    if rc:
+        raise AB2Error(rc, "ab2_problem_poisson")
+    return _take(p)
+
+
+def diffusion(nx, ny=None, nz=None, sigma=1.0, smooth=4.0, seed=0) -> CsrProblem:
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    p = C.POINTER(Problem)()
+    rc = lib().ab2_problem_diffusion(nx, ny, nz, sigma, smooth, seed, C.byref(p))
+    if rc:
+        raise AB2Error(rc, "ab2_problem_diffusion")
+    return _take(p)
+
+
+def convdiff(nx, ny=None, nz=None, peclet=10.0, modes=8, seed=0) -> CsrProblem:
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    p = C.POINTER(Problem)()
+    rc = lib().ab2_problem_convdiff(nx, ny, nz, peclet, modes, seed, C.byref(p))
+    if rc:
+        raise AB2Error(rc, "ab2_problem_convdiff")
+    return _take(p)

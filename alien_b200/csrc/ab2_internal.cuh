@@ -1,0 +1,181 @@
+// ab2_internal.cuh -- internal types and helpers of libab2 (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <exception>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "ab2.h"
+
+namespace ab2 {
+
+constexpr int kThreads = 256;          // default block size of streaming kernels
+constexpr int kMaxRedBlocks = 2048;    // cap on blocks of one deterministic reduction
+constexpr int kMaxRedComps = 4;        // values reduced together by one fused kernel
+constexpr int kRedSlots = 8;           // independent reduction slots per context
+constexpr int kEllSlice = 32;          // rows per sliced-ELL slice
+constexpr int kStageCap = 2048;        // nnz staged in shared memory per CSR row block
+
+// Thrown inside libab2 only; every ABI function catches and maps it to a code.
+struct Error {
+  int code;
+  std::string msg;
+};
+
+}  // namespace ab2
+
+struct ab2_context {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  long long launches = 0;
+  // Deterministic reductions: block partials, arrival counters, results.
+  double* d_partials = nullptr;       // kRedSlots * kMaxRedComps * kMaxRedBlocks
+  unsigned int* d_counters = nullptr; // kRedSlots
+  double* d_results = nullptr;        // kRedSlots * kMaxRedComps
+  double* h_pinned = nullptr;         // 64 doubles of pinned staging
+};
+
+struct ab2_vector {
+  ab2_context* ctx = nullptr;
+  int n = 0;
+  double* d = nullptr;
+};
+
+struct ab2_scalar {
+  ab2_context* ctx = nullptr;
+  double* d = nullptr;
+};
+
+struct ab2_matrix {
+  ab2_context* ctx = nullptr;
+  int n = 0;
+  long long nnz = 0;
+  int formats = 0;
+  long long device_bytes = 0;
+  // CSR (always present: ILU0, invdiag and L/U products use it)
+  int* d_rp = nullptr;
+  int* d_ci = nullptr;
+  double* d_v = nullptr;
+  int* d_dcol = nullptr;      // first position with col >= row (the diagonal)
+  float* d_v32 = nullptr;     // FP32 copy when AB2_FMT_F32
+  // row blocks for the shared-memory staged CSR kernel
+  int n_row_blocks = 0;
+  int* d_row_blocks = nullptr;
+  // sliced ELL (BEllPack, 32-row slices, slot-major inside a slice)
+  long long ell_stored = 0;
+  int* d_ell_off = nullptr;   // n_slices + 1 prefix of slice widths
+  int* d_ell_ci = nullptr;    // -1 marks padding
+  double* d_ell_v = nullptr;
+  float* d_ell_v32 = nullptr;
+  // host mirror of the profile, used by symbolic set-up (ILU0 wavefronts)
+  std::vector<int> h_rp, h_ci;
+};
+
+namespace ab2 {
+
+// c + a*b and c - a*b with the product and the sum rounded separately: the
+// rounding of Alien's `y += a*x` loops as its stock build compiles them
+// (SpMV, addL/UMult, ILU0).  BLAS-1 updates use fma() instead, as CBLAS does.
+__device__ __forceinline__ double mul_add_rn(double a, double b, double c) { return __dadd_rn(c, __dmul_rn(a, b)); }
+__device__ __forceinline__ float mul_add_rn(float a, float b, float c) { return __fadd_rn(c, __fmul_rn(a, b)); }
+__device__ __forceinline__ double mul_sub_rn(double a, double b, double c) { return __dsub_rn(c, __dmul_rn(a, b)); }
+__device__ __forceinline__ float mul_sub_rn(float a, float b, float c) { return __fsub_rn(c, __fmul_rn(a, b)); }
+
+inline void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation) throw Error{AB2_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e)};
+    throw Error{AB2_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+  }
+}
+
+#define AB2_CUDA(call) ::ab2::check_cuda((call), #call)
+
+inline void check_launch(ab2_context* ctx, const char* what) {
+  ctx->launches += 1;
+  check_cuda(cudaGetLastError(), what);
+}
+
+inline void require(bool cond, const char* msg) {
+  if (!cond) throw Error{AB2_ERR_BAD_ARG, msg};
+}
+
+template <class T>
+T* dev_alloc(size_t count, long long* accounted = nullptr) {
+  T* p = nullptr;
+  if (count == 0) count = 1;
+  check_cuda(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+  if (accounted) *accounted += (long long)(count * sizeof(T));
+  return p;
+}
+
+inline void dev_free(void* p) {
+  if (p) cudaFree(p);
+}
+
+inline int grid_for(long long n, int threads = kThreads, int cap = 148 * 32) {
+  long long g = (n + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+// Runs f, mapping exceptions to ABI codes and recording the message on ctx.
+template <class F>
+int guard(ab2_context* ctx, F&& f) {
+  try {
+    f();
+    return AB2_OK;
+  } catch (const Error& e) {
+    if (ctx) ctx->last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (ctx) ctx->last_error = "host allocation failed";
+    return AB2_ERR_OOM;
+  } catch (const std::exception& e) {
+    if (ctx) ctx->last_error = e.what();
+    return AB2_ERR_CUDA;
+  } catch (...) {
+    if (ctx) ctx->last_error = "unknown failure";
+    return AB2_ERR_CUDA;
+  }
+}
+
+// ----------------------------------------------------------------- internal ops
+// Plain device-pointer versions of the algebra, shared by the ABI entry points,
+// the preconditioners and the solvers.  All enqueue on ctx->stream.
+struct RedSlot {
+  double* partials;
+  unsigned int* counter;
+  double* result;  // kMaxRedComps doubles on the device
+};
+RedSlot red_slot(ab2_context* ctx, int slot);
+
+void op_fill(ab2_context* ctx, int n, double a, double* x);
+void op_copy(ab2_context* ctx, int n, const double* x, double* y);
+void op_axpy(ab2_context* ctx, int n, double a, const double* x, double* y);
+void op_aypx(ab2_context* ctx, int n, double a, double* y, const double* x);
+void op_scal(ab2_context* ctx, int n, double a, double* x);
+void op_pmult(ab2_context* ctx, int n, const double* x, const double* y, double* w);
+void op_reciprocal(ab2_context* ctx, int n, double* x);
+// out[0] = x.y (device pointer, written by the last block)
+void op_dot(ab2_context* ctx, int n, const double* x, const double* y, double* out, int slot = 0);
+void op_norm0(ab2_context* ctx, int n, const double* x, double* out, int slot = 0);
+void op_norm1(ab2_context* ctx, int n, const double* x, double* out, int slot = 0);
+double read_scalar(ab2_context* ctx, const double* d);
+
+// SpMV family (spmv.cu)
+void op_spmv(ab2_context* ctx, const ab2_matrix* A, const double* x, double* y, int variant);
+void op_add_lu_mult(ab2_context* ctx, const ab2_matrix* A, double alpha, const double* x, double* y, bool lower);
+void op_inv_diag(ab2_context* ctx, const ab2_matrix* A, double* inv);
+void op_diagonal(ab2_context* ctx, const ab2_matrix* A, double* d);
+void op_mult_inv_diag(ab2_context* ctx, const ab2_matrix* A, double* y);
+int resolve_variant(const ab2_matrix* A, int variant);
+
+}  // namespace ab2

@@ -1,0 +1,347 @@
+// context.cu -- contexts, vectors, device scalars and the BLAS-1 part of the
+// algebra (SimpleCSRInternalLinearAlgebra.cc:74-257 / CBLASMPIKernel.h:37-125
+// on the CPU side, SYCLKernelInternal.h:110-1087 on the SYCL side).
+//
+// BLAS-1 rounding follows the reference's operations one for one:
+//   axpy  y = fma(a, x, y)     scal  x = a*x      pointwiseMult  w = x*y
+//   aypx  y = fma(a, y, x)     dot   deterministic tree (reduce.cuh)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "ab2_internal.cuh"
+#include "reduce.cuh"
+
+namespace ab2 {
+
+namespace {
+
+__global__ void k_fill(int n, double a, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = a;
+}
+__global__ void k_copy(int n, const double* __restrict__ x, double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = x[i];
+}
+__global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = fma(a, x[i], y[i]);
+}
+__global__ void k_aypx(int n, double a, double* __restrict__ y, const double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = fma(a, y[i], x[i]);
+}
+__global__ void k_scal(int n, double a, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = a * x[i];
+}
+// x, y and w may alias (the reference calls pointwiseMult(d, y, y)).
+__global__ void k_pmult(int n, const double* x, const double* y, double* w) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w[i] = x[i] * y[i];
+}
+__global__ void k_reciprocal(int n, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = 1.0 / x[i];
+}
+
+__global__ void k_dot(int n, const double* __restrict__ x, const double* __restrict__ y, double* partials,
+                      unsigned int* counter, double* out) {
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] = fma(x[i], y[i], acc[0]);
+  grid_reduce<1>(acc, partials, counter, out);
+}
+__global__ void k_asum(int n, const double* __restrict__ x, double* partials, unsigned int* counter, double* out) {
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] += fabs(x[i]);
+  grid_reduce<1>(acc, partials, counter, out);
+}
+__global__ void k_amax(int n, const double* __restrict__ x, double* partials, unsigned int* counter, double* out) {
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] = fmax(acc[0], fabs(x[i]));
+  grid_reduce<1, Combine::Max>(acc, partials, counter, out);
+}
+
+// Grid of a reduction over n values: a function of n only (determinism).
+int red_grid(int n) { return grid_for(n, kThreads, kMaxRedBlocks); }
+
+}  // namespace
+
+RedSlot red_slot(ab2_context* ctx, int slot) {
+  return RedSlot{ctx->d_partials + (size_t)slot * kMaxRedComps * kMaxRedBlocks, ctx->d_counters + slot,
+                 ctx->d_results + (size_t)slot * kMaxRedComps};
+}
+
+void op_fill(ab2_context* ctx, int n, double a, double* x) {
+  k_fill<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, a, x);
+  check_launch(ctx, "fill");
+}
+void op_copy(ab2_context* ctx, int n, const double* x, double* y) {
+  if (x == y) return;
+  k_copy<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, x, y);
+  check_launch(ctx, "copy");
+}
+void op_axpy(ab2_context* ctx, int n, double a, const double* x, double* y) {
+  k_axpy<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, a, x, y);
+  check_launch(ctx, "axpy");
+}
+void op_aypx(ab2_context* ctx, int n, double a, double* y, const double* x) {
+  k_aypx<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, a, y, x);
+  check_launch(ctx, "aypx");
+}
+void op_scal(ab2_context* ctx, int n, double a, double* x) {
+  k_scal<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, a, x);
+  check_launch(ctx, "scal");
+}
+void op_pmult(ab2_context* ctx, int n, const double* x, const double* y, double* w) {
+  k_pmult<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, x, y, w);
+  check_launch(ctx, "pointwise_mult");
+}
+void op_reciprocal(ab2_context* ctx, int n, double* x) {
+  k_reciprocal<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, x);
+  check_launch(ctx, "reciprocal");
+}
+void op_dot(ab2_context* ctx, int n, const double* x, const double* y, double* out, int slot) {
+  RedSlot s = red_slot(ctx, slot);
+  k_dot<<<red_grid(n), kThreads, 0, ctx->stream>>>(n, x, y, s.partials, s.counter, out);
+  check_launch(ctx, "dot");
+}
+void op_norm1(ab2_context* ctx, int n, const double* x, double* out, int slot) {
+  RedSlot s = red_slot(ctx, slot);
+  k_asum<<<red_grid(n), kThreads, 0, ctx->stream>>>(n, x, s.partials, s.counter, out);
+  check_launch(ctx, "norm1");
+}
+void op_norm0(ab2_context* ctx, int n, const double* x, double* out, int slot) {
+  RedSlot s = red_slot(ctx, slot);
+  k_amax<<<red_grid(n), kThreads, 0, ctx->stream>>>(n, x, s.partials, s.counter, out);
+  check_launch(ctx, "norm0");
+}
+double read_scalar(ab2_context* ctx, const double* d) {
+  AB2_CUDA(cudaMemcpyAsync(ctx->h_pinned, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  return ctx->h_pinned[0];
+}
+
+}  // namespace ab2
+
+using namespace ab2;
+
+namespace {
+
+int check_vec(const ab2_vector* v, int n) {
+  if (!v || v->n != n) return AB2_ERR_BAD_ARG;
+  return AB2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ab2_context_create(int device, ab2_context** out) {
+  if (!out) return AB2_ERR_BAD_ARG;
+  *out = nullptr;
+  ab2_context* ctx = new (std::nothrow) ab2_context();
+  if (!ctx) return AB2_ERR_OOM;
+  int rc = guard(ctx, [&] {
+    int count = 0;
+    AB2_CUDA(cudaGetDeviceCount(&count));
+    require(device >= 0 && device < count, "device index out of range");
+    ctx->device = device;
+    AB2_CUDA(cudaSetDevice(device));
+    AB2_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+    AB2_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->d_partials = dev_alloc<double>((size_t)kRedSlots * kMaxRedComps * kMaxRedBlocks);
+    ctx->d_counters = dev_alloc<unsigned int>(kRedSlots);
+    ctx->d_results = dev_alloc<double>((size_t)kRedSlots * kMaxRedComps);
+    AB2_CUDA(cudaMemset(ctx->d_counters, 0, sizeof(unsigned int) * kRedSlots));
+    AB2_CUDA(cudaMallocHost((void**)&ctx->h_pinned, 64 * sizeof(double)));
+  });
+  if (rc != AB2_OK) {
+    fprintf(stderr, "ab2_context_create: %s\n", ctx->last_error.c_str());
+    ab2_context_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return AB2_OK;
+}
+
+int ab2_context_destroy(ab2_context* ctx) {
+  if (!ctx) return AB2_ERR_BAD_ARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  dev_free(ctx->d_partials);
+  dev_free(ctx->d_counters);
+  dev_free(ctx->d_results);
+  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return AB2_OK;
+}
+
+const char* ab2_last_error_message(const ab2_context* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int ab2_context_stream(const ab2_context* ctx, void** stream) {
+  if (!ctx || !stream) return AB2_ERR_BAD_ARG;
+  *stream = (void*)ctx->stream;
+  return AB2_OK;
+}
+
+int ab2_synchronize(ab2_context* ctx) {
+  if (!ctx) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { AB2_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+int ab2_context_launch_count(const ab2_context* ctx, long long* count) {
+  if (!ctx || !count) return AB2_ERR_BAD_ARG;
+  *count = ctx->launches;
+  return AB2_OK;
+}
+
+// ---------------------------------------------------------------- vectors
+int ab2_vector_create(ab2_context* ctx, int n, ab2_vector** out) {
+  if (!ctx || !out || n < 0) return AB2_ERR_BAD_ARG;
+  *out = nullptr;
+  ab2_vector* v = new (std::nothrow) ab2_vector();
+  if (!v) return AB2_ERR_OOM;
+  int rc = guard(ctx, [&] {
+    v->ctx = ctx;
+    v->n = n;
+    v->d = dev_alloc<double>((size_t)n);
+    AB2_CUDA(cudaMemsetAsync(v->d, 0, sizeof(double) * (size_t)std::max(n, 1), ctx->stream));
+  });
+  if (rc != AB2_OK) {
+    delete v;
+    return rc;
+  }
+  *out = v;
+  return AB2_OK;
+}
+
+int ab2_vector_destroy(ab2_vector* v) {
+  if (!v) return AB2_ERR_BAD_ARG;
+  if (v->ctx) cudaStreamSynchronize(v->ctx->stream);
+  dev_free(v->d);
+  delete v;
+  return AB2_OK;
+}
+
+int ab2_vector_size(const ab2_vector* v, int* n) {
+  if (!v || !n) return AB2_ERR_BAD_ARG;
+  *n = v->n;
+  return AB2_OK;
+}
+
+int ab2_vector_upload(ab2_context* ctx, ab2_vector* v, const double* host) {
+  if (!ctx || !v || (!host && v->n)) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    AB2_CUDA(cudaMemcpyAsync(v->d, host, sizeof(double) * (size_t)v->n, cudaMemcpyHostToDevice, ctx->stream));
+  });
+}
+
+int ab2_vector_download(ab2_context* ctx, const ab2_vector* v, double* host) {
+  if (!ctx || !v || (!host && v->n)) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    AB2_CUDA(cudaMemcpyAsync(host, v->d, sizeof(double) * (size_t)v->n, cudaMemcpyDeviceToHost, ctx->stream));
+    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int ab2_vector_device_ptr(const ab2_vector* v, void** dptr) {
+  if (!v || !dptr) return AB2_ERR_BAD_ARG;
+  *dptr = (void*)v->d;
+  return AB2_OK;
+}
+
+// ---------------------------------------------------------------- BLAS-1
+int ab2_axpy(ab2_context* ctx, double a, const ab2_vector* x, ab2_vector* y) {
+  if (!ctx || !x || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_axpy(ctx, x->n, a, x->d, y->d); });
+}
+int ab2_aypx(ab2_context* ctx, double a, ab2_vector* y, const ab2_vector* x) {
+  if (!ctx || !x || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_aypx(ctx, x->n, a, y->d, x->d); });
+}
+int ab2_copy(ab2_context* ctx, const ab2_vector* x, ab2_vector* y) {
+  if (!ctx || !x || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_copy(ctx, x->n, x->d, y->d); });
+}
+int ab2_scal(ab2_context* ctx, double a, ab2_vector* x) {
+  if (!ctx || !x) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_scal(ctx, x->n, a, x->d); });
+}
+int ab2_pointwise_mult(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, ab2_vector* w) {
+  if (!ctx || !x || check_vec(y, x->n) || check_vec(w, x->n)) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_pmult(ctx, x->n, x->d, y->d, w->d); });
+}
+int ab2_assign(ab2_context* ctx, ab2_vector* x, double a) {
+  if (!ctx || !x) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_fill(ctx, x->n, a, x->d); });
+}
+int ab2_reciprocal(ab2_context* ctx, ab2_vector* x) {
+  if (!ctx || !x) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_reciprocal(ctx, x->n, x->d); });
+}
+int ab2_dot(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, double* result) {
+  if (!ctx || !x || !result || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    RedSlot s = red_slot(ctx, 0);
+    op_dot(ctx, x->n, x->d, y->d, s.result, 0);
+    *result = read_scalar(ctx, s.result);
+  });
+}
+int ab2_norm2(ab2_context* ctx, const ab2_vector* x, double* result) {
+  if (!ctx || !x || !result) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    RedSlot s = red_slot(ctx, 0);
+    op_dot(ctx, x->n, x->d, x->d, s.result, 0);
+    *result = std::sqrt(read_scalar(ctx, s.result));
+  });
+}
+int ab2_norm1(ab2_context* ctx, const ab2_vector* x, double* result) {
+  if (!ctx || !x || !result) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    RedSlot s = red_slot(ctx, 0);
+    op_norm1(ctx, x->n, x->d, s.result, 0);
+    *result = read_scalar(ctx, s.result);
+  });
+}
+int ab2_norm0(ab2_context* ctx, const ab2_vector* x, double* result) {
+  if (!ctx || !x || !result) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    RedSlot s = red_slot(ctx, 0);
+    op_norm0(ctx, x->n, x->d, s.result, 0);
+    *result = read_scalar(ctx, s.result);
+  });
+}
+
+// ---------------------------------------------------------------- device scalars
+int ab2_scalar_create(ab2_context* ctx, ab2_scalar** out) {
+  if (!ctx || !out) return AB2_ERR_BAD_ARG;
+  *out = nullptr;
+  ab2_scalar* s = new (std::nothrow) ab2_scalar();
+  if (!s) return AB2_ERR_OOM;
+  int rc = guard(ctx, [&] {
+    s->ctx = ctx;
+    s->d = dev_alloc<double>(1);
+    AB2_CUDA(cudaMemsetAsync(s->d, 0, sizeof(double), ctx->stream));
+  });
+  if (rc != AB2_OK) {
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return AB2_OK;
+}
+int ab2_scalar_destroy(ab2_scalar* s) {
+  if (!s) return AB2_ERR_BAD_ARG;
+  if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
+  dev_free(s->d);
+  delete s;
+  return AB2_OK;
+}
+int ab2_dot_async(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, ab2_scalar* result) {
+  if (!ctx || !x || !result || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_dot(ctx, x->n, x->d, y->d, result->d, 0); });
+}
+int ab2_scalar_get(ab2_context* ctx, const ab2_scalar* s, double* value) {
+  if (!ctx || !s || !value) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { *value = read_scalar(ctx, s->d); });
+}
+
+}  // extern "C"

@@ -1,0 +1,478 @@
+// precond.cu -- Diag, ILU(0) and Chebyshev preconditioners on the device.
+//
+//   Diag       DiagPreconditioner.h:49-68            z = (1/a_ii) . r
+//   ILU(0)     ILU0Preconditioner.h:71-248           IKJ factorisation, forward
+//              (sequential branch)                   unit-L sweep, backward U sweep
+//   Chebyshev  ChebyshevPreconditioner.h:73-202,     power-method bounds, then the
+//              392-434 (_algo2)                      Ifpack2-style polynomial
+//
+// ILU(0): the factorisation and both sweeps keep the reference's arithmetic row
+// by row (same column order, product and difference rounded apart, an IEEE
+// division by the pivot),
+// so the factor and every application are bit-identical to the sequential CPU
+// code.  Parallelism comes from the wavefronts of the triangular graphs: rows
+// in the same wavefront are independent.  The factorisation runs one launch
+// per wavefront (set-up only).  The sweeps run as ONE launch each with no
+// grid-wide barrier: warps take 32-row chunks in wavefront order from an
+// atomic ticket and wait, per dependency, until the producer's value has been
+// stored.  The value itself is the flag: the output vector is pre-filled with
+// a signalling-NaN sentinel that arithmetic never produces, and a consumer
+// polls the 8-byte word with ld.relaxed.gpu until it changes.  Tickets are
+// handed out in order, so the chunk a warp waits on was taken earlier by a
+// running warp, and every wait is bounded (clock64 budget) -- on expiry the
+// kernel records an error and finishes instead of hanging.
+//
+// Chebyshev: each polynomial step is one fused SpMV kernel whose epilogue forms
+// r = x - A y, z = D^-1 r, p = beta p + z and y' = y + a p in registers, with the
+// reference's rounding (scal then axpy for p, fma for y).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <random>
+
+#include "ab2_internal.cuh"
+#include "precond.cuh"
+#include "spmv_view.cuh"
+
+namespace ab2 {
+
+namespace {
+
+constexpr unsigned long long kSentinel = 0x7FF4A1B2C3D4E5F6ull;  // signalling NaN
+constexpr long long kWaitCycles = 4000000000LL;                  // ~2 s at 1.965 GHz
+
+__device__ __forceinline__ double ld_relaxed(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return __longlong_as_double((long long)v);
+}
+
+__device__ __forceinline__ void st_relaxed(double* p, double x) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(x))
+               : "memory");
+}
+
+// Waits until *p no longer holds the sentinel; bounded.
+__device__ __forceinline__ double wait_value(const double* p, int* err) {
+  double v = ld_relaxed(p);
+  if ((unsigned long long)__double_as_longlong(v) != kSentinel) return v;
+  const long long t0 = clock64();
+  for (unsigned it = 1;; ++it) {
+    if (it > 8) __nanosleep(it > 64 ? 256 : 32);
+    v = ld_relaxed(p);
+    if ((unsigned long long)__double_as_longlong(v) != kSentinel) return v;
+    if ((it & 63) == 0) {
+      if (clock64() - t0 > kWaitCycles || *(volatile int*)err) {
+        atomicOr(err, 1);
+        return __longlong_as_double(0x7FF8000000000000LL);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ double not_sentinel(double v) {
+  return (unsigned long long)__double_as_longlong(v) == kSentinel ? __longlong_as_double(0x7FF8000000000000LL) : v;
+}
+
+__global__ void k_fill_bits(long long n, unsigned long long bits, double* x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = __longlong_as_double((long long)bits);
+}
+
+// One wavefront of the IKJ factorisation (ILU0Preconditioner.h:156-178): for
+// each k left of the diagonal, a_ik /= a_kk, then a_ij -= a_ik a_kj for every
+// j > k present in both rows (two-pointer merge of the sorted rows).
+__global__ void k_ilu_factor_level(const int* __restrict__ rows, int count, const int* __restrict__ rp,
+                                   const int* __restrict__ ci, const int* __restrict__ dcol, double* __restrict__ lu) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const int i = rows[t];
+  if (i < 0) return;
+  const int end = rp[i + 1];
+  const int di = dcol[i];
+  for (int k = rp[i]; k < di; ++k) {
+    const int kr = ci[k];
+    const int dk = dcol[kr];
+    const double piv = dk < rp[kr + 1] ? lu[dk] : 0.0;
+    const double aik = lu[k] / piv;
+    lu[k] = aik;
+    int l = rp[kr];
+    const int le = rp[kr + 1];
+    for (int j = k + 1; j < end; ++j) {
+      const int cj = ci[j];
+      while (l < le && ci[l] < cj) ++l;
+      if (l == le) break;
+      if (ci[l] == cj) lu[j] = mul_sub_rn(aik, lu[l], lu[j]);
+    }
+  }
+}
+
+// Forward sweep x_i = y_i - sum_{k<dcol} l_ik x_k (solveL, ILU0Preconditioner.h:181-198).
+// Also leaves z at the sentinel for the backward sweep (after y_i was read, so
+// y and z may be the same vector).
+__global__ void __launch_bounds__(256) k_ilu_lsweep(int len, const int* __restrict__ perm, const int* __restrict__ rp,
+                                                    const int* __restrict__ ci, const int* __restrict__ dcol,
+                                                    const double* __restrict__ lu, const double* y, double* t, double* z,
+                                                    unsigned int* tickets, int* err) {
+  const int lane = threadIdx.x & 31;
+  const int nchunks = len >> 5;
+  for (;;) {
+    int chunk = 0;
+    if (lane == 0) chunk = (int)atomicAdd(tickets, 1u);
+    chunk = __shfl_sync(0xffffffffu, chunk, 0);
+    if (chunk >= nchunks) break;
+    const int row = perm[chunk * 32 + lane];
+    if (row >= 0) {
+      double acc = y[row];
+      const int e = dcol[row];
+      for (int k = rp[row]; k < e; ++k) {
+        const double l = lu[k];
+        const double xv = wait_value(t + ci[k], err);
+        acc = mul_sub_rn(l, xv, acc);
+      }
+      z[row] = __longlong_as_double((long long)kSentinel);
+      st_relaxed(t + row, not_sentinel(acc));
+    }
+  }
+  // The backward sweep's ticket is reset here: it is not in use while this runs.
+  if (blockIdx.x == 0 && threadIdx.x == 0) tickets[1] = 0u;
+}
+
+// Backward sweep x_i = (y_i - sum_{k>dcol} u_ik x_k) / u_ii (solveU, :200-231).
+// Puts t back to the sentinel for the next forward sweep.
+__global__ void __launch_bounds__(256) k_ilu_usweep(int len, const int* __restrict__ perm, const int* __restrict__ rp,
+                                                    const int* __restrict__ ci, const int* __restrict__ dcol,
+                                                    const double* __restrict__ lu, double* t, double* z,
+                                                    unsigned int* tickets, int* err) {
+  const int lane = threadIdx.x & 31;
+  const int nchunks = len >> 5;
+  for (;;) {
+    int chunk = 0;
+    if (lane == 0) chunk = (int)atomicAdd(tickets + 1, 1u);
+    chunk = __shfl_sync(0xffffffffu, chunk, 0);
+    if (chunk >= nchunks) break;
+    const int row = perm[chunk * 32 + lane];
+    if (row >= 0) {
+      const int dk = dcol[row];
+      const int e = rp[row + 1];
+      double acc = t[row];
+      for (int k = dk + 1; k < e; ++k) {
+        const double u = lu[k];
+        const double xv = wait_value(z + ci[k], err);
+        acc = mul_sub_rn(u, xv, acc);
+      }
+      const double piv = dk < e ? lu[dk] : 0.0;
+      t[row] = __longlong_as_double((long long)kSentinel);
+      st_relaxed(z + row, not_sentinel(acc / piv));
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) tickets[0] = 0u;
+}
+
+// Chebyshev step (ChebyshevPreconditioner.h:392-434 with y_cur the iterate):
+//   r = x - A y_cur ; z = D^-1 r ; p = first ? z : beta*p + z ; y_next = y_cur + a p
+template <class View>
+__global__ void __launch_bounds__(kThreads) k_cheb_step(int n, View A, const double* __restrict__ x,
+                                                        const double* __restrict__ ycur, const double* __restrict__ inv,
+                                                        double* __restrict__ p, double* __restrict__ ynext, double a,
+                                                        double bcoef, int first) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  const double ay = A.row(row, ycur);
+  const double r = fma(-1.0, ay, x[row]);
+  const double z = inv[row] * r;
+  const double pn = first ? z : __dadd_rn(__dmul_rn(bcoef, p[row]), z);
+  p[row] = pn;
+  ynext[row] = fma(a, pn, ycur[row]);
+}
+
+__global__ void k_pmult2(int n, const double* __restrict__ a, const double* x, double* y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a[i] * x[i];
+}
+
+void ilu_symbolic(const ab2_matrix* A, Ilu0Data& d) {
+  const int n = A->n;
+  const int* rp = A->h_rp.data();
+  const int* ci = A->h_ci.data();
+  std::vector<int> dc(n);
+  for (int i = 0; i < n; ++i) {
+    int k = rp[i];
+    while (k < rp[i + 1] && ci[k] < i) ++k;
+    dc[i] = k;
+  }
+  std::vector<int> lev_l(n, 0), lev_u(n, 0);
+  int max_l = -1, max_u = -1;
+  for (int i = 0; i < n; ++i) {
+    int lv = 0;
+    for (int k = rp[i]; k < dc[i]; ++k) lv = std::max(lv, lev_l[ci[k]] + 1);
+    lev_l[i] = lv;
+    max_l = std::max(max_l, lv);
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    int lv = 0;
+    for (int k = dc[i] + 1; k < rp[i + 1]; ++k) lv = std::max(lv, lev_u[ci[k]] + 1);
+    lev_u[i] = lv;
+    max_u = std::max(max_u, lv);
+  }
+  auto build = [n](const std::vector<int>& lev, int nlev, bool descending, std::vector<int>& perm,
+                   std::vector<int>& ptr) {
+    std::vector<int> cnt(nlev, 0);
+    for (int i = 0; i < n; ++i) cnt[lev[i]]++;
+    ptr.assign(nlev + 1, 0);
+    for (int l = 0; l < nlev; ++l) ptr[l + 1] = ptr[l] + ((cnt[l] + 31) / 32) * 32;
+    perm.assign(ptr[nlev], -1);
+    std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+    if (!descending) {
+      for (int i = 0; i < n; ++i) perm[fill[lev[i]]++] = i;
+    } else {
+      for (int i = n - 1; i >= 0; --i) perm[fill[lev[i]]++] = i;
+    }
+  };
+  std::vector<int> perm_u, ptr_u;
+  d.levels_l = max_l + 1;
+  d.levels_u = max_u + 1;
+  build(lev_l, d.levels_l, false, d.h_perm_l, d.lev_ptr_l);
+  build(lev_u, d.levels_u, true, perm_u, ptr_u);
+  d.len_l = (int)d.h_perm_l.size();
+  d.len_u = (int)perm_u.size();
+  d.d_perm_l = dev_alloc<int>(d.h_perm_l.size());
+  d.d_perm_u = dev_alloc<int>(perm_u.size());
+  AB2_CUDA(cudaMemcpy(d.d_perm_l, d.h_perm_l.data(), sizeof(int) * d.h_perm_l.size(), cudaMemcpyHostToDevice));
+  AB2_CUDA(cudaMemcpy(d.d_perm_u, perm_u.data(), sizeof(int) * perm_u.size(), cudaMemcpyHostToDevice));
+}
+
+int sweep_blocks(ab2_context* ctx, int len) {
+  const int warps = len / 32;
+  const int blocks = (warps + 7) / 8;
+  return std::max(1, std::min(blocks, ctx->num_sms * 8));
+}
+
+void ilu_init(ab2_context* ctx, ab2_precond* pc) {
+  const ab2_matrix* A = pc->A;
+  Ilu0Data& d = pc->ilu;
+  ilu_symbolic(A, d);
+  d.d_lu = dev_alloc<double>((size_t)A->nnz);
+  d.d_tmp = dev_alloc<double>((size_t)A->n);
+  d.d_counters = dev_alloc<unsigned int>(2);
+  d.d_err = dev_alloc<int>(1);
+  AB2_CUDA(cudaMemsetAsync(d.d_counters, 0, 2 * sizeof(unsigned int), ctx->stream));
+  AB2_CUDA(cudaMemsetAsync(d.d_err, 0, sizeof(int), ctx->stream));
+  AB2_CUDA(cudaMemcpyAsync(d.d_lu, A->d_v, sizeof(double) * (size_t)A->nnz, cudaMemcpyDeviceToDevice, ctx->stream));
+  k_fill_bits<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, kSentinel, d.d_tmp);
+  check_launch(ctx, "ilu_fill");
+  for (int l = 1; l < d.levels_l; ++l) {  // wavefront 0 rows have nothing left of the diagonal
+    const int a = d.lev_ptr_l[l], b = d.lev_ptr_l[l + 1];
+    const int cnt = b - a;
+    if (cnt == 0) continue;
+    k_ilu_factor_level<<<(cnt + 127) / 128, 128, 0, ctx->stream>>>(d.d_perm_l + a, cnt, A->d_rp, A->d_ci, A->d_dcol,
+                                                                   d.d_lu);
+    check_launch(ctx, "ilu_factor");
+  }
+}
+
+void cheb_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o) {
+  const ab2_matrix* A = pc->A;
+  const int n = A->n;
+  ChebData& c = pc->cheb;
+  c.order = o->poly_order;
+  c.d_p = dev_alloc<double>((size_t)n);
+  c.d_y[0] = dev_alloc<double>((size_t)n);
+  c.d_y[1] = dev_alloc<double>((size_t)n);
+  c.d_xcopy = dev_alloc<double>((size_t)n);
+  double* x = dev_alloc<double>((size_t)n);
+  double* y = c.d_y[0];
+  double* s = red_slot(ctx, 0).result;
+  op_fill(ctx, n, 0.0, y);
+  op_fill(ctx, n, 0.0, c.d_p);
+  // Both power methods draw their start vector from a default-seeded
+  // std::mt19937 with U(-1,1), index order (computeBeta :124-129, computeAlpha :166-172).
+  std::vector<double> h(n);
+  auto power = [&](bool shift, double b) {
+    std::mt19937 gen;
+    std::uniform_real_distribution<> dis(-1., 1.);
+    for (int i = 0; i < n; ++i) h[i] = dis(gen);
+    AB2_CUDA(cudaMemcpyAsync(x, h.data(), sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    op_dot(ctx, n, x, x, s);
+    const double nrm = std::sqrt(read_scalar(ctx, s));
+    op_scal(ctx, n, 1 / nrm, x);
+    double est = 0.0;
+    for (int it = 0; it < o->poly_factor_max_iter; ++it) {
+      op_spmv(ctx, A, x, y, pc->variant);
+      op_pmult(ctx, n, pc->d_inv, y, y);
+      if (shift) op_axpy(ctx, n, -b, x, y);
+      op_dot(ctx, n, y, x, s);
+      const double xax = read_scalar(ctx, s);
+      op_dot(ctx, n, x, x, s);
+      const double xdx = read_scalar(ctx, s);
+      est = xax / xdx;
+      op_dot(ctx, n, y, y, s);
+      const double nr = std::sqrt(read_scalar(ctx, s));
+      op_scal(ctx, n, 1 / nr, y);
+      op_copy(ctx, n, y, x);
+    }
+    return shift ? est + b : est;
+  };
+  c.beta = power(false, 0.0);
+  c.alpha = power(true, c.beta);
+  if (o->poly_factor != 0.) c.alpha = c.beta / o->poly_factor;
+  dev_free(x);
+  op_fill(ctx, n, 0.0, y);
+  // Step coefficients of _algo2, evaluated in the reference's order.
+  const double dd = (c.beta + c.alpha) / 2;
+  const double cc = (c.beta - c.alpha) / 2;
+  const int steps = std::max(1, c.order);
+  c.a.assign(steps, 0.0);
+  c.b.assign(steps, 0.0);
+  double a = 2 / dd;
+  c.a[0] = a;
+  for (int i = 1; i < steps; ++i) {
+    const double beta = a * (cc / 2.) * (cc / 2.);
+    a = 1. / (dd - beta);
+    c.b[i] = beta;
+    c.a[i] = a;
+  }
+}
+
+}  // namespace
+
+void pc_apply(ab2_context* ctx, const ab2_precond* pc, const double* x, double* y) {
+  const int n = pc->A->n;
+  if (n == 0) return;
+  switch (pc->kind) {
+    case AB2_PC_NONE: op_copy(ctx, n, x, y); break;
+    case AB2_PC_DIAG:
+      k_pmult2<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, pc->d_inv, x, y);
+      check_launch(ctx, "diag_apply");
+      break;
+    case AB2_PC_ILU0: {
+      const Ilu0Data& d = pc->ilu;
+      const ab2_matrix* A = pc->A;
+      k_ilu_lsweep<<<sweep_blocks(ctx, d.len_l), 256, 0, ctx->stream>>>(d.len_l, d.d_perm_l, A->d_rp, A->d_ci, A->d_dcol,
+                                                                        d.d_lu, x, d.d_tmp, y, d.d_counters, d.d_err);
+      check_launch(ctx, "ilu_lsweep");
+      k_ilu_usweep<<<sweep_blocks(ctx, d.len_u), 256, 0, ctx->stream>>>(d.len_u, d.d_perm_u, A->d_rp, A->d_ci, A->d_dcol,
+                                                                        d.d_lu, d.d_tmp, y, d.d_counters, d.d_err);
+      check_launch(ctx, "ilu_usweep");
+      break;
+    }
+    case AB2_PC_CHEB: {
+      const ChebData& c = pc->cheb;
+      const double* xin = x;
+      if (x == y) {
+        op_copy(ctx, n, x, c.d_xcopy);
+        xin = c.d_xcopy;
+      }
+      const int steps = std::max(1, c.order);
+      const double* cur = xin;
+      for (int i = 0; i < steps; ++i) {
+        double* next = (i == steps - 1) ? y : c.d_y[i & 1];
+        with_view<double>(pc->A, pc->variant, [&](auto view) {
+          k_cheb_step<<<(n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(n, view, xin, cur, pc->d_inv, c.d_p,
+                                                                                   next, c.a[i], c.b[i], i == 0);
+        });
+        check_launch(ctx, "cheb_step");
+        cur = next;
+      }
+      break;
+    }
+    default: throw Error{AB2_ERR_BAD_ARG, "unknown preconditioner"};
+  }
+}
+
+void pc_reset(ab2_context* ctx, const ab2_precond* pc) {
+  if (pc->kind != AB2_PC_ILU0) return;
+  const Ilu0Data& d = pc->ilu;
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  k_fill_bits<<<grid_for(pc->A->n), kThreads, 0, ctx->stream>>>(pc->A->n, kSentinel, d.d_tmp);
+  check_launch(ctx, "ilu_fill");
+  AB2_CUDA(cudaMemsetAsync(d.d_counters, 0, 2 * sizeof(unsigned int), ctx->stream));
+  AB2_CUDA(cudaMemsetAsync(d.d_err, 0, sizeof(int), ctx->stream));
+}
+
+int pc_error(ab2_context* ctx, const ab2_precond* pc) {
+  if (pc->kind != AB2_PC_ILU0) return 0;
+  int e = 0;
+  AB2_CUDA(cudaMemcpyAsync(&e, pc->ilu.d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  return e;
+}
+
+}  // namespace ab2
+
+using namespace ab2;
+
+extern "C" {
+
+int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_options* o, ab2_precond** out) {
+  if (!ctx || !A || !o || !out) return AB2_ERR_BAD_ARG;
+  *out = nullptr;
+  if (o->kind < AB2_PC_NONE || o->kind > AB2_PC_CHEB) return AB2_ERR_BAD_ARG;
+  ab2_precond* pc = new (std::nothrow) ab2_precond();
+  if (!pc) return AB2_ERR_OOM;
+  int rc = guard(ctx, [&] {
+    pc->ctx = ctx;
+    pc->A = A;
+    pc->kind = o->kind;
+    if (o->kind == AB2_PC_DIAG || o->kind == AB2_PC_CHEB) {
+      pc->d_inv = dev_alloc<double>((size_t)A->n);
+      // init(): assign(inv, 1) then computeInvDiag (DiagPreconditioner.h:49-54)
+      op_inv_diag(ctx, A, pc->d_inv);
+    }
+    if (o->kind == AB2_PC_ILU0) ilu_init(ctx, pc);
+    if (o->kind == AB2_PC_CHEB) {
+      require(o->poly_factor_max_iter >= 0, "poly_factor_max_iter must be >= 0");
+      cheb_init(ctx, pc, o);
+    }
+    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+  if (rc != AB2_OK) {
+    ab2_precond_destroy(pc);
+    return rc;
+  }
+  *out = pc;
+  return AB2_OK;
+}
+
+int ab2_precond_apply(ab2_context* ctx, const ab2_precond* pc, const ab2_vector* x, ab2_vector* y) {
+  if (!ctx || !pc || !x || !y || x->n != pc->A->n || y->n != pc->A->n) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { pc_apply(ctx, pc, x->d, y->d); });
+}
+
+int ab2_precond_destroy(ab2_precond* pc) {
+  if (!pc) return AB2_ERR_BAD_ARG;
+  if (pc->ctx) cudaStreamSynchronize(pc->ctx->stream);
+  dev_free(pc->d_inv);
+  dev_free(pc->ilu.d_lu);
+  dev_free(pc->ilu.d_perm_l);
+  dev_free(pc->ilu.d_perm_u);
+  dev_free(pc->ilu.d_tmp);
+  dev_free(pc->ilu.d_counters);
+  dev_free(pc->ilu.d_err);
+  dev_free(pc->cheb.d_p);
+  dev_free(pc->cheb.d_y[0]);
+  dev_free(pc->cheb.d_y[1]);
+  dev_free(pc->cheb.d_xcopy);
+  delete pc;
+  return AB2_OK;
+}
+
+int ab2_precond_get_info(const ab2_precond* pc, ab2_precond_info* info) {
+  if (!pc || !info) return AB2_ERR_BAD_ARG;
+  info->kind = pc->kind;
+  info->cheb_alpha = pc->cheb.alpha;
+  info->cheb_beta = pc->cheb.beta;
+  info->ilu_levels_lower = pc->ilu.levels_l;
+  info->ilu_levels_upper = pc->ilu.levels_u;
+  return AB2_OK;
+}
+
+int ab2_precond_ilu0_values(ab2_context* ctx, const ab2_precond* pc, double* lu) {
+  if (!ctx || !pc || !lu || pc->kind != AB2_PC_ILU0) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    AB2_CUDA(cudaMemcpyAsync(lu, pc->ilu.d_lu, sizeof(double) * (size_t)pc->A->nnz, cudaMemcpyDeviceToHost, ctx->stream));
+    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,468 @@
+// spmv.cu -- device matrices and the SpMV family.
+//
+// Reference counterparts:
+//   y = A x        SimpleCSRMatrixMultT.h:172-191 (CSR, row-sequential sum)
+//                  SYCLBEllPackMatrix.cc:624-688   (BEllPack, one work-item per row)
+//   y += a L/U x   SimpleCSRMatrixMultT.h:193-233
+//   1/a_ii         SimpleCSRMatrixMultT.h:478-509 (diagonal found through dcol,
+//                  CSRStructInfo.h:291-309)
+//   conversion     SimpleCSRtoSYCLMatrixConverter.cc:74-104, BEllPack layout
+//                  SYCLBEllPackMatrix.cc:70-215
+//
+// Every variant sums a row's products in column order, rounding each product
+// and each partial sum (mul_add_rn) exactly as the reference loop does, so all
+// variants give bit-identical y.  The
+// sliced-ELL layout keeps 32-row slices (not the reference's 1024) and stores
+// slot j of the slice's rows contiguously, so the 32 lanes of a warp read 256
+// contiguous bytes of values and 128 of column indices per slot.  Padding slots
+// carry column -1 and are skipped, so padding never touches x.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "ab2_internal.cuh"
+
+namespace ab2 {
+
+namespace {
+
+// ----------------------------------------------------------------- set-up kernels
+__global__ void k_validate(int n, const int* __restrict__ rp, const int* __restrict__ ci, int* bad) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    const int a = rp[row], b = rp[row + 1];
+    if (b < a) {
+      atomicOr(bad, 1);
+      continue;
+    }
+    int prev = -1;
+    for (int k = a; k < b; ++k) {
+      const int c = ci[k];
+      if (c < 0 || c >= n) atomicOr(bad, 2);
+      if (c <= prev) atomicOr(bad, 4);
+      prev = c;
+    }
+  }
+}
+
+__global__ void k_dcol(int n, const int* __restrict__ rp, const int* __restrict__ ci, int* __restrict__ dcol) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    int k = rp[row];
+    const int e = rp[row + 1];
+    while (k < e && ci[k] < row) ++k;
+    dcol[row] = k;
+  }
+}
+
+template <class T>
+__global__ void k_ell_fill(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
+                           const int* __restrict__ off, int* __restrict__ eci, T* __restrict__ ev) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    const int s = row / kEllSlice, lane = row % kEllSlice;
+    const int w = off[s + 1] - off[s];
+    const size_t base = (size_t)off[s] * kEllSlice + lane;
+    const int a = rp[row], len = rp[row + 1] - a;
+    for (int j = 0; j < w; ++j) {
+      const size_t at = base + (size_t)j * kEllSlice;
+      eci[at] = j < len ? ci[a + j] : -1;
+      ev[at] = j < len ? (T)v[a + j] : (T)0;
+    }
+  }
+}
+
+// Padding rows past n in the last slice.
+__global__ void k_ell_pad_tail(int n, int n_pad, const int* __restrict__ off, int* __restrict__ eci) {
+  const int row = n + blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n_pad) return;
+  const int s = row / kEllSlice, lane = row % kEllSlice;
+  const int w = off[s + 1] - off[s];
+  for (int j = 0; j < w; ++j) eci[(size_t)off[s] * kEllSlice + lane + (size_t)j * kEllSlice] = -1;
+}
+
+__global__ void k_to_f32(long long m, const double* __restrict__ a, float* __restrict__ b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+// ----------------------------------------------------------------- SpMV kernels
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_spmv_csr_scalar(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                                              const T* __restrict__ v, const T* __restrict__ x,
+                                                              T* __restrict__ y) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    T acc = 0;
+    const int e = rp[row + 1];
+    for (int k = rp[row]; k < e; ++k) acc = mul_add_rn(v[k], __ldg(x + ci[k]), acc);
+    y[row] = acc;
+  }
+}
+
+// One block per row block: the block's values and columns are staged into
+// shared memory with coalesced loads, then each thread sums one row from there.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_spmv_csr_staged(const int* __restrict__ blocks, const int* __restrict__ rp,
+                                                              const int* __restrict__ ci, const T* __restrict__ v,
+                                                              const T* __restrict__ x, T* __restrict__ y) {
+  __shared__ T s_v[kStageCap];
+  __shared__ int s_c[kStageCap];
+  const int r0 = blocks[blockIdx.x], r1 = blocks[blockIdx.x + 1];
+  const int k0 = rp[r0], k1 = rp[r1];
+  const int cnt = k1 - k0;
+  if (cnt <= kStageCap) {
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      s_v[t] = __ldcs(v + k0 + t);
+      s_c[t] = __ldcs(ci + k0 + t);
+    }
+    __syncthreads();
+    for (int row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
+      const int a = rp[row] - k0, b = rp[row + 1] - k0;
+      T acc = 0;
+      for (int k = a; k < b; ++k) acc = mul_add_rn(s_v[k], __ldg(x + s_c[k]), acc);
+      y[row] = acc;
+    }
+  } else {
+    // A single row longer than the staging buffer: sequential in thread 0 to
+    // keep the reference's summation order (rare; not on the stencil path).
+    if (threadIdx.x == 0) {
+      for (int row = r0; row < r1; ++row) {
+        T acc = 0;
+        for (int k = rp[row]; k < rp[row + 1]; ++k) acc = mul_add_rn(v[k], __ldg(x + ci[k]), acc);
+        y[row] = acc;
+      }
+    }
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_spmv_ell(int n, const int* __restrict__ off, const int* __restrict__ eci,
+                                                       const T* __restrict__ ev, const T* __restrict__ x,
+                                                       T* __restrict__ y) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  const int s = row >> 5, lane = row & 31;
+  const int o = off[s];
+  const int w = off[s + 1] - o;
+  const size_t base = (size_t)o * kEllSlice + lane;
+  const int* cp = eci + base;
+  const T* vp = ev + base;
+  T acc = 0;
+  int j = 0;
+  for (; j + 8 <= w; j += 8) {
+    int c[8];
+    T a[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      c[u] = __ldcs(cp + (size_t)(j + u) * kEllSlice);
+      a[u] = __ldcs(vp + (size_t)(j + u) * kEllSlice);
+    }
+    T xv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : (T)0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (c[u] >= 0) acc = mul_add_rn(a[u], xv[u], acc);
+  }
+  for (; j < w; ++j) {
+    const int c = __ldcs(cp + (size_t)j * kEllSlice);
+    const T a = __ldcs(vp + (size_t)j * kEllSlice);
+    if (c >= 0) acc = mul_add_rn(a, __ldg(x + c), acc);
+  }
+  y[row] = acc;
+}
+
+__global__ void k_add_lu(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
+                         const int* __restrict__ dcol, double alpha, const double* __restrict__ x, double* __restrict__ y,
+                         bool lower) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    double acc = y[row];
+    const int a = lower ? rp[row] : dcol[row] + 1;
+    const int b = lower ? dcol[row] : rp[row + 1];
+    for (int k = a; k < b; ++k) acc = mul_add_rn(__dmul_rn(alpha, v[k]), x[ci[k]], acc);
+    y[row] = acc;
+  }
+}
+
+// The reference divides by values[dcol[row]] whatever column sits there; a row
+// with nothing at or right of the diagonal reads 0 here (giving inf).
+__global__ void k_inv_diag(int n, const int* __restrict__ rp, const double* __restrict__ v, const int* __restrict__ dcol,
+                           double* __restrict__ inv) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    const int d = dcol[row];
+    inv[row] = 1. / (d < rp[row + 1] ? v[d] : 0.0);
+  }
+}
+
+__global__ void k_mult_inv_diag(int n, const int* __restrict__ rp, const double* __restrict__ v,
+                                const int* __restrict__ dcol, double* __restrict__ y) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    const int d = dcol[row];
+    y[row] = y[row] / (d < rp[row + 1] ? v[d] : 0.0);
+  }
+}
+
+__global__ void k_diagonal(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
+                           const int* __restrict__ dcol, double* __restrict__ d) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    const int k = dcol[row];
+    d[row] = (k < rp[row + 1] && ci[k] == row) ? v[k] : 0.0;
+  }
+}
+
+// Greedy row blocks: at most kThreads rows and kStageCap nonzeros per block
+// (a longer row gets a block of its own).
+std::vector<int> make_row_blocks(int n, const int* rp) {
+  std::vector<int> b;
+  b.push_back(0);
+  int r = 0;
+  while (r < n) {
+    int start = r;
+    long long nz = 0;
+    while (r < n && r - start < kThreads) {
+      const int len = rp[r + 1] - rp[r];
+      if (nz + len > kStageCap) break;
+      nz += len;
+      ++r;
+    }
+    if (r == start) ++r;  // a single row above the cap
+    b.push_back(r);
+  }
+  return b;
+}
+
+}  // namespace
+
+int resolve_variant(const ab2_matrix* A, int variant) {
+  if (variant == AB2_SPMV_AUTO) return (A->formats & AB2_FMT_ELL) ? AB2_SPMV_ELL : AB2_SPMV_CSR_STAGED;
+  return variant;
+}
+
+template <class T>
+void spmv_t(ab2_context* ctx, const ab2_matrix* A, const T* v_csr, const T* v_ell, const T* x, T* y, int variant) {
+  const int n = A->n;
+  if (n == 0) return;
+  switch (resolve_variant(A, variant)) {
+    case AB2_SPMV_CSR_SCALAR:
+      k_spmv_csr_scalar<T><<<grid_for(n, kThreads, 1 << 30), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, v_csr, x, y);
+      break;
+    case AB2_SPMV_CSR_STAGED:
+      k_spmv_csr_staged<T><<<A->n_row_blocks, kThreads, 0, ctx->stream>>>(A->d_row_blocks, A->d_rp, A->d_ci, v_csr, x, y);
+      break;
+    case AB2_SPMV_ELL:
+      require(v_ell != nullptr, "matrix has no sliced-ELL copy in this precision");
+      k_spmv_ell<T><<<(n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(n, A->d_ell_off, A->d_ell_ci, v_ell, x, y);
+      break;
+    default: throw Error{AB2_ERR_BAD_ARG, "unknown SpMV variant"};
+  }
+  check_launch(ctx, "spmv");
+}
+
+void op_spmv(ab2_context* ctx, const ab2_matrix* A, const double* x, double* y, int variant) {
+  spmv_t<double>(ctx, A, A->d_v, A->d_ell_v, x, y, variant);
+}
+
+void op_spmv_f32(ab2_context* ctx, const ab2_matrix* A, const float* x, float* y, int variant) {
+  require(A->d_v32 != nullptr, "matrix has no FP32 copy (AB2_FMT_F32)");
+  spmv_t<float>(ctx, A, A->d_v32, A->d_ell_v32, x, y, variant);
+}
+
+void op_add_lu_mult(ab2_context* ctx, const ab2_matrix* A, double alpha, const double* x, double* y, bool lower) {
+  k_add_lu<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, A->d_rp, A->d_ci, A->d_v, A->d_dcol, alpha, x, y, lower);
+  check_launch(ctx, "add_lu_mult");
+}
+
+void op_inv_diag(ab2_context* ctx, const ab2_matrix* A, double* inv) {
+  k_inv_diag<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, A->d_rp, A->d_v, A->d_dcol, inv);
+  check_launch(ctx, "inv_diag");
+}
+
+void op_mult_inv_diag(ab2_context* ctx, const ab2_matrix* A, double* y) {
+  k_mult_inv_diag<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, A->d_rp, A->d_v, A->d_dcol, y);
+  check_launch(ctx, "mult_inv_diag");
+}
+
+void op_diagonal(ab2_context* ctx, const ab2_matrix* A, double* d) {
+  k_diagonal<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, A->d_rp, A->d_ci, A->d_v, A->d_dcol, d);
+  check_launch(ctx, "diagonal");
+}
+
+// Fills the value arrays (CSR, ELL and the FP32 copies) from the device CSR values.
+static void refresh_values(ab2_context* ctx, ab2_matrix* A) {
+  const int n = A->n;
+  if (A->formats & AB2_FMT_ELL) {
+    k_ell_fill<double><<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, A->d_v, A->d_ell_off, A->d_ell_ci,
+                                                                  A->d_ell_v);
+    check_launch(ctx, "ell_fill");
+  }
+  if (A->formats & AB2_FMT_F32) {
+    k_to_f32<<<grid_for(A->nnz), kThreads, 0, ctx->stream>>>(A->nnz, A->d_v, A->d_v32);
+    check_launch(ctx, "to_f32");
+    if (A->formats & AB2_FMT_ELL) {
+      k_ell_fill<float><<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, A->d_v, A->d_ell_off, A->d_ell_ci,
+                                                                  A->d_ell_v32);
+      check_launch(ctx, "ell_fill_f32");
+    }
+  }
+}
+
+}  // namespace ab2
+
+using namespace ab2;
+
+extern "C" {
+
+int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int* cols, const double* vals, int formats,
+                          ab2_matrix** out) {
+  if (!ctx || !out || n < 0 || !row_ptr || (n > 0 && (!cols || !vals))) return AB2_ERR_BAD_ARG;
+  *out = nullptr;
+  if (row_ptr[0] != 0 || row_ptr[n] < 0) {
+    ctx->last_error = "row_ptr must start at 0 and end at nnz >= 0";
+    return AB2_ERR_BAD_ARG;
+  }
+  ab2_matrix* A = new (std::nothrow) ab2_matrix();
+  if (!A) return AB2_ERR_OOM;
+  int rc = guard(ctx, [&] {
+    A->ctx = ctx;
+    A->n = n;
+    A->nnz = row_ptr[n];
+    A->formats = (formats | AB2_FMT_CSR);
+    const size_t nnz = (size_t)A->nnz;
+    A->h_rp.assign(row_ptr, row_ptr + n + 1);
+    A->h_ci.assign(cols, cols + nnz);
+    A->d_rp = dev_alloc<int>((size_t)n + 1, &A->device_bytes);
+    A->d_ci = dev_alloc<int>(nnz, &A->device_bytes);
+    A->d_v = dev_alloc<double>(nnz, &A->device_bytes);
+    A->d_dcol = dev_alloc<int>((size_t)n, &A->device_bytes);
+    AB2_CUDA(cudaMemcpyAsync(A->d_rp, row_ptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));
+    AB2_CUDA(cudaMemcpyAsync(A->d_ci, cols, sizeof(int) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+    AB2_CUDA(cudaMemcpyAsync(A->d_v, vals, sizeof(double) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+    if (n > 0) {
+      // Device-side profile check: every later kernel indexes x by these columns.
+      int* d_bad = dev_alloc<int>(1);
+      AB2_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), ctx->stream));
+      k_validate<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, d_bad);
+      check_launch(ctx, "validate");
+      int bad = 0;
+      AB2_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+      AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+      dev_free(d_bad);
+      if (bad & 1) throw Error{AB2_ERR_BAD_ARG, "row_ptr is not non-decreasing"};
+      if (bad & 2) throw Error{AB2_ERR_BAD_ARG, "column index out of range"};
+      if (bad & 4) throw Error{AB2_ERR_BAD_ARG, "columns must be strictly increasing inside each row"};
+      k_dcol<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, A->d_dcol);
+      check_launch(ctx, "dcol");
+    }
+    std::vector<int> blocks = make_row_blocks(n, row_ptr);
+    A->n_row_blocks = (int)blocks.size() - 1;
+    A->d_row_blocks = dev_alloc<int>(blocks.size(), &A->device_bytes);
+    AB2_CUDA(cudaMemcpyAsync(A->d_row_blocks, blocks.data(), sizeof(int) * blocks.size(), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    if (A->formats & AB2_FMT_ELL) {
+      const int ns = (n + kEllSlice - 1) / kEllSlice;
+      std::vector<int> off((size_t)ns + 1);
+      long long acc = 0;
+      for (int s = 0; s < ns; ++s) {
+        off[s] = (int)acc;
+        int w = 0;
+        for (int l = 0; l < kEllSlice && s * kEllSlice + l < n; ++l)
+          w = std::max(w, row_ptr[s * kEllSlice + l + 1] - row_ptr[s * kEllSlice + l]);
+        acc += w;
+      }
+      require(acc * kEllSlice < (1LL << 31) * 8, "matrix too large for the sliced-ELL layout");
+      off[ns] = (int)acc;
+      A->ell_stored = acc * kEllSlice;
+      A->d_ell_off = dev_alloc<int>(off.size(), &A->device_bytes);
+      A->d_ell_ci = dev_alloc<int>((size_t)A->ell_stored, &A->device_bytes);
+      A->d_ell_v = dev_alloc<double>((size_t)A->ell_stored, &A->device_bytes);
+      AB2_CUDA(cudaMemcpyAsync(A->d_ell_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, ctx->stream));
+      const int n_pad = ns * kEllSlice;
+      if (n_pad > n) {
+        k_ell_pad_tail<<<1, kEllSlice, 0, ctx->stream>>>(n, n_pad, A->d_ell_off, A->d_ell_ci);
+        check_launch(ctx, "ell_pad_tail");
+      }
+    }
+    if (A->formats & AB2_FMT_F32) {
+      A->d_v32 = dev_alloc<float>(nnz, &A->device_bytes);
+      if (A->formats & AB2_FMT_ELL) A->d_ell_v32 = dev_alloc<float>((size_t)A->ell_stored, &A->device_bytes);
+    }
+    refresh_values(ctx, A);
+    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+  if (rc != AB2_OK) {
+    ab2_matrix_destroy(A);
+    return rc;
+  }
+  *out = A;
+  return AB2_OK;
+}
+
+int ab2_matrix_update_values(ab2_context* ctx, ab2_matrix* A, const double* vals) {
+  if (!ctx || !A || (!vals && A->nnz)) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    AB2_CUDA(cudaMemcpyAsync(A->d_v, vals, sizeof(double) * (size_t)A->nnz, cudaMemcpyHostToDevice, ctx->stream));
+    refresh_values(ctx, A);
+  });
+}
+
+int ab2_matrix_destroy(ab2_matrix* A) {
+  if (!A) return AB2_ERR_BAD_ARG;
+  if (A->ctx) cudaStreamSynchronize(A->ctx->stream);
+  dev_free(A->d_rp);
+  dev_free(A->d_ci);
+  dev_free(A->d_v);
+  dev_free(A->d_dcol);
+  dev_free(A->d_v32);
+  dev_free(A->d_row_blocks);
+  dev_free(A->d_ell_off);
+  dev_free(A->d_ell_ci);
+  dev_free(A->d_ell_v);
+  dev_free(A->d_ell_v32);
+  delete A;
+  return AB2_OK;
+}
+
+int ab2_matrix_get_info(const ab2_matrix* A, ab2_matrix_info* info) {
+  if (!A || !info) return AB2_ERR_BAD_ARG;
+  info->n = A->n;
+  info->nnz = A->nnz;
+  info->ell_stored = A->ell_stored;
+  info->ell_slice = kEllSlice;
+  info->formats = A->formats;
+  info->device_bytes = A->device_bytes;
+  return AB2_OK;
+}
+
+int ab2_mult(ab2_context* ctx, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y) {
+  return ab2_mult_variant(ctx, A, x, y, AB2_SPMV_AUTO);
+}
+
+int ab2_mult_variant(ab2_context* ctx, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y, int variant) {
+  if (!ctx || !A || !x || !y || x->n != A->n || y->n != A->n || x->d == y->d) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_spmv(ctx, A, x->d, y->d, variant); });
+}
+
+int ab2_add_lmult(ab2_context* ctx, double alpha, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y) {
+  if (!ctx || !A || !x || !y || x->n != A->n || y->n != A->n || x->d == y->d) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_add_lu_mult(ctx, A, alpha, x->d, y->d, true); });
+}
+
+int ab2_add_umult(ab2_context* ctx, double alpha, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y) {
+  if (!ctx || !A || !x || !y || x->n != A->n || y->n != A->n || x->d == y->d) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_add_lu_mult(ctx, A, alpha, x->d, y->d, false); });
+}
+
+int ab2_compute_inv_diag(ab2_context* ctx, const ab2_matrix* A, ab2_vector* inv) {
+  if (!ctx || !A || !inv || inv->n != A->n) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_inv_diag(ctx, A, inv->d); });
+}
+
+int ab2_mult_inv_diag(ab2_context* ctx, const ab2_matrix* A, ab2_vector* y) {
+  if (!ctx || !A || !y || y->n != A->n) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_mult_inv_diag(ctx, A, y->d); });
+}
+
+int ab2_diagonal(ab2_context* ctx, const ab2_matrix* A, ab2_vector* d) {
+  if (!ctx || !A || !d || d->n != A->n) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] { op_diagonal(ctx, A, d->d); });
+}
+
+}  // extern "C"

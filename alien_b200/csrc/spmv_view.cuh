@@ -1,0 +1,78 @@
+// spmv_view.cuh -- per-row SpMV views used by the fused kernels.
+//
+// A view computes sum_k a_k x[c_k] for one row in column order, rounding as
+// the loop of SimpleCSRMatrixMultT.h:184-190 does, so a fused kernel that
+// calls it produces exactly the y of the standalone SpMV kernels.
+#pragma once
+
+#include "ab2_internal.cuh"
+
+namespace ab2 {
+
+template <class T>
+struct CsrView {
+  const int* __restrict__ rp;
+  const int* __restrict__ ci;
+  const T* __restrict__ v;
+  __device__ __forceinline__ T row(int r, const T* __restrict__ x) const {
+    T acc = 0;
+    const int e = rp[r + 1];
+    for (int k = rp[r]; k < e; ++k) acc = mul_add_rn(__ldcs(v + k), __ldg(x + __ldcs(ci + k)), acc);
+    return acc;
+  }
+};
+
+template <class T>
+struct EllView {
+  const int* __restrict__ off;
+  const int* __restrict__ ci;
+  const T* __restrict__ v;
+  __device__ __forceinline__ T row(int r, const T* __restrict__ x) const {
+    const int s = r >> 5, lane = r & 31;
+    const int o = off[s];
+    const int w = off[s + 1] - o;
+    const size_t base = (size_t)o * kEllSlice + lane;
+    const int* cp = ci + base;
+    const T* vp = v + base;
+    T acc = 0;
+    int j = 0;
+    for (; j + 8 <= w; j += 8) {
+      int c[8];
+      T a[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        c[u] = __ldcs(cp + (size_t)(j + u) * kEllSlice);
+        a[u] = __ldcs(vp + (size_t)(j + u) * kEllSlice);
+      }
+      T xv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : (T)0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (c[u] >= 0) acc = mul_add_rn(a[u], xv[u], acc);
+    }
+    for (; j < w; ++j) {
+      const int c = __ldcs(cp + (size_t)j * kEllSlice);
+      const T a = __ldcs(vp + (size_t)j * kEllSlice);
+      if (c >= 0) acc = mul_add_rn(a, __ldg(x + c), acc);
+    }
+    return acc;
+  }
+};
+
+// Calls f(view) with the view the variant selects (ELL when present, else CSR).
+template <class T, class F>
+void with_view(const ab2_matrix* A, int variant, F&& f) {
+  const bool f32 = sizeof(T) == 4;
+  const int v = resolve_variant(A, variant);
+  const T* ev = (const T*)(f32 ? (const void*)A->d_ell_v32 : (const void*)A->d_ell_v);
+  const T* cv = (const T*)(f32 ? (const void*)A->d_v32 : (const void*)A->d_v);
+  if (v == AB2_SPMV_ELL && ev) {
+    f(EllView<T>{A->d_ell_off, A->d_ell_ci, ev});
+  } else {
+    require(cv != nullptr, "matrix values missing in the requested precision");
+    f(CsrView<T>{A->d_rp, A->d_ci, cv});
+  }
+}
+
+}  // namespace ab2

@@ -1,0 +1,210 @@
+/*
+ * ab2.h -- C ABI of libab2, the B200 (sm_100a) internal linear algebra and
+ * Krylov solver backend for Alien.
+ *
+ * Every entry point takes plain pointers and sizes, returns AB2_OK (0) or a
+ * negative AB2_ERR_* code, and never lets a C++ exception cross the boundary.
+ * ab2_last_error_message() gives the text of the last failure on a context.
+ *
+ * Threading: a context owns one CUDA stream and is not thread safe; use one
+ * context per host thread.  Every call is ordered on the context's stream.
+ * Only calls that hand a value back to host memory synchronise
+ * (ab2_vector_download, ab2_dot, ab2_norm*, ab2_scalar_get, ab2_solver_solve).
+ *
+ * Reference interfaces replaced (paths are inside arcaneframework/alien):
+ *   algebra ops  src/core/alien/kernels/simple_csr/algebra/SimpleCSRInternalLinearAlgebra.h:55-173
+ *                src/core/alien/kernels/sycl/algebra/SYCLInternalLinearAlgebra.h:46-141
+ *   matrix/vec   src/core/alien/kernels/sycl/converters/SimpleCSRtoSYCLMatrixConverter.cc:74-104,
+ *                SimpleCSRtoSYCLVectorConverter.cc, SYCLtoSimpleCSRVectorConverter.cc:60-70
+ *   solvers      src/core/alien/expression/krylov/{CG.h:59-150, BiCGStab.h:152-300, Iteration.h:34-136}
+ *   precond.     src/core/alien/expression/krylov/{DiagPreconditioner.h:49-68,
+ *                ILU0Preconditioner.h:71-323, ChebyshevPreconditioner.h:73-202,392-444}
+ *   status       src/core/alien/expression/solver/ILinearSolver.h:63-83 (SolverStatus)
+ */
+#ifndef AB2_H
+#define AB2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ codes */
+#define AB2_OK 0
+#define AB2_ERR_CUDA (-1)          /* a CUDA runtime call failed */
+#define AB2_ERR_OOM (-2)           /* device or pinned allocation failed */
+#define AB2_ERR_BREAKDOWN (-3)     /* Krylov breakdown (NullValueException in CG.h/BiCGStab.h) */
+#define AB2_ERR_NOT_CONVERGED (-4) /* reserved: solves report non-convergence in ab2_status */
+#define AB2_ERR_TIMEOUT (-5)       /* a bounded device-side wait gave up */
+#define AB2_ERR_BAD_ARG (-6)       /* null handle, size mismatch, bad enum */
+#define AB2_ERR_UNSUPPORTED (-7)   /* valid request this build does not provide */
+
+/* breakdown scalar, as the string passed to NullValueException */
+#define AB2_BREAKDOWN_NONE 0
+#define AB2_BREAKDOWN_ALPHA 1
+#define AB2_BREAKDOWN_BETA 2
+#define AB2_BREAKDOWN_RHO 3
+
+/* matrix storage formats kept on the device (bit flags) */
+#define AB2_FMT_CSR 1   /* CSR, int32 columns, as SimpleCSR */
+#define AB2_FMT_ELL 2   /* sliced ELL (BEllPack) with 32-row slices */
+#define AB2_FMT_F32 4   /* additionally keep an FP32 copy of the values */
+
+/* SpMV variants (ab2_mult_variant) */
+#define AB2_SPMV_AUTO 0
+#define AB2_SPMV_CSR_SCALAR 1 /* one thread per row, values read straight from HBM */
+#define AB2_SPMV_CSR_STAGED 2 /* row blocks staged through shared memory */
+#define AB2_SPMV_ELL 3        /* sliced ELL, one thread per row, coalesced slots */
+
+/* solvers / preconditioners (same names as the krylov example's options) */
+#define AB2_SOLVER_CG 0
+#define AB2_SOLVER_BICGSTAB 1
+
+#define AB2_PC_NONE 0
+#define AB2_PC_DIAG 1
+#define AB2_PC_ILU0 2
+#define AB2_PC_CHEB 3
+
+/* ------------------------------------------------------------------ handles */
+typedef struct ab2_context ab2_context;
+typedef struct ab2_matrix ab2_matrix;
+typedef struct ab2_vector ab2_vector;
+typedef struct ab2_precond ab2_precond;
+typedef struct ab2_solver ab2_solver;
+
+/* ------------------------------------------------------------------ context */
+int ab2_context_create(int device, ab2_context** ctx);
+int ab2_context_destroy(ab2_context* ctx);
+const char* ab2_last_error_message(const ab2_context* ctx);
+/* cudaStream_t of the context, for callers that record events on it */
+int ab2_context_stream(const ab2_context* ctx, void** stream);
+int ab2_synchronize(ab2_context* ctx);
+/* number of kernels libab2 has launched on this context since creation */
+int ab2_context_launch_count(const ab2_context* ctx, long long* count);
+
+/* ------------------------------------------------------------------ matrix */
+/* Copies a host CSR matrix (columns sorted ascending inside each row, as
+ * Alien's profilers produce) to the device in the requested formats.
+ * The caller keeps ownership of the host arrays. */
+int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int* cols, const double* vals,
+                          int formats, ab2_matrix** mat);
+/* New values for the same profile (row_ptr[n] doubles). */
+int ab2_matrix_update_values(ab2_context* ctx, ab2_matrix* mat, const double* vals);
+int ab2_matrix_destroy(ab2_matrix* mat);
+
+typedef struct {
+  int n;
+  long long nnz;
+  long long ell_stored; /* slots in the sliced-ELL arrays, padding included (0 if absent) */
+  int ell_slice;        /* rows per slice (32) */
+  int formats;          /* AB2_FMT_* present */
+  long long device_bytes;
+} ab2_matrix_info;
+int ab2_matrix_get_info(const ab2_matrix* mat, ab2_matrix_info* info);
+
+/* ------------------------------------------------------------------ vector */
+int ab2_vector_create(ab2_context* ctx, int n, ab2_vector** vec);
+int ab2_vector_destroy(ab2_vector* vec);
+int ab2_vector_size(const ab2_vector* vec, int* n);
+int ab2_vector_upload(ab2_context* ctx, ab2_vector* vec, const double* host);
+int ab2_vector_download(ab2_context* ctx, const ab2_vector* vec, double* host);
+/* raw device pointer (double*) of the vector's storage */
+int ab2_vector_device_ptr(const ab2_vector* vec, void** dptr);
+
+/* ------------------------------------------------------------------ algebra
+ * Method-for-method the IInternalLinearAlgebra surface of SimpleCSR/SYCL.
+ * All FP64.  Vector arguments must all have the matrix's row count. */
+int ab2_mult(ab2_context* ctx, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y);         /* y = A x */
+int ab2_mult_variant(ab2_context* ctx, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y, int variant);
+int ab2_add_lmult(ab2_context* ctx, double alpha, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y); /* y += a L x */
+int ab2_add_umult(ab2_context* ctx, double alpha, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y); /* y += a U x */
+int ab2_compute_inv_diag(ab2_context* ctx, const ab2_matrix* A, ab2_vector* inv_diag);           /* d = 1/a_ii */
+int ab2_mult_inv_diag(ab2_context* ctx, const ab2_matrix* A, ab2_vector* y);                      /* y = y / a_ii */
+int ab2_axpy(ab2_context* ctx, double alpha, const ab2_vector* x, ab2_vector* y);                  /* y += a x */
+int ab2_aypx(ab2_context* ctx, double alpha, ab2_vector* y, const ab2_vector* x);                  /* y = a y + x */
+int ab2_copy(ab2_context* ctx, const ab2_vector* x, ab2_vector* y);                                /* y = x */
+int ab2_scal(ab2_context* ctx, double alpha, ab2_vector* x);                                       /* x = a x */
+int ab2_pointwise_mult(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, ab2_vector* w); /* w = x.y */
+int ab2_assign(ab2_context* ctx, ab2_vector* x, double alpha);                                     /* x = a */
+int ab2_diagonal(ab2_context* ctx, const ab2_matrix* A, ab2_vector* d);                            /* d = a_ii */
+int ab2_reciprocal(ab2_context* ctx, ab2_vector* x);                                               /* x = 1/x */
+/* reductions: result copied to host (synchronises) */
+int ab2_dot(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, double* result);
+int ab2_norm0(ab2_context* ctx, const ab2_vector* x, double* result); /* max |x_i| */
+int ab2_norm1(ab2_context* ctx, const ab2_vector* x, double* result); /* sum |x_i| */
+int ab2_norm2(ab2_context* ctx, const ab2_vector* x, double* result); /* sqrt(x.x) */
+
+/* Device scalars: the "future" form of dot (SimpleCSRInternalLinearAlgebra.h:74-98).
+ * ab2_dot_async enqueues x.y into a device slot without synchronising;
+ * ab2_scalar_get waits for it. */
+typedef struct ab2_scalar ab2_scalar;
+int ab2_scalar_create(ab2_context* ctx, ab2_scalar** s);
+int ab2_scalar_destroy(ab2_scalar* s);
+int ab2_dot_async(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, ab2_scalar* result);
+int ab2_scalar_get(ab2_context* ctx, const ab2_scalar* s, double* value);
+
+/* ------------------------------------------------------------------ preconditioners */
+typedef struct {
+  int kind;                 /* AB2_PC_* */
+  double poly_factor;       /* Chebyshev: 0 = both bounds by power method; else alpha = beta/factor */
+  int poly_order;           /* Chebyshev polynomial order (3 = three SpMVs per application) */
+  int poly_factor_max_iter; /* Chebyshev: power-method steps per bound */
+} ab2_precond_options;
+
+/* init(): Diag computes 1/a_ii; ILU0 factorises on the device; Chebyshev
+ * estimates its bounds.  The matrix must outlive the preconditioner. */
+int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_options* opts, ab2_precond** pc);
+int ab2_precond_apply(ab2_context* ctx, const ab2_precond* pc, const ab2_vector* x, ab2_vector* y); /* y = M^-1 x */
+int ab2_precond_destroy(ab2_precond* pc);
+
+typedef struct {
+  int kind;
+  double cheb_alpha; /* lower bound used by Chebyshev */
+  double cheb_beta;  /* upper bound used by Chebyshev */
+  int ilu_levels_lower; /* wavefronts of the L sweep */
+  int ilu_levels_upper; /* wavefronts of the U sweep */
+} ab2_precond_info;
+int ab2_precond_get_info(const ab2_precond* pc, ab2_precond_info* info);
+/* ILU(0) factor values in CSR order (row_ptr[n] doubles), for checking. */
+int ab2_precond_ilu0_values(ab2_context* ctx, const ab2_precond* pc, double* lu);
+
+/* ------------------------------------------------------------------ solver */
+typedef struct {
+  int solver;   /* AB2_SOLVER_* */
+  int precond;  /* AB2_PC_* */
+  double tol;   /* stop when r.r < tol^2 b.b (recursive residual, Iteration.h:83-90) */
+  int max_iter;
+  double poly_factor;
+  int poly_order;
+  int poly_factor_max_iter;
+  int spmv_variant; /* AB2_SPMV_* used inside the loop */
+  int use_graph;    /* 1: iteration loop in a CUDA graph with a device-side while condition */
+} ab2_solver_options;
+
+typedef struct {
+  int succeeded;          /* Iteration::getStatus() */
+  int iterations;         /* Iteration::operator()() */
+  int error;              /* AB2_OK, AB2_ERR_BREAKDOWN, AB2_ERR_TIMEOUT */
+  int breakdown;          /* AB2_BREAKDOWN_* */
+  double residual;        /* sqrt(last stop value / b.b): recursive relative residual */
+  double true_residual;   /* ||b - A x|| / ||b|| recomputed after the solve */
+  double nrm2_b;          /* b.b */
+  double setup_ms;        /* preconditioner init + graph build of the last ab2_solver_create */
+  double solve_ms;        /* device time of the last solve */
+} ab2_status;
+
+void ab2_solver_options_default(ab2_solver_options* opts);
+int ab2_solver_create(ab2_context* ctx, const ab2_matrix* A, const ab2_solver_options* opts, ab2_solver** s);
+/* x holds the initial guess on entry, the solution on exit. */
+int ab2_solver_solve(ab2_solver* s, const ab2_vector* b, ab2_vector* x, ab2_status* status);
+/* residual history: the stop test's r.r values of the last solve */
+int ab2_solver_history(const ab2_solver* s, double* hist, int cap, int* len);
+int ab2_solver_destroy(ab2_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AB2_H */

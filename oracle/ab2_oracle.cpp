@@ -1,0 +1,562 @@
+// ab2_oracle.cpp -- CPU oracle for the alien-b200 hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the checker: it is loaded by the
+// tests, by __graft_entry__.smoke() and by bench.py's cpu_baseline leg, and by
+// nothing else.  The product (libab2) never links or calls it.
+//
+// It restates, sequentially and in plain C++, the arithmetic of Alien's
+// SimpleCSR internal algebra and of the header-only Krylov templates:
+//
+//   SpMV            src/core/alien/kernels/simple_csr/algebra/SimpleCSRMatrixMultT.h:172-191
+//   addL/UMult      SimpleCSRMatrixMultT.h:193-233
+//   invdiag         SimpleCSRMatrixMultT.h:494-509, dcol from CSRStructInfo.h:291-309
+//   BLAS-1          src/core/alien/kernels/simple_csr/algebra/CBLASMPIKernel.h:37-125
+//                   (norm2 = sqrt(dot), SimpleCSRInternalLinearAlgebra.cc:102-108)
+//   Iteration       src/core/alien/expression/krylov/Iteration.h:44-90
+//   CG              src/core/alien/expression/krylov/CG.h:59-150
+//   BiCGStab        src/core/alien/expression/krylov/BiCGStab.h:45-136 (its Iteration), 152-300
+//   Diag            src/core/alien/expression/krylov/DiagPreconditioner.h:49-68
+//   ILU0            src/core/alien/expression/krylov/ILU0Preconditioner.h:71-248 (sequential branch)
+//   Chebyshev       src/core/alien/expression/krylov/ChebyshevPreconditioner.h:73-202, 392-434
+//   BEllPack layout src/core/alien/kernels/sycl/data/SYCLBEllPackMatrix.cc:70-88 (slice S)
+//
+// Floating-point conventions (the GPU path follows the same ones, so it can
+// match bit for bit wherever the reference's own order is sequential):
+//   * loops written in Alien's sources as `a += b*c` / `a -= b*c` (SpMV,
+//     addL/UMult, ILU0 factorisation and sweeps) round the product and the sum
+//     separately: that is how the stock build compiles them (ISO -std=c++17
+//     turns contraction off; without -march there is no FMA anyway).  The
+//     reference templates built by oracle/Makefile confirm it bit for bit;
+//   * BLAS-1 (cblas_daxpy etc.) is one fma per element, as CBLAS kernels on
+//     FMA hardware compute it;
+//   * dot products sum sequentially with fma, which is one admissible order of
+//     cblas_ddot; the GPU uses a fixed tree, so dots agree to rounding only.
+// The file is compiled with -ffp-contract=off so that only explicit std::fma
+// calls fuse.
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <vector>
+#include <algorithm>
+
+#include "simplecsr_kernels.h"
+
+extern "C" {
+
+// Codes shared with include/ab2.h (same numeric values).
+enum {
+  ORC_OK = 0,
+  ORC_ERR_BREAKDOWN = -3,
+  ORC_ERR_BAD_ARG = -6,
+};
+enum { ORC_SOLVER_CG = 0, ORC_SOLVER_BICGSTAB = 1 };
+enum { ORC_PC_NONE = 0, ORC_PC_DIAG = 1, ORC_PC_ILU0 = 2, ORC_PC_CHEB = 3 };
+// Which scalar broke down (the string passed to NullValueException).
+enum { ORC_BD_NONE = 0, ORC_BD_ALPHA = 1, ORC_BD_BETA = 2, ORC_BD_RHO = 3 };
+
+typedef struct {
+  int solver;               // ORC_SOLVER_*
+  int precond;              // ORC_PC_*
+  double tol;
+  int max_iter;
+  double poly_factor;       // Chebyshev "factor" (0 = computed bounds)
+  int poly_order;           // Chebyshev polynomial order
+  int poly_factor_max_iter; // power-method steps for each bound
+} orc_options;
+
+typedef struct {
+  int iterations;        // Iteration::operator()()
+  int converged;         // Iteration::getStatus()
+  int error;             // ORC_OK or ORC_ERR_BREAKDOWN
+  int breakdown;         // ORC_BD_*
+  double nrm2_b;         // b.b
+  double last_rr;        // last value the stop test compared (r.r or s.s)
+  double cheb_alpha;     // Chebyshev bounds actually used
+  double cheb_beta;
+  int history_len;       // entries written into hist
+} orc_result;
+
+}  // extern "C"
+
+namespace {
+
+using namespace ab2_oracle;
+
+// Stop test shared by CG (Iteration.h) and BiCGStab (its nested Iteration).
+struct StopTest {
+  int n;
+  int max_iter;
+  int iter = 0;
+  double criteria;
+  double nrm2_b;
+  bool status = false;
+  double last = 0.0;
+  double* hist;
+  int hist_cap;
+  int hist_len = 0;
+
+  StopTest(int n_, const double* b, double tol, int max_it, double* h, int cap)
+      : n(n_), max_iter(max_it), hist(h), hist_cap(cap) {
+    nrm2_b = dot(n, b, b);
+    criteria = tol * tol * nrm2_b;
+    status = (nrm2_b == 0.0);
+  }
+  bool null_rhs() const { return nrm2_b == 0.0; }
+  bool stop(const double* r) {
+    if (iter >= max_iter) return true;
+    last = dot(n, r, r);
+    if (hist && hist_len < hist_cap) hist[hist_len] = last;
+    ++hist_len;
+    status = last < criteria;
+    return status;
+  }
+  void next() { ++iter; }
+};
+
+struct Breakdown {
+  int which;
+};
+
+// ---------------------------------------------------------------- preconditioners
+struct Precond {
+  virtual ~Precond() {}
+  virtual void apply(const double* x, double* y) = 0;
+};
+
+struct Identity : Precond {
+  int n;
+  explicit Identity(int n_) : n(n_) {}
+  void apply(const double* x, double* y) override { copy(n, x, y); }
+};
+
+struct Diag : Precond {
+  int n;
+  std::vector<double> inv;
+  explicit Diag(const Csr& A) : n(A.n), inv(A.n, 1.0) {
+    std::vector<int> d = diag_offsets(A);
+    for (int i = 0; i < n; ++i) inv[i] = 1.0 / A.v[d[i]];
+  }
+  void apply(const double* x, double* y) override { pmult(n, inv.data(), x, y); }
+};
+
+// In-place IKJ ILU(0) on a copy of the values (ILU0Preconditioner.h:156-178),
+// then the forward/backward sweeps of solveL/solveU (:181-231).
+struct Ilu0 : Precond {
+  int n;
+  const int* rp;
+  const int* ci;
+  std::vector<int> d;
+  std::vector<double> lu;
+  std::vector<double> tmp;
+
+  explicit Ilu0(const Csr& A) : n(A.n), rp(A.rp), ci(A.ci), lu(A.v, A.v + A.rp[A.n]), tmp(A.n) {
+    d = diag_offsets(A);
+    std::vector<int> work(n, -1);
+    for (int i = 1; i < n; ++i) {
+      for (int k = rp[i]; k < d[i]; ++k) {
+        const int kr = ci[k];
+        const double aik = lu[k] / lu[d[kr]];
+        lu[k] = aik;
+        for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = l;
+        for (int j = k + 1; j < rp[i + 1]; ++j) {
+          const int kj = work[ci[j]];
+          if (kj != -1) lu[j] = lu[j] - aik * lu[kj];
+        }
+        for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = -1;
+      }
+    }
+  }
+  void solve_l(const double* y, double* x) const {
+    for (int i = 0; i < n; ++i) {
+      double v = y[i];
+      for (int k = rp[i]; k < d[i]; ++k) v = v - lu[k] * x[ci[k]];
+      x[i] = v;
+    }
+  }
+  void solve_u(const double* y, double* x) const {
+    for (int i = n - 1; i >= 0; --i) {
+      const int dk = d[i];
+      double v = y[i];
+      for (int k = dk + 1; k < rp[i + 1]; ++k) v = v - lu[k] * x[ci[k]];
+      x[i] = v / lu[dk];
+    }
+  }
+  void apply(const double* y, double* x) override {
+    solve_l(y, tmp.data());
+    solve_u(tmp.data(), x);
+  }
+};
+
+// Chebyshev polynomial preconditioner, non-Saad branch (_algo2).
+struct Cheb : Precond {
+  const Csr A;
+  int n;
+  int order;
+  std::vector<double> inv, y_, r_, p_, z_;
+  double alpha = 0.0, beta = 0.0;
+
+  Cheb(const Csr& A_, double factor, int order_, int max_iter)
+      : A(A_), n(A_.n), order(order_), inv(A_.n, 1.0), y_(A_.n, 0.0), r_(A_.n, 0.0), p_(A_.n, 0.0),
+        z_(A_.n, 0.0) {
+    std::vector<int> d = diag_offsets(A);
+    for (int i = 0; i < n; ++i) inv[i] = 1.0 / A.v[d[i]];
+    beta = power_bound(max_iter, /*shift=*/false, 0.0);
+    alpha = power_bound(max_iter, /*shift=*/true, beta);
+    if (factor != 0.0) alpha = beta / factor;
+  }
+
+  // computeBeta (:118-156) when shift is false, computeAlpha (:158-202) otherwise.
+  // Both draw their start vector from a default-constructed std::mt19937 with
+  // U(-1,1) in index order, which makes them deterministic.
+  double power_bound(int max_iter, bool shift, double b) {
+    std::vector<double> x(n);
+    std::mt19937 gen;
+    std::uniform_real_distribution<> dis(-1., 1.);
+    for (int i = 0; i < n; ++i) x[i] = dis(gen);
+    double nrm = std::sqrt(dot(n, x.data(), x.data()));
+    scal(n, 1 / nrm, x.data());
+    double est = 0.0;
+    for (int it = 0; it < max_iter; ++it) {
+      spmv(A, x.data(), y_.data());
+      pmult(n, inv.data(), y_.data(), y_.data());
+      if (shift) axpy(n, -b, x.data(), y_.data());
+      const double xax = dot(n, y_.data(), x.data());
+      const double xdx = dot(n, x.data(), x.data());
+      est = xax / xdx;
+      const double nr = std::sqrt(dot(n, y_.data(), y_.data()));
+      scal(n, 1 / nr, y_.data());
+      copy(n, y_.data(), x.data());
+    }
+    if (shift) est += b;
+    return est;
+  }
+
+  void apply(const double* x, double* y) override {
+    const double dd = (beta + alpha) / 2;
+    const double c = (beta - alpha) / 2;
+    copy(n, x, y);
+    spmv(A, y, y_.data());
+    copy(n, x, r_.data());
+    axpy(n, -1., y_.data(), r_.data());
+    pmult(n, inv.data(), r_.data(), z_.data());
+    copy(n, z_.data(), p_.data());
+    double a = 2 / dd;
+    axpy(n, a, p_.data(), y);
+    for (int i = 1; i < order; ++i) {
+      spmv(A, y, y_.data());
+      copy(n, x, r_.data());
+      axpy(n, -1., y_.data(), r_.data());
+      pmult(n, inv.data(), r_.data(), z_.data());
+      const double bcoef = a * (c / 2.) * (c / 2.);
+      a = 1. / (dd - bcoef);
+      scal(n, bcoef, p_.data());
+      axpy(n, 1., z_.data(), p_.data());
+      axpy(n, a, p_.data(), y);
+    }
+  }
+};
+
+// ---------------------------------------------------------------- solvers
+void cg(const Csr& A, Precond& M, StopTest& it, const double* b, double* x) {
+  if (it.null_rhs()) return;
+  const int n = A.n;
+  std::vector<double> p(n), z(n), q(n), r(n);
+  double rho = 0, rho1 = 0, alpha = 0;
+  copy(n, b, r.data());
+  spmv(A, x, p.data());
+  axpy(n, -1., p.data(), r.data());
+
+  M.apply(r.data(), z.data());
+  rho1 = dot(n, r.data(), z.data());
+  copy(n, z.data(), p.data());
+  spmv(A, p.data(), q.data());
+  alpha = dot(n, p.data(), q.data());
+  if (alpha == 0) {
+    if (it.stop(r.data())) { it.next(); return; }
+    throw Breakdown{ORC_BD_ALPHA};
+  }
+  alpha = rho1 / alpha;
+  axpy(n, alpha, p.data(), x);
+  axpy(n, -alpha, q.data(), r.data());
+  rho = rho1;
+  it.next();
+
+  while (!it.stop(r.data())) {
+    M.apply(r.data(), z.data());
+    rho1 = dot(n, r.data(), z.data());
+    alpha = rho1 / rho;
+    axpy(n, alpha, p.data(), z.data());
+    copy(n, z.data(), p.data());
+    spmv(A, p.data(), q.data());
+    alpha = dot(n, q.data(), p.data());
+    if (alpha == 0) {
+      if (it.stop(r.data())) { it.next(); return; }
+      throw Breakdown{ORC_BD_ALPHA};
+    }
+    alpha = rho1 / alpha;
+    axpy(n, alpha, p.data(), x);
+    axpy(n, -alpha, q.data(), r.data());
+    rho = rho1;
+    it.next();
+  }
+}
+
+void bicgstab(const Csr& A, Precond& M, StopTest& it, const double* b, double* x) {
+  if (it.null_rhs()) return;
+  const int n = A.n;
+  std::vector<double> p(n), phat(n), s(n), shat(n), t(n), v(n), r(n), r0(n);
+  double rho = 0, rho1 = 0, alpha = 0, beta = 0, omega = 0;
+
+  copy(n, b, r.data());
+  spmv(A, x, r0.data());
+  axpy(n, -1., r0.data(), r.data());
+  copy(n, r.data(), r0.data());
+  copy(n, r.data(), p.data());
+  rho1 = dot(n, r.data(), r0.data());
+
+  M.apply(p.data(), phat.data());
+  spmv(A, phat.data(), v.data());
+  alpha = dot(n, v.data(), r0.data());
+  if (alpha == 0) throw Breakdown{ORC_BD_ALPHA};
+  alpha = rho1 / alpha;
+  copy(n, r.data(), s.data());
+  axpy(n, -alpha, v.data(), s.data());
+
+  if (it.stop(s.data())) {
+    it.next();
+    axpy(n, alpha, phat.data(), x);
+    return;
+  }
+
+  M.apply(s.data(), shat.data());
+  spmv(A, shat.data(), t.data());
+  omega = dot(n, t.data(), s.data());
+  beta = dot(n, t.data(), t.data());
+  if (beta == 0) {
+    if (it.stop(r.data())) {
+      it.next();
+      axpy(n, alpha, phat.data(), x);
+      return;
+    }
+    throw Breakdown{ORC_BD_BETA};
+  }
+  omega = omega / beta;
+  axpy(n, omega, shat.data(), x);
+  axpy(n, alpha, phat.data(), x);
+  copy(n, s.data(), r.data());
+  axpy(n, -omega, t.data(), r.data());
+  rho = rho1;
+  it.next();
+
+  while (!it.stop(r.data())) {
+    rho1 = dot(n, r.data(), r0.data());
+    beta = (rho1 / rho) * (alpha / omega);
+    axpy(n, -omega, v.data(), p.data());
+    scal(n, beta, p.data());
+    axpy(n, 1., r.data(), p.data());
+    if (rho == 0) throw Breakdown{ORC_BD_RHO};
+
+    M.apply(p.data(), phat.data());
+    spmv(A, phat.data(), v.data());
+    alpha = dot(n, v.data(), r0.data());
+    if (alpha == 0) throw Breakdown{ORC_BD_ALPHA};
+    alpha = rho1 / alpha;
+    copy(n, r.data(), s.data());
+    axpy(n, -alpha, v.data(), s.data());
+    // Early exit on ||s|| without ++iter (BiCGStab.h:259-263).
+    if (it.stop(s.data())) {
+      axpy(n, alpha, phat.data(), x);
+      return;
+    }
+
+    M.apply(s.data(), shat.data());
+    spmv(A, shat.data(), t.data());
+    omega = dot(n, t.data(), s.data());
+    beta = dot(n, t.data(), t.data());
+    if (beta == 0) {
+      if (it.stop(s.data())) {
+        axpy(n, alpha, phat.data(), x);
+        return;
+      }
+      throw Breakdown{ORC_BD_BETA};
+    }
+    omega = omega / beta;
+    axpy(n, omega, shat.data(), x);
+    axpy(n, alpha, phat.data(), x);
+    copy(n, s.data(), r.data());
+    axpy(n, -omega, t.data(), r.data());
+    rho = rho1;
+    it.next();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_spmv(int n, const int* rp, const int* ci, const double* v, const double* x, double* y) {
+  if (n < 0) return ORC_ERR_BAD_ARG;
+  spmv(Csr{n, rp, ci, v}, x, y);
+  return ORC_OK;
+}
+
+// y += alpha * (strict lower part of A) x   (SimpleCSRMatrixMultT.h:193-212)
+int orc_add_lmult(int n, const int* rp, const int* ci, const double* v, double alpha, const double* x,
+                  double* y) {
+  Csr A{n, rp, ci, v};
+  std::vector<int> d = diag_offsets(A);
+  for (int i = 0; i < n; ++i) {
+    double acc = y[i];
+    for (int k = rp[i]; k < d[i]; ++k) acc = acc + alpha * v[k] * x[ci[k]];
+    y[i] = acc;
+  }
+  return ORC_OK;
+}
+
+// y += alpha * (strict upper part of A) x   (SimpleCSRMatrixMultT.h:214-233)
+int orc_add_umult(int n, const int* rp, const int* ci, const double* v, double alpha, const double* x,
+                  double* y) {
+  Csr A{n, rp, ci, v};
+  std::vector<int> d = diag_offsets(A);
+  for (int i = 0; i < n; ++i) {
+    double acc = y[i];
+    for (int k = d[i] + 1; k < rp[i + 1]; ++k) acc = acc + alpha * v[k] * x[ci[k]];
+    y[i] = acc;
+  }
+  return ORC_OK;
+}
+
+int orc_diag_offsets(int n, const int* rp, const int* ci, int* dcol) {
+  std::vector<int> d = diag_offsets(Csr{n, rp, ci, nullptr});
+  std::copy(d.begin(), d.end(), dcol);
+  return ORC_OK;
+}
+
+int orc_inv_diag(int n, const int* rp, const int* ci, const double* v, double* inv) {
+  Csr A{n, rp, ci, v};
+  std::vector<int> d = diag_offsets(A);
+  for (int i = 0; i < n; ++i) inv[i] = 1. / v[d[i]];
+  return ORC_OK;
+}
+
+double orc_dot(int n, const double* x, const double* y) { return dot(n, x, y); }
+
+// y += a x (cblas_daxpy, CBLASMPIKernel.h:48-53)
+int orc_axpy(int n, double a, const double* x, double* y) {
+  axpy(n, a, x, y);
+  return ORC_OK;
+}
+
+// y = a y + x, one fma per element (the aypx the algebra interface names)
+int orc_aypx(int n, double a, double* y, const double* x) {
+  for (int i = 0; i < n; ++i) y[i] = std::fma(a, y[i], x[i]);
+  return ORC_OK;
+}
+
+// ILU(0) factor values, written into lu (nnz entries).
+int orc_ilu0_factor(int n, const int* rp, const int* ci, const double* v, double* lu) {
+  Ilu0 f(Csr{n, rp, ci, v});
+  std::copy(f.lu.begin(), f.lu.end(), lu);
+  return ORC_OK;
+}
+
+int orc_ilu0_apply(int n, const int* rp, const int* ci, const double* v, const double* y, double* x) {
+  Ilu0 f(Csr{n, rp, ci, v});
+  f.apply(y, x);
+  return ORC_OK;
+}
+
+// Chebyshev bounds (alpha = lambda_min estimate, beta = lambda_max estimate).
+int orc_cheb_bounds(int n, const int* rp, const int* ci, const double* v, double factor, int max_iter,
+                    double* alpha, double* beta) {
+  Cheb c(Csr{n, rp, ci, v}, factor, 1, max_iter);
+  *alpha = c.alpha;
+  *beta = c.beta;
+  return ORC_OK;
+}
+
+int orc_cheb_apply(int n, const int* rp, const int* ci, const double* v, double factor, int order,
+                   int max_iter, const double* x, double* y) {
+  Cheb c(Csr{n, rp, ci, v}, factor, order, max_iter);
+  c.apply(x, y);
+  return ORC_OK;
+}
+
+// Full solve: x holds the initial guess on entry and the solution on exit.
+// hist (optional, hist_cap entries) receives every value the stop test compares.
+int orc_solve(int n, const int* rp, const int* ci, const double* v, const double* b, double* x,
+              const orc_options* o, orc_result* res, double* hist, int hist_cap) {
+  if (!o || !res || n < 0) return ORC_ERR_BAD_ARG;
+  std::memset(res, 0, sizeof(*res));
+  Csr A{n, rp, ci, v};
+  Identity pid(n);
+  Diag* pd = nullptr;
+  Ilu0* pi = nullptr;
+  Cheb* pc = nullptr;
+  Precond* M = &pid;
+  switch (o->precond) {
+    case ORC_PC_NONE: break;
+    case ORC_PC_DIAG: M = pd = new Diag(A); break;
+    case ORC_PC_ILU0: M = pi = new Ilu0(A); break;
+    case ORC_PC_CHEB:
+      M = pc = new Cheb(A, o->poly_factor, o->poly_order, o->poly_factor_max_iter);
+      res->cheb_alpha = pc->alpha;
+      res->cheb_beta = pc->beta;
+      break;
+    default: return ORC_ERR_BAD_ARG;
+  }
+  StopTest it(n, b, o->tol, o->max_iter, hist, hist_cap);
+  int rc = ORC_OK;
+  try {
+    if (o->solver == ORC_SOLVER_CG) cg(A, *M, it, b, x);
+    else if (o->solver == ORC_SOLVER_BICGSTAB) bicgstab(A, *M, it, b, x);
+    else rc = ORC_ERR_BAD_ARG;
+  } catch (const Breakdown& e) {
+    rc = ORC_ERR_BREAKDOWN;
+    res->breakdown = e.which;
+  }
+  res->iterations = it.iter;
+  res->converged = it.status ? 1 : 0;
+  res->error = rc;
+  res->nrm2_b = it.nrm2_b;
+  res->last_rr = it.last;
+  res->history_len = it.hist_len;
+  delete pd;
+  delete pi;
+  delete pc;
+  return rc;
+}
+
+// BEllPack layout with slice S (SYCLBEllPackMatrix.cc:70-88 computes the slice
+// widths; the value at (slice s, slot j, lane l) lives at off[s]*S + j*S + l,
+// padding uses column 0 and value 0).
+int orc_ell_layout(int n, const int* rp, const int* ci, const double* v, int S, int* slice_off,
+                   int* ell_cols, double* ell_vals) {
+  const int ns = (n + S - 1) / S;
+  int off = 0;
+  for (int s = 0; s < ns; ++s) {
+    slice_off[s] = off;
+    int w = 0;
+    for (int l = 0; l < S && s * S + l < n; ++l) w = std::max(w, rp[s * S + l + 1] - rp[s * S + l]);
+    off += w;
+  }
+  slice_off[ns] = off;
+  if (!ell_cols) return ORC_OK;
+  for (int s = 0; s < ns; ++s) {
+    const int w = slice_off[s + 1] - slice_off[s];
+    for (int l = 0; l < S; ++l) {
+      const int row = s * S + l;
+      const int len = row < n ? rp[row + 1] - rp[row] : 0;
+      for (int j = 0; j < w; ++j) {
+        const size_t at = (size_t)slice_off[s] * S + (size_t)j * S + l;
+        ell_cols[at] = j < len ? ci[rp[row] + j] : 0;
+        ell_vals[at] = j < len ? v[rp[row] + j] : 0.0;
+      }
+    }
+  }
+  return ORC_OK;
+}
+
+}  // extern "C"

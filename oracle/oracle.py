@@ -1,0 +1,239 @@
+"""CPU oracle loader -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs import
+this module.  It wraps two shared libraries built by oracle/Makefile:
+
+* ``_build/libab2_oracle.so`` -- this repo's sequential restatement of Alien's
+  SimpleCSR algebra and Krylov templates (ab2_oracle.cpp, citations there);
+* ``_ref/libalien_ref.so`` -- Alien's OWN header-only Krylov templates
+  (CG.h, BiCGStab.h, Iteration.h, Diag/ILU0/Chebyshev preconditioners)
+  compiled from the reference sources over a SimpleCSR-restating CPU algebra
+  (ref/ref_driver.cpp).  It pins the restatement: the tests require both to
+  agree result for result.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "libab2_oracle.so"
+REF_SO = HERE / "_ref" / "libalien_ref.so"
+
+SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
+PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3}
+BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho", 9: "other"}
+
+
+class Options(C.Structure):
+    _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
+                ("poly_factor", C.c_double), ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("error", C.c_int), ("breakdown", C.c_int),
+                ("nrm2_b", C.c_double), ("last_rr", C.c_double), ("cheb_alpha", C.c_double),
+                ("cheb_beta", C.c_double), ("history_len", C.c_int)]
+
+
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+
+
+def build() -> None:
+    """Builds the oracle (and the reference-template library when the
+    reference sources are present)."""
+    subprocess.run(["make", "-s", "-f", str(HERE / "Makefile")], check=True)
+
+
+def _load(path: Path, prefix: str) -> C.CDLL:
+    if not path.exists():
+        raise ImportError(f"{path} missing: run make -f oracle/Makefile")
+    L = C.CDLL(str(path))
+    f = getattr(L, f"{prefix}_solve")
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, _IP, _IP, _DP, _DP, _DP, C.POINTER(Options), C.POINTER(Result), _DP, C.c_int]
+    for name in ("ilu0_factor",):
+        g = getattr(L, f"{prefix}_{name}")
+        g.restype = C.c_int
+        g.argtypes = [C.c_int, _IP, _IP, _DP, _DP]
+    g = getattr(L, f"{prefix}_ilu0_apply")
+    g.restype = C.c_int
+    g.argtypes = [C.c_int, _IP, _IP, _DP, _DP, _DP]
+    g = getattr(L, f"{prefix}_cheb_apply")
+    g.restype = C.c_int
+    g.argtypes = [C.c_int, _IP, _IP, _DP, C.c_double, C.c_int, C.c_int, _DP, _DP]
+    return L
+
+
+_orc = None
+_ref = None
+
+
+def orc() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        L = _load(ORACLE_SO, "orc")
+        L.orc_spmv.argtypes = [C.c_int, _IP, _IP, _DP, _DP, _DP]
+        L.orc_add_lmult.argtypes = [C.c_int, _IP, _IP, _DP, C.c_double, _DP, _DP]
+        L.orc_add_umult.argtypes = [C.c_int, _IP, _IP, _DP, C.c_double, _DP, _DP]
+        L.orc_diag_offsets.argtypes = [C.c_int, _IP, _IP, _IP]
+        L.orc_inv_diag.argtypes = [C.c_int, _IP, _IP, _DP, _DP]
+        L.orc_dot.argtypes = [C.c_int, _DP, _DP]
+        L.orc_dot.restype = C.c_double
+        L.orc_axpy.argtypes = [C.c_int, C.c_double, _DP, _DP]
+        L.orc_aypx.argtypes = [C.c_int, C.c_double, _DP, _DP]
+        L.orc_cheb_bounds.argtypes = [C.c_int, _IP, _IP, _DP, C.c_double, C.c_int, _DP, _DP]
+        L.orc_ell_layout.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, _IP, _IP, _DP]
+        _orc = L
+    return _orc
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        _ref = _load(REF_SO, "ref")
+    return _ref
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_IP)
+
+
+@dataclass
+class OracleSolve:
+    x: np.ndarray
+    iterations: int
+    converged: bool
+    error: int
+    breakdown: str | None
+    nrm2_b: float
+    last_rr: float
+    cheb_alpha: float
+    cheb_beta: float
+    history: np.ndarray
+
+    @property
+    def residual(self) -> float:
+        return float(np.sqrt(self.last_rr / self.nrm2_b)) if self.nrm2_b > 0 else 0.0
+
+
+def solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8, max_iter=1000, poly_factor=0.0,
+          poly_order=3, poly_factor_max_iter=10, which="oracle") -> OracleSolve:
+    """Runs the restatement (which='oracle') or the reference templates (which='ref')."""
+    rp, ci, v, bb = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(b, np.float64)
+    n = rp.size - 1
+    x = np.zeros(n) if x0 is None else _c(x0, np.float64).copy()
+    o = Options(SOLVER[solver], PRECOND[precond], tol, max_iter, poly_factor, poly_order, poly_factor_max_iter)
+    r = Result()
+    cap = 2 * max_iter + 8
+    hist = np.zeros(cap)
+    L = orc() if which == "oracle" else ref()
+    fn = L.orc_solve if which == "oracle" else L.ref_solve
+    fn(n, _ip(rp), _ip(ci), _dp(v), _dp(bb), _dp(x), C.byref(o), C.byref(r), _dp(hist), cap)
+    return OracleSolve(x, r.iterations, bool(r.converged), r.error, BREAKDOWN.get(r.breakdown), r.nrm2_b, r.last_rr,
+                       r.cheb_alpha, r.cheb_beta, hist[:min(r.history_len, cap)].copy())
+
+
+def spmv(row_ptr, cols, vals, x) -> np.ndarray:
+    rp, ci, v, xx = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(x, np.float64)
+    y = np.empty(rp.size - 1)
+    orc().orc_spmv(rp.size - 1, _ip(rp), _ip(ci), _dp(v), _dp(xx), _dp(y))
+    return y
+
+
+def add_lu_mult(row_ptr, cols, vals, alpha, x, y, lower: bool) -> np.ndarray:
+    rp, ci, v, xx = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(x, np.float64)
+    yy = _c(y, np.float64).copy()
+    f = orc().orc_add_lmult if lower else orc().orc_add_umult
+    f(rp.size - 1, _ip(rp), _ip(ci), _dp(v), alpha, _dp(xx), _dp(yy))
+    return yy
+
+
+def inv_diag(row_ptr, cols, vals) -> np.ndarray:
+    rp, ci, v = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64)
+    out = np.empty(rp.size - 1)
+    orc().orc_inv_diag(rp.size - 1, _ip(rp), _ip(ci), _dp(v), _dp(out))
+    return out
+
+
+def dot(x, y) -> float:
+    xx, yy = _c(x, np.float64), _c(y, np.float64)
+    return orc().orc_dot(xx.size, _dp(xx), _dp(yy))
+
+
+def axpy(a, x, y) -> np.ndarray:
+    """y + a x with one fma per element (cblas_daxpy)."""
+    xx, yy = _c(x, np.float64), _c(y, np.float64).copy()
+    orc().orc_axpy(xx.size, a, _dp(xx), _dp(yy))
+    return yy
+
+
+def aypx(a, y, x) -> np.ndarray:
+    xx, yy = _c(x, np.float64), _c(y, np.float64).copy()
+    orc().orc_aypx(xx.size, a, _dp(yy), _dp(xx))
+    return yy
+
+
+def ilu0_factor(row_ptr, cols, vals, which="oracle") -> np.ndarray:
+    rp, ci, v = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64)
+    out = np.empty(v.size)
+    L = orc() if which == "oracle" else ref()
+    getattr(L, "orc_ilu0_factor" if which == "oracle" else "ref_ilu0_factor")(rp.size - 1, _ip(rp), _ip(ci), _dp(v),
+                                                                                _dp(out))
+    return out
+
+
+def ilu0_apply(row_ptr, cols, vals, y, which="oracle") -> np.ndarray:
+    rp, ci, v, yy = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(y, np.float64)
+    out = np.empty(rp.size - 1)
+    L = orc() if which == "oracle" else ref()
+    getattr(L, "orc_ilu0_apply" if which == "oracle" else "ref_ilu0_apply")(rp.size - 1, _ip(rp), _ip(ci), _dp(v),
+                                                                              _dp(yy), _dp(out))
+    return out
+
+
+def cheb_apply(row_ptr, cols, vals, x, factor=0.0, order=3, max_iter=10, which="oracle") -> np.ndarray:
+    rp, ci, v, xx = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(x, np.float64)
+    out = np.empty(rp.size - 1)
+    L = orc() if which == "oracle" else ref()
+    getattr(L, "orc_cheb_apply" if which == "oracle" else "ref_cheb_apply")(rp.size - 1, _ip(rp), _ip(ci), _dp(v),
+                                                                              factor, order, max_iter, _dp(xx),
+                                                                              _dp(out))
+    return out
+
+
+def cheb_bounds(row_ptr, cols, vals, factor=0.0, max_iter=10) -> tuple[float, float]:
+    rp, ci, v = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64)
+    a, b = C.c_double(), C.c_double()
+    orc().orc_cheb_bounds(rp.size - 1, _ip(rp), _ip(ci), _dp(v), factor, max_iter, C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+def ell_layout(row_ptr, cols, vals, slice_rows=32):
+    rp, ci, v = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64)
+    n = rp.size - 1
+    ns = (n + slice_rows - 1) // slice_rows
+    off = np.empty(ns + 1, dtype=np.int32)
+    orc().orc_ell_layout(n, _ip(rp), _ip(ci), _dp(v), slice_rows, _ip(off), None, None)
+    stored = int(off[-1]) * slice_rows
+    ec = np.empty(stored, dtype=np.int32)
+    ev = np.empty(stored)
+    orc().orc_ell_layout(n, _ip(rp), _ip(ci), _dp(v), slice_rows, _ip(off), _ip(ec), _dp(ev))
+    return off, ec, ev

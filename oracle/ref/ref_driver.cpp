@@ -1,0 +1,360 @@
+// ref_driver.cpp -- runs Alien's OWN header-only Krylov templates on the CPU.
+//
+// TEST INFRASTRUCTURE ONLY (oracle).  Built by oracle/Makefile into
+// oracle/_ref/libalien_ref.so, straight from the reference sources where they
+// lie (ALIEN_REF_SRC, default the read-only reference checkout's src/core):
+//   alien/expression/krylov/{Iteration,CG,BiCGStab,DiagPreconditioner,
+//                            ILU0Preconditioner,ChebyshevPreconditioner}.h
+//   alien/handlers/scalar/CSRModifierViewT.h
+// Nothing of those files is copied here.  What this file supplies is the
+// minimum the templates need from the rest of Alien, which cannot be built in
+// this image (Arccore, MPI and Boost are absent):
+//   * a CPU algebra (ShimAlgebra) that satisfies the AlgebraT concept used by
+//     the templates and restates SimpleCSRInternalLinearAlgebra
+//     (kernels/simple_csr/algebra/SimpleCSRInternalLinearAlgebra.h:55-173)
+//     through oracle/simplecsr_kernels.h;
+//   * a sequential CSR matrix/profile type exposing the members that
+//     ILU0Preconditioner.h:51-61 and CSRModifierViewT.h:105-145 touch;
+//   * ITraceMng, MatrixDistribution and LUSendRecvTraits stand-ins (the
+//     parallel branches that use the latter are never taken: isParallel()
+//     is false on one process).
+// The exported C entry points mirror oracle/ab2_oracle.cpp's, so tests can
+// check the restatement against the reference templates result for result.
+
+#include <cmath>
+#include <cstring>
+#include <iostream>
+#include <memory>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../simplecsr_kernels.h"
+
+namespace Alien {
+
+class ITraceMng {
+ public:
+  std::ostream& info() { return std::cerr; }
+};
+
+struct MatrixDistribution {};
+
+template <typename Tag>
+class LUSendRecvTraits;
+
+namespace shim {
+
+struct Tag {};
+
+struct Profile {
+  typedef int IndexType;
+  int n = 0;
+  std::vector<int> rp, ci, dc;
+  std::size_t getNRows() const { return (std::size_t)n; }
+  std::size_t getNnz() const { return ci.size(); }
+  const int* kcol() const { return rp.data(); }
+  const int* cols() const { return ci.data(); }
+  const int* dcol() const { return dc.data(); }
+};
+
+struct DistInfo {
+  std::vector<int> m_local_row_size;
+  std::vector<int> m_cols;
+  int m_first_upper_ghost_index = 0;
+  const int* dcol(const Profile&) const { return nullptr; }
+};
+
+struct Matrix {
+  typedef double ValueType;
+  typedef Profile ProfileType;
+  typedef Tag TagType;
+  typedef DistInfo DistStructInfo;
+  static const bool on_host_only = true;
+
+  std::shared_ptr<Profile> profile;
+  std::vector<double> values;
+  DistInfo dist_info;
+  MatrixDistribution dist;
+
+  bool isParallel() const { return false; }
+  std::size_t getAllocSize() const { return (std::size_t)profile->n; }
+  MatrixDistribution const& distribution() const { return dist; }
+  Matrix* cloneTo(void*) const { return new Matrix(*this); }
+  Profile const& getProfile() const { return *profile; }
+  DistInfo const& getDistStructInfo() const { return dist_info; }
+  double* data() { return values.data(); }
+  const double* data() const { return values.data(); }
+  void notifyChanges() {}
+  void endUpdate() {}
+  ab2_oracle::Csr csr() const { return ab2_oracle::Csr{profile->n, profile->rp.data(), profile->ci.data(), values.data()}; }
+};
+
+struct Vector {
+  std::vector<double> v;
+  double* data() { return v.data(); }
+  const double* data() const { return v.data(); }
+  int size() const { return (int)v.size(); }
+};
+
+struct LUOp {
+  LUOp(Matrix&, MatrixDistribution const&, std::vector<int>&) {}
+  void recvLowerNeighbLUData(double*) {}
+  void sendUpperNeighbLUData(double*) {}
+};
+
+}  // namespace shim
+
+template <>
+class LUSendRecvTraits<shim::Tag> {
+ public:
+  typedef shim::LUOp matrix_op_type;
+  typedef void vector_op_type;
+};
+
+// The AlgebraT concept as the Krylov templates call it.
+class ShimAlgebra {
+ public:
+  typedef shim::Matrix Matrix;
+  typedef shim::Vector Vector;
+  typedef int ResourceType;
+
+  struct NullValueException {
+    std::string which;
+    explicit NullValueException(std::string const& w) : which(w) {}
+  };
+
+  template <typename T>
+  class Future {
+   public:
+    explicit Future(T& v) : m_value(v) {}
+    T& operator()() { return m_value; }
+    T get() { return m_value; }
+
+   private:
+    T& m_value;
+  };
+  typedef Future<double> FutureType;
+
+  // r.r values seen by the stop test (Iteration only uses the future form of dot).
+  std::vector<double> history;
+  bool skip_first = true;
+
+  static ResourceType resource(Matrix const& A) { return A.profile->n; }
+  void allocate(ResourceType n, Vector& v) { v.v.assign((std::size_t)n, 0.0); }
+  template <typename T0, typename... T>
+  void allocate(ResourceType n, T0& v0, T&... rest) {
+    allocate(n, v0);
+    allocate(n, rest...);
+  }
+  void free(Vector& v) { v.v.clear(); }
+  template <typename T0, typename... T>
+  void free(T0& v0, T&... rest) {
+    free(v0);
+    free(rest...);
+  }
+
+  void mult(Matrix const& A, Vector const& x, Vector& y) const { ab2_oracle::spmv(A.csr(), x.data(), y.data()); }
+  void copy(Vector const& x, Vector& y) const { ab2_oracle::copy(x.size(), x.data(), y.data()); }
+  void axpy(double a, Vector const& x, Vector& y) const { ab2_oracle::axpy(x.size(), a, x.data(), y.data()); }
+  void scal(double a, Vector& x) const { ab2_oracle::scal(x.size(), a, x.data()); }
+  double dot(Vector const& x, Vector const& y) const { return ab2_oracle::dot(x.size(), x.data(), y.data()); }
+  void dot(Vector const& x, Vector const& y, FutureType& f) {
+    f() = ab2_oracle::dot(x.size(), x.data(), y.data());
+    if (&x == &y) {
+      if (skip_first) skip_first = false;
+      else history.push_back(f());
+    }
+  }
+  double norm2(Vector const& x) const { return std::sqrt(dot(x, x)); }
+  void pointwiseMult(Vector const& x, Vector const& y, Vector& w) const {
+    ab2_oracle::pmult(x.size(), x.data(), y.data(), w.data());
+  }
+  void assign(Vector& x, double a) const {
+    for (auto& e : x.v) e = a;
+  }
+  template <typename LambdaT>
+  void assign(Vector& x, LambdaT const& f) const {
+    for (std::size_t i = 0; i < x.v.size(); ++i) x.v[i] = f(i);
+  }
+  void computeInvDiag(Matrix const& A, Vector& inv) const {
+    std::vector<int> d = ab2_oracle::diag_offsets(A.csr());
+    for (int i = 0; i < A.profile->n; ++i) inv.v[i] = 1. / A.values[d[i]];
+  }
+  template <typename PrecondT>
+  void exec(PrecondT& precond, Vector const& x, Vector& y) {
+    precond.solve(*this, x, y);
+  }
+};
+
+}  // namespace Alien
+
+#include <alien/expression/krylov/Iteration.h>
+#include <alien/expression/krylov/CG.h>
+#include <alien/expression/krylov/BiCGStab.h>
+#include <alien/expression/krylov/DiagPreconditioner.h>
+#include <alien/expression/krylov/ChebyshevPreconditioner.h>
+#include <alien/expression/krylov/ILU0Preconditioner.h>
+
+extern "C" {
+
+// Same layout as orc_options / orc_result in ab2_oracle.cpp.
+typedef struct {
+  int solver;
+  int precond;
+  double tol;
+  int max_iter;
+  double poly_factor;
+  int poly_order;
+  int poly_factor_max_iter;
+} ref_options;
+
+typedef struct {
+  int iterations;
+  int converged;
+  int error;
+  int breakdown;
+  double nrm2_b;
+  double last_rr;
+  double cheb_alpha;
+  double cheb_beta;
+  int history_len;
+} ref_result;
+
+}  // extern "C"
+
+namespace {
+
+using Alien::ShimAlgebra;
+
+Alien::shim::Matrix make_matrix(int n, const int* rp, const int* ci, const double* v) {
+  Alien::shim::Matrix A;
+  A.profile = std::make_shared<Alien::shim::Profile>();
+  A.profile->n = n;
+  A.profile->rp.assign(rp, rp + n + 1);
+  A.profile->ci.assign(ci, ci + rp[n]);
+  A.profile->dc = ab2_oracle::diag_offsets(ab2_oracle::Csr{n, rp, ci, nullptr});
+  A.values.assign(v, v + rp[n]);
+  return A;
+}
+
+int breakdown_code(std::string const& w) {
+  if (w == "alpha") return 1;
+  if (w == "beta") return 2;
+  if (w == "rho") return 3;
+  return 9;
+}
+
+template <typename SolverT, typename PrecondT>
+int run(ShimAlgebra& alg, SolverT& solver, PrecondT& pc, Alien::Iteration<ShimAlgebra>& it,
+        Alien::shim::Matrix const& A, Alien::shim::Vector const& b, Alien::shim::Vector& x, ref_result* res) {
+  try {
+    solver.solve(pc, it, A, b, x);
+  } catch (ShimAlgebra::NullValueException const& e) {
+    res->error = -3;
+    res->breakdown = breakdown_code(e.which);
+  }
+  return res->error;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_solve(int n, const int* rp, const int* ci, const double* v, const double* b, double* x,
+              const ref_options* o, ref_result* res, double* hist, int hist_cap) {
+  std::memset(res, 0, sizeof(*res));
+  ShimAlgebra alg;
+  Alien::shim::Matrix A = make_matrix(n, rp, ci, v);
+  Alien::shim::Vector vb, vx;
+  vb.v.assign(b, b + n);
+  vx.v.assign(x, x + n);
+  Alien::Iteration<ShimAlgebra> it(alg, vb, o->tol, o->max_iter, nullptr);
+
+  auto finish = [&]() {
+    for (int i = 0; i < n; ++i) x[i] = vx.v[i];
+    res->iterations = it();
+    res->converged = it.getStatus() ? 1 : 0;
+    res->nrm2_b = ab2_oracle::dot(n, b, b);
+    res->history_len = (int)alg.history.size();
+    res->last_rr = alg.history.empty() ? 0.0 : alg.history.back();
+    for (int i = 0; i < (int)alg.history.size() && i < hist_cap && hist; ++i) hist[i] = alg.history[i];
+  };
+
+  auto with_solver = [&](auto& pc) {
+    if (o->solver == 0) {
+      Alien::CG<ShimAlgebra> s(alg, nullptr);
+      run(alg, s, pc, it, A, vb, vx, res);
+    } else {
+      Alien::BiCGStab<ShimAlgebra> s(alg, nullptr);
+      run(alg, s, pc, it, A, vb, vx, res);
+    }
+  };
+
+  switch (o->precond) {
+    case 1: {
+      Alien::DiagPreconditioner<ShimAlgebra> pc(alg, A);
+      pc.init();
+      with_solver(pc);
+      break;
+    }
+    case 2: {
+      Alien::ILU0Preconditioner<ShimAlgebra> pc(alg, A, nullptr);
+      pc.init();
+      with_solver(pc);
+      break;
+    }
+    case 3: {
+      Alien::ChebyshevPreconditioner<ShimAlgebra> pc(alg, A, o->poly_factor, o->poly_order,
+                                                     o->poly_factor_max_iter, nullptr);
+      pc.init();
+      with_solver(pc);
+      break;
+    }
+    default: return -6;
+  }
+  finish();
+  return res->error;
+}
+
+// ILU(0) factor computed by the reference's LUFactorisationAlgo.
+int ref_ilu0_factor(int n, const int* rp, const int* ci, const double* v, double* lu) {
+  ShimAlgebra alg;
+  Alien::shim::Matrix A = make_matrix(n, rp, ci, v);
+  Alien::LUFactorisationAlgo<Alien::shim::Matrix, Alien::shim::Vector> algo;
+  algo.init(alg, A);
+  const Alien::shim::Matrix& LU = algo.getLUMatrix();
+  std::memcpy(lu, LU.values.data(), sizeof(double) * (size_t)rp[n]);
+  return 0;
+}
+
+// One application of the reference's ILU0Preconditioner: x = (LU)^-1 y.
+int ref_ilu0_apply(int n, const int* rp, const int* ci, const double* v, const double* y, double* x) {
+  ShimAlgebra alg;
+  Alien::shim::Matrix A = make_matrix(n, rp, ci, v);
+  Alien::ILU0Preconditioner<ShimAlgebra> pc(alg, A, nullptr);
+  pc.init();
+  Alien::shim::Vector vy, vx;
+  vy.v.assign(y, y + n);
+  vx.v.assign((std::size_t)n, 0.0);
+  alg.exec(pc, vy, vx);
+  std::memcpy(x, vx.v.data(), sizeof(double) * (size_t)n);
+  return 0;
+}
+
+// One application of the reference's ChebyshevPreconditioner (non-Saad).
+int ref_cheb_apply(int n, const int* rp, const int* ci, const double* v, double factor, int order, int max_iter,
+                   const double* xin, double* yout) {
+  ShimAlgebra alg;
+  Alien::shim::Matrix A = make_matrix(n, rp, ci, v);
+  Alien::ChebyshevPreconditioner<ShimAlgebra> pc(alg, A, factor, order, max_iter, nullptr);
+  pc.init();
+  Alien::shim::Vector vx, vy;
+  vx.v.assign(xin, xin + n);
+  vy.v.assign((std::size_t)n, 0.0);
+  alg.exec(pc, vx, vy);
+  std::memcpy(yout, vy.v.data(), sizeof(double) * (size_t)n);
+  return 0;
+}
+
+}  // extern "C"

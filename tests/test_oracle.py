@@ -1,0 +1,119 @@
+"""The CPU oracle, pinned (no GPU needed).
+
+* the known-answer checks of Alien's own algebra test
+  (src/refsemantic/tests/TestMVExpr.cc:105-167) hold for the oracle algebra;
+* the restatement (oracle/ab2_oracle.cpp) reproduces, bit for bit, the solves
+  recorded in tests/golden/solves.json from Alien's own Krylov templates
+  (oracle/_ref, generated by tests/golden/make_golden.py);
+* when oracle/_ref is present, restatement and reference templates agree on
+  further random systems too.
+"""
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import problems
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "solves.json").read_text())
+
+
+def unhex(a):
+    return np.array([float.fromhex(v) for v in a])
+
+
+# ----------------------------------------------------------------- TestMVExpr KATs
+def test_testmvexpr_known_answers():
+    rp, ci, v = problems.laplacian_1d(10)
+    n, lam = 10, 0.5
+    x = np.ones(n)
+    nrm = lambda a: np.sqrt(O.dot(a, a))  # norm2 = sqrt(dot), CBLASMPIKernel.h:113-124
+    assert nrm(x) == np.sqrt(10)
+    y = lam * x
+    assert nrm(y) == np.sqrt(10 * 0.25)
+    y = O.spmv(rp, ci, v, x)
+    assert nrm(y) == np.sqrt(2)
+    r = y - O.spmv(rp, ci, v, x)
+    assert nrm(r) == 0.0
+    y = y + lam * x
+    assert nrm(y) == np.sqrt(2 * 1.5 * 1.5 + (n - 2) * 0.25)
+    y = O.spmv(rp, ci, v, lam * x)
+    assert nrm(y) == np.sqrt(0.5)
+    y = np.arange(n, dtype=np.float64)
+    assert O.dot(x, y) == 45
+    assert O.dot(lam * x, y) == 22.5
+    assert O.dot(x, r + y) == 45
+    assert O.dot(x, O.spmv(rp, ci, v, y)) == 9
+    # ||lambda A||_F = lambda ||A||_F
+    assert np.sqrt(O.dot(lam * v, lam * v)) == lam * np.sqrt(O.dot(v, v))
+
+
+# ----------------------------------------------------------------- golden solves
+@pytest.mark.parametrize("case", GOLDEN["cases"], ids=lambda c: f"{c['problem']}-{c['solver']}-{c['precond']}-m{c['max_iter']}")
+def test_restatement_matches_reference_templates(case):
+    P = problems.get(case["problem"])
+    meta = GOLDEN["problems"][case["problem"]]
+    assert hashlib.sha256(P.vals.tobytes()).hexdigest() == meta["vals_sha256"]
+    assert hashlib.sha256(P.b.tobytes()).hexdigest() == meta["b_sha256"]
+    kw = {k: case[k] for k in ("solver", "precond", "tol", "max_iter", "poly_factor", "poly_order",
+                               "poly_factor_max_iter")}
+    r = O.solve(P.row_ptr, P.cols, P.vals, P.b, which="oracle", **kw)
+    assert r.iterations == case["iterations"]
+    assert r.converged == case["converged"]
+    assert r.breakdown == case["breakdown"]
+    assert r.history.size == case["history_len"]
+    assert hashlib.sha256(r.history.tobytes()).hexdigest() == case["history_sha256"]
+    assert hashlib.sha256(r.x.tobytes()).hexdigest() == case["x_sha256"]
+    np.testing.assert_array_equal(r.x[case["x_index"]], unhex(case["x_sample"]))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("seed", [0, 1, 2])
+@pytest.mark.parametrize("solver,pc", [("cg", "diag"), ("bicgs", "ilu0"), ("bicgs", "diag"), ("cg", "ilu0"),
+                                       ("bicgs", "cheb")])
+def test_restatement_vs_reference_random(seed, solver, pc):
+    P = problems.ragged(300 + 37 * seed, seed=100 + seed)
+    kw = dict(solver=solver, precond=pc, tol=1e-10, max_iter=60, poly_factor=0.0, poly_order=3,
+              poly_factor_max_iter=8)
+    a = O.solve(P.row_ptr, P.cols, P.vals, P.b, which="oracle", **kw)
+    r = O.solve(P.row_ptr, P.cols, P.vals, P.b, which="ref", **kw)
+    assert a.iterations == r.iterations and a.converged == r.converged
+    np.testing.assert_array_equal(a.x, r.x)
+    np.testing.assert_array_equal(a.history, r.history)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", ["poisson16", "diffusion12", "convdiff_10x11x12", "ragged"])
+def test_ilu0_and_chebyshev_vs_reference(name):
+    P = problems.get(name)
+    np.testing.assert_array_equal(O.ilu0_factor(P.row_ptr, P.cols, P.vals, "oracle"),
+                                  O.ilu0_factor(P.row_ptr, P.cols, P.vals, "ref"))
+    np.testing.assert_array_equal(O.ilu0_apply(P.row_ptr, P.cols, P.vals, P.b, "oracle"),
+                                  O.ilu0_apply(P.row_ptr, P.cols, P.vals, P.b, "ref"))
+    np.testing.assert_array_equal(O.cheb_apply(P.row_ptr, P.cols, P.vals, P.b, 0.0, 3, 12, "oracle"),
+                                  O.cheb_apply(P.row_ptr, P.cols, P.vals, P.b, 0.0, 3, 12, "ref"))
+
+
+def test_krylov_config1_iteration_count():
+    """32^3 Poisson, b = A x_true (seed 0), Jacobi-PCG to 1e-8."""
+    P = problems.get("poisson32")
+    r = O.solve(P.row_ptr, P.cols, P.vals, P.b, solver="cg", precond="diag", tol=1e-8, max_iter=1000)
+    assert r.converged and r.iterations == 105
+    assert np.linalg.norm(r.x - P.x_true) / np.linalg.norm(P.x_true) < 1e-6
+
+
+def test_ell_layout_matches_csr():
+    P = problems.get("ragged")
+    off, ec, ev = O.ell_layout(P.row_ptr, P.cols, P.vals, 32)
+    n = P.n
+    for row in range(0, n, 37):
+        s, lane = divmod(row, 32)
+        w = off[s + 1] - off[s]
+        slots = off[s] * 32 + np.arange(w) * 32 + lane
+        a, b = P.row_ptr[row], P.row_ptr[row + 1]
+        assert np.array_equal(ec[slots][: b - a], P.cols[a:b])
+        assert np.array_equal(ev[slots][: b - a], P.vals[a:b])
+        assert np.all(ev[slots][b - a:] == 0)
