@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
 #include <exception>
 #include <new>
@@ -30,6 +31,10 @@ struct Error {
 }  // namespace ab2
 
 struct ab2_context {
+  // Every object created on a context holds a reference, so objects may be
+  // destroyed after ab2_context_destroy (as garbage-collected bindings do);
+  // the context's memory goes when the last reference does.
+  std::atomic<int> refs{1};
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
@@ -117,6 +122,19 @@ T* dev_alloc(size_t count, long long* accounted = nullptr) {
 
 inline void dev_free(void* p) {
   if (p) cudaFree(p);
+}
+
+// Context references (see ab2_context::refs).
+inline ab2_context* ctx_retain(ab2_context* ctx) {
+  ctx->refs.fetch_add(1);
+  return ctx;
+}
+void ctx_release(ab2_context* ctx);  // frees the context with its last reference
+
+// Makes ctx's device current and waits for its stream: every destroy starts here.
+inline void ctx_quiesce(ab2_context* ctx) {
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
 }
 
 inline int grid_for(long long n, int threads = kThreads, int cap = 148 * 32) {

@@ -63,6 +63,17 @@ int red_grid(int n) { return grid_for(n, kThreads, kMaxRedBlocks); }
 
 }  // namespace
 
+void ctx_release(ab2_context* ctx) {
+  if (ctx->refs.fetch_sub(1) != 1) return;
+  ctx_quiesce(ctx);
+  dev_free(ctx->d_partials);
+  dev_free(ctx->d_counters);
+  dev_free(ctx->d_results);
+  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
 RedSlot red_slot(ab2_context* ctx, int slot) {
   return RedSlot{ctx->d_partials + (size_t)slot * kMaxRedComps * kMaxRedBlocks, ctx->d_counters + slot,
                  ctx->d_results + (size_t)slot * kMaxRedComps};
@@ -163,14 +174,7 @@ int ab2_context_create(int device, ab2_context** out) {
 
 int ab2_context_destroy(ab2_context* ctx) {
   if (!ctx) return AB2_ERR_BAD_ARG;
-  cudaSetDevice(ctx->device);
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  dev_free(ctx->d_partials);
-  dev_free(ctx->d_counters);
-  dev_free(ctx->d_results);
-  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
-  delete ctx;
+  ctx_release(ctx);
   return AB2_OK;
 }
 
@@ -199,14 +203,14 @@ int ab2_vector_create(ab2_context* ctx, int n, ab2_vector** out) {
   *out = nullptr;
   ab2_vector* v = new (std::nothrow) ab2_vector();
   if (!v) return AB2_ERR_OOM;
+  v->ctx = ctx_retain(ctx);
   int rc = guard(ctx, [&] {
-    v->ctx = ctx;
     v->n = n;
     v->d = dev_alloc<double>((size_t)n);
     AB2_CUDA(cudaMemsetAsync(v->d, 0, sizeof(double) * (size_t)std::max(n, 1), ctx->stream));
   });
   if (rc != AB2_OK) {
-    delete v;
+    ab2_vector_destroy(v);
     return rc;
   }
   *out = v;
@@ -215,8 +219,9 @@ int ab2_vector_create(ab2_context* ctx, int n, ab2_vector** out) {
 
 int ab2_vector_destroy(ab2_vector* v) {
   if (!v) return AB2_ERR_BAD_ARG;
-  if (v->ctx) cudaStreamSynchronize(v->ctx->stream);
+  ctx_quiesce(v->ctx);
   dev_free(v->d);
+  ctx_release(v->ctx);
   delete v;
   return AB2_OK;
 }
@@ -316,13 +321,13 @@ int ab2_scalar_create(ab2_context* ctx, ab2_scalar** out) {
   *out = nullptr;
   ab2_scalar* s = new (std::nothrow) ab2_scalar();
   if (!s) return AB2_ERR_OOM;
+  s->ctx = ctx_retain(ctx);
   int rc = guard(ctx, [&] {
-    s->ctx = ctx;
     s->d = dev_alloc<double>(1);
     AB2_CUDA(cudaMemsetAsync(s->d, 0, sizeof(double), ctx->stream));
   });
   if (rc != AB2_OK) {
-    delete s;
+    ab2_scalar_destroy(s);
     return rc;
   }
   *out = s;
@@ -330,8 +335,9 @@ int ab2_scalar_create(ab2_context* ctx, ab2_scalar** out) {
 }
 int ab2_scalar_destroy(ab2_scalar* s) {
   if (!s) return AB2_ERR_BAD_ARG;
-  if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
+  ctx_quiesce(s->ctx);
   dev_free(s->d);
+  ctx_release(s->ctx);
   delete s;
   return AB2_OK;
 }

@@ -484,8 +484,8 @@ int ab2_solver_create(ab2_context* ctx, const ab2_matrix* A, const ab2_solver_op
   *out = nullptr;
   ab2_solver* S = new (std::nothrow) ab2_solver();
   if (!S) return AB2_ERR_OOM;
+  S->ctx = ctx_retain(ctx);
   int rc = guard(ctx, [&] {
-    S->ctx = ctx;
     S->A = A;
     S->opts = *o;
     AB2_CUDA(cudaEventCreate(&S->ev0));
@@ -604,7 +604,7 @@ int ab2_solver_history(const ab2_solver* S, double* hist, int cap, int* len) {
 
 int ab2_solver_destroy(ab2_solver* S) {
   if (!S) return AB2_ERR_BAD_ARG;
-  if (S->ctx) cudaStreamSynchronize(S->ctx->stream);
+  if (S->ctx) ctx_quiesce(S->ctx);
   if (S->exec) cudaGraphExecDestroy(S->exec);
   if (S->graph) cudaGraphDestroy(S->graph);
   if (S->pc) ab2_precond_destroy(S->pc);
@@ -614,6 +614,7 @@ int ab2_solver_destroy(ab2_solver* S) {
   if (S->h_st) cudaFreeHost(S->h_st);
   if (S->ev0) cudaEventDestroy(S->ev0);
   if (S->ev1) cudaEventDestroy(S->ev1);
+  if (S->ctx) ctx_release(S->ctx);
   delete S;
   return AB2_OK;
 }

@@ -29,6 +29,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <random>
 
 #include "ab2_internal.cuh"
@@ -234,6 +235,9 @@ void ilu_symbolic(const ab2_matrix* A, Ilu0Data& d) {
   d.levels_u = max_u + 1;
   build(lev_l, d.levels_l, false, d.h_perm_l, d.lev_ptr_l);
   build(lev_u, d.levels_u, true, perm_u, ptr_u);
+  d.widest_l = d.widest_u = 1;
+  for (int l = 0; l < d.levels_l; ++l) d.widest_l = std::max(d.widest_l, (d.lev_ptr_l[l + 1] - d.lev_ptr_l[l]) / 32);
+  for (int l = 0; l < d.levels_u; ++l) d.widest_u = std::max(d.widest_u, (ptr_u[l + 1] - ptr_u[l]) / 32);
   d.len_l = (int)d.h_perm_l.size();
   d.len_u = (int)perm_u.size();
   d.d_perm_l = dev_alloc<int>(d.h_perm_l.size());
@@ -242,9 +246,18 @@ void ilu_symbolic(const ab2_matrix* A, Ilu0Data& d) {
   AB2_CUDA(cudaMemcpy(d.d_perm_u, perm_u.data(), sizeof(int) * perm_u.size(), cudaMemcpyHostToDevice));
 }
 
-int sweep_blocks(ab2_context* ctx, int len) {
-  const int warps = len / 32;
-  const int blocks = (warps + 7) / 8;
+// Warps of a sweep: a few wavefronts' worth.  Every warp beyond the ones the
+// current wavefront can use only polls, and polling traffic slows the L2 the
+// producers write through, so the grid is sized to keep about three
+// wavefronts in flight (the AB2_ILU_WINDOW environment variable overrides the
+// three, for tuning).
+int sweep_blocks(ab2_context* ctx, int len, int widest_chunks) {
+  static const int window = [] {
+    const char* e = std::getenv("AB2_ILU_WINDOW");
+    return e ? std::max(1, std::atoi(e)) : 3;
+  }();
+  const long long warps = std::min<long long>((long long)widest_chunks * window, len / 32);
+  const int blocks = (int)((warps + 7) / 8);
   return std::max(1, std::min(blocks, ctx->num_sms * 8));
 }
 
@@ -348,11 +361,11 @@ void pc_apply(ab2_context* ctx, const ab2_precond* pc, const double* x, double* 
     case AB2_PC_ILU0: {
       const Ilu0Data& d = pc->ilu;
       const ab2_matrix* A = pc->A;
-      k_ilu_lsweep<<<sweep_blocks(ctx, d.len_l), 256, 0, ctx->stream>>>(d.len_l, d.d_perm_l, A->d_rp, A->d_ci, A->d_dcol,
-                                                                        d.d_lu, x, d.d_tmp, y, d.d_counters, d.d_err);
+      k_ilu_lsweep<<<sweep_blocks(ctx, d.len_l, d.widest_l), 256, 0, ctx->stream>>>(
+          d.len_l, d.d_perm_l, A->d_rp, A->d_ci, A->d_dcol, d.d_lu, x, d.d_tmp, y, d.d_counters, d.d_err);
       check_launch(ctx, "ilu_lsweep");
-      k_ilu_usweep<<<sweep_blocks(ctx, d.len_u), 256, 0, ctx->stream>>>(d.len_u, d.d_perm_u, A->d_rp, A->d_ci, A->d_dcol,
-                                                                        d.d_lu, d.d_tmp, y, d.d_counters, d.d_err);
+      k_ilu_usweep<<<sweep_blocks(ctx, d.len_u, d.widest_u), 256, 0, ctx->stream>>>(
+          d.len_u, d.d_perm_u, A->d_rp, A->d_ci, A->d_dcol, d.d_lu, d.d_tmp, y, d.d_counters, d.d_err);
       check_launch(ctx, "ilu_usweep");
       break;
     }
@@ -410,8 +423,8 @@ int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_
   if (o->kind < AB2_PC_NONE || o->kind > AB2_PC_CHEB) return AB2_ERR_BAD_ARG;
   ab2_precond* pc = new (std::nothrow) ab2_precond();
   if (!pc) return AB2_ERR_OOM;
+  pc->ctx = ctx_retain(ctx);
   int rc = guard(ctx, [&] {
-    pc->ctx = ctx;
     pc->A = A;
     pc->kind = o->kind;
     if (o->kind == AB2_PC_DIAG || o->kind == AB2_PC_CHEB) {
@@ -441,7 +454,7 @@ int ab2_precond_apply(ab2_context* ctx, const ab2_precond* pc, const ab2_vector*
 
 int ab2_precond_destroy(ab2_precond* pc) {
   if (!pc) return AB2_ERR_BAD_ARG;
-  if (pc->ctx) cudaStreamSynchronize(pc->ctx->stream);
+  if (pc->ctx) ctx_quiesce(pc->ctx);
   dev_free(pc->d_inv);
   dev_free(pc->ilu.d_lu);
   dev_free(pc->ilu.d_perm_l);
@@ -453,6 +466,7 @@ int ab2_precond_destroy(ab2_precond* pc) {
   dev_free(pc->cheb.d_y[0]);
   dev_free(pc->cheb.d_y[1]);
   dev_free(pc->cheb.d_xcopy);
+  if (pc->ctx) ctx_release(pc->ctx);
   delete pc;
   return AB2_OK;
 }

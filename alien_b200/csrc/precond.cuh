@@ -18,6 +18,7 @@ struct Ilu0Data {
   int* d_perm_u = nullptr;
   int len_l = 0, len_u = 0;
   int levels_l = 0, levels_u = 0;
+  int widest_l = 1, widest_u = 1;   // chunks in the widest wavefront
   std::vector<int> lev_ptr_l;       // host: wavefront starts in perm_l (factorisation launches)
   std::vector<int> h_perm_l;
   double* d_tmp = nullptr;          // L-sweep output, left at the sentinel between applications

@@ -22,6 +22,7 @@
 #include <cstring>
 
 #include "ab2_internal.cuh"
+#include "spmv_view.cuh"
 
 namespace ab2 {
 
@@ -143,31 +144,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_ell(int n, const int* __restr
   const int o = off[s];
   const int w = off[s + 1] - o;
   const size_t base = (size_t)o * kEllSlice + lane;
-  const int* cp = eci + base;
-  const T* vp = ev + base;
-  T acc = 0;
-  int j = 0;
-  for (; j + 8 <= w; j += 8) {
-    int c[8];
-    T a[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      c[u] = __ldcs(cp + (size_t)(j + u) * kEllSlice);
-      a[u] = __ldcs(vp + (size_t)(j + u) * kEllSlice);
-    }
-    T xv[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : (T)0;
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (c[u] >= 0) acc = mul_add_rn(a[u], xv[u], acc);
-  }
-  for (; j < w; ++j) {
-    const int c = __ldcs(cp + (size_t)j * kEllSlice);
-    const T a = __ldcs(vp + (size_t)j * kEllSlice);
-    if (c >= 0) acc = mul_add_rn(a, __ldg(x + c), acc);
-  }
-  y[row] = acc;
+  y[row] = EllView<T>::ell_row_sum(eci + base, ev + base, w, x);
 }
 
 __global__ void k_add_lu(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
@@ -320,8 +297,8 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
   }
   ab2_matrix* A = new (std::nothrow) ab2_matrix();
   if (!A) return AB2_ERR_OOM;
+  A->ctx = ctx_retain(ctx);
   int rc = guard(ctx, [&] {
-    A->ctx = ctx;
     A->n = n;
     A->nnz = row_ptr[n];
     A->formats = (formats | AB2_FMT_CSR);
@@ -405,7 +382,7 @@ int ab2_matrix_update_values(ab2_context* ctx, ab2_matrix* A, const double* vals
 
 int ab2_matrix_destroy(ab2_matrix* A) {
   if (!A) return AB2_ERR_BAD_ARG;
-  if (A->ctx) cudaStreamSynchronize(A->ctx->stream);
+  if (A->ctx) ctx_quiesce(A->ctx);
   dev_free(A->d_rp);
   dev_free(A->d_ci);
   dev_free(A->d_v);
@@ -416,6 +393,7 @@ int ab2_matrix_destroy(ab2_matrix* A) {
   dev_free(A->d_ell_ci);
   dev_free(A->d_ell_v);
   dev_free(A->d_ell_v32);
+  if (A->ctx) ctx_release(A->ctx);
   delete A;
   return AB2_OK;
 }

@@ -34,15 +34,21 @@ struct EllView {
     const size_t base = (size_t)o * kEllSlice + lane;
     const int* cp = ci + base;
     const T* vp = v + base;
+    return ell_row_sum(cp, vp, w, x);
+  }
+
+  // Slots in groups of 8, all loads of a group issued before the first use
+  // (a 7-point row is one group), predicated on the slice width.
+  static __device__ __forceinline__ T ell_row_sum(const int* cp, const T* vp, int w, const T* __restrict__ x) {
     T acc = 0;
-    int j = 0;
-    for (; j + 8 <= w; j += 8) {
+    for (int j = 0; j < w; j += 8) {
       int c[8];
       T a[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
-        c[u] = __ldcs(cp + (size_t)(j + u) * kEllSlice);
-        a[u] = __ldcs(vp + (size_t)(j + u) * kEllSlice);
+        const bool in = j + u < w;
+        c[u] = in ? __ldcs(cp + (size_t)(j + u) * kEllSlice) : -1;
+        a[u] = in ? __ldcs(vp + (size_t)(j + u) * kEllSlice) : (T)0;
       }
       T xv[8];
 #pragma unroll
@@ -50,11 +56,6 @@ struct EllView {
 #pragma unroll
       for (int u = 0; u < 8; ++u)
         if (c[u] >= 0) acc = mul_add_rn(a[u], xv[u], acc);
-    }
-    for (; j < w; ++j) {
-      const int c = __ldcs(cp + (size_t)j * kEllSlice);
-      const T a = __ldcs(vp + (size_t)j * kEllSlice);
-      if (c >= 0) acc = mul_add_rn(a, __ldg(x + c), acc);
     }
     return acc;
   }
