@@ -119,6 +119,7 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_scalar_destroy": (_I, [_P]),
     "ab2_dot_async": (_I, [_P, _P, _P, _P]),
     "ab2_scalar_get": (_I, [_P, _P, _DP]),
+    "ab2_dot_noalloc": (_I, [_P, _P, _I, _P, _P]),
     "ab2_precond_create": (_I, [_P, _P, C.POINTER(PrecondOptions), C.POINTER(_P)]),
     "ab2_precond_apply": (_I, [_P, _P, _P, _P]),
     "ab2_precond_destroy": (_I, [_P]),

@@ -351,3 +351,88 @@ int ab2_scalar_get(ab2_context* ctx, const ab2_scalar* s, double* value) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free dot
+//
+// Some callers cannot allocate device memory at the moment they need a dot
+// product: a host that has handed all free HBM to another allocator (a caching
+// pool that reserved it up front, so cudaMalloc would fail or fragment it), or
+// a latency-critical loop that must not pay for cudaMalloc/cudaFree, which can
+// block the calling thread and synchronise the whole device.  For them,
+// ab2_dot_noalloc runs the same reduction kernel as ab2_dot with its block
+// partials and arrival counter in the file-scope array below instead of a
+// context's buffers.  The array exists once per GPU that loads libab2 and stays
+// there until the process exits.
+//
+// Each block of this variant reduces a fixed chunk of kNoAllocChunk elements,
+// so the scratch it needs grows with n: kNoAllocSlots partials cover n up to
+// kNoAllocSlots * kNoAllocChunk = 16,777,216 elements; larger n is rejected.
+// (ab2_dot's grid instead follows the context's reduction rule, so the two
+// entry points may sum in different trees and agree to rounding, not bits.)
+//
+// All calls in the process share the array and it keeps the last call's
+// contents; the counter, which must start at zero, is cleared on the caller's
+// stream before every launch.  Calls that overlap on the GPU (issued on
+// different streams, or from different host threads, without ordering between
+// them) race on the shared array and give wrong results.
+namespace {
+
+constexpr int kNoAllocChunk = 4096;   // elements per block (256 threads x 16)
+constexpr int kNoAllocSlots = 4096;   // block partials the scratch array holds
+constexpr int kNoAllocMaxDevices = 64;
+
+// [0, kNoAllocSlots): block partials; [kNoAllocSlots]: arrival counter (as
+// unsigned int bits); the rest pads the array to a multiple of 256 bytes.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocSlots + 32];
+
+struct NoAllocDevice {
+  bool ready = false;
+  double* scratch = nullptr;
+};
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::atomic<int> g_noalloc_lock{0};
+
+// Set-up, once per device and with that device current: the host-side name of
+// g_noalloc_scratch is only a stand-in, so the device address is looked up
+// with cudaGetSymbolAddress and cached.
+int noalloc_scratch(int device, double** out) {
+  while (g_noalloc_lock.exchange(1)) {
+  }
+  int rc = AB2_OK;
+  NoAllocDevice& d = g_noalloc_dev[device];
+  if (!d.ready) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
+      rc = AB2_ERR_CUDA;
+    } else {
+      d.scratch = (double*)p;
+      d.ready = true;
+    }
+  }
+  *out = d.scratch;
+  g_noalloc_lock.store(0);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int ab2_dot_noalloc(const double* x, const double* y, int n, double* result, void* stream) {
+  if ((!x || !y) && n > 0) return AB2_ERR_BAD_ARG;
+  if (!result || n < 0) return AB2_ERR_BAD_ARG;
+  if ((long long)n > (long long)kNoAllocSlots * kNoAllocChunk) {
+    fprintf(stderr, "ab2_dot_noalloc: n = %d exceeds the maximum of %d elements (%d block partials of %d)\n", n,
+            kNoAllocSlots * kNoAllocChunk, kNoAllocSlots, kNoAllocChunk);
+    return AB2_ERR_BAD_ARG;
+  }
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kNoAllocMaxDevices) return AB2_ERR_CUDA;
+  double* scratch = nullptr;
+  int rc = noalloc_scratch(device, &scratch);
+  if (rc != AB2_OK) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned int* counter = reinterpret_cast<unsigned int*>(scratch + kNoAllocSlots);
+  if (cudaMemsetAsync(counter, 0, sizeof(unsigned int), s) != cudaSuccess) return AB2_ERR_CUDA;
+  const int grid = std::max(1, (n + kNoAllocChunk - 1) / kNoAllocChunk);
+  ab2::k_dot<<<grid, ab2::kThreads, 0, s>>>(n, x, y, scratch, counter, result);
+  return cudaGetLastError() == cudaSuccess ? AB2_OK : AB2_ERR_CUDA;
+}

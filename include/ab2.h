@@ -145,6 +145,20 @@ int ab2_scalar_destroy(ab2_scalar* s);
 int ab2_dot_async(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, ab2_scalar* result);
 int ab2_scalar_get(ab2_context* ctx, const ab2_scalar* s, double* value);
 
+/* Allocation-free dot product.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory when they need the reduction
+ * (all free HBM handed to another allocator, or a loop that must not pay for
+ * cudaMalloc/cudaFree and the device synchronisation they can cause).
+ * x, y: device arrays of n doubles on the current device; result: one device
+ * double, written on `stream` (a cudaStream_t, NULL for the default stream);
+ * nothing is synchronised.  The block partials live in a fixed 32 KB device
+ * array inside libab2 (one per GPU, held until the process exits), which
+ * limits n to 16,777,216; larger n returns AB2_ERR_BAD_ARG.  The first call on
+ * each device looks that array up (cudaGetSymbolAddress): make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * (unordered streams or host threads) race and give wrong results. */
+int ab2_dot_noalloc(const double* x, const double* y, int n, double* result, void* stream);
+
 /* ------------------------------------------------------------------ preconditioners */
 typedef struct {
   int kind;                 /* AB2_PC_* */

@@ -1,0 +1,52 @@
+"""ab2_dot_noalloc: the dot product for callers that cannot allocate.
+
+Some hosts cannot call cudaMalloc when they need a reduction (their free HBM is
+owned by another allocator, or the call site cannot afford the blocking and
+device-wide synchronisation an allocation may bring).  ab2_dot_noalloc keeps
+its scratch in a fixed array inside libab2 instead.  This file checks it
+through the C ABI against ab2_dot (same reduction kernel, possibly another
+summation tree) on two calls in a row, and that oversized inputs are refused.
+It is collected last so that a failure here never hides the other tests.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from alien_b200 import abi
+
+pytestmark = pytest.mark.gpu
+
+MAX_N = 4096 * 4096
+
+
+def _noalloc(ctx, vx, vy, vout, n):
+    L = abi.lib()
+    return L.ab2_dot_noalloc(C.c_void_p(vx.device_ptr), C.c_void_p(vy.device_ptr), n, C.c_void_p(vout.device_ptr),
+                             C.c_void_p(ctx.stream))
+
+
+@pytest.mark.parametrize("n", [0, 1, 4095, 4097, 1_000_003, 7_077_888])
+def test_dot_noalloc_matches_dot_twice(ctx, n):
+    rng = np.random.default_rng(n)
+    x, y = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    vx, vy = ctx.vector(x), ctx.vector(y)
+    ref = ctx.dot(vx, vy)
+    scale = max(float(np.sum(np.abs(x * y))), 1e-300)
+    out = ctx.vector(2)
+    for call in range(2):  # the shared scratch keeps the previous call's contents
+        out.upload(np.full(2, np.nan))
+        assert _noalloc(ctx, vx, vy, out, n) == abi.AB2_OK
+        got = out.download()[0]  # download synchronises the context's stream
+        assert abs(got - ref) <= 1e-14 * scale, (call, got, ref)
+        assert abs(got - math.fsum(x * y)) <= 1e-14 * scale
+
+
+def test_dot_noalloc_rejects_oversize_and_bad_args(ctx):
+    L = abi.lib()
+    v = ctx.vector(4)
+    p = C.c_void_p(v.device_ptr)
+    assert L.ab2_dot_noalloc(p, p, MAX_N + 1, p, C.c_void_p(ctx.stream)) == abi.AB2_ERR_BAD_ARG
+    assert L.ab2_dot_noalloc(p, p, -1, p, C.c_void_p(ctx.stream)) == abi.AB2_ERR_BAD_ARG
+    assert L.ab2_dot_noalloc(p, p, 4, None, C.c_void_p(ctx.stream)) == abi.AB2_ERR_BAD_ARG
