@@ -30,6 +30,7 @@ FMT_CSR, FMT_ELL, FMT_F32 = 1, 2, 4
 SPMV_AUTO, SPMV_CSR_SCALAR, SPMV_CSR_STAGED, SPMV_ELL = 0, 1, 2, 3
 SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
 PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3}
+ILU_SCHEDULE = {"auto": 0, "wavefront": 1, "stencil": 2}
 BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho"}
 
 
@@ -39,6 +40,11 @@ class AB2Error(RuntimeError):
         self.code = code
 
 
+class ContextInfo(C.Structure):
+    _fields_ = [("device", C.c_int), ("num_sms", C.c_int), ("reduction_threads", C.c_int),
+                ("reduction_max_blocks", C.c_int)]
+
+
 class MatrixInfo(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("ell_stored", C.c_longlong), ("ell_slice", C.c_int),
                 ("formats", C.c_int), ("device_bytes", C.c_longlong)]
@@ -46,18 +52,20 @@ class MatrixInfo(C.Structure):
 
 class PrecondOptions(C.Structure):
     _fields_ = [("kind", C.c_int), ("poly_factor", C.c_double), ("poly_order", C.c_int),
-                ("poly_factor_max_iter", C.c_int)]
+                ("poly_factor_max_iter", C.c_int), ("ilu_schedule", C.c_int), ("cheb_saad", C.c_int),
+                ("cheb_lanczos", C.c_int)]
 
 
 class PrecondInfo(C.Structure):
     _fields_ = [("kind", C.c_int), ("cheb_alpha", C.c_double), ("cheb_beta", C.c_double),
-                ("ilu_levels_lower", C.c_int), ("ilu_levels_upper", C.c_int)]
+                ("ilu_levels_lower", C.c_int), ("ilu_levels_upper", C.c_int), ("ilu_schedule", C.c_int)]
 
 
 class SolverOptions(C.Structure):
     _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
                 ("poly_factor", C.c_double), ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int),
-                ("spmv_variant", C.c_int), ("use_graph", C.c_int)]
+                ("spmv_variant", C.c_int), ("use_graph", C.c_int), ("ilu_schedule", C.c_int),
+                ("cheb_saad", C.c_int), ("cheb_lanczos", C.c_int)]
 
 
 class Status(C.Structure):
@@ -87,6 +95,7 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_context_stream": (_I, [_P, C.POINTER(_P)]),
     "ab2_synchronize": (_I, [_P]),
     "ab2_context_launch_count": (_I, [_P, C.POINTER(C.c_longlong)]),
+    "ab2_context_get_info": (_I, [_P, C.POINTER(ContextInfo)]),
     "ab2_matrix_create_csr": (_I, [_P, _I, _IP, _IP, _DP, _I, C.POINTER(_P)]),
     "ab2_matrix_update_values": (_I, [_P, _P, _DP]),
     "ab2_matrix_destroy": (_I, [_P]),
@@ -200,6 +209,12 @@ class Context:
         s = _P()
         self.check(lib().ab2_context_stream(self.h, C.byref(s)))
         return s.value or 0
+
+    @property
+    def info(self) -> ContextInfo:
+        i = ContextInfo()
+        self.check(lib().ab2_context_get_info(self.h, C.byref(i)))
+        return i
 
     @property
     def launches(self) -> int:
@@ -353,9 +368,11 @@ class Vector:
 
 class Precond:
     def __init__(self, ctx: Context, A: Matrix, kind: str = "diag", poly_factor: float = 0.0, poly_order: int = 3,
-                 poly_factor_max_iter: int = 10):
+                 poly_factor_max_iter: int = 10, ilu_schedule: str = "auto", cheb_saad: bool = False,
+                 cheb_lanczos: bool = False):
         self.ctx, self.A = ctx, A
-        o = PrecondOptions(PRECOND[kind], poly_factor, poly_order, poly_factor_max_iter)
+        o = PrecondOptions(PRECOND[kind], poly_factor, poly_order, poly_factor_max_iter, ILU_SCHEDULE[ilu_schedule],
+                           int(cheb_saad), int(cheb_lanczos))
         h = _P()
         ctx.check(lib().ab2_precond_create(ctx.h, A.h, C.byref(o), C.byref(h)), "precond_create")
         self.h = h
@@ -400,7 +417,8 @@ class SolveResult:
 
 
 def solver_options(solver="cg", precond="diag", tol=1e-8, max_iter=1000, poly_factor=0.0, poly_order=3,
-                   poly_factor_max_iter=10, spmv_variant=SPMV_AUTO, use_graph=True) -> SolverOptions:
+                   poly_factor_max_iter=10, spmv_variant=SPMV_AUTO, use_graph=True,
+                   ilu_schedule="auto", cheb_saad=False, cheb_lanczos=False) -> SolverOptions:
     o = SolverOptions()
     lib().ab2_solver_options_default(C.byref(o))
     o.solver = SOLVER[solver]
@@ -412,6 +430,9 @@ def solver_options(solver="cg", precond="diag", tol=1e-8, max_iter=1000, poly_fa
     o.poly_factor_max_iter = poly_factor_max_iter
     o.spmv_variant = spmv_variant
     o.use_graph = 1 if use_graph else 0
+    o.ilu_schedule = ILU_SCHEDULE[ilu_schedule]
+    o.cheb_saad = int(cheb_saad)
+    o.cheb_lanczos = int(cheb_lanczos)
     return o
 
 

@@ -174,6 +174,8 @@ struct RedSlot {
   double* result;  // kMaxRedComps doubles on the device
 };
 RedSlot red_slot(ab2_context* ctx, int slot);
+// Blocks of every grid reduction over n values (256 threads each).
+int red_grid(const ab2_context* ctx, int n);
 
 void op_fill(ab2_context* ctx, int n, double a, double* x);
 void op_copy(ab2_context* ctx, int n, const double* x, double* y);

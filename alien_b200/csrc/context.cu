@@ -58,10 +58,14 @@ __global__ void k_amax(int n, const double* __restrict__ x, double* partials, un
   grid_reduce<1, Combine::Max>(acc, partials, counter, out);
 }
 
-// Grid of a reduction over n values: a function of n only (determinism).
-int red_grid(int n) { return grid_for(n, kThreads, kMaxRedBlocks); }
-
 }  // namespace
+
+// Grid of every reduction over n values, standalone or fused: one block per
+// 256 values, at most 8 blocks per SM.  A function of n and the device only,
+// so the summation tree -- and the rounding -- is the same on every run.
+int red_grid(const ab2_context* ctx, int n) {
+  return grid_for(n, kThreads, std::min(kMaxRedBlocks, ctx->num_sms * (2048 / kThreads)));
+}
 
 void ctx_release(ab2_context* ctx) {
   if (ctx->refs.fetch_sub(1) != 1) return;
@@ -110,17 +114,17 @@ void op_reciprocal(ab2_context* ctx, int n, double* x) {
 }
 void op_dot(ab2_context* ctx, int n, const double* x, const double* y, double* out, int slot) {
   RedSlot s = red_slot(ctx, slot);
-  k_dot<<<red_grid(n), kThreads, 0, ctx->stream>>>(n, x, y, s.partials, s.counter, out);
+  k_dot<<<red_grid(ctx, n), kThreads, 0, ctx->stream>>>(n, x, y, s.partials, s.counter, out);
   check_launch(ctx, "dot");
 }
 void op_norm1(ab2_context* ctx, int n, const double* x, double* out, int slot) {
   RedSlot s = red_slot(ctx, slot);
-  k_asum<<<red_grid(n), kThreads, 0, ctx->stream>>>(n, x, s.partials, s.counter, out);
+  k_asum<<<red_grid(ctx, n), kThreads, 0, ctx->stream>>>(n, x, s.partials, s.counter, out);
   check_launch(ctx, "norm1");
 }
 void op_norm0(ab2_context* ctx, int n, const double* x, double* out, int slot) {
   RedSlot s = red_slot(ctx, slot);
-  k_amax<<<red_grid(n), kThreads, 0, ctx->stream>>>(n, x, s.partials, s.counter, out);
+  k_amax<<<red_grid(ctx, n), kThreads, 0, ctx->stream>>>(n, x, s.partials, s.counter, out);
   check_launch(ctx, "norm0");
 }
 double read_scalar(ab2_context* ctx, const double* d) {
@@ -189,6 +193,15 @@ int ab2_context_stream(const ab2_context* ctx, void** stream) {
 int ab2_synchronize(ab2_context* ctx) {
   if (!ctx) return AB2_ERR_BAD_ARG;
   return guard(ctx, [&] { AB2_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+int ab2_context_get_info(const ab2_context* ctx, ab2_context_info* info) {
+  if (!ctx || !info) return AB2_ERR_BAD_ARG;
+  info->device = ctx->device;
+  info->num_sms = ctx->num_sms;
+  info->reduction_threads = kThreads;
+  info->reduction_max_blocks = std::min(kMaxRedBlocks, ctx->num_sms * (2048 / kThreads));
+  return AB2_OK;
 }
 
 int ab2_context_launch_count(const ab2_context* ctx, long long* count) {

@@ -70,9 +70,8 @@ __device__ __forceinline__ void set_loop(cudaGraphConditionalHandle h, int use_g
   if (use_graph) cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
-int fused_grid(ab2_context* ctx, int n) {
-  return grid_for(n, kCtlThreads, std::min(kMaxRedBlocks, ctx->num_sms * (2048 / kCtlThreads)));
-}
+static_assert(kCtlThreads == kThreads, "fused reductions use the standalone reduction tree");
+int fused_grid(ab2_context* ctx, int n) { return red_grid(ctx, n); }
 
 __global__ void k_state_init(SolveState* st, double tol, int max_iter, double* x, const double* b, double* hist,
                              int hist_cap) {
@@ -496,6 +495,9 @@ int ab2_solver_create(ab2_context* ctx, const ab2_matrix* A, const ab2_solver_op
     po.poly_factor = o->poly_factor;
     po.poly_order = o->poly_order;
     po.poly_factor_max_iter = o->poly_factor_max_iter;
+    po.ilu_schedule = o->ilu_schedule;
+    po.cheb_saad = o->cheb_saad;
+    po.cheb_lanczos = o->cheb_lanczos;
     int prc = ab2_precond_create(ctx, A, &po, &S->pc);
     if (prc != AB2_OK) throw Error{prc, ctx->last_error};
     S->pc->variant = o->spmv_variant;

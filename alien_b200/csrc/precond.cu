@@ -34,51 +34,38 @@
 
 #include "ab2_internal.cuh"
 #include "precond.cuh"
+#include "sentinel.cuh"
 #include "spmv_view.cuh"
 
 namespace ab2 {
 
 namespace {
 
-constexpr unsigned long long kSentinel = 0x7FF4A1B2C3D4E5F6ull;  // signalling NaN
-constexpr long long kWaitCycles = 4000000000LL;                  // ~2 s at 1.965 GHz
-
-__device__ __forceinline__ double ld_relaxed(const double* p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return __longlong_as_double((long long)v);
-}
-
-__device__ __forceinline__ void st_relaxed(double* p, double x) {
-  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(x))
-               : "memory");
-}
-
-// Waits until *p no longer holds the sentinel; bounded.
-__device__ __forceinline__ double wait_value(const double* p, int* err) {
-  double v = ld_relaxed(p);
-  if ((unsigned long long)__double_as_longlong(v) != kSentinel) return v;
-  const long long t0 = clock64();
-  for (unsigned it = 1;; ++it) {
-    if (it > 8) __nanosleep(it > 64 ? 256 : 32);
-    v = ld_relaxed(p);
-    if ((unsigned long long)__double_as_longlong(v) != kSentinel) return v;
-    if ((it & 63) == 0) {
-      if (clock64() - t0 > kWaitCycles || *(volatile int*)err) {
-        atomicOr(err, 1);
-        return __longlong_as_double(0x7FF8000000000000LL);
-      }
+// acc - sum_{k in [kb, ke)} a_k x[c_k], k ascending, waiting for each x value to
+// be produced.  Up to 8 dependencies are loaded at once, so a row whose inputs
+// are ready costs one round trip to L2 instead of one per dependency; only the
+// values still at the sentinel are polled again.
+__device__ __forceinline__ double sweep_row(double acc, int kb, int ke, const int* __restrict__ ci,
+                                            const double* __restrict__ lu, const double* x, int* err) {
+  for (int k0 = kb; k0 < ke; k0 += 8) {
+    double a[8], v[8];
+    int c[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const bool in = k0 + u < ke;
+      c[u] = in ? ci[k0 + u] : 0;
+      a[u] = in ? lu[k0 + u] : 0.0;
     }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = k0 + u < ke ? ld_relaxed(x + c[u]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k0 + u < ke && is_sentinel(v[u])) v[u] = wait_value(x + c[u], err);
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k0 + u < ke) acc = mul_sub_rn(a[u], v[u], acc);
   }
-}
-
-__device__ __forceinline__ double not_sentinel(double v) {
-  return (unsigned long long)__double_as_longlong(v) == kSentinel ? __longlong_as_double(0x7FF8000000000000LL) : v;
-}
-
-__global__ void k_fill_bits(long long n, unsigned long long bits, double* x) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    x[i] = __longlong_as_double((long long)bits);
+  return acc;
 }
 
 // One wavefront of the IKJ factorisation (ILU0Preconditioner.h:156-178): for
@@ -125,13 +112,7 @@ __global__ void __launch_bounds__(256) k_ilu_lsweep(int len, const int* __restri
     if (chunk >= nchunks) break;
     const int row = perm[chunk * 32 + lane];
     if (row >= 0) {
-      double acc = y[row];
-      const int e = dcol[row];
-      for (int k = rp[row]; k < e; ++k) {
-        const double l = lu[k];
-        const double xv = wait_value(t + ci[k], err);
-        acc = mul_sub_rn(l, xv, acc);
-      }
+      const double acc = sweep_row(y[row], rp[row], dcol[row], ci, lu, t, err);
       z[row] = __longlong_as_double((long long)kSentinel);
       st_relaxed(t + row, not_sentinel(acc));
     }
@@ -157,12 +138,7 @@ __global__ void __launch_bounds__(256) k_ilu_usweep(int len, const int* __restri
     if (row >= 0) {
       const int dk = dcol[row];
       const int e = rp[row + 1];
-      double acc = t[row];
-      for (int k = dk + 1; k < e; ++k) {
-        const double u = lu[k];
-        const double xv = wait_value(z + ci[k], err);
-        acc = mul_sub_rn(u, xv, acc);
-      }
+      const double acc = sweep_row(t[row], dk + 1, e, ci, lu, z, err);
       const double piv = dk < e ? lu[dk] : 0.0;
       t[row] = __longlong_as_double((long long)kSentinel);
       st_relaxed(z + row, not_sentinel(acc / piv));
@@ -182,10 +158,80 @@ __global__ void __launch_bounds__(kThreads) k_cheb_step(int n, View A, const dou
   if (row >= n) return;
   const double ay = A.row(row, ycur);
   const double r = fma(-1.0, ay, x[row]);
-  const double z = inv[row] * r;
+  const double z = __dmul_rn(inv[row], r);
   const double pn = first ? z : __dadd_rn(__dmul_rn(bcoef, p[row]), z);
   p[row] = pn;
   ynext[row] = fma(a, pn, ycur[row]);
+}
+
+// _algo1 start (ChebyshevPreconditioner.h:329-336): r = D^-1 x ; w = r / theta ; y = w.
+// x and y may be the same vector (x_i is read before y_i is written).
+__global__ void k_cheb1_start(int n, const double* x, const double* __restrict__ inv, double inv_theta,
+                              double* __restrict__ r, double* __restrict__ w, double* y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double rv = inv[i] * x[i];
+    const double wv = inv_theta * rv;
+    r[i] = rv;
+    w[i] = wv;
+    y[i] = wv;
+  }
+}
+
+// _algo1 step (:342-354): r -= D^-1 A w ; w = c1 w + c2 r ; y += w, with the
+// rounding of pointwiseMult, axpy(-1), scal, axpy(c2), axpy(1).
+template <class View>
+__global__ void __launch_bounds__(kThreads) k_cheb1_step(int n, View A, const double* __restrict__ inv,
+                                                         double* __restrict__ r, const double* __restrict__ wcur,
+                                                         double* __restrict__ wnext, double* __restrict__ y,
+                                                         double c1, double c2) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  // __dmul_rn: the products are rounded on their own, as pointwiseMult and
+  // scal round them; a plain '*' could be fused into the following update.
+  const double my = __dmul_rn(inv[row], A.row(row, wcur));
+  const double rv = fma(-1.0, my, r[row]);
+  r[row] = rv;
+  const double wv = fma(c2, rv, __dmul_rn(c1, wcur[row]));
+  wnext[row] = wv;
+  y[row] = fma(1.0, wv, y[row]);
+}
+
+__global__ void k_sqrt(int n, const double* __restrict__ a, double* __restrict__ s) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s[i] = sqrt(a[i]);
+}
+
+// Smallest and largest eigenvalue of the symmetric tridiagonal matrix with
+// diagonal a[0..m) and off-diagonal b[0..m-1): bisection on Sturm counts,
+// 128 halvings of the Gershgorin interval.
+void tridiag_extremes(const std::vector<double>& a, const std::vector<double>& b, double* lmin, double* lmax) {
+  const int m = (int)a.size();
+  double lo = a[0], hi = a[0];
+  for (int i = 0; i < m; ++i) {
+    const double rad = (i > 0 ? std::fabs(b[i - 1]) : 0.0) + (i + 1 < m ? std::fabs(b[i]) : 0.0);
+    lo = std::min(lo, a[i] - rad);
+    hi = std::max(hi, a[i] + rad);
+  }
+  auto below = [&](double x) {
+    int cnt = 0;
+    double d = 1.0;
+    for (int i = 0; i < m; ++i) {
+      d = (a[i] - x) - (i > 0 ? b[i - 1] * b[i - 1] / d : 0.0);
+      if (d == 0.0) d = -1e-300;
+      cnt += d < 0.0;
+    }
+    return cnt;
+  };
+  auto kth = [&](int k) {
+    double l = lo, h = hi;
+    for (int it = 0; it < 128; ++it) {
+      const double mid = 0.5 * (l + h);
+      if (below(mid) >= k) h = mid;
+      else l = mid;
+    }
+    return h;
+  };
+  *lmin = kth(1);
+  *lmax = kth(m);
 }
 
 __global__ void k_pmult2(int n, const double* __restrict__ a, const double* x, double* y) {
@@ -261,10 +307,9 @@ int sweep_blocks(ab2_context* ctx, int len, int widest_chunks) {
   return std::max(1, std::min(blocks, ctx->num_sms * 8));
 }
 
-void ilu_init(ab2_context* ctx, ab2_precond* pc) {
+void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule) {
   const ab2_matrix* A = pc->A;
   Ilu0Data& d = pc->ilu;
-  ilu_symbolic(A, d);
   d.d_lu = dev_alloc<double>((size_t)A->nnz);
   d.d_tmp = dev_alloc<double>((size_t)A->n);
   d.d_counters = dev_alloc<unsigned int>(2);
@@ -274,6 +319,10 @@ void ilu_init(ab2_context* ctx, ab2_precond* pc) {
   AB2_CUDA(cudaMemcpyAsync(d.d_lu, A->d_v, sizeof(double) * (size_t)A->nnz, cudaMemcpyDeviceToDevice, ctx->stream));
   k_fill_bits<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, kSentinel, d.d_tmp);
   check_launch(ctx, "ilu_fill");
+  if (schedule != AB2_ILU_WAVEFRONT && ilu_stencil_setup(ctx, A, d)) return;
+  require(schedule != AB2_ILU_STENCIL, "ILU0 tile schedule requested but the matrix is not a 3-D 7-point "
+                                       "matrix in lexicographic order");
+  ilu_symbolic(A, d);
   for (int l = 1; l < d.levels_l; ++l) {  // wavefront 0 rows have nothing left of the diagonal
     const int a = d.lev_ptr_l[l], b = d.lev_ptr_l[l + 1];
     const int cnt = b - a;
@@ -296,6 +345,8 @@ void cheb_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o) 
   double* x = dev_alloc<double>((size_t)n);
   double* y = c.d_y[0];
   double* s = red_slot(ctx, 0).result;
+  double* s_out = s;
+  c.saad = o->cheb_saad != 0;
   op_fill(ctx, n, 0.0, y);
   op_fill(ctx, n, 0.0, c.d_p);
   // Both power methods draw their start vector from a default-seeded
@@ -326,17 +377,82 @@ void cheb_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o) 
     }
     return shift ? est + b : est;
   };
-  c.beta = power(false, 0.0);
-  c.alpha = power(true, c.beta);
+  // Lanczos on S A S, S = diag(sqrt(1/a_ii)), from the same start vector:
+  // alpha = smallest Ritz value, beta = 1.1 x the largest.
+  auto lanczos = [&](int steps) {
+    double* s = dev_alloc<double>((size_t)n);
+    double* vp = dev_alloc<double>((size_t)n);
+    double* t = dev_alloc<double>((size_t)n);
+    double* w = c.d_xcopy;  // free until the first application
+    k_sqrt<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, pc->d_inv, s);
+    check_launch(ctx, "sqrt");
+    std::mt19937 gen;
+    std::uniform_real_distribution<> dis(-1., 1.);
+    for (int i = 0; i < n; ++i) h[i] = dis(gen);
+    AB2_CUDA(cudaMemcpyAsync(x, h.data(), sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    op_dot(ctx, n, x, x, s_out);
+    const double nrm = std::sqrt(read_scalar(ctx, s_out));
+    op_scal(ctx, n, 1 / nrm, x);
+    std::vector<double> ta, tb;
+    double bprev = 0.0;
+    const int m = std::max(steps, 1);
+    for (int j = 0; j < m; ++j) {
+      op_pmult(ctx, n, s, x, t);
+      op_spmv(ctx, A, t, w, pc->variant);
+      op_pmult(ctx, n, s, w, w);
+      if (j > 0) op_axpy(ctx, n, -bprev, vp, w);
+      op_dot(ctx, n, w, x, s_out);
+      const double aj = read_scalar(ctx, s_out);
+      op_axpy(ctx, n, -aj, x, w);
+      op_dot(ctx, n, w, w, s_out);
+      const double bj = std::sqrt(read_scalar(ctx, s_out));
+      ta.push_back(aj);
+      if (bj == 0.0 || j + 1 == m) break;
+      tb.push_back(bj);
+      op_copy(ctx, n, x, vp);
+      op_copy(ctx, n, w, x);
+      op_scal(ctx, n, 1 / bj, x);
+      bprev = bj;
+    }
+    double lmin = 0.0, lmax = 0.0;
+    tridiag_extremes(ta, tb, &lmin, &lmax);
+    c.alpha = lmin;
+    c.beta = 1.1 * lmax;
+    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+    dev_free(s);
+    dev_free(vp);
+    dev_free(t);
+  };
+  if (o->cheb_lanczos) {
+    lanczos(o->poly_factor_max_iter);
+  } else {
+    c.beta = power(false, 0.0);
+    c.alpha = power(true, c.beta);
+  }
   if (o->poly_factor != 0.) c.alpha = c.beta / o->poly_factor;
   dev_free(x);
   op_fill(ctx, n, 0.0, y);
-  // Step coefficients of _algo2, evaluated in the reference's order.
-  const double dd = (c.beta + c.alpha) / 2;
-  const double cc = (c.beta - c.alpha) / 2;
   const int steps = std::max(1, c.order);
   c.a.assign(steps, 0.0);
   c.b.assign(steps, 0.0);
+  if (c.saad) {
+    // _algo1 scalars (ChebyshevPreconditioner.h:316-351), in the reference's order.
+    const double delta = (c.beta - c.alpha) / 2;
+    const double theta = (c.beta + c.alpha) / 2;
+    const double sigma = theta / delta;
+    double rho_old = 1. / sigma;
+    c.inv_theta = 1 / theta;
+    for (int k = 1; k < steps; ++k) {
+      const double rho = 1. / (2 * sigma - rho_old);
+      c.a[k] = rho * rho_old;
+      c.b[k] = 2 * rho / delta;
+      rho_old = rho;
+    }
+    return;
+  }
+  // Step coefficients of _algo2, evaluated in the reference's order.
+  const double dd = (c.beta + c.alpha) / 2;
+  const double cc = (c.beta - c.alpha) / 2;
   double a = 2 / dd;
   c.a[0] = a;
   for (int i = 1; i < steps; ++i) {
@@ -361,6 +477,10 @@ void pc_apply(ab2_context* ctx, const ab2_precond* pc, const double* x, double* 
     case AB2_PC_ILU0: {
       const Ilu0Data& d = pc->ilu;
       const ab2_matrix* A = pc->A;
+      if (d.stencil) {
+        ilu_stencil_apply(ctx, A, d, x, y);
+        break;
+      }
       k_ilu_lsweep<<<sweep_blocks(ctx, d.len_l, d.widest_l), 256, 0, ctx->stream>>>(
           d.len_l, d.d_perm_l, A->d_rp, A->d_ci, A->d_dcol, d.d_lu, x, d.d_tmp, y, d.d_counters, d.d_err);
       check_launch(ctx, "ilu_lsweep");
@@ -371,12 +491,27 @@ void pc_apply(ab2_context* ctx, const ab2_precond* pc, const double* x, double* 
     }
     case AB2_PC_CHEB: {
       const ChebData& c = pc->cheb;
+      const int steps = std::max(1, c.order);
+      if (c.saad) {
+        double* r = c.d_p;
+        k_cheb1_start<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, x, pc->d_inv, c.inv_theta, r, c.d_y[0], y);
+        check_launch(ctx, "cheb1_start");
+        for (int k = 1; k < steps; ++k) {
+          const double* wcur = c.d_y[(k - 1) & 1];
+          double* wnext = c.d_y[k & 1];
+          with_view<double>(pc->A, pc->variant, [&](auto view) {
+            k_cheb1_step<<<(n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(n, view, pc->d_inv, r, wcur,
+                                                                                      wnext, y, c.a[k], c.b[k]);
+          });
+          check_launch(ctx, "cheb1_step");
+        }
+        break;
+      }
       const double* xin = x;
       if (x == y) {
         op_copy(ctx, n, x, c.d_xcopy);
         xin = c.d_xcopy;
       }
-      const int steps = std::max(1, c.order);
       const double* cur = xin;
       for (int i = 0; i < steps; ++i) {
         double* next = (i == steps - 1) ? y : c.d_y[i & 1];
@@ -400,6 +535,8 @@ void pc_reset(ab2_context* ctx, const ab2_precond* pc) {
   k_fill_bits<<<grid_for(pc->A->n), kThreads, 0, ctx->stream>>>(pc->A->n, kSentinel, d.d_tmp);
   check_launch(ctx, "ilu_fill");
   AB2_CUDA(cudaMemsetAsync(d.d_counters, 0, 2 * sizeof(unsigned int), ctx->stream));
+  if (d.d_tile_tickets) AB2_CUDA(cudaMemsetAsync(d.d_tile_tickets, 0, 3 * sizeof(unsigned int), ctx->stream));
+  if (d.stencil) ilu_stencil_reset(ctx, d);
   AB2_CUDA(cudaMemsetAsync(d.d_err, 0, sizeof(int), ctx->stream));
 }
 
@@ -432,7 +569,10 @@ int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_
       // init(): assign(inv, 1) then computeInvDiag (DiagPreconditioner.h:49-54)
       op_inv_diag(ctx, A, pc->d_inv);
     }
-    if (o->kind == AB2_PC_ILU0) ilu_init(ctx, pc);
+    if (o->kind == AB2_PC_ILU0) {
+      require(o->ilu_schedule >= AB2_ILU_AUTO && o->ilu_schedule <= AB2_ILU_STENCIL, "unknown ILU0 schedule");
+      ilu_init(ctx, pc, o->ilu_schedule);
+    }
     if (o->kind == AB2_PC_CHEB) {
       require(o->poly_factor_max_iter >= 0, "poly_factor_max_iter must be >= 0");
       cheb_init(ctx, pc, o);
@@ -462,6 +602,8 @@ int ab2_precond_destroy(ab2_precond* pc) {
   dev_free(pc->ilu.d_tmp);
   dev_free(pc->ilu.d_counters);
   dev_free(pc->ilu.d_err);
+  dev_free(pc->ilu.d_bands);
+  dev_free(pc->ilu.d_tile_tickets);
   dev_free(pc->cheb.d_p);
   dev_free(pc->cheb.d_y[0]);
   dev_free(pc->cheb.d_y[1]);
@@ -478,6 +620,7 @@ int ab2_precond_get_info(const ab2_precond* pc, ab2_precond_info* info) {
   info->cheb_beta = pc->cheb.beta;
   info->ilu_levels_lower = pc->ilu.levels_l;
   info->ilu_levels_upper = pc->ilu.levels_u;
+  info->ilu_schedule = pc->kind != AB2_PC_ILU0 ? 0 : pc->ilu.stencil ? AB2_ILU_STENCIL : AB2_ILU_WAVEFRONT;
   return AB2_OK;
 }
 

@@ -5,7 +5,11 @@
 
 #include "ab2_internal.cuh"
 
+struct ab2_matrix;
+
 namespace ab2 {
+
+struct Ilu0Data;
 
 // ILU(0) on the device.  The factor keeps the CSR profile of A (L strictly
 // below dcol with unit diagonal implied, U from dcol on), as
@@ -24,15 +28,29 @@ struct Ilu0Data {
   double* d_tmp = nullptr;          // L-sweep output, left at the sentinel between applications
   unsigned int* d_counters = nullptr;  // [0]: L-sweep chunk ticket, [1]: U-sweep chunk ticket
   int* d_err = nullptr;             // set when a bounded wait gives up
+  // 7-point lexicographic matrices: tile-walk schedule (ilu_stencil.cu)
+  bool stencil = false;
+  int st_nx = 0, st_ny = 0, st_nz = 0;
+  double* d_bands = nullptr;            // 8 n-vectors: L(-k,-j,-i) U(+i,+j,+k) pivot diag
+  unsigned int* d_tile_tickets = nullptr;  // factorisation, L sweep, U sweep
 };
+
+// Detects a 3-D 7-point matrix in lexicographic order and, if found,
+// factorises it on the tile-walk schedule (bands + CSR copy in d_lu).
+bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d);
+void ilu_stencil_apply(ab2_context* ctx, const ab2_matrix* A, const Ilu0Data& d, const double* y, double* z);
+// Puts the sweeps' propagation arrays back to the sentinel (after a failed application).
+void ilu_stencil_reset(ab2_context* ctx, const Ilu0Data& d);
 
 struct ChebData {
   double alpha = 0, beta = 0;
   int order = 0;
-  std::vector<double> a;   // alpha_i of each step (step 0: 2/d)
-  std::vector<double> b;   // beta_i of each step >= 1
-  double* d_p = nullptr;
-  double* d_y[2] = {nullptr, nullptr};
+  bool saad = false;
+  std::vector<double> a;   // _algo2: alpha_i of each step (step 0: 2/d); _algo1: rho rho_old of step i
+  std::vector<double> b;   // _algo2: beta_i of each step >= 1;          _algo1: 2 rho / delta of step i
+  double inv_theta = 0;    // _algo1: 1 / theta
+  double* d_p = nullptr;   // _algo2: p; _algo1: r
+  double* d_y[2] = {nullptr, nullptr};  // _algo2: iterates; _algo1: w (ping-pong)
   double* d_xcopy = nullptr;
 };
 

@@ -1,0 +1,70 @@
+// sentinel.cuh -- value-as-flag synchronisation for the triangular sweeps.
+//
+// A sweep's output vector is pre-filled with a signalling-NaN bit pattern that
+// arithmetic never produces (results of arithmetic are quiet NaNs).  A
+// producer stores the final 8-byte value with st.relaxed.gpu; a consumer polls
+// the word with ld.relaxed.gpu until it is no longer the sentinel.  Because
+// the payload is the flag, no fence or separate ready bit is needed.  Every
+// wait is bounded by a clock64 budget: on expiry the waiter records an error
+// and returns a quiet NaN, so a kernel always finishes.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace ab2 {
+namespace {
+
+constexpr unsigned long long kSentinel = 0x7FF4A1B2C3D4E5F6ull;  // signalling NaN
+constexpr long long kWaitCycles = 4000000000LL;                  // ~2 s at 1.965 GHz
+
+// No "memory" clobber: the load must not be merged or hoisted out of a
+// polling loop (volatile), but ordinary loads around it may still be
+// scheduled freely; the value is the synchronisation.
+__device__ __forceinline__ double ld_relaxed(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
+  return __longlong_as_double((long long)v);
+}
+
+__device__ __forceinline__ void st_relaxed(double* p, double x) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(x))
+               : "memory");
+}
+
+__device__ __forceinline__ bool is_sentinel(double v) {
+  return (unsigned long long)__double_as_longlong(v) == kSentinel;
+}
+
+__device__ __forceinline__ double sentinel_value() { return __longlong_as_double((long long)kSentinel); }
+
+// Waits until *p no longer holds the sentinel; bounded.
+__device__ __forceinline__ double wait_value(const double* p, int* err) {
+  double v = ld_relaxed(p);
+  if (!is_sentinel(v)) return v;
+  const long long t0 = clock64();
+  for (unsigned it = 1;; ++it) {
+    if (it > 8) __nanosleep(it > 64 ? 256 : 32);
+    v = ld_relaxed(p);
+    if (!is_sentinel(v)) return v;
+    if ((it & 63) == 0) {
+      if (clock64() - t0 > kWaitCycles || *(volatile int*)err) {
+        atomicOr(err, 1);
+        return __longlong_as_double(0x7FF8000000000000LL);
+      }
+    }
+  }
+}
+
+// A computed value that happens to carry the sentinel's bits (only possible
+// if it was copied from an input holding them) is stored as a quiet NaN.
+__device__ __forceinline__ double not_sentinel(double v) {
+  return is_sentinel(v) ? __longlong_as_double(0x7FF8000000000000LL) : v;
+}
+
+__global__ void k_fill_bits(long long n, unsigned long long bits, double* x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = __longlong_as_double((long long)bits);
+}
+
+}  // namespace
+}  // namespace ab2

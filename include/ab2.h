@@ -84,6 +84,19 @@ int ab2_synchronize(ab2_context* ctx);
 /* number of kernels libab2 has launched on this context since creation */
 int ab2_context_launch_count(const ab2_context* ctx, long long* count);
 
+/* Every dot product and norm is a grid reduction of reduction_threads-thread
+ * blocks, one block per reduction_threads values up to reduction_max_blocks
+ * blocks; each thread sums its strided values with fma, blocks and then the
+ * block partials are combined by fixed shuffle trees.  The tree depends only
+ * on n and the device, so results are reproducible bit for bit. */
+typedef struct {
+  int device;
+  int num_sms;
+  int reduction_threads;
+  int reduction_max_blocks;
+} ab2_context_info;
+int ab2_context_get_info(const ab2_context* ctx, ab2_context_info* info);
+
 /* ------------------------------------------------------------------ matrix */
 /* Copies a host CSR matrix (columns sorted ascending inside each row, as
  * Alien's profilers produce) to the device in the requested formats.
@@ -160,11 +173,27 @@ int ab2_scalar_get(ab2_context* ctx, const ab2_scalar* s, double* value);
 int ab2_dot_noalloc(const double* x, const double* y, int n, double* result, void* stream);
 
 /* ------------------------------------------------------------------ preconditioners */
+/* ILU(0) schedules; both give the same factor and applications bit for bit.
+ * WAVEFRONT: any CSR matrix; rows grouped by wavefront of the triangular
+ *   graphs, one warp per 32 rows, cross-warp waits through global memory.
+ * STENCIL: 3-D 7-point matrices in lexicographic order; 16x16 tiles of
+ *   grid lines per CTA walk their diagonals through shared memory.
+ * AUTO: STENCIL when the matrix has that structure, else WAVEFRONT. */
+#define AB2_ILU_AUTO 0
+#define AB2_ILU_WAVEFRONT 1
+#define AB2_ILU_STENCIL 2
+
 typedef struct {
   int kind;                 /* AB2_PC_* */
   double poly_factor;       /* Chebyshev: 0 = both bounds by power method; else alpha = beta/factor */
   int poly_order;           /* Chebyshev polynomial order (3 = three SpMVs per application) */
-  int poly_factor_max_iter; /* Chebyshev: power-method steps per bound */
+  int poly_factor_max_iter; /* Chebyshev: power-method steps per bound (Lanczos steps with cheb_lanczos) */
+  int ilu_schedule;         /* AB2_ILU_* */
+  int cheb_saad;    /* 0: ChebyshevPreconditioner<.., false> (_algo2, y starts at x, the reference default);
+                       1: ChebyshevPreconditioner<.., true> (_algo1, y starts at 0: a symmetric operator) */
+  int cheb_lanczos; /* 0: bounds by the reference's two power methods; 1: alpha = smallest and
+                       beta = 1.1 x largest Ritz value of poly_factor_max_iter Lanczos steps on
+                       D^-1/2 A D^-1/2 (no counterpart in the reference) */
 } ab2_precond_options;
 
 /* init(): Diag computes 1/a_ii; ILU0 factorises on the device; Chebyshev
@@ -179,6 +208,7 @@ typedef struct {
   double cheb_beta;  /* upper bound used by Chebyshev */
   int ilu_levels_lower; /* wavefronts of the L sweep */
   int ilu_levels_upper; /* wavefronts of the U sweep */
+  int ilu_schedule;     /* AB2_ILU_WAVEFRONT or AB2_ILU_STENCIL as chosen */
 } ab2_precond_info;
 int ab2_precond_get_info(const ab2_precond* pc, ab2_precond_info* info);
 /* ILU(0) factor values in CSR order (row_ptr[n] doubles), for checking. */
@@ -195,6 +225,9 @@ typedef struct {
   int poly_factor_max_iter;
   int spmv_variant; /* AB2_SPMV_* used inside the loop */
   int use_graph;    /* 1: iteration loop in a CUDA graph with a device-side while condition */
+  int ilu_schedule; /* AB2_ILU_* */
+  int cheb_saad;    /* see ab2_precond_options */
+  int cheb_lanczos;
 } ab2_solver_options;
 
 typedef struct {

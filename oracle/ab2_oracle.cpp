@@ -64,6 +64,13 @@ typedef struct {
   double poly_factor;       // Chebyshev "factor" (0 = computed bounds)
   int poly_order;           // Chebyshev polynomial order
   int poly_factor_max_iter; // power-method steps for each bound
+  // Summation order of every dot product: 0 = sequential (one admissible
+  // cblas_ddot order, the reference templates' shim uses it); 1 = libab2's
+  // device tree with `tree_blocks` blocks at most (bit-exact GPU checks).
+  int dot_mode;
+  int tree_blocks;
+  int cheb_saad;     // 1: ChebyshevPreconditioner<AlgebraT, true> (_algo1)
+  int cheb_lanczos;  // 1: bounds from poly_factor_max_iter Lanczos steps
 } orc_options;
 
 typedef struct {
@@ -84,6 +91,59 @@ namespace {
 
 using namespace ab2_oracle;
 
+// One warp's __shfl_down_sync tree (offsets 16..1): lane l adds lane l+off's
+// value when l+off < 32; the result is lane 0's.
+double warp_tree(const double* in) {
+  double v[32], w[32];
+  for (int l = 0; l < 32; ++l) v[l] = in[l];
+  for (int off = 16; off > 0; off >>= 1) {
+    for (int l = 0; l < 32; ++l) w[l] = v[l] + (l + off < 32 ? v[l + off] : v[l]);
+    for (int l = 0; l < 32; ++l) v[l] = w[l];
+  }
+  return v[0];
+}
+
+// libab2's deterministic grid reduction (reduce.cuh), restated: G blocks of
+// 256 threads, G = min(max(ceil(n/256), 1), max_blocks); thread g sums
+// x_i y_i for i = g, g + 256G, ... with fma; each warp's values go through
+// warp_tree, the 8 warp sums through another; then lane l of the last block
+// adds the block partials l, l+32, ... in order and a final warp_tree.
+double tree_dot(int n, const double* x, const double* y, int max_blocks) {
+  const int T = 256;
+  long long g = ((long long)n + T - 1) / T;
+  if (g < 1) g = 1;
+  if (g > max_blocks) g = max_blocks;
+  const int G = (int)g;
+  const long long stride = (long long)G * T;
+  std::vector<double> partial(G);
+  double th[256], ws[32];
+  for (int b = 0; b < G; ++b) {
+    for (int t = 0; t < T; ++t) {
+      double acc = 0.0;
+      for (long long i = (long long)b * T + t; i < n; i += stride) acc = std::fma(x[i], y[i], acc);
+      th[t] = acc;
+    }
+    for (int l = 0; l < 32; ++l) ws[l] = l < T / 32 ? warp_tree(th + 32 * l) : 0.0;
+    partial[b] = warp_tree(ws);
+  }
+  double lanes[32];
+  for (int l = 0; l < 32; ++l) {
+    double s = 0.0;
+    for (int b = l; b < G; b += 32) s = s + partial[b];
+    lanes[l] = s;
+  }
+  return warp_tree(lanes);
+}
+
+thread_local int g_dot_mode = 0;
+thread_local int g_tree_blocks = 1184;
+thread_local bool g_cheb_saad = false;
+thread_local bool g_cheb_lanczos = false;
+
+double vdot(int n, const double* x, const double* y) {
+  return g_dot_mode == 1 ? tree_dot(n, x, y, g_tree_blocks) : dot(n, x, y);
+}
+
 // Stop test shared by CG (Iteration.h) and BiCGStab (its nested Iteration).
 struct StopTest {
   int n;
@@ -99,14 +159,14 @@ struct StopTest {
 
   StopTest(int n_, const double* b, double tol, int max_it, double* h, int cap)
       : n(n_), max_iter(max_it), hist(h), hist_cap(cap) {
-    nrm2_b = dot(n, b, b);
+    nrm2_b = vdot(n,b, b);
     criteria = tol * tol * nrm2_b;
     status = (nrm2_b == 0.0);
   }
   bool null_rhs() const { return nrm2_b == 0.0; }
   bool stop(const double* r) {
     if (iter >= max_iter) return true;
-    last = dot(n, r, r);
+    last = vdot(n,r, r);
     if (hist && hist_len < hist_cap) hist[hist_len] = last;
     ++hist_len;
     status = last < criteria;
@@ -190,21 +250,100 @@ struct Ilu0 : Precond {
 };
 
 // Chebyshev polynomial preconditioner, non-Saad branch (_algo2).
+// Smallest and largest eigenvalue of the symmetric tridiagonal matrix with
+// diagonal a[0..m) and off-diagonal b[0..m-1), by bisection on Sturm counts
+// (128 halvings of the Gershgorin interval).
+void tridiag_extremes(const std::vector<double>& a, const std::vector<double>& b, double* lmin, double* lmax) {
+  const int m = (int)a.size();
+  double lo = a[0], hi = a[0];
+  for (int i = 0; i < m; ++i) {
+    const double r = (i > 0 ? std::fabs(b[i - 1]) : 0.0) + (i + 1 < m ? std::fabs(b[i]) : 0.0);
+    lo = std::min(lo, a[i] - r);
+    hi = std::max(hi, a[i] + r);
+  }
+  auto below = [&](double x) {  // eigenvalues < x
+    int cnt = 0;
+    double d = 1.0;
+    for (int i = 0; i < m; ++i) {
+      d = (a[i] - x) - (i > 0 ? b[i - 1] * b[i - 1] / d : 0.0);
+      if (d == 0.0) d = -1e-300;
+      cnt += d < 0.0;
+    }
+    return cnt;
+  };
+  auto kth = [&](int k) {  // smallest x with below(x) >= k
+    double l = lo, h = hi;
+    for (int it = 0; it < 128; ++it) {
+      const double mid = 0.5 * (l + h);
+      if (below(mid) >= k) h = mid;
+      else l = mid;
+    }
+    return h;
+  };
+  *lmin = kth(1);
+  *lmax = kth(m);
+}
+
 struct Cheb : Precond {
   const Csr A;
   int n;
   int order;
-  std::vector<double> inv, y_, r_, p_, z_;
+  bool saad;
+  std::vector<double> inv, y_, r_, p_, z_, w_;
   double alpha = 0.0, beta = 0.0;
 
-  Cheb(const Csr& A_, double factor, int order_, int max_iter)
-      : A(A_), n(A_.n), order(order_), inv(A_.n, 1.0), y_(A_.n, 0.0), r_(A_.n, 0.0), p_(A_.n, 0.0),
-        z_(A_.n, 0.0) {
+  // saad: ChebyshevPreconditioner<AlgebraT, true> (_algo1, zero start, a
+  // symmetric operator); otherwise the default _algo2.  lanczos: bounds from
+  // `max_iter` Lanczos steps on D^-1/2 A D^-1/2 (this repo's addition)
+  // instead of the reference's two power methods.
+  Cheb(const Csr& A_, double factor, int order_, int max_iter, bool saad_ = false, bool lanczos = false)
+      : A(A_), n(A_.n), order(order_), saad(saad_), inv(A_.n, 1.0), y_(A_.n, 0.0), r_(A_.n, 0.0), p_(A_.n, 0.0),
+        z_(A_.n, 0.0), w_(A_.n, 0.0) {
     std::vector<int> d = diag_offsets(A);
     for (int i = 0; i < n; ++i) inv[i] = 1.0 / A.v[d[i]];
-    beta = power_bound(max_iter, /*shift=*/false, 0.0);
-    alpha = power_bound(max_iter, /*shift=*/true, beta);
+    if (lanczos) {
+      lanczos_bounds(max_iter);
+    } else {
+      beta = power_bound(max_iter, /*shift=*/false, 0.0);
+      alpha = power_bound(max_iter, /*shift=*/true, beta);
+    }
     if (factor != 0.0) alpha = beta / factor;
+  }
+
+  // Lanczos on B = S A S, S = diag(sqrt(1/a_ii)), from the same mt19937 start
+  // vector as the power methods; alpha = smallest Ritz value, beta = 1.1 x the
+  // largest (Ritz values lie inside the spectrum; the margin keeps the
+  // polynomial positive on all of it).
+  void lanczos_bounds(int steps) {
+    std::vector<double> s(n), v(n), vp(n, 0.0), t(n), w(n);
+    for (int i = 0; i < n; ++i) s[i] = std::sqrt(inv[i]);
+    std::mt19937 gen;
+    std::uniform_real_distribution<> dis(-1., 1.);
+    for (int i = 0; i < n; ++i) v[i] = dis(gen);
+    const double nrm = std::sqrt(vdot(n, v.data(), v.data()));
+    scal(n, 1 / nrm, v.data());
+    std::vector<double> a, b;
+    double bprev = 0.0;
+    for (int j = 0; j < std::max(steps, 1); ++j) {
+      pmult(n, s.data(), v.data(), t.data());
+      spmv(A, t.data(), w.data());
+      pmult(n, s.data(), w.data(), w.data());
+      if (j > 0) axpy(n, -bprev, vp.data(), w.data());
+      const double aj = vdot(n, w.data(), v.data());
+      axpy(n, -aj, v.data(), w.data());
+      const double bj = std::sqrt(vdot(n, w.data(), w.data()));
+      a.push_back(aj);
+      if (bj == 0.0 || j + 1 == std::max(steps, 1)) break;
+      b.push_back(bj);
+      copy(n, v.data(), vp.data());
+      copy(n, w.data(), v.data());
+      scal(n, 1 / bj, v.data());
+      bprev = bj;
+    }
+    double lmin = 0.0, lmax = 0.0;
+    tridiag_extremes(a, b, &lmin, &lmax);
+    alpha = lmin;
+    beta = 1.1 * lmax;
   }
 
   // computeBeta (:118-156) when shift is false, computeAlpha (:158-202) otherwise.
@@ -215,17 +354,17 @@ struct Cheb : Precond {
     std::mt19937 gen;
     std::uniform_real_distribution<> dis(-1., 1.);
     for (int i = 0; i < n; ++i) x[i] = dis(gen);
-    double nrm = std::sqrt(dot(n, x.data(), x.data()));
+    double nrm = std::sqrt(vdot(n,x.data(), x.data()));
     scal(n, 1 / nrm, x.data());
     double est = 0.0;
     for (int it = 0; it < max_iter; ++it) {
       spmv(A, x.data(), y_.data());
       pmult(n, inv.data(), y_.data(), y_.data());
       if (shift) axpy(n, -b, x.data(), y_.data());
-      const double xax = dot(n, y_.data(), x.data());
-      const double xdx = dot(n, x.data(), x.data());
+      const double xax = vdot(n,y_.data(), x.data());
+      const double xdx = vdot(n,x.data(), x.data());
       est = xax / xdx;
-      const double nr = std::sqrt(dot(n, y_.data(), y_.data()));
+      const double nr = std::sqrt(vdot(n,y_.data(), y_.data()));
       scal(n, 1 / nr, y_.data());
       copy(n, y_.data(), x.data());
     }
@@ -233,7 +372,8 @@ struct Cheb : Precond {
     return est;
   }
 
-  void apply(const double* x, double* y) override {
+  // _algo2 (ChebyshevPreconditioner.h:392-434), the default.
+  void apply_default(const double* x, double* y) {
     const double dd = (beta + alpha) / 2;
     const double c = (beta - alpha) / 2;
     copy(n, x, y);
@@ -256,6 +396,35 @@ struct Cheb : Precond {
       axpy(n, a, p_.data(), y);
     }
   }
+
+  void apply(const double* x, double* y) override {
+    if (saad) apply_saad(x, y);
+    else apply_default(x, y);
+  }
+
+  // _algo1 (ChebyshevPreconditioner.h:286-360): r = D^-1 x, w = r / theta,
+  // y = w, then order-1 steps of the three-term recurrence.
+  void apply_saad(const double* x, double* y) {
+    const double delta = (beta - alpha) / 2;
+    const double theta = (beta + alpha) / 2;
+    pmult(n, inv.data(), x, r_.data());
+    const double sigma = theta / delta;
+    double rho_old = 1. / sigma;
+    double rho = rho_old;
+    copy(n, r_.data(), w_.data());
+    scal(n, 1 / theta, w_.data());
+    copy(n, w_.data(), y);
+    for (int k = 1; k < order; ++k) {
+      spmv(A, w_.data(), y_.data());
+      pmult(n, inv.data(), y_.data(), y_.data());
+      axpy(n, -1., y_.data(), r_.data());
+      rho = 1. / (2 * sigma - rho_old);
+      scal(n, rho * rho_old, w_.data());
+      axpy(n, 2 * rho / delta, r_.data(), w_.data());
+      axpy(n, 1., w_.data(), y);
+      rho_old = rho;
+    }
+  }
 };
 
 // ---------------------------------------------------------------- solvers
@@ -269,10 +438,10 @@ void cg(const Csr& A, Precond& M, StopTest& it, const double* b, double* x) {
   axpy(n, -1., p.data(), r.data());
 
   M.apply(r.data(), z.data());
-  rho1 = dot(n, r.data(), z.data());
+  rho1 = vdot(n,r.data(), z.data());
   copy(n, z.data(), p.data());
   spmv(A, p.data(), q.data());
-  alpha = dot(n, p.data(), q.data());
+  alpha = vdot(n,p.data(), q.data());
   if (alpha == 0) {
     if (it.stop(r.data())) { it.next(); return; }
     throw Breakdown{ORC_BD_ALPHA};
@@ -285,12 +454,12 @@ void cg(const Csr& A, Precond& M, StopTest& it, const double* b, double* x) {
 
   while (!it.stop(r.data())) {
     M.apply(r.data(), z.data());
-    rho1 = dot(n, r.data(), z.data());
+    rho1 = vdot(n,r.data(), z.data());
     alpha = rho1 / rho;
     axpy(n, alpha, p.data(), z.data());
     copy(n, z.data(), p.data());
     spmv(A, p.data(), q.data());
-    alpha = dot(n, q.data(), p.data());
+    alpha = vdot(n,q.data(), p.data());
     if (alpha == 0) {
       if (it.stop(r.data())) { it.next(); return; }
       throw Breakdown{ORC_BD_ALPHA};
@@ -314,11 +483,11 @@ void bicgstab(const Csr& A, Precond& M, StopTest& it, const double* b, double* x
   axpy(n, -1., r0.data(), r.data());
   copy(n, r.data(), r0.data());
   copy(n, r.data(), p.data());
-  rho1 = dot(n, r.data(), r0.data());
+  rho1 = vdot(n,r.data(), r0.data());
 
   M.apply(p.data(), phat.data());
   spmv(A, phat.data(), v.data());
-  alpha = dot(n, v.data(), r0.data());
+  alpha = vdot(n,v.data(), r0.data());
   if (alpha == 0) throw Breakdown{ORC_BD_ALPHA};
   alpha = rho1 / alpha;
   copy(n, r.data(), s.data());
@@ -332,8 +501,8 @@ void bicgstab(const Csr& A, Precond& M, StopTest& it, const double* b, double* x
 
   M.apply(s.data(), shat.data());
   spmv(A, shat.data(), t.data());
-  omega = dot(n, t.data(), s.data());
-  beta = dot(n, t.data(), t.data());
+  omega = vdot(n,t.data(), s.data());
+  beta = vdot(n,t.data(), t.data());
   if (beta == 0) {
     if (it.stop(r.data())) {
       it.next();
@@ -351,7 +520,7 @@ void bicgstab(const Csr& A, Precond& M, StopTest& it, const double* b, double* x
   it.next();
 
   while (!it.stop(r.data())) {
-    rho1 = dot(n, r.data(), r0.data());
+    rho1 = vdot(n,r.data(), r0.data());
     beta = (rho1 / rho) * (alpha / omega);
     axpy(n, -omega, v.data(), p.data());
     scal(n, beta, p.data());
@@ -360,7 +529,7 @@ void bicgstab(const Csr& A, Precond& M, StopTest& it, const double* b, double* x
 
     M.apply(p.data(), phat.data());
     spmv(A, phat.data(), v.data());
-    alpha = dot(n, v.data(), r0.data());
+    alpha = vdot(n,v.data(), r0.data());
     if (alpha == 0) throw Breakdown{ORC_BD_ALPHA};
     alpha = rho1 / alpha;
     copy(n, r.data(), s.data());
@@ -373,8 +542,8 @@ void bicgstab(const Csr& A, Precond& M, StopTest& it, const double* b, double* x
 
     M.apply(s.data(), shat.data());
     spmv(A, shat.data(), t.data());
-    omega = dot(n, t.data(), s.data());
-    beta = dot(n, t.data(), t.data());
+    omega = vdot(n,t.data(), s.data());
+    beta = vdot(n,t.data(), t.data());
     if (beta == 0) {
       if (it.stop(s.data())) {
         axpy(n, alpha, phat.data(), x);
@@ -443,6 +612,9 @@ int orc_inv_diag(int n, const int* rp, const int* ci, const double* v, double* i
 
 double orc_dot(int n, const double* x, const double* y) { return dot(n, x, y); }
 
+// The device's reduction tree (see tree_dot), for bit-exact checks of libab2.
+double orc_dot_tree(int n, const double* x, const double* y, int max_blocks) { return tree_dot(n, x, y, max_blocks); }
+
 // y += a x (cblas_daxpy, CBLASMPIKernel.h:48-53)
 int orc_axpy(int n, double a, const double* x, double* y) {
   axpy(n, a, x, y);
@@ -468,10 +640,18 @@ int orc_ilu0_apply(int n, const int* rp, const int* ci, const double* v, const d
   return ORC_OK;
 }
 
+// Dot summation order for the calls that take no options (Chebyshev set-up
+// and application); orc_solve sets it from its options.
+int orc_set_dot_mode(int mode, int tree_blocks) {
+  g_dot_mode = mode;
+  g_tree_blocks = tree_blocks > 0 ? tree_blocks : 1184;
+  return ORC_OK;
+}
+
 // Chebyshev bounds (alpha = lambda_min estimate, beta = lambda_max estimate).
 int orc_cheb_bounds(int n, const int* rp, const int* ci, const double* v, double factor, int max_iter,
                     double* alpha, double* beta) {
-  Cheb c(Csr{n, rp, ci, v}, factor, 1, max_iter);
+  Cheb c(Csr{n, rp, ci, v}, factor, 1, max_iter, g_cheb_saad, g_cheb_lanczos);
   *alpha = c.alpha;
   *beta = c.beta;
   return ORC_OK;
@@ -479,8 +659,15 @@ int orc_cheb_bounds(int n, const int* rp, const int* ci, const double* v, double
 
 int orc_cheb_apply(int n, const int* rp, const int* ci, const double* v, double factor, int order,
                    int max_iter, const double* x, double* y) {
-  Cheb c(Csr{n, rp, ci, v}, factor, order, max_iter);
+  Cheb c(Csr{n, rp, ci, v}, factor, order, max_iter, g_cheb_saad, g_cheb_lanczos);
   c.apply(x, y);
+  return ORC_OK;
+}
+
+// Chebyshev variant for the two calls above (orc_solve takes it as options).
+int orc_set_cheb_variant(int saad, int lanczos) {
+  g_cheb_saad = saad != 0;
+  g_cheb_lanczos = lanczos != 0;
   return ORC_OK;
 }
 
@@ -490,6 +677,8 @@ int orc_solve(int n, const int* rp, const int* ci, const double* v, const double
               const orc_options* o, orc_result* res, double* hist, int hist_cap) {
   if (!o || !res || n < 0) return ORC_ERR_BAD_ARG;
   std::memset(res, 0, sizeof(*res));
+  g_dot_mode = o->dot_mode;
+  g_tree_blocks = o->tree_blocks > 0 ? o->tree_blocks : 1184;
   Csr A{n, rp, ci, v};
   Identity pid(n);
   Diag* pd = nullptr;
@@ -501,7 +690,8 @@ int orc_solve(int n, const int* rp, const int* ci, const double* v, const double
     case ORC_PC_DIAG: M = pd = new Diag(A); break;
     case ORC_PC_ILU0: M = pi = new Ilu0(A); break;
     case ORC_PC_CHEB:
-      M = pc = new Cheb(A, o->poly_factor, o->poly_order, o->poly_factor_max_iter);
+      M = pc = new Cheb(A, o->poly_factor, o->poly_order, o->poly_factor_max_iter, o->cheb_saad != 0,
+                        o->cheb_lanczos != 0);
       res->cheb_alpha = pc->alpha;
       res->cheb_beta = pc->beta;
       break;

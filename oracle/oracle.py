@@ -30,8 +30,14 @@ BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho", 9: "other"}
 
 
 class Options(C.Structure):
+    # The reference driver reads the first seven fields only.
     _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
-                ("poly_factor", C.c_double), ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int)]
+                ("poly_factor", C.c_double), ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int),
+                ("dot_mode", C.c_int), ("tree_blocks", C.c_int), ("cheb_saad", C.c_int),
+                ("cheb_lanczos", C.c_int)]
+
+
+DOT_SEQUENTIAL, DOT_DEVICE_TREE = 0, 1
 
 
 class Result(C.Structure):
@@ -85,6 +91,10 @@ def orc() -> C.CDLL:
         L.orc_inv_diag.argtypes = [C.c_int, _IP, _IP, _DP, _DP]
         L.orc_dot.argtypes = [C.c_int, _DP, _DP]
         L.orc_dot.restype = C.c_double
+        L.orc_dot_tree.argtypes = [C.c_int, _DP, _DP, C.c_int]
+        L.orc_dot_tree.restype = C.c_double
+        L.orc_set_dot_mode.argtypes = [C.c_int, C.c_int]
+        L.orc_set_cheb_variant.argtypes = [C.c_int, C.c_int]
         L.orc_axpy.argtypes = [C.c_int, C.c_double, _DP, _DP]
         L.orc_aypx.argtypes = [C.c_int, C.c_double, _DP, _DP]
         L.orc_cheb_bounds.argtypes = [C.c_int, _IP, _IP, _DP, C.c_double, C.c_int, _DP, _DP]
@@ -101,6 +111,7 @@ def ref() -> C.CDLL:
     global _ref
     if _ref is None:
         _ref = _load(REF_SO, "ref")
+        _ref.ref_set_cheb_saad.argtypes = [C.c_int]
     return _ref
 
 
@@ -135,12 +146,18 @@ class OracleSolve:
 
 
 def solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8, max_iter=1000, poly_factor=0.0,
-          poly_order=3, poly_factor_max_iter=10, which="oracle") -> OracleSolve:
-    """Runs the restatement (which='oracle') or the reference templates (which='ref')."""
+          poly_order=3, poly_factor_max_iter=10, which="oracle", dot_mode=DOT_SEQUENTIAL,
+          tree_blocks=1184, cheb_saad=False, cheb_lanczos=False) -> OracleSolve:
+    """Runs the restatement (which='oracle') or the reference templates (which='ref').
+    dot_mode=DOT_DEVICE_TREE makes the restatement sum every dot product in
+    libab2's reduction tree (tree_blocks = its block cap), for bit-exact checks.
+    cheb_saad selects ChebyshevPreconditioner<.., true>; cheb_lanczos (oracle
+    only: no reference counterpart) takes the bounds from Lanczos steps."""
     rp, ci, v, bb = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(b, np.float64)
     n = rp.size - 1
     x = np.zeros(n) if x0 is None else _c(x0, np.float64).copy()
-    o = Options(SOLVER[solver], PRECOND[precond], tol, max_iter, poly_factor, poly_order, poly_factor_max_iter)
+    o = Options(SOLVER[solver], PRECOND[precond], tol, max_iter, poly_factor, poly_order, poly_factor_max_iter,
+                dot_mode, tree_blocks, int(cheb_saad), int(cheb_lanczos))
     r = Result()
     cap = 2 * max_iter + 8
     hist = np.zeros(cap)
@@ -178,6 +195,17 @@ def dot(x, y) -> float:
     return orc().orc_dot(xx.size, _dp(xx), _dp(yy))
 
 
+def dot_tree(x, y, tree_blocks: int) -> float:
+    """x.y summed in libab2's device reduction tree."""
+    xx, yy = _c(x, np.float64), _c(y, np.float64)
+    return orc().orc_dot_tree(xx.size, _dp(xx), _dp(yy), tree_blocks)
+
+
+def set_dot_mode(mode: int, tree_blocks: int = 1184) -> None:
+    """Dot order for the Chebyshev helpers below (solve() takes it as options)."""
+    orc().orc_set_dot_mode(mode, tree_blocks)
+
+
 def axpy(a, x, y) -> np.ndarray:
     """y + a x with one fma per element (cblas_daxpy)."""
     xx, yy = _c(x, np.float64), _c(y, np.float64).copy()
@@ -209,9 +237,14 @@ def ilu0_apply(row_ptr, cols, vals, y, which="oracle") -> np.ndarray:
     return out
 
 
-def cheb_apply(row_ptr, cols, vals, x, factor=0.0, order=3, max_iter=10, which="oracle") -> np.ndarray:
+def cheb_apply(row_ptr, cols, vals, x, factor=0.0, order=3, max_iter=10, which="oracle", dot_mode=DOT_SEQUENTIAL,
+               tree_blocks=1184, saad=False, lanczos=False) -> np.ndarray:
     rp, ci, v, xx = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(x, np.float64)
     out = np.empty(rp.size - 1)
+    set_dot_mode(dot_mode, tree_blocks)
+    orc().orc_set_cheb_variant(int(saad), int(lanczos))
+    if which != "oracle":
+        ref().ref_set_cheb_saad(int(saad))
     L = orc() if which == "oracle" else ref()
     getattr(L, "orc_cheb_apply" if which == "oracle" else "ref_cheb_apply")(rp.size - 1, _ip(rp), _ip(ci), _dp(v),
                                                                               factor, order, max_iter, _dp(xx),
@@ -219,9 +252,12 @@ def cheb_apply(row_ptr, cols, vals, x, factor=0.0, order=3, max_iter=10, which="
     return out
 
 
-def cheb_bounds(row_ptr, cols, vals, factor=0.0, max_iter=10) -> tuple[float, float]:
+def cheb_bounds(row_ptr, cols, vals, factor=0.0, max_iter=10, dot_mode=DOT_SEQUENTIAL,
+                tree_blocks=1184, lanczos=False) -> tuple[float, float]:
     rp, ci, v = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64)
     a, b = C.c_double(), C.c_double()
+    set_dot_mode(dot_mode, tree_blocks)
+    orc().orc_set_cheb_variant(0, int(lanczos))
     orc().orc_cheb_bounds(rp.size - 1, _ip(rp), _ip(ci), _dp(v), factor, max_iter, C.byref(a), C.byref(b))
     return a.value, b.value
 

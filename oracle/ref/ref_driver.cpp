@@ -33,9 +33,14 @@
 
 namespace Alien {
 
+// Discards everything: ChebyshevPreconditioner's Saad branch (_algo1) writes
+// to the trace manager unconditionally.
 class ITraceMng {
  public:
-  std::ostream& info() { return std::cerr; }
+  std::ostream& info() {
+    static std::ostream sink(nullptr);
+    return sink;
+  }
 };
 
 struct MatrixDistribution {};
@@ -198,7 +203,9 @@ class ShimAlgebra {
 
 extern "C" {
 
-// Same layout as orc_options / orc_result in ab2_oracle.cpp.
+// Same layout as orc_options / orc_result in ab2_oracle.cpp (dot_mode,
+// tree_blocks and cheb_lanczos have no meaning here: the templates sum dots
+// sequentially and only know the power-method bounds).
 typedef struct {
   int solver;
   int precond;
@@ -207,6 +214,10 @@ typedef struct {
   double poly_factor;
   int poly_order;
   int poly_factor_max_iter;
+  int dot_mode;
+  int tree_blocks;
+  int cheb_saad;
+  int cheb_lanczos;
 } ref_options;
 
 typedef struct {
@@ -226,6 +237,9 @@ typedef struct {
 namespace {
 
 using Alien::ShimAlgebra;
+
+Alien::ITraceMng g_trace;
+thread_local bool g_saad = false;
 
 Alien::shim::Matrix make_matrix(int n, const int* rp, const int* ci, const double* v) {
   Alien::shim::Matrix A;
@@ -305,10 +319,17 @@ int ref_solve(int n, const int* rp, const int* ci, const double* v, const double
       break;
     }
     case 3: {
-      Alien::ChebyshevPreconditioner<ShimAlgebra> pc(alg, A, o->poly_factor, o->poly_order,
-                                                     o->poly_factor_max_iter, nullptr);
-      pc.init();
-      with_solver(pc);
+      if (o->cheb_saad) {
+        Alien::ChebyshevPreconditioner<ShimAlgebra, true> pc(alg, A, o->poly_factor, o->poly_order,
+                                                             o->poly_factor_max_iter, &g_trace);
+        pc.init();
+        with_solver(pc);
+      } else {
+        Alien::ChebyshevPreconditioner<ShimAlgebra> pc(alg, A, o->poly_factor, o->poly_order,
+                                                       o->poly_factor_max_iter, nullptr);
+        pc.init();
+        with_solver(pc);
+      }
       break;
     }
     default: return -6;
@@ -347,13 +368,25 @@ int ref_cheb_apply(int n, const int* rp, const int* ci, const double* v, double 
                    const double* xin, double* yout) {
   ShimAlgebra alg;
   Alien::shim::Matrix A = make_matrix(n, rp, ci, v);
-  Alien::ChebyshevPreconditioner<ShimAlgebra> pc(alg, A, factor, order, max_iter, nullptr);
-  pc.init();
   Alien::shim::Vector vx, vy;
   vx.v.assign(xin, xin + n);
   vy.v.assign((std::size_t)n, 0.0);
-  alg.exec(pc, vx, vy);
+  if (g_saad) {
+    Alien::ChebyshevPreconditioner<ShimAlgebra, true> pc(alg, A, factor, order, max_iter, &g_trace);
+    pc.init();
+    alg.exec(pc, vx, vy);
+  } else {
+    Alien::ChebyshevPreconditioner<ShimAlgebra> pc(alg, A, factor, order, max_iter, nullptr);
+    pc.init();
+    alg.exec(pc, vx, vy);
+  }
   std::memcpy(yout, vy.v.data(), sizeof(double) * (size_t)n);
+  return 0;
+}
+
+// Chebyshev template instance used by ref_cheb_apply (1: saad = true).
+int ref_set_cheb_saad(int saad) {
+  g_saad = saad != 0;
   return 0;
 }
 

@@ -40,7 +40,10 @@ for prob in PROBLEMS:
     for solver in ("cg", "bicgs"):
         for pc in ("diag", "ilu0", "cheb"):
             CASES.append(dict(problem=prob, solver=solver, precond=pc, tol=1e-8, max_iter=300, poly_factor=0.0,
-                              poly_order=3, poly_factor_max_iter=20))
+                              poly_order=3, poly_factor_max_iter=20, cheb_saad=False))
+        # ChebyshevPreconditioner<AlgebraT, true> (Saad's recurrence, _algo1)
+        CASES.append(dict(problem=prob, solver=solver, precond="cheb", tol=1e-8, max_iter=300, poly_factor=0.0,
+                          poly_order=3, poly_factor_max_iter=20, cheb_saad=True))
 # edge cases the reference's control flow has
 CASES += [
     dict(problem="poisson16", solver="cg", precond="diag", tol=1e-8, max_iter=1, poly_factor=0.0, poly_order=3,

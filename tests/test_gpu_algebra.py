@@ -94,6 +94,7 @@ def test_dot_norms(ctx, n):
     assert abs(d - exact) <= 1e-14 * scale
     assert abs(d - O.dot(x, y)) <= (1e-14 + n * 2.3e-16) * scale
     assert ctx.dot(vx, vy) == d  # deterministic tree
+    assert d == O.dot_tree(x, y, ctx.info.reduction_max_blocks)  # and exactly the documented one
     xx = math.fsum(x * x)
     assert abs(ctx.norm2(vx) - math.sqrt(xx)) <= 1e-14 * max(math.sqrt(xx), 1e-300)
     assert abs(ctx.norm1(vx) - math.fsum(np.abs(x))) <= 1e-14 * max(math.fsum(np.abs(x)), 1e-300)

@@ -60,6 +60,7 @@ def test_restatement_matches_reference_templates(case):
     assert hashlib.sha256(P.b.tobytes()).hexdigest() == meta["b_sha256"]
     kw = {k: case[k] for k in ("solver", "precond", "tol", "max_iter", "poly_factor", "poly_order",
                                "poly_factor_max_iter")}
+    kw["cheb_saad"] = case.get("cheb_saad", False)
     r = O.solve(P.row_ptr, P.cols, P.vals, P.b, which="oracle", **kw)
     assert r.iterations == case["iterations"]
     assert r.converged == case["converged"]
@@ -93,8 +94,24 @@ def test_ilu0_and_chebyshev_vs_reference(name):
                                   O.ilu0_factor(P.row_ptr, P.cols, P.vals, "ref"))
     np.testing.assert_array_equal(O.ilu0_apply(P.row_ptr, P.cols, P.vals, P.b, "oracle"),
                                   O.ilu0_apply(P.row_ptr, P.cols, P.vals, P.b, "ref"))
-    np.testing.assert_array_equal(O.cheb_apply(P.row_ptr, P.cols, P.vals, P.b, 0.0, 3, 12, "oracle"),
-                                  O.cheb_apply(P.row_ptr, P.cols, P.vals, P.b, 0.0, 3, 12, "ref"))
+    for saad in (False, True):
+        np.testing.assert_array_equal(O.cheb_apply(P.row_ptr, P.cols, P.vals, P.b, 0.0, 3, 12, "oracle", saad=saad),
+                                      O.cheb_apply(P.row_ptr, P.cols, P.vals, P.b, 0.0, 3, 12, "ref", saad=saad))
+
+
+def test_lanczos_bounds_bracket_the_spectrum():
+    """Lanczos bounds (no reference counterpart): the Ritz interval lies inside
+    the spectrum of D^-1 A, the upper bound is widened by 10%."""
+    P = problems.get("diffusion12")
+    A = np.zeros((P.n, P.n))
+    for r in range(P.n):
+        A[r, P.cols[P.row_ptr[r]:P.row_ptr[r + 1]]] = P.vals[P.row_ptr[r]:P.row_ptr[r + 1]]
+    s = 1.0 / np.sqrt(np.diag(A))
+    ev = np.linalg.eigvalsh(s[:, None] * A * s[None, :])
+    a, b = O.cheb_bounds(P.row_ptr, P.cols, P.vals, 0.0, 20, lanczos=True)
+    assert ev[0] <= a <= ev[-1]
+    assert ev[-1] <= b <= 1.1 * ev[-1] * (1 + 1e-12)
+    assert abs(b / 1.1 - ev[-1]) < 1e-3 * ev[-1]
 
 
 def test_krylov_config1_iteration_count():
