@@ -111,17 +111,24 @@ inline void require(bool cond, const char* msg) {
   if (!cond) throw Error{AB2_ERR_BAD_ARG, msg};
 }
 
+// Device memory comes from the device's stream-ordered pool (cudaMallocAsync
+// on the context's stream; the context raises the pool's release threshold so
+// freed blocks stay cached for the next solver instead of going back to the
+// driver).  dev_alloc waits for the stream, so the block is valid for any use
+// -- including synchronous copies on other streams -- when it returns;
+// dev_free is ordered after all work already queued on the stream.
 template <class T>
-T* dev_alloc(size_t count, long long* accounted = nullptr) {
+T* dev_alloc(ab2_context* ctx, size_t count, long long* accounted = nullptr) {
   T* p = nullptr;
   if (count == 0) count = 1;
-  check_cuda(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+  check_cuda(cudaMallocAsync((void**)&p, count * sizeof(T), ctx->stream), "cudaMallocAsync");
+  check_cuda(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
   if (accounted) *accounted += (long long)(count * sizeof(T));
   return p;
 }
 
-inline void dev_free(void* p) {
-  if (p) cudaFree(p);
+inline void dev_free(ab2_context* ctx, void* p) {
+  if (p) cudaFreeAsync(p, ctx->stream);
 }
 
 // Context references (see ab2_context::refs).

@@ -70,9 +70,9 @@ int red_grid(const ab2_context* ctx, int n) {
 void ctx_release(ab2_context* ctx) {
   if (ctx->refs.fetch_sub(1) != 1) return;
   ctx_quiesce(ctx);
-  dev_free(ctx->d_partials);
-  dev_free(ctx->d_counters);
-  dev_free(ctx->d_results);
+  dev_free(ctx, ctx->d_partials);
+  dev_free(ctx, ctx->d_counters);
+  dev_free(ctx, ctx->d_results);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -161,9 +161,16 @@ int ab2_context_create(int device, ab2_context** out) {
     AB2_CUDA(cudaSetDevice(device));
     AB2_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
     AB2_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    ctx->d_partials = dev_alloc<double>((size_t)kRedSlots * kMaxRedComps * kMaxRedBlocks);
-    ctx->d_counters = dev_alloc<unsigned int>(kRedSlots);
-    ctx->d_results = dev_alloc<double>((size_t)kRedSlots * kMaxRedComps);
+    // Keep freed blocks in the device's default pool (dev_alloc draws from
+    // it): solvers and preconditioners created per solve then reuse memory
+    // instead of mapping and unmapping hundreds of MB each time.
+    cudaMemPool_t pool;
+    AB2_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    AB2_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    ctx->d_partials = dev_alloc<double>(ctx, (size_t)kRedSlots * kMaxRedComps * kMaxRedBlocks);
+    ctx->d_counters = dev_alloc<unsigned int>(ctx, kRedSlots);
+    ctx->d_results = dev_alloc<double>(ctx, (size_t)kRedSlots * kMaxRedComps);
     AB2_CUDA(cudaMemset(ctx->d_counters, 0, sizeof(unsigned int) * kRedSlots));
     AB2_CUDA(cudaMallocHost((void**)&ctx->h_pinned, 64 * sizeof(double)));
   });
@@ -219,7 +226,7 @@ int ab2_vector_create(ab2_context* ctx, int n, ab2_vector** out) {
   v->ctx = ctx_retain(ctx);
   int rc = guard(ctx, [&] {
     v->n = n;
-    v->d = dev_alloc<double>((size_t)n);
+    v->d = dev_alloc<double>(v->ctx, (size_t)n);
     AB2_CUDA(cudaMemsetAsync(v->d, 0, sizeof(double) * (size_t)std::max(n, 1), ctx->stream));
   });
   if (rc != AB2_OK) {
@@ -233,7 +240,7 @@ int ab2_vector_create(ab2_context* ctx, int n, ab2_vector** out) {
 int ab2_vector_destroy(ab2_vector* v) {
   if (!v) return AB2_ERR_BAD_ARG;
   ctx_quiesce(v->ctx);
-  dev_free(v->d);
+  dev_free(v->ctx, v->d);
   ctx_release(v->ctx);
   delete v;
   return AB2_OK;
@@ -336,7 +343,7 @@ int ab2_scalar_create(ab2_context* ctx, ab2_scalar** out) {
   if (!s) return AB2_ERR_OOM;
   s->ctx = ctx_retain(ctx);
   int rc = guard(ctx, [&] {
-    s->d = dev_alloc<double>(1);
+    s->d = dev_alloc<double>(s->ctx, 1);
     AB2_CUDA(cudaMemsetAsync(s->d, 0, sizeof(double), ctx->stream));
   });
   if (rc != AB2_OK) {
@@ -349,7 +356,7 @@ int ab2_scalar_create(ab2_context* ctx, ab2_scalar** out) {
 int ab2_scalar_destroy(ab2_scalar* s) {
   if (!s) return AB2_ERR_BAD_ARG;
   ctx_quiesce(s->ctx);
-  dev_free(s->d);
+  dev_free(s->ctx, s->d);
   ctx_release(s->ctx);
   delete s;
   return AB2_OK;

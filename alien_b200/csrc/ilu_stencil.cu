@@ -7,31 +7,47 @@
 // for bit those of the wavefront kernels in precond.cu and of the sequential
 // reference.  Only the schedule differs.
 //
-// In a 3-D 7-point matrix numbered i + nx (j + ny k), row (i,j,k) of the
-// forward sweep depends on (i,j,k-1), (i,j-1,k) and (i-1,j,k).  A CTA of
-// 16 x 16 threads owns a 16 x 16 tile of z-lines, one thread per line, and
-// walks the tile's diagonals i+j+k = s: at step s thread (i,j) computes cell
-// k = s - i - j.  Its k-1 input is its own previous value (a register), the
+// Schedule.  In a 3-D 7-point matrix numbered i + nx (j + ny k), row (i,j,k)
+// of the forward sweep depends on (i,j,k-1), (i,j-1,k) and (i-1,j,k).  A CTA
+// of 16 x 16 threads owns a 16 x 16 tile of z-lines, one thread per line, and
+// walks the tile's diagonals: at step s thread (li,lj) computes cell
+// k = s - li - lj.  Its k-1 input is its own previous value (a register), the
 // i-1 and j-1 inputs were computed by neighbouring threads at step s-1 (shared
 // memory, one __syncthreads per step).  Only the first line of a tile reads a
-// value owned by another tile; those come through global memory with the
-// sentinel-value wait of sentinel.cuh, loaded ahead with the band values.
-// Tiles are claimed from an atomic ticket in the order the dependencies run (a
-// tile waits only on tiles with a smaller ticket), so no co-residency is
-// needed.  The backward sweep runs the same walk on the mirrored grid; the
-// factorisation runs it too: in a 7-point matrix ILU(0) changes only the
-// diagonal, and row (i,j,k) needs the final pivots of the same three
-// neighbours (value propagated: the pivot).
+// value owned by another tile, 15 steps ahead in that tile's walk; those come
+// through global memory with the sentinel-value wait of sentinel.cuh.  Tiles
+// are claimed from an atomic ticket in dependency order (a tile waits only on
+// tiles with a smaller ticket), so no co-residency is needed.
 //
-// Measured on B200 at 192^3 this schedule applies the factor in 1.7 ms
-// against 3.45 ms for the wavefront schedule and sets up in ~6 ms instead of
-// ~220 ms; a warp-per-8x4-tile variant (shuffles instead of shared memory)
-// measured 2.9 ms.  Each step of a walk costs about one L2 round trip, so the
-// ~574 dependent steps of a sweep, not bandwidth, bound it.
+// Walk layout.  At one step the 256 threads of a tile touch 31 different
+// z-planes, so in natural order every warp access would be 32 separate cache
+// lines, and a step would cost the LSU ~1.2 us instead of ~0.16 us (measured on
+// B200 for this access pattern against the same walk on contiguous data).  The
+// sweeps therefore read and write arrays stored in WALK order: index
+// ((tile * nsteps + s) * 256 + thread), nsteps = nz + 30 rounded up to the
+// prefetch depth, so one warp access is 32 consecutive doubles.  The factor
+// bands are gathered into that order once at set-up; each application gathers
+// y in (one bulk kernel), runs the two walks, and scatters z out (one bulk
+// kernel) -- bulk kernels have the whole GPU to hide scattered addresses, a
+// wavefront step does not.
 //
-// The factor is kept in eight structure-of-arrays bands (L to -k/-j/-i, U to
-// +i/+j/+k, pivot, original diagonal) so each thread's loads are plain
-// indexed reads, and a copy in CSR order for ab2_precond_ilu0_values.
+// The backward sweep is the forward walk run backwards: the U walk's thread
+// (li,lj) of tile T at step s handles the cell the L walk handles at the
+// mirrored position (15-li, 15-lj, ntiles-1-T, nsteps-1-s), whose walk index is
+// walk_n - 1 - w (the U walk's cells then start nsteps - nz - 30 steps
+// late).  So both walks use the same arrays, the U walk through the reversed
+// index, and both are coalesced.  Its dependencies (+i, +j, +k) are
+// then again "previous thread / previous tile / own previous step".
+//
+// The factorisation runs once per set-up on the natural-order bands with the
+// same walk (pivots propagate; in a 7-point matrix ILU(0) changes only the
+// diagonal and the L values).
+//
+// Measured on B200, one application at 192^3: 1.02 ms (gather + two walks +
+// scatter), against 1.69 ms for the same walk on natural-order arrays and
+// 3.45 ms for the wavefront schedule of precond.cu.  A lone tile steps in
+// ~0.24 us; the rest is the trail each of the 22 tile boundaries on the
+// critical path adds.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,8 +61,13 @@ namespace ab2 {
 namespace {
 
 constexpr int kTile = 16;
-
-enum { kFactor = 0, kLower = 1, kUpper = 2 };
+constexpr int kTileThreads = kTile * kTile;
+constexpr int kWalkPrefetch = 8;  // steps a walk loads ahead; the walk length is padded to a multiple
+// Steps ahead a walk loads its neighbouring tiles' values.  A consumer tile
+// trails its producer by this distance plus the 15-step skew and the
+// store-to-load latency; 2..7 measured within 3% of each other at 64^3-192^3
+// on B200, 4 the best.
+constexpr int kWalkPrefetchB = 4;
 
 struct Geom {
   int nx, ny, nz, ntx, nty;
@@ -107,81 +128,55 @@ __global__ void k_stencil_pack(int n, Geom g, const int* __restrict__ rp, Bands 
   }
 }
 
-// Per-step inputs loaded prefetch_depth<MODE>() steps ahead: band values of
-// the step's cell, and the value owned by the neighbouring tile (bi / bj,
-// first line of the tile only), possibly still the sentinel when loaded.
-struct Pre {
-  double a0, a1, a2, a3, u0, u1, u2, bi, bj;
+// The factorisation walk (set-up only, natural-order bands): row (i,j,k)
+// divides its L entries by the pivots of its -k, -j, -i neighbours and
+// subtracts l * u (the neighbour's U entry towards this row) from its diagonal,
+// columns ascending; the resulting pivot propagates.
+struct PreF {
+  double d, lk, lj, li, uk, uj, ui, bi, bj;
 };
 
-template <int MODE>
-__host__ __device__ constexpr int prefetch_depth() {
-  return MODE == kFactor ? 4 : 8;
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(kTile* kTile) k_stencil_wave(Geom g, Bands b, const double* in, double* out,
-                                                                double* reset, unsigned int* tickets, int* err) {
-  constexpr int kPrefetch = prefetch_depth<MODE>();
+__global__ void __launch_bounds__(kTileThreads) k_stencil_factor(Geom g, Bands b, unsigned int* tickets, int* err) {
+  constexpr int kPrefetch = 4;
   __shared__ double s_val[2][kTile][kTile + 1];
   __shared__ int s_tile;
   const int li = threadIdx.x % kTile, lj = threadIdx.x / kTile;
   const int ntiles = g.ntx * g.nty;
   const int nsteps = g.nz + 2 * (kTile - 1);
-  constexpr bool up = MODE == kUpper;
-  const int di = up ? 1 : -1;  // global offset of the i-neighbour read (j: di*nx)
-  double* wave = MODE == kFactor ? b.P : out;  // the array whose values propagate
-
+  double* wave = b.P;
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) s_tile = (int)atomicAdd(tickets + MODE, 1u);
+    if (threadIdx.x == 0) s_tile = (int)atomicAdd(tickets, 1u);
     __syncthreads();
     const int tile = s_tile;
     if (tile >= ntiles) break;
-    const int ai = (tile % g.ntx) * kTile + li;  // walk coordinates (mirrored for the U sweep)
+    const int ai = (tile % g.ntx) * kTile + li;
     const int aj = (tile / g.ntx) * kTile + lj;
     const bool active = ai < g.nx && aj < g.ny;
-    const int gi = up ? g.nx - 1 - ai : ai;
-    const int gj = up ? g.ny - 1 - aj : aj;
-    const long long line = active ? gi + (long long)g.nx * gj : 0;
-
+    const long long line = active ? ai + (long long)g.nx * aj : 0;
     auto cell = [&](int s, long long& r) {
       const int ak = s - li - lj;
       if (!active || ak < 0 || ak >= g.nz) return -1;
-      r = line + g.nxny * (up ? g.nz - 1 - ak : ak);
+      r = line + g.nxny * ak;
       return ak;
     };
-    auto load = [&](int s, Pre& p) {
+    auto load = [&](int s, PreF& p) {
       long long r = 0;
       if (cell(s, r) < 0) return;
-      if (lj == 0 && aj > 0) p.bj = ld_relaxed(wave + r + di * (long long)g.nx);
-      if (li == 0 && ai > 0) p.bi = ld_relaxed(wave + r + di);
-      if (MODE == kFactor) {
-        p.a0 = b.D[r];
-        p.a1 = b.Lk[r];
-        p.a2 = b.Lj[r];
-        p.a3 = b.Li[r];
-        p.u0 = r >= g.nxny ? b.Uk[r - g.nxny] : 0.0;
-        p.u1 = r >= g.nx ? b.Uj[r - g.nx] : 0.0;
-        p.u2 = r >= 1 ? b.Ui[r - 1] : 0.0;
-      } else if (MODE == kLower) {
-        p.a0 = in[r];
-        p.a1 = b.Lk[r];
-        p.a2 = b.Lj[r];
-        p.a3 = b.Li[r];
-      } else {
-        p.a0 = in[r];
-        p.a1 = b.Ui[r];
-        p.a2 = b.Uj[r];
-        p.a3 = b.Uk[r];
-        p.u0 = b.P[r];
-      }
+      if (lj == 0 && aj > 0) p.bj = ld_relaxed(wave + r - g.nx);
+      if (li == 0 && ai > 0) p.bi = ld_relaxed(wave + r - 1);
+      p.d = b.D[r];
+      p.lk = b.Lk[r];
+      p.lj = b.Lj[r];
+      p.li = b.Li[r];
+      p.uk = r >= g.nxny ? b.Uk[r - g.nxny] : 0.0;
+      p.uj = r >= g.nx ? b.Uj[r - g.nx] : 0.0;
+      p.ui = r >= 1 ? b.Ui[r - 1] : 0.0;
     };
-
-    Pre pre[kPrefetch];
+    PreF pre[kPrefetch];
 #pragma unroll
     for (int u = 0; u < kPrefetch; ++u) {
-      pre[u] = Pre{0, 0, 0, 0, 0, 0, 0, 0, 0};
+      pre[u] = PreF{0, 0, 0, 0, 0, 0, 0, 0, 0};
       load(u, pre[u]);
     }
     double own = 0.0;
@@ -190,7 +185,7 @@ __global__ void __launch_bounds__(kTile* kTile) k_stencil_wave(Geom g, Bands b, 
       for (int u = 0; u < kPrefetch; ++u) {
         const int s = s0 + u;
         if (s < nsteps) {
-          const Pre c = pre[u];
+          const PreF c = pre[u];
           load(s + kPrefetch, pre[u]);
           long long r = 0;
           const int ak = cell(s, r);
@@ -198,47 +193,28 @@ __global__ void __launch_bounds__(kTile* kTile) k_stencil_wave(Geom g, Bands b, 
           if (ak >= 0) {
             const double* prev = &s_val[(s + 1) & 1][0][0];
             double vi = 0.0, vj = 0.0;
-            if (aj > 0) {
+            if (aj > 0)
               vj = lj > 0 ? prev[(lj - 1) * (kTile + 1) + li]
-                          : (is_sentinel(c.bj) ? wait_value(wave + r + di * (long long)g.nx, err) : c.bj);
+                          : (is_sentinel(c.bj) ? wait_value(wave + r - g.nx, err) : c.bj);
+            if (ai > 0)
+              vi = li > 0 ? prev[lj * (kTile + 1) + li - 1] : (is_sentinel(c.bi) ? wait_value(wave + r - 1, err) : c.bi);
+            double d = c.d;  // a_ik /= pivot_k, then a_ii -= a_ik a_ki, columns ascending (-k, -j, -i)
+            if (ak > 0) {
+              const double l = c.lk / own;
+              d = mul_sub_rn(l, c.uk, d);
+              b.Lk[r] = l;
+            }
+            if (aj > 0) {
+              const double l = c.lj / vj;
+              d = mul_sub_rn(l, c.uj, d);
+              b.Lj[r] = l;
             }
             if (ai > 0) {
-              vi = li > 0 ? prev[lj * (kTile + 1) + li - 1] : (is_sentinel(c.bi) ? wait_value(wave + r + di, err) : c.bi);
+              const double l = c.li / vi;
+              d = mul_sub_rn(l, c.ui, d);
+              b.Li[r] = l;
             }
-            if (MODE == kFactor) {
-              // a_ik /= pivot_k, then a_ii -= a_ik a_ki, columns ascending (-k, -j, -i)
-              double d = c.a0;
-              if (ak > 0) {
-                const double l = c.a1 / own;
-                d = mul_sub_rn(l, c.u0, d);
-                b.Lk[r] = l;
-              }
-              if (aj > 0) {
-                const double l = c.a2 / vj;
-                d = mul_sub_rn(l, c.u1, d);
-                b.Lj[r] = l;
-              }
-              if (ai > 0) {
-                const double l = c.a3 / vi;
-                d = mul_sub_rn(l, c.u2, d);
-                b.Li[r] = l;
-              }
-              val = d;
-            } else if (MODE == kLower) {
-              double acc = c.a0;  // columns ascending: -k, -j, -i
-              if (ak > 0) acc = mul_sub_rn(c.a1, own, acc);
-              if (aj > 0) acc = mul_sub_rn(c.a2, vj, acc);
-              if (ai > 0) acc = mul_sub_rn(c.a3, vi, acc);
-              reset[r] = sentinel_value();  // after in[r] was read: in and reset may alias
-              val = acc;
-            } else {
-              double acc = c.a0;  // columns ascending: +i, +j, +k
-              if (ai > 0) acc = mul_sub_rn(c.a1, vi, acc);
-              if (aj > 0) acc = mul_sub_rn(c.a2, vj, acc);
-              if (ak > 0) acc = mul_sub_rn(c.a3, own, acc);
-              reset[r] = sentinel_value();
-              val = acc / c.u0;
-            }
+            val = d;
             st_relaxed(wave + r, not_sentinel(val));
             own = val;
           }
@@ -248,11 +224,181 @@ __global__ void __launch_bounds__(kTile* kTile) k_stencil_wave(Geom g, Bands b, 
       }
     }
   }
-  // Hand the other sweep its ticket back (it does not run concurrently).
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (MODE == kLower) tickets[kUpper] = 0u;
-    if (MODE == kUpper) tickets[kLower] = 0u;
+}
+
+// ------------------------------------------------------------------ walk layout
+struct Walk {
+  int nx, ny, nz, ntx, nty, nsteps;
+  long long nxny, nw;  // nw = ntx nty nsteps 256
+};
+
+// The natural row handled at walk index w of the L walk, or -1 (padding).
+__device__ __forceinline__ long long walk_row(const Walk& g, long long w) {
+  const int t = (int)(w & (kTileThreads - 1));
+  const long long q = w >> 8;
+  const int s = (int)(q % g.nsteps);
+  const int tile = (int)(q / g.nsteps);
+  const int li = t & (kTile - 1), lj = t >> 4;
+  const int i = (tile % g.ntx) * kTile + li, j = (tile / g.ntx) * kTile + lj, k = s - li - lj;
+  if (i >= g.nx || j >= g.ny || k < 0 || k >= g.nz) return -1;
+  return i + (long long)g.nx * j + g.nxny * k;
+}
+
+// dst[w] = src[row(w)] (0 on padding).
+__global__ void k_walk_gather(Walk g, const double* __restrict__ src, double* __restrict__ dst) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < g.nw; w += (long long)gridDim.x * blockDim.x) {
+    const long long r = walk_row(g, w);
+    dst[w] = r >= 0 ? __ldg(src + r) : 0.0;
   }
+}
+
+// dst[row(w)] = src[w], and src[w] back to the sentinel for the next walk.
+__global__ void k_walk_scatter(Walk g, double* __restrict__ src, double* __restrict__ dst) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < g.nw; w += (long long)gridDim.x * blockDim.x) {
+    const long long r = walk_row(g, w);
+    if (r >= 0) {
+      dst[r] = src[w];
+      src[w] = sentinel_value();
+    }
+  }
+}
+
+struct WalkArrays {
+  const double *Lk, *Lj, *Li, *Ui, *Uj, *Uk, *P;
+};
+
+// Per-step inputs, loaded kWalkPrefetch steps ahead: the right-hand side,
+// three band values (L: -k,-j,-i ; U: +i,+j,+k), the pivot (U walk), and the
+// value owned by the neighbouring tile (bi / bj, first line of the tile only),
+// possibly still the sentinel when loaded.
+struct PreW {
+  double y, a1, a2, a3, piv, bi, bj;
+};
+
+// One triangular sweep in walk layout.  UP = false: forward sweep
+// x_i = y_i - sum_{k<dcol} l_ik x_k (solveL, ILU0Preconditioner.h:181-198) from
+// `in` into `wave`.  UP = true: backward sweep x_i = (y_i - sum_{k>dcol} u_ik x_k)
+// / u_ii (solveU, :200-231), reading `in` through the reversed index and
+// putting it back to the sentinel.  `wave` must hold the sentinel on entry.
+//
+// A step is a handful of instructions per thread, and with one 256-thread CTA
+// per SM the schedulers have two warps each, so the step time is close to
+// the instruction count: every array is reached through a per-thread pointer
+// that moves once per group of kWalkPrefetch steps, with constant offsets
+// inside the unrolled group.
+template <bool UP, int kPreB = kWalkPrefetchB>
+__global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArrays b, double* in, double* wave,
+                                                              unsigned int* tickets, int* err) {
+  constexpr int kPre = kWalkPrefetch;
+  static_assert(kPreB >= 1 && kPreB < kPre, "boundary values are loaded inside the band prefetch window");
+  constexpr long long kStep = UP ? -kTileThreads : kTileThreads;  // element stride of one step
+  __shared__ double s_val[2][kTile][kTile + 1];
+  __shared__ int s_tile;
+  const int li = threadIdx.x % kTile, lj = threadIdx.x / kTile;
+  const int ntiles = g.ntx * g.nty;
+  const int nsteps = g.nsteps;
+  // Walk coordinates of the grid's first cell (the U walk's tiles are the
+  // mirror images of the L walk's, so a partial tile comes first, and its
+  // cells start nsteps - nz - 30 steps into the walk).
+  const int ox = UP ? g.ntx * kTile - g.nx : 0;
+  const int oy = UP ? g.nty * kTile - g.ny : 0;
+  const int oz = UP ? nsteps - g.nz - 2 * (kTile - 1) : 0;
+  auto phys = [&](long long w) { return UP ? g.nw - 1 - w : w; };
+
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_tile = (int)atomicAdd(tickets + (UP ? 2 : 1), 1u);
+    __syncthreads();
+    const int tile = s_tile;
+    if (tile >= ntiles) break;
+    const int ai = (tile % g.ntx) * kTile + li;
+    const int aj = (tile / g.ntx) * kTile + lj;
+    const bool active = ai >= ox && ai < ox + g.nx && aj >= oy && aj < oy + g.ny;
+    const bool has_i = ai > ox, has_j = aj > oy;  // walk predecessor along i / j
+    const bool bnd_i = li == 0 && has_i, bnd_j = lj == 0 && has_j;  // that predecessor is in another tile
+    // valid steps: s_lo <= s < s_hi (cell k = s - li - lj - oz in [0, nz))
+    const int s_lo = active ? li + lj + oz : nsteps;
+    const int s_hi = active ? s_lo + g.nz : nsteps;
+    const long long tbase = (long long)tile * nsteps * kTileThreads;
+    // Step-0 pointers.  Own cell: walk index tbase + thread.  Neighbouring
+    // tile's cell at the same k: 15 steps further in that tile's walk.
+    const long long w_own = phys(tbase + threadIdx.x);
+    const long long w_bi = phys(tbase - (long long)nsteps * kTileThreads + 15 * kTileThreads + lj * kTile + 15);
+    const long long w_bj = phys(tbase - (long long)g.ntx * nsteps * kTileThreads + 15 * kTileThreads + 15 * kTile + li);
+    const double* p_y = in + w_own;
+    const double* p_a1 = (UP ? b.Ui : b.Lk) + w_own;
+    const double* p_a2 = (UP ? b.Uj : b.Lj) + w_own;
+    const double* p_a3 = (UP ? b.Uk : b.Li) + w_own;
+    const double* p_piv = b.P + w_own;
+    double* p_in = in + w_own;
+    double* p_out = wave + w_own;
+    const double* p_bi = wave + (bnd_i ? w_bi : w_own);
+    const double* p_bj = wave + (bnd_j ? w_bj : w_own);
+
+    // Loads of step s (offset o = s * kStep from the step-0 pointers).
+    auto load_b = [&](int s, long long o, PreW& p) {
+      if (s < s_lo || s >= s_hi) return;
+      if (bnd_j) p.bj = ld_relaxed(p_bj + o);
+      if (bnd_i) p.bi = ld_relaxed(p_bi + o);
+    };
+    auto load = [&](int s, long long o, PreW& p) {
+      if (s < s_lo || s >= s_hi) return;
+      // Read-only path: none of these is written during the walk except
+      // in[] by the U walk, after its one read here.
+      p.y = __ldg(p_y + o);
+      p.a1 = __ldg(p_a1 + o);
+      p.a2 = __ldg(p_a2 + o);
+      p.a3 = __ldg(p_a3 + o);
+      if (UP) p.piv = __ldg(p_piv + o);
+    };
+
+    PreW pre[kPre];
+#pragma unroll
+    for (int u = 0; u < kPre; ++u) {
+      pre[u] = PreW{0, 0, 0, 0, 0, 0, 0};
+      load(u, u * kStep, pre[u]);
+      if (u < kPreB) load_b(u, u * kStep, pre[u]);
+    }
+    double own = 0.0;
+    for (int s0 = 0; s0 < nsteps; s0 += kPre) {  // nsteps is a multiple of kPre
+      const long long o0 = (long long)s0 * kStep;
+#pragma unroll
+      for (int u = 0; u < kPre; ++u) {
+        const int s = s0 + u;
+        const long long o = o0 + u * kStep;
+        const PreW c = pre[u];
+        load(s + kPre, o + kPre * kStep, pre[u]);
+        load_b(s + kPreB, o + kPreB * kStep, pre[(u + kPreB) % kPre]);
+        double val = 0.0;
+        if (s >= s_lo && s < s_hi) {
+          const double* prev = &s_val[(s + 1) & 1][0][0];
+          double vi = 0.0, vj = 0.0;
+          if (has_j) vj = lj > 0 ? prev[(lj - 1) * (kTile + 1) + li] : is_sentinel(c.bj) ? wait_value(p_bj + o, err) : c.bj;
+          if (has_i) vi = li > 0 ? prev[lj * (kTile + 1) + li - 1] : is_sentinel(c.bi) ? wait_value(p_bi + o, err) : c.bi;
+          const bool has_k = s > s_lo;
+          double acc = c.y;
+          if (!UP) {  // columns ascending: -k, -j, -i
+            if (has_k) acc = mul_sub_rn(c.a1, own, acc);
+            if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
+            if (has_i) acc = mul_sub_rn(c.a3, vi, acc);
+            val = acc;
+          } else {  // columns ascending: +i, +j, +k
+            if (has_i) acc = mul_sub_rn(c.a1, vi, acc);
+            if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
+            if (has_k) acc = mul_sub_rn(c.a3, own, acc);
+            p_in[o] = sentinel_value();  // the L walk's output, ready for the next application
+            val = acc / c.piv;
+          }
+          st_relaxed(p_out + o, not_sentinel(val));
+          own = val;
+        }
+        s_val[s & 1][lj][li] = val;
+        __syncthreads();
+      }
+    }
+  }
+  // Hand the other sweep its ticket back (it does not run concurrently).
+  if (blockIdx.x == 0 && threadIdx.x == 0) tickets[UP ? 1 : 2] = 0u;
 }
 
 Geom geom_of(const Ilu0Data& d) {
@@ -266,13 +412,40 @@ Geom geom_of(const Ilu0Data& d) {
   return g;
 }
 
-Bands bands_of(const Ilu0Data& d, int n) {
-  double* p = d.d_bands;
+Walk walk_of(const Ilu0Data& d) {
+  const Geom g = geom_of(d);
+  Walk w;
+  w.nx = g.nx;
+  w.ny = g.ny;
+  w.nz = g.nz;
+  w.ntx = g.ntx;
+  w.nty = g.nty;
+  w.nsteps = (g.nz + 2 * (kTile - 1) + kWalkPrefetch - 1) / kWalkPrefetch * kWalkPrefetch;
+  w.nxny = g.nxny;
+  w.nw = (long long)g.ntx * g.nty * w.nsteps * kTileThreads;
+  return w;
+}
+
+Bands bands_of(double* p, int n) {
   const size_t m = (size_t)n;
   return Bands{p, p + m, p + 2 * m, p + 3 * m, p + 4 * m, p + 5 * m, p + 6 * m, p + 7 * m};
 }
 
-int wave_grid(ab2_context* ctx, const Geom& g) { return std::max(1, std::min(g.ntx * g.nty, ctx->num_sms * 2)); }
+// d_walk: Lk Lj Li Ui Uj Uk P | y | L-walk output | U-walk output
+enum { kWalkBands = 7, kWalkY = 7, kWalkL = 8, kWalkU = 9, kWalkArrays = 10 };
+
+double* walk_array(const Ilu0Data& d, int a) { return d.d_walk + (size_t)a * (size_t)d.walk_n; }
+
+WalkArrays walk_bands(const Ilu0Data& d) {
+  return WalkArrays{walk_array(d, 0), walk_array(d, 1), walk_array(d, 2), walk_array(d, 3),
+                    walk_array(d, 4), walk_array(d, 5), walk_array(d, 6)};
+}
+
+int wave_grid(ab2_context* ctx, int ntiles) { return std::max(1, std::min(ntiles, ctx->num_sms * 2)); }
+
+int bulk_grid(ab2_context* ctx, long long n) {
+  return (int)std::max(1LL, std::min((n + kThreads - 1) / kThreads, (long long)ctx->num_sms * 16));
+}
 
 }  // namespace
 
@@ -297,52 +470,76 @@ bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d) {
   d.st_ny = (int)ny;
   d.st_nz = (int)nz;
   const Geom g = geom_of(d);
-  int* d_bad = dev_alloc<int>(1);
+  int* d_bad = dev_alloc<int>(ctx, 1);
   AB2_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), ctx->stream));
   k_stencil_check<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, g, A->d_rp, A->d_ci, d_bad);
   check_launch(ctx, "stencil_check");
   int bad = 0;
   AB2_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   AB2_CUDA(cudaStreamSynchronize(ctx->stream));
-  dev_free(d_bad);
+  dev_free(ctx, d_bad);
   if (bad) return false;
 
-  d.d_bands = dev_alloc<double>((size_t)n * 8);
-  d.d_tile_tickets = dev_alloc<unsigned int>(3);
+  // Factorisation on natural-order bands.
+  d.d_bands = dev_alloc<double>(ctx, (size_t)n * 8);
+  d.d_tile_tickets = dev_alloc<unsigned int>(ctx, 3);
   AB2_CUDA(cudaMemsetAsync(d.d_tile_tickets, 0, 3 * sizeof(unsigned int), ctx->stream));
-  const Bands b = bands_of(d, n);
+  const Bands b = bands_of(d.d_bands, n);
   k_stencil_extract<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, g, A->d_rp, A->d_v, b);
   check_launch(ctx, "stencil_extract");
   k_fill_bits<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, kSentinel, b.P);
   check_launch(ctx, "stencil_fill");
-  k_stencil_wave<kFactor><<<wave_grid(ctx, g), kTile * kTile, 0, ctx->stream>>>(g, b, nullptr, nullptr, nullptr,
-                                                                                d.d_tile_tickets, d.d_err);
+  k_stencil_factor<<<wave_grid(ctx, g.ntx * g.nty), kTileThreads, 0, ctx->stream>>>(g, b, d.d_tile_tickets, d.d_err);
   check_launch(ctx, "stencil_factor");
   k_stencil_pack<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, g, A->d_rp, b, d.d_lu);
   check_launch(ctx, "stencil_pack");
+
+  // The sweeps' arrays in walk order.
+  const Walk w = walk_of(d);
+  d.walk_n = w.nw;
+  d.d_walk = dev_alloc<double>(ctx, (size_t)kWalkArrays * (size_t)w.nw);
+  const double* nat[kWalkBands] = {b.Lk, b.Lj, b.Li, b.Ui, b.Uj, b.Uk, b.P};
+  for (int a = 0; a < kWalkBands; ++a) {
+    k_walk_gather<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, nat[a], walk_array(d, a));
+    check_launch(ctx, "walk_gather");
+  }
+  AB2_CUDA(cudaMemsetAsync(walk_array(d, kWalkY), 0, sizeof(double) * (size_t)w.nw, ctx->stream));
+  k_fill_bits<<<bulk_grid(ctx, 2 * w.nw), kThreads, 0, ctx->stream>>>(2 * w.nw, kSentinel, walk_array(d, kWalkL));
+  check_launch(ctx, "walk_fill");
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  dev_free(ctx, d.d_bands);
+  d.d_bands = nullptr;
   d.stencil = true;
   d.levels_l = d.levels_u = (int)(nx + ny + nz - 2);
   return true;
 }
 
-// y -> d_tmp (forward walk; leaves z at the sentinel) -> z (backward walk;
-// puts d_tmp back to the sentinel).
+// y -> walk order -> L walk -> U walk (reversed index) -> z.
 void ilu_stencil_apply(ab2_context* ctx, const ab2_matrix* A, const Ilu0Data& d, const double* y, double* z) {
-  const Geom g = geom_of(d);
-  const Bands b = bands_of(d, A->n);
-  k_stencil_wave<kLower><<<wave_grid(ctx, g), kTile * kTile, 0, ctx->stream>>>(g, b, y, d.d_tmp, z, d.d_tile_tickets,
-                                                                               d.d_err);
-  check_launch(ctx, "stencil_lsweep");
-  k_stencil_wave<kUpper><<<wave_grid(ctx, g), kTile * kTile, 0, ctx->stream>>>(g, b, d.d_tmp, z, d.d_tmp,
-                                                                               d.d_tile_tickets, d.d_err);
-  check_launch(ctx, "stencil_usweep");
+  (void)A;
+  const Walk w = walk_of(d);
+  const WalkArrays b = walk_bands(d);
+  const int tiles = w.ntx * w.nty;
+  double* yw = walk_array(d, kWalkY);
+  double* lw = walk_array(d, kWalkL);
+  double* uw = walk_array(d, kWalkU);
+  k_walk_gather<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, y, yw);
+  check_launch(ctx, "walk_gather");
+  k_walk_sweep<false><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, yw, lw, d.d_tile_tickets, d.d_err);
+  check_launch(ctx, "walk_lsweep");
+  k_walk_sweep<true><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, lw, uw, d.d_tile_tickets, d.d_err);
+  check_launch(ctx, "walk_usweep");
+  k_walk_scatter<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, uw, z);
+  check_launch(ctx, "walk_scatter");
 }
 
-// The sweeps' propagation vector (d_tmp) is refilled by pc_reset; nothing else
-// of this schedule needs resetting besides the tickets.
+// After a failed application: both propagation arrays back to the sentinel
+// (the tickets are reset by pc_reset).
 void ilu_stencil_reset(ab2_context* ctx, const Ilu0Data& d) {
-  (void)ctx;
-  (void)d;
+  if (!d.d_walk) return;
+  k_fill_bits<<<bulk_grid(ctx, 2 * d.walk_n), kThreads, 0, ctx->stream>>>(2 * d.walk_n, kSentinel,
+                                                                          walk_array(d, kWalkL));
+  check_launch(ctx, "walk_fill");
 }
 
 }  // namespace ab2

@@ -503,14 +503,14 @@ int ab2_solver_create(ab2_context* ctx, const ab2_matrix* A, const ab2_solver_op
     S->pc->variant = o->spmv_variant;
     const int nw = o->solver == AB2_SOLVER_CG ? 4 : 8;
     for (int i = 0; i < nw; ++i) {
-      S->w[i] = dev_alloc<double>((size_t)A->n);
+      S->w[i] = dev_alloc<double>(ctx, (size_t)A->n);
       AB2_CUDA(cudaMemsetAsync(S->w[i], 0, sizeof(double) * (size_t)std::max(A->n, 1), ctx->stream));
     }
-    S->d_st = dev_alloc<SolveState>(1);
+    S->d_st = dev_alloc<SolveState>(ctx, 1);
     AB2_CUDA(cudaMemsetAsync(S->d_st, 0, sizeof(SolveState), ctx->stream));
     AB2_CUDA(cudaMallocHost((void**)&S->h_st, sizeof(SolveState)));
     S->hist_cap = 2 * o->max_iter + 8;  // BiCGStab tests s and r each iteration
-    S->d_hist = dev_alloc<double>((size_t)S->hist_cap);
+    S->d_hist = dev_alloc<double>(ctx, (size_t)S->hist_cap);
     if (o->use_graph) build_graph(S);
     AB2_CUDA(cudaEventRecord(S->ev1, ctx->stream));
     AB2_CUDA(cudaEventSynchronize(S->ev1));
@@ -610,9 +610,9 @@ int ab2_solver_destroy(ab2_solver* S) {
   if (S->exec) cudaGraphExecDestroy(S->exec);
   if (S->graph) cudaGraphDestroy(S->graph);
   if (S->pc) ab2_precond_destroy(S->pc);
-  for (double* p : S->w) dev_free(p);
-  dev_free(S->d_st);
-  dev_free(S->d_hist);
+  for (double* p : S->w) dev_free(S->ctx, p);
+  dev_free(S->ctx, S->d_st);
+  dev_free(S->ctx, S->d_hist);
   if (S->h_st) cudaFreeHost(S->h_st);
   if (S->ev0) cudaEventDestroy(S->ev0);
   if (S->ev1) cudaEventDestroy(S->ev1);

@@ -286,8 +286,8 @@ void ilu_symbolic(const ab2_matrix* A, Ilu0Data& d) {
   for (int l = 0; l < d.levels_u; ++l) d.widest_u = std::max(d.widest_u, (ptr_u[l + 1] - ptr_u[l]) / 32);
   d.len_l = (int)d.h_perm_l.size();
   d.len_u = (int)perm_u.size();
-  d.d_perm_l = dev_alloc<int>(d.h_perm_l.size());
-  d.d_perm_u = dev_alloc<int>(perm_u.size());
+  d.d_perm_l = dev_alloc<int>(A->ctx, d.h_perm_l.size());
+  d.d_perm_u = dev_alloc<int>(A->ctx, perm_u.size());
   AB2_CUDA(cudaMemcpy(d.d_perm_l, d.h_perm_l.data(), sizeof(int) * d.h_perm_l.size(), cudaMemcpyHostToDevice));
   AB2_CUDA(cudaMemcpy(d.d_perm_u, perm_u.data(), sizeof(int) * perm_u.size(), cudaMemcpyHostToDevice));
 }
@@ -310,10 +310,10 @@ int sweep_blocks(ab2_context* ctx, int len, int widest_chunks) {
 void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule) {
   const ab2_matrix* A = pc->A;
   Ilu0Data& d = pc->ilu;
-  d.d_lu = dev_alloc<double>((size_t)A->nnz);
-  d.d_tmp = dev_alloc<double>((size_t)A->n);
-  d.d_counters = dev_alloc<unsigned int>(2);
-  d.d_err = dev_alloc<int>(1);
+  d.d_lu = dev_alloc<double>(ctx, (size_t)A->nnz);
+  d.d_tmp = dev_alloc<double>(ctx, (size_t)A->n);
+  d.d_counters = dev_alloc<unsigned int>(ctx, 2);
+  d.d_err = dev_alloc<int>(ctx, 1);
   AB2_CUDA(cudaMemsetAsync(d.d_counters, 0, 2 * sizeof(unsigned int), ctx->stream));
   AB2_CUDA(cudaMemsetAsync(d.d_err, 0, sizeof(int), ctx->stream));
   AB2_CUDA(cudaMemcpyAsync(d.d_lu, A->d_v, sizeof(double) * (size_t)A->nnz, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -338,11 +338,11 @@ void cheb_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o) 
   const int n = A->n;
   ChebData& c = pc->cheb;
   c.order = o->poly_order;
-  c.d_p = dev_alloc<double>((size_t)n);
-  c.d_y[0] = dev_alloc<double>((size_t)n);
-  c.d_y[1] = dev_alloc<double>((size_t)n);
-  c.d_xcopy = dev_alloc<double>((size_t)n);
-  double* x = dev_alloc<double>((size_t)n);
+  c.d_p = dev_alloc<double>(ctx, (size_t)n);
+  c.d_y[0] = dev_alloc<double>(ctx, (size_t)n);
+  c.d_y[1] = dev_alloc<double>(ctx, (size_t)n);
+  c.d_xcopy = dev_alloc<double>(ctx, (size_t)n);
+  double* x = dev_alloc<double>(ctx, (size_t)n);
   double* y = c.d_y[0];
   double* s = red_slot(ctx, 0).result;
   double* s_out = s;
@@ -380,9 +380,9 @@ void cheb_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o) 
   // Lanczos on S A S, S = diag(sqrt(1/a_ii)), from the same start vector:
   // alpha = smallest Ritz value, beta = 1.1 x the largest.
   auto lanczos = [&](int steps) {
-    double* s = dev_alloc<double>((size_t)n);
-    double* vp = dev_alloc<double>((size_t)n);
-    double* t = dev_alloc<double>((size_t)n);
+    double* s = dev_alloc<double>(ctx, (size_t)n);
+    double* vp = dev_alloc<double>(ctx, (size_t)n);
+    double* t = dev_alloc<double>(ctx, (size_t)n);
     double* w = c.d_xcopy;  // free until the first application
     k_sqrt<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, pc->d_inv, s);
     check_launch(ctx, "sqrt");
@@ -419,9 +419,9 @@ void cheb_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o) 
     c.alpha = lmin;
     c.beta = 1.1 * lmax;
     AB2_CUDA(cudaStreamSynchronize(ctx->stream));
-    dev_free(s);
-    dev_free(vp);
-    dev_free(t);
+    dev_free(ctx, s);
+    dev_free(ctx, vp);
+    dev_free(ctx, t);
   };
   if (o->cheb_lanczos) {
     lanczos(o->poly_factor_max_iter);
@@ -430,7 +430,7 @@ void cheb_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o) 
     c.alpha = power(true, c.beta);
   }
   if (o->poly_factor != 0.) c.alpha = c.beta / o->poly_factor;
-  dev_free(x);
+  dev_free(ctx, x);
   op_fill(ctx, n, 0.0, y);
   const int steps = std::max(1, c.order);
   c.a.assign(steps, 0.0);
@@ -565,7 +565,7 @@ int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_
     pc->A = A;
     pc->kind = o->kind;
     if (o->kind == AB2_PC_DIAG || o->kind == AB2_PC_CHEB) {
-      pc->d_inv = dev_alloc<double>((size_t)A->n);
+      pc->d_inv = dev_alloc<double>(ctx, (size_t)A->n);
       // init(): assign(inv, 1) then computeInvDiag (DiagPreconditioner.h:49-54)
       op_inv_diag(ctx, A, pc->d_inv);
     }
@@ -595,19 +595,20 @@ int ab2_precond_apply(ab2_context* ctx, const ab2_precond* pc, const ab2_vector*
 int ab2_precond_destroy(ab2_precond* pc) {
   if (!pc) return AB2_ERR_BAD_ARG;
   if (pc->ctx) ctx_quiesce(pc->ctx);
-  dev_free(pc->d_inv);
-  dev_free(pc->ilu.d_lu);
-  dev_free(pc->ilu.d_perm_l);
-  dev_free(pc->ilu.d_perm_u);
-  dev_free(pc->ilu.d_tmp);
-  dev_free(pc->ilu.d_counters);
-  dev_free(pc->ilu.d_err);
-  dev_free(pc->ilu.d_bands);
-  dev_free(pc->ilu.d_tile_tickets);
-  dev_free(pc->cheb.d_p);
-  dev_free(pc->cheb.d_y[0]);
-  dev_free(pc->cheb.d_y[1]);
-  dev_free(pc->cheb.d_xcopy);
+  dev_free(pc->ctx, pc->d_inv);
+  dev_free(pc->ctx, pc->ilu.d_lu);
+  dev_free(pc->ctx, pc->ilu.d_perm_l);
+  dev_free(pc->ctx, pc->ilu.d_perm_u);
+  dev_free(pc->ctx, pc->ilu.d_tmp);
+  dev_free(pc->ctx, pc->ilu.d_counters);
+  dev_free(pc->ctx, pc->ilu.d_err);
+  dev_free(pc->ctx, pc->ilu.d_bands);
+  dev_free(pc->ctx, pc->ilu.d_walk);
+  dev_free(pc->ctx, pc->ilu.d_tile_tickets);
+  dev_free(pc->ctx, pc->cheb.d_p);
+  dev_free(pc->ctx, pc->cheb.d_y[0]);
+  dev_free(pc->ctx, pc->cheb.d_y[1]);
+  dev_free(pc->ctx, pc->cheb.d_xcopy);
   if (pc->ctx) ctx_release(pc->ctx);
   delete pc;
   return AB2_OK;

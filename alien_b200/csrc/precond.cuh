@@ -31,8 +31,13 @@ struct Ilu0Data {
   // 7-point lexicographic matrices: tile-walk schedule (ilu_stencil.cu)
   bool stencil = false;
   int st_nx = 0, st_ny = 0, st_nz = 0;
-  double* d_bands = nullptr;            // 8 n-vectors: L(-k,-j,-i) U(+i,+j,+k) pivot diag
+  double* d_bands = nullptr;            // set-up only: 8 n-vectors L(-k,-j,-i) U(+i,+j,+k) pivot diag
   unsigned int* d_tile_tickets = nullptr;  // factorisation, L sweep, U sweep
+  // Walk layout (ilu_stencil.cu): 10 arrays of walk_n doubles -- the factor's
+  // L(-k,-j,-i), U(+i,+j,+k) and pivot bands, the gathered right-hand side,
+  // and the two sweeps' propagation arrays.
+  long long walk_n = 0;
+  double* d_walk = nullptr;
 };
 
 // Detects a 3-D 7-point matrix in lexicographic order and, if found,

@@ -6,6 +6,10 @@
 // writes the NC results.  The grid size is a function of the problem size
 // only, so the summation tree -- and therefore the rounding -- is identical on
 // every run.  The result stays on the device: no host round trip per dot.
+//
+// T is the accumulation type: double for the FP64 path, float for the FP32
+// inner solves of the mixed-precision solver (partials and results then live
+// in the same slot buffers, reinterpreted).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -14,41 +18,46 @@ namespace ab2 {
 
 enum class Combine { Sum, Max };
 
-template <Combine C>
-__device__ __forceinline__ double combine(double a, double b) {
+template <Combine C, class T>
+__device__ __forceinline__ T combine(T a, T b) {
   if constexpr (C == Combine::Sum) return a + b;
   else return a > b ? a : b;
 }
 
-template <Combine C>
-__device__ __forceinline__ double warp_reduce(double v) {
+template <Combine C, class T>
+__device__ __forceinline__ T warp_reduce(T v) {
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) v = combine<C>(v, __shfl_down_sync(0xffffffffu, v, off));
+  for (int off = 16; off > 0; off >>= 1) v = combine<C, T>(v, __shfl_down_sync(0xffffffffu, v, off));
   return v;
+}
+
+template <Combine C, class T>
+__device__ __forceinline__ T reduce_identity() {
+  return C == Combine::Sum ? T(0) : -T(1) / T(0);
 }
 
 // Reduces acc[0..NC) over the whole grid.  Must be called by every thread of
 // every block (no early returns before it).  Returns true in the thread that
 // wrote the final results (thread 0 of the last block), so callers can run
 // scalar epilogues there; `out` then holds the NC results.
-template <int NC, Combine C = Combine::Sum>
-__device__ __forceinline__ bool grid_reduce(double (&acc)[NC], double* partials, unsigned int* counter, double* out) {
-  __shared__ double s_warp[NC][32];
+template <int NC, Combine C = Combine::Sum, class T>
+__device__ __forceinline__ bool grid_reduce(T (&acc)[NC], T* partials, unsigned int* counter, T* out) {
+  __shared__ T s_warp[NC][32];
   __shared__ bool s_last;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
-    double v = warp_reduce<C>(acc[c]);
+    T v = warp_reduce<C, T>(acc[c]);
     if (lane == 0) s_warp[c][warp] = v;
   }
   __syncthreads();
   if (warp == 0) {
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      double v = lane < nwarps ? s_warp[c][lane] : (C == Combine::Sum ? 0.0 : -1.0 / 0.0);
-      v = warp_reduce<C>(v);
+      T v = lane < nwarps ? s_warp[c][lane] : reduce_identity<C, T>();
+      v = warp_reduce<C, T>(v);
       if (lane == 0) partials[(size_t)c * gridDim.x + blockIdx.x] = v;
     }
     if (lane == 0) {
@@ -63,9 +72,9 @@ __device__ __forceinline__ bool grid_reduce(double (&acc)[NC], double* partials,
     __threadfence();
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      double v = (C == Combine::Sum ? 0.0 : -1.0 / 0.0);
-      for (int b = lane; b < (int)gridDim.x; b += 32) v = combine<C>(v, __ldcg(partials + (size_t)c * gridDim.x + b));
-      v = warp_reduce<C>(v);
+      T v = reduce_identity<C, T>();
+      for (int b = lane; b < (int)gridDim.x; b += 32) v = combine<C, T>(v, __ldcg(partials + (size_t)c * gridDim.x + b));
+      v = warp_reduce<C, T>(v);
       if (lane == 0) out[c] = v;
     }
     if (lane == 0) {

@@ -37,8 +37,10 @@ __device__ __forceinline__ bool is_sentinel(double v) {
 
 __device__ __forceinline__ double sentinel_value() { return __longlong_as_double((long long)kSentinel); }
 
-// Waits until *p no longer holds the sentinel; bounded.
-__device__ __forceinline__ double wait_value(const double* p, int* err) {
+// Waits until *p no longer holds the sentinel; bounded.  Out of line: callers
+// take this path rarely, and inlining its loop at every call site of an
+// unrolled walk costs registers and instruction cache on the common path.
+__device__ __noinline__ double wait_value(const double* p, int* err) {
   double v = ld_relaxed(p);
   if (!is_sentinel(v)) return v;
   const long long t0 = clock64();

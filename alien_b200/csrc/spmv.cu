@@ -305,23 +305,23 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
     const size_t nnz = (size_t)A->nnz;
     A->h_rp.assign(row_ptr, row_ptr + n + 1);
     A->h_ci.assign(cols, cols + nnz);
-    A->d_rp = dev_alloc<int>((size_t)n + 1, &A->device_bytes);
-    A->d_ci = dev_alloc<int>(nnz, &A->device_bytes);
-    A->d_v = dev_alloc<double>(nnz, &A->device_bytes);
-    A->d_dcol = dev_alloc<int>((size_t)n, &A->device_bytes);
+    A->d_rp = dev_alloc<int>(ctx, (size_t)n + 1, &A->device_bytes);
+    A->d_ci = dev_alloc<int>(ctx, nnz, &A->device_bytes);
+    A->d_v = dev_alloc<double>(ctx, nnz, &A->device_bytes);
+    A->d_dcol = dev_alloc<int>(ctx, (size_t)n, &A->device_bytes);
     AB2_CUDA(cudaMemcpyAsync(A->d_rp, row_ptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));
     AB2_CUDA(cudaMemcpyAsync(A->d_ci, cols, sizeof(int) * nnz, cudaMemcpyHostToDevice, ctx->stream));
     AB2_CUDA(cudaMemcpyAsync(A->d_v, vals, sizeof(double) * nnz, cudaMemcpyHostToDevice, ctx->stream));
     if (n > 0) {
       // Device-side profile check: every later kernel indexes x by these columns.
-      int* d_bad = dev_alloc<int>(1);
+      int* d_bad = dev_alloc<int>(ctx, 1);
       AB2_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), ctx->stream));
       k_validate<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, d_bad);
       check_launch(ctx, "validate");
       int bad = 0;
       AB2_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
       AB2_CUDA(cudaStreamSynchronize(ctx->stream));
-      dev_free(d_bad);
+      dev_free(ctx, d_bad);
       if (bad & 1) throw Error{AB2_ERR_BAD_ARG, "row_ptr is not non-decreasing"};
       if (bad & 2) throw Error{AB2_ERR_BAD_ARG, "column index out of range"};
       if (bad & 4) throw Error{AB2_ERR_BAD_ARG, "columns must be strictly increasing inside each row"};
@@ -330,7 +330,7 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
     }
     std::vector<int> blocks = make_row_blocks(n, row_ptr);
     A->n_row_blocks = (int)blocks.size() - 1;
-    A->d_row_blocks = dev_alloc<int>(blocks.size(), &A->device_bytes);
+    A->d_row_blocks = dev_alloc<int>(ctx, blocks.size(), &A->device_bytes);
     AB2_CUDA(cudaMemcpyAsync(A->d_row_blocks, blocks.data(), sizeof(int) * blocks.size(), cudaMemcpyHostToDevice,
                              ctx->stream));
     if (A->formats & AB2_FMT_ELL) {
@@ -347,9 +347,9 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
       require(acc * kEllSlice < (1LL << 31) * 8, "matrix too large for the sliced-ELL layout");
       off[ns] = (int)acc;
       A->ell_stored = acc * kEllSlice;
-      A->d_ell_off = dev_alloc<int>(off.size(), &A->device_bytes);
-      A->d_ell_ci = dev_alloc<int>((size_t)A->ell_stored, &A->device_bytes);
-      A->d_ell_v = dev_alloc<double>((size_t)A->ell_stored, &A->device_bytes);
+      A->d_ell_off = dev_alloc<int>(ctx, off.size(), &A->device_bytes);
+      A->d_ell_ci = dev_alloc<int>(ctx, (size_t)A->ell_stored, &A->device_bytes);
+      A->d_ell_v = dev_alloc<double>(ctx, (size_t)A->ell_stored, &A->device_bytes);
       AB2_CUDA(cudaMemcpyAsync(A->d_ell_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, ctx->stream));
       const int n_pad = ns * kEllSlice;
       if (n_pad > n) {
@@ -358,8 +358,8 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
       }
     }
     if (A->formats & AB2_FMT_F32) {
-      A->d_v32 = dev_alloc<float>(nnz, &A->device_bytes);
-      if (A->formats & AB2_FMT_ELL) A->d_ell_v32 = dev_alloc<float>((size_t)A->ell_stored, &A->device_bytes);
+      A->d_v32 = dev_alloc<float>(ctx, nnz, &A->device_bytes);
+      if (A->formats & AB2_FMT_ELL) A->d_ell_v32 = dev_alloc<float>(ctx, (size_t)A->ell_stored, &A->device_bytes);
     }
     refresh_values(ctx, A);
     AB2_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -383,16 +383,16 @@ int ab2_matrix_update_values(ab2_context* ctx, ab2_matrix* A, const double* vals
 int ab2_matrix_destroy(ab2_matrix* A) {
   if (!A) return AB2_ERR_BAD_ARG;
   if (A->ctx) ctx_quiesce(A->ctx);
-  dev_free(A->d_rp);
-  dev_free(A->d_ci);
-  dev_free(A->d_v);
-  dev_free(A->d_dcol);
-  dev_free(A->d_v32);
-  dev_free(A->d_row_blocks);
-  dev_free(A->d_ell_off);
-  dev_free(A->d_ell_ci);
-  dev_free(A->d_ell_v);
-  dev_free(A->d_ell_v32);
+  dev_free(A->ctx, A->d_rp);
+  dev_free(A->ctx, A->d_ci);
+  dev_free(A->ctx, A->d_v);
+  dev_free(A->ctx, A->d_dcol);
+  dev_free(A->ctx, A->d_v32);
+  dev_free(A->ctx, A->d_row_blocks);
+  dev_free(A->ctx, A->d_ell_off);
+  dev_free(A->ctx, A->d_ell_ci);
+  dev_free(A->ctx, A->d_ell_v);
+  dev_free(A->ctx, A->d_ell_v32);
   if (A->ctx) ctx_release(A->ctx);
   delete A;
   return AB2_OK;

@@ -2,7 +2,7 @@
 7-point diffusion system, plain FP64 drop-in path, one B200 per rank.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--n 192] [--precond ilu0|cheb|diag]
+                    [--n 192] [--method ilu0|jacobi|cheb3_saad_power20|cheb3_saad_lanczos20]
 
 Workload (per rank): 192^3 cells, log10 k = seeded Gaussian random field
 (std 1, smoothing length 4 cells), harmonic-mean faces, Dirichlet faces,
@@ -40,6 +40,17 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+# Plain FP64 forms timed on the same system (CG to ||r||/||b|| < 1e-8).
+# "ilu0" is the headline (the configuration names CG+ILU0 first); the others
+# are reported beside it under "methods".
+METHODS = {
+    "ilu0": dict(precond="ilu0"),
+    "jacobi": dict(precond="diag"),
+    "cheb3_saad_power20": dict(precond="cheb", cheb_saad=True, poly_order=3, poly_factor_max_iter=20),
+    "cheb3_saad_lanczos20": dict(precond="cheb", cheb_saad=True, cheb_lanczos=True, poly_order=3,
+                                 poly_factor_max_iter=20),
+}
 
 
 def peaks():
@@ -135,6 +146,27 @@ def spmv_bytes(info, n: int) -> int:
     return int(info.ell_stored * 12 + 4 * (n // 32 + 1) + 16 * n)
 
 
+def ilu_bytes(n: int, nnz: int) -> int:
+    """ILU0 apply (both sweeps), algorithmic minimum for the stencil layout:
+    every factor value read once (no column indices: the stencil fixes
+    them), y read once, x written once."""
+    return int(8 * nnz + 16 * n)
+
+
+def iteration_bytes(method: str, n: int, nnz: int) -> int:
+    """Fused-schedule lower bound of one PCG iteration (FP64), from the CSR
+    SpMV bytes B = 12 nnz + 4(n+1) + 16 n: Jacobi B + 104 n; ILU0
+    B + B_LU + 120 n with B_LU = 12 nnz + 4(n+1) + 8 n; Chebyshev(3)
+    4 B + 200 n."""
+    b_spmv = 12 * nnz + 4 * (n + 1) + 16 * n
+    pc = METHODS[method]["precond"]
+    if pc == "diag":
+        return b_spmv + 104 * n
+    if pc == "ilu0":
+        return b_spmv + (12 * nnz + 4 * (n + 1) + 8 * n) + 120 * n
+    return 4 * b_spmv + 200 * n
+
+
 def load_traffic():
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
@@ -146,17 +178,34 @@ def load_traffic():
 
 
 # ----------------------------------------------------------------------------- reference arm
-def reference_sample(P, precond: str, iterations_hint: int | None, sample_iters=(2, 8)):
+def reference_method(method: str) -> tuple[dict, str]:
+    """The reference configuration that times `method` on the CPU: the same
+    preconditioner through Alien's own templates.  Lanczos bounds have no
+    reference counterpart; its nearest reference form (power-method bounds,
+    same Saad recurrence) stands in and the sample says so."""
+    kw = dict(poly_factor=0.0, poly_order=3, poly_factor_max_iter=20, cheb_saad=False)
+    m = METHODS[method]
+    kw["precond"] = m["precond"]
+    if m["precond"] == "cheb":
+        kw["cheb_saad"] = True
+        kw["poly_order"] = m["poly_order"]
+        kw["poly_factor_max_iter"] = m["poly_factor_max_iter"]
+    label = {"ilu0": "ILU0Preconditioner.h", "diag": "DiagPreconditioner.h",
+             "cheb": "ChebyshevPreconditioner<.., true>.h (power-method bounds)"}[m["precond"]]
+    return kw, label
+
+
+def reference_sample(P, method: str, iterations_hint: int | None, sample_iters=(2, 8)):
     """Alien's own templates (oracle/_ref) on one host core: set-up + a few
     iterations, extrapolated to `iterations_hint` (the iteration count this
     solve takes; the templates and the GPU agree on it to +-2)."""
     from oracle import oracle as O
 
+    kw, _ = reference_method(method)
     times = []
     for m in sample_iters:
         t = time.perf_counter()
-        r = O.solve(P.row_ptr, P.cols, P.vals, P.b, solver="cg", precond=precond, tol=1e-8, max_iter=m,
-                    poly_factor=0.0, poly_order=3, poly_factor_max_iter=20, which="ref")
+        r = O.solve(P.row_ptr, P.cols, P.vals, P.b, solver="cg", tol=1e-8, max_iter=m, which="ref", **kw)
         times.append((r.iterations, time.perf_counter() - t))
     (i1, t1), (i2, t2) = times
     per_iter = (t2 - t1) / max(i2 - i1, 1)
@@ -172,10 +221,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=192)
-    ap.add_argument("--precond", default="ilu0", choices=["ilu0", "cheb", "diag"])
+    ap.add_argument("--method", default="ilu0", choices=sorted(METHODS))
     ap.add_argument("--max-iter", type=int, default=20000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-methods", action="store_true", help="time the headline method only")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="drive the Krylov loop from the host instead of the CUDA graph (same kernels; for "
+                         "profilers that do not see kernels inside conditional graph nodes)")
     a = ap.parse_args()
 
     world, rank, local = dist_init()
@@ -183,11 +236,10 @@ def main():
 
     n1 = a.n
     P = abi.diffusion(n1, n1, n1, sigma=1.0, smooth=4.0, seed=rank)
-    workload = f"diffusion3d_{n1}^3_grf_sigma1_len4_cg_{a.precond}_tol1e-8"
+    workload = f"diffusion3d_{n1}^3_grf_sigma1_len4_cg_{a.method}_tol1e-8"
     config = {"workload": workload, "rows": P.n, "nnz": P.nnz, "precision": "fp64", "solver": "cg",
-              "precond": a.precond, "tol": 1e-8, "formats": "csr+ell32", "l2": "inputs larger than L2 (no flush)",
+              "method": a.method, "tol": 1e-8, "formats": "csr+ell32", "l2": "inputs larger than L2 (no flush)",
               "parallelism": f"independent systems x{world}"}
-    cheb_kw = dict(poly_factor=0.0, poly_order=3, poly_factor_max_iter=20)
 
     if a.impl == "reference":
         if rank != 0:
@@ -195,9 +247,15 @@ def main():
         hint_file = ROOT / "profiles" / "iterations.json"
         hints = json.loads(hint_file.read_text()) if hint_file.exists() else {}
         hint = hints.get(workload)
+        rkw, label = reference_method(a.method)
+        if hint is None and P.n <= 300_000:  # small enough to count the iterations with one full solve
+            from oracle import oracle as O
+
+            hint = O.solve(P.row_ptr, P.cols, P.vals, P.b, solver="cg", tol=1e-8, max_iter=a.max_iter, which="ref",
+                           **rkw).iterations
         steps = []
         for i in range(a.warmup + a.steps):
-            v, setup, per_iter, spent = reference_sample(P, a.precond, hint)
+            v, setup, per_iter, spent = reference_sample(P, a.method, hint)
             if i >= a.warmup:
                 steps.append(v)
         value = float(np.median(steps))
@@ -206,8 +264,9 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
                 "impl": "reference", "config": config,
                 "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": "reference",
-                                 "sample": f"Alien CG.h+{a.precond} templates, set-up + 2 and 8 iterations on the full "
-                                           f"system, per-iteration time scaled to {hint or 'sampled'} iterations"},
+                                 "sample": f"Alien CG.h + {label} on 1 host core: set-up + 2 and 8 iterations on "
+                                           f"the full system, per-iteration time scaled to {hint or 'sampled'} "
+                                           f"iterations"},
                 "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
@@ -220,11 +279,16 @@ def main():
     A = ctx.matrix(P.row_ptr, P.cols, P.vals, abi.FMT_CSR | abi.FMT_ELL)
     b = ctx.vector(P.b)
     x = ctx.vector(P.n)
-    kw = dict(solver="cg", precond=a.precond, tol=1e-8, max_iter=a.max_iter, **cheb_kw)
 
-    def step():
+    def solver_kw(method):
+        return dict(solver="cg", tol=1e-8, max_iter=a.max_iter, poly_factor=0.0, use_graph=not a.host_loop,
+                    **METHODS[method])
+
+    kw = solver_kw(a.method)
+
+    def step(kw=kw):
         S = abi.Solver(ctx, A, **kw)
-        x.upload(np.zeros(P.n))
+        ctx.assign(x, 0.0)
         st = S.solve(b, x)
         S.close()
         return st
@@ -253,28 +317,63 @@ def main():
     xs = x.download()
     err = float(np.linalg.norm(xs - P.x_true) / np.linalg.norm(P.x_true))
 
-    # Dominant kernel: the sliced-ELL SpMV, timed alone with events on the same stream.
+    # Every plain-FP64 method on the same system: one warm + one timed solve each.
+    methods = {}
+    for m in ([] if a.no_methods else sorted(METHODS)):
+        mkw = solver_kw(m)
+        step(mkw)
+        ctx.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        mst = step(mkw)
+        m1.record(stream)
+        m1.synchronize()
+        s = m0.elapsed_time(m1) / 1e3
+        methods[m] = {"s": round(s, 5), "iterations": mst.iterations, "converged": bool(mst.succeeded),
+                      "true_rel_residual": mst.true_residual, "setup_ms": round(mst.setup_ms, 3),
+                      "solve_ms": round(mst.solve_ms, 3),
+                      "solver_gbs": round(mst.iterations * iteration_bytes(m, P.n, P.nnz) / (mst.solve_ms * 1e-3)
+                                          / 1e9, 1)}
+
+    pk, pk_kind = peaks()
+    traffic = load_traffic()
+
+    def timed(f, reps):
+        for _ in range(3):
+            f()
+        k0 = torch.cuda.Event(enable_timing=True)
+        k1 = torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        for _ in range(reps):
+            f()
+        k1.record(stream)
+        k1.synchronize()
+        return k0.elapsed_time(k1) / reps
+
+    def roof(kernel, nbytes, ms, key):
+        g = nbytes / (ms * 1e-3) / 1e9
+        return {"bound": "hbm", "kernel": kernel, "achieved": round(g, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": round(g / pk["hbm_gbs"], 4), "peak_source": pk_kind, "algorithmic_bytes": int(nbytes),
+                "launch_us": round(ms * 1e3, 2), "traffic": traffic.get(key)}
+
+    # The sliced-ELL SpMV, timed alone with events on the same stream.
     info = A.info
     vy = ctx.vector(P.n)
-    for _ in range(5):
-        ctx.mult(A, b, vy, abi.SPMV_ELL)
-    k0 = torch.cuda.Event(enable_timing=True)
-    k1 = torch.cuda.Event(enable_timing=True)
-    reps = 50
-    k0.record(stream)
-    for _ in range(reps):
-        ctx.mult(A, b, vy, abi.SPMV_ELL)
-    k1.record(stream)
-    k1.synchronize()
-    spmv_ms = k0.elapsed_time(k1) / reps
-    B = spmv_bytes(info, P.n)
-    pk, pk_kind = peaks()
-    achieved = B / (spmv_ms * 1e-3) / 1e9
-    traffic = load_traffic().get(f"spmv_ell_{n1}")
-    roofline = {"bound": "hbm", "kernel": "k_spmv_ell (sliced ELL-32 FP64 SpMV)", "achieved": round(achieved, 1),
-                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
-                "peak_source": pk_kind, "algorithmic_bytes": B, "launch_us": round(spmv_ms * 1e3, 2),
-                "traffic": traffic}
+    spmv_ms = timed(lambda: ctx.mult(A, b, vy, abi.SPMV_ELL), 50)
+    spmv_roof = roof("k_spmv_ell (sliced ELL-32 FP64 SpMV)", spmv_bytes(info, P.n), spmv_ms, f"spmv_ell_{n1}")
+    achieved = spmv_roof["achieved"]
+
+    # The headline step's dominant kernel: for ILU0 the two triangular sweeps
+    # (one precond apply), else the SpMV.
+    if METHODS[a.method]["precond"] == "ilu0":
+        pc = abi.Precond(ctx, A, "ilu0")
+        ilu_ms = timed(lambda: pc.apply(b, vy), 20)
+        roofline = roof("k_stencil_wave<kLower>+k_stencil_wave<kUpper> (ILU0 apply, tiled wavefront)",
+                        ilu_bytes(P.n, P.nnz), ilu_ms, f"ilu0_apply_{n1}")
+        pc.close()
+    else:
+        roofline = spmv_roof
 
     # End to end through the C ABI from host arrays.
     e2e = None
@@ -304,9 +403,10 @@ def main():
         from oracle import oracle as O
 
         if O.ref_available():
-            v, setup, per_iter, spent = reference_sample(P, a.precond, st.iterations)
+            v, setup, per_iter, spent = reference_sample(P, a.method, st.iterations)
+            _, label = reference_method(a.method)
             cpu = {"value": round(v, 3), "unit": "s", "cores": 1, "kind": "reference",
-                   "sample": f"Alien CG.h+{a.precond} templates (oracle/_ref) on 1 host core: set-up + 2 and 8 "
+                   "sample": f"Alien CG.h + {label} (oracle/_ref) on 1 host core: set-up + 2 and 8 "
                              f"iterations of the same system ({spent:.1f} s), scaled to {st.iterations} iterations "
                              f"(set-up {setup:.2f} s, {per_iter*1e3:.1f} ms/iteration)"}
 
@@ -318,8 +418,10 @@ def main():
                 "iterations": st.iterations, "converged": bool(st.succeeded),
                 "true_rel_residual": st.true_residual, "rel_error_vs_x_true": err,
                 "setup_ms": round(st.setup_ms, 3), "solve_ms": round(st.solve_ms, 3),
-                "spmv_gbs": round(achieved, 1), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": int(launches), "clocks": clk.summary()}
+                "solver_gbs": round(st.iterations * iteration_bytes(a.method, P.n, P.nnz) / (st.solve_ms * 1e-3)
+                                    / 1e9, 1),
+                "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "methods": methods,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
