@@ -74,6 +74,20 @@ class Status(C.Structure):
                 ("setup_ms", C.c_double), ("solve_ms", C.c_double)]
 
 
+class MixedOptions(C.Structure):
+    _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("tol", C.c_double), ("max_outer", C.c_int),
+                ("inner_tol", C.c_double), ("inner_max_iter", C.c_int), ("poly_factor", C.c_double),
+                ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int), ("cheb_saad", C.c_int),
+                ("cheb_lanczos", C.c_int), ("ilu_schedule", C.c_int), ("spmv_variant", C.c_int),
+                ("use_graph", C.c_int)]
+
+
+class MixedStatus(C.Structure):
+    _fields_ = [("succeeded", C.c_int), ("outer_iterations", C.c_int), ("inner_iterations", C.c_int),
+                ("error", C.c_int), ("true_residual", C.c_double), ("setup_ms", C.c_double),
+                ("solve_ms", C.c_double)]
+
+
 class Problem(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("row_ptr", C.POINTER(C.c_int)), ("cols", C.POINTER(C.c_int)), ("vals", C.POINTER(C.c_double)),
@@ -139,6 +153,11 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_solver_solve": (_I, [_P, _P, _P, C.POINTER(Status)]),
     "ab2_solver_history": (_I, [_P, _DP, _I, _IP]),
     "ab2_solver_destroy": (_I, [_P]),
+    "ab2_mixed_options_default": (None, [C.POINTER(MixedOptions)]),
+    "ab2_mixed_create": (_I, [_P, _P, C.POINTER(MixedOptions), C.POINTER(_P)]),
+    "ab2_mixed_solve": (_I, [_P, _P, _P, C.POINTER(MixedStatus)]),
+    "ab2_mixed_history": (_I, [_P, _DP, _I, _IP]),
+    "ab2_mixed_destroy": (_I, [_P]),
     "ab2_problem_poisson": (_I, [_I, _I, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_diffusion": (_I, [_I, _I, _I, _D, _D, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_convdiff": (_I, [_I, _I, _I, _D, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
@@ -463,6 +482,76 @@ class Solver:
     def close(self):
         if self.h:
             lib().ab2_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class MixedResult:
+    succeeded: bool
+    outer_iterations: int
+    inner_iterations: int
+    error: int
+    true_residual: float
+    setup_ms: float
+    solve_ms: float
+
+
+def mixed_options(solver="cg", precond="diag", tol=1e-8, max_outer=20, inner_tol=1e-4, inner_max_iter=1000,
+                  poly_factor=0.0, poly_order=3, poly_factor_max_iter=20, cheb_saad=False, cheb_lanczos=False,
+                  ilu_schedule="auto", spmv_variant=SPMV_AUTO, use_graph=True) -> MixedOptions:
+    o = MixedOptions()
+    lib().ab2_mixed_options_default(C.byref(o))
+    o.solver = SOLVER[solver]
+    o.precond = PRECOND[precond]
+    o.tol = tol
+    o.max_outer = max_outer
+    o.inner_tol = inner_tol
+    o.inner_max_iter = inner_max_iter
+    o.poly_factor = poly_factor
+    o.poly_order = poly_order
+    o.poly_factor_max_iter = poly_factor_max_iter
+    o.cheb_saad = int(cheb_saad)
+    o.cheb_lanczos = int(cheb_lanczos)
+    o.ilu_schedule = ILU_SCHEDULE[ilu_schedule]
+    o.spmv_variant = spmv_variant
+    o.use_graph = 1 if use_graph else 0
+    return o
+
+
+class Mixed:
+    """ab2_mixed: FP32 CG/BiCGStab inside FP64 iterative refinement (the matrix
+    needs FMT_F32)."""
+
+    def __init__(self, ctx: Context, A: Matrix, **opts):
+        self.ctx, self.A = ctx, A
+        self.opts = mixed_options(**opts)
+        h = _P()
+        ctx.check(lib().ab2_mixed_create(ctx.h, A.h, C.byref(self.opts), C.byref(h)), "mixed_create")
+        self.h = h
+
+    def solve(self, b: Vector, x: Vector) -> MixedResult:
+        st = MixedStatus()
+        self.ctx.check(lib().ab2_mixed_solve(self.h, b.h, x.h, C.byref(st)), "mixed_solve")
+        return MixedResult(bool(st.succeeded), st.outer_iterations, st.inner_iterations, st.error,
+                           st.true_residual, st.setup_ms, st.solve_ms)
+
+    def history(self) -> np.ndarray:
+        n = C.c_int()
+        lib().ab2_mixed_history(self.h, None, 0, C.byref(n))
+        out = np.empty(max(n.value, 0), dtype=np.float64)
+        if n.value:
+            self.ctx.check(lib().ab2_mixed_history(self.h, _dp(out), n.value, C.byref(n)), "mixed_history")
+        return out
+
+    def close(self):
+        if self.h:
+            lib().ab2_mixed_destroy(self.h)
             self.h = None
 
     def __del__(self):

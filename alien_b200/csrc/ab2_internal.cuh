@@ -92,6 +92,13 @@ __device__ __forceinline__ double mul_add_rn(double a, double b, double c) { ret
 __device__ __forceinline__ float mul_add_rn(float a, float b, float c) { return __fadd_rn(c, __fmul_rn(a, b)); }
 __device__ __forceinline__ double mul_sub_rn(double a, double b, double c) { return __dsub_rn(c, __dmul_rn(a, b)); }
 __device__ __forceinline__ float mul_sub_rn(float a, float b, float c) { return __fsub_rn(c, __fmul_rn(a, b)); }
+// Single roundings for kernels templated on the value type.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
 inline void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {
@@ -196,6 +203,9 @@ void op_dot(ab2_context* ctx, int n, const double* x, const double* y, double* o
 void op_norm0(ab2_context* ctx, int n, const double* x, double* out, int slot = 0);
 void op_norm1(ab2_context* ctx, int n, const double* x, double* out, int slot = 0);
 double read_scalar(ab2_context* ctx, const double* d);
+// Precision conversions (round to nearest; widening is exact).
+void op_to_f32(ab2_context* ctx, long long m, const double* a, float* b);
+void op_to_f64(ab2_context* ctx, long long m, const float* a, double* b);
 
 // SpMV family (spmv.cu)
 void op_spmv(ab2_context* ctx, const ab2_matrix* A, const double* x, double* y, int variant);

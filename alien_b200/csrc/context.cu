@@ -83,6 +83,24 @@ RedSlot red_slot(ab2_context* ctx, int slot) {
                  ctx->d_results + (size_t)slot * kMaxRedComps};
 }
 
+namespace {
+template <class S, class D>
+__global__ void k_convert(long long m, const S* __restrict__ a, D* __restrict__ b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (D)a[i];
+}
+}  // namespace
+
+void op_to_f32(ab2_context* ctx, long long m, const double* a, float* b) {
+  k_convert<<<grid_for(m), kThreads, 0, ctx->stream>>>(m, a, b);
+  check_launch(ctx, "to_f32");
+}
+
+void op_to_f64(ab2_context* ctx, long long m, const float* a, double* b) {
+  k_convert<<<grid_for(m), kThreads, 0, ctx->stream>>>(m, a, b);
+  check_launch(ctx, "to_f64");
+}
+
 void op_fill(ab2_context* ctx, int n, double a, double* x) {
   k_fill<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, a, x);
   check_launch(ctx, "fill");

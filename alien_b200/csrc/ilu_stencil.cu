@@ -244,35 +244,40 @@ __device__ __forceinline__ long long walk_row(const Walk& g, long long w) {
   return i + (long long)g.nx * j + g.nxny * k;
 }
 
-// dst[w] = src[row(w)] (0 on padding).
-__global__ void k_walk_gather(Walk g, const double* __restrict__ src, double* __restrict__ dst) {
+// dst[w] = src[row(w)] (0 on padding), rounded to T (the FP32 walk arrays
+// are gathered from the FP64 factor).
+template <class S, class T>
+__global__ void k_walk_gather(Walk g, const S* __restrict__ src, T* __restrict__ dst) {
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < g.nw; w += (long long)gridDim.x * blockDim.x) {
     const long long r = walk_row(g, w);
-    dst[w] = r >= 0 ? __ldg(src + r) : 0.0;
+    dst[w] = r >= 0 ? (T)__ldg(src + r) : T(0);
   }
 }
 
 // dst[row(w)] = src[w], and src[w] back to the sentinel for the next walk.
-__global__ void k_walk_scatter(Walk g, double* __restrict__ src, double* __restrict__ dst) {
+template <class T>
+__global__ void k_walk_scatter(Walk g, T* __restrict__ src, T* __restrict__ dst) {
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < g.nw; w += (long long)gridDim.x * blockDim.x) {
     const long long r = walk_row(g, w);
     if (r >= 0) {
       dst[r] = src[w];
-      src[w] = sentinel_value();
+      src[w] = sentinel_of<T>();
     }
   }
 }
 
+template <class T>
 struct WalkArrays {
-  const double *Lk, *Lj, *Li, *Ui, *Uj, *Uk, *P;
+  const T *Lk, *Lj, *Li, *Ui, *Uj, *Uk, *P;
 };
 
 // Per-step inputs, loaded kWalkPrefetch steps ahead: the right-hand side,
 // three band values (L: -k,-j,-i ; U: +i,+j,+k), the pivot (U walk), and the
 // value owned by the neighbouring tile (bi / bj, first line of the tile only),
 // possibly still the sentinel when loaded.
+template <class T>
 struct PreW {
-  double y, a1, a2, a3, piv, bi, bj;
+  T y, a1, a2, a3, piv, bi, bj;
 };
 
 // One triangular sweep in walk layout.  UP = false: forward sweep
@@ -286,13 +291,13 @@ struct PreW {
 // the instruction count: every array is reached through a per-thread pointer
 // that moves once per group of kWalkPrefetch steps, with constant offsets
 // inside the unrolled group.
-template <bool UP, int kPreB = kWalkPrefetchB>
-__global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArrays b, double* in, double* wave,
+template <bool UP, class T, int kPreB = kWalkPrefetchB>
+__global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArrays<T> b, T* in, T* wave,
                                                               unsigned int* tickets, int* err) {
   constexpr int kPre = kWalkPrefetch;
   static_assert(kPreB >= 1 && kPreB < kPre, "boundary values are loaded inside the band prefetch window");
   constexpr long long kStep = UP ? -kTileThreads : kTileThreads;  // element stride of one step
-  __shared__ double s_val[2][kTile][kTile + 1];
+  __shared__ T s_val[2][kTile][kTile + 1];
   __shared__ int s_tile;
   const int li = threadIdx.x % kTile, lj = threadIdx.x / kTile;
   const int ntiles = g.ntx * g.nty;
@@ -325,23 +330,23 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArra
     const long long w_own = phys(tbase + threadIdx.x);
     const long long w_bi = phys(tbase - (long long)nsteps * kTileThreads + 15 * kTileThreads + lj * kTile + 15);
     const long long w_bj = phys(tbase - (long long)g.ntx * nsteps * kTileThreads + 15 * kTileThreads + 15 * kTile + li);
-    const double* p_y = in + w_own;
-    const double* p_a1 = (UP ? b.Ui : b.Lk) + w_own;
-    const double* p_a2 = (UP ? b.Uj : b.Lj) + w_own;
-    const double* p_a3 = (UP ? b.Uk : b.Li) + w_own;
-    const double* p_piv = b.P + w_own;
-    double* p_in = in + w_own;
-    double* p_out = wave + w_own;
-    const double* p_bi = wave + (bnd_i ? w_bi : w_own);
-    const double* p_bj = wave + (bnd_j ? w_bj : w_own);
+    const T* p_y = in + w_own;
+    const T* p_a1 = (UP ? b.Ui : b.Lk) + w_own;
+    const T* p_a2 = (UP ? b.Uj : b.Lj) + w_own;
+    const T* p_a3 = (UP ? b.Uk : b.Li) + w_own;
+    const T* p_piv = b.P + w_own;
+    T* p_in = in + w_own;
+    T* p_out = wave + w_own;
+    const T* p_bi = wave + (bnd_i ? w_bi : w_own);
+    const T* p_bj = wave + (bnd_j ? w_bj : w_own);
 
     // Loads of step s (offset o = s * kStep from the step-0 pointers).
-    auto load_b = [&](int s, long long o, PreW& p) {
+    auto load_b = [&](int s, long long o, PreW<T>& p) {
       if (s < s_lo || s >= s_hi) return;
       if (bnd_j) p.bj = ld_relaxed(p_bj + o);
       if (bnd_i) p.bi = ld_relaxed(p_bi + o);
     };
-    auto load = [&](int s, long long o, PreW& p) {
+    auto load = [&](int s, long long o, PreW<T>& p) {
       if (s < s_lo || s >= s_hi) return;
       // Read-only path: none of these is written during the walk except
       // in[] by the U walk, after its one read here.
@@ -352,31 +357,31 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArra
       if (UP) p.piv = __ldg(p_piv + o);
     };
 
-    PreW pre[kPre];
+    PreW<T> pre[kPre];
 #pragma unroll
     for (int u = 0; u < kPre; ++u) {
-      pre[u] = PreW{0, 0, 0, 0, 0, 0, 0};
+      pre[u] = PreW<T>{0, 0, 0, 0, 0, 0, 0};
       load(u, u * kStep, pre[u]);
       if (u < kPreB) load_b(u, u * kStep, pre[u]);
     }
-    double own = 0.0;
+    T own = 0;
     for (int s0 = 0; s0 < nsteps; s0 += kPre) {  // nsteps is a multiple of kPre
       const long long o0 = (long long)s0 * kStep;
 #pragma unroll
       for (int u = 0; u < kPre; ++u) {
         const int s = s0 + u;
         const long long o = o0 + u * kStep;
-        const PreW c = pre[u];
+        const PreW<T> c = pre[u];
         load(s + kPre, o + kPre * kStep, pre[u]);
         load_b(s + kPreB, o + kPreB * kStep, pre[(u + kPreB) % kPre]);
-        double val = 0.0;
+        T val = 0;
         if (s >= s_lo && s < s_hi) {
-          const double* prev = &s_val[(s + 1) & 1][0][0];
-          double vi = 0.0, vj = 0.0;
+          const T* prev = &s_val[(s + 1) & 1][0][0];
+          T vi = 0, vj = 0;
           if (has_j) vj = lj > 0 ? prev[(lj - 1) * (kTile + 1) + li] : is_sentinel(c.bj) ? wait_value(p_bj + o, err) : c.bj;
           if (has_i) vi = li > 0 ? prev[lj * (kTile + 1) + li - 1] : is_sentinel(c.bi) ? wait_value(p_bi + o, err) : c.bi;
           const bool has_k = s > s_lo;
-          double acc = c.y;
+          T acc = c.y;
           if (!UP) {  // columns ascending: -k, -j, -i
             if (has_k) acc = mul_sub_rn(c.a1, own, acc);
             if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
@@ -386,7 +391,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArra
             if (has_i) acc = mul_sub_rn(c.a1, vi, acc);
             if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
             if (has_k) acc = mul_sub_rn(c.a3, own, acc);
-            p_in[o] = sentinel_value();  // the L walk's output, ready for the next application
+            p_in[o] = sentinel_of<T>();  // the L walk's output, ready for the next application
             val = acc / c.piv;
           }
           st_relaxed(p_out + o, not_sentinel(val));
@@ -431,14 +436,19 @@ Bands bands_of(double* p, int n) {
   return Bands{p, p + m, p + 2 * m, p + 3 * m, p + 4 * m, p + 5 * m, p + 6 * m, p + 7 * m};
 }
 
-// d_walk: Lk Lj Li Ui Uj Uk P | y | L-walk output | U-walk output
+// d_walk (and d_walk32): Lk Lj Li Ui Uj Uk P | y | L-walk output | U-walk output
 enum { kWalkBands = 7, kWalkY = 7, kWalkL = 8, kWalkU = 9, kWalkArrays = 10 };
 
-double* walk_array(const Ilu0Data& d, int a) { return d.d_walk + (size_t)a * (size_t)d.walk_n; }
+template <class T>
+T* walk_array(T* base, const Ilu0Data& d, int a) {
+  return base + (size_t)a * (size_t)d.walk_n;
+}
 
-WalkArrays walk_bands(const Ilu0Data& d) {
-  return WalkArrays{walk_array(d, 0), walk_array(d, 1), walk_array(d, 2), walk_array(d, 3),
-                    walk_array(d, 4), walk_array(d, 5), walk_array(d, 6)};
+template <class T>
+WalkArrays<T> walk_bands(T* base, const Ilu0Data& d) {
+  return WalkArrays<T>{walk_array(base, d, 0), walk_array(base, d, 1), walk_array(base, d, 2),
+                       walk_array(base, d, 3), walk_array(base, d, 4), walk_array(base, d, 5),
+                       walk_array(base, d, 6)};
 }
 
 int wave_grid(ab2_context* ctx, int ntiles) { return std::max(1, std::min(ntiles, ctx->num_sms * 2)); }
@@ -500,11 +510,12 @@ bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d) {
   d.d_walk = dev_alloc<double>(ctx, (size_t)kWalkArrays * (size_t)w.nw);
   const double* nat[kWalkBands] = {b.Lk, b.Lj, b.Li, b.Ui, b.Uj, b.Uk, b.P};
   for (int a = 0; a < kWalkBands; ++a) {
-    k_walk_gather<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, nat[a], walk_array(d, a));
+    k_walk_gather<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, nat[a], walk_array(d.d_walk, d, a));
     check_launch(ctx, "walk_gather");
   }
-  AB2_CUDA(cudaMemsetAsync(walk_array(d, kWalkY), 0, sizeof(double) * (size_t)w.nw, ctx->stream));
-  k_fill_bits<<<bulk_grid(ctx, 2 * w.nw), kThreads, 0, ctx->stream>>>(2 * w.nw, kSentinel, walk_array(d, kWalkL));
+  AB2_CUDA(cudaMemsetAsync(walk_array(d.d_walk, d, kWalkY), 0, sizeof(double) * (size_t)w.nw, ctx->stream));
+  k_fill_bits<<<bulk_grid(ctx, 2 * w.nw), kThreads, 0, ctx->stream>>>(2 * w.nw, kSentinel,
+                                                                      walk_array(d.d_walk, d, kWalkL));
   check_launch(ctx, "walk_fill");
   AB2_CUDA(cudaStreamSynchronize(ctx->stream));
   dev_free(ctx, d.d_bands);
@@ -514,32 +525,66 @@ bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d) {
   return true;
 }
 
-// y -> walk order -> L walk -> U walk (reversed index) -> z.
-void ilu_stencil_apply(ab2_context* ctx, const ab2_matrix* A, const Ilu0Data& d, const double* y, double* z) {
-  (void)A;
+namespace {
+
+template <class T>
+void walk_apply(ab2_context* ctx, const Ilu0Data& d, T* base, const T* y, T* z) {
   const Walk w = walk_of(d);
-  const WalkArrays b = walk_bands(d);
+  const WalkArrays<T> b = walk_bands(base, d);
   const int tiles = w.ntx * w.nty;
-  double* yw = walk_array(d, kWalkY);
-  double* lw = walk_array(d, kWalkL);
-  double* uw = walk_array(d, kWalkU);
+  T* yw = walk_array(base, d, kWalkY);
+  T* lw = walk_array(base, d, kWalkL);
+  T* uw = walk_array(base, d, kWalkU);
   k_walk_gather<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, y, yw);
   check_launch(ctx, "walk_gather");
-  k_walk_sweep<false><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, yw, lw, d.d_tile_tickets, d.d_err);
+  k_walk_sweep<false, T><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, yw, lw, d.d_tile_tickets,
+                                                                                d.d_err);
   check_launch(ctx, "walk_lsweep");
-  k_walk_sweep<true><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, lw, uw, d.d_tile_tickets, d.d_err);
+  k_walk_sweep<true, T><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, lw, uw, d.d_tile_tickets,
+                                                                               d.d_err);
   check_launch(ctx, "walk_usweep");
   k_walk_scatter<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, uw, z);
   check_launch(ctx, "walk_scatter");
 }
 
-// After a failed application: both propagation arrays back to the sentinel
+}  // namespace
+
+// y -> walk order -> L walk -> U walk (reversed index) -> z.
+void ilu_stencil_apply(ab2_context* ctx, const ab2_matrix* A, const Ilu0Data& d, const double* y, double* z) {
+  (void)A;
+  walk_apply(ctx, d, d.d_walk, y, z);
+}
+
+// FP32 walk arrays: the FP64 factor's bands rounded to float.
+void ilu_stencil_enable_f32(ab2_context* ctx, Ilu0Data& d) {
+  if (d.d_walk32) return;
+  const Walk w = walk_of(d);
+  d.d_walk32 = dev_alloc<float>(ctx, (size_t)kWalkArrays * (size_t)w.nw);
+  op_to_f32(ctx, kWalkBands * w.nw, d.d_walk, d.d_walk32);
+  AB2_CUDA(cudaMemsetAsync(walk_array(d.d_walk32, d, kWalkY), 0, sizeof(float) * (size_t)w.nw, ctx->stream));
+  k_fill_bits32<<<bulk_grid(ctx, 2 * w.nw), kThreads, 0, ctx->stream>>>(2 * w.nw, kSentinel32,
+                                                                        walk_array(d.d_walk32, d, kWalkL));
+  check_launch(ctx, "walk_fill32");
+}
+
+void ilu_stencil_apply_f32(ab2_context* ctx, const Ilu0Data& d, const float* y, float* z) {
+  require(d.d_walk32 != nullptr, "FP32 ILU0 arrays not built");
+  walk_apply(ctx, d, d.d_walk32, y, z);
+}
+
+// After a failed application: the propagation arrays back to the sentinel
 // (the tickets are reset by pc_reset).
 void ilu_stencil_reset(ab2_context* ctx, const Ilu0Data& d) {
-  if (!d.d_walk) return;
-  k_fill_bits<<<bulk_grid(ctx, 2 * d.walk_n), kThreads, 0, ctx->stream>>>(2 * d.walk_n, kSentinel,
-                                                                          walk_array(d, kWalkL));
-  check_launch(ctx, "walk_fill");
+  if (d.d_walk) {
+    k_fill_bits<<<bulk_grid(ctx, 2 * d.walk_n), kThreads, 0, ctx->stream>>>(2 * d.walk_n, kSentinel,
+                                                                            walk_array(d.d_walk, d, kWalkL));
+    check_launch(ctx, "walk_fill");
+  }
+  if (d.d_walk32) {
+    k_fill_bits32<<<bulk_grid(ctx, 2 * d.walk_n), kThreads, 0, ctx->stream>>>(2 * d.walk_n, kSentinel32,
+                                                                              walk_array(d.d_walk32, d, kWalkL));
+    check_launch(ctx, "walk_fill32");
+  }
 }
 
 }  // namespace ab2

@@ -19,6 +19,11 @@
 // itself is a CUDA graph: a conditional WHILE node whose body holds one
 // iteration's kernels; the control kernel clears the condition when the solve
 // is over.  (use_graph = 0 runs the same kernels from a host loop instead.)
+//
+// The engine (Krylov<T>) is templated on the value type: T = double is the
+// drop-in solver; T = float is the inner solver of the mixed-precision
+// refinement (mixed.cu), with FP32 values, FP32 accumulation in every dot and
+// FP32 scalars.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,39 +31,26 @@
 #include <cstring>
 
 #include "ab2_internal.cuh"
+#include "krylov.cuh"
 #include "precond.cuh"
 #include "reduce.cuh"
 #include "spmv_view.cuh"
 
 namespace ab2 {
 
-// Device-resident solver state (one per solver object).
-struct SolveState {
-  double nrm2_b, crit;
-  double rr;      // last value the stop test compared
-  double rho, rho1, den, alpha, beta, omega;
-  double rr_r;    // BiCGStab: r.r of the current r (the beta==0 branch of the first step tests r)
-  double* x;
-  const double* b;
-  double* hist;
-  int hist_cap, hist_len;
-  int iter, max_iter;
-  int first, done, converged, error, breakdown;
-  int exit_fixup;  // BiCGStab exits on ||s||: x += alpha phat still to do
-  int bodies;      // loop bodies executed (for launch accounting)
-};
-
 namespace {
 
 constexpr int kCtlThreads = 256;
 
-__device__ __forceinline__ void record(SolveState* st, double v) {
+template <class T>
+__device__ __forceinline__ void record(SolveStateT<T>* st, T v) {
   if (st->hist_len < st->hist_cap) st->hist[st->hist_len] = v;
   st->hist_len += 1;
 }
 
 // Iteration::stop(r) with the dot product already computed.
-__device__ __forceinline__ bool stop_test(SolveState* st, double dot_rr) {
+template <class T>
+__device__ __forceinline__ bool stop_test(SolveStateT<T>* st, T dot_rr) {
   if (st->iter >= st->max_iter) return true;
   st->rr = dot_rr;
   record(st, dot_rr);
@@ -71,10 +63,30 @@ __device__ __forceinline__ void set_loop(cudaGraphConditionalHandle h, int use_g
 }
 
 static_assert(kCtlThreads == kThreads, "fused reductions use the standalone reduction tree");
-int fused_grid(ab2_context* ctx, int n) { return red_grid(ctx, n); }
 
-__global__ void k_state_init(SolveState* st, double tol, int max_iter, double* x, const double* b, double* hist,
-                             int hist_cap) {
+// A reduction slot's buffers seen as T (FP32 partials fit the FP64 slots).
+template <class T>
+struct Red {
+  T* partials;
+  unsigned int* counter;
+  T* result;
+};
+template <class T>
+Red<T> red_of(ab2_context* ctx, int slot) {
+  RedSlot s = red_slot(ctx, slot);
+  return Red<T>{reinterpret_cast<T*>(s.partials), s.counter, reinterpret_cast<T*>(s.result)};
+}
+
+// b.b into st->nrm2_b: the same tree as op_dot.
+template <class T>
+__global__ void __launch_bounds__(kCtlThreads) k_bb(int n, const T* __restrict__ b, SolveStateT<T>* st, Red<T> red) {
+  T acc[1] = {T(0)};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] = fma_rn(b[i], b[i], acc[0]);
+  if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) st->nrm2_b = red.result[0];
+}
+
+template <class T>
+__global__ void k_state_init(SolveStateT<T>* st, T tol, int max_iter, T* x, const T* b, T* hist, int hist_cap) {
   st->crit = tol * tol * st->nrm2_b;
   st->rr = st->crit + 1;
   st->x = x;
@@ -96,19 +108,18 @@ __global__ void k_state_init(SolveState* st, double tol, int max_iter, double* x
 
 // r = b - A x (copy b, mult A x, axpy -1).  With r0 != nullptr (BiCGStab):
 // also r0 = r and rho1 = r.r0.
-template <class View>
-__global__ void __launch_bounds__(kCtlThreads) k_residual(int n, View A, SolveState* st, double* r, double* r0,
-                                                          RedSlot red) {
-  const double* x = st->x;
-  const double* b = st->b;
-  double acc[1] = {0.0};
+template <class View, class T>
+__global__ void __launch_bounds__(kCtlThreads) k_residual(int n, View A, SolveStateT<T>* st, T* r, T* r0, Red<T> red) {
+  const T* x = st->x;
+  const T* b = st->b;
+  T acc[1] = {T(0)};
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-    const double ax = A.row(row, x);
-    const double rv = fma(-1.0, ax, b[row]);
+    const T ax = A.row(row, x);
+    const T rv = fma_rn(T(-1), ax, b[row]);
     r[row] = rv;
     if (r0) {
       r0[row] = rv;
-      acc[0] = fma(rv, rv, acc[0]);
+      acc[0] = fma_rn(rv, rv, acc[0]);
     }
   }
   if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) {
@@ -118,62 +129,64 @@ __global__ void __launch_bounds__(kCtlThreads) k_residual(int n, View A, SolveSt
 
 // ------------------------------------------------------------------ CG
 // rho1 = r.z ; beta = rho1/rho (CG.h:117-118, the code names it alpha)
-__global__ void __launch_bounds__(kCtlThreads) k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z,
-                                                       SolveState* st, RedSlot red) {
-  double acc[1] = {0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] = fma(r[i], z[i], acc[0]);
+template <class T>
+__global__ void __launch_bounds__(kCtlThreads) k_cg_rz(int n, const T* __restrict__ r, const T* __restrict__ z,
+                                                       SolveStateT<T>* st, Red<T> red) {
+  T acc[1] = {T(0)};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] = fma_rn(r[i], z[i], acc[0]);
   if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) {
     st->rho1 = red.result[0];
-    st->beta = st->first ? 0.0 : st->rho1 / st->rho;
+    st->beta = st->first ? T(0) : st->rho1 / st->rho;
   }
 }
 
 // p = z (first step, CG.h:89) or z += beta p ; p = z (CG.h:119-120)
-__global__ void k_cg_p(int n, const double* __restrict__ z, double* __restrict__ p, const SolveState* st) {
-  const double beta = st->beta;
+template <class T>
+__global__ void k_cg_p(int n, const T* __restrict__ z, T* __restrict__ p, const SolveStateT<T>* st) {
+  const T beta = st->beta;
   const int first = st->first;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    p[i] = first ? z[i] : fma(beta, p[i], z[i]);
+    p[i] = first ? z[i] : fma_rn(beta, p[i], z[i]);
 }
 
 // q = A p ; den = q.p
-template <class View>
-__global__ void __launch_bounds__(kCtlThreads) k_cg_spmv(int n, View A, const double* __restrict__ p,
-                                                         double* __restrict__ q, SolveState* st, RedSlot red) {
-  double acc[1] = {0.0};
+template <class View, class T>
+__global__ void __launch_bounds__(kCtlThreads) k_cg_spmv(int n, View A, const T* __restrict__ p, T* __restrict__ q,
+                                                         SolveStateT<T>* st, Red<T> red) {
+  T acc[1] = {T(0)};
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-    const double qv = A.row(row, p);
+    const T qv = A.row(row, p);
     q[row] = qv;
-    acc[0] = fma(qv, p[row], acc[0]);
+    acc[0] = fma_rn(qv, p[row], acc[0]);
   }
   if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) st->den = red.result[0];
 }
 
 // alpha = rho1/den ; x += alpha p ; r -= alpha q ; then the loop's stop test on r.
-__global__ void __launch_bounds__(kCtlThreads) k_cg_update(int n, const double* __restrict__ p,
-                                                           const double* __restrict__ q, double* __restrict__ r,
-                                                           SolveState* st, RedSlot red, cudaGraphConditionalHandle h,
-                                                           int use_graph) {
+template <class T>
+__global__ void __launch_bounds__(kCtlThreads) k_cg_update(int n, const T* __restrict__ p, const T* __restrict__ q,
+                                                           T* __restrict__ r, SolveStateT<T>* st, Red<T> red,
+                                                           cudaGraphConditionalHandle h, int use_graph) {
   if (st->done) {
     if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(h, use_graph, 0);
     return;
   }
-  const double den = st->den;
-  const bool ok = den != 0;
-  const double alpha = ok ? st->rho1 / den : 0.0;
-  double* x = st->x;
-  double acc[1] = {0.0};
+  const T den = st->den;
+  const bool ok = den != T(0);
+  const T alpha = ok ? st->rho1 / den : T(0);
+  T* x = st->x;
+  T acc[1] = {T(0)};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double rv = r[i];
+    T rv = r[i];
     if (ok) {
-      x[i] = fma(alpha, p[i], x[i]);
-      rv = fma(-alpha, q[i], rv);
+      x[i] = fma_rn(alpha, p[i], x[i]);
+      rv = fma_rn(-alpha, q[i], rv);
       r[i] = rv;
     }
-    acc[0] = fma(rv, rv, acc[0]);
+    acc[0] = fma_rn(rv, rv, acc[0]);
   }
   if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) {
-    const double rr = red.result[0];
+    const T rr = red.result[0];
     st->bodies += 1;
     if (!ok) {
       // CG.h:96-104 / 131-139: converged after all, or breakdown "alpha"
@@ -196,30 +209,31 @@ __global__ void __launch_bounds__(kCtlThreads) k_cg_update(int n, const double* 
 
 // ------------------------------------------------------------------ BiCGStab
 // p = r (first) or p = r + beta (p - omega v)  (BiCGStab.h:273-276, three BLAS-1 calls)
-__global__ void k_bicg_p(int n, const double* __restrict__ r, const double* __restrict__ v, double* __restrict__ p,
-                         const SolveState* st) {
+template <class T>
+__global__ void k_bicg_p(int n, const T* __restrict__ r, const T* __restrict__ v, T* __restrict__ p,
+                         const SolveStateT<T>* st) {
   const int first = st->first;
-  const double beta = st->beta, omega = st->omega;
+  const T beta = st->beta, omega = st->omega;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (first) p[i] = r[i];
-    else p[i] = __dadd_rn(r[i], __dmul_rn(beta, fma(-omega, v[i], p[i])));
+    else p[i] = add_rn(r[i], mul_rn(beta, fma_rn(-omega, v[i], p[i])));
   }
 }
 
 // v = A phat ; alpha = rho1 / (v.r0), breakdown "alpha" on zero
-template <class View>
-__global__ void __launch_bounds__(kCtlThreads) k_bicg_v(int n, View A, const double* __restrict__ phat,
-                                                        const double* __restrict__ r0, double* __restrict__ v,
-                                                        SolveState* st, RedSlot red) {
-  double acc[1] = {0.0};
+template <class View, class T>
+__global__ void __launch_bounds__(kCtlThreads) k_bicg_v(int n, View A, const T* __restrict__ phat,
+                                                        const T* __restrict__ r0, T* __restrict__ v, SolveStateT<T>* st,
+                                                        Red<T> red) {
+  T acc[1] = {T(0)};
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-    const double vv = A.row(row, phat);
+    const T vv = A.row(row, phat);
     v[row] = vv;
-    acc[0] = fma(vv, r0[row], acc[0]);
+    acc[0] = fma_rn(vv, r0[row], acc[0]);
   }
   if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) {
-    const double d = red.result[0];
-    if (d == 0) {
+    const T d = red.result[0];
+    if (d == T(0)) {
       st->error = AB2_ERR_BREAKDOWN;
       st->breakdown = AB2_BREAKDOWN_ALPHA;
       st->done = 1;
@@ -230,18 +244,19 @@ __global__ void __launch_bounds__(kCtlThreads) k_bicg_v(int n, View A, const dou
 }
 
 // s = r - alpha v ; stop test on s (exit with x += alpha phat) ; also r.r for the first step
-__global__ void __launch_bounds__(kCtlThreads) k_bicg_s(int n, const double* __restrict__ r, const double* __restrict__ v,
-                                                        double* __restrict__ s, SolveState* st, RedSlot red) {
+template <class T>
+__global__ void __launch_bounds__(kCtlThreads) k_bicg_s(int n, const T* __restrict__ r, const T* __restrict__ v,
+                                                        T* __restrict__ s, SolveStateT<T>* st, Red<T> red) {
   const bool live = !st->done;
-  const double alpha = st->alpha;
-  double acc[2] = {0.0, 0.0};
+  const T alpha = st->alpha;
+  T acc[2] = {T(0), T(0)};
   if (live) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-      const double rv = r[i];
-      const double sv = fma(-alpha, v[i], rv);
+      const T rv = r[i];
+      const T sv = fma_rn(-alpha, v[i], rv);
       s[i] = sv;
-      acc[0] = fma(sv, sv, acc[0]);
-      acc[1] = fma(rv, rv, acc[1]);
+      acc[0] = fma_rn(sv, sv, acc[0]);
+      acc[1] = fma_rn(rv, rv, acc[1]);
     }
   }
   if (grid_reduce<2>(acc, red.partials, red.counter, red.result)) {
@@ -257,26 +272,26 @@ __global__ void __launch_bounds__(kCtlThreads) k_bicg_s(int n, const double* __r
 }
 
 // t = A shat ; omega = t.s / t.t, beta==0 handling (BiCGStab.h:202-216, 266-282)
-template <class View>
-__global__ void __launch_bounds__(kCtlThreads) k_bicg_t(int n, View A, const double* __restrict__ shat,
-                                                        const double* __restrict__ s, double* __restrict__ t,
-                                                        SolveState* st, RedSlot red) {
+template <class View, class T>
+__global__ void __launch_bounds__(kCtlThreads) k_bicg_t(int n, View A, const T* __restrict__ shat,
+                                                        const T* __restrict__ s, T* __restrict__ t, SolveStateT<T>* st,
+                                                        Red<T> red) {
   const bool live = !st->done;
-  double acc[2] = {0.0, 0.0};
+  T acc[2] = {T(0), T(0)};
   if (live) {
     for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-      const double tv = A.row(row, shat);
+      const T tv = A.row(row, shat);
       t[row] = tv;
-      acc[0] = fma(tv, s[row], acc[0]);
-      acc[1] = fma(tv, tv, acc[1]);
+      acc[0] = fma_rn(tv, s[row], acc[0]);
+      acc[1] = fma_rn(tv, tv, acc[1]);
     }
   }
   if (grid_reduce<2>(acc, red.partials, red.counter, red.result)) {
     if (live) {
-      const double ts = red.result[0], tt = red.result[1];
-      if (tt == 0) {
+      const T ts = red.result[0], tt = red.result[1];
+      if (tt == T(0)) {
         // first step: stop(r); later steps: stop(s) -- s.s is the value just tested
-        const double v = st->first ? st->rr_r : st->rr;
+        const T v = st->first ? st->rr_r : st->rr;
         if (stop_test(st, v)) {
           if (st->first) st->iter += 1;
           st->exit_fixup = 1;
@@ -294,29 +309,30 @@ __global__ void __launch_bounds__(kCtlThreads) k_bicg_t(int n, View A, const dou
 
 // x += omega shat ; x += alpha phat ; r = s - omega t ; loop stop test on r ;
 // rho1 = r.r0 ; beta = (rho1/rho)(alpha/omega) ; breakdown "rho" on rho == 0.
-__global__ void __launch_bounds__(kCtlThreads) k_bicg_update(int n, const double* __restrict__ shat,
-                                                             const double* __restrict__ phat, const double* __restrict__ s,
-                                                             const double* __restrict__ t, const double* __restrict__ r0,
-                                                             double* __restrict__ r, SolveState* st, RedSlot red,
-                                                             cudaGraphConditionalHandle h, int use_graph) {
-  double* x = st->x;
+template <class T>
+__global__ void __launch_bounds__(kCtlThreads) k_bicg_update(int n, const T* __restrict__ shat, const T* __restrict__ phat,
+                                                             const T* __restrict__ s, const T* __restrict__ t,
+                                                             const T* __restrict__ r0, T* __restrict__ r,
+                                                             SolveStateT<T>* st, Red<T> red, cudaGraphConditionalHandle h,
+                                                             int use_graph) {
+  T* x = st->x;
   const int done = st->done;
   const int fix = st->exit_fixup;
-  const double alpha = st->alpha, omega = st->omega;
-  double acc[2] = {0.0, 0.0};
+  const T alpha = st->alpha, omega = st->omega;
+  T acc[2] = {T(0), T(0)};
   if (done) {
     if (fix) {
       for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        x[i] = fma(alpha, phat[i], x[i]);
+        x[i] = fma_rn(alpha, phat[i], x[i]);
     }
   } else {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-      double xv = fma(omega, shat[i], x[i]);
-      x[i] = fma(alpha, phat[i], xv);
-      const double rv = fma(-omega, t[i], s[i]);
+      T xv = fma_rn(omega, shat[i], x[i]);
+      x[i] = fma_rn(alpha, phat[i], xv);
+      const T rv = fma_rn(-omega, t[i], s[i]);
       r[i] = rv;
-      acc[0] = fma(rv, rv, acc[0]);
-      acc[1] = fma(rv, r0[i], acc[1]);
+      acc[0] = fma_rn(rv, rv, acc[0]);
+      acc[1] = fma_rn(rv, r0[i], acc[1]);
     }
   }
   if (grid_reduce<2>(acc, red.partials, red.counter, red.result)) {
@@ -332,7 +348,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_bicg_update(int n, const double
       } else {
         st->rho1 = red.result[1];
         st->beta = (st->rho1 / st->rho) * (st->alpha / st->omega);
-        if (st->rho == 0) {
+        if (st->rho == T(0)) {
           st->error = AB2_ERR_BREAKDOWN;
           st->breakdown = AB2_BREAKDOWN_RHO;
           st->done = 1;
@@ -343,7 +359,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_bicg_update(int n, const double
   }
 }
 
-// True residual ||b - A x||^2 into out[0], b.b into out[1].
+// True residual ||b - A x||^2 into out[0], b.b into out[1] (FP64).
 template <class View>
 __global__ void __launch_bounds__(kCtlThreads) k_true_residual(int n, View A, const double* __restrict__ x,
                                                                const double* __restrict__ b, RedSlot red) {
@@ -358,6 +374,170 @@ __global__ void __launch_bounds__(kCtlThreads) k_true_residual(int n, View A, co
 
 }  // namespace
 
+namespace {
+
+template <class T>
+void pc_apply_t(ab2_context* ctx, const ab2_precond* pc, const T* x, T* y) {
+  if constexpr (sizeof(T) == sizeof(double)) pc_apply(ctx, pc, x, y);
+  else pc_apply_f32(ctx, pc, x, y);
+}
+
+}  // namespace
+
+// Enqueues one loop iteration.  Returns the number of kernels it launched.
+template <class T>
+int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
+  const int n = A->n;
+  const int g = red_grid(ctx, n);
+  const int ge = grid_for(n);
+  const long long before = ctx->launches;
+  SolveStateT<T>* st = d_st;
+  if (solver == AB2_SOLVER_CG) {
+    T *r = w[0], *z = w[1], *p = w[2], *q = w[3];
+    pc_apply_t(ctx, pc, r, z);
+    k_cg_rz<<<g, kCtlThreads, 0, ctx->stream>>>(n, r, z, st, red_of<T>(ctx, 1));
+    check_launch(ctx, "cg_rz");
+    k_cg_p<<<ge, kThreads, 0, ctx->stream>>>(n, z, p, st);
+    check_launch(ctx, "cg_p");
+    with_view<T>(A, variant, [&](auto view) {
+      k_cg_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red_of<T>(ctx, 2));
+    });
+    check_launch(ctx, "cg_spmv");
+    k_cg_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p, q, r, st, red_of<T>(ctx, 3), h, graph_loop);
+    check_launch(ctx, "cg_update");
+  } else {
+    T *r = w[0], *r0 = w[1], *p = w[2], *phat = w[3], *v = w[4], *s = w[5], *shat = w[6], *t = w[7];
+    k_bicg_p<<<ge, kThreads, 0, ctx->stream>>>(n, r, v, p, st);
+    check_launch(ctx, "bicg_p");
+    pc_apply_t(ctx, pc, p, phat);
+    with_view<T>(A, variant, [&](auto view) {
+      k_bicg_v<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, phat, r0, v, st, red_of<T>(ctx, 1));
+    });
+    check_launch(ctx, "bicg_v");
+    k_bicg_s<<<g, kCtlThreads, 0, ctx->stream>>>(n, r, v, s, st, red_of<T>(ctx, 2));
+    check_launch(ctx, "bicg_s");
+    pc_apply_t(ctx, pc, s, shat);
+    with_view<T>(A, variant, [&](auto view) {
+      k_bicg_t<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, shat, s, t, st, red_of<T>(ctx, 3));
+    });
+    check_launch(ctx, "bicg_t");
+    k_bicg_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, shat, phat, s, t, r0, r, st, red_of<T>(ctx, 4), h,
+                                                       graph_loop);
+    check_launch(ctx, "bicg_update");
+  }
+  return (int)(ctx->launches - before);
+}
+
+template <class T>
+void Krylov<T>::build_graph() {
+  AB2_CUDA(cudaGraphCreate(&graph, 0));
+  AB2_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  AB2_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  AB2_CUDA(cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  int launched = 0;
+  try {
+    launched = enqueue_body(handle, 1);
+  } catch (...) {
+    cudaGraph_t dummy;
+    cudaStreamEndCapture(ctx->stream, &dummy);
+    throw;
+  }
+  AB2_CUDA(cudaStreamEndCapture(ctx->stream, &body));
+  ctx->launches -= launched;  // captured, not launched
+  body_launches = launched;
+  AB2_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+}
+
+template <class T>
+void Krylov<T>::init(ab2_context* c, const ab2_matrix* a, const ab2_precond* p, int solver_kind, int spmv_variant,
+                     int graph_loop, int max_iter) {
+  ctx = c;
+  A = a;
+  pc = p;
+  solver = solver_kind;
+  variant = spmv_variant;
+  use_graph = graph_loop;
+  const int nw = solver == AB2_SOLVER_CG ? 4 : 8;
+  for (int i = 0; i < nw; ++i) {
+    w[i] = dev_alloc<T>(ctx, (size_t)A->n);
+    AB2_CUDA(cudaMemsetAsync(w[i], 0, sizeof(T) * (size_t)std::max(A->n, 1), ctx->stream));
+  }
+  d_st = dev_alloc<SolveStateT<T>>(ctx, 1);
+  AB2_CUDA(cudaMemsetAsync(d_st, 0, sizeof(SolveStateT<T>), ctx->stream));
+  AB2_CUDA(cudaMallocHost((void**)&h_st, sizeof(SolveStateT<T>)));
+  std::memset(h_st, 0, sizeof(SolveStateT<T>));
+  hist_cap = 2 * max_iter + 8;  // BiCGStab tests s and r each iteration
+  d_hist = dev_alloc<T>(ctx, (size_t)hist_cap);
+  if (use_graph) build_graph();
+}
+
+template <class T>
+void Krylov<T>::solve(const T* b, T* x, T tol, int max_iter) {
+  const int n = A->n;
+  const int g = red_grid(ctx, n);
+  // Iteration ctor: b.b and the criterion (Iteration.h:44-68)
+  k_bb<<<g, kCtlThreads, 0, ctx->stream>>>(n, b, d_st, red_of<T>(ctx, 0));
+  check_launch(ctx, "dot");
+  k_state_init<<<1, 1, 0, ctx->stream>>>(d_st, tol, max_iter, x, b, d_hist, hist_cap);
+  check_launch(ctx, "state_init");
+  // r = b - A x (and r0, rho1 for BiCGStab)
+  T* r0 = solver == AB2_SOLVER_BICGSTAB ? w[1] : nullptr;
+  with_view<T>(A, variant, [&](auto view) {
+    k_residual<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, d_st, w[0], r0, red_of<T>(ctx, 0));
+  });
+  check_launch(ctx, "residual");
+  // Null right-hand side: the reference returns before any iteration.
+  AB2_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(SolveStateT<T>), cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (!h_st->done) {
+    if (use_graph) {
+      AB2_CUDA(cudaGraphLaunch(exec, ctx->stream));
+    } else {
+      // Host-driven loop over the same kernels, checking the flag in batches.
+      for (;;) {
+        const int batch = 8;
+        for (int i = 0; i < batch; ++i) enqueue_body(0, 0);
+        AB2_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(SolveStateT<T>), cudaMemcpyDeviceToHost, ctx->stream));
+        AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (h_st->done) break;
+      }
+    }
+  }
+  AB2_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(SolveStateT<T>), cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (use_graph) ctx->launches += (long long)h_st->bodies * body_launches;
+}
+
+template <class T>
+void Krylov<T>::release() {
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  exec = nullptr;
+  graph = nullptr;
+  if (ctx) {
+    for (T*& p : w) {
+      dev_free(ctx, p);
+      p = nullptr;
+    }
+    dev_free(ctx, d_st);
+    dev_free(ctx, d_hist);
+  }
+  d_st = nullptr;
+  d_hist = nullptr;
+  if (h_st) cudaFreeHost(h_st);
+  h_st = nullptr;
+}
+
+template struct Krylov<double>;
+template struct Krylov<float>;
+
 }  // namespace ab2
 
 using namespace ab2;
@@ -367,98 +547,11 @@ struct ab2_solver {
   const ab2_matrix* A = nullptr;
   ab2_solver_options opts{};
   ab2_precond* pc = nullptr;
-  // CG: r z p q ; BiCGStab: r r0 p phat v s shat t
-  double* w[8] = {};
-  SolveState* d_st = nullptr;
-  SolveState* h_st = nullptr;
-  double* d_hist = nullptr;
-  int hist_cap = 0;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  cudaGraphConditionalHandle handle = 0;
-  int body_launches = 0;
+  Krylov<double> eng;
   double setup_ms = 0;
   double solve_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
-
-namespace ab2 {
-namespace {
-
-// Enqueues one loop iteration.  Returns the number of kernels it launched.
-int enqueue_body(ab2_solver* S, cudaGraphConditionalHandle h, int use_graph) {
-  ab2_context* ctx = S->ctx;
-  const ab2_matrix* A = S->A;
-  const int n = A->n;
-  const int g = fused_grid(ctx, n);
-  const int ge = grid_for(n);
-  const long long before = ctx->launches;
-  SolveState* st = S->d_st;
-  if (S->opts.solver == AB2_SOLVER_CG) {
-    double *r = S->w[0], *z = S->w[1], *p = S->w[2], *q = S->w[3];
-    pc_apply(ctx, S->pc, r, z);
-    k_cg_rz<<<g, kCtlThreads, 0, ctx->stream>>>(n, r, z, st, red_slot(ctx, 1));
-    check_launch(ctx, "cg_rz");
-    k_cg_p<<<ge, kThreads, 0, ctx->stream>>>(n, z, p, st);
-    check_launch(ctx, "cg_p");
-    with_view<double>(A, S->opts.spmv_variant, [&](auto view) {
-      k_cg_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red_slot(ctx, 2));
-    });
-    check_launch(ctx, "cg_spmv");
-    k_cg_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p, q, r, st, red_slot(ctx, 3), h, use_graph);
-    check_launch(ctx, "cg_update");
-  } else {
-    double *r = S->w[0], *r0 = S->w[1], *p = S->w[2], *phat = S->w[3], *v = S->w[4], *s = S->w[5], *shat = S->w[6],
-           *t = S->w[7];
-    k_bicg_p<<<ge, kThreads, 0, ctx->stream>>>(n, r, v, p, st);
-    check_launch(ctx, "bicg_p");
-    pc_apply(ctx, S->pc, p, phat);
-    with_view<double>(A, S->opts.spmv_variant, [&](auto view) {
-      k_bicg_v<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, phat, r0, v, st, red_slot(ctx, 1));
-    });
-    check_launch(ctx, "bicg_v");
-    k_bicg_s<<<g, kCtlThreads, 0, ctx->stream>>>(n, r, v, s, st, red_slot(ctx, 2));
-    check_launch(ctx, "bicg_s");
-    pc_apply(ctx, S->pc, s, shat);
-    with_view<double>(A, S->opts.spmv_variant, [&](auto view) {
-      k_bicg_t<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, shat, s, t, st, red_slot(ctx, 3));
-    });
-    check_launch(ctx, "bicg_t");
-    k_bicg_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, shat, phat, s, t, r0, r, st, red_slot(ctx, 4), h, use_graph);
-    check_launch(ctx, "bicg_update");
-  }
-  return (int)(ctx->launches - before);
-}
-
-void build_graph(ab2_solver* S) {
-  ab2_context* ctx = S->ctx;
-  AB2_CUDA(cudaGraphCreate(&S->graph, 0));
-  AB2_CUDA(cudaGraphConditionalHandleCreate(&S->handle, S->graph, 1, cudaGraphCondAssignDefault));
-  cudaGraphNodeParams cp = {};
-  cp.type = cudaGraphNodeTypeConditional;
-  cp.conditional.handle = S->handle;
-  cp.conditional.type = cudaGraphCondTypeWhile;
-  cp.conditional.size = 1;
-  cudaGraphNode_t node;
-  AB2_CUDA(cudaGraphAddNode(&node, S->graph, nullptr, 0, &cp));
-  cudaGraph_t body = cp.conditional.phGraph_out[0];
-  AB2_CUDA(cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  int launched = 0;
-  try {
-    launched = enqueue_body(S, S->handle, 1);
-  } catch (...) {
-    cudaGraph_t dummy;
-    cudaStreamEndCapture(ctx->stream, &dummy);
-    throw;
-  }
-  AB2_CUDA(cudaStreamEndCapture(ctx->stream, &body));
-  ctx->launches -= launched;  // captured, not launched
-  S->body_launches = launched;
-  AB2_CUDA(cudaGraphInstantiate(&S->exec, S->graph, 0));
-}
-
-}  // namespace
-}  // namespace ab2
 
 extern "C" {
 
@@ -501,17 +594,7 @@ int ab2_solver_create(ab2_context* ctx, const ab2_matrix* A, const ab2_solver_op
     int prc = ab2_precond_create(ctx, A, &po, &S->pc);
     if (prc != AB2_OK) throw Error{prc, ctx->last_error};
     S->pc->variant = o->spmv_variant;
-    const int nw = o->solver == AB2_SOLVER_CG ? 4 : 8;
-    for (int i = 0; i < nw; ++i) {
-      S->w[i] = dev_alloc<double>(ctx, (size_t)A->n);
-      AB2_CUDA(cudaMemsetAsync(S->w[i], 0, sizeof(double) * (size_t)std::max(A->n, 1), ctx->stream));
-    }
-    S->d_st = dev_alloc<SolveState>(ctx, 1);
-    AB2_CUDA(cudaMemsetAsync(S->d_st, 0, sizeof(SolveState), ctx->stream));
-    AB2_CUDA(cudaMallocHost((void**)&S->h_st, sizeof(SolveState)));
-    S->hist_cap = 2 * o->max_iter + 8;  // BiCGStab tests s and r each iteration
-    S->d_hist = dev_alloc<double>(ctx, (size_t)S->hist_cap);
-    if (o->use_graph) build_graph(S);
+    S->eng.init(ctx, A, S->pc, o->solver, o->spmv_variant, o->use_graph, o->max_iter);
     AB2_CUDA(cudaEventRecord(S->ev1, ctx->stream));
     AB2_CUDA(cudaEventSynchronize(S->ev1));
     float ms = 0;
@@ -534,42 +617,13 @@ int ab2_solver_solve(ab2_solver* S, const ab2_vector* b, ab2_vector* x, ab2_stat
     const int n = S->A->n;
     const ab2_solver_options& o = S->opts;
     AB2_CUDA(cudaEventRecord(S->ev0, ctx->stream));
-    // Iteration ctor: b.b and the criterion (Iteration.h:44-68)
-    op_dot(ctx, n, b->d, b->d, &S->d_st->nrm2_b, 0);
-    k_state_init<<<1, 1, 0, ctx->stream>>>(S->d_st, o.tol, o.max_iter, x->d, b->d, S->d_hist, S->hist_cap);
-    check_launch(ctx, "state_init");
-    const int g = fused_grid(ctx, n);
-    // r = b - A x (and r0, rho1 for BiCGStab)
-    double* r0 = o.solver == AB2_SOLVER_BICGSTAB ? S->w[1] : nullptr;
-    with_view<double>(S->A, o.spmv_variant, [&](auto view) {
-      k_residual<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, S->d_st, S->w[0], r0, red_slot(ctx, 0));
-    });
-    check_launch(ctx, "residual");
-    // Null right-hand side: the reference returns before any iteration.
-    AB2_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(SolveState), cudaMemcpyDeviceToHost, ctx->stream));
-    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (!S->h_st->done) {
-      if (o.use_graph) {
-        AB2_CUDA(cudaGraphLaunch(S->exec, ctx->stream));
-      } else {
-        // Host-driven loop over the same kernels, checking the flag in batches.
-        for (;;) {
-          const int batch = 8;
-          for (int i = 0; i < batch; ++i) enqueue_body(S, 0, 0);
-          AB2_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(SolveState), cudaMemcpyDeviceToHost, ctx->stream));
-          AB2_CUDA(cudaStreamSynchronize(ctx->stream));
-          if (S->h_st->done) break;
-        }
-      }
-    }
+    S->eng.solve(b->d, x->d, o.tol, o.max_iter);
     AB2_CUDA(cudaEventRecord(S->ev1, ctx->stream));
-    AB2_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(SolveState), cudaMemcpyDeviceToHost, ctx->stream));
-    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+    AB2_CUDA(cudaEventSynchronize(S->ev1));
     float ms = 0;
     AB2_CUDA(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
     S->solve_ms = ms;
-    const SolveState& st = *S->h_st;
-    if (o.use_graph) ctx->launches += (long long)st.bodies * S->body_launches;
+    const SolveState& st = *S->eng.h_st;
     int pe = pc_error(ctx, S->pc);
     status->succeeded = st.converged;
     status->iterations = st.iter;
@@ -583,7 +637,7 @@ int ab2_solver_solve(ab2_solver* S, const ab2_vector* b, ab2_vector* x, ab2_stat
     // ||b - A x|| / ||b|| (reported, not part of the timed solve)
     RedSlot red = red_slot(ctx, 5);
     with_view<double>(S->A, o.spmv_variant, [&](auto view) {
-      k_true_residual<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, x->d, b->d, red);
+      k_true_residual<<<red_grid(ctx, n), kCtlThreads, 0, ctx->stream>>>(n, view, x->d, b->d, red);
     });
     check_launch(ctx, "true_residual");
     AB2_CUDA(cudaMemcpyAsync(ctx->h_pinned, red.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -594,11 +648,12 @@ int ab2_solver_solve(ab2_solver* S, const ab2_vector* b, ab2_vector* x, ab2_stat
 
 int ab2_solver_history(const ab2_solver* S, double* hist, int cap, int* len) {
   if (!S || !len || (cap > 0 && !hist)) return AB2_ERR_BAD_ARG;
-  const int have = std::min(S->h_st ? S->h_st->hist_len : 0, S->hist_cap);
-  *len = S->h_st ? S->h_st->hist_len : 0;
+  const SolveState* st = S->eng.h_st;
+  const int have = std::min(st ? st->hist_len : 0, S->eng.hist_cap);
+  *len = st ? st->hist_len : 0;
   const int m = std::min(have, cap);
   if (m > 0) {
-    if (cudaMemcpy(hist, S->d_hist, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cudaMemcpy(hist, S->eng.d_hist, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost) != cudaSuccess)
       return AB2_ERR_CUDA;
   }
   return AB2_OK;
@@ -607,13 +662,8 @@ int ab2_solver_history(const ab2_solver* S, double* hist, int cap, int* len) {
 int ab2_solver_destroy(ab2_solver* S) {
   if (!S) return AB2_ERR_BAD_ARG;
   if (S->ctx) ctx_quiesce(S->ctx);
-  if (S->exec) cudaGraphExecDestroy(S->exec);
-  if (S->graph) cudaGraphDestroy(S->graph);
+  S->eng.release();
   if (S->pc) ab2_precond_destroy(S->pc);
-  for (double* p : S->w) dev_free(S->ctx, p);
-  dev_free(S->ctx, S->d_st);
-  dev_free(S->ctx, S->d_hist);
-  if (S->h_st) cudaFreeHost(S->h_st);
   if (S->ev0) cudaEventDestroy(S->ev0);
   if (S->ev1) cudaEventDestroy(S->ev1);
   if (S->ctx) ctx_release(S->ctx);

@@ -1,0 +1,66 @@
+// krylov.cuh -- the device-resident Krylov engine shared by the FP64 solver
+// (krylov.cu) and the FP32 inner solves of the mixed-precision solver (mixed.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ab2_internal.cuh"
+
+struct ab2_precond;
+
+namespace ab2 {
+
+// Device-resident solver state (one per engine).
+template <class T>
+struct SolveStateT {
+  T nrm2_b, crit;
+  T rr;      // last value the stop test compared
+  T rho, rho1, den, alpha, beta, omega;
+  T rr_r;    // BiCGStab: r.r of the current r (the beta==0 branch of the first step tests r)
+  T* x;
+  const T* b;
+  T* hist;
+  int hist_cap, hist_len;
+  int iter, max_iter;
+  int first, done, converged, error, breakdown;
+  int exit_fixup;  // BiCGStab exits on ||s||: x += alpha phat still to do
+  int bodies;      // loop bodies executed (for launch accounting)
+};
+
+using SolveState = SolveStateT<double>;
+
+// One CG or BiCGStab engine over value type T (double or float): work
+// vectors, state, stop-test history and the loop graph, reused by every solve.
+template <class T>
+struct Krylov {
+  ab2_context* ctx = nullptr;
+  const ab2_matrix* A = nullptr;
+  const ab2_precond* pc = nullptr;  // applied in T
+  int solver = AB2_SOLVER_CG;
+  int variant = AB2_SPMV_AUTO;
+  int use_graph = 1;
+  T* w[8] = {};  // CG: r z p q ; BiCGStab: r r0 p phat v s shat t
+  SolveStateT<T>* d_st = nullptr;
+  SolveStateT<T>* h_st = nullptr;  // pinned copy, valid after solve()
+  T* d_hist = nullptr;
+  int hist_cap = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphConditionalHandle handle = 0;
+  int body_launches = 0;
+
+  // Allocates the work vectors (max_iter sizes the history) and builds the graph.
+  void init(ab2_context* c, const ab2_matrix* a, const ab2_precond* p, int solver_kind, int spmv_variant, int graph_loop,
+            int max_iter);
+  // Solves A x = b from the x given, to r.r < tol^2 b.b or max_iter
+  // iterations (max_iter <= the init value).  Synchronises; h_st holds the
+  // final state and ctx->launches counts every kernel.
+  void solve(const T* b, T* x, T tol, int max_iter);
+  void release();
+
+ private:
+  int enqueue_body(cudaGraphConditionalHandle h, int graph_loop);
+  void build_graph();
+};
+
+}  // namespace ab2

@@ -45,19 +45,20 @@ namespace {
 // be produced.  Up to 8 dependencies are loaded at once, so a row whose inputs
 // are ready costs one round trip to L2 instead of one per dependency; only the
 // values still at the sentinel are polled again.
-__device__ __forceinline__ double sweep_row(double acc, int kb, int ke, const int* __restrict__ ci,
-                                            const double* __restrict__ lu, const double* x, int* err) {
+template <class T>
+__device__ __forceinline__ T sweep_row(T acc, int kb, int ke, const int* __restrict__ ci, const T* __restrict__ lu,
+                                       const T* x, int* err) {
   for (int k0 = kb; k0 < ke; k0 += 8) {
-    double a[8], v[8];
+    T a[8], v[8];
     int c[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const bool in = k0 + u < ke;
       c[u] = in ? ci[k0 + u] : 0;
-      a[u] = in ? lu[k0 + u] : 0.0;
+      a[u] = in ? lu[k0 + u] : T(0);
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u) v[u] = k0 + u < ke ? ld_relaxed(x + c[u]) : 0.0;
+    for (int u = 0; u < 8; ++u) v[u] = k0 + u < ke ? ld_relaxed(x + c[u]) : T(0);
 #pragma unroll
     for (int u = 0; u < 8; ++u)
       if (k0 + u < ke && is_sentinel(v[u])) v[u] = wait_value(x + c[u], err);
@@ -99,9 +100,10 @@ __global__ void k_ilu_factor_level(const int* __restrict__ rows, int count, cons
 // Forward sweep x_i = y_i - sum_{k<dcol} l_ik x_k (solveL, ILU0Preconditioner.h:181-198).
 // Also leaves z at the sentinel for the backward sweep (after y_i was read, so
 // y and z may be the same vector).
+template <class T>
 __global__ void __launch_bounds__(256) k_ilu_lsweep(int len, const int* __restrict__ perm, const int* __restrict__ rp,
                                                     const int* __restrict__ ci, const int* __restrict__ dcol,
-                                                    const double* __restrict__ lu, const double* y, double* t, double* z,
+                                                    const T* __restrict__ lu, const T* y, T* t, T* z,
                                                     unsigned int* tickets, int* err) {
   const int lane = threadIdx.x & 31;
   const int nchunks = len >> 5;
@@ -112,8 +114,8 @@ __global__ void __launch_bounds__(256) k_ilu_lsweep(int len, const int* __restri
     if (chunk >= nchunks) break;
     const int row = perm[chunk * 32 + lane];
     if (row >= 0) {
-      const double acc = sweep_row(y[row], rp[row], dcol[row], ci, lu, t, err);
-      z[row] = __longlong_as_double((long long)kSentinel);
+      const T acc = sweep_row(y[row], rp[row], dcol[row], ci, lu, t, err);
+      z[row] = sentinel_of<T>();
       st_relaxed(t + row, not_sentinel(acc));
     }
   }
@@ -123,9 +125,10 @@ __global__ void __launch_bounds__(256) k_ilu_lsweep(int len, const int* __restri
 
 // Backward sweep x_i = (y_i - sum_{k>dcol} u_ik x_k) / u_ii (solveU, :200-231).
 // Puts t back to the sentinel for the next forward sweep.
+template <class T>
 __global__ void __launch_bounds__(256) k_ilu_usweep(int len, const int* __restrict__ perm, const int* __restrict__ rp,
                                                     const int* __restrict__ ci, const int* __restrict__ dcol,
-                                                    const double* __restrict__ lu, double* t, double* z,
+                                                    const T* __restrict__ lu, T* t, T* z,
                                                     unsigned int* tickets, int* err) {
   const int lane = threadIdx.x & 31;
   const int nchunks = len >> 5;
@@ -138,9 +141,9 @@ __global__ void __launch_bounds__(256) k_ilu_usweep(int len, const int* __restri
     if (row >= 0) {
       const int dk = dcol[row];
       const int e = rp[row + 1];
-      const double acc = sweep_row(t[row], dk + 1, e, ci, lu, z, err);
-      const double piv = dk < e ? lu[dk] : 0.0;
-      t[row] = __longlong_as_double((long long)kSentinel);
+      const T acc = sweep_row(t[row], dk + 1, e, ci, lu, z, err);
+      const T piv = dk < e ? lu[dk] : T(0);
+      t[row] = sentinel_of<T>();
       st_relaxed(z + row, not_sentinel(acc / piv));
     }
   }
@@ -149,28 +152,28 @@ __global__ void __launch_bounds__(256) k_ilu_usweep(int len, const int* __restri
 
 // Chebyshev step (ChebyshevPreconditioner.h:392-434 with y_cur the iterate):
 //   r = x - A y_cur ; z = D^-1 r ; p = first ? z : beta*p + z ; y_next = y_cur + a p
-template <class View>
-__global__ void __launch_bounds__(kThreads) k_cheb_step(int n, View A, const double* __restrict__ x,
-                                                        const double* __restrict__ ycur, const double* __restrict__ inv,
-                                                        double* __restrict__ p, double* __restrict__ ynext, double a,
-                                                        double bcoef, int first) {
+template <class View, class T>
+__global__ void __launch_bounds__(kThreads) k_cheb_step(int n, View A, const T* __restrict__ x, const T* __restrict__ ycur,
+                                                        const T* __restrict__ inv, T* __restrict__ p,
+                                                        T* __restrict__ ynext, T a, T bcoef, int first) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= n) return;
-  const double ay = A.row(row, ycur);
-  const double r = fma(-1.0, ay, x[row]);
-  const double z = __dmul_rn(inv[row], r);
-  const double pn = first ? z : __dadd_rn(__dmul_rn(bcoef, p[row]), z);
+  const T ay = A.row(row, ycur);
+  const T r = fma_rn(T(-1), ay, x[row]);
+  const T z = mul_rn(inv[row], r);
+  const T pn = first ? z : add_rn(mul_rn(bcoef, p[row]), z);
   p[row] = pn;
-  ynext[row] = fma(a, pn, ycur[row]);
+  ynext[row] = fma_rn(a, pn, ycur[row]);
 }
 
 // _algo1 start (ChebyshevPreconditioner.h:329-336): r = D^-1 x ; w = r / theta ; y = w.
 // x and y may be the same vector (x_i is read before y_i is written).
-__global__ void k_cheb1_start(int n, const double* x, const double* __restrict__ inv, double inv_theta,
-                              double* __restrict__ r, double* __restrict__ w, double* y) {
+template <class T>
+__global__ void k_cheb1_start(int n, const T* x, const T* __restrict__ inv, T inv_theta, T* __restrict__ r,
+                              T* __restrict__ w, T* y) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double rv = inv[i] * x[i];
-    const double wv = inv_theta * rv;
+    const T rv = mul_rn(inv[i], x[i]);
+    const T wv = mul_rn(inv_theta, rv);
     r[i] = rv;
     w[i] = wv;
     y[i] = wv;
@@ -179,21 +182,20 @@ __global__ void k_cheb1_start(int n, const double* x, const double* __restrict__
 
 // _algo1 step (:342-354): r -= D^-1 A w ; w = c1 w + c2 r ; y += w, with the
 // rounding of pointwiseMult, axpy(-1), scal, axpy(c2), axpy(1).
-template <class View>
-__global__ void __launch_bounds__(kThreads) k_cheb1_step(int n, View A, const double* __restrict__ inv,
-                                                         double* __restrict__ r, const double* __restrict__ wcur,
-                                                         double* __restrict__ wnext, double* __restrict__ y,
-                                                         double c1, double c2) {
+template <class View, class T>
+__global__ void __launch_bounds__(kThreads) k_cheb1_step(int n, View A, const T* __restrict__ inv, T* __restrict__ r,
+                                                         const T* __restrict__ wcur, T* __restrict__ wnext,
+                                                         T* __restrict__ y, T c1, T c2) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= n) return;
-  // __dmul_rn: the products are rounded on their own, as pointwiseMult and
+  // mul_rn: the products are rounded on their own, as pointwiseMult and
   // scal round them; a plain '*' could be fused into the following update.
-  const double my = __dmul_rn(inv[row], A.row(row, wcur));
-  const double rv = fma(-1.0, my, r[row]);
+  const T my = mul_rn(inv[row], A.row(row, wcur));
+  const T rv = fma_rn(T(-1), my, r[row]);
   r[row] = rv;
-  const double wv = fma(c2, rv, __dmul_rn(c1, wcur[row]));
+  const T wv = fma_rn(c2, rv, mul_rn(c1, wcur[row]));
   wnext[row] = wv;
-  y[row] = fma(1.0, wv, y[row]);
+  y[row] = fma_rn(T(1), wv, y[row]);
 }
 
 __global__ void k_sqrt(int n, const double* __restrict__ a, double* __restrict__ s) {
@@ -234,8 +236,9 @@ void tridiag_extremes(const std::vector<double>& a, const std::vector<double>& b
   *lmax = kth(m);
 }
 
-__global__ void k_pmult2(int n, const double* __restrict__ a, const double* x, double* y) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a[i] * x[i];
+template <class T>
+__global__ void k_pmult2(int n, const T* __restrict__ a, const T* x, T* y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = mul_rn(a[i], x[i]);
 }
 
 void ilu_symbolic(const ab2_matrix* A, Ilu0Data& d) {
@@ -465,27 +468,67 @@ void cheb_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o) 
 
 }  // namespace
 
-void pc_apply(ab2_context* ctx, const ab2_precond* pc, const double* x, double* y) {
+namespace {
+
+// The FP64 or FP32 arrays of a preconditioner.
+template <class T>
+struct PcArrays;
+template <>
+struct PcArrays<double> {
+  const double* inv;
+  const double* lu;
+  double* tmp;
+  double *p, *y0, *y1, *xcopy;
+  explicit PcArrays(const ab2_precond* pc)
+      : inv(pc->d_inv), lu(pc->ilu.d_lu), tmp(pc->ilu.d_tmp), p(pc->cheb.d_p), y0(pc->cheb.d_y[0]),
+        y1(pc->cheb.d_y[1]), xcopy(pc->cheb.d_xcopy) {}
+};
+template <>
+struct PcArrays<float> {
+  const float* inv;
+  const float* lu;
+  float* tmp;
+  float *p, *y0, *y1, *xcopy;
+  explicit PcArrays(const ab2_precond* pc) : inv(pc->d_inv32), lu(pc->d_lu32), tmp(pc->d_tmp32) {
+    const size_t n = (size_t)pc->A->n;
+    float* c = pc->d_cheb32;
+    p = c;
+    y0 = c ? c + n : nullptr;
+    y1 = c ? c + 2 * n : nullptr;
+    xcopy = c ? c + 3 * n : nullptr;
+  }
+};
+
+template <class T>
+void copy_t(ab2_context* ctx, int n, const T* x, T* y) {
+  if (x == y) return;
+  AB2_CUDA(cudaMemcpyAsync(y, x, sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
+}
+
+template <class T>
+void apply_t(ab2_context* ctx, const ab2_precond* pc, const T* x, T* y) {
   const int n = pc->A->n;
   if (n == 0) return;
+  const PcArrays<T> w(pc);
   switch (pc->kind) {
-    case AB2_PC_NONE: op_copy(ctx, n, x, y); break;
+    case AB2_PC_NONE: copy_t(ctx, n, x, y); break;
     case AB2_PC_DIAG:
-      k_pmult2<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, pc->d_inv, x, y);
+      k_pmult2<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, w.inv, x, y);
       check_launch(ctx, "diag_apply");
       break;
     case AB2_PC_ILU0: {
       const Ilu0Data& d = pc->ilu;
       const ab2_matrix* A = pc->A;
       if (d.stencil) {
-        ilu_stencil_apply(ctx, A, d, x, y);
+        if constexpr (sizeof(T) == 8) ilu_stencil_apply(ctx, A, d, x, y);
+        else ilu_stencil_apply_f32(ctx, d, x, y);
         break;
       }
-      k_ilu_lsweep<<<sweep_blocks(ctx, d.len_l, d.widest_l), 256, 0, ctx->stream>>>(
-          d.len_l, d.d_perm_l, A->d_rp, A->d_ci, A->d_dcol, d.d_lu, x, d.d_tmp, y, d.d_counters, d.d_err);
+      k_ilu_lsweep<T><<<sweep_blocks(ctx, d.len_l, d.widest_l), 256, 0, ctx->stream>>>(
+          d.len_l, d.d_perm_l, A->d_rp, A->d_ci, A->d_dcol, w.lu, x, w.tmp, y, d.d_counters, d.d_err);
       check_launch(ctx, "ilu_lsweep");
-      k_ilu_usweep<<<sweep_blocks(ctx, d.len_u, d.widest_u), 256, 0, ctx->stream>>>(
-          d.len_u, d.d_perm_u, A->d_rp, A->d_ci, A->d_dcol, d.d_lu, d.d_tmp, y, d.d_counters, d.d_err);
+      k_ilu_usweep<T><<<sweep_blocks(ctx, d.len_u, d.widest_u), 256, 0, ctx->stream>>>(
+          d.len_u, d.d_perm_u, A->d_rp, A->d_ci, A->d_dcol, w.lu, w.tmp, y, d.d_counters, d.d_err);
       check_launch(ctx, "ilu_usweep");
       break;
     }
@@ -493,31 +536,33 @@ void pc_apply(ab2_context* ctx, const ab2_precond* pc, const double* x, double* 
       const ChebData& c = pc->cheb;
       const int steps = std::max(1, c.order);
       if (c.saad) {
-        double* r = c.d_p;
-        k_cheb1_start<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, x, pc->d_inv, c.inv_theta, r, c.d_y[0], y);
+        T* r = w.p;
+        T* wv[2] = {w.y0, w.y1};
+        k_cheb1_start<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, x, w.inv, (T)c.inv_theta, r, wv[0], y);
         check_launch(ctx, "cheb1_start");
         for (int k = 1; k < steps; ++k) {
-          const double* wcur = c.d_y[(k - 1) & 1];
-          double* wnext = c.d_y[k & 1];
-          with_view<double>(pc->A, pc->variant, [&](auto view) {
-            k_cheb1_step<<<(n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(n, view, pc->d_inv, r, wcur,
-                                                                                      wnext, y, c.a[k], c.b[k]);
+          const T* wcur = wv[(k - 1) & 1];
+          T* wnext = wv[k & 1];
+          with_view<T>(pc->A, pc->variant, [&](auto view) {
+            k_cheb1_step<<<(n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(n, view, w.inv, r, wcur, wnext,
+                                                                                      y, (T)c.a[k], (T)c.b[k]);
           });
           check_launch(ctx, "cheb1_step");
         }
         break;
       }
-      const double* xin = x;
+      const T* xin = x;
       if (x == y) {
-        op_copy(ctx, n, x, c.d_xcopy);
-        xin = c.d_xcopy;
+        copy_t(ctx, n, x, w.xcopy);
+        xin = w.xcopy;
       }
-      const double* cur = xin;
+      const T* cur = xin;
+      T* ys[2] = {w.y0, w.y1};
       for (int i = 0; i < steps; ++i) {
-        double* next = (i == steps - 1) ? y : c.d_y[i & 1];
-        with_view<double>(pc->A, pc->variant, [&](auto view) {
-          k_cheb_step<<<(n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(n, view, xin, cur, pc->d_inv, c.d_p,
-                                                                                   next, c.a[i], c.b[i], i == 0);
+        T* next = (i == steps - 1) ? y : ys[i & 1];
+        with_view<T>(pc->A, pc->variant, [&](auto view) {
+          k_cheb_step<<<(n + kThreads - 1) / kThreads, kThreads, 0, ctx->stream>>>(n, view, xin, cur, w.inv, w.p, next,
+                                                                                   (T)c.a[i], (T)c.b[i], i == 0);
         });
         check_launch(ctx, "cheb_step");
         cur = next;
@@ -528,12 +573,53 @@ void pc_apply(ab2_context* ctx, const ab2_precond* pc, const double* x, double* 
   }
 }
 
+}  // namespace
+
+void pc_apply(ab2_context* ctx, const ab2_precond* pc, const double* x, double* y) { apply_t(ctx, pc, x, y); }
+
+void pc_enable_f32(ab2_context* ctx, ab2_precond* pc) {
+  if (pc->f32) return;
+  const ab2_matrix* A = pc->A;
+  const int n = A->n;
+  if (pc->d_inv) {
+    pc->d_inv32 = dev_alloc<float>(ctx, (size_t)n);
+    op_to_f32(ctx, n, pc->d_inv, pc->d_inv32);
+  }
+  if (pc->kind == AB2_PC_CHEB) {
+    require(A->d_v32 != nullptr, "FP32 Chebyshev needs the matrix's FP32 values (AB2_FMT_F32)");
+    pc->d_cheb32 = dev_alloc<float>(ctx, 4 * (size_t)std::max(n, 1));
+    AB2_CUDA(cudaMemsetAsync(pc->d_cheb32, 0, sizeof(float) * 4 * (size_t)std::max(n, 1), ctx->stream));
+  }
+  if (pc->kind == AB2_PC_ILU0) {
+    if (pc->ilu.stencil) {
+      ilu_stencil_enable_f32(ctx, pc->ilu);
+    } else {
+      pc->d_lu32 = dev_alloc<float>(ctx, (size_t)A->nnz);
+      op_to_f32(ctx, A->nnz, pc->ilu.d_lu, pc->d_lu32);
+      pc->d_tmp32 = dev_alloc<float>(ctx, (size_t)n);
+      k_fill_bits32<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, kSentinel32, pc->d_tmp32);
+      check_launch(ctx, "ilu_fill32");
+    }
+  }
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  pc->f32 = true;
+}
+
+void pc_apply_f32(ab2_context* ctx, const ab2_precond* pc, const float* x, float* y) {
+  require(pc->f32, "preconditioner has no FP32 form (pc_enable_f32)");
+  apply_t(ctx, pc, x, y);
+}
+
 void pc_reset(ab2_context* ctx, const ab2_precond* pc) {
   if (pc->kind != AB2_PC_ILU0) return;
   const Ilu0Data& d = pc->ilu;
   AB2_CUDA(cudaStreamSynchronize(ctx->stream));
   k_fill_bits<<<grid_for(pc->A->n), kThreads, 0, ctx->stream>>>(pc->A->n, kSentinel, d.d_tmp);
   check_launch(ctx, "ilu_fill");
+  if (pc->d_tmp32) {
+    k_fill_bits32<<<grid_for(pc->A->n), kThreads, 0, ctx->stream>>>(pc->A->n, kSentinel32, pc->d_tmp32);
+    check_launch(ctx, "ilu_fill32");
+  }
   AB2_CUDA(cudaMemsetAsync(d.d_counters, 0, 2 * sizeof(unsigned int), ctx->stream));
   if (d.d_tile_tickets) AB2_CUDA(cudaMemsetAsync(d.d_tile_tickets, 0, 3 * sizeof(unsigned int), ctx->stream));
   if (d.stencil) ilu_stencil_reset(ctx, d);
@@ -604,11 +690,16 @@ int ab2_precond_destroy(ab2_precond* pc) {
   dev_free(pc->ctx, pc->ilu.d_err);
   dev_free(pc->ctx, pc->ilu.d_bands);
   dev_free(pc->ctx, pc->ilu.d_walk);
+  dev_free(pc->ctx, pc->ilu.d_walk32);
   dev_free(pc->ctx, pc->ilu.d_tile_tickets);
   dev_free(pc->ctx, pc->cheb.d_p);
   dev_free(pc->ctx, pc->cheb.d_y[0]);
   dev_free(pc->ctx, pc->cheb.d_y[1]);
   dev_free(pc->ctx, pc->cheb.d_xcopy);
+  dev_free(pc->ctx, pc->d_inv32);
+  dev_free(pc->ctx, pc->d_lu32);
+  dev_free(pc->ctx, pc->d_tmp32);
+  dev_free(pc->ctx, pc->d_cheb32);
   if (pc->ctx) ctx_release(pc->ctx);
   delete pc;
   return AB2_OK;

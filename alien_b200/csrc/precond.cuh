@@ -38,6 +38,7 @@ struct Ilu0Data {
   // and the two sweeps' propagation arrays.
   long long walk_n = 0;
   double* d_walk = nullptr;
+  float* d_walk32 = nullptr;  // the same arrays in FP32 (mixed-precision inner solves), built on demand
 };
 
 // Detects a 3-D 7-point matrix in lexicographic order and, if found,
@@ -46,6 +47,9 @@ bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d);
 void ilu_stencil_apply(ab2_context* ctx, const ab2_matrix* A, const Ilu0Data& d, const double* y, double* z);
 // Puts the sweeps' propagation arrays back to the sentinel (after a failed application).
 void ilu_stencil_reset(ab2_context* ctx, const Ilu0Data& d);
+// FP32 copies of the walk arrays (the FP64 factor rounded) and the FP32 application.
+void ilu_stencil_enable_f32(ab2_context* ctx, Ilu0Data& d);
+void ilu_stencil_apply_f32(ab2_context* ctx, const Ilu0Data& d, const float* y, float* z);
 
 struct ChebData {
   double alpha = 0, beta = 0;
@@ -69,12 +73,23 @@ struct ab2_precond {
   double* d_inv = nullptr;  // 1/a_ii (Diag, Chebyshev)
   ab2::Ilu0Data ilu;
   ab2::ChebData cheb;
+  // FP32 form for the inner solves of the mixed-precision solver
+  // (pc_enable_f32): the FP64 set-up's results rounded to float.
+  bool f32 = false;
+  float* d_inv32 = nullptr;
+  float* d_lu32 = nullptr;    // wavefront ILU(0) factor
+  float* d_tmp32 = nullptr;   // wavefront ILU(0) forward-sweep output (sentinel between applications)
+  float* d_cheb32 = nullptr;  // Chebyshev work vectors p | y0 | y1 | xcopy
 };
 
 namespace ab2 {
 
 // y = M^-1 x, stream ordered, capturable in a CUDA graph.
 void pc_apply(ab2_context* ctx, const ab2_precond* pc, const double* x, double* y);
+// Builds the FP32 form (the matrix must carry FP32 values for Chebyshev), and
+// applies it: the same operations in float.
+void pc_enable_f32(ab2_context* ctx, ab2_precond* pc);
+void pc_apply_f32(ab2_context* ctx, const ab2_precond* pc, const float* x, float* y);
 // Resets ILU0 sweep state after a failed (timed-out) application.
 void pc_reset(ab2_context* ctx, const ab2_precond* pc);
 int pc_error(ab2_context* ctx, const ab2_precond* pc);

@@ -2,7 +2,8 @@
 //
 // A sweep's output vector is pre-filled with a signalling-NaN bit pattern that
 // arithmetic never produces (results of arithmetic are quiet NaNs).  A
-// producer stores the final 8-byte value with st.relaxed.gpu; a consumer polls
+// producer stores the final 8-byte (FP32 sweeps: 4-byte) value with
+// st.relaxed.gpu; a consumer polls
 // the word with ld.relaxed.gpu until it is no longer the sentinel.  Because
 // the payload is the flag, no fence or separate ready bit is needed.  Every
 // wait is bounded by a clock64 budget: on expiry the waiter records an error
@@ -66,6 +67,57 @@ __device__ __forceinline__ double not_sentinel(double v) {
 __global__ void k_fill_bits(long long n, unsigned long long bits, double* x) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     x[i] = __longlong_as_double((long long)bits);
+}
+
+// ---- 4-byte words (the FP32 sweeps of the mixed-precision solver)
+constexpr unsigned int kSentinel32 = 0x7FA1B2C3u;  // signalling NaN (quiet bit clear)
+
+__device__ __forceinline__ float ld_relaxed(const float* p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return __uint_as_float(v);
+}
+
+__device__ __forceinline__ void st_relaxed(float* p, float x) {
+  asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(__float_as_uint(x)) : "memory");
+}
+
+__device__ __forceinline__ bool is_sentinel(float v) { return __float_as_uint(v) == kSentinel32; }
+
+__device__ __noinline__ float wait_value(const float* p, int* err) {
+  float v = ld_relaxed(p);
+  if (!is_sentinel(v)) return v;
+  const long long t0 = clock64();
+  for (unsigned it = 1;; ++it) {
+    if (it > 8) __nanosleep(it > 64 ? 256 : 32);
+    v = ld_relaxed(p);
+    if (!is_sentinel(v)) return v;
+    if ((it & 63) == 0) {
+      if (clock64() - t0 > kWaitCycles || *(volatile int*)err) {
+        atomicOr(err, 1);
+        return __uint_as_float(0x7FC00000u);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ float not_sentinel(float v) { return is_sentinel(v) ? __uint_as_float(0x7FC00000u) : v; }
+
+__global__ void k_fill_bits32(long long n, unsigned int bits, float* x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = __uint_as_float(bits);
+}
+
+// The sentinel of either word size, for templated sweeps.
+template <class T>
+__device__ __forceinline__ T sentinel_of();
+template <>
+__device__ __forceinline__ double sentinel_of<double>() {
+  return __longlong_as_double((long long)kSentinel);
+}
+template <>
+__device__ __forceinline__ float sentinel_of<float>() {
+  return __uint_as_float(kSentinel32);
 }
 
 }  // namespace

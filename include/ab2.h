@@ -250,6 +250,54 @@ int ab2_solver_solve(ab2_solver* s, const ab2_vector* b, ab2_vector* x, ab2_stat
 int ab2_solver_history(const ab2_solver* s, double* hist, int cap, int* len);
 int ab2_solver_destroy(ab2_solver* s);
 
+/* ------------------------------------------------------------------ mixed precision
+ * FP32 Krylov inside FP64 iterative refinement.  No counterpart in the
+ * reference (its solvers run in the matrix's value type); the inner solver is
+ * the reference's CG.h / BiCGStab.h and preconditioners instantiated in float.
+ * Each refinement step: r = b - A x and ||r|| in FP64; stop when
+ * ||r|| / ||b|| < tol; inner solve A32 d = float(r / ||r||) from d = 0 to the
+ * recursive residual inner_tol (FP32 values, FP32 accumulation, FP32
+ * scalars); x += ||r|| d in FP64.  The matrix must carry FP32 values
+ * (AB2_FMT_F32); the FP32 preconditioner is the FP64 set-up rounded. */
+typedef struct ab2_mixed ab2_mixed;
+
+typedef struct {
+  int solver;          /* inner: AB2_SOLVER_CG or AB2_SOLVER_BICGSTAB */
+  int precond;         /* inner, applied in FP32: AB2_PC_* */
+  double tol;          /* outer: true relative residual ||b - A x|| / ||b||, FP64 */
+  int max_outer;       /* refinement steps */
+  double inner_tol;    /* inner: relative residual of each FP32 solve, in (0, 1) */
+  int inner_max_iter;  /* inner: iterations per refinement step */
+  double poly_factor;  /* Chebyshev settings as in ab2_precond_options */
+  int poly_order;
+  int poly_factor_max_iter;
+  int cheb_saad;
+  int cheb_lanczos;
+  int ilu_schedule;    /* AB2_ILU_* */
+  int spmv_variant;    /* AB2_SPMV_* for both precisions */
+  int use_graph;       /* inner loop in a CUDA graph */
+} ab2_mixed_options;
+
+typedef struct {
+  int succeeded;          /* final true relative residual < tol */
+  int outer_iterations;   /* refinement steps (inner solves) taken */
+  int inner_iterations;   /* FP32 Krylov iterations over all steps */
+  int error;              /* AB2_OK; AB2_ERR_NOT_CONVERGED (max_outer reached, or a step did not
+                             reduce the true residual); AB2_ERR_BREAKDOWN (an inner solve broke
+                             down before its first iteration); AB2_ERR_TIMEOUT */
+  double true_residual;   /* final ||b - A x|| / ||b||, FP64 */
+  double setup_ms;        /* FP64 preconditioner set-up + FP32 copies + graph build */
+  double solve_ms;        /* device time of the last solve */
+} ab2_mixed_status;
+
+void ab2_mixed_options_default(ab2_mixed_options* opts);
+int ab2_mixed_create(ab2_context* ctx, const ab2_matrix* A, const ab2_mixed_options* opts, ab2_mixed** m);
+/* x holds the initial guess on entry, the solution on exit (FP64). */
+int ab2_mixed_solve(ab2_mixed* m, const ab2_vector* b, ab2_vector* x, ab2_mixed_status* status);
+/* true relative residual before each refinement step and at the end of the last solve */
+int ab2_mixed_history(const ab2_mixed* m, double* res, int cap, int* len);
+int ab2_mixed_destroy(ab2_mixed* m);
+
 #ifdef __cplusplus
 }
 #endif

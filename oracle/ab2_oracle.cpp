@@ -49,6 +49,7 @@ extern "C" {
 enum {
   ORC_OK = 0,
   ORC_ERR_BREAKDOWN = -3,
+  ORC_ERR_NOT_CONVERGED = -4,
   ORC_ERR_BAD_ARG = -6,
 };
 enum { ORC_SOLVER_CG = 0, ORC_SOLVER_BICGSTAB = 1 };
@@ -85,6 +86,34 @@ typedef struct {
   int history_len;       // entries written into hist
 } orc_result;
 
+// Mixed-precision refinement (libab2's ab2_mixed, no reference counterpart):
+// FP64 residual and update, FP32 inner CG/BiCGStab from the reference
+// templates' arithmetic instantiated in float.
+typedef struct {
+  int solver;               // inner ORC_SOLVER_*
+  int precond;              // inner ORC_PC_* (FP64 set-up, applied in float)
+  double tol;               // true relative residual, FP64
+  int max_outer;
+  double inner_tol;
+  int inner_max_iter;
+  double poly_factor;
+  int poly_order;
+  int poly_factor_max_iter;
+  int cheb_saad;
+  int cheb_lanczos;
+  int dot_mode;             // as orc_options, for the FP64 and the FP32 dots
+  int tree_blocks;
+} orc_mixed_options;
+
+typedef struct {
+  int succeeded;
+  int outer_iterations;
+  int inner_iterations;
+  int error;                // ORC_OK, ORC_ERR_NOT_CONVERGED, ORC_ERR_BREAKDOWN
+  double true_residual;
+  int history_len;          // true relative residuals written into hist
+} orc_mixed_result;
+
 }  // extern "C"
 
 namespace {
@@ -93,8 +122,9 @@ using namespace ab2_oracle;
 
 // One warp's __shfl_down_sync tree (offsets 16..1): lane l adds lane l+off's
 // value when l+off < 32; the result is lane 0's.
-double warp_tree(const double* in) {
-  double v[32], w[32];
+template <class T>
+T warp_tree(const T* in) {
+  T v[32], w[32];
   for (int l = 0; l < 32; ++l) v[l] = in[l];
   for (int off = 16; off > 0; off >>= 1) {
     for (int l = 0; l < 32; ++l) w[l] = v[l] + (l + off < 32 ? v[l + off] : v[l]);
@@ -107,28 +137,30 @@ double warp_tree(const double* in) {
 // 256 threads, G = min(max(ceil(n/256), 1), max_blocks); thread g sums
 // x_i y_i for i = g, g + 256G, ... with fma; each warp's values go through
 // warp_tree, the 8 warp sums through another; then lane l of the last block
-// adds the block partials l, l+32, ... in order and a final warp_tree.
-double tree_dot(int n, const double* x, const double* y, int max_blocks) {
-  const int T = 256;
-  long long g = ((long long)n + T - 1) / T;
+// adds the block partials l, l+32, ... in order and a final warp_tree.  In T
+// throughout (float for the FP32 inner solves).
+template <class T>
+T tree_dot(int n, const T* x, const T* y, int max_blocks) {
+  const int TH = 256;
+  long long g = ((long long)n + TH - 1) / TH;
   if (g < 1) g = 1;
   if (g > max_blocks) g = max_blocks;
   const int G = (int)g;
-  const long long stride = (long long)G * T;
-  std::vector<double> partial(G);
-  double th[256], ws[32];
+  const long long stride = (long long)G * TH;
+  std::vector<T> partial(G);
+  T th[256], ws[32];
   for (int b = 0; b < G; ++b) {
-    for (int t = 0; t < T; ++t) {
-      double acc = 0.0;
-      for (long long i = (long long)b * T + t; i < n; i += stride) acc = std::fma(x[i], y[i], acc);
+    for (int t = 0; t < TH; ++t) {
+      T acc = 0;
+      for (long long i = (long long)b * TH + t; i < n; i += stride) acc = std::fma(x[i], y[i], acc);
       th[t] = acc;
     }
-    for (int l = 0; l < 32; ++l) ws[l] = l < T / 32 ? warp_tree(th + 32 * l) : 0.0;
+    for (int l = 0; l < 32; ++l) ws[l] = l < TH / 32 ? warp_tree(th + 32 * l) : T(0);
     partial[b] = warp_tree(ws);
   }
-  double lanes[32];
+  T lanes[32];
   for (int l = 0; l < 32; ++l) {
-    double s = 0.0;
+    T s = 0;
     for (int b = l; b < G; b += 32) s = s + partial[b];
     lanes[l] = s;
   }
@@ -140,33 +172,34 @@ thread_local int g_tree_blocks = 1184;
 thread_local bool g_cheb_saad = false;
 thread_local bool g_cheb_lanczos = false;
 
-double vdot(int n, const double* x, const double* y) {
+template <class T>
+T vdot(int n, const T* x, const T* y) {
   return g_dot_mode == 1 ? tree_dot(n, x, y, g_tree_blocks) : dot(n, x, y);
 }
 
 // Stop test shared by CG (Iteration.h) and BiCGStab (its nested Iteration).
+template <class T>
 struct StopTest {
   int n;
   int max_iter;
   int iter = 0;
-  double criteria;
-  double nrm2_b;
+  T criteria;
+  T nrm2_b;
   bool status = false;
-  double last = 0.0;
-  double* hist;
+  T last = 0;
+  T* hist;
   int hist_cap;
   int hist_len = 0;
 
-  StopTest(int n_, const double* b, double tol, int max_it, double* h, int cap)
-      : n(n_), max_iter(max_it), hist(h), hist_cap(cap) {
-    nrm2_b = vdot(n,b, b);
+  StopTest(int n_, const T* b, T tol, int max_it, T* h, int cap) : n(n_), max_iter(max_it), hist(h), hist_cap(cap) {
+    nrm2_b = vdot(n, b, b);
     criteria = tol * tol * nrm2_b;
-    status = (nrm2_b == 0.0);
+    status = (nrm2_b == 0);
   }
-  bool null_rhs() const { return nrm2_b == 0.0; }
-  bool stop(const double* r) {
+  bool null_rhs() const { return nrm2_b == 0; }
+  bool stop(const T* r) {
     if (iter >= max_iter) return true;
-    last = vdot(n,r, r);
+    last = vdot(n, r, r);
     if (hist && hist_len < hist_cap) hist[hist_len] = last;
     ++hist_len;
     status = last < criteria;
@@ -180,70 +213,78 @@ struct Breakdown {
 };
 
 // ---------------------------------------------------------------- preconditioners
+// Set up in FP64 from the FP64 matrix (as the reference does); applied in T:
+// the FP32 form rounds the FP64 set-up's results, as libab2's pc_enable_f32.
+template <class T>
 struct Precond {
   virtual ~Precond() {}
-  virtual void apply(const double* x, double* y) = 0;
+  virtual void apply(const T* x, T* y) = 0;
 };
 
-struct Identity : Precond {
+template <class T>
+struct Identity : Precond<T> {
   int n;
   explicit Identity(int n_) : n(n_) {}
-  void apply(const double* x, double* y) override { copy(n, x, y); }
+  void apply(const T* x, T* y) override { copy(n, x, y); }
 };
 
-struct Diag : Precond {
+template <class T>
+struct Diag : Precond<T> {
   int n;
-  std::vector<double> inv;
-  explicit Diag(const Csr& A) : n(A.n), inv(A.n, 1.0) {
+  std::vector<T> inv;
+  explicit Diag(const Csr& A) : n(A.n), inv(A.n, T(1)) {
     std::vector<int> d = diag_offsets(A);
-    for (int i = 0; i < n; ++i) inv[i] = 1.0 / A.v[d[i]];
+    for (int i = 0; i < n; ++i) inv[i] = (T)(1.0 / A.v[d[i]]);
   }
-  void apply(const double* x, double* y) override { pmult(n, inv.data(), x, y); }
+  void apply(const T* x, T* y) override { pmult(n, inv.data(), x, y); }
 };
 
 // In-place IKJ ILU(0) on a copy of the values (ILU0Preconditioner.h:156-178),
-// then the forward/backward sweeps of solveL/solveU (:181-231).
-struct Ilu0 : Precond {
+// in FP64, then the forward/backward sweeps of solveL/solveU (:181-231) in T.
+template <class T>
+struct Ilu0 : Precond<T> {
   int n;
   const int* rp;
   const int* ci;
   std::vector<int> d;
-  std::vector<double> lu;
-  std::vector<double> tmp;
+  std::vector<double> lu64;
+  std::vector<T> lu;
+  std::vector<T> tmp;
 
-  explicit Ilu0(const Csr& A) : n(A.n), rp(A.rp), ci(A.ci), lu(A.v, A.v + A.rp[A.n]), tmp(A.n) {
+  explicit Ilu0(const Csr& A) : n(A.n), rp(A.rp), ci(A.ci), lu64(A.v, A.v + A.rp[A.n]), tmp(A.n) {
     d = diag_offsets(A);
     std::vector<int> work(n, -1);
     for (int i = 1; i < n; ++i) {
       for (int k = rp[i]; k < d[i]; ++k) {
         const int kr = ci[k];
-        const double aik = lu[k] / lu[d[kr]];
-        lu[k] = aik;
+        const double aik = lu64[k] / lu64[d[kr]];
+        lu64[k] = aik;
         for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = l;
         for (int j = k + 1; j < rp[i + 1]; ++j) {
           const int kj = work[ci[j]];
-          if (kj != -1) lu[j] = lu[j] - aik * lu[kj];
+          if (kj != -1) lu64[j] = lu64[j] - aik * lu64[kj];
         }
         for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = -1;
       }
     }
+    lu.assign(lu64.begin(), lu64.end());
   }
-  void solve_l(const double* y, double* x) const {
+  void solve_l(const T* y, T* x) const {
     for (int i = 0; i < n; ++i) {
-      double v = y[i];
+      T v = y[i];
       for (int k = rp[i]; k < d[i]; ++k) v = v - lu[k] * x[ci[k]];
       x[i] = v;
     }
   }
-  void solve_u(const double* y, double* x) const {
+  void solve_u(const T* y, T* x) const {
     for (int i = n - 1; i >= 0; --i) {
       const int dk = d[i];
-      double v = y[i];
+      T v = y[i];
       for (int k = dk + 1; k < rp[i + 1]; ++k) v = v - lu[k] * x[ci[k]];
       x[i] = v / lu[dk];
     }
   }
-  void apply(const double* y, double* x) override {
+  void apply(const T* y, T* x) override {
     solve_l(y, tmp.data());
     solve_u(tmp.data(), x);
   }
@@ -284,23 +325,30 @@ void tridiag_extremes(const std::vector<double>& a, const std::vector<double>& b
   *lmax = kth(m);
 }
 
-struct Cheb : Precond {
-  const Csr A;
+template <class T>
+struct Cheb : Precond<T> {
+  const Csr A64;     // bounds are estimated in FP64 on the FP64 matrix
+  const CsrT<T> A;   // the matrix the application multiplies by
   int n;
   int order;
   bool saad;
-  std::vector<double> inv, y_, r_, p_, z_, w_;
+  std::vector<double> inv64, y64;
+  std::vector<T> inv, y_, r_, p_, z_, w_;
   double alpha = 0.0, beta = 0.0;
+  // step coefficients, evaluated in FP64 in the reference's order
+  std::vector<double> ca, cb;  // _algo2: alpha_i, beta_i ; _algo1: rho rho_old, 2 rho / delta
+  double inv_theta = 0.0;      // _algo1: 1 / theta
 
   // saad: ChebyshevPreconditioner<AlgebraT, true> (_algo1, zero start, a
   // symmetric operator); otherwise the default _algo2.  lanczos: bounds from
   // `max_iter` Lanczos steps on D^-1/2 A D^-1/2 (this repo's addition)
-  // instead of the reference's two power methods.
-  Cheb(const Csr& A_, double factor, int order_, int max_iter, bool saad_ = false, bool lanczos = false)
-      : A(A_), n(A_.n), order(order_), saad(saad_), inv(A_.n, 1.0), y_(A_.n, 0.0), r_(A_.n, 0.0), p_(A_.n, 0.0),
-        z_(A_.n, 0.0), w_(A_.n, 0.0) {
-    std::vector<int> d = diag_offsets(A);
-    for (int i = 0; i < n; ++i) inv[i] = 1.0 / A.v[d[i]];
+  // instead of the reference's two power methods.  vT: the matrix values in T.
+  Cheb(const Csr& A_, const T* vT, double factor, int order_, int max_iter, bool saad_ = false, bool lanczos = false)
+      : A64(A_), A{A_.n, A_.rp, A_.ci, vT}, n(A_.n), order(order_), saad(saad_), inv64(A_.n, 1.0), y64(A_.n, 0.0),
+        inv(A_.n, T(1)), y_(A_.n, T(0)), r_(A_.n, T(0)), p_(A_.n, T(0)), z_(A_.n, T(0)), w_(A_.n, T(0)) {
+    std::vector<int> d = diag_offsets(A64);
+    for (int i = 0; i < n; ++i) inv64[i] = 1.0 / A64.v[d[i]];
+    for (int i = 0; i < n; ++i) inv[i] = (T)inv64[i];
     if (lanczos) {
       lanczos_bounds(max_iter);
     } else {
@@ -308,6 +356,37 @@ struct Cheb : Precond {
       alpha = power_bound(max_iter, /*shift=*/true, beta);
     }
     if (factor != 0.0) alpha = beta / factor;
+    coefficients();
+  }
+
+  void coefficients() {
+    const int steps = std::max(1, order);
+    ca.assign(steps, 0.0);
+    cb.assign(steps, 0.0);
+    if (saad) {  // ChebyshevPreconditioner.h:316-351
+      const double delta = (beta - alpha) / 2;
+      const double theta = (beta + alpha) / 2;
+      const double sigma = theta / delta;
+      double rho_old = 1. / sigma;
+      inv_theta = 1 / theta;
+      for (int k = 1; k < steps; ++k) {
+        const double rho = 1. / (2 * sigma - rho_old);
+        ca[k] = rho * rho_old;
+        cb[k] = 2 * rho / delta;
+        rho_old = rho;
+      }
+      return;
+    }
+    const double dd = (beta + alpha) / 2;  // :392-434
+    const double c = (beta - alpha) / 2;
+    double a = 2 / dd;
+    ca[0] = a;
+    for (int i = 1; i < steps; ++i) {
+      const double bcoef = a * (c / 2.) * (c / 2.);
+      a = 1. / (dd - bcoef);
+      cb[i] = bcoef;
+      ca[i] = a;
+    }
   }
 
   // Lanczos on B = S A S, S = diag(sqrt(1/a_ii)), from the same mt19937 start
@@ -316,7 +395,7 @@ struct Cheb : Precond {
   // polynomial positive on all of it).
   void lanczos_bounds(int steps) {
     std::vector<double> s(n), v(n), vp(n, 0.0), t(n), w(n);
-    for (int i = 0; i < n; ++i) s[i] = std::sqrt(inv[i]);
+    for (int i = 0; i < n; ++i) s[i] = std::sqrt(inv64[i]);
     std::mt19937 gen;
     std::uniform_real_distribution<> dis(-1., 1.);
     for (int i = 0; i < n; ++i) v[i] = dis(gen);
@@ -326,7 +405,7 @@ struct Cheb : Precond {
     double bprev = 0.0;
     for (int j = 0; j < std::max(steps, 1); ++j) {
       pmult(n, s.data(), v.data(), t.data());
-      spmv(A, t.data(), w.data());
+      spmv(A64, t.data(), w.data());
       pmult(n, s.data(), w.data(), w.data());
       if (j > 0) axpy(n, -bprev, vp.data(), w.data());
       const double aj = vdot(n, w.data(), v.data());
@@ -354,88 +433,77 @@ struct Cheb : Precond {
     std::mt19937 gen;
     std::uniform_real_distribution<> dis(-1., 1.);
     for (int i = 0; i < n; ++i) x[i] = dis(gen);
-    double nrm = std::sqrt(vdot(n,x.data(), x.data()));
+    double nrm = std::sqrt(vdot(n, x.data(), x.data()));
     scal(n, 1 / nrm, x.data());
     double est = 0.0;
     for (int it = 0; it < max_iter; ++it) {
-      spmv(A, x.data(), y_.data());
-      pmult(n, inv.data(), y_.data(), y_.data());
-      if (shift) axpy(n, -b, x.data(), y_.data());
-      const double xax = vdot(n,y_.data(), x.data());
-      const double xdx = vdot(n,x.data(), x.data());
+      spmv(A64, x.data(), y64.data());
+      pmult(n, inv64.data(), y64.data(), y64.data());
+      if (shift) axpy(n, -b, x.data(), y64.data());
+      const double xax = vdot(n, y64.data(), x.data());
+      const double xdx = vdot(n, x.data(), x.data());
       est = xax / xdx;
-      const double nr = std::sqrt(vdot(n,y_.data(), y_.data()));
-      scal(n, 1 / nr, y_.data());
-      copy(n, y_.data(), x.data());
+      const double nr = std::sqrt(vdot(n, y64.data(), y64.data()));
+      scal(n, 1 / nr, y64.data());
+      copy(n, y64.data(), x.data());
     }
     if (shift) est += b;
     return est;
   }
 
   // _algo2 (ChebyshevPreconditioner.h:392-434), the default.
-  void apply_default(const double* x, double* y) {
-    const double dd = (beta + alpha) / 2;
-    const double c = (beta - alpha) / 2;
+  void apply_default(const T* x, T* y) {
     copy(n, x, y);
     spmv(A, y, y_.data());
     copy(n, x, r_.data());
-    axpy(n, -1., y_.data(), r_.data());
+    axpy(n, T(-1), y_.data(), r_.data());
     pmult(n, inv.data(), r_.data(), z_.data());
     copy(n, z_.data(), p_.data());
-    double a = 2 / dd;
-    axpy(n, a, p_.data(), y);
+    axpy(n, (T)ca[0], p_.data(), y);
     for (int i = 1; i < order; ++i) {
       spmv(A, y, y_.data());
       copy(n, x, r_.data());
-      axpy(n, -1., y_.data(), r_.data());
+      axpy(n, T(-1), y_.data(), r_.data());
       pmult(n, inv.data(), r_.data(), z_.data());
-      const double bcoef = a * (c / 2.) * (c / 2.);
-      a = 1. / (dd - bcoef);
-      scal(n, bcoef, p_.data());
-      axpy(n, 1., z_.data(), p_.data());
-      axpy(n, a, p_.data(), y);
+      scal(n, (T)cb[i], p_.data());
+      axpy(n, T(1), z_.data(), p_.data());
+      axpy(n, (T)ca[i], p_.data(), y);
     }
   }
 
-  void apply(const double* x, double* y) override {
+  void apply(const T* x, T* y) override {
     if (saad) apply_saad(x, y);
     else apply_default(x, y);
   }
 
   // _algo1 (ChebyshevPreconditioner.h:286-360): r = D^-1 x, w = r / theta,
   // y = w, then order-1 steps of the three-term recurrence.
-  void apply_saad(const double* x, double* y) {
-    const double delta = (beta - alpha) / 2;
-    const double theta = (beta + alpha) / 2;
+  void apply_saad(const T* x, T* y) {
     pmult(n, inv.data(), x, r_.data());
-    const double sigma = theta / delta;
-    double rho_old = 1. / sigma;
-    double rho = rho_old;
     copy(n, r_.data(), w_.data());
-    scal(n, 1 / theta, w_.data());
+    scal(n, (T)inv_theta, w_.data());
     copy(n, w_.data(), y);
     for (int k = 1; k < order; ++k) {
       spmv(A, w_.data(), y_.data());
       pmult(n, inv.data(), y_.data(), y_.data());
-      axpy(n, -1., y_.data(), r_.data());
-      rho = 1. / (2 * sigma - rho_old);
-      scal(n, rho * rho_old, w_.data());
-      axpy(n, 2 * rho / delta, r_.data(), w_.data());
-      axpy(n, 1., w_.data(), y);
-      rho_old = rho;
+      axpy(n, T(-1), y_.data(), r_.data());
+      scal(n, (T)ca[k], w_.data());
+      axpy(n, (T)cb[k], r_.data(), w_.data());
+      axpy(n, T(1), w_.data(), y);
     }
   }
 };
 
 // ---------------------------------------------------------------- solvers
-void cg(const Csr& A, Precond& M, StopTest& it, const double* b, double* x) {
+template <class T>
+void cg(const CsrT<T>& A, Precond<T>& M, StopTest<T>& it, const T* b, T* x) {
   if (it.null_rhs()) return;
   const int n = A.n;
-  std::vector<double> p(n), z(n), q(n), r(n);
-  double rho = 0, rho1 = 0, alpha = 0;
+  std::vector<T> p(n), z(n), q(n), r(n);
+  T rho = 0, rho1 = 0, alpha = 0;
   copy(n, b, r.data());
   spmv(A, x, p.data());
-  axpy(n, -1., p.data(), r.data());
+  axpy(n, T(-1), p.data(), r.data());
 
   M.apply(r.data(), z.data());
   rho1 = vdot(n,r.data(), z.data());
@@ -472,15 +540,16 @@ void cg(const Csr& A, Precond& M, StopTest& it, const double* b, double* x) {
   }
 }
 
-void bicgstab(const Csr& A, Precond& M, StopTest& it, const double* b, double* x) {
+template <class T>
+void bicgstab(const CsrT<T>& A, Precond<T>& M, StopTest<T>& it, const T* b, T* x) {
   if (it.null_rhs()) return;
   const int n = A.n;
-  std::vector<double> p(n), phat(n), s(n), shat(n), t(n), v(n), r(n), r0(n);
-  double rho = 0, rho1 = 0, alpha = 0, beta = 0, omega = 0;
+  std::vector<T> p(n), phat(n), s(n), shat(n), t(n), v(n), r(n), r0(n);
+  T rho = 0, rho1 = 0, alpha = 0, beta = 0, omega = 0;
 
   copy(n, b, r.data());
   spmv(A, x, r0.data());
-  axpy(n, -1., r0.data(), r.data());
+  axpy(n, T(-1), r0.data(), r.data());
   copy(n, r.data(), r0.data());
   copy(n, r.data(), p.data());
   rho1 = vdot(n,r.data(), r0.data());
@@ -524,7 +593,7 @@ void bicgstab(const Csr& A, Precond& M, StopTest& it, const double* b, double* x
     beta = (rho1 / rho) * (alpha / omega);
     axpy(n, -omega, v.data(), p.data());
     scal(n, beta, p.data());
-    axpy(n, 1., r.data(), p.data());
+    axpy(n, T(1), r.data(), p.data());
     if (rho == 0) throw Breakdown{ORC_BD_RHO};
 
     M.apply(p.data(), phat.data());
@@ -629,13 +698,13 @@ int orc_aypx(int n, double a, double* y, const double* x) {
 
 // ILU(0) factor values, written into lu (nnz entries).
 int orc_ilu0_factor(int n, const int* rp, const int* ci, const double* v, double* lu) {
-  Ilu0 f(Csr{n, rp, ci, v});
+  Ilu0<double> f(Csr{n, rp, ci, v});
   std::copy(f.lu.begin(), f.lu.end(), lu);
   return ORC_OK;
 }
 
 int orc_ilu0_apply(int n, const int* rp, const int* ci, const double* v, const double* y, double* x) {
-  Ilu0 f(Csr{n, rp, ci, v});
+  Ilu0<double> f(Csr{n, rp, ci, v});
   f.apply(y, x);
   return ORC_OK;
 }
@@ -651,7 +720,7 @@ int orc_set_dot_mode(int mode, int tree_blocks) {
 // Chebyshev bounds (alpha = lambda_min estimate, beta = lambda_max estimate).
 int orc_cheb_bounds(int n, const int* rp, const int* ci, const double* v, double factor, int max_iter,
                     double* alpha, double* beta) {
-  Cheb c(Csr{n, rp, ci, v}, factor, 1, max_iter, g_cheb_saad, g_cheb_lanczos);
+  Cheb<double> c(Csr{n, rp, ci, v}, v, factor, 1, max_iter, g_cheb_saad, g_cheb_lanczos);
   *alpha = c.alpha;
   *beta = c.beta;
   return ORC_OK;
@@ -659,7 +728,7 @@ int orc_cheb_bounds(int n, const int* rp, const int* ci, const double* v, double
 
 int orc_cheb_apply(int n, const int* rp, const int* ci, const double* v, double factor, int order,
                    int max_iter, const double* x, double* y) {
-  Cheb c(Csr{n, rp, ci, v}, factor, order, max_iter, g_cheb_saad, g_cheb_lanczos);
+  Cheb<double> c(Csr{n, rp, ci, v}, v, factor, order, max_iter, g_cheb_saad, g_cheb_lanczos);
   c.apply(x, y);
   return ORC_OK;
 }
@@ -680,24 +749,24 @@ int orc_solve(int n, const int* rp, const int* ci, const double* v, const double
   g_dot_mode = o->dot_mode;
   g_tree_blocks = o->tree_blocks > 0 ? o->tree_blocks : 1184;
   Csr A{n, rp, ci, v};
-  Identity pid(n);
-  Diag* pd = nullptr;
-  Ilu0* pi = nullptr;
-  Cheb* pc = nullptr;
-  Precond* M = &pid;
+  Identity<double> pid(n);
+  Diag<double>* pd = nullptr;
+  Ilu0<double>* pi = nullptr;
+  Cheb<double>* pc = nullptr;
+  Precond<double>* M = &pid;
   switch (o->precond) {
     case ORC_PC_NONE: break;
-    case ORC_PC_DIAG: M = pd = new Diag(A); break;
-    case ORC_PC_ILU0: M = pi = new Ilu0(A); break;
+    case ORC_PC_DIAG: M = pd = new Diag<double>(A); break;
+    case ORC_PC_ILU0: M = pi = new Ilu0<double>(A); break;
     case ORC_PC_CHEB:
-      M = pc = new Cheb(A, o->poly_factor, o->poly_order, o->poly_factor_max_iter, o->cheb_saad != 0,
-                        o->cheb_lanczos != 0);
+      M = pc = new Cheb<double>(A, v, o->poly_factor, o->poly_order, o->poly_factor_max_iter, o->cheb_saad != 0,
+                                o->cheb_lanczos != 0);
       res->cheb_alpha = pc->alpha;
       res->cheb_beta = pc->beta;
       break;
     default: return ORC_ERR_BAD_ARG;
   }
-  StopTest it(n, b, o->tol, o->max_iter, hist, hist_cap);
+  StopTest<double> it(n, b, o->tol, o->max_iter, hist, hist_cap);
   int rc = ORC_OK;
   try {
     if (o->solver == ORC_SOLVER_CG) cg(A, *M, it, b, x);
@@ -717,6 +786,121 @@ int orc_solve(int n, const int* rp, const int* ci, const double* v, const double
   delete pi;
   delete pc;
   return rc;
+}
+
+// ---------------------------------------------------------------- FP32 pieces
+// y = A32 x in float (the FP64 values rounded), products and sums rounded apart.
+int orc_spmv32(int n, const int* rp, const int* ci, const float* v32, const float* x, float* y) {
+  spmv(CsrT<float>{n, rp, ci, v32}, x, y);
+  return ORC_OK;
+}
+
+// The device tree in float (FP32 dots of the mixed solver's inner solves).
+float orc_dot_tree32(int n, const float* x, const float* y, int max_blocks) { return tree_dot(n, x, y, max_blocks); }
+
+// ILU(0): the FP64 factor rounded to float, sweeps in float.
+int orc_ilu0_apply32(int n, const int* rp, const int* ci, const double* v, const float* y, float* x) {
+  Ilu0<float> f(Csr{n, rp, ci, v});
+  f.apply(y, x);
+  return ORC_OK;
+}
+
+// Chebyshev in float: bounds and coefficients in FP64 (dot order from
+// orc_set_dot_mode), application in float on the FP32 values.
+int orc_cheb_apply32(int n, const int* rp, const int* ci, const double* v, const float* v32, double factor, int order,
+                     int max_iter, const float* x, float* y) {
+  Cheb<float> c(Csr{n, rp, ci, v}, v32, factor, order, max_iter, g_cheb_saad, g_cheb_lanczos);
+  c.apply(x, y);
+  return ORC_OK;
+}
+
+// One refinement step at a time, as libab2's ab2_mixed_solve: r = b - A x and
+// ||r|| in FP64; stop below tol; inner FP32 solve of A32 d = float(r/||r||)
+// from d = 0; x += ||r|| d.  Stops without success after max_outer steps or
+// when a step does not reduce the true residual.
+int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const double* b, double* x,
+                    const orc_mixed_options* o, orc_mixed_result* res, double* hist, int hist_cap) {
+  if (!o || !res || n < 0) return ORC_ERR_BAD_ARG;
+  std::memset(res, 0, sizeof(*res));
+  g_dot_mode = o->dot_mode;
+  g_tree_blocks = o->tree_blocks > 0 ? o->tree_blocks : 1184;
+  const Csr A{n, rp, ci, v};
+  std::vector<float> v32(v, v + (n > 0 ? rp[n] : 0));
+  const CsrT<float> A32{n, rp, ci, v32.data()};
+  Identity<float> pid(n);
+  Diag<float>* pd = nullptr;
+  Ilu0<float>* pi = nullptr;
+  Cheb<float>* pc = nullptr;
+  Precond<float>* M = &pid;
+  switch (o->precond) {
+    case ORC_PC_NONE: break;
+    case ORC_PC_DIAG: M = pd = new Diag<float>(A); break;
+    case ORC_PC_ILU0: M = pi = new Ilu0<float>(A); break;
+    case ORC_PC_CHEB:
+      M = pc = new Cheb<float>(A, v32.data(), o->poly_factor, o->poly_order, o->poly_factor_max_iter,
+                               o->cheb_saad != 0, o->cheb_lanczos != 0);
+      break;
+    default: return ORC_ERR_BAD_ARG;
+  }
+  std::vector<double> r(n), ax(n);
+  std::vector<float> r32(n), d32(n);
+  const double bb = vdot(n, b, b);
+  int outer = 0, inner = 0, rc = ORC_OK;
+  bool ok = false;
+  double resid = 0.0;
+  auto push = [&](double val) {
+    if (hist && res->history_len < hist_cap) hist[res->history_len] = val;
+    res->history_len += 1;
+  };
+  if (bb == 0.0) {
+    ok = true;
+  } else {
+    const double nb = std::sqrt(bb);
+    double prev = INFINITY;
+    for (;;) {
+      spmv(A, x, ax.data());
+      for (int i = 0; i < n; ++i) r[i] = b[i] - ax[i];
+      const double rr = vdot(n, r.data(), r.data());
+      resid = std::sqrt(rr) / nb;
+      push(resid);
+      if (resid < o->tol) {
+        ok = true;
+        break;
+      }
+      if (outer >= o->max_outer || !(resid < prev) || rr == 0.0) {
+        rc = ORC_ERR_NOT_CONVERGED;
+        break;
+      }
+      prev = resid;
+      const double sc = 1.0 / std::sqrt(rr);
+      for (int i = 0; i < n; ++i) r32[i] = (float)(r[i] * sc);
+      std::fill(d32.begin(), d32.end(), 0.0f);
+      StopTest<float> it(n, r32.data(), (float)o->inner_tol, o->inner_max_iter, nullptr, 0);
+      try {
+        if (o->solver == ORC_SOLVER_CG) cg(A32, *M, it, r32.data(), d32.data());
+        else bicgstab(A32, *M, it, r32.data(), d32.data());
+      } catch (const Breakdown&) {
+        if (it.iter == 0) {
+          inner += it.iter;
+          rc = ORC_ERR_BREAKDOWN;
+          break;
+        }
+      }
+      inner += it.iter;
+      const double s = std::sqrt(rr);
+      for (int i = 0; i < n; ++i) x[i] = std::fma(s, (double)d32[i], x[i]);
+      ++outer;
+    }
+  }
+  res->succeeded = ok ? 1 : 0;
+  res->outer_iterations = outer;
+  res->inner_iterations = inner;
+  res->error = ok ? ORC_OK : rc;
+  res->true_residual = resid;
+  delete pd;
+  delete pi;
+  delete pc;
+  return ORC_OK;
 }
 
 // BEllPack layout with slice S (SYCLBEllPackMatrix.cc:70-88 computes the slice

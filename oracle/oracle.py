@@ -46,8 +46,21 @@ class Result(C.Structure):
                 ("cheb_beta", C.c_double), ("history_len", C.c_int)]
 
 
+class MixedOptions(C.Structure):
+    _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("tol", C.c_double), ("max_outer", C.c_int),
+                ("inner_tol", C.c_double), ("inner_max_iter", C.c_int), ("poly_factor", C.c_double),
+                ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int), ("cheb_saad", C.c_int),
+                ("cheb_lanczos", C.c_int), ("dot_mode", C.c_int), ("tree_blocks", C.c_int)]
+
+
+class MixedResult(C.Structure):
+    _fields_ = [("succeeded", C.c_int), ("outer_iterations", C.c_int), ("inner_iterations", C.c_int),
+                ("error", C.c_int), ("true_residual", C.c_double), ("history_len", C.c_int)]
+
+
 _DP = C.POINTER(C.c_double)
 _IP = C.POINTER(C.c_int)
+_FP = C.POINTER(C.c_float)
 
 
 def build() -> None:
@@ -99,6 +112,13 @@ def orc() -> C.CDLL:
         L.orc_aypx.argtypes = [C.c_int, C.c_double, _DP, _DP]
         L.orc_cheb_bounds.argtypes = [C.c_int, _IP, _IP, _DP, C.c_double, C.c_int, _DP, _DP]
         L.orc_ell_layout.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, _IP, _IP, _DP]
+        L.orc_spmv32.argtypes = [C.c_int, _IP, _IP, _FP, _FP, _FP]
+        L.orc_dot_tree32.argtypes = [C.c_int, _FP, _FP, C.c_int]
+        L.orc_dot_tree32.restype = C.c_float
+        L.orc_ilu0_apply32.argtypes = [C.c_int, _IP, _IP, _DP, _FP, _FP]
+        L.orc_cheb_apply32.argtypes = [C.c_int, _IP, _IP, _DP, _FP, C.c_double, C.c_int, C.c_int, _FP, _FP]
+        L.orc_mixed_solve.argtypes = [C.c_int, _IP, _IP, _DP, _DP, _DP, C.POINTER(MixedOptions),
+                                      C.POINTER(MixedResult), _DP, C.c_int]
         _orc = L
     return _orc
 
@@ -125,6 +145,10 @@ def _dp(a):
 
 def _ip(a):
     return a.ctypes.data_as(_IP)
+
+
+def _fp(a):
+    return a.ctypes.data_as(_FP)
 
 
 @dataclass
@@ -273,3 +297,67 @@ def ell_layout(row_ptr, cols, vals, slice_rows=32):
     ev = np.empty(stored)
     orc().orc_ell_layout(n, _ip(rp), _ip(ci), _dp(v), slice_rows, _ip(off), _ip(ec), _dp(ev))
     return off, ec, ev
+
+
+# ---------------------------------------------------------------- FP32 / mixed precision
+# No reference counterpart: the reference's arithmetic instantiated in float
+# (values rounded from FP64; preconditioner set-up in FP64, then rounded).
+
+def spmv32(row_ptr, cols, vals, x) -> np.ndarray:
+    rp, ci = _c(row_ptr, np.int32), _c(cols, np.int32)
+    v32, xx = _c(np.asarray(vals, np.float64).astype(np.float32), np.float32), _c(x, np.float32)
+    y = np.empty(rp.size - 1, dtype=np.float32)
+    orc().orc_spmv32(rp.size - 1, _ip(rp), _ip(ci), _fp(v32), _fp(xx), _fp(y))
+    return y
+
+
+def dot_tree32(x, y, tree_blocks: int) -> np.float32:
+    xx, yy = _c(x, np.float32), _c(y, np.float32)
+    return np.float32(orc().orc_dot_tree32(xx.size, _fp(xx), _fp(yy), tree_blocks))
+
+
+def ilu0_apply32(row_ptr, cols, vals, y) -> np.ndarray:
+    rp, ci, v, yy = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(y, np.float32)
+    out = np.empty(rp.size - 1, dtype=np.float32)
+    orc().orc_ilu0_apply32(rp.size - 1, _ip(rp), _ip(ci), _dp(v), _fp(yy), _fp(out))
+    return out
+
+
+def cheb_apply32(row_ptr, cols, vals, x, factor=0.0, order=3, max_iter=10, dot_mode=DOT_SEQUENTIAL,
+                 tree_blocks=1184, saad=False, lanczos=False) -> np.ndarray:
+    rp, ci, v = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64)
+    v32, xx = _c(v.astype(np.float32), np.float32), _c(x, np.float32)
+    out = np.empty(rp.size - 1, dtype=np.float32)
+    set_dot_mode(dot_mode, tree_blocks)
+    orc().orc_set_cheb_variant(int(saad), int(lanczos))
+    orc().orc_cheb_apply32(rp.size - 1, _ip(rp), _ip(ci), _dp(v), _fp(v32), factor, order, max_iter, _fp(xx),
+                           _fp(out))
+    return out
+
+
+@dataclass
+class MixedSolve:
+    x: np.ndarray
+    succeeded: bool
+    outer_iterations: int
+    inner_iterations: int
+    error: int
+    true_residual: float
+    history: np.ndarray
+
+
+def mixed_solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8, max_outer=20,
+                inner_tol=1e-4, inner_max_iter=1000, poly_factor=0.0, poly_order=3, poly_factor_max_iter=20,
+                cheb_saad=False, cheb_lanczos=False, dot_mode=DOT_SEQUENTIAL, tree_blocks=1184) -> MixedSolve:
+    """FP32 inner Krylov in FP64 refinement, as libab2's ab2_mixed_solve."""
+    rp, ci, v, bb = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(b, np.float64)
+    n = rp.size - 1
+    x = np.zeros(n) if x0 is None else _c(x0, np.float64).copy()
+    o = MixedOptions(SOLVER[solver], PRECOND[precond], tol, max_outer, inner_tol, inner_max_iter, poly_factor,
+                     poly_order, poly_factor_max_iter, int(cheb_saad), int(cheb_lanczos), dot_mode, tree_blocks)
+    r = MixedResult()
+    cap = max_outer + 2
+    hist = np.zeros(cap)
+    orc().orc_mixed_solve(n, _ip(rp), _ip(ci), _dp(v), _dp(bb), _dp(x), C.byref(o), C.byref(r), _dp(hist), cap)
+    return MixedSolve(x, bool(r.succeeded), r.outer_iterations, r.inner_iterations, r.error, r.true_residual,
+                      hist[:min(r.history_len, cap)].copy())

@@ -14,15 +14,20 @@
 
 namespace ab2_oracle {
 
-struct Csr {
+// T is double for the reference's algebra; float instantiations restate the
+// FP32 inner solves of the mixed-precision solver (same operations in float).
+template <class T>
+struct CsrT {
   int n;
   const int* rp;
   const int* ci;
-  const double* v;
+  const T* v;
 };
+using Csr = CsrT<double>;
 
 // dcol[i] = first position k in row i with col >= i (CSRStructInfo.h:291-309).
-inline std::vector<int> diag_offsets(const Csr& A) {
+template <class T>
+inline std::vector<int> diag_offsets(const CsrT<T>& A) {
   std::vector<int> d(A.n);
   for (int i = 0; i < A.n; ++i) {
     int k = A.rp[i];
@@ -32,9 +37,10 @@ inline std::vector<int> diag_offsets(const Csr& A) {
   return d;
 }
 
-inline void spmv(const Csr& A, const double* x, double* y) {
+template <class T>
+inline void spmv(const CsrT<T>& A, const T* x, T* y) {
   for (int i = 0; i < A.n; ++i) {
-    double acc = 0.0;
+    T acc = 0;
     for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) acc = acc + A.v[k] * x[A.ci[k]];
     y[i] = acc;
   }
@@ -43,21 +49,27 @@ inline void spmv(const Csr& A, const double* x, double* y) {
 // BLAS-1 as CBLAS kernels compute it on FMA hardware: axpy is one fma per
 // element; ddot is summed sequentially here (its order is implementation
 // defined; the GPU sums the same products in a fixed tree).
-inline double dot(int n, const double* x, const double* y) {
-  double s = 0.0;
+template <class T>
+inline T dot(int n, const T* x, const T* y) {
+  T s = 0;
   for (int i = 0; i < n; ++i) s = std::fma(x[i], y[i], s);
   return s;
 }
-inline void axpy(int n, double a, const double* x, double* y) {
+template <class T>
+inline void axpy(int n, T a, const T* x, T* y) {
   for (int i = 0; i < n; ++i) y[i] = std::fma(a, x[i], y[i]);
 }
-inline void scal(int n, double a, double* x) {
+template <class T>
+inline void scal(int n, T a, T* x) {
   for (int i = 0; i < n; ++i) x[i] = a * x[i];
 }
-inline void copy(int n, const double* x, double* y) { std::memcpy(y, x, sizeof(double) * (size_t)n); }
-inline void pmult(int n, const double* x, const double* y, double* w) {
+template <class T>
+inline void copy(int n, const T* x, T* y) {
+  std::memcpy(y, x, sizeof(T) * (size_t)n);
+}
+template <class T>
+inline void pmult(int n, const T* x, const T* y, T* w) {
   for (int i = 0; i < n; ++i) w[i] = x[i] * y[i];
 }
-
 
 }  // namespace ab2_oracle

@@ -134,3 +134,39 @@ def test_ell_layout_matches_csr():
         assert np.array_equal(ec[slots][: b - a], P.cols[a:b])
         assert np.array_equal(ev[slots][: b - a], P.vals[a:b])
         assert np.all(ev[slots][b - a:] == 0)
+
+
+# ----------------------------------------------------------------- mixed precision (no reference counterpart)
+@pytest.mark.parametrize("name,solver,pc", [("poisson16", "cg", "diag"), ("poisson16", "cg", "ilu0"),
+                                            ("convdiff_10x11x12", "bicgs", "ilu0"), ("ragged", "bicgs", "diag")])
+def test_mixed_refinement_restatement(name, solver, pc):
+    """The FP32-inner / FP64-refinement restatement reaches the FP64 tolerance,
+    each step cuts the true residual by about the inner tolerance, and the
+    result agrees with a plain FP64 solve."""
+    P = problems.get(name)
+    r = O.mixed_solve(P.row_ptr, P.cols, P.vals, P.b, solver=solver, precond=pc, tol=1e-10, inner_tol=1e-4)
+    assert r.succeeded and r.error == 0 and r.true_residual < 1e-10
+    assert r.history[0] == 1.0 and np.all(np.diff(r.history) < 0)
+    assert r.outer_iterations <= 4
+    x64 = O.solve(P.row_ptr, P.cols, P.vals, P.b, solver=solver, precond="ilu0", tol=1e-13, max_iter=5000).x
+    assert np.linalg.norm(r.x - x64) / np.linalg.norm(x64) < 1e-8
+
+
+def test_fp32_pieces_are_float_restatements():
+    """FP32 SpMV and tree dot equal the same sums done in numpy float32 with
+    the same order (row-sequential SpMV; the tree for the dot)."""
+    P = problems.get("diffusion12")
+    x = np.random.default_rng(1).uniform(-1, 1, P.n).astype(np.float32)
+    y = O.spmv32(P.row_ptr, P.cols, P.vals, x)
+    v32 = P.vals.astype(np.float32)
+    for i in range(0, P.n, 97):
+        acc = np.float32(0)
+        for k in range(P.row_ptr[i], P.row_ptr[i + 1]):
+            acc = np.float32(acc + np.float32(v32[k] * x[P.cols[k]]))
+        assert acc == y[i]
+    d = O.dot_tree32(x, x, 1184)
+    assert abs(float(d) - float(np.dot(x.astype(np.float64), x.astype(np.float64)))) < 1e-5 * float(d)
+    # FP32 ILU(0) application is close to the FP64 one
+    z32 = O.ilu0_apply32(P.row_ptr, P.cols, P.vals, x)
+    z64 = O.ilu0_apply(P.row_ptr, P.cols, P.vals, x.astype(np.float64))
+    assert np.max(np.abs(z32 - z64)) < 1e-5 * np.max(np.abs(z64))
