@@ -214,6 +214,110 @@ def reference_sample(P, method: str, iterations_hint: int | None, sample_iters=(
     return setup + per_iter * iters, setup, per_iter, sum(t for _, t in times)
 
 
+def timed_solve(torch, stream, make, run):
+    """One warm + one timed (set-up + solve) pass on the library's stream."""
+    obj = make()
+    run(obj)
+    obj.close()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    obj = make()
+    res = run(obj)
+    e1.record(stream)
+    e1.synchronize()
+    hist = obj.history() if hasattr(obj, "history") else None
+    obj.close()
+    return e0.elapsed_time(e1) / 1e3, res, hist
+
+
+MIXED_METHODS = {  # mixed-precision forms of the FP64 methods, same system, same 1e-8 true residual
+    "ilu0": dict(precond="ilu0"),
+    "jacobi": dict(precond="diag"),
+    "cheb3_saad_lanczos20": dict(precond="cheb", cheb_saad=True, cheb_lanczos=True, poly_order=3,
+                                 poly_factor_max_iter=20),
+}
+
+
+def mixed_section(abi, ctx, stream, A, P, b, x, methods, a):
+    """Mixed precision (FP32 inner Krylov, FP64 refinement): the 192^3
+    system to true relative residual 1e-8 beside each FP64 method, and the
+    128^3 convection-diffusion system (BiCGStab + ILU0 inner, 1e-10) with its
+    error against an FP64 BiCGStab solution."""
+    import torch
+
+    out = {"diffusion3d_192": {}, "note": "time = set-up + solve on the device (CUDA events); "
+                                         "speedups against the FP64 solver on the same system; errors "
+                                         "against an FP64 CG+ILU0 solution to 1e-12"}
+    x_fp64 = x.download()  # the FP64 headline solution (CG + ILU0, 1e-8)
+    S = abi.Solver(ctx, A, solver="cg", precond="ilu0", tol=1e-12, max_iter=a.max_iter)
+    ctx.assign(x, 0.0)
+    S.solve(b, x)
+    S.close()
+    x_ref = x.download()
+    out["fp64_cg_ilu0_1e-8_rel_error"] = float(np.linalg.norm(x_fp64 - x_ref) / np.linalg.norm(x_ref))
+    fp64_best = min(v["s"] for v in methods.values()) if methods else None
+    for m, kw in MIXED_METHODS.items():
+        def make(kw=kw):
+            return abi.Mixed(ctx, A, solver="cg", tol=1e-8, max_outer=20, inner_tol=1e-4, inner_max_iter=5000,
+                             use_graph=not a.host_loop, **kw)
+
+        def run(M):
+            ctx.assign(x, 0.0)
+            return M.solve(b, x)
+
+        t, st, hist = timed_solve(torch, stream, make, run)
+        xs = x.download()
+        entry = {"s": round(t, 5), "converged": bool(st.succeeded), "true_rel_residual": st.true_residual,
+                 "outer_iterations": st.outer_iterations, "inner_iterations": st.inner_iterations,
+                 "setup_ms": round(st.setup_ms, 3), "solve_ms": round(st.solve_ms, 3),
+                 "rel_error_vs_fp64_1e-12": float(np.linalg.norm(xs - x_ref) / np.linalg.norm(x_ref)),
+                 "residual_history": [float(h) for h in hist]}
+        if m in methods:
+            entry["speedup_vs_fp64_same_precond"] = round(methods[m]["s"] / t, 3)
+        if "ilu0" in methods:
+            entry["speedup_vs_fp64_cg_ilu0"] = round(methods["ilu0"]["s"] / t, 3)
+        if fp64_best:
+            entry["speedup_vs_fastest_fp64"] = round(fp64_best / t, 3)
+        out["diffusion3d_192"][m] = entry
+    ctx.assign(x, 0.0)
+
+    # 128^3 convection-diffusion, nonsymmetric: mixed BiCGStab + ILU0 to 1e-10 vs FP64 BiCGStab + ILU0.
+    n3 = 128 if a.n >= 128 else a.n
+    Q = abi.convdiff(n3, n3, n3, peclet=10.0, modes=8, seed=0)
+    AQ = ctx.matrix(Q.row_ptr, Q.cols, Q.vals, abi.FMT_CSR | abi.FMT_ELL | abi.FMT_F32)
+    bq, xq = ctx.vector(Q.b), ctx.vector(Q.n)
+
+    def run_q(S):
+        ctx.assign(xq, 0.0)
+        return S.solve(bq, xq)
+
+    t64, st64, _ = timed_solve(torch, stream, lambda: abi.Solver(ctx, AQ, solver="bicgs", precond="ilu0", tol=1e-10,
+                                                                 max_iter=5000, use_graph=not a.host_loop), run_q)
+    tm, stm, hist = timed_solve(torch, stream, lambda: abi.Mixed(ctx, AQ, solver="bicgs", precond="ilu0", tol=1e-10,
+                                                                 max_outer=20, inner_tol=1e-4, inner_max_iter=5000,
+                                                                 use_graph=not a.host_loop), run_q)
+    xm = xq.download()
+    # the FP64 BiCGStab solution the error is stated against: tightened to 1e-12
+    S = abi.Solver(ctx, AQ, solver="bicgs", precond="ilu0", tol=1e-12, max_iter=5000)
+    ctx.assign(xq, 0.0)
+    S.solve(bq, xq)
+    S.close()
+    x64 = xq.download()
+    out[f"convdiff3d_{n3}"] = {
+        "workload": f"convdiff3d_{n3}^3_peclet10_modes8_bicgstab_ilu0_tol1e-10", "rows": Q.n, "nnz": Q.nnz,
+        "mixed": {"s": round(tm, 5), "converged": bool(stm.succeeded), "true_rel_residual": stm.true_residual,
+                  "outer_iterations": stm.outer_iterations, "inner_iterations": stm.inner_iterations,
+                  "residual_history": [float(h) for h in hist],
+                  "rel_error_vs_fp64_bicgstab_1e-12": float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))},
+        "fp64": {"s": round(t64, 5), "converged": bool(st64.succeeded), "iterations": st64.iterations,
+                 "true_rel_residual": st64.true_residual},
+        "speedup": round(t64 / tm, 3)}
+    for o in (bq, xq, AQ):
+        o.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -226,6 +330,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-methods", action="store_true", help="time the headline method only")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurements")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Krylov loop from the host instead of the CUDA graph (same kernels; for "
                          "profilers that do not see kernels inside conditional graph nodes)")
@@ -276,7 +381,7 @@ def main():
     torch.cuda.set_device(local)
     ctx = abi.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
-    A = ctx.matrix(P.row_ptr, P.cols, P.vals, abi.FMT_CSR | abi.FMT_ELL)
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals, abi.FMT_CSR | abi.FMT_ELL | abi.FMT_F32)
     b = ctx.vector(P.b)
     x = ctx.vector(P.n)
 
@@ -335,6 +440,8 @@ def main():
                       "solve_ms": round(mst.solve_ms, 3),
                       "solver_gbs": round(mst.iterations * iteration_bytes(m, P.n, P.nnz) / (mst.solve_ms * 1e-3)
                                           / 1e9, 1)}
+
+    mixed = None if a.no_mixed else mixed_section(abi, ctx, stream, A, P, b, x, methods, a)
 
     pk, pk_kind = peaks()
     traffic = load_traffic()
@@ -420,7 +527,7 @@ def main():
                 "setup_ms": round(st.setup_ms, 3), "solve_ms": round(st.solve_ms, 3),
                 "solver_gbs": round(st.iterations * iteration_bytes(a.method, P.n, P.nnz) / (st.solve_ms * 1e-3)
                                     / 1e9, 1),
-                "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "methods": methods,
+                "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "methods": methods, "mixed": mixed,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     if world > 1:
