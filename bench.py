@@ -107,37 +107,21 @@ class Clocks:
 
 
 def dist_init():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    from alien_b200 import dist
 
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
+    return dist.init("nccl")
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
+    from alien_b200 import dist
 
-        dist.barrier()
+    dist.barrier(world)
 
 
 def max_over_ranks(world, value: float) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from alien_b200 import dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return dist.reduce_max(world, value)
 
 
 def spmv_bytes(info, n: int) -> int:
@@ -530,10 +514,9 @@ def main():
                 "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "methods": methods, "mixed": mixed,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
+    from alien_b200 import dist
 
-        dist.destroy_process_group()
+    dist.finish(world)
     return 0
 
 
