@@ -88,6 +88,26 @@ class MixedStatus(C.Structure):
                 ("solve_ms", C.c_double)]
 
 
+class BatchOptions(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_outer", C.c_int), ("inner_tol", C.c_double), ("inner_max_iter", C.c_int),
+                ("spmv_variant", C.c_int), ("cluster_size", C.c_int), ("threads", C.c_int), ("tune_iters", C.c_int)]
+
+
+class BatchTrial(C.Structure):
+    _fields_ = [("spmv_variant", C.c_int), ("cluster_size", C.c_int), ("threads", C.c_int), ("ms", C.c_float)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("nsys", C.c_int), ("rows", C.c_longlong), ("spmv_variant", C.c_int), ("cluster_size", C.c_int),
+                ("threads", C.c_int), ("tuned", C.c_int), ("tune_ms", C.c_double), ("setup_ms", C.c_double),
+                ("trials", C.c_int)]
+
+
+class BatchStatus(C.Structure):
+    _fields_ = [("systems_converged", C.c_int), ("max_outer", C.c_int), ("inner_total", C.c_longlong),
+                ("inner_max", C.c_int), ("max_residual", C.c_double), ("solve_ms", C.c_double)]
+
+
 class Problem(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("row_ptr", C.POINTER(C.c_int)), ("cols", C.POINTER(C.c_int)), ("vals", C.POINTER(C.c_double)),
@@ -158,6 +178,13 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_mixed_solve": (_I, [_P, _P, _P, C.POINTER(MixedStatus)]),
     "ab2_mixed_history": (_I, [_P, _DP, _I, _IP]),
     "ab2_mixed_destroy": (_I, [_P]),
+    "ab2_batch_options_default": (None, [C.POINTER(BatchOptions)]),
+    "ab2_batch_create": (_I, [_P, _P, _I, _IP, C.POINTER(BatchOptions), C.POINTER(_P)]),
+    "ab2_batch_solve": (_I, [_P, _P, _P, C.POINTER(BatchStatus)]),
+    "ab2_batch_results": (_I, [_P, _IP, _IP, _IP, _DP]),
+    "ab2_batch_get_info": (_I, [_P, C.POINTER(BatchInfo)]),
+    "ab2_batch_trials": (_I, [_P, C.POINTER(BatchTrial), _I]),
+    "ab2_batch_destroy": (_I, [_P]),
     "ab2_problem_poisson": (_I, [_I, _I, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_diffusion": (_I, [_I, _I, _I, _D, _D, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_convdiff": (_I, [_I, _I, _I, _D, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
@@ -561,6 +588,74 @@ class Mixed:
             pass
 
 
+@dataclass
+class BatchResult:
+    systems_converged: int
+    max_outer: int
+    inner_total: int
+    inner_max: int
+    max_residual: float
+    solve_ms: float
+
+
+class Batch:
+    """ab2_batch: independent systems (diagonal blocks of A, rows
+    sys_offsets[s]..sys_offsets[s+1]-1) solved in one persistent launch; A
+    needs FMT_F32.  cluster_size / threads / spmv_variant = 0 / 0 / SPMV_AUTO
+    let the autotuner pick."""
+
+    def __init__(self, ctx: Context, A: Matrix, sys_offsets, tol=1e-8, max_outer=20, inner_tol=1e-4,
+                 inner_max_iter=5000, spmv_variant=SPMV_AUTO, cluster_size=0, threads=0, tune_iters=8):
+        self.ctx, self.A = ctx, A
+        self.offsets = np.ascontiguousarray(sys_offsets, dtype=np.int32)
+        self.nsys = self.offsets.size - 1
+        o = BatchOptions()
+        lib().ab2_batch_options_default(C.byref(o))
+        o.tol, o.max_outer, o.inner_tol, o.inner_max_iter = tol, max_outer, inner_tol, inner_max_iter
+        o.spmv_variant, o.cluster_size, o.threads, o.tune_iters = spmv_variant, cluster_size, threads, tune_iters
+        h = _P()
+        ctx.check(lib().ab2_batch_create(ctx.h, A.h, self.nsys, _ip(self.offsets), C.byref(o), C.byref(h)),
+                  "batch_create")
+        self.h = h
+
+    def solve(self, b: Vector, x: Vector) -> BatchResult:
+        st = BatchStatus()
+        self.ctx.check(lib().ab2_batch_solve(self.h, b.h, x.h, C.byref(st)), "batch_solve")
+        return BatchResult(st.systems_converged, st.max_outer, st.inner_total, st.inner_max, st.max_residual,
+                           st.solve_ms)
+
+    def results(self):
+        conv = np.empty(self.nsys, dtype=np.int32)
+        outer = np.empty(self.nsys, dtype=np.int32)
+        inner = np.empty(self.nsys, dtype=np.int32)
+        res = np.empty(self.nsys)
+        self.ctx.check(lib().ab2_batch_results(self.h, _ip(conv), _ip(outer), _ip(inner), _dp(res)), "batch_results")
+        return conv.astype(bool), outer, inner, res
+
+    @property
+    def info(self) -> BatchInfo:
+        i = BatchInfo()
+        self.ctx.check(lib().ab2_batch_get_info(self.h, C.byref(i)), "batch_info")
+        return i
+
+    def trials(self) -> list[tuple[int, int, int, float]]:
+        n = self.info.trials
+        arr = (BatchTrial * max(n, 1))()
+        self.ctx.check(lib().ab2_batch_trials(self.h, arr, n), "batch_trials")
+        return [(t.spmv_variant, t.cluster_size, t.threads, t.ms) for t in arr[:n]]
+
+    def close(self):
+        if self.h:
+            lib().ab2_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---------------------------------------------------------------------------- problems
 @dataclass
 class CsrProblem:
@@ -620,3 +715,59 @@ def convdiff(nx, ny=None, nz=None, peclet=10.0, modes=8, seed=0) -> CsrProblem:
     if rc:
         raise AB2Error(rc, "ab2_problem_convdiff")
     return _take(p)
+
+
+@dataclass
+class BatchProblem:
+    """Independent systems stacked as one block-diagonal CSR matrix."""
+    problem: CsrProblem
+    sys_offsets: np.ndarray
+    dims: list  # (nx, ny, nz) of each system
+
+    @property
+    def nsys(self) -> int:
+        return self.sys_offsets.size - 1
+
+
+def batch_problem(nsys=512, min_rows=2000, max_rows=200000, seed=0, sigma=1.0, smooth=2.0) -> BatchProblem:
+    """nsys heterogeneous-diffusion systems (log10 k ~ smoothed N(0, sigma^2)),
+    each 2-D 5-point or 3-D 7-point by a seeded coin, row counts log-uniform in
+    [min_rows, max_rows] (grid side round(n^(1/d))), seed seed*100003 + s for
+    system s, stacked as the diagonal blocks of one CSR matrix."""
+    lib()
+    parts, dims = [], []
+    for s in range(nsys):
+        u0 = lib().ab2_rng_uniform(seed, 1000 + s, 0)
+        u1 = lib().ab2_rng_uniform(seed, 1000 + s, 1)
+        n = float(np.exp(np.log(min_rows) + u0 * (np.log(max_rows) - np.log(min_rows))))
+        if u1 < 0.5:
+            side = max(2, int(round(n ** 0.5)))
+            dim = (side, side, 1)
+        else:
+            side = max(2, int(round(n ** (1 / 3))))
+            dim = (side, side, side)
+        P = diffusion(*dim, sigma=sigma, smooth=smooth, seed=seed * 100003 + s)
+        parts.append(P)
+        dims.append(dim)
+    offs = np.zeros(nsys + 1, dtype=np.int64)
+    for s, P in enumerate(parts):
+        offs[s + 1] = offs[s] + P.n
+    nnz = sum(P.nnz for P in parts)
+    rp = np.empty(int(offs[-1]) + 1, dtype=np.int64)
+    ci = np.empty(nnz, dtype=np.int32)
+    vals = np.empty(nnz)
+    xt = np.empty(int(offs[-1]))
+    b = np.empty(int(offs[-1]))
+    e = 0
+    rp[0] = 0
+    for s, P in enumerate(parts):
+        o = int(offs[s])
+        rp[o + 1:o + P.n + 1] = P.row_ptr[1:].astype(np.int64) + e
+        ci[e:e + P.nnz] = P.cols + o
+        vals[e:e + P.nnz] = P.vals
+        xt[o:o + P.n] = P.x_true
+        b[o:o + P.n] = P.b
+        e += P.nnz
+    assert rp[-1] < 2**31
+    prob = CsrProblem(int(offs[-1]), rp.astype(np.int32), ci, vals, xt, b, None, (int(offs[-1]), 1, 1))
+    return BatchProblem(prob, offs.astype(np.int32), dims)

@@ -298,6 +298,67 @@ int ab2_mixed_solve(ab2_mixed* m, const ab2_vector* b, ab2_vector* x, ab2_mixed_
 int ab2_mixed_history(const ab2_mixed* m, double* res, int cap, int* len);
 int ab2_mixed_destroy(ab2_mixed* m);
 
+/* ------------------------------------------------------------------ batched systems
+ * Many independent systems of uneven sizes in ONE persistent launch.  No
+ * counterpart in the reference (its solvers take one system at a time); the
+ * per-system method is CG.h's Jacobi-PCG in FP32 inside FP64 refinement (as
+ * ab2_mixed).  The systems are the diagonal blocks of one block-diagonal
+ * matrix: system s is rows sys_offsets[s] .. sys_offsets[s+1]-1, and no row
+ * may reference a column outside its block.  The matrix must carry FP32
+ * values (AB2_FMT_F32).  A grid of thread-block clusters, as many as fit on
+ * the GPU at once, takes systems largest first from a ticket; a cluster
+ * solves its system to the per-system true relative residual tol, then takes
+ * the next.  The SpMV format, the CTAs per system (cluster size) and the
+ * threads per CTA are picked by timing every candidate on the batch at
+ * creation (the autotuner) unless fixed in the options. */
+typedef struct ab2_batch ab2_batch;
+
+typedef struct {
+  double tol;          /* per system: ||b_s - A_s x_s|| / ||b_s|| (FP64) */
+  int max_outer;       /* refinement steps per system */
+  double inner_tol;    /* FP32 inner CG: relative recursive residual, in (0, 1) */
+  int inner_max_iter;  /* FP32 iterations per refinement step */
+  int spmv_variant;    /* AB2_SPMV_AUTO (autotune), AB2_SPMV_ELL or AB2_SPMV_CSR_SCALAR */
+  int cluster_size;    /* CTAs per system: 0 (autotune), 1, 2, 4 or 8 */
+  int threads;         /* threads per CTA: 0 (autotune) or 64..1024, a multiple of 32 */
+  int tune_iters;      /* FP32 iterations per system in each autotuning trial (0: 8) */
+} ab2_batch_options;
+
+typedef struct {
+  int spmv_variant, cluster_size, threads;
+  float ms;            /* one trial: one refinement step of tune_iters iterations, every system */
+} ab2_batch_trial;
+
+typedef struct {
+  int nsys;
+  long long rows;
+  int spmv_variant, cluster_size, threads;  /* configuration in use */
+  int tuned;            /* 1 if the autotuner chose it */
+  double tune_ms;       /* time spent autotuning */
+  double setup_ms;      /* creation, autotuning included */
+  int trials;           /* number of autotuning trials (ab2_batch_trials) */
+} ab2_batch_info;
+
+typedef struct {
+  int systems_converged;
+  int max_outer;        /* most refinement steps any system took */
+  long long inner_total;/* FP32 iterations, all systems */
+  int inner_max;        /* most FP32 iterations any system took */
+  double max_residual;  /* largest final true relative residual */
+  double solve_ms;      /* device time of the solve (one launch) */
+} ab2_batch_status;
+
+void ab2_batch_options_default(ab2_batch_options* opts);
+int ab2_batch_create(ab2_context* ctx, const ab2_matrix* A, int nsys, const int* sys_offsets,
+                     const ab2_batch_options* opts, ab2_batch** batch);
+/* x holds the initial guesses on entry, the solutions on exit (FP64). */
+int ab2_batch_solve(ab2_batch* batch, const ab2_vector* b, ab2_vector* x, ab2_batch_status* status);
+/* per-system results of the last solve (host arrays of nsys; any may be NULL) */
+int ab2_batch_results(const ab2_batch* batch, int* converged, int* outer, int* inner, double* residual);
+int ab2_batch_get_info(const ab2_batch* batch, ab2_batch_info* info);
+int ab2_batch_trials(const ab2_batch* batch, ab2_batch_trial* trials, int cap);
+int ab2_batch_destroy(ab2_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -903,6 +903,145 @@ int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const 
   return ORC_OK;
 }
 
+// ---------------------------------------------------------------- batched systems
+// libab2's ab2_batch restated (batch.cu, no reference counterpart): per system,
+// FP32 Jacobi-PCG (CG.h's loop) inside FP64 refinement, every dot reduced the
+// way one thread-block cluster does it -- CTA c of `csize` owns rows
+// [lo_c, hi_c) (a contiguous 1/csize share), thread t of `threads` sums rows
+// lo_c + t, lo_c + t + threads, ... with fma, warps and then warp 0 reduce with
+// the shuffle tree, and the csize CTA partials are added in rank order.
+}  // extern "C"
+
+namespace {
+
+template <class T, int NC, class RowFn>
+void cluster_reduce(int s0, int s1, int csize, int threads, RowFn fn, T (&out)[NC]) {
+  const int chunk = (s1 - s0 + csize - 1) / csize;
+  const int nw = (threads + 31) / 32;
+  T total[NC];
+  for (int c = 0; c < NC; ++c) total[c] = T(0);
+  std::vector<T> acc((size_t)threads * NC);
+  for (int cta = 0; cta < csize; ++cta) {
+    const int lo = std::min(s1, s0 + cta * chunk), hi = std::min(s1, lo + chunk);
+    std::fill(acc.begin(), acc.end(), T(0));
+    for (int t = 0; t < threads; ++t)
+      for (int i = lo + t; i < hi; i += threads) fn(i, &acc[(size_t)t * NC]);
+    for (int c = 0; c < NC; ++c) {
+      T ws[32];
+      for (int w = 0; w < 32; ++w) {
+        if (w < nw) {
+          T lanes[32];
+          for (int l = 0; l < 32; ++l) lanes[l] = w * 32 + l < threads ? acc[(size_t)(w * 32 + l) * NC + c] : T(0);
+          ws[w] = warp_tree(lanes);
+        } else {
+          ws[w] = T(0);
+        }
+      }
+      total[c] = total[c] + warp_tree(ws);
+    }
+  }
+  for (int c = 0; c < NC; ++c) out[c] = total[c];
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_batch_solve(int n, const int* rp, const int* ci, const double* v, int nsys, const int* off, const double* b,
+                    double* x, double tol, int max_outer, double inner_tol, int inner_max_iter, int csize, int threads,
+                    int* conv_out, int* outer_out, int* inner_out, double* res_out) {
+  if (n < 0 || nsys < 0 || csize < 1 || threads < 32) return ORC_ERR_BAD_ARG;
+  const Csr A{n, rp, ci, v};
+  std::vector<float> v32(v, v + (n > 0 ? rp[n] : 0));
+  std::vector<int> d = diag_offsets(A);
+  std::vector<float> inv32(n);
+  for (int i = 0; i < n; ++i) inv32[i] = (float)(1.0 / v[d[i]]);
+  std::vector<double> r64(n);
+  std::vector<float> r(n), z(n), p(n), q(n), dd(n);
+  auto row64 = [&](int i) {  // row i of A x, product and sum rounded apart
+    double acc = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) acc = acc + v[k] * x[ci[k]];
+    return acc;
+  };
+  auto row32 = [&](int i, const float* y) {
+    float acc = 0.f;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) acc = acc + v32[k] * y[ci[k]];
+    return acc;
+  };
+  const float itol = (float)inner_tol;
+  for (int s = 0; s < nsys; ++s) {
+    const int s0 = off[s], s1 = off[s + 1];
+    double bb[1];
+    cluster_reduce<double, 1>(s0, s1, csize, threads, [&](int i, double* a) { a[0] = std::fma(b[i], b[i], a[0]); }, bb);
+    int outer = 0, inner = 0, converged = bb[0] == 0.0 ? 1 : 0;
+    double res = 0.0, prev = INFINITY;
+    while (!converged) {
+      double rr[1];
+      cluster_reduce<double, 1>(s0, s1, csize, threads, [&](int i, double* a) {
+        const double rv = b[i] - row64(i);
+        r64[i] = rv;
+        a[0] = std::fma(rv, rv, a[0]);
+      }, rr);
+      res = std::sqrt(rr[0]) / std::sqrt(bb[0]);
+      if (res < tol) {
+        converged = 1;
+        break;
+      }
+      if (outer >= max_outer || !(res < prev) || rr[0] == 0.0) break;
+      prev = res;
+      const double scale = 1.0 / std::sqrt(rr[0]);
+      float acc[2];
+      cluster_reduce<float, 2>(s0, s1, csize, threads, [&](int i, float* a) {
+        const float rv = (float)(r64[i] * scale);
+        const float zv = inv32[i] * rv;
+        r[i] = rv;
+        z[i] = zv;
+        p[i] = zv;
+        dd[i] = 0.f;
+        a[0] = std::fma(rv, zv, a[0]);
+        a[1] = std::fma(rv, rv, a[1]);
+      }, acc);
+      const float crit = itol * itol * acc[1];
+      float rho = acc[0];
+      int it = 0;
+      for (;;) {
+        float pq[1];
+        cluster_reduce<float, 1>(s0, s1, csize, threads, [&](int i, float* a) {
+          const float qv = row32(i, p.data());
+          q[i] = qv;
+          a[0] = std::fma(p[i], qv, a[0]);
+        }, pq);
+        if (pq[0] == 0.f) break;
+        const float alpha = rho / pq[0];
+        float rz[2];
+        cluster_reduce<float, 2>(s0, s1, csize, threads, [&](int i, float* a) {
+          dd[i] = std::fma(alpha, p[i], dd[i]);
+          const float rv = std::fma(-alpha, q[i], r[i]);
+          r[i] = rv;
+          const float zv = inv32[i] * rv;
+          z[i] = zv;
+          a[0] = std::fma(rv, zv, a[0]);
+          a[1] = std::fma(rv, rv, a[1]);
+        }, rz);
+        ++it;
+        if (rz[1] < crit || it >= inner_max_iter) break;
+        const float beta = rz[0] / rho;
+        rho = rz[0];
+        for (int i = s0; i < s1; ++i) p[i] = std::fma(beta, p[i], z[i]);
+      }
+      inner += it;
+      const double sr = std::sqrt(rr[0]);
+      for (int i = s0; i < s1; ++i) x[i] = std::fma(sr, (double)dd[i], x[i]);
+      ++outer;
+    }
+    if (conv_out) conv_out[s] = converged;
+    if (outer_out) outer_out[s] = outer;
+    if (inner_out) inner_out[s] = inner;
+    if (res_out) res_out[s] = res;
+  }
+  return ORC_OK;
+}
+
 // BEllPack layout with slice S (SYCLBEllPackMatrix.cc:70-88 computes the slice
 // widths; the value at (slice s, slot j, lane l) lives at off[s]*S + j*S + l,
 // padding uses column 0 and value 0).

@@ -117,6 +117,8 @@ def orc() -> C.CDLL:
         L.orc_dot_tree32.restype = C.c_float
         L.orc_ilu0_apply32.argtypes = [C.c_int, _IP, _IP, _DP, _FP, _FP]
         L.orc_cheb_apply32.argtypes = [C.c_int, _IP, _IP, _DP, _FP, C.c_double, C.c_int, C.c_int, _FP, _FP]
+        L.orc_batch_solve.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, _IP, _DP, _DP, C.c_double, C.c_int,
+                                      C.c_double, C.c_int, C.c_int, C.c_int, _IP, _IP, _IP, _DP]
         L.orc_mixed_solve.argtypes = [C.c_int, _IP, _IP, _DP, _DP, _DP, C.POINTER(MixedOptions),
                                       C.POINTER(MixedResult), _DP, C.c_int]
         _orc = L
@@ -361,3 +363,27 @@ def mixed_solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", to
     orc().orc_mixed_solve(n, _ip(rp), _ip(ci), _dp(v), _dp(bb), _dp(x), C.byref(o), C.byref(r), _dp(hist), cap)
     return MixedSolve(x, bool(r.succeeded), r.outer_iterations, r.inner_iterations, r.error, r.true_residual,
                       hist[:min(r.history_len, cap)].copy())
+
+
+@dataclass
+class BatchSolve:
+    x: np.ndarray
+    converged: np.ndarray
+    outer: np.ndarray
+    inner: np.ndarray
+    residual: np.ndarray
+
+
+def batch_solve(row_ptr, cols, vals, sys_offsets, b, x0=None, tol=1e-8, max_outer=20, inner_tol=1e-4,
+                inner_max_iter=5000, cluster_size=4, threads=256) -> BatchSolve:
+    """libab2's batched solver restated for a given cluster size and CTA width
+    (each fixes the reduction trees, hence the rounding)."""
+    rp, ci, v, bb = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(b, np.float64)
+    off = _c(sys_offsets, np.int32)
+    n, ns = rp.size - 1, off.size - 1
+    x = np.zeros(n) if x0 is None else _c(x0, np.float64).copy()
+    conv, outer, inner = (np.zeros(ns, dtype=np.int32) for _ in range(3))
+    res = np.zeros(ns)
+    orc().orc_batch_solve(n, _ip(rp), _ip(ci), _dp(v), ns, _ip(off), _dp(bb), _dp(x), tol, max_outer, inner_tol,
+                          inner_max_iter, cluster_size, threads, _ip(conv), _ip(outer), _ip(inner), _dp(res))
+    return BatchSolve(x, conv.astype(bool), outer, inner, res)
