@@ -737,8 +737,8 @@ def batch_problem(nsys=512, min_rows=2000, max_rows=200000, seed=0, sigma=1.0, s
     lib()
     parts, dims = [], []
     for s in range(nsys):
-        u0 = lib().ab2_rng_uniform(seed, 1000 + s, 0)
-        u1 = lib().ab2_rng_uniform(seed, 1000 + s, 1)
+        u0 = 0.5 * (lib().ab2_rng_uniform(seed, 1000 + s, 0) + 1.0)  # U[0, 1)
+        u1 = 0.5 * (lib().ab2_rng_uniform(seed, 1000 + s, 1) + 1.0)
         n = float(np.exp(np.log(min_rows) + u0 * (np.log(max_rows) - np.log(min_rows))))
         if u1 < 0.5:
             side = max(2, int(round(n ** 0.5)))

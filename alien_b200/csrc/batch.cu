@@ -254,13 +254,16 @@ struct ab2_batch {
 namespace ab2 {
 namespace {
 
+// Launches the persistent kernel over the first nsys_run systems of the
+// largest-first order.  Returns false (nothing launched) when not even one
+// cluster of this shape fits on the GPU.
 template <class V64, class V32>
-void launch_batch(ab2_batch* B, V64 a64, V32 a32, int csize, int threads, const double* b, double* x, int max_outer,
-                  int inner_max_iter) {
+bool launch_batch(ab2_batch* B, V64 a64, V32 a32, int csize, int threads, const double* b, double* x, int max_outer,
+                  int inner_max_iter, int nsys_run) {
   ab2_context* ctx = B->ctx;
   const size_t N = (size_t)B->A->n;
   BatchArgs<V64, V32> args;
-  args.nsys = B->nsys;
+  args.nsys = nsys_run;
   args.sys_off = B->d_off;
   args.order = B->d_order;
   args.ticket = B->d_ticket;
@@ -295,34 +298,43 @@ void launch_batch(ab2_batch* B, V64 a64, V32 a32, int csize, int threads, const 
   cfg.stream = ctx->stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  if (csize > 8)  // 16-CTA clusters are beyond the portable size
+    AB2_CUDA(cudaFuncSetAttribute(k_batch_cg<V64, V32>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   int nclusters = 0;
   AB2_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, (void*)k_batch_cg<V64, V32>, &cfg));
-  nclusters = std::max(1, std::min(nclusters, B->nsys));
+  if (nclusters < 1) return false;
+  nclusters = std::min(nclusters, nsys_run);
   cfg.gridDim = dim3((unsigned)(nclusters * csize));
   AB2_CUDA(cudaMemsetAsync(B->d_ticket, 0, sizeof(unsigned int), ctx->stream));
   AB2_CUDA(cudaLaunchKernelEx(&cfg, k_batch_cg<V64, V32>, args));
   check_launch(ctx, "batch_cg");
+  return true;
 }
 
-void run_batch(ab2_batch* B, int variant, int csize, int threads, const double* b, double* x, int max_outer,
-               int inner_max_iter) {
+bool run_batch(ab2_batch* B, int variant, int csize, int threads, const double* b, double* x, int max_outer,
+               int inner_max_iter, int nsys_run) {
+  bool ok = false;
   with_view<double>(B->A, variant, [&](auto v64) {
     with_view<float>(B->A, variant, [&](auto v32) {
       // both views in the same format (decltype of a captured parameter may be a reference)
       using V64 = std::remove_cv_t<std::remove_reference_t<decltype(v64)>>;
       using V32 = std::remove_cv_t<std::remove_reference_t<decltype(v32)>>;
       if constexpr (std::is_same_v<V64, EllView<double>> == std::is_same_v<V32, EllView<float>>) {
-        launch_batch(B, v64, v32, csize, threads, b, x, max_outer, inner_max_iter);
+        ok = launch_batch(B, v64, v32, csize, threads, b, x, max_outer, inner_max_iter, nsys_run);
       } else {
         throw Error{AB2_ERR_UNSUPPORTED, "batched solver: FP64 and FP32 values in different formats"};
       }
     });
   });
+  return ok;
 }
 
 // Times every candidate (SpMV format x CTAs per system x threads per CTA) on
-// the batch itself: one refinement step of `tune_iters` FP32 iterations for
-// every system from b = 1, and keeps the fastest.
+// the batch itself, from b = 1, and keeps the one with the smallest score =
+// (one refinement step of `tune_iters` FP32 iterations for every system: the
+// throughput of the launch) + (4 x tune_iters iterations of the largest system
+// alone: the latency of the long pole, which bounds a batch whose hardest
+// system needs many iterations).  Shapes that do not fit are skipped.
 void autotune(ab2_batch* B) {
   ab2_context* ctx = B->ctx;
   const int N = B->A->n;
@@ -336,7 +348,8 @@ void autotune(ab2_batch* B) {
   } else {
     variants.push_back(B->opts.spmv_variant);
   }
-  std::vector<int> csizes = B->opts.cluster_size ? std::vector<int>{B->opts.cluster_size} : std::vector<int>{1, 2, 4, 8};
+  std::vector<int> csizes =
+      B->opts.cluster_size ? std::vector<int>{B->opts.cluster_size} : std::vector<int>{1, 2, 4, 8, 16};
   std::vector<int> widths = B->opts.threads ? std::vector<int>{B->opts.threads} : std::vector<int>{256, 512};
   const int iters = B->opts.tune_iters > 0 ? B->opts.tune_iters : 8;
   float best = 1e30f;
@@ -347,15 +360,24 @@ void autotune(ab2_batch* B) {
   for (int v : variants)
     for (int c : csizes)
       for (int t : widths) {
-        op_fill(ctx, N, 0.0, x);
-        run_batch(B, v, c, t, b, x, 1, iters);  // warm
-        op_fill(ctx, N, 0.0, x);
-        AB2_CUDA(cudaEventRecord(e0, ctx->stream));
-        run_batch(B, v, c, t, b, x, 1, iters);
-        AB2_CUDA(cudaEventRecord(e1, ctx->stream));
-        AB2_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
-        AB2_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        bool fits = true;
+        for (int part = 0; part < 2 && fits; ++part) {
+          const int nrun = part == 0 ? B->nsys : 1;
+          const int it = part == 0 ? iters : 4 * iters;
+          op_fill(ctx, N, 0.0, x);
+          fits = run_batch(B, v, c, t, b, x, 1, it, nrun);  // warm
+          if (!fits) break;
+          op_fill(ctx, N, 0.0, x);
+          AB2_CUDA(cudaEventRecord(e0, ctx->stream));
+          run_batch(B, v, c, t, b, x, 1, it, nrun);
+          AB2_CUDA(cudaEventRecord(e1, ctx->stream));
+          AB2_CUDA(cudaEventSynchronize(e1));
+          float part_ms = 0;
+          AB2_CUDA(cudaEventElapsedTime(&part_ms, e0, e1));
+          ms += part_ms;
+        }
+        if (!fits) continue;
         B->trials.push_back(ab2_batch_trial{v, c, t, ms});
         if (ms < best) {
           best = ms;
@@ -405,7 +427,7 @@ int ab2_batch_create(ab2_context* ctx, const ab2_matrix* A, int nsys, const int*
   if (o->spmv_variant != AB2_SPMV_AUTO && o->spmv_variant != AB2_SPMV_ELL && o->spmv_variant != AB2_SPMV_CSR_SCALAR)
     return AB2_ERR_BAD_ARG;
   if (!(o->cluster_size == 0 || o->cluster_size == 1 || o->cluster_size == 2 || o->cluster_size == 4 ||
-        o->cluster_size == 8))
+        o->cluster_size == 8 || o->cluster_size == 16))
     return AB2_ERR_BAD_ARG;
   if (o->threads != 0 && (o->threads < 64 || o->threads > 1024 || o->threads % 32 != 0)) return AB2_ERR_BAD_ARG;
   if (!(o->tol >= 0) || !(o->inner_tol > 0 && o->inner_tol < 1) || o->max_outer < 0 || o->inner_max_iter < 1)
@@ -486,7 +508,9 @@ int ab2_batch_solve(ab2_batch* B, const ab2_vector* b, ab2_vector* x, ab2_batch_
   std::memset(status, 0, sizeof(*status));
   return guard(ctx, [&] {
     AB2_CUDA(cudaEventRecord(B->ev0, ctx->stream));
-    run_batch(B, B->variant, B->csize, B->threads, b->d, x->d, B->opts.max_outer, B->opts.inner_max_iter);
+    if (!run_batch(B, B->variant, B->csize, B->threads, b->d, x->d, B->opts.max_outer, B->opts.inner_max_iter,
+                   B->nsys))
+      throw Error{AB2_ERR_UNSUPPORTED, "batched solver: no cluster of the configured shape fits on this GPU"};
     AB2_CUDA(cudaEventRecord(B->ev1, ctx->stream));
     AB2_CUDA(cudaEventSynchronize(B->ev1));
     float ms = 0;

@@ -319,14 +319,15 @@ typedef struct {
   double inner_tol;    /* FP32 inner CG: relative recursive residual, in (0, 1) */
   int inner_max_iter;  /* FP32 iterations per refinement step */
   int spmv_variant;    /* AB2_SPMV_AUTO (autotune), AB2_SPMV_ELL or AB2_SPMV_CSR_SCALAR */
-  int cluster_size;    /* CTAs per system: 0 (autotune), 1, 2, 4 or 8 */
+  int cluster_size;    /* CTAs per system: 0 (autotune), 1, 2, 4, 8 or 16 (16: where the GPU places it) */
   int threads;         /* threads per CTA: 0 (autotune) or 64..1024, a multiple of 32 */
   int tune_iters;      /* FP32 iterations per system in each autotuning trial (0: 8) */
 } ab2_batch_options;
 
 typedef struct {
   int spmv_variant, cluster_size, threads;
-  float ms;            /* one trial: one refinement step of tune_iters iterations, every system */
+  float ms;            /* one trial's score: tune_iters FP32 iterations of every system plus
+                          4 x tune_iters of the largest system alone (throughput + long pole) */
 } ab2_batch_trial;
 
 typedef struct {

@@ -55,7 +55,8 @@ def test_batch_autotuner_picks_the_fastest_trial(ctx, batch):
     S, st, x = run(ctx, batch, tol=1e-8)
     info = S.info
     trials = S.trials()
-    assert info.tuned and len(trials) == info.trials == 2 * 4 * 2  # formats x cluster sizes x widths
+    # formats x cluster sizes (1, 2, 4, 8 always fit; 16 where the GPU places it) x widths
+    assert info.tuned and len(trials) == info.trials and 2 * 4 * 2 <= len(trials) <= 2 * 5 * 2
     best = min(trials, key=lambda t: t[3])
     assert (info.spmv_variant, info.cluster_size, info.threads) == best[:3]
     P = batch.problem
