@@ -108,6 +108,16 @@ class BatchStatus(C.Structure):
                 ("inner_max", C.c_int), ("max_residual", C.c_double), ("solve_ms", C.c_double)]
 
 
+class FcgOptions(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_iter", C.c_int), ("fallback_ratio", C.c_double)]
+
+
+class FcgStatus(C.Structure):
+    _fields_ = [("succeeded", C.c_int), ("iterations", C.c_int), ("gnn_steps", C.c_int), ("fallback_steps", C.c_int),
+                ("switched_at", C.c_int), ("error", C.c_int), ("true_residual", C.c_double),
+                ("solve_ms", C.c_double)]
+
+
 class Problem(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("row_ptr", C.POINTER(C.c_int)), ("cols", C.POINTER(C.c_int)), ("vals", C.POINTER(C.c_double)),
@@ -185,6 +195,17 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_batch_get_info": (_I, [_P, C.POINTER(BatchInfo)]),
     "ab2_batch_trials": (_I, [_P, C.POINTER(BatchTrial), _I]),
     "ab2_batch_destroy": (_I, [_P]),
+    "ab2_gnn_param_count": (_I, []),
+    "ab2_gnn_create": (_I, [_P, C.POINTER(C.c_float), C.c_ulonglong, C.POINTER(_P)]),
+    "ab2_gnn_get_params": (_I, [_P, C.POINTER(C.c_float)]),
+    "ab2_gnn_set_params": (_I, [_P, C.POINTER(C.c_float)]),
+    "ab2_gnn_bind": (_I, [_P, _P]),
+    "ab2_gnn_apply": (_I, [_P, _P, _P]),
+    "ab2_gnn_loss_grad": (_I, [_P, _P, _P, _DP, C.POINTER(C.c_float)]),
+    "ab2_gnn_train_step": (_I, [_P, _P, _P, _D, _DP]),
+    "ab2_gnn_destroy": (_I, [_P]),
+    "ab2_fcg_options_default": (None, [C.POINTER(FcgOptions)]),
+    "ab2_fcg_solve": (_I, [_P, _P, _P, _P, _P, _P, C.POINTER(FcgOptions), C.POINTER(FcgStatus)]),
     "ab2_problem_poisson": (_I, [_I, _I, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_diffusion": (_I, [_I, _I, _I, _D, _D, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_convdiff": (_I, [_I, _I, _I, _D, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
@@ -654,6 +675,96 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def _fp32(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Gnn:
+    """ab2_gnn: the learned preconditioner (network on the matrix graph),
+    trained on the GPU by libab2's own forward/backward kernels."""
+
+    def __init__(self, ctx: Context, params=None, seed: int = 0):
+        self.ctx = ctx
+        h = _P()
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        if p is not None and p.size != self.param_count():
+            raise ValueError(f"expected {self.param_count()} parameters, got {p.size}")
+        ctx.check(lib().ab2_gnn_create(ctx.h, None if p is None else _fp32(p), seed, C.byref(h)), "gnn_create")
+        self.h = h
+        self.A = None
+
+    @staticmethod
+    def param_count() -> int:
+        return lib().ab2_gnn_param_count()
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.empty(self.param_count(), dtype=np.float32)
+        self.ctx.check(lib().ab2_gnn_get_params(self.h, _fp32(out)), "gnn_get_params")
+        return out
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self.ctx.check(lib().ab2_gnn_set_params(self.h, _fp32(p)), "gnn_set_params")
+
+    def bind(self, A: Matrix):
+        self.ctx.check(lib().ab2_gnn_bind(self.h, A.h), "gnn_bind")
+        self.A = A
+
+    def apply(self, r: Vector, z: Vector):
+        self.ctx.check(lib().ab2_gnn_apply(self.h, r.h, z.h), "gnn_apply")
+
+    def loss_grad(self, r: Vector, e: Vector):
+        L = C.c_double()
+        g = np.empty(self.param_count(), dtype=np.float32)
+        self.ctx.check(lib().ab2_gnn_loss_grad(self.h, r.h, e.h, C.byref(L), _fp32(g)), "gnn_loss_grad")
+        return L.value, g
+
+    def train_step(self, r: Vector, e: Vector, lr: float = 1e-3) -> float:
+        L = C.c_double()
+        self.ctx.check(lib().ab2_gnn_train_step(self.h, r.h, e.h, lr, C.byref(L)), "gnn_train_step")
+        return L.value
+
+    def close(self):
+        if self.h:
+            lib().ab2_gnn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class FcgResult:
+    succeeded: bool
+    iterations: int
+    gnn_steps: int
+    fallback_steps: int
+    switched_at: int
+    error: int
+    true_residual: float
+    solve_ms: float
+
+
+def fcg_solve(ctx: Context, A: Matrix, b: Vector, x: Vector, gnn: Gnn | None = None, fallback: "Precond | None" = None,
+              tol: float = 1e-8, max_iter: int = 5000, fallback_ratio: float = 1.0) -> FcgResult:
+    """Flexible CG with the learned preconditioner, the fallback (ILU0)
+    taking over from the first network step that reduces ||r|| by less than
+    fallback_ratio."""
+    o = FcgOptions()
+    lib().ab2_fcg_options_default(C.byref(o))
+    o.tol, o.max_iter, o.fallback_ratio = tol, max_iter, fallback_ratio
+    st = FcgStatus()
+    ctx.check(lib().ab2_fcg_solve(ctx.h, A.h, gnn.h if gnn else None, fallback.h if fallback else None, b.h, x.h,
+                                  C.byref(o), C.byref(st)), "fcg_solve")
+    return FcgResult(bool(st.succeeded), st.iterations, st.gnn_steps, st.fallback_steps, st.switched_at, st.error,
+                     st.true_residual, st.solve_ms)
 
 
 # ---------------------------------------------------------------------------- problems

@@ -360,6 +360,63 @@ int ab2_batch_get_info(const ab2_batch* batch, ab2_batch_info* info);
 int ab2_batch_trials(const ab2_batch* batch, ab2_batch_trial* trials, int cap);
 int ab2_batch_destroy(ab2_batch* batch);
 
+/* ------------------------------------------------------------------ learned preconditioner
+ * No counterpart in the reference.  A message-passing network on the matrix
+ * graph maps a residual r to z ~ A^-1 r:
+ *   s = rms(r); h1 = relu(W0 [r_i/s, log(a_ii)/10] + b0)                     (2 -> 64)
+ *   4 layers: m_i = sum_j sigmoid(u e_ij + c) h_j, e_ij = log|a_ij| - log a_ii,
+ *             h <- relu(W [h ; m] + b)                                       (128 -> 64)
+ *   z_i = s (wd . h_i + bd) / a_ii
+ * Weights are kept in FP32 for training and used as BF16 in the dense layers
+ * (tensor cores, FP32 accumulation); activations are stored in BF16.
+ * Training (on the GPU, hand-written backward kernels, Adam): pairs (r, e) of
+ * a residual and the error it leaves, loss (z-e)^T A (z-e) / e^T A e.
+ * Parameters: ab2_gnn_param_count() floats in the order W0 (64x2), b0, W1..W4
+ * (64x128 each, row = output), b1..b4, u1..u4, c1..c4, wd, bd.  The matrix must
+ * have a positive diagonal and a structurally symmetric pattern. */
+typedef struct ab2_gnn ab2_gnn;
+
+int ab2_gnn_param_count(void);
+/* params: NULL for a seeded He-style initialisation */
+int ab2_gnn_create(ab2_context* ctx, const float* params, unsigned long long seed, ab2_gnn** gnn);
+int ab2_gnn_get_params(const ab2_gnn* gnn, float* params);
+int ab2_gnn_set_params(ab2_gnn* gnn, const float* params);
+/* Reads the graph features of A and sizes the activation buffers (A must outlive the binding). */
+int ab2_gnn_bind(ab2_gnn* gnn, const ab2_matrix* A);
+int ab2_gnn_apply(ab2_gnn* gnn, const ab2_vector* r, ab2_vector* z);   /* z = network(r), r != z */
+/* loss of one (r, e) pair and its gradient (grad: host array of param_count floats, or NULL) */
+int ab2_gnn_loss_grad(ab2_gnn* gnn, const ab2_vector* r, const ab2_vector* e, double* loss, float* grad);
+/* one Adam step (beta1 0.9, beta2 0.999) on one pair; loss before the step */
+int ab2_gnn_train_step(ab2_gnn* gnn, const ab2_vector* r, const ab2_vector* e, double lr, double* loss);
+int ab2_gnn_destroy(ab2_gnn* gnn);
+
+/* Flexible CG (Polak-Ribiere beta: the preconditioner may change between
+ * steps) with the network as preconditioner; the fallback preconditioner
+ * (ILU(0)) takes over, for the rest of the solve, from the first network step
+ * that reduces ||r|| by less than the factor fallback_ratio (1.0: a step that
+ * does not reduce it at all).  gnn = NULL: flexible CG with the fallback only.
+ * Stops when ||r|| / ||b|| < tol (the true residual is reported after). */
+typedef struct {
+  double tol;
+  int max_iter;
+  double fallback_ratio;
+} ab2_fcg_options;
+
+typedef struct {
+  int succeeded;
+  int iterations;
+  int gnn_steps;        /* preconditioner applications by the network */
+  int fallback_steps;   /* ... by the fallback */
+  int switched_at;      /* iteration where the fallback took over, -1 if it did not */
+  int error;            /* AB2_OK, AB2_ERR_NOT_CONVERGED, AB2_ERR_BREAKDOWN, AB2_ERR_TIMEOUT */
+  double true_residual;
+  double solve_ms;
+} ab2_fcg_status;
+
+void ab2_fcg_options_default(ab2_fcg_options* opts);
+int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* gnn, const ab2_precond* fallback,
+                  const ab2_vector* b, ab2_vector* x, const ab2_fcg_options* opts, ab2_fcg_status* status);
+
 #ifdef __cplusplus
 }
 #endif
