@@ -1,15 +1,20 @@
 // gnn.cu -- the learned preconditioner: a message-passing network on the
 // matrix graph, its training kernels, and flexible CG with ILU(0) fallback.
 // No counterpart in the reference; the network is defined (and checked) by
-// oracle/gnn_oracle.py:
-//   s = rms(r); x0_i = [r_i/s, log(a_ii)/10]; h1 = relu(W0 x0 + b0)            (2 -> 64)
-//   4 x { g_ij = sigmoid(u e_ij + c), e_ij = log|a_ij| - log a_ii ;
+// oracle/gnn_oracle.py.  It works on the diagonal-scaled system
+// D^-1/2 A D^-1/2, so neither inputs nor outputs carry the coefficients'
+// orders of magnitude:
+//   xr_i = r_i / sqrt(a_ii), s = rms(xr); x0_i = [xr_i/s, log(a_ii)/10]
+//   h1 = relu(W0 x0 + b0)                                                      (2 -> 64)
+//   4 x { g_ij = sigmoid(u e_ij + c), e_ij = log|a_ij| - (log a_ii + log a_jj)/2 ;
 //         m_i = sum_j g_ij h_j ; h <- relu(W [h; m] + b) }                       (128 -> 64)
-//   z_i = s (wd . h_i + bd) / a_ii
-// Activations are stored in BF16 ([n][64], 128 B per node); the dense layers
-// are BF16 x BF16 -> FP32 tensor-core MMAs (mma.sync m16n8k16; a warp computes
-// 16 nodes x 64 outputs over K = 128); aggregation is a warp per node with two
-// features per lane.  Training: hand-written backward kernels (loss
+//   z_i = s (wd . h5_i + bd + ws x0_i) / sqrt(a_ii)       (ws: the Jacobi skip)
+// Activations are stored in BF16 ([n][64], 128 B per node).  Each layer is
+// one fused kernel: neighbour gather, BF16 x BF16 -> FP32 tensor-core MMAs
+// (mma.sync m16n8k16; a warp computes 16 nodes x 64 outputs over K = 128) and
+// the bias/relu epilogue; the first layer recomputes h1 from x0 instead of
+// reading it, the last one applies the decoder in its epilogue, so inference
+// moves about 2 x 128 B per node and layer.  Training: hand-written backward kernels (loss
 // (z-e)^T A (z-e) / e^T A e on (residual, error) pairs), per-block partial
 // sums reduced in a fixed order (deterministic), Adam on FP32 master weights
 // with BF16 copies for the forward.
@@ -43,7 +48,8 @@ constexpr int kOffU = kOffB + kLayers * kH;
 constexpr int kOffC = kOffU + kLayers;
 constexpr int kOffWd = kOffC + kLayers;
 constexpr int kOffBd = kOffWd + kH;
-constexpr int kParams = kOffBd + 1;
+constexpr int kOffWs = kOffBd + 1;
+constexpr int kParams = kOffWs + 1;
 
 typedef __nv_bfloat16 bf16;
 
@@ -67,21 +73,30 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], 
 }
 
 // ------------------------------------------------------------------ graph features
-// diag, 1/diag, log(diag)/10 per row; per CSR entry the edge feature
-// log|a_ij| - log a_ii (0 and flagged on the diagonal) and the position of the
-// transposed entry (the pattern must be structurally symmetric).
+// Per row: 1/sqrt(a_ii) and log(a_ii)/10; per CSR entry the edge feature
+// log|a_ij| - (log a_ii + log a_jj)/2 (the entry of D^-1/2 A D^-1/2) and the
+// position of the transposed entry (the pattern must be structurally
+// symmetric).  bad |= 1: a row without a positive diagonal; |= 2: no (j, i).
+__device__ __forceinline__ bool diag_of(int r, const int* __restrict__ rp, const int* __restrict__ ci,
+                                        const double* __restrict__ v, const int* __restrict__ dcol, double* d) {
+  const int dk = dcol[r];
+  if (dk < rp[r + 1] && ci[dk] == r && v[dk] > 0) {
+    *d = v[dk];
+    return true;
+  }
+  return false;
+}
+
 __global__ void k_gnn_prep(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
-                           const int* __restrict__ dcol, float* __restrict__ invd, float* __restrict__ logd10,
+                           const int* __restrict__ dcol, float* __restrict__ isd, float* __restrict__ logd10,
                            float* __restrict__ efeat, int* __restrict__ tidx, int* bad) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int dk = dcol[i];
-    const bool has_d = dk < rp[i + 1] && ci[dk] == i && v[dk] > 0;
-    if (!has_d) {
+    double d = 1.0;
+    if (!diag_of(i, rp, ci, v, dcol, &d)) {
       atomicOr(bad, 1);
       continue;
     }
-    const double d = v[dk];
-    invd[i] = (float)(1.0 / d);
+    isd[i] = (float)(1.0 / sqrt(d));
     logd10[i] = (float)(log(d) / 10.0);
     for (int k = rp[i]; k < rp[i + 1]; ++k) {
       const int j = ci[k];
@@ -90,7 +105,9 @@ __global__ void k_gnn_prep(int n, const int* __restrict__ rp, const int* __restr
         tidx[k] = -1;
         continue;
       }
-      efeat[k] = (float)(log(fabs(v[k])) - log(d));
+      double dj = 1.0;
+      if (!diag_of(j, rp, ci, v, dcol, &dj)) atomicOr(bad, 1);
+      efeat[k] = (float)(log(fabs(v[k])) - 0.5 * (log(d) + log(dj)));
       int t = -1;  // (j, i) in row j (columns sorted: binary search)
       int lo = rp[j], hi = rp[j + 1] - 1;
       while (lo <= hi) {
@@ -108,107 +125,324 @@ __global__ void k_gnn_prep(int n, const int* __restrict__ rp, const int* __restr
   }
 }
 
-// ------------------------------------------------------------------ forward
-// h1 = relu(W0 [r_i/s, logd10_i] + b0), one thread per node.
-__global__ void k_gnn_encode(int n, const double* __restrict__ r, const double* __restrict__ rr,
-                             const float* __restrict__ logd10, const float* __restrict__ P, bf16* __restrict__ h1) {
-  const double rms = sqrt(*rr / (double)max(n, 1));
-  const float inv_s = rms > 0 ? (float)(1.0 / rms) : 0.f;
+// The forward pass reads the graph as a padded neighbour table: per node nbw
+// (a multiple of 8) slots of (column, edge feature) in CSR order, -1 marking
+// padding -- one 32-byte load per 8 neighbours instead of a row-pointer load
+// followed by dependent column loads.
+__global__ void k_gnn_nbr(int n, const int* __restrict__ rp, const int* __restrict__ ci, const float* __restrict__ efeat,
+                          int nbw, int* __restrict__ nb_idx, float* __restrict__ nb_ef) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float x0 = (float)r[i] * inv_s, x1 = logd10[i];
-    unsigned* out = reinterpret_cast<unsigned*>(h1 + (size_t)i * kH);
-#pragma unroll 8
-    for (int j = 0; j < kH; j += 2) {
-      const float p0 = fmaf(P[kOffW0 + 2 * j], x0, fmaf(P[kOffW0 + 2 * j + 1], x1, P[kOffB0 + j]));
-      const float p1 = fmaf(P[kOffW0 + 2 * j + 2], x0, fmaf(P[kOffW0 + 2 * j + 3], x1, P[kOffB0 + j + 1]));
-      out[j / 2] = pack_bf16(fmaxf(p0, 0.f), fmaxf(p1, 0.f));
-    }
-  }
-}
-
-// m_i = sum_{j != i} sigmoid(u e_ij + c) h_j: a warp per node, lane = features 2l, 2l+1.
-__global__ void k_gnn_aggregate(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                const float* __restrict__ efeat, const float* __restrict__ P, int layer,
-                                const bf16* __restrict__ h, bf16* __restrict__ m) {
-  const int lane = threadIdx.x & 31;
-  const float u = P[kOffU + layer], c = P[kOffC + layer];
-  const unsigned* hv = reinterpret_cast<const unsigned*>(h);
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
-    float a0 = 0.f, a1 = 0.f;
+    int w = 0;
     for (int k = rp[i]; k < rp[i + 1]; ++k) {
-      const int j = ci[k];
-      if (j == i) continue;
-      const float g = sigmoidf(fmaf(u, efeat[k], c));
-      const float2 x = unpack_bf16(hv[(size_t)j * (kH / 2) + lane]);
-      a0 = fmaf(g, x.x, a0);
-      a1 = fmaf(g, x.y, a1);
+      if (ci[k] == i) continue;
+      nb_idx[(size_t)i * nbw + w] = ci[k];
+      nb_ef[(size_t)i * nbw + w] = efeat[k];
+      ++w;
     }
-    reinterpret_cast<unsigned*>(m)[(size_t)i * (kH / 2) + lane] = pack_bf16(a0, a1);
+    for (; w < nbw; ++w) {
+      nb_idx[(size_t)i * nbw + w] = -1;
+      nb_ef[(size_t)i * nbw + w] = 0.f;
+    }
   }
 }
 
-// h_out = relu(W [h ; m] + b) on tensor cores.  W (64 x 128, BF16) is staged
-// in shared memory with padded rows; a warp takes 16 nodes at a time.
-__global__ void __launch_bounds__(256) k_gnn_dense(int n, const bf16* __restrict__ h, const bf16* __restrict__ m,
-                                                   const bf16* __restrict__ W, const float* __restrict__ bias,
-                                                   bf16* __restrict__ hout) {
-  __shared__ __align__(16) bf16 Ws[kH * kWStride];
-  __shared__ float bs[kH];
-  for (int t = threadIdx.x; t < kH * kIn; t += blockDim.x) Ws[(t / kIn) * kWStride + t % kIn] = W[t];
-  if (threadIdx.x < kH) bs[threadIdx.x] = bias[threadIdx.x];
+// ------------------------------------------------------------------ forward
+// xr_i = r_i / sqrt(a_ii) (FP32) and s = rms(xr): s2[0] = s, s2[1] = 1/s (0 if s = 0).
+__global__ void __launch_bounds__(kThreads) k_gnn_scale(int n, const double* __restrict__ r, const float* __restrict__ isd,
+                                                        float* __restrict__ xr, double* partials, unsigned* counter,
+                                                        double* red_out, double* s2) {
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float t = (float)(r[i] * (double)isd[i]);
+    xr[i] = t;
+    acc[0] = fma((double)t, (double)t, acc[0]);
+  }
+  if (grid_reduce<1>(acc, partials, counter, red_out)) {
+    const double s = sqrt(red_out[0] / (double)max(n, 1));
+    s2[0] = s;
+    s2[1] = s > 0 ? 1.0 / s : 0.0;
+  }
+}
+
+// One message-passing layer, fused, on tensor cores for both of its products:
+//   m = G H_nb       (G: the 16 nodes' gates as a 16 x K BF16 matrix, one
+//                     nonzero run per row; H_nb: the K = 16 nbw neighbour rows)
+//   h_out = relu(W [h ; m] + b)
+// A warp takes 16 nodes at a time (persistent: it walks the tiles with a
+// stride).  The neighbour rows (padding slots zero-filled) are copied into the
+// warp's shared memory with cp.async, 8 lanes per 128-byte row so that every
+// copy instruction moves 4 whole rows.  The neighbour-table entries of the
+// warp's next tile are loaded while the current one computes, so a tile waits
+// on one memory latency.  Gates are computed one (node, slot) pair per lane
+// and shuffled straight into A fragments (G is block diagonal: row g of a
+// 16-column chunk is nonzero only where the chunk's pairs belong to node g).
+// The aggregation is K/16 mma.sync m16n8k16 steps (B from the neighbour rows
+// via ldmatrix.trans); its FP32 accumulators, rounded to BF16, are already in
+// the A-fragment layout of the dense layer's last four k-steps; the own rows'
+// fragments are read from global memory.  W (64 x 128, BF16) is staged once
+// per CTA and read with ldmatrix.  Epilogue: bias, relu, BF16, 128-byte row
+// stores through shared memory; LAST fuses the decoder
+// z_i = s (wd . h5_i + bd + ws x0_i) / sqrt(a_ii).
+// Optional stores (training): m_out, h_out (LAST).
+struct LayerArgs {
+  int n;
+  int nbw;              // neighbour slots per node (even, <= kMaxNbw)
+  const int* nb_idx;    // [n][nbw], -1 = padding
+  const float* nb_ef;   // [n][nbw] edge features
+  const float* P;       // FP32 parameters
+  const bf16* W;        // this layer's W in BF16 (64 x 128, row = output)
+  int layer;
+  const bf16* h_in;     // h_l
+  const float* xr;      // r_i / sqrt(a_ii)
+  const float* isd;
+  const double* s2;     // s, 1/s
+  bf16* m_out;          // m_l (or null)
+  bf16* h_out;          // h_{l+1} (or null when LAST)
+  double* z;            // LAST: the network's output
+};
+
+constexpr int kMaxNbw = 16;
+constexpr int kMaxRounds = kMaxNbw / 2;  // 32 (node, slot) pairs a round
+constexpr int kLayerWarps = 4;
+constexpr int kRowStride = kH + 8;       // bf16: 144-byte rows, conflict-free ldmatrix
+__host__ __device__ constexpr int agg_k(int nbw) { return 16 * nbw; }  // nbw even: a multiple of 32
+size_t layer_smem_bytes(int nbw) {
+  return sizeof(bf16) * ((size_t)kH * kWStride + (size_t)kLayerWarps * agg_k(nbw) * kRowStride) +
+         sizeof(float) * 2 * kH;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool fill) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(fill ? 16 : 0));
+}
+__device__ __forceinline__ void ldsm_x4(unsigned (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x4_t(unsigned (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
+  return make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
+}
+
+template <bool LAST>
+__global__ void __launch_bounds__(kLayerWarps * 32) k_gnn_layer(const LayerArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  bf16* Ws = reinterpret_cast<bf16*>(smem);
+  float* bs = reinterpret_cast<float*>(Ws + kH * kWStride);
+  float* wds = bs + kH;
+  for (int t = threadIdx.x; t < kH * kIn / 8; t += blockDim.x)
+    *reinterpret_cast<uint4*>(Ws + (t >> 4) * kWStride + (t & 15) * 8) = reinterpret_cast<const uint4*>(a.W)[t];
+  for (int t = threadIdx.x; t < kH; t += blockDim.x) {
+    bs[t] = a.P[kOffB + a.layer * kH + t];
+    wds[t] = a.P[kOffWd + t];
+  }
   __syncthreads();
-  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  const unsigned* hv = reinterpret_cast<const unsigned*>(h);
-  const unsigned* mv = reinterpret_cast<const unsigned*>(m);
-  for (int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile * 16 < n; tile += warps) {
-    const int r0 = tile * 16 + g, r1 = r0 + 8;
-    const bool ok0 = r0 < n, ok1 = r1 < n;
+  const unsigned kFull = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nbw = a.nbw, K = agg_k(nbw), rounds = K / 32;
+  bf16* Nb = reinterpret_cast<bf16*>(wds + kH) + warp * K * kRowStride;  // neighbour rows [K][kRowStride]
+  const float u = a.P[kOffU + a.layer], c = a.P[kOffC + a.layer];
+  const int g = lane >> 2, t = lane & 3;
+  const int lrow = (lane & 7) + ((lane >> 3) & 1) * 8, lcol = (lane >> 4) * 8;  // ldmatrix x4 lane address
+  const int wrow = (lane & 7) + (lane >> 4) * 8, wcol = ((lane >> 3) & 1) * 8;  // W fragments
+  const int ntiles = (a.n + 15) / 16;
+  const int stride = gridDim.x * kLayerWarps;
+  // neighbour-table entries of pair 32 r + lane of a tile
+  int pidx[kMaxRounds];
+  float pef[kMaxRounds];
+  auto fetch = [&](int tile) {
+#pragma unroll
+    for (int r = 0; r < kMaxRounds; ++r) {
+      pidx[r] = -1;
+      pef[r] = 0.f;
+      const long long e = (long long)tile * 16 * nbw + 32 * r + lane;
+      if (r < rounds && tile < ntiles && e < (long long)a.n * nbw) {
+        pidx[r] = a.nb_idx[e];
+        pef[r] = a.nb_ef[e];
+      }
+    }
+  };
+  fetch(blockIdx.x * kLayerWarps + warp);
+  for (int tile = blockIdx.x * kLayerWarps + warp; tile < ntiles; tile += stride) {
+    const int base = tile * 16;
+    // ---- neighbour rows into shared memory; gates of this lane's pairs
+    float gr[kMaxRounds];
+#pragma unroll
+    for (int r = 0; r < kMaxRounds; ++r) {
+      gr[r] = 0.f;
+      if (r < rounds) {
+        const int j = pidx[r];
+        if (j >= 0) gr[r] = bf16r(sigmoidf(fmaf(u, pef[r], c)));
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {  // rows 32 r + 4 q .. + 3, 8 lanes each
+          const int src = q * 4 + (lane >> 3);
+          const int jj = __shfl_sync(kFull, j, src);
+          cp_async16(Nb + (32 * r + src) * kRowStride + (lane & 7) * 8,
+                     a.h_in + (size_t)max(jj, 0) * kH + (lane & 7) * 8, jj >= 0);
+        }
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    fetch(tile + stride);  // the next tile's table entries, in flight during this tile
+    // own rows' A fragments (k-steps 0..3) straight from global memory
+    unsigned hA[4][4];
+    {
+      const unsigned* hv = reinterpret_cast<const unsigned*>(a.h_in);
+      const int r0 = base + g, r1 = r0 + 8;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        const int col = ks * 16 + 2 * t;
+        hA[ks][0] = r0 < a.n ? __ldg(hv + (((size_t)r0 * kH + col) >> 1)) : 0u;
+        hA[ks][1] = r1 < a.n ? __ldg(hv + (((size_t)r1 * kH + col) >> 1)) : 0u;
+        hA[ks][2] = r0 < a.n ? __ldg(hv + (((size_t)r0 * kH + col + 8) >> 1)) : 0u;
+        hA[ks][3] = r1 < a.n ? __ldg(hv + (((size_t)r1 * kH + col + 8) >> 1)) : 0u;
+      }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncwarp();
+    // ---- aggregation m = G H_nb on tensor cores
+    float accm[8][4];
+#pragma unroll
+    for (int nb = 0; nb < 8; ++nb) accm[nb][0] = accm[nb][1] = accm[nb][2] = accm[nb][3] = 0.f;
+#pragma unroll
+    for (int r = 0; r < kMaxRounds; ++r) {
+      if (r < rounds) {
+#pragma unroll
+        for (int hlf = 0; hlf < 2; ++hlf) {
+          const int k0 = 32 * r + 16 * hlf;
+          // pairs k0 + 2t (+1) and k0 + 2t + 8 (+1): gates from lanes 16 hlf + 2t + {0, 1, 8, 9}
+          const float g0 = __shfl_sync(kFull, gr[r], 16 * hlf + 2 * t);
+          const float g1 = __shfl_sync(kFull, gr[r], 16 * hlf + 2 * t + 1);
+          const float g8 = __shfl_sync(kFull, gr[r], 16 * hlf + 2 * t + 8);
+          const float g9 = __shfl_sync(kFull, gr[r], 16 * hlf + 2 * t + 9);
+          const int na = (k0 + 2 * t) / nbw, nc = (k0 + 2 * t + 8) / nbw;  // their nodes
+          const unsigned pa = pack_bf16(g0, g1), pc = pack_bf16(g8, g9);
+          const unsigned af[4] = {na == g ? pa : 0u, na == g + 8 ? pa : 0u, nc == g ? pc : 0u, nc == g + 8 ? pc : 0u};
+#pragma unroll
+          for (int n0 = 0; n0 < kH; n0 += 16) {
+            unsigned bf[4];
+            ldsm_x4_t(bf, Nb + (k0 + lrow) * kRowStride + n0 + lcol);
+            mma_bf16(accm[n0 / 8], af, bf[0], bf[1]);
+            mma_bf16(accm[n0 / 8 + 1], af, bf[2], bf[3]);
+          }
+        }
+      }
+    }
+    // m in BF16, already laid out as the A fragments of k-steps 4..7
+    unsigned mA[4][4];
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      mA[ks][0] = pack_bf16(accm[2 * ks][0], accm[2 * ks][1]);
+      mA[ks][1] = pack_bf16(accm[2 * ks][2], accm[2 * ks][3]);
+      mA[ks][2] = pack_bf16(accm[2 * ks + 1][0], accm[2 * ks + 1][1]);
+      mA[ks][3] = pack_bf16(accm[2 * ks + 1][2], accm[2 * ks + 1][3]);
+    }
+    // ---- dense layer [h ; m] W^T on tensor cores
     float acc[8][4];
 #pragma unroll
     for (int nb = 0; nb < 8; ++nb) acc[nb][0] = acc[nb][1] = acc[nb][2] = acc[nb][3] = 0.f;
 #pragma unroll
     for (int ks = 0; ks < 8; ++ks) {
-      const unsigned* src = ks < 4 ? hv : mv;
-      const int col = (ks & 3) * 16 + 2 * t;  // feature of a0 (bf16 index within the 64)
-      unsigned a[4];
-      a[0] = ok0 ? src[((size_t)r0 * kH + col) >> 1] : 0u;
-      a[1] = ok1 ? src[((size_t)r1 * kH + col) >> 1] : 0u;
-      a[2] = ok0 ? src[((size_t)r0 * kH + col + 8) >> 1] : 0u;
-      a[3] = ok1 ? src[((size_t)r1 * kH + col + 8) >> 1] : 0u;
-      const int k0 = ks * 16 + 2 * t;
 #pragma unroll
-      for (int nb = 0; nb < 8; ++nb) {
-        const bf16* wrow = Ws + (nb * 8 + g) * kWStride;
-        const unsigned b0 = *reinterpret_cast<const unsigned*>(wrow + k0);
-        const unsigned b1 = *reinterpret_cast<const unsigned*>(wrow + k0 + 8);
-        mma_bf16(acc[nb], a, b0, b1);
+      for (int n0 = 0; n0 < kH; n0 += 16) {
+        unsigned bf[4];
+        ldsm_x4(bf, Ws + (n0 + wrow) * kWStride + ks * 16 + wcol);
+        const unsigned(&af)[4] = ks < 4 ? hA[ks] : mA[ks - 4];
+        mma_bf16(acc[n0 / 8], af, bf[0], bf[1]);
+        mma_bf16(acc[n0 / 8 + 1], af, bf[2], bf[3]);
       }
     }
-    unsigned* out = reinterpret_cast<unsigned*>(hout);
+    __syncwarp();  // every lane is done with the neighbour rows: rows 0..31 stage the outputs
+    bf16* Ms = Nb;
+    bf16* Hs = Nb + 16 * kRowStride;
+    if (a.m_out) {
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        *reinterpret_cast<unsigned*>(Ms + g * kRowStride + ks * 16 + 2 * t) = mA[ks][0];
+        *reinterpret_cast<unsigned*>(Ms + (g + 8) * kRowStride + ks * 16 + 2 * t) = mA[ks][1];
+        *reinterpret_cast<unsigned*>(Ms + g * kRowStride + ks * 16 + 8 + 2 * t) = mA[ks][2];
+        *reinterpret_cast<unsigned*>(Ms + (g + 8) * kRowStride + ks * 16 + 8 + 2 * t) = mA[ks][3];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int idx = q * 32 + lane, row = idx >> 3, c8 = idx & 7;
+        if (base + row < a.n)
+          reinterpret_cast<uint4*>(a.m_out + (size_t)(base + row) * kH)[c8] =
+              *reinterpret_cast<const uint4*>(Ms + row * kRowStride + c8 * 8);
+      }
+    }
+    // ---- epilogue: bias, relu, BF16
+    float y0 = 0.f, y1 = 0.f;
+    unsigned o0[8], o1[8];
 #pragma unroll
     for (int nb = 0; nb < 8; ++nb) {
-      const int c = nb * 8 + 2 * t;
-      if (ok0) out[((size_t)r0 * kH + c) >> 1] = pack_bf16(fmaxf(acc[nb][0] + bs[c], 0.f), fmaxf(acc[nb][1] + bs[c + 1], 0.f));
-      if (ok1) out[((size_t)r1 * kH + c) >> 1] = pack_bf16(fmaxf(acc[nb][2] + bs[c], 0.f), fmaxf(acc[nb][3] + bs[c + 1], 0.f));
+      const int cc = nb * 8 + 2 * t;
+      const float h00 = bf16r(fmaxf(acc[nb][0] + bs[cc], 0.f)), h01 = bf16r(fmaxf(acc[nb][1] + bs[cc + 1], 0.f));
+      const float h10 = bf16r(fmaxf(acc[nb][2] + bs[cc], 0.f)), h11 = bf16r(fmaxf(acc[nb][3] + bs[cc + 1], 0.f));
+      o0[nb] = pack_bf16(h00, h01);
+      o1[nb] = pack_bf16(h10, h11);
+      if constexpr (LAST) {
+        y0 = fmaf(wds[cc], h00, fmaf(wds[cc + 1], h01, y0));
+        y1 = fmaf(wds[cc], h10, fmaf(wds[cc + 1], h11, y1));
+      }
     }
+    if (a.h_out) {
+#pragma unroll
+      for (int nb = 0; nb < 8; ++nb) {
+        *reinterpret_cast<unsigned*>(Hs + g * kRowStride + nb * 8 + 2 * t) = o0[nb];
+        *reinterpret_cast<unsigned*>(Hs + (g + 8) * kRowStride + nb * 8 + 2 * t) = o1[nb];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int idx = q * 32 + lane, row = idx >> 3, c8 = idx & 7;
+        if (base + row < a.n)
+          reinterpret_cast<uint4*>(a.h_out + (size_t)(base + row) * kH)[c8] =
+              *reinterpret_cast<const uint4*>(Hs + row * kRowStride + c8 * 8);
+      }
+    }
+    if constexpr (LAST) {
+      y0 += __shfl_xor_sync(kFull, y0, 1);
+      y0 += __shfl_xor_sync(kFull, y0, 2);
+      y1 += __shfl_xor_sync(kFull, y1, 1);
+      y1 += __shfl_xor_sync(kFull, y1, 2);
+      if (t == 0) {
+        const double s = a.s2[0], is = a.s2[1];
+        const float bd = a.P[kOffBd], ws = a.P[kOffWs];
+        const int r0 = base + g, r1 = r0 + 8;
+        if (r0 < a.n) a.z[r0] = s * (double)(y0 + bd + ws * (float)(a.xr[r0] * is)) * (double)a.isd[r0];
+        if (r1 < a.n) a.z[r1] = s * (double)(y1 + bd + ws * (float)(a.xr[r1] * is)) * (double)a.isd[r1];
+      }
+    }
+    __syncwarp();  // the staging rows are refilled by the next tile's copies
   }
 }
 
-// z_i = s (wd . h5_i + bd) / a_ii (FP64 out, for the solver).
-__global__ void k_gnn_decode(int n, const bf16* __restrict__ h5, const float* __restrict__ P,
-                             const float* __restrict__ invd, const double* __restrict__ rr, double* __restrict__ z) {
-  const double rms = sqrt(*rr / (double)max(n, 1));
-  const unsigned* hv = reinterpret_cast<const unsigned*>(h5);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float y = P[kOffBd];
-#pragma unroll 8
-    for (int j = 0; j < kH / 2; ++j) {
-      const float2 x = unpack_bf16(hv[(size_t)i * (kH / 2) + j]);
-      y = fmaf(P[kOffWd + 2 * j], x.x, y);
-      y = fmaf(P[kOffWd + 2 * j + 1], x.y, y);
-    }
-    z[i] = rms * (double)y * (double)invd[i];
+// h1 = relu(W0 x0 + b0), x0 = [xr / s, log(a_ii)/10]: 8 lanes per node, 8 features a lane.
+__global__ void __launch_bounds__(kThreads) k_gnn_encode(int n, const float* __restrict__ xr,
+                                                         const float* __restrict__ logd10, const double* __restrict__ s2,
+                                                         const float* __restrict__ P, bf16* __restrict__ h1) {
+  const int sub = threadIdx.x & 7;
+  const float inv_s = (float)s2[1];
+  float w0a[8], w0b[8], b0v[8];
+#pragma unroll
+  for (int f = 0; f < 8; ++f) {
+    w0a[f] = P[kOffW0 + 2 * (8 * sub + f)];
+    w0b[f] = P[kOffW0 + 2 * (8 * sub + f) + 1];
+    b0v[f] = P[kOffB0 + 8 * sub + f];
+  }
+  for (long long v = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 3; v < n;
+       v += ((long long)gridDim.x * blockDim.x) >> 3) {
+    const float x = xr[v] * inv_s, l = logd10[v];
+    float f8[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) f8[q] = fmaxf(fmaf(w0a[q], x, fmaf(w0b[q], l, b0v[q])), 0.f);
+    reinterpret_cast<uint4*>(h1 + (size_t)v * kH)[sub] = pack8(f8);
   }
 }
 
@@ -223,33 +457,38 @@ __global__ void k_gnn_wcopy(const float* __restrict__ P, bf16* __restrict__ Wb) 
 // k_gnn_reduce_partials adds them in block order (deterministic).
 constexpr int kWarpsPerBlock = 8;
 
-// dy_i = dz_i s / a_ii ; dh5_i = dy_i wd ; partials of grad wd (64) and bd (1).
-__global__ void __launch_bounds__(256) k_gnn_decode_bwd(int n, const double* __restrict__ dz, const double* __restrict__ rr,
-                                                        const float* __restrict__ invd, const bf16* __restrict__ h5,
-                                                        const float* __restrict__ P, float* __restrict__ dh,
-                                                        float* __restrict__ part) {
-  __shared__ float s_acc[kWarpsPerBlock][kH + 1];
+// dy_i = dz_i s / sqrt(a_ii) ; dh5_i = dy_i wd ; partials of grad wd (64), bd and ws.
+__global__ void __launch_bounds__(256) k_gnn_decode_bwd(int n, const double* __restrict__ dz, const double* __restrict__ s2,
+                                                        const float* __restrict__ isd, const float* __restrict__ xr,
+                                                        const bf16* __restrict__ h5, const float* __restrict__ P,
+                                                        float* __restrict__ dh, float* __restrict__ part) {
+  __shared__ float s_acc[kWarpsPerBlock][kH + 2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const double rms = sqrt(*rr / (double)max(n, 1));
+  const double s = s2[0];
+  const float is = (float)s2[1];
   const unsigned* hv = reinterpret_cast<const unsigned*>(h5);
   const float w0 = P[kOffWd + 2 * lane], w1 = P[kOffWd + 2 * lane + 1];
-  float g0 = 0.f, g1 = 0.f, gb = 0.f;
+  float g0 = 0.f, g1 = 0.f, gb = 0.f, gs = 0.f;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
-    const float dy = (float)(dz[i] * rms * (double)invd[i]);
+    const float dy = (float)(dz[i] * s * (double)isd[i]);
     const float2 x = unpack_bf16(hv[(size_t)i * (kH / 2) + lane]);
     g0 = fmaf(dy, x.x, g0);
     g1 = fmaf(dy, x.y, g1);
     gb += dy;
+    gs = fmaf(dy, xr[i] * is, gs);
     reinterpret_cast<float2*>(dh)[(size_t)i * (kH / 2) + lane] = make_float2(dy * w0, dy * w1);
   }
   s_acc[warp][2 * lane] = g0;
   s_acc[warp][2 * lane + 1] = g1;
-  if (lane == 0) s_acc[warp][kH] = gb;
+  if (lane == 0) {
+    s_acc[warp][kH] = gb;
+    s_acc[warp][kH + 1] = gs;
+  }
   __syncthreads();
-  for (int k = threadIdx.x; k <= kH; k += blockDim.x) {
-    float s = 0.f;
-    for (int w = 0; w < kWarpsPerBlock; ++w) s += s_acc[w][k];
-    part[(size_t)blockIdx.x * (kH + 1) + k] = s;
+  for (int k = threadIdx.x; k < kH + 2; k += blockDim.x) {
+    float v = 0.f;
+    for (int w = 0; w < kWarpsPerBlock; ++w) v += s_acc[w][k];
+    part[(size_t)blockIdx.x * (kH + 2) + k] = v;
   }
 }
 
@@ -397,17 +636,16 @@ __global__ void __launch_bounds__(256) k_gnn_wgrad(int n, const float* __restric
 }
 
 // Partials of grad W0 (64 x 2) and b0: dpre0 = dh1 (.) (h1 > 0), x0 recomputed.
-__global__ void __launch_bounds__(256) k_gnn_encode_bwd(int n, const double* __restrict__ r, const double* __restrict__ rr,
+__global__ void __launch_bounds__(256) k_gnn_encode_bwd(int n, const float* __restrict__ xr, const double* __restrict__ s2,
                                                         const float* __restrict__ logd10, const bf16* __restrict__ h1,
                                                         const float* __restrict__ dh, float* __restrict__ part) {
   __shared__ float s_acc[kWarpsPerBlock][3 * kH];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const double rms = sqrt(*rr / (double)max(n, 1));
-  const float inv_s = rms > 0 ? (float)(1.0 / rms) : 0.f;
+  const float inv_s = (float)s2[1];
   const unsigned* hv = reinterpret_cast<const unsigned*>(h1);
   float a[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // (W0[o][0], W0[o][1], b0[o]) for o = 2 lane, 2 lane + 1
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += (gridDim.x * blockDim.x) >> 5) {
-    const float x0 = (float)r[i] * inv_s, x1 = logd10[i];
+    const float x0 = xr[i] * inv_s, x1 = logd10[i];
     const float2 hh = unpack_bf16(hv[(size_t)i * (kH / 2) + lane]);
     const float2 d = reinterpret_cast<const float2*>(dh)[(size_t)i * (kH / 2) + lane];
     const float d0 = hh.x > 0.f ? d.x : 0.f, d1 = hh.y > 0.f ? d.y : 0.f;
@@ -455,6 +693,77 @@ __global__ void k_gnn_adam(int np, float* __restrict__ P, const float* __restric
   }
 }
 
+// ------------------------------------------------------------------ flexible CG
+// Scalars of the flexible CG loop, kept on the device so that one iteration
+// needs a single host read (of rr, for the stop and fallback decisions).
+struct FcgScalars {
+  double rz;     // r . z of the current direction
+  double pq;     // p . A p
+  double rr;     // r . r after the update
+  double beta;
+  int breakdown; // p . A p == 0
+};
+
+// alpha = rz / pq; x += alpha p; r_old = r; r -= alpha q; rr = r . r.
+__global__ void __launch_bounds__(kThreads) k_fcg_update(int n, const double* __restrict__ p, const double* __restrict__ q,
+                                                         double* __restrict__ x, double* __restrict__ r,
+                                                         double* __restrict__ r_old, FcgScalars* sc, double* partials,
+                                                         unsigned* counter, double* red_out) {
+  const double pq = sc->pq;
+  const bool ok = pq != 0.0;
+  const double alpha = ok ? sc->rz / pq : 0.0;
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double rv = r[i];
+    r_old[i] = rv;
+    if (ok) {
+      x[i] = fma(alpha, p[i], x[i]);
+      rv = fma(-alpha, q[i], rv);
+      r[i] = rv;
+    }
+    acc[0] = fma(rv, rv, acc[0]);
+  }
+  if (grid_reduce<1>(acc, partials, counter, red_out)) {
+    sc->rr = red_out[0];
+    if (!ok) sc->breakdown = 1;
+  }
+}
+
+// Polak-Ribiere: beta = z . (r - r_old) / rz_old; rz = z . r.
+__global__ void __launch_bounds__(kThreads) k_fcg_dots(int n, const double* __restrict__ z, const double* __restrict__ r,
+                                                       const double* __restrict__ r_old, FcgScalars* sc, double* partials,
+                                                       unsigned* counter, double* red_out) {
+  double acc[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double zi = z[i];
+    acc[0] = fma(zi, r[i], acc[0]);
+    acc[1] = fma(zi, r_old[i], acc[1]);
+  }
+  if (grid_reduce<2>(acc, partials, counter, red_out)) {
+    const double rz_old = sc->rz;
+    sc->beta = rz_old != 0.0 ? (red_out[0] - red_out[1]) / rz_old : 0.0;
+    sc->rz = red_out[0];
+  }
+}
+
+// first direction: rz = r . z (beta = 0, p = z follows)
+__global__ void __launch_bounds__(kThreads) k_fcg_rz(int n, const double* __restrict__ z, const double* __restrict__ r,
+                                                     FcgScalars* sc, double* partials, unsigned* counter,
+                                                     double* red_out) {
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] = fma(z[i], r[i], acc[0]);
+  if (grid_reduce<1>(acc, partials, counter, red_out)) {
+    sc->rz = red_out[0];
+    sc->beta = 0.0;
+  }
+}
+
+// p = z + beta p
+__global__ void k_fcg_dir(int n, const double* __restrict__ z, double* __restrict__ p, const FcgScalars* sc) {
+  const double beta = sc->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = fma(beta, p[i], z[i]);
+}
+
 }  // namespace
 }  // namespace ab2
 
@@ -471,11 +780,15 @@ struct ab2_gnn {
   // binding to a matrix
   const ab2_matrix* A = nullptr;
   int n = 0;
-  float *d_invd = nullptr, *d_logd10 = nullptr, *d_efeat = nullptr;
+  float *d_isd = nullptr, *d_logd10 = nullptr, *d_efeat = nullptr;
   int* d_tidx = nullptr;
+  int nbw = 0;               // neighbour table: slots per node
+  int* d_nb_idx = nullptr;
+  float* d_nb_ef = nullptr;
   bf16* d_h = nullptr;       // h1..h5, n x 64 each
   bf16* d_m = nullptr;       // m1..m4
-  double* d_rr = nullptr;
+  float* d_xr = nullptr;     // r_i / sqrt(a_ii) of the last forward
+  double* d_s2 = nullptr;    // its scale s and 1/s
   float *d_dh = nullptr, *d_dh2 = nullptr, *d_dm = nullptr;
   double *d_z = nullptr, *d_d = nullptr, *d_Ad = nullptr, *d_Ae = nullptr;
   float* d_part = nullptr;
@@ -497,14 +810,18 @@ bf16* mbuf(ab2_gnn* G, int l) { return G->d_m + (size_t)l * G->n * kH; }
 
 void release_binding(ab2_gnn* G) {
   ab2_context* ctx = G->ctx;
-  for (void* p : {(void*)G->d_invd, (void*)G->d_logd10, (void*)G->d_efeat, (void*)G->d_tidx, (void*)G->d_h,
-                  (void*)G->d_m, (void*)G->d_rr, (void*)G->d_dh, (void*)G->d_dh2, (void*)G->d_dm, (void*)G->d_z,
-                  (void*)G->d_d, (void*)G->d_Ad, (void*)G->d_Ae, (void*)G->d_part, (void*)G->d_red})
+  for (void* p : {(void*)G->d_isd, (void*)G->d_logd10, (void*)G->d_efeat, (void*)G->d_tidx, (void*)G->d_h,
+                  (void*)G->d_m, (void*)G->d_xr, (void*)G->d_s2, (void*)G->d_dh, (void*)G->d_dh2, (void*)G->d_dm,
+                  (void*)G->d_z, (void*)G->d_d, (void*)G->d_Ad, (void*)G->d_Ae, (void*)G->d_part, (void*)G->d_red,
+                  (void*)G->d_nb_idx, (void*)G->d_nb_ef})
     dev_free(ctx, p);
-  G->d_invd = G->d_logd10 = G->d_efeat = nullptr;
+  G->d_nb_idx = nullptr;
+  G->d_nb_ef = nullptr;
+  G->nbw = 0;
+  G->d_isd = G->d_logd10 = G->d_efeat = G->d_xr = nullptr;
   G->d_tidx = nullptr;
   G->d_h = G->d_m = nullptr;
-  G->d_rr = nullptr;
+  G->d_s2 = nullptr;
   G->d_dh = G->d_dh2 = G->d_dm = nullptr;
   G->d_z = G->d_d = G->d_Ad = G->d_Ae = nullptr;
   G->d_part = G->d_red = nullptr;
@@ -512,24 +829,58 @@ void release_binding(ab2_gnn* G) {
   G->n = 0;
 }
 
-// z = network(r) (FP64 in and out).
-void gnn_forward(ab2_gnn* G, const double* r, double* z) {
+template <bool LAST>
+void launch_layer(ab2_context* ctx, const LayerArgs& la) {
+  static thread_local int configured_device = -1, per_sm = 0, per_sm_nbw = -1;  // per device and table width
+  if (configured_device != ctx->device) {
+    AB2_CUDA(cudaFuncSetAttribute(k_gnn_layer<LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)layer_smem_bytes(kMaxNbw)));
+    configured_device = ctx->device;
+    per_sm_nbw = -1;
+  }
+  if (per_sm_nbw != la.nbw) {
+    AB2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gnn_layer<LAST>, kLayerWarps * 32,
+                                                           layer_smem_bytes(la.nbw)));
+    per_sm = std::max(per_sm, 1);
+    per_sm_nbw = la.nbw;
+  }
+  const int ntiles = (la.n + 15) / 16;
+  const int grid = std::max(1, std::min((ntiles + kLayerWarps - 1) / kLayerWarps, per_sm * ctx->num_sms));
+  k_gnn_layer<LAST><<<grid, kLayerWarps * 32, layer_smem_bytes(la.nbw), ctx->stream>>>(la);
+  check_launch(ctx, "gnn_layer");
+}
+
+// z = network(r) (FP64 in and out).  training: keep m1..m4 and h5 for the
+// backward pass (h1..h4 are always written).
+void gnn_forward(ab2_gnn* G, const double* r, double* z, bool training = false) {
   ab2_context* ctx = G->ctx;
   const int n = G->n;
-  const ab2_matrix* A = G->A;
-  op_dot(ctx, n, r, r, G->d_rr, 0);
-  k_gnn_encode<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, r, G->d_rr, G->d_logd10, G->d_P, hbuf(G, 0));
+  RedSlot red = red_slot(ctx, 5);
+  k_gnn_scale<<<red_grid(ctx, n), kThreads, 0, ctx->stream>>>(n, r, G->d_isd, G->d_xr, red.partials, red.counter,
+                                                             red.result, G->d_s2);
+  check_launch(ctx, "gnn_scale");
+  k_gnn_encode<<<grid_for((long long)n * 8), kThreads, 0, ctx->stream>>>(n, G->d_xr, G->d_logd10, G->d_s2, G->d_P,
+                                                                         hbuf(G, 0));
   check_launch(ctx, "gnn_encode");
   for (int l = 0; l < kLayers; ++l) {
-    k_gnn_aggregate<<<warp_grid(ctx, n), 256, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, G->d_efeat, G->d_P, l,
-                                                                hbuf(G, l), mbuf(G, l));
-    check_launch(ctx, "gnn_aggregate");
-    k_gnn_dense<<<tile_grid(ctx, n), 256, 0, ctx->stream>>>(n, hbuf(G, l), mbuf(G, l), G->d_Wb + (size_t)l * kH * kIn,
-                                                            G->d_P + kOffB + l * kH, hbuf(G, l + 1));
-    check_launch(ctx, "gnn_dense");
+    LayerArgs la{};
+    la.n = n;
+    la.nbw = G->nbw;
+    la.nb_idx = G->d_nb_idx;
+    la.nb_ef = G->d_nb_ef;
+    la.P = G->d_P;
+    la.W = G->d_Wb + (size_t)l * kH * kIn;
+    la.layer = l;
+    la.h_in = hbuf(G, l);
+    la.xr = G->d_xr;
+    la.isd = G->d_isd;
+    la.s2 = G->d_s2;
+    la.m_out = training ? mbuf(G, l) : nullptr;
+    la.h_out = (training || l + 1 < kLayers) ? hbuf(G, l + 1) : nullptr;
+    la.z = l + 1 == kLayers ? z : nullptr;
+    if (l + 1 < kLayers) launch_layer<false>(ctx, la);
+    else launch_layer<true>(ctx, la);
   }
-  k_gnn_decode<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, hbuf(G, kLayers), G->d_P, G->d_invd, G->d_rr, z);
-  check_launch(ctx, "gnn_decode");
 }
 
 void reduce_into(ab2_gnn* G, int nb, int width, float* out) {
@@ -542,7 +893,7 @@ double gnn_loss_grad(ab2_gnn* G, const double* r, const double* e) {
   ab2_context* ctx = G->ctx;
   const ab2_matrix* A = G->A;
   const int n = G->n;
-  gnn_forward(G, r, G->d_z);
+  gnn_forward(G, r, G->d_z, true);
   op_copy(ctx, n, G->d_z, G->d_d);
   op_axpy(ctx, n, -1.0, e, G->d_d);
   op_spmv(ctx, A, G->d_d, G->d_Ad, AB2_SPMV_AUTO);
@@ -555,10 +906,10 @@ double gnn_loss_grad(ab2_gnn* G, const double* r, const double* e) {
   require(eAe > 0, "gnn training pair: e^T A e must be positive");
   op_scal(ctx, n, 2.0 / eAe, G->d_Ad);  // dz
   const int wg = warp_grid(ctx, n);
-  k_gnn_decode_bwd<<<wg, 256, 0, ctx->stream>>>(n, G->d_Ad, G->d_rr, G->d_invd, hbuf(G, kLayers), G->d_P, G->d_dh,
-                                                G->d_part);
+  k_gnn_decode_bwd<<<wg, 256, 0, ctx->stream>>>(n, G->d_Ad, G->d_s2, G->d_isd, G->d_xr, hbuf(G, kLayers), G->d_P,
+                                                G->d_dh, G->d_part);
   check_launch(ctx, "gnn_decode_bwd");
-  reduce_into(G, wg, kH + 1, G->d_grad + kOffWd);
+  reduce_into(G, wg, kH + 2, G->d_grad + kOffWd);
   float* dh = G->d_dh;
   float* dh2 = G->d_dh2;
   for (int l = kLayers - 1; l >= 0; --l) {
@@ -581,7 +932,7 @@ double gnn_loss_grad(ab2_gnn* G, const double* r, const double* e) {
     AB2_CUDA(cudaMemcpyAsync(G->d_grad + kOffC + l, G->d_red + 1, sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
     std::swap(dh, dh2);
   }
-  k_gnn_encode_bwd<<<wg, 256, 0, ctx->stream>>>(n, r, G->d_rr, G->d_logd10, hbuf(G, 0), dh, G->d_part);
+  k_gnn_encode_bwd<<<wg, 256, 0, ctx->stream>>>(n, G->d_xr, G->d_s2, G->d_logd10, hbuf(G, 0), dh, G->d_part);
   check_launch(ctx, "gnn_encode_bwd");
   reduce_into(G, wg, 3 * kH, G->d_grad + kOffW0);
   return dAd / eAe;
@@ -606,12 +957,14 @@ int ab2_gnn_create(ab2_context* ctx, const float* params, unsigned long long see
       std::copy(params, params + kParams, h.begin());
     } else {  // He-style normal initialisation
       std::mt19937_64 gen(seed);
-      std::normal_distribution<float> w0(0.f, 1.f), wl(0.f, std::sqrt(2.f / kIn)), wd(0.f, std::sqrt(1.f / kH));
+      std::normal_distribution<float> w0(0.f, 1.f), wl(0.f, std::sqrt(2.f / kIn)),
+          wd(0.f, 0.1f * std::sqrt(1.f / kH));  // small: the network starts close to its Jacobi skip
       for (int k = 0; k < 2 * kH; ++k) h[kOffW0 + k] = w0(gen);
       for (int k = 0; k < kLayers * kH * kIn; ++k) h[kOffW + k] = wl(gen);
       for (int k = 0; k < kLayers * kH; ++k) h[kOffB + k] = 0.01f;
       for (int l = 0; l < kLayers; ++l) h[kOffU + l] = 0.5f;
       for (int k = 0; k < kH; ++k) h[kOffWd + k] = wd(gen);
+      h[kOffWs] = 1.f;
     }
     G->d_P = dev_alloc<float>(ctx, kParams);
     G->d_grad = dev_alloc<float>(ctx, kParams);
@@ -661,13 +1014,14 @@ int ab2_gnn_bind(ab2_gnn* G, const ab2_matrix* A) {
     const int n = A->n;
     G->A = A;
     G->n = n;
-    G->d_invd = dev_alloc<float>(ctx, (size_t)n);
+    G->d_isd = dev_alloc<float>(ctx, (size_t)n);
     G->d_logd10 = dev_alloc<float>(ctx, (size_t)n);
     G->d_efeat = dev_alloc<float>(ctx, (size_t)A->nnz);
     G->d_tidx = dev_alloc<int>(ctx, (size_t)A->nnz);
     G->d_h = dev_alloc<bf16>(ctx, (size_t)(kLayers + 1) * n * kH);
     G->d_m = dev_alloc<bf16>(ctx, (size_t)kLayers * n * kH);
-    G->d_rr = dev_alloc<double>(ctx, 1);
+    G->d_xr = dev_alloc<float>(ctx, (size_t)n);
+    G->d_s2 = dev_alloc<double>(ctx, 2);
     G->d_dh = dev_alloc<float>(ctx, (size_t)n * kH);
     G->d_dh2 = dev_alloc<float>(ctx, (size_t)n * kH);
     G->d_dm = dev_alloc<float>(ctx, (size_t)n * kH);
@@ -680,13 +1034,27 @@ int ab2_gnn_bind(ab2_gnn* G, const ab2_matrix* A) {
     G->d_red = dev_alloc<float>(ctx, (size_t)(kH * kIn + kH));
     int* d_bad = dev_alloc<int>(ctx, 1);
     AB2_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), ctx->stream));
-    k_gnn_prep<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, A->d_v, A->d_dcol, G->d_invd,
+    k_gnn_prep<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, A->d_v, A->d_dcol, G->d_isd,
                                                           G->d_logd10, G->d_efeat, G->d_tidx, d_bad);
     check_launch(ctx, "gnn_prep");
     int bad = 0;
     AB2_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     AB2_CUDA(cudaStreamSynchronize(ctx->stream));
     dev_free(ctx, d_bad);
+    if (!bad) {
+      int maxlen = 0;  // off-diagonal entries of the longest row (every row has its diagonal)
+      for (int i = 0; i < n; ++i) maxlen = std::max(maxlen, A->h_rp[i + 1] - A->h_rp[i] - 1);
+      G->nbw = std::max(2, (maxlen + 1) / 2 * 2);
+      if (G->nbw > kMaxNbw) {
+        release_binding(G);
+        throw Error{AB2_ERR_UNSUPPORTED, "learned preconditioner: at most 16 off-diagonal entries a row"};
+      }
+      G->d_nb_idx = dev_alloc<int>(ctx, (size_t)n * G->nbw);
+      G->d_nb_ef = dev_alloc<float>(ctx, (size_t)n * G->nbw);
+      k_gnn_nbr<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, G->d_efeat, G->nbw, G->d_nb_idx,
+                                                           G->d_nb_ef);
+      check_launch(ctx, "gnn_nbr");
+    }
     if (bad) {
       release_binding(G);
       throw Error{AB2_ERR_BAD_ARG, bad & 1 ? "learned preconditioner needs a positive diagonal in every row"
@@ -753,7 +1121,8 @@ void ab2_fcg_options_default(ab2_fcg_options* o) {
 // Flexible CG (Polak-Ribiere beta, as the preconditioner changes between
 // steps): z = network(r) while the network's steps reduce ||r|| by at least
 // the factor fallback_ratio, the fallback preconditioner from the first step
-// that does not (for the rest of the solve).  No network: the fallback only.
+// that does not (for the rest of the solve, restarting the search direction
+// there).  No network: the fallback only.
 int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_precond* fallback,
                   const ab2_vector* b, ab2_vector* x, const ab2_fcg_options* o, ab2_fcg_status* st) {
   if (!ctx || !A || !b || !x || !o || !st || b->n != A->n || x->n != A->n) return AB2_ERR_BAD_ARG;
@@ -767,16 +1136,19 @@ int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_p
     cudaEvent_t e0, e1;
     AB2_CUDA(cudaEventCreate(&e0));
     AB2_CUDA(cudaEventCreate(&e1));
-    AB2_CUDA(cudaEventRecord(e0, ctx->stream));
     double* r = dev_alloc<double>(ctx, (size_t)n);
-    double* rp = dev_alloc<double>(ctx, (size_t)n);
+    double* r_old = dev_alloc<double>(ctx, (size_t)n);
     double* z = dev_alloc<double>(ctx, (size_t)n);
     double* p = dev_alloc<double>(ctx, (size_t)n);
     double* q = dev_alloc<double>(ctx, (size_t)n);
-    double* s = red_slot(ctx, 7).result;
+    FcgScalars* sc = dev_alloc<FcgScalars>(ctx, 1);
+    AB2_CUDA(cudaMemsetAsync(sc, 0, sizeof(FcgScalars), ctx->stream));
+    AB2_CUDA(cudaEventRecord(e0, ctx->stream));
+    RedSlot red = red_slot(ctx, 7);
+    const int rg = red_grid(ctx, n);
     auto dot = [&](const double* u, const double* v) {
-      op_dot(ctx, n, u, v, s, 7);
-      return read_scalar(ctx, s);
+      op_dot(ctx, n, u, v, red.result, 7);
+      return read_scalar(ctx, red.result);
     };
     bool use_gnn = G != nullptr;
     auto precond = [&](const double* in, double* out) {
@@ -801,36 +1173,47 @@ int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_p
     bool ok = nb == 0.0 || rn / nb < o->tol;
     if (!ok) {
       precond(r, z);
+      k_fcg_rz<<<rg, kThreads, 0, ctx->stream>>>(n, z, r, sc, red.partials, red.counter, red.result);
+      check_launch(ctx, "fcg_rz");
       op_copy(ctx, n, z, p);
-      double rz = dot(r, z);
       while (it < o->max_iter) {
         op_spmv(ctx, A, p, q, AB2_SPMV_AUTO);
-        const double pq = dot(p, q);
-        if (pq == 0.0) {
+        op_dot(ctx, n, p, q, &sc->pq, 7);
+        k_fcg_update<<<rg, kThreads, 0, ctx->stream>>>(n, p, q, x->d, r, r_old, sc, red.partials, red.counter,
+                                                       red.result);
+        check_launch(ctx, "fcg_update");
+        FcgScalars h;
+        AB2_CUDA(cudaMemcpyAsync(ctx->h_pinned, sc, sizeof(FcgScalars), cudaMemcpyDeviceToHost, ctx->stream));
+        AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+        std::memcpy(&h, ctx->h_pinned, sizeof(FcgScalars));
+        if (h.breakdown) {
           st->error = AB2_ERR_BREAKDOWN;
           break;
         }
-        const double alpha = rz / pq;
-        op_axpy(ctx, n, alpha, p, x->d);
-        op_copy(ctx, n, r, rp);
-        op_axpy(ctx, n, -alpha, q, r);
         ++it;
-        const double rn_new = std::sqrt(dot(r, r));
+        const double rn_new = std::sqrt(h.rr);
         if (rn_new / nb < o->tol) {
           ok = true;
           rn = rn_new;
           break;
         }
+        bool restart = false;
         if (use_gnn && fallback && rn_new > o->fallback_ratio * rn) {
-          use_gnn = false;  // ILU(0) takes over from here
+          use_gnn = false;  // ILU(0) takes over from here, with a fresh direction
+          restart = true;
           st->switched_at = it;
         }
         rn = rn_new;
         precond(r, z);
-        op_axpy(ctx, n, -1.0, r, rp);  // rp = r_old - r_new
-        const double beta = -dot(z, rp) / rz;
-        rz = dot(r, z);
-        op_aypx(ctx, n, beta, p, z);   // p = beta p + z
+        if (restart) {
+          k_fcg_rz<<<rg, kThreads, 0, ctx->stream>>>(n, z, r, sc, red.partials, red.counter, red.result);
+          check_launch(ctx, "fcg_rz");
+        } else {
+          k_fcg_dots<<<rg, kThreads, 0, ctx->stream>>>(n, z, r, r_old, sc, red.partials, red.counter, red.result);
+          check_launch(ctx, "fcg_dots");
+        }
+        k_fcg_dir<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, z, p, sc);  // beta = 0 after a restart
+        check_launch(ctx, "fcg_dir");
       }
     }
     AB2_CUDA(cudaEventRecord(e1, ctx->stream));
@@ -845,7 +1228,8 @@ int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_p
     st->iterations = it;
     st->solve_ms = ms;
     if (!ok && st->error == AB2_OK) st->error = AB2_ERR_NOT_CONVERGED;
-    for (double* v : {r, rp, z, p, q}) dev_free(ctx, v);
+    for (double* v : {r, r_old, z, p, q}) dev_free(ctx, v);
+    dev_free(ctx, sc);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   });

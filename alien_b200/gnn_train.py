@@ -14,6 +14,7 @@ backward and the optimiser all run on the device).
 from __future__ import annotations
 
 import argparse
+import json
 import time
 from pathlib import Path
 
@@ -60,11 +61,16 @@ def pairs(ctx: abi.Context, P: abi.CsrProblem, A: abi.Matrix, iterates=ITERATES)
 
 
 def train(ctx: abi.Context, net: abi.Gnn, fields: int = 64, side: int = 64, steps_per_pair: int = 4,
-          lr: float = 1e-3, seed: int = 1000, iterates=ITERATES, log_every: int = 0) -> list[float]:
-    """Trains `net` in place; returns the loss of every step."""
+          lr: float = 1e-3, seed: int = 1000, iterates=ITERATES, log_every: int = 0,
+          lr_final: float | None = None) -> list[float]:
+    """Trains `net` in place; returns the loss of every step.  The learning
+    rate decays geometrically from lr to lr_final over the fields."""
     hist: list[float] = []
     t0 = time.perf_counter()
+    lr0 = lr
     for f in range(fields):
+        if lr_final is not None and fields > 1:
+            lr = lr0 * (lr_final / lr0) ** (f / (fields - 1))
         P = field(side, seed + f)
         A = ctx.matrix(P.row_ptr, P.cols, P.vals)
         net.bind(A)
@@ -90,6 +96,7 @@ def main() -> int:
     ap.add_argument("--side", type=int, default=64)
     ap.add_argument("--steps-per-pair", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr-final", type=float, default=1e-4)
     ap.add_argument("--seed", type=int, default=1000)
     ap.add_argument("--init-seed", type=int, default=0)
     ap.add_argument("--out", default=str(Path(__file__).resolve().parent / "gnn_weights.npy"))
@@ -97,10 +104,19 @@ def main() -> int:
     ctx = abi.Context(0)
     net = abi.Gnn(ctx, None, seed=a.init_seed)  # libab2's seeded He-style initialisation
     t = time.perf_counter()
-    hist = train(ctx, net, a.fields, a.side, a.steps_per_pair, a.lr, a.seed, log_every=max(1, a.fields // 16))
+    hist = train(ctx, net, a.fields, a.side, a.steps_per_pair, a.lr, a.seed, log_every=max(1, a.fields // 16),
+                 lr_final=a.lr_final)
+    elapsed = time.perf_counter() - t
     np.save(a.out, net.params)
     n = max(1, len(hist) // 20)
-    print(f"trained {len(hist)} steps on {a.fields} fields of {a.side}^3 in {time.perf_counter() - t:.1f} s; "
+    chunks = np.array_split(np.asarray(hist), 20)
+    summary = {"fields": a.fields, "side": a.side, "field_seeds": [a.seed, a.seed + a.fields - 1],
+               "sigma": 1.5, "smoothing_length": [2.0, 8.0], "iterates": list(ITERATES),
+               "steps_per_pair": a.steps_per_pair, "steps": len(hist), "lr": [a.lr, a.lr_final], "optimizer": "adam",
+               "init_seed": a.init_seed, "seconds": round(elapsed, 1),
+               "loss_mean_by_twentieth": [round(float(c.mean()), 4) for c in chunks if c.size]}
+    Path(a.out).with_suffix(".json").write_text(json.dumps(summary, indent=1) + "\n")
+    print(f"trained {len(hist)} steps on {a.fields} fields of {a.side}^3 in {elapsed:.1f} s; "
           f"loss first {np.mean(hist[:n]):.4f} last {np.mean(hist[-n:]):.4f}; weights -> {a.out}")
     return 0
 

@@ -362,18 +362,22 @@ int ab2_batch_destroy(ab2_batch* batch);
 
 /* ------------------------------------------------------------------ learned preconditioner
  * No counterpart in the reference.  A message-passing network on the matrix
- * graph maps a residual r to z ~ A^-1 r:
- *   s = rms(r); h1 = relu(W0 [r_i/s, log(a_ii)/10] + b0)                     (2 -> 64)
- *   4 layers: m_i = sum_j sigmoid(u e_ij + c) h_j, e_ij = log|a_ij| - log a_ii,
+ * graph maps a residual r to z ~ A^-1 r, working on the diagonal-scaled
+ * system D^-1/2 A D^-1/2 (unit diagonal):
+ *   xr_i = r_i / sqrt(a_ii), s = rms(xr), x0_i = [xr_i / s, log(a_ii)/10]
+ *   h1 = relu(W0 x0 + b0)                                                    (2 -> 64)
+ *   4 layers: m_i = sum_j sigmoid(u e_ij + c) h_j,
+ *             e_ij = log|a_ij| - (log a_ii + log a_jj)/2,
  *             h <- relu(W [h ; m] + b)                                       (128 -> 64)
- *   z_i = s (wd . h_i + bd) / a_ii
+ *   z_i = s (wd . h_i + bd + ws x0_i[0]) / sqrt(a_ii)
+ * With wd = 0, bd = 0, ws = 1 the network is Jacobi (z = r / a_ii).
  * Weights are kept in FP32 for training and used as BF16 in the dense layers
  * (tensor cores, FP32 accumulation); activations are stored in BF16.
  * Training (on the GPU, hand-written backward kernels, Adam): pairs (r, e) of
  * a residual and the error it leaves, loss (z-e)^T A (z-e) / e^T A e.
  * Parameters: ab2_gnn_param_count() floats in the order W0 (64x2), b0, W1..W4
- * (64x128 each, row = output), b1..b4, u1..u4, c1..c4, wd, bd.  The matrix must
- * have a positive diagonal and a structurally symmetric pattern. */
+ * (64x128 each, row = output), b1..b4, u1..u4, c1..c4, wd, bd, ws.  The matrix
+ * must have a positive diagonal and a structurally symmetric pattern. */
 typedef struct ab2_gnn ab2_gnn;
 
 int ab2_gnn_param_count(void);
@@ -392,9 +396,10 @@ int ab2_gnn_destroy(ab2_gnn* gnn);
 
 /* Flexible CG (Polak-Ribiere beta: the preconditioner may change between
  * steps) with the network as preconditioner; the fallback preconditioner
- * (ILU(0)) takes over, for the rest of the solve, from the first network step
- * that reduces ||r|| by less than the factor fallback_ratio (1.0: a step that
- * does not reduce it at all).  gnn = NULL: flexible CG with the fallback only.
+ * (ILU(0)) takes over, for the rest of the solve and with a fresh search
+ * direction, from the first network step that reduces ||r|| by less than the
+ * factor fallback_ratio (1.0: a step that does not reduce it at all).
+ * gnn = NULL: flexible CG with the fallback only.
  * Stops when ||r|| / ||b|| < tol (the true residual is reported after). */
 typedef struct {
   double tol;

@@ -7,21 +7,27 @@ checked against finite differences of itself (float64) and against the GPU
 (BF16 operands, FP32 accumulation) within BF16 tolerances.
 
 Network (a message-passing network on the matrix graph, weights shared over
-nodes):
-  s      = sqrt(mean(r^2))                      residual scale
-  x0_i   = [r_i / s, log(a_ii) / 10]            node features
-  e_ij   = log|a_ij| - log(a_ii)                edge features (off-diagonal entries)
+nodes).  It works on the symmetrically diagonal-scaled system
+D^-1/2 A D^-1/2 (unit diagonal), so that neither its inputs nor its outputs
+carry the coefficients' orders of magnitude:
+  d_i    = sqrt(a_ii)
+  t_i    = r_i / d_i,  s = sqrt(mean(t^2))       scaled residual and its scale
+  x0_i   = [t_i / s, log(a_ii) / 10]            node features
+  e_ij   = log|a_ij| - (log a_ii + log a_jj)/2  edge features (off-diagonal entries)
   h1     = relu(W0 x0 + b0)                     W0: 64 x 2
   layer l = 1..4:
     g_ij = sigmoid(u_l e_ij + c_l)              edge gate
     m_i  = sum_j g_ij h_l[j]                    aggregation over the row's neighbours
     h_l+1 = relu(W_l [h_l ; m] + b_l)           W_l: 64 x 128 (tensor cores on the GPU)
-  y_i    = w_d . h5_i + b_d
-  z_i    = s * y_i / a_ii                       z = M(r), the preconditioned residual
+  y_i    = w_d . h5_i + b_d + w_s x0_i[0]       w_s: linear skip of the scaled residual
+  z_i    = s * y_i / d_i                        z = M(r), the preconditioned residual
+With w_d = 0, b_d = 0 and w_s = 1 the network is exactly Jacobi (z = r / a_ii);
+the initialisation starts close to that and training learns the correction.
 Loss for a (residual r, error e) pair: L = (z - e)^T A (z - e) / (e^T A e).
 
 `bf16=True` rounds what the GPU rounds: the dense layers' weights and inputs
-[h ; m] and the stored activations, round-to-nearest-even.
+[h ; m], the aggregation's gates and the stored activations,
+round-to-nearest-even (the backward pass treats the roundings as identity).
 """
 from __future__ import annotations
 
@@ -52,14 +58,15 @@ class Params:
     c: np.ndarray             # LAYERS
     wd: np.ndarray            # 64
     bd: float = 0.0
+    ws: float = 1.0
 
     def copy(self) -> "Params":
         return Params(self.W0.copy(), self.b0.copy(), [w.copy() for w in self.W], [v.copy() for v in self.b],
-                      self.u.copy(), self.c.copy(), self.wd.copy(), float(self.bd))
+                      self.u.copy(), self.c.copy(), self.wd.copy(), float(self.bd), float(self.ws))
 
     def flat(self) -> np.ndarray:
         return np.concatenate([self.W0.ravel(), self.b0, *[w.ravel() for w in self.W], *self.b, self.u, self.c,
-                               self.wd, [self.bd]]).astype(np.float64)
+                               self.wd, [self.bd, self.ws]]).astype(np.float64)
 
     @staticmethod
     def unflat(v: np.ndarray) -> "Params":
@@ -80,17 +87,18 @@ class Params:
         c = take(LAYERS)
         wd = take(H)
         bd = float(take(1)[0])
-        return Params(W0, b0, W, b, u, c, wd, bd)
+        ws = float(take(1)[0])
+        return Params(W0, b0, W, b, u, c, wd, bd, ws)
 
 
-def init_params(seed: int = 0) -> Params:
-    """He-style initialisation, seeded (the GPU trainer starts from the same values)."""
+def init_params(seed: int = 0, wd_scale: float = 1.0) -> Params:
+    """He-style initialisation, seeded; w_s = 1 (the Jacobi skip)."""
     rng = np.random.default_rng(seed)
     W0 = rng.normal(0, np.sqrt(2 / 2), (H, 2)).astype(np.float32)
     W = [rng.normal(0, np.sqrt(2 / (2 * H)), (H, 2 * H)).astype(np.float32) for _ in range(LAYERS)]
     return Params(W0, np.zeros(H, np.float32), W, [np.full(H, 0.01, np.float32) for _ in range(LAYERS)],
                   np.full(LAYERS, 0.5, np.float32), np.zeros(LAYERS, np.float32),
-                  (rng.normal(0, np.sqrt(1 / H), H)).astype(np.float32), 0.0)
+                  (wd_scale * rng.normal(0, np.sqrt(1 / H), H)).astype(np.float32), 0.0, 1.0)
 
 
 @dataclass
@@ -103,7 +111,7 @@ class Graph:
     diag: np.ndarray
     edge_row: np.ndarray      # row of each off-diagonal entry
     edge_col: np.ndarray
-    edge_feat: np.ndarray     # log|a_ij| - log a_ii
+    edge_feat: np.ndarray     # log|a_ij| - (log a_ii + log a_jj) / 2
 
     @staticmethod
     def from_csr(rp, ci, vals) -> "Graph":
@@ -114,7 +122,7 @@ class Graph:
         diag[rows[on]] = vals[on]
         off = ~on
         er, ec = rows[off], ci[off]
-        ef = np.log(np.abs(vals[off])) - np.log(diag[er])
+        ef = np.log(np.abs(vals[off])) - 0.5 * (np.log(diag[er]) + np.log(diag[ec]))
         return Graph(n, np.asarray(rp), np.asarray(ci), np.asarray(vals, np.float64), diag, er, ec, ef)
 
     def matvec(self, x):
@@ -132,15 +140,18 @@ def forward(p: Params, G: Graph, r: np.ndarray, bf16_round: bool = False):
     """Returns z and the activations the backward pass needs."""
     rd = (lambda a: bf16(a).astype(np.float64)) if bf16_round else (lambda a: np.asarray(a, np.float64))
     r = np.asarray(r, np.float64)
-    s = float(np.sqrt(np.mean(r * r)))
-    x0 = np.stack([r / s if s > 0 else np.zeros_like(r), np.log(G.diag) / 10.0], axis=1)
+    sd = np.sqrt(G.diag)
+    t = r / sd
+    s = float(np.sqrt(np.mean(t * t)))
+    x0 = np.stack([t / s if s > 0 else np.zeros_like(t), np.log(G.diag) / 10.0], axis=1)
     pre0 = x0 @ p.W0.astype(np.float64).T + p.b0
     h = rd(np.maximum(pre0, 0.0))
     cache = {"s": s, "x0": x0, "pre0": pre0, "h": [h], "m": [], "pre": [], "g": []}
     for l in range(LAYERS):
         g = _sig(float(p.u[l]) * G.edge_feat + float(p.c[l]))
+        gm = rd(g) if bf16_round else g  # the GPU's aggregation is a BF16 x BF16 -> FP32 tensor-core product
         m = np.zeros((G.n, H))
-        np.add.at(m, G.edge_row, g[:, None] * h[G.edge_col])
+        np.add.at(m, G.edge_row, gm[:, None] * h[G.edge_col])
         m = rd(m)
         inp = np.concatenate([h, m], axis=1)
         pre = inp @ rd(p.W[l]).T + p.b[l]
@@ -149,8 +160,8 @@ def forward(p: Params, G: Graph, r: np.ndarray, bf16_round: bool = False):
         cache["pre"].append(pre)
         cache["g"].append(g)
         cache["h"].append(h)
-    y = h @ p.wd.astype(np.float64) + p.bd
-    z = s * y / G.diag
+    y = h @ p.wd.astype(np.float64) + p.bd + p.ws * x0[:, 0]
+    z = s * y / sd
     return z, cache
 
 
@@ -170,10 +181,11 @@ def backward(p: Params, G: Graph, r, e, bf16_round: bool = False):
     L = float(d @ Ad) / eAe
     dz = 2.0 * Ad / eAe
     s = C["s"]
-    dy = dz * s / G.diag
+    dy = dz * s / np.sqrt(G.diag)
     h5 = C["h"][-1]
     gwd = h5.T @ dy
     gbd = float(dy.sum())
+    gws = float(dy @ C["x0"][:, 0])
     dh = np.outer(dy, p.wd.astype(np.float64))
     gW, gb, gu, gc = [None] * LAYERS, [None] * LAYERS, np.zeros(LAYERS), np.zeros(LAYERS)
     for l in reversed(range(LAYERS)):
@@ -196,4 +208,4 @@ def backward(p: Params, G: Graph, r, e, bf16_round: bool = False):
     dpre0 = dh * (C["pre0"] > 0)
     gW0 = dpre0.T @ C["x0"]
     gb0 = dpre0.sum(axis=0)
-    return L, Params(gW0, gb0, gW, gb, gu, gc, gwd, gbd)
+    return L, Params(gW0, gb0, gW, gb, gu, gc, gwd, gbd, gws)

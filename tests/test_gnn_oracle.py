@@ -18,7 +18,7 @@ def test_backward_matches_finite_differences():
     v, gv = p.flat(), grad.flat()
     scale = np.max(np.abs(gv))
     off = {"W0": 0, "b0": 128, "W": 192, "b": 192 + 4 * 8192, "u": 192 + 4 * 8192 + 256}
-    idx = list(rng.choice(v.size, 60, replace=False)) + [off["u"], off["u"] + 3, off["u"] + 4, v.size - 1, 5, 130]
+    idx = list(rng.choice(v.size, 60, replace=False)) + [off["u"], off["u"] + 3, off["u"] + 4, v.size - 2, v.size - 1, 5, 130]
     eps = 1e-6
     for k in idx:
         vp, vm = v.copy(), v.copy()
@@ -31,3 +31,19 @@ def test_backward_matches_finite_differences():
 def test_bf16_rounding_is_nearest_even():
     x = np.array([1.0, 1.00390625, 1.005859375, -3.0, 0.0], dtype=np.float32)
     assert np.array_equal(G.bf16(x), np.array([1.0, 1.0, 1.0078125, -3.0, 0.0], dtype=np.float32))
+
+
+def test_skip_alone_is_jacobi_and_scaling_invariant():
+    """w_d = 0, b_d = 0, w_s = 1 gives z = r / a_ii exactly; and the network
+    output is equivariant under a positive scaling of the residual."""
+    P = abi.diffusion(5, 4, 3, sigma=1.5, smooth=2.0, seed=5)
+    g = G.Graph.from_csr(P.row_ptr, P.cols, P.vals)
+    r = np.random.default_rng(1).normal(size=P.n)
+    p = G.init_params(0)
+    z, _ = G.forward(p, g, r)
+    z2, _ = G.forward(p, g, 1e6 * r)
+    np.testing.assert_allclose(z2, 1e6 * z, rtol=1e-12)
+    p.wd[:] = 0.0
+    p.bd, p.ws = 0.0, 1.0
+    z, _ = G.forward(p, g, r)
+    np.testing.assert_allclose(z, r / g.diag, rtol=1e-14)

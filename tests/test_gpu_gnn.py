@@ -18,8 +18,8 @@ pytestmark = pytest.mark.gpu
 
 def blocks(v):
     off = [0, 128, 192, 192 + 4 * 8192, 192 + 4 * 8192 + 256, 192 + 4 * 8192 + 260, 192 + 4 * 8192 + 264,
-           192 + 4 * 8192 + 328, v.size]
-    names = ["W0", "b0", "W", "b", "u", "c", "wd", "bd"]
+           192 + 4 * 8192 + 328, 192 + 4 * 8192 + 329, v.size]
+    names = ["W0", "b0", "W", "b", "u", "c", "wd", "bd", "ws"]
     return {nm: v[a:b] for nm, a, b in zip(names, off[:-1], off[1:])}
 
 
@@ -42,6 +42,22 @@ def test_forward_matches_oracle(ctx, system):
     zo, _ = G.forward(p, G.Graph.from_csr(P.row_ptr, P.cols, P.vals), r, bf16_round=True)
     assert np.linalg.norm(z - zo) / np.linalg.norm(zo) < 2e-2
     assert np.all(np.isfinite(z))
+
+
+def test_jacobi_skip_alone_is_jacobi(ctx, system):
+    """With the decoder's hidden weights and bias zero and the skip 1, the
+    network is z = r / a_ii (the scaled residual passes through FP32)."""
+    P, r, _ = system
+    p = G.init_params(2)
+    p.wd[:] = 0.0
+    p.bd, p.ws = 0.0, 1.0
+    net = abi.Gnn(ctx, p.flat().astype(np.float32))
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals)
+    net.bind(A)
+    vr, vz = ctx.vector(r), ctx.vector(P.n)
+    net.apply(vr, vz)
+    d = G.Graph.from_csr(P.row_ptr, P.cols, P.vals).diag
+    np.testing.assert_allclose(vz.download(), r / d, rtol=1e-6, atol=0)
 
 
 def test_gradient_matches_oracle(ctx, system):
@@ -82,4 +98,10 @@ def test_training_reduces_loss_and_fcg_converges(ctx):
     x2 = ctx.vector(P.n)
     base = abi.fcg_solve(ctx, A, b, x2, gnn=None, fallback=ilu, tol=1e-8, max_iter=2000)
     assert base.succeeded and base.gnn_steps == 0
-    np.testing.assert_allclose(x.download(), x2.download(), rtol=0, atol=1e-5 * np.abs(x2.download()).max())
+    # both judged against the plain solver's converged solution (CG + ILU(0) to 1e-13); the
+    # coefficients span nine decades, so a 1e-8 residual leaves errors well above 1e-8
+    xs = ctx.vector(P.n)
+    abi.Solver(ctx, A, solver="cg", precond="ilu0", tol=1e-13, max_iter=5000).solve(b, xs)
+    xs = xs.download()
+    for v in (x, x2):
+        assert np.linalg.norm(v.download() - xs) / np.linalg.norm(xs) < 1e-3
