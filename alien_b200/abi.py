@@ -109,7 +109,8 @@ class BatchStatus(C.Structure):
 
 
 class FcgOptions(C.Structure):
-    _fields_ = [("tol", C.c_double), ("max_iter", C.c_int), ("fallback_ratio", C.c_double)]
+    _fields_ = [("tol", C.c_double), ("max_iter", C.c_int), ("fallback_ratio", C.c_double), ("truncation", C.c_int),
+                ("fallback_mode", C.c_int)]
 
 
 class FcgStatus(C.Structure):
@@ -753,13 +754,18 @@ class FcgResult:
 
 
 def fcg_solve(ctx: Context, A: Matrix, b: Vector, x: Vector, gnn: Gnn | None = None, fallback: "Precond | None" = None,
-              tol: float = 1e-8, max_iter: int = 5000, fallback_ratio: float = 1.0) -> FcgResult:
-    """Flexible CG with the learned preconditioner, the fallback (ILU0)
-    taking over from the first network step that reduces ||r|| by less than
-    fallback_ratio."""
+              tol: float = 1e-8, max_iter: int = 5000, fallback_ratio: float = 1.0,
+              truncation: int | None = None, fallback_mode: str | None = None) -> FcgResult:
+    """Flexible CG (truncated A-orthogonalisation over `truncation` directions)
+    with the learned preconditioner, the fallback (ILU0) taking over from the
+    first network step that reduces ||r|| by less than fallback_ratio."""
     o = FcgOptions()
     lib().ab2_fcg_options_default(C.byref(o))
     o.tol, o.max_iter, o.fallback_ratio = tol, max_iter, fallback_ratio
+    if truncation is not None:
+        o.truncation = truncation
+    if fallback_mode is not None:
+        o.fallback_mode = {"sticky": 0, "step": 1}[fallback_mode]
     st = FcgStatus()
     ctx.check(lib().ab2_fcg_solve(ctx.h, A.h, gnn.h if gnn else None, fallback.h if fallback else None, b.h, x.h,
                                   C.byref(o), C.byref(st)), "fcg_solve")

@@ -694,74 +694,86 @@ __global__ void k_gnn_adam(int np, float* __restrict__ P, const float* __restric
 }
 
 // ------------------------------------------------------------------ flexible CG
-// Scalars of the flexible CG loop, kept on the device so that one iteration
-// needs a single host read (of rr, for the stop and fallback decisions).
+// Notay's FCG(m): p_k = z_k - sum_i (z_k . q_i / d_i) p_i over the last m
+// directions (q_i = A p_i, d_i = p_i . q_i), alpha_k = p_k . r_k / d_k.  The
+// scalars stay on the device; one iteration needs a single host read (of rr,
+// for the stop and fallback decisions).
+constexpr int kMaxTrunc = 16;
 struct FcgScalars {
-  double rz;     // r . z of the current direction
-  double pq;     // p . A p
-  double rr;     // r . r after the update
-  double beta;
-  int breakdown; // p . A p == 0
+  double rr;                // r . r after the update
+  double alpha;
+  double d[kMaxTrunc];      // p_i . A p_i, by window slot
+  double coef[kMaxTrunc];   // z . A p_i / d_i of the current step
+  int breakdown;            // p . A p == 0
+};
+struct Window {
+  const double* v[kMaxTrunc];
 };
 
-// alpha = rz / pq; x += alpha p; r_old = r; r -= alpha q; rr = r . r.
-__global__ void __launch_bounds__(kThreads) k_fcg_update(int n, const double* __restrict__ p, const double* __restrict__ q,
-                                                         double* __restrict__ x, double* __restrict__ r,
-                                                         double* __restrict__ r_old, FcgScalars* sc, double* partials,
-                                                         unsigned* counter, double* red_out) {
-  const double pq = sc->pq;
-  const bool ok = pq != 0.0;
-  const double alpha = ok ? sc->rz / pq : 0.0;
-  double acc[1] = {0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double rv = r[i];
-    r_old[i] = rv;
-    if (ok) {
-      x[i] = fma(alpha, p[i], x[i]);
-      rv = fma(-alpha, q[i], rv);
-      r[i] = rv;
-    }
-    acc[0] = fma(rv, rv, acc[0]);
-  }
-  if (grid_reduce<1>(acc, partials, counter, red_out)) {
-    sc->rr = red_out[0];
-    if (!ok) sc->breakdown = 1;
-  }
-}
-
-// Polak-Ribiere: beta = z . (r - r_old) / rz_old; rz = z . r.
-__global__ void __launch_bounds__(kThreads) k_fcg_dots(int n, const double* __restrict__ z, const double* __restrict__ r,
-                                                       const double* __restrict__ r_old, FcgScalars* sc, double* partials,
-                                                       unsigned* counter, double* red_out) {
-  double acc[2] = {0.0, 0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double zi = z[i];
-    acc[0] = fma(zi, r[i], acc[0]);
-    acc[1] = fma(zi, r_old[i], acc[1]);
-  }
-  if (grid_reduce<2>(acc, partials, counter, red_out)) {
-    const double rz_old = sc->rz;
-    sc->beta = rz_old != 0.0 ? (red_out[0] - red_out[1]) / rz_old : 0.0;
-    sc->rz = red_out[0];
-  }
-}
-
-// first direction: rz = r . z (beta = 0, p = z follows)
-__global__ void __launch_bounds__(kThreads) k_fcg_rz(int n, const double* __restrict__ z, const double* __restrict__ r,
+// coef_k = z . q_k / d_k for the window's slots 0..count-1
+__global__ void __launch_bounds__(kThreads) k_fcg_zq(int n, const double* __restrict__ z, const Window q, int count,
                                                      FcgScalars* sc, double* partials, unsigned* counter,
                                                      double* red_out) {
-  double acc[1] = {0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] = fma(z[i], r[i], acc[0]);
-  if (grid_reduce<1>(acc, partials, counter, red_out)) {
-    sc->rz = red_out[0];
-    sc->beta = 0.0;
+  double acc[kMaxTrunc];
+#pragma unroll
+  for (int k = 0; k < kMaxTrunc; ++k) acc[k] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double zi = z[i];
+#pragma unroll
+    for (int k = 0; k < kMaxTrunc; ++k)
+      if (k < count) acc[k] = fma(zi, q.v[k][i], acc[k]);
+  }
+  if (grid_reduce<kMaxTrunc>(acc, partials, counter, red_out)) {
+    for (int k = 0; k < count; ++k) sc->coef[k] = sc->d[k] != 0.0 ? red_out[k] / sc->d[k] : 0.0;
   }
 }
 
-// p = z + beta p
-__global__ void k_fcg_dir(int n, const double* __restrict__ z, double* __restrict__ p, const FcgScalars* sc) {
-  const double beta = sc->beta;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = fma(beta, p[i], z[i]);
+// p = z - sum_k coef_k p_k (p may be one of the window's vectors: element-wise in place)
+__global__ void k_fcg_dir(int n, const double* __restrict__ z, const Window pw, int count, const FcgScalars* sc,
+                          double* p) {
+  double coef[kMaxTrunc];
+#pragma unroll
+  for (int k = 0; k < kMaxTrunc; ++k) coef[k] = k < count ? sc->coef[k] : 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = z[i];
+#pragma unroll
+    for (int k = 0; k < kMaxTrunc; ++k)
+      if (k < count) v = fma(-coef[k], pw.v[k][i], v);
+    p[i] = v;
+  }
+}
+
+// d_slot = p . q, alpha = p . r / d_slot (breakdown if d_slot == 0)
+__global__ void __launch_bounds__(kThreads) k_fcg_pq(int n, const double* __restrict__ p, const double* __restrict__ q,
+                                                     const double* __restrict__ r, int slot, FcgScalars* sc,
+                                                     double* partials, unsigned* counter, double* red_out) {
+  double acc[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double pi = p[i];
+    acc[0] = fma(pi, q[i], acc[0]);
+    acc[1] = fma(pi, r[i], acc[1]);
+  }
+  if (grid_reduce<2>(acc, partials, counter, red_out)) {
+    const double d = red_out[0];
+    sc->d[slot] = d;
+    sc->alpha = d != 0.0 ? red_out[1] / d : 0.0;
+    if (d == 0.0) sc->breakdown = 1;
+  }
+}
+
+// x += alpha p; r -= alpha q; rr = r . r
+__global__ void __launch_bounds__(kThreads) k_fcg_update(int n, const double* __restrict__ p, const double* __restrict__ q,
+                                                         double* __restrict__ x, double* __restrict__ r, FcgScalars* sc,
+                                                         double* partials, unsigned* counter, double* red_out) {
+  const double alpha = sc->alpha;
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] = fma(alpha, p[i], x[i]);
+    const double rv = fma(-alpha, q[i], r[i]);
+    r[i] = rv;
+    acc[0] = fma(rv, rv, acc[0]);
+  }
+  if (grid_reduce<1>(acc, partials, counter, red_out)) sc->rr = red_out[0];
 }
 
 }  // namespace
@@ -1116,13 +1128,16 @@ void ab2_fcg_options_default(ab2_fcg_options* o) {
   o->tol = 1e-8;
   o->max_iter = 5000;
   o->fallback_ratio = 1.0;
+  o->truncation = 8;
+  o->fallback_mode = AB2_FCG_FALLBACK_STEP;
 }
 
-// Flexible CG (Polak-Ribiere beta, as the preconditioner changes between
-// steps): z = network(r) while the network's steps reduce ||r|| by at least
-// the factor fallback_ratio, the fallback preconditioner from the first step
-// that does not (for the rest of the solve, restarting the search direction
-// there).  No network: the fallback only.
+// Flexible CG, FCG(m) (truncated A-orthogonalisation of the directions, so
+// that a preconditioner which is not a fixed linear operator keeps them
+// conjugate): z = network(r) while the network's steps reduce ||r|| by at
+// least the factor fallback_ratio, the fallback preconditioner from the first
+// step that does not (for the rest of the solve, the direction window
+// cleared).  No network: the fallback only.
 int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_precond* fallback,
                   const ab2_vector* b, ab2_vector* x, const ab2_fcg_options* o, ab2_fcg_status* st) {
   if (!ctx || !A || !b || !x || !o || !st || b->n != A->n || x->n != A->n) return AB2_ERR_BAD_ARG;
@@ -1131,18 +1146,24 @@ int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_p
   if (fallback && fallback->A != A) return AB2_ERR_BAD_ARG;
   std::memset(st, 0, sizeof(*st));
   st->switched_at = -1;
+  if (!(o->truncation >= 1 && o->truncation <= kMaxTrunc)) return AB2_ERR_BAD_ARG;
+  if (o->fallback_mode != AB2_FCG_FALLBACK_STICKY && o->fallback_mode != AB2_FCG_FALLBACK_STEP) return AB2_ERR_BAD_ARG;
   return guard(ctx, [&] {
     const int n = A->n;
+    const int m = o->truncation;
     cudaEvent_t e0, e1;
     AB2_CUDA(cudaEventCreate(&e0));
     AB2_CUDA(cudaEventCreate(&e1));
     double* r = dev_alloc<double>(ctx, (size_t)n);
-    double* r_old = dev_alloc<double>(ctx, (size_t)n);
     double* z = dev_alloc<double>(ctx, (size_t)n);
-    double* p = dev_alloc<double>(ctx, (size_t)n);
-    double* q = dev_alloc<double>(ctx, (size_t)n);
+    double* pv = dev_alloc<double>(ctx, (size_t)m * n);  // window of directions
+    double* qv = dev_alloc<double>(ctx, (size_t)m * n);  // and their products with A
     FcgScalars* sc = dev_alloc<FcgScalars>(ctx, 1);
+    double* zq_part = dev_alloc<double>(ctx, (size_t)kMaxTrunc * kMaxRedBlocks);
+    double* zq_out = dev_alloc<double>(ctx, kMaxTrunc);
+    unsigned* zq_counter = dev_alloc<unsigned>(ctx, 1);
     AB2_CUDA(cudaMemsetAsync(sc, 0, sizeof(FcgScalars), ctx->stream));
+    AB2_CUDA(cudaMemsetAsync(zq_counter, 0, sizeof(unsigned), ctx->stream));
     AB2_CUDA(cudaEventRecord(e0, ctx->stream));
     RedSlot red = red_slot(ctx, 7);
     const int rg = red_grid(ctx, n);
@@ -1150,7 +1171,8 @@ int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_p
       op_dot(ctx, n, u, v, red.result, 7);
       return read_scalar(ctx, red.result);
     };
-    bool use_gnn = G != nullptr;
+    bool use_gnn = G != nullptr;      // the network preconditions the next step
+    bool gnn_retired = G == nullptr;  // STICKY fallback has taken over
     auto precond = [&](const double* in, double* out) {
       if (use_gnn) {
         gnn_forward(G, in, out);
@@ -1165,71 +1187,78 @@ int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_p
       }
     };
     const double nb = std::sqrt(dot(b->d, b->d));
-    op_spmv(ctx, A, x->d, q, AB2_SPMV_AUTO);
+    op_spmv(ctx, A, x->d, z, AB2_SPMV_AUTO);
     op_copy(ctx, n, b->d, r);
-    op_axpy(ctx, n, -1.0, q, r);
+    op_axpy(ctx, n, -1.0, z, r);
     double rn = std::sqrt(dot(r, r));
-    int it = 0;
+    int it = 0, count = 0, next = 0;
     bool ok = nb == 0.0 || rn / nb < o->tol;
-    if (!ok) {
+    while (!ok && it < o->max_iter) {
       precond(r, z);
-      k_fcg_rz<<<rg, kThreads, 0, ctx->stream>>>(n, z, r, sc, red.partials, red.counter, red.result);
-      check_launch(ctx, "fcg_rz");
-      op_copy(ctx, n, z, p);
-      while (it < o->max_iter) {
-        op_spmv(ctx, A, p, q, AB2_SPMV_AUTO);
-        op_dot(ctx, n, p, q, &sc->pq, 7);
-        k_fcg_update<<<rg, kThreads, 0, ctx->stream>>>(n, p, q, x->d, r, r_old, sc, red.partials, red.counter,
-                                                       red.result);
-        check_launch(ctx, "fcg_update");
-        FcgScalars h;
-        AB2_CUDA(cudaMemcpyAsync(ctx->h_pinned, sc, sizeof(FcgScalars), cudaMemcpyDeviceToHost, ctx->stream));
-        AB2_CUDA(cudaStreamSynchronize(ctx->stream));
-        std::memcpy(&h, ctx->h_pinned, sizeof(FcgScalars));
-        if (h.breakdown) {
-          st->error = AB2_ERR_BREAKDOWN;
-          break;
+      double* p = pv + (size_t)next * n;
+      double* q = qv + (size_t)next * n;
+      if (count > 0) {
+        Window wq{}, wp{};
+        for (int k = 0; k < count; ++k) {
+          wq.v[k] = qv + (size_t)k * n;
+          wp.v[k] = pv + (size_t)k * n;
         }
-        ++it;
-        const double rn_new = std::sqrt(h.rr);
-        if (rn_new / nb < o->tol) {
-          ok = true;
-          rn = rn_new;
-          break;
-        }
-        bool restart = false;
-        if (use_gnn && fallback && rn_new > o->fallback_ratio * rn) {
-          use_gnn = false;  // ILU(0) takes over from here, with a fresh direction
-          restart = true;
-          st->switched_at = it;
-        }
-        rn = rn_new;
-        precond(r, z);
-        if (restart) {
-          k_fcg_rz<<<rg, kThreads, 0, ctx->stream>>>(n, z, r, sc, red.partials, red.counter, red.result);
-          check_launch(ctx, "fcg_rz");
-        } else {
-          k_fcg_dots<<<rg, kThreads, 0, ctx->stream>>>(n, z, r, r_old, sc, red.partials, red.counter, red.result);
-          check_launch(ctx, "fcg_dots");
-        }
-        k_fcg_dir<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, z, p, sc);  // beta = 0 after a restart
+        k_fcg_zq<<<rg, kThreads, 0, ctx->stream>>>(n, z, wq, count, sc, zq_part, zq_counter, zq_out);
+        check_launch(ctx, "fcg_zq");
+        k_fcg_dir<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, z, wp, count, sc, p);
         check_launch(ctx, "fcg_dir");
+      } else {
+        op_copy(ctx, n, z, p);
       }
+      op_spmv(ctx, A, p, q, AB2_SPMV_AUTO);
+      k_fcg_pq<<<rg, kThreads, 0, ctx->stream>>>(n, p, q, r, next, sc, red.partials, red.counter, red.result);
+      check_launch(ctx, "fcg_pq");
+      k_fcg_update<<<rg, kThreads, 0, ctx->stream>>>(n, p, q, x->d, r, sc, red.partials, red.counter, red.result);
+      check_launch(ctx, "fcg_update");
+      FcgScalars h;
+      AB2_CUDA(cudaMemcpyAsync(ctx->h_pinned, sc, sizeof(FcgScalars), cudaMemcpyDeviceToHost, ctx->stream));
+      AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+      std::memcpy(&h, ctx->h_pinned, sizeof(FcgScalars));
+      if (h.breakdown) {
+        st->error = AB2_ERR_BREAKDOWN;
+        break;
+      }
+      ++it;
+      const double rn_new = std::sqrt(h.rr);
+      if (rn_new / nb < o->tol) {
+        ok = true;
+        rn = rn_new;
+        break;
+      }
+      const bool failed = use_gnn && fallback && rn_new > o->fallback_ratio * rn;
+      if (failed && st->switched_at < 0) st->switched_at = it;
+      if (failed && o->fallback_mode == AB2_FCG_FALLBACK_STICKY) {
+        use_gnn = false;  // ILU(0) takes over from here, with the window cleared
+        gnn_retired = true;
+        count = 0;
+        next = 0;
+      } else {
+        count = std::min(count + 1, m);
+        next = (next + 1) % m;
+        use_gnn = !gnn_retired && !failed;  // STEP: the fallback for one step after a failed network step
+      }
+      rn = rn_new;
     }
     AB2_CUDA(cudaEventRecord(e1, ctx->stream));
     AB2_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
     AB2_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    op_spmv(ctx, A, x->d, q, AB2_SPMV_AUTO);
+    op_spmv(ctx, A, x->d, z, AB2_SPMV_AUTO);
     op_copy(ctx, n, b->d, r);
-    op_axpy(ctx, n, -1.0, q, r);
+    op_axpy(ctx, n, -1.0, z, r);
     st->true_residual = nb > 0 ? std::sqrt(dot(r, r)) / nb : 0.0;
     st->succeeded = ok ? 1 : 0;
     st->iterations = it;
     st->solve_ms = ms;
     if (!ok && st->error == AB2_OK) st->error = AB2_ERR_NOT_CONVERGED;
-    for (double* v : {r, r_old, z, p, q}) dev_free(ctx, v);
+    for (double* v : {r, z, pv, qv, zq_part, zq_out}) dev_free(ctx, v);
     dev_free(ctx, sc);
+    dev_free(ctx, zq_counter);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   });

@@ -356,6 +356,138 @@ def batch_section(abi, ctx, stream, a):
     return out
 
 
+GNN_WEIGHTS = ROOT / "alien_b200" / "gnn_weights.npy"
+
+
+def gnn_apply_bytes(n: int, nbw: int) -> int:
+    """Algorithmic bytes of one network application: scale (r, 1/sqrt(a_ii)
+    read, x_r written), encoder (x_r, log a_ii read, h1 written), three layers
+    (h read once, the nbw-slot neighbour table, h written) and the last layer
+    (h and the table read, x_r and 1/sqrt(a_ii) read, z written)."""
+    per_node = (8 + 4 + 4) + (4 + 4 + 128) + 3 * (128 + 8 * nbw + 128) + (128 + 8 * nbw + 4 + 4 + 8)
+    return n * per_node
+
+
+def learned_section(abi, ctx, stream, a):
+    """The learned preconditioner: flexible CG (FCG(8)) on held-out
+    heterogeneous fields (128^3, log10 k ~ smoothed N(0, 1.5^2), smoothing
+    length drawn in [2, 8] cells; training used other seeds) to relative
+    residual 1e-8: the trained network alone; the network with ILU(0) for the
+    step after each network step that does not reduce the residual; the
+    network with its learned part removed (only its Jacobi skip: the method
+    without it); ILU(0) alone; and the plain FP64 CG + ILU(0) / CG + Jacobi
+    solvers.  Errors against the plain solver's converged solution (CG + ILU(0)
+    to 1e-12)."""
+    import torch
+
+    from alien_b200 import gnn_train
+
+    if not GNN_WEIGHTS.exists():
+        return {"unavailable": "no trained weights: python -m alien_b200.gnn_train"}
+    side = 128 if a.n >= 128 else a.n
+    seeds = (5_000_017, 5_000_018)
+    meta = json.loads(GNN_WEIGHTS.with_suffix(".json").read_text()) if GNN_WEIGHTS.with_suffix(".json").exists() else {}
+    out = {"training": meta, "fields": [],
+           "note": "time = set-up (network binding / ILU0 factor) + solve, CUDA events on the library stream; "
+                   "flexible CG keeps 8 directions"}
+    for seed in seeds:
+        out["fields"].append(learned_field(abi, ctx, stream, a, gnn_train.field(side, seed),
+                                           f"diffusion3d_{side}^3_grf_sigma1.5_len2-8_heldout_seed{seed}_tol1e-8"))
+    f0 = out["fields"][0]
+    out["apply_ms"] = f0.pop("apply_ms")
+    out["network_roofline"] = f0.pop("network_roofline")
+    out["fields"][-1].pop("apply_ms", None)
+    out["fields"][-1].pop("network_roofline", None)
+    return out
+
+
+def learned_field(abi, ctx, stream, a, P, workload):
+    import torch
+
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals)
+    b, x = ctx.vector(P.b), ctx.vector(P.n)
+    S = abi.Solver(ctx, A, solver="cg", precond="ilu0", tol=1e-12, max_iter=a.max_iter)
+    S.solve(b, x)
+    S.close()
+    xs = x.download()
+
+    def err():
+        v = x.download()
+        return float(np.linalg.norm(v - xs) / np.linalg.norm(xs))
+
+    out = {"workload": workload, "rows": P.n, "nnz": P.nnz}
+
+    def run_solver(S):
+        ctx.assign(x, 0.0)
+        return S.solve(b, x)
+
+    for name, pc in (("cg_ilu0", "ilu0"), ("cg_jacobi", "diag")):
+        t, st, _ = timed_solve(torch, stream, lambda pc=pc: abi.Solver(ctx, A, solver="cg", precond=pc, tol=1e-8,
+                                                                       max_iter=a.max_iter), run_solver)
+        out[name] = {"s": round(t, 5), "iterations": st.iterations, "converged": bool(st.succeeded),
+                     "true_rel_residual": st.true_residual, "rel_error": err()}
+
+    w = np.load(GNN_WEIGHTS)
+    trained = abi.Gnn(ctx, w)
+    w_skip = w.copy()
+    w_skip[192 + 4 * 8192 + 264:192 + 4 * 8192 + 329] = 0.0  # decoder wd, bd: only the Jacobi skip is left
+    skip_only = abi.Gnn(ctx, w_skip)
+
+    class Fcg:
+        def __init__(self, net, fallback):
+            self.net, self.pc = net, None
+            if net is not None:
+                net.bind(A)
+            if fallback:
+                self.pc = abi.Precond(ctx, A, "ilu0")
+
+        def close(self):
+            if self.pc is not None:
+                self.pc.close()
+
+    def run_fcg(F, cap=3000):
+        ctx.assign(x, 0.0)
+        return abi.fcg_solve(ctx, A, b, x, gnn=F.net, fallback=F.pc, tol=1e-8, max_iter=cap, fallback_ratio=1.0)
+
+    for name, net, fb in (("fcg_ilu0", None, True), ("fcg_gnn_ilu0_fallback", trained, True),
+                          ("fcg_gnn", trained, False), ("fcg_network_skip_only", skip_only, False)):
+        t, st, _ = timed_solve(torch, stream, lambda net=net, fb=fb: Fcg(net, fb), run_fcg)
+        out[name] = {"s": round(t, 5), "iterations": st.iterations, "converged": bool(st.succeeded),
+                     "network_steps": st.gnn_steps, "ilu0_steps": st.fallback_steps, "switched_at": st.switched_at,
+                     "true_rel_residual": st.true_residual, "rel_error": err(), "solve_ms": round(st.solve_ms, 3)}
+    # one network application and one ILU(0) application, alone
+    trained.bind(A)
+    pc = abi.Precond(ctx, A, "ilu0")
+    vz = ctx.vector(P.n)
+
+    def per_call(f, reps=20):
+        for _ in range(3):
+            f()
+        k0 = torch.cuda.Event(enable_timing=True)
+        k1 = torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        for _ in range(reps):
+            f()
+        k1.record(stream)
+        k1.synchronize()
+        return k0.elapsed_time(k1) / reps
+
+    g_ms = per_call(lambda: trained.apply(b, vz))
+    i_ms = per_call(lambda: pc.apply(b, vz))
+    nbw = max(2, (int(np.diff(P.row_ptr).max()) - 1 + 1) // 2 * 2)
+    gb = gnn_apply_bytes(P.n, nbw)
+    pk, pk_kind = peaks()
+    out["apply_ms"] = {"network": round(g_ms, 4), "ilu0": round(i_ms, 4)}
+    out["network_roofline"] = {"bound": "hbm", "algorithmic_bytes": int(gb), "achieved": round(gb / g_ms / 1e6, 1),
+                               "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": round(gb / g_ms / 1e6 / pk["hbm_gbs"], 4),
+                               "peak_source": pk_kind}
+    out["speedup_vs_cg_ilu0"] = {k: round(out["cg_ilu0"]["s"] / out[k]["s"], 3)
+                                 for k in ("fcg_ilu0", "fcg_gnn_ilu0_fallback", "fcg_gnn")}
+    for o in (pc, vz, trained, skip_only, b, x, A):
+        o.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -371,6 +503,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurements")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-systems measurement")
     ap.add_argument("--batch-systems", type=int, default=512)
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner measurement")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Krylov loop from the host instead of the CUDA graph (same kernels; for "
                          "profilers that do not see kernels inside conditional graph nodes)")
@@ -483,6 +616,7 @@ def main():
 
     mixed = None if a.no_mixed else mixed_section(abi, ctx, stream, A, P, b, x, methods, a)
     batched = None if a.no_batch else batch_section(abi, ctx, stream, a)
+    learned = None if a.no_learned else learned_section(abi, ctx, stream, a)
 
     pk, pk_kind = peaks()
     traffic = load_traffic()
@@ -569,6 +703,7 @@ def main():
                 "solver_gbs": round(st.iterations * iteration_bytes(a.method, P.n, P.nnz) / (st.solve_ms * 1e-3)
                                     / 1e9, 1),
                 "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "methods": methods, "mixed": mixed, "batched": batched,
+                "learned": learned,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     from alien_b200 import dist

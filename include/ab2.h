@@ -394,17 +394,26 @@ int ab2_gnn_loss_grad(ab2_gnn* gnn, const ab2_vector* r, const ab2_vector* e, do
 int ab2_gnn_train_step(ab2_gnn* gnn, const ab2_vector* r, const ab2_vector* e, double lr, double* loss);
 int ab2_gnn_destroy(ab2_gnn* gnn);
 
-/* Flexible CG (Polak-Ribiere beta: the preconditioner may change between
- * steps) with the network as preconditioner; the fallback preconditioner
- * (ILU(0)) takes over, for the rest of the solve and with a fresh search
- * direction, from the first network step that reduces ||r|| by less than the
- * factor fallback_ratio (1.0: a step that does not reduce it at all).
+#define AB2_FCG_FALLBACK_STICKY 0 /* the fallback keeps the rest of the solve (direction window cleared) */
+#define AB2_FCG_FALLBACK_STEP 1   /* the fallback preconditions the step after each failed network step */
+
+/* Flexible CG with truncated A-orthogonalisation (Notay's FCG(m)): each new
+ * direction p = z - sum_i (z . A p_i / p_i . A p_i) p_i over the last
+ * `truncation` directions, alpha = p . r / p . A p, so that a preconditioner
+ * that is not a fixed linear operator (the network) keeps the directions
+ * conjugate.  The network is the preconditioner; a network step "fails" when
+ * it reduces ||r|| by less than the factor fallback_ratio (1.0: a step that
+ * does not reduce it at all).  Then the fallback (ILU(0)) takes over: for the
+ * rest of the solve with the direction window cleared (STICKY), or for the
+ * next step only, the network resuming after it (STEP, the default).
  * gnn = NULL: flexible CG with the fallback only.
  * Stops when ||r|| / ||b|| < tol (the true residual is reported after). */
 typedef struct {
   double tol;
   int max_iter;
   double fallback_ratio;
+  int truncation;       /* directions kept, 1..16 (1: PCG with a fixed SPD preconditioner) */
+  int fallback_mode;    /* AB2_FCG_FALLBACK_STICKY or AB2_FCG_FALLBACK_STEP */
 } ab2_fcg_options;
 
 typedef struct {
@@ -412,7 +421,7 @@ typedef struct {
   int iterations;
   int gnn_steps;        /* preconditioner applications by the network */
   int fallback_steps;   /* ... by the fallback */
-  int switched_at;      /* iteration where the fallback took over, -1 if it did not */
+  int switched_at;      /* iteration of the first failed network step, -1 if none failed */
   int error;            /* AB2_OK, AB2_ERR_NOT_CONVERGED, AB2_ERR_BREAKDOWN, AB2_ERR_TIMEOUT */
   double true_residual;
   double solve_ms;
