@@ -198,21 +198,26 @@ def reference_sample(P, method: str, iterations_hint: int | None, sample_iters=(
     return setup + per_iter * iters, setup, per_iter, sum(t for _, t in times)
 
 
-def timed_solve(torch, stream, make, run):
-    """One warm + one timed (set-up + solve) pass on the library's stream."""
+def timed_solve(torch, stream, make, run, reps=3):
+    """One warm pass, then `reps` timed (set-up + solve) passes on the
+    library's stream; returns the median time and the median pass's result."""
     obj = make()
     run(obj)
     obj.close()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    obj = make()
-    res = run(obj)
-    e1.record(stream)
-    e1.synchronize()
-    hist = obj.history() if hasattr(obj, "history") else None
-    obj.close()
-    return e0.elapsed_time(e1) / 1e3, res, hist
+    runs = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        obj = make()
+        res = run(obj)
+        e1.record(stream)
+        e1.synchronize()
+        hist = obj.history() if hasattr(obj, "history") else None
+        obj.close()
+        runs.append((e0.elapsed_time(e1) / 1e3, res, hist))
+    runs.sort(key=lambda v: v[0])
+    return runs[len(runs) // 2]
 
 
 MIXED_METHODS = {  # mixed-precision forms of the FP64 methods, same system, same 1e-8 true residual
@@ -595,19 +600,23 @@ def main():
     xs = x.download()
     err = float(np.linalg.norm(xs - P.x_true) / np.linalg.norm(P.x_true))
 
-    # Every plain-FP64 method on the same system: one warm + one timed solve each.
+    # Every plain-FP64 method on the same system: one warm + three timed solves each, the median kept.
     methods = {}
     for m in ([] if a.no_methods else sorted(METHODS)):
         mkw = solver_kw(m)
         step(mkw)
         ctx.synchronize()
-        m0 = torch.cuda.Event(enable_timing=True)
-        m1 = torch.cuda.Event(enable_timing=True)
-        m0.record(stream)
-        mst = step(mkw)
-        m1.record(stream)
-        m1.synchronize()
-        s = m0.elapsed_time(m1) / 1e3
+        runs = []
+        for _ in range(3):
+            m0 = torch.cuda.Event(enable_timing=True)
+            m1 = torch.cuda.Event(enable_timing=True)
+            m0.record(stream)
+            mst = step(mkw)
+            m1.record(stream)
+            m1.synchronize()
+            runs.append((m0.elapsed_time(m1) / 1e3, mst))
+        runs.sort(key=lambda v: v[0])
+        s, mst = runs[1]
         methods[m] = {"s": round(s, 5), "iterations": mst.iterations, "converged": bool(mst.succeeded),
                       "true_rel_residual": mst.true_residual, "setup_ms": round(mst.setup_ms, 3),
                       "solve_ms": round(mst.solve_ms, 3),
