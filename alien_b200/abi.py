@@ -29,7 +29,7 @@ AB2_ERR_UNSUPPORTED = -7
 FMT_CSR, FMT_ELL, FMT_F32 = 1, 2, 4
 SPMV_AUTO, SPMV_CSR_SCALAR, SPMV_CSR_STAGED, SPMV_ELL = 0, 1, 2, 3
 SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
-PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3}
+PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3, "filu0": 4, "neumann": 5}
 ILU_SCHEDULE = {"auto": 0, "wavefront": 1, "stencil": 2}
 BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho"}
 
@@ -53,19 +53,22 @@ class MatrixInfo(C.Structure):
 class PrecondOptions(C.Structure):
     _fields_ = [("kind", C.c_int), ("poly_factor", C.c_double), ("poly_order", C.c_int),
                 ("poly_factor_max_iter", C.c_int), ("ilu_schedule", C.c_int), ("cheb_saad", C.c_int),
-                ("cheb_lanczos", C.c_int)]
+                ("cheb_lanczos", C.c_int), ("filu_factor_iter", C.c_int), ("filu_solver_iter", C.c_int),
+                ("filu_tol", C.c_double)]
 
 
 class PrecondInfo(C.Structure):
     _fields_ = [("kind", C.c_int), ("cheb_alpha", C.c_double), ("cheb_beta", C.c_double),
-                ("ilu_levels_lower", C.c_int), ("ilu_levels_upper", C.c_int), ("ilu_schedule", C.c_int)]
+                ("ilu_levels_lower", C.c_int), ("ilu_levels_upper", C.c_int), ("ilu_schedule", C.c_int),
+                ("neumann_factor", C.c_double)]
 
 
 class SolverOptions(C.Structure):
     _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
                 ("poly_factor", C.c_double), ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int),
                 ("spmv_variant", C.c_int), ("use_graph", C.c_int), ("ilu_schedule", C.c_int),
-                ("cheb_saad", C.c_int), ("cheb_lanczos", C.c_int)]
+                ("cheb_saad", C.c_int), ("cheb_lanczos", C.c_int), ("filu_factor_iter", C.c_int),
+                ("filu_solver_iter", C.c_int), ("filu_tol", C.c_double)]
 
 
 class Status(C.Structure):
@@ -79,7 +82,8 @@ class MixedOptions(C.Structure):
                 ("inner_tol", C.c_double), ("inner_max_iter", C.c_int), ("poly_factor", C.c_double),
                 ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int), ("cheb_saad", C.c_int),
                 ("cheb_lanczos", C.c_int), ("ilu_schedule", C.c_int), ("spmv_variant", C.c_int),
-                ("use_graph", C.c_int)]
+                ("use_graph", C.c_int), ("filu_factor_iter", C.c_int),
+                ("filu_solver_iter", C.c_int), ("filu_tol", C.c_double)]
 
 
 class MixedStatus(C.Structure):
@@ -437,10 +441,11 @@ class Vector:
 class Precond:
     def __init__(self, ctx: Context, A: Matrix, kind: str = "diag", poly_factor: float = 0.0, poly_order: int = 3,
                  poly_factor_max_iter: int = 10, ilu_schedule: str = "auto", cheb_saad: bool = False,
-                 cheb_lanczos: bool = False):
+                 cheb_lanczos: bool = False, filu_factor_iter: int = 0, filu_solver_iter: int = 3,
+                 filu_tol: float = 0.0):
         self.ctx, self.A = ctx, A
         o = PrecondOptions(PRECOND[kind], poly_factor, poly_order, poly_factor_max_iter, ILU_SCHEDULE[ilu_schedule],
-                           int(cheb_saad), int(cheb_lanczos))
+                           int(cheb_saad), int(cheb_lanczos), filu_factor_iter, filu_solver_iter, filu_tol)
         h = _P()
         ctx.check(lib().ab2_precond_create(ctx.h, A.h, C.byref(o), C.byref(h)), "precond_create")
         self.h = h
@@ -486,7 +491,8 @@ class SolveResult:
 
 def solver_options(solver="cg", precond="diag", tol=1e-8, max_iter=1000, poly_factor=0.0, poly_order=3,
                    poly_factor_max_iter=10, spmv_variant=SPMV_AUTO, use_graph=True,
-                   ilu_schedule="auto", cheb_saad=False, cheb_lanczos=False) -> SolverOptions:
+                   ilu_schedule="auto", cheb_saad=False, cheb_lanczos=False, filu_factor_iter=0,
+                   filu_solver_iter=3, filu_tol=0.0) -> SolverOptions:
     o = SolverOptions()
     lib().ab2_solver_options_default(C.byref(o))
     o.solver = SOLVER[solver]
@@ -501,6 +507,9 @@ def solver_options(solver="cg", precond="diag", tol=1e-8, max_iter=1000, poly_fa
     o.ilu_schedule = ILU_SCHEDULE[ilu_schedule]
     o.cheb_saad = int(cheb_saad)
     o.cheb_lanczos = int(cheb_lanczos)
+    o.filu_factor_iter = filu_factor_iter
+    o.filu_solver_iter = filu_solver_iter
+    o.filu_tol = filu_tol
     return o
 
 
@@ -553,7 +562,8 @@ class MixedResult:
 
 def mixed_options(solver="cg", precond="diag", tol=1e-8, max_outer=20, inner_tol=1e-4, inner_max_iter=1000,
                   poly_factor=0.0, poly_order=3, poly_factor_max_iter=20, cheb_saad=False, cheb_lanczos=False,
-                  ilu_schedule="auto", spmv_variant=SPMV_AUTO, use_graph=True) -> MixedOptions:
+                  ilu_schedule="auto", spmv_variant=SPMV_AUTO, use_graph=True, filu_factor_iter=0,
+                  filu_solver_iter=3, filu_tol=0.0) -> MixedOptions:
     o = MixedOptions()
     lib().ab2_mixed_options_default(C.byref(o))
     o.solver = SOLVER[solver]
@@ -570,6 +580,9 @@ def mixed_options(solver="cg", precond="diag", tol=1e-8, max_outer=20, inner_tol
     o.ilu_schedule = ILU_SCHEDULE[ilu_schedule]
     o.spmv_variant = spmv_variant
     o.use_graph = 1 if use_graph else 0
+    o.filu_factor_iter = filu_factor_iter
+    o.filu_solver_iter = filu_solver_iter
+    o.filu_tol = filu_tol
     return o
 
 

@@ -567,6 +567,7 @@ void ab2_solver_options_default(ab2_solver_options* o) {
   o->poly_factor_max_iter = 10;
   o->spmv_variant = AB2_SPMV_AUTO;
   o->use_graph = 1;
+  o->filu_solver_iter = 3;  // the krylov example's filu-solver-niter default
 }
 
 int ab2_solver_create(ab2_context* ctx, const ab2_matrix* A, const ab2_solver_options* o, ab2_solver** out) {
@@ -591,6 +592,9 @@ int ab2_solver_create(ab2_context* ctx, const ab2_matrix* A, const ab2_solver_op
     po.ilu_schedule = o->ilu_schedule;
     po.cheb_saad = o->cheb_saad;
     po.cheb_lanczos = o->cheb_lanczos;
+    po.filu_factor_iter = o->filu_factor_iter;
+    po.filu_solver_iter = o->filu_solver_iter;
+    po.filu_tol = o->filu_tol;
     int prc = ab2_precond_create(ctx, A, &po, &S->pc);
     if (prc != AB2_OK) throw Error{prc, ctx->last_error};
     S->pc->variant = o->spmv_variant;

@@ -5,6 +5,7 @@
 //              (sequential branch)                   unit-L sweep, backward U sweep
 //   Chebyshev  ChebyshevPreconditioner.h:73-202,     power-method bounds, then the
 //              392-434 (_algo2)                      Ifpack2-style polynomial
+//   FILU0, Neumann: filu.cu
 //
 // ILU(0): the factorisation and both sweeps keep the reference's arithmetic row
 // by row (same column order, product and difference rounded apart, an IEEE
@@ -310,6 +311,8 @@ int sweep_blocks(ab2_context* ctx, int len, int widest_chunks) {
   return std::max(1, std::min(blocks, ctx->num_sms * 8));
 }
 
+}  // namespace
+
 void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule) {
   const ab2_matrix* A = pc->A;
   Ilu0Data& d = pc->ilu;
@@ -335,6 +338,17 @@ void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule) {
     check_launch(ctx, "ilu_factor");
   }
 }
+
+void ilu_drop_schedule(ab2_context* ctx, Ilu0Data& d) {
+  for (void* p : {(void*)d.d_perm_l, (void*)d.d_perm_u, (void*)d.d_tmp, (void*)d.d_counters, (void*)d.d_err,
+                  (void*)d.d_bands, (void*)d.d_walk, (void*)d.d_walk32, (void*)d.d_tile_tickets})
+    dev_free(ctx, p);
+  double* lu = d.d_lu;
+  d = Ilu0Data{};
+  d.d_lu = lu;
+}
+
+namespace {
 
 void cheb_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o) {
   const ab2_matrix* A = pc->A;
@@ -569,6 +583,8 @@ void apply_t(ab2_context* ctx, const ab2_precond* pc, const T* x, T* y) {
       }
       break;
     }
+    case AB2_PC_FILU0: filu_apply<T>(ctx, pc, x, y); break;
+    case AB2_PC_NEUMANN: neumann_apply<T>(ctx, pc, x, y); break;
     default: throw Error{AB2_ERR_BAD_ARG, "unknown preconditioner"};
   }
 }
@@ -601,6 +617,8 @@ void pc_enable_f32(ab2_context* ctx, ab2_precond* pc) {
       check_launch(ctx, "ilu_fill32");
     }
   }
+  if (pc->kind == AB2_PC_FILU0) filu_enable_f32(ctx, pc);
+  if (pc->kind == AB2_PC_NEUMANN) neumann_enable_f32(ctx, pc);
   AB2_CUDA(cudaStreamSynchronize(ctx->stream));
   pc->f32 = true;
 }
@@ -643,7 +661,7 @@ extern "C" {
 int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_options* o, ab2_precond** out) {
   if (!ctx || !A || !o || !out) return AB2_ERR_BAD_ARG;
   *out = nullptr;
-  if (o->kind < AB2_PC_NONE || o->kind > AB2_PC_CHEB) return AB2_ERR_BAD_ARG;
+  if (o->kind < AB2_PC_NONE || o->kind > AB2_PC_NEUMANN) return AB2_ERR_BAD_ARG;
   ab2_precond* pc = new (std::nothrow) ab2_precond();
   if (!pc) return AB2_ERR_OOM;
   pc->ctx = ctx_retain(ctx);
@@ -663,6 +681,8 @@ int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_
       require(o->poly_factor_max_iter >= 0, "poly_factor_max_iter must be >= 0");
       cheb_init(ctx, pc, o);
     }
+    if (o->kind == AB2_PC_FILU0) filu_init(ctx, pc, o);
+    if (o->kind == AB2_PC_NEUMANN) neumann_init(ctx, pc, o);
     AB2_CUDA(cudaStreamSynchronize(ctx->stream));
   });
   if (rc != AB2_OK) {
@@ -700,6 +720,7 @@ int ab2_precond_destroy(ab2_precond* pc) {
   dev_free(pc->ctx, pc->d_lu32);
   dev_free(pc->ctx, pc->d_tmp32);
   dev_free(pc->ctx, pc->d_cheb32);
+  filu_neumann_release(pc->ctx, pc);
   if (pc->ctx) ctx_release(pc->ctx);
   delete pc;
   return AB2_OK;
@@ -713,11 +734,12 @@ int ab2_precond_get_info(const ab2_precond* pc, ab2_precond_info* info) {
   info->ilu_levels_lower = pc->ilu.levels_l;
   info->ilu_levels_upper = pc->ilu.levels_u;
   info->ilu_schedule = pc->kind != AB2_PC_ILU0 ? 0 : pc->ilu.stencil ? AB2_ILU_STENCIL : AB2_ILU_WAVEFRONT;
+  info->neumann_factor = pc->neu.omega;
   return AB2_OK;
 }
 
 int ab2_precond_ilu0_values(ab2_context* ctx, const ab2_precond* pc, double* lu) {
-  if (!ctx || !pc || !lu || pc->kind != AB2_PC_ILU0) return AB2_ERR_BAD_ARG;
+  if (!ctx || !pc || !lu || (pc->kind != AB2_PC_ILU0 && pc->kind != AB2_PC_FILU0)) return AB2_ERR_BAD_ARG;
   return guard(ctx, [&] {
     AB2_CUDA(cudaMemcpyAsync(lu, pc->ilu.d_lu, sizeof(double) * (size_t)pc->A->nnz, cudaMemcpyDeviceToHost, ctx->stream));
     AB2_CUDA(cudaStreamSynchronize(ctx->stream));

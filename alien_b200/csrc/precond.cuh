@@ -63,6 +63,49 @@ struct ChebData {
   double* d_xcopy = nullptr;
 };
 
+// FILU0 (FILU0Preconditioner.h): the factor in CSR order (exact ILU(0) or
+// fixed-point sweeps), its strict L and strict U parts as sliced ELL (32-row
+// slices, slot-major, column -1 for padding, CSR order kept inside each row)
+// and 1/u_ii; the application is solver_iter Jacobi sweeps for L then for U.
+struct FiluData {
+  int factor_iter = 0, solver_iter = 0;
+  double tol = 0;
+  int* d_l_off = nullptr;  // slice offsets (in 32-row slot groups), n_slices + 1
+  int* d_l_ci = nullptr;
+  double* d_l_v = nullptr;
+  int* d_u_off = nullptr;
+  int* d_u_ci = nullptr;
+  double* d_u_v = nullptr;
+  double* d_inv = nullptr;        // 1/u_ii
+  double* d_t[2] = {nullptr, nullptr};  // sweep work vectors
+  float* d_l_v32 = nullptr;       // FP32 forms (pc_enable_f32)
+  float* d_u_v32 = nullptr;
+  float* d_inv32 = nullptr;
+  float* d_t32 = nullptr;         // 2 n
+};
+
+// Neumann polynomial (NeumannPolyPreconditioner.h): omega and the order.
+struct NeumannData {
+  double omega = 0;
+  int order = 0;
+  double* d_t[3] = {nullptr, nullptr, nullptr};  // ping-pong iterates + a copy of an aliased input
+  float* d_t32 = nullptr;                         // 3 n
+};
+
+// ILU(0) set-up into pc->ilu (precond.cu): factor plus the sweep schedule.
+void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule);
+void filu_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o);
+void neumann_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o);
+template <class T>
+void filu_apply(ab2_context* ctx, const ab2_precond* pc, const T* x, T* y);
+template <class T>
+void neumann_apply(ab2_context* ctx, const ab2_precond* pc, const T* x, T* y);
+void filu_enable_f32(ab2_context* ctx, ab2_precond* pc);
+void neumann_enable_f32(ab2_context* ctx, ab2_precond* pc);
+void filu_neumann_release(ab2_context* ctx, ab2_precond* pc);
+// Keeps the ILU(0) factor (d_lu) and frees the sweep schedule's arrays.
+void ilu_drop_schedule(ab2_context* ctx, Ilu0Data& d);
+
 }  // namespace ab2
 
 struct ab2_precond {
@@ -73,6 +116,8 @@ struct ab2_precond {
   double* d_inv = nullptr;  // 1/a_ii (Diag, Chebyshev)
   ab2::Ilu0Data ilu;
   ab2::ChebData cheb;
+  ab2::FiluData fil;
+  ab2::NeumannData neu;
   // FP32 form for the inner solves of the mixed-precision solver
   // (pc_enable_f32): the FP64 set-up's results rounded to float.
   bool f32 = false;

@@ -66,6 +66,8 @@ extern "C" {
 #define AB2_PC_DIAG 1
 #define AB2_PC_ILU0 2
 #define AB2_PC_CHEB 3
+#define AB2_PC_FILU0 4   /* FILU0Preconditioner.h: ILU(0) by fixed-point sweeps, Jacobi sweeps for L and U */
+#define AB2_PC_NEUMANN 5 /* NeumannPolyPreconditioner.h: omega (I + G + ... + G^order) x, G = I - omega A */
 
 /* ------------------------------------------------------------------ handles */
 typedef struct ab2_context ab2_context;
@@ -194,10 +196,19 @@ typedef struct {
   int cheb_lanczos; /* 0: bounds by the reference's two power methods; 1: alpha = smallest and
                        beta = 1.1 x largest Ritz value of poly_factor_max_iter Lanczos steps on
                        D^-1/2 A D^-1/2 (no counterpart in the reference) */
+  int filu_factor_iter; /* FILU0 "nb-factor-iter": 0 = the exact ILU(0) factor; k > 0 = k fixed-point
+                           sweeps from A (FLUFactorisationAlgo::factorizeMultiIter) */
+  int filu_solver_iter; /* FILU0 "nb-solver-iter": Jacobi sweeps per triangular solve (0: identity) */
+  double filu_tol;      /* FILU0 "tol": accepted and unused, as in the reference */
 } ab2_precond_options;
 
 /* init(): Diag computes 1/a_ii; ILU0 factorises on the device; Chebyshev
- * estimates its bounds.  The matrix must outlive the preconditioner. */
+ * estimates its bounds; FILU0 factorises (exactly or by fixed-point sweeps)
+ * and stores L and U as sliced ELL; Neumann takes poly_factor as omega, or
+ * (poly_factor = 0) 1 / the power-method estimate of |lambda_max| after
+ * poly_factor_max_iter steps -- from a default-seeded std::mt19937 start vector
+ * where NeumannPolyPreconditioner.h:143-145 seeds from std::random_device.
+ * The matrix must outlive the preconditioner. */
 int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_options* opts, ab2_precond** pc);
 int ab2_precond_apply(ab2_context* ctx, const ab2_precond* pc, const ab2_vector* x, ab2_vector* y); /* y = M^-1 x */
 int ab2_precond_destroy(ab2_precond* pc);
@@ -209,6 +220,7 @@ typedef struct {
   int ilu_levels_lower; /* wavefronts of the L sweep */
   int ilu_levels_upper; /* wavefronts of the U sweep */
   int ilu_schedule;     /* AB2_ILU_WAVEFRONT or AB2_ILU_STENCIL as chosen */
+  double neumann_factor; /* omega used by Neumann */
 } ab2_precond_info;
 int ab2_precond_get_info(const ab2_precond* pc, ab2_precond_info* info);
 /* ILU(0) factor values in CSR order (row_ptr[n] doubles), for checking. */
@@ -228,6 +240,9 @@ typedef struct {
   int ilu_schedule; /* AB2_ILU_* */
   int cheb_saad;    /* see ab2_precond_options */
   int cheb_lanczos;
+  int filu_factor_iter; /* see ab2_precond_options */
+  int filu_solver_iter;
+  double filu_tol;
 } ab2_solver_options;
 
 typedef struct {
@@ -276,6 +291,9 @@ typedef struct {
   int ilu_schedule;    /* AB2_ILU_* */
   int spmv_variant;    /* AB2_SPMV_* for both precisions */
   int use_graph;       /* inner loop in a CUDA graph */
+  int filu_factor_iter; /* see ab2_precond_options */
+  int filu_solver_iter;
+  double filu_tol;
 } ab2_mixed_options;
 
 typedef struct {

@@ -319,6 +319,57 @@ class ILU0Preconditioner {
   std::shared_ptr<ab2_precond> m_pc;
 };
 
+// FILU0 on the GPU: the interface of FILU0Preconditioner.h:320-430
+// (setParameter "nb-factor-iter" / "nb-solver-iter" / "tol", init, solve) over
+// ab2_precond.  The reference's FLUFactorisationAlgo factorises on host
+// arrays; here the factor sweeps run on the device with the same arithmetic
+// and the application is the device-algebra branch of solveL/solveU, bit for
+// bit.  (NeumannPolyPreconditioner.h needs nothing beyond the algebra: the
+// reference template runs on Alien::B200::Algebra as it is.)
+template <typename AlgebraT = Algebra>
+class FILU0Preconditioner {
+ public:
+  typedef AlgebraT AlgebraType;
+  typedef typename AlgebraType::Matrix MatrixType;
+  typedef typename AlgebraType::Vector VectorType;
+  typedef typename MatrixType::ValueType ValueType;
+
+  template <typename TraceT = void>
+  FILU0Preconditioner(AlgebraType& algebra, MatrixType const& matrix, TraceT* = nullptr)
+      : m_algebra(algebra), m_matrix(matrix) {}
+
+  void setParameter(std::string param, int value) {
+    if (param.compare("nb-factor-iter") == 0) m_factor_iter = value;
+    else if (param.compare("nb-solver-iter") == 0) m_solver_iter = value;
+  }
+  void setParameter(std::string param, double value) {
+    if (param.compare("tol") == 0) m_tol = value;
+  }
+  void init() {
+    ab2_precond_options o{};
+    o.kind = AB2_PC_FILU0;
+    o.filu_factor_iter = m_factor_iter;
+    o.filu_solver_iter = m_solver_iter;
+    o.filu_tol = m_tol;
+    ab2_precond* p = nullptr;
+    const Context& ctx = m_algebra.context();
+    ctx.check(ab2_precond_create(ctx.handle(), m_matrix.handle(), &o, &p), "ab2_precond_create");
+    m_pc = std::shared_ptr<ab2_precond>(p, [](ab2_precond* q) { ab2_precond_destroy(q); });
+  }
+  void solve(AlgebraType& algebra, VectorType const& y, VectorType& x) const {
+    const Context& ctx = algebra.context();
+    ctx.check(ab2_precond_apply(ctx.handle(), m_pc.get(), y.handle(), x.handle()), "ab2_precond_apply");
+  }
+  void solve(VectorType const& y, VectorType& x) const { solve(m_algebra, y, x); }
+
+ private:
+  AlgebraType& m_algebra;
+  MatrixType const& m_matrix;
+  int m_factor_iter = 0, m_solver_iter = 0;
+  double m_tol = 0;
+  std::shared_ptr<ab2_precond> m_pc;
+};
+
 // The fused device-resident solvers: the whole Krylov loop on the GPU
 // (ab2_solver_*), or FP32 Krylov inside FP64 refinement (ab2_mixed_*).
 class Solver {

@@ -53,7 +53,7 @@ enum {
   ORC_ERR_BAD_ARG = -6,
 };
 enum { ORC_SOLVER_CG = 0, ORC_SOLVER_BICGSTAB = 1 };
-enum { ORC_PC_NONE = 0, ORC_PC_DIAG = 1, ORC_PC_ILU0 = 2, ORC_PC_CHEB = 3 };
+enum { ORC_PC_NONE = 0, ORC_PC_DIAG = 1, ORC_PC_ILU0 = 2, ORC_PC_CHEB = 3, ORC_PC_FILU0 = 4, ORC_PC_NEUMANN = 5 };
 // Which scalar broke down (the string passed to NullValueException).
 enum { ORC_BD_NONE = 0, ORC_BD_ALPHA = 1, ORC_BD_BETA = 2, ORC_BD_RHO = 3 };
 
@@ -72,6 +72,8 @@ typedef struct {
   int tree_blocks;
   int cheb_saad;     // 1: ChebyshevPreconditioner<AlgebraT, true> (_algo1)
   int cheb_lanczos;  // 1: bounds from poly_factor_max_iter Lanczos steps
+  int filu_factor_iter;  // FILU0 nb-factor-iter (0: exact ILU(0) factor)
+  int filu_solver_iter;  // FILU0 nb-solver-iter
 } orc_options;
 
 typedef struct {
@@ -103,6 +105,8 @@ typedef struct {
   int cheb_lanczos;
   int dot_mode;             // as orc_options, for the FP64 and the FP32 dots
   int tree_blocks;
+  int filu_factor_iter;
+  int filu_solver_iter;
 } orc_mixed_options;
 
 typedef struct {
@@ -239,8 +243,29 @@ struct Diag : Precond<T> {
   void apply(const T* x, T* y) override { pmult(n, inv.data(), x, y); }
 };
 
-// In-place IKJ ILU(0) on a copy of the values (ILU0Preconditioner.h:156-178),
-// in FP64, then the forward/backward sweeps of solveL/solveU (:181-231) in T.
+// In-place IKJ ILU(0) (ILU0Preconditioner.h:156-178), in FP64.
+void ilu0_factor_inplace(const Csr& A, const std::vector<int>& d, std::vector<double>& lu64) {
+  const int n = A.n;
+  const int* rp = A.rp;
+  const int* ci = A.ci;
+  std::vector<int> work(n, -1);
+  for (int i = 1; i < n; ++i) {
+    for (int k = rp[i]; k < d[i]; ++k) {
+      const int kr = ci[k];
+      const double aik = lu64[k] / lu64[d[kr]];
+      lu64[k] = aik;
+      for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = l;
+      for (int j = k + 1; j < rp[i + 1]; ++j) {
+        const int kj = work[ci[j]];
+        if (kj != -1) lu64[j] = lu64[j] - aik * lu64[kj];
+      }
+      for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = -1;
+    }
+  }
+}
+
+// ILU(0) on a copy of the values, in FP64, then the forward/backward sweeps
+// of solveL/solveU (ILU0Preconditioner.h:181-231) in T.
 template <class T>
 struct Ilu0 : Precond<T> {
   int n;
@@ -253,20 +278,7 @@ struct Ilu0 : Precond<T> {
 
   explicit Ilu0(const Csr& A) : n(A.n), rp(A.rp), ci(A.ci), lu64(A.v, A.v + A.rp[A.n]), tmp(A.n) {
     d = diag_offsets(A);
-    std::vector<int> work(n, -1);
-    for (int i = 1; i < n; ++i) {
-      for (int k = rp[i]; k < d[i]; ++k) {
-        const int kr = ci[k];
-        const double aik = lu64[k] / lu64[d[kr]];
-        lu64[k] = aik;
-        for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = l;
-        for (int j = k + 1; j < rp[i + 1]; ++j) {
-          const int kj = work[ci[j]];
-          if (kj != -1) lu64[j] = lu64[j] - aik * lu64[kj];
-        }
-        for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = -1;
-      }
-    }
+    ilu0_factor_inplace(A, d, lu64);
     lu.assign(lu64.begin(), lu64.end());
   }
   void solve_l(const T* y, T* x) const {
@@ -287,6 +299,133 @@ struct Ilu0 : Precond<T> {
   void apply(const T* y, T* x) override {
     solve_l(y, tmp.data());
     solve_u(tmp.data(), x);
+  }
+};
+
+// FILU0 (FILU0Preconditioner.h, FLUFactorisationAlgo): the factor is the
+// exact ILU(0) one (nb-factor-iter = 0, init :67-68) or factor_iter
+// fixed-point sweeps (factorizeMultiIter :119-145, called on the factor
+// matrix itself by init :72, so "matrix values" and the iterate are the same
+// storage: each sweep starts from the previous iterate, not from A) updating
+// every row i >= 1 against a copy v0 of the previous iterate
+// (_factorizeRow :270-300: aik = v[k] / v0[pivot of row k]; v[j] -= aik v0[kj]).
+// Application (solve :245-267), the device-algebra branch of solveL/solveU
+// (:161-175, :218-226): m_x = x; solver_iter times m_x <- x - L m_x
+// (copy, copy, addLMult(-1): SimpleCSRMatrixMultT.h:193-212 with alpha = -1);
+// y = m_x; solver_iter times y <- (1/u_ii) (m_x - U y) (addUMult(-1),
+// pointwiseMult).  Factor in FP64; the FP32 form rounds factor and 1/u_ii.
+template <class T>
+struct Filu0 : Precond<T> {
+  int n;
+  const int* rp;
+  const int* ci;
+  int S;
+  std::vector<int> d;
+  std::vector<double> lu64;
+  std::vector<T> lu, inv, mx, xk;
+
+  Filu0(const Csr& A, int factor_iter, int solver_iter)
+      : n(A.n), rp(A.rp), ci(A.ci), S(solver_iter), lu64(A.v, A.v + A.rp[A.n]), mx(A.n), xk(A.n) {
+    d = diag_offsets(A);
+    if (factor_iter == 0) {
+      ilu0_factor_inplace(A, d, lu64);
+    } else {
+      std::vector<double> prev(A.v, A.v + A.rp[A.n]);
+      std::vector<int> work(n, -1);
+      for (int it = 0; it < factor_iter; ++it) {
+        std::vector<double> cur(prev);
+        for (int i = 1; i < n; ++i) {
+          for (int k = rp[i]; k < d[i]; ++k) {
+            const int kr = ci[k];
+            const double aik = cur[k] / prev[d[kr]];
+            cur[k] = aik;
+            for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = l;
+            for (int j = k + 1; j < rp[i + 1]; ++j) {
+              const int kj = work[ci[j]];
+              if (kj != -1) cur[j] = cur[j] - aik * prev[kj];
+            }
+            for (int l = rp[kr]; l < rp[kr + 1]; ++l) work[ci[l]] = -1;
+          }
+        }
+        prev.swap(cur);
+      }
+      lu64.swap(prev);
+    }
+    lu.assign(lu64.begin(), lu64.end());
+    inv.resize(n);
+    for (int i = 0; i < n; ++i) inv[i] = (T)(1.0 / lu64[d[i]]);
+  }
+  void apply(const T* x, T* y) override {
+    if (S == 0) {
+      copy(n, x, y);
+      return;
+    }
+    copy(n, x, mx.data());
+    for (int it = 0; it < S; ++it) {
+      copy(n, mx.data(), xk.data());
+      for (int i = 0; i < n; ++i) {
+        T v = x[i];
+        for (int k = rp[i]; k < d[i]; ++k) v = v + (T(-1) * lu[k]) * xk[ci[k]];
+        mx[i] = v;
+      }
+    }
+    copy(n, mx.data(), y);
+    for (int it = 0; it < S; ++it) {
+      copy(n, y, xk.data());
+      for (int i = 0; i < n; ++i) {
+        T v = mx[i];
+        for (int k = d[i] + 1; k < rp[i + 1]; ++k) v = v + (T(-1) * lu[k]) * xk[ci[k]];
+        y[i] = inv[i] * v;
+      }
+    }
+  }
+};
+
+// Neumann polynomial (NeumannPolyPreconditioner.h): solve (:103-119)
+// y = x; order times { t = A y; m = y; m = fma(-omega, t, m) (axpy);
+// m = fma(1, x, m) (axpy); y = m }; y = omega y (scal).  omega = factor, or
+// (factor = 0) computeFactor (:133-168): x random, y = A x, then
+// max_iter times x = y, y = A x, est = |y| / |y_prev|; omega = 1/est.  The
+// reference draws x from std::random_device; here (as libab2) from a
+// default-seeded std::mt19937, U(-1,1) in index order.
+template <class T>
+struct Neumann : Precond<T> {
+  CsrT<T> A;
+  int n, order;
+  double omega;
+  std::vector<T> y, t, ay;
+
+  Neumann(const Csr& A64, const T* vals, double factor, int order_, int max_iter)
+      : A{A64.n, A64.rp, A64.ci, vals}, n(A64.n), order(order_), omega(factor), y(A64.n), t(A64.n), ay(A64.n) {
+    if (omega != 0.0) return;
+    std::vector<double> x(n), yy(n);
+    std::mt19937 gen;
+    std::uniform_real_distribution<> dis(-1., 1.);
+    for (int i = 0; i < n; ++i) x[i] = dis(gen);
+    spmv(A64, x.data(), yy.data());
+    double nk = std::sqrt(vdot(n, yy.data(), yy.data()));
+    double f = 0.0;
+    for (int it = 0; it < max_iter; ++it) {
+      copy(n, yy.data(), x.data());
+      spmv(A64, x.data(), yy.data());
+      const double nrm = std::sqrt(vdot(n, yy.data(), yy.data()));
+      f = nrm / nk;
+      nk = nrm;
+    }
+    omega = 1. / f;
+  }
+  void apply(const T* x, T* out) override {
+    const T w = (T)omega;
+    copy(n, x, y.data());
+    for (int i = 0; i < order; ++i) {
+      spmv(A, y.data(), ay.data());
+      copy(n, y.data(), t.data());
+      axpy(n, -w, ay.data(), t.data());
+      axpy(n, T(1), x, t.data());
+      copy(n, t.data(), y.data());
+    }
+    copy(n, y.data(), out);
+    scal(n, w, out);
   }
 };
 
@@ -753,6 +892,7 @@ int orc_solve(int n, const int* rp, const int* ci, const double* v, const double
   Diag<double>* pd = nullptr;
   Ilu0<double>* pi = nullptr;
   Cheb<double>* pc = nullptr;
+  Precond<double>* pother = nullptr;
   Precond<double>* M = &pid;
   switch (o->precond) {
     case ORC_PC_NONE: break;
@@ -764,6 +904,13 @@ int orc_solve(int n, const int* rp, const int* ci, const double* v, const double
       res->cheb_alpha = pc->alpha;
       res->cheb_beta = pc->beta;
       break;
+    case ORC_PC_FILU0: M = pother = new Filu0<double>(A, o->filu_factor_iter, o->filu_solver_iter); break;
+    case ORC_PC_NEUMANN: {
+      auto* pn = new Neumann<double>(A, v, o->poly_factor, o->poly_order, o->poly_factor_max_iter);
+      M = pother = pn;
+      res->cheb_alpha = pn->omega;  // the omega used, reported in the first bound's slot
+      break;
+    }
     default: return ORC_ERR_BAD_ARG;
   }
   StopTest<double> it(n, b, o->tol, o->max_iter, hist, hist_cap);
@@ -785,7 +932,27 @@ int orc_solve(int n, const int* rp, const int* ci, const double* v, const double
   delete pd;
   delete pi;
   delete pc;
+  delete pother;
   return rc;
+}
+
+// One FILU0 application (the device-algebra branch), FP64; lu (optional)
+// receives the factor in CSR order.
+int orc_filu0_apply(int n, const int* rp, const int* ci, const double* v, int factor_iter, int solver_iter,
+                    const double* y, double* x, double* lu) {
+  Filu0<double> M(Csr{n, rp, ci, v}, factor_iter, solver_iter);
+  M.apply(y, x);
+  if (lu) std::memcpy(lu, M.lu64.data(), sizeof(double) * (size_t)rp[n]);
+  return ORC_OK;
+}
+
+// One Neumann application; omega (optional) receives the factor used.
+int orc_neumann_apply(int n, const int* rp, const int* ci, const double* v, double factor, int order, int max_iter,
+                      const double* x, double* y, double* omega) {
+  Neumann<double> M(Csr{n, rp, ci, v}, v, factor, order, max_iter);
+  M.apply(x, y);
+  if (omega) *omega = M.omega;
+  return ORC_OK;
 }
 
 // ---------------------------------------------------------------- FP32 pieces
@@ -831,6 +998,7 @@ int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const 
   Diag<float>* pd = nullptr;
   Ilu0<float>* pi = nullptr;
   Cheb<float>* pc = nullptr;
+  Precond<float>* pother = nullptr;
   Precond<float>* M = &pid;
   switch (o->precond) {
     case ORC_PC_NONE: break;
@@ -839,6 +1007,10 @@ int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const 
     case ORC_PC_CHEB:
       M = pc = new Cheb<float>(A, v32.data(), o->poly_factor, o->poly_order, o->poly_factor_max_iter,
                                o->cheb_saad != 0, o->cheb_lanczos != 0);
+      break;
+    case ORC_PC_FILU0: M = pother = new Filu0<float>(A, o->filu_factor_iter, o->filu_solver_iter); break;
+    case ORC_PC_NEUMANN:
+      M = pother = new Neumann<float>(A, v32.data(), o->poly_factor, o->poly_order, o->poly_factor_max_iter);
       break;
     default: return ORC_ERR_BAD_ARG;
   }
@@ -900,6 +1072,7 @@ int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const 
   delete pd;
   delete pi;
   delete pc;
+  delete pother;
   return ORC_OK;
 }
 

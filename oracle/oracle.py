@@ -25,16 +25,16 @@ ORACLE_SO = HERE / "_build" / "libab2_oracle.so"
 REF_SO = HERE / "_ref" / "libalien_ref.so"
 
 SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
-PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3}
+PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3, "filu0": 4, "neumann": 5}
 BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho", 9: "other"}
 
 
 class Options(C.Structure):
-    # The reference driver reads the first seven fields only.
+    # The reference driver ignores dot_mode, tree_blocks and cheb_lanczos.
     _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
                 ("poly_factor", C.c_double), ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int),
                 ("dot_mode", C.c_int), ("tree_blocks", C.c_int), ("cheb_saad", C.c_int),
-                ("cheb_lanczos", C.c_int)]
+                ("cheb_lanczos", C.c_int), ("filu_factor_iter", C.c_int), ("filu_solver_iter", C.c_int)]
 
 
 DOT_SEQUENTIAL, DOT_DEVICE_TREE = 0, 1
@@ -50,7 +50,8 @@ class MixedOptions(C.Structure):
     _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("tol", C.c_double), ("max_outer", C.c_int),
                 ("inner_tol", C.c_double), ("inner_max_iter", C.c_int), ("poly_factor", C.c_double),
                 ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int), ("cheb_saad", C.c_int),
-                ("cheb_lanczos", C.c_int), ("dot_mode", C.c_int), ("tree_blocks", C.c_int)]
+                ("cheb_lanczos", C.c_int), ("dot_mode", C.c_int), ("tree_blocks", C.c_int),
+                ("filu_factor_iter", C.c_int), ("filu_solver_iter", C.c_int)]
 
 
 class MixedResult(C.Structure):
@@ -86,6 +87,12 @@ def _load(path: Path, prefix: str) -> C.CDLL:
     g = getattr(L, f"{prefix}_cheb_apply")
     g.restype = C.c_int
     g.argtypes = [C.c_int, _IP, _IP, _DP, C.c_double, C.c_int, C.c_int, _DP, _DP]
+    g = getattr(L, f"{prefix}_filu0_apply")
+    g.restype = C.c_int
+    g.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, C.c_int, _DP, _DP, _DP]
+    g = getattr(L, f"{prefix}_neumann_apply")
+    g.restype = C.c_int
+    g.argtypes = [C.c_int, _IP, _IP, _DP, C.c_double, C.c_int, C.c_int, _DP, _DP, _DP]
     return L
 
 
@@ -173,7 +180,8 @@ class OracleSolve:
 
 def solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8, max_iter=1000, poly_factor=0.0,
           poly_order=3, poly_factor_max_iter=10, which="oracle", dot_mode=DOT_SEQUENTIAL,
-          tree_blocks=1184, cheb_saad=False, cheb_lanczos=False) -> OracleSolve:
+          tree_blocks=1184, cheb_saad=False, cheb_lanczos=False, filu_factor_iter=0,
+          filu_solver_iter=3) -> OracleSolve:
     """Runs the restatement (which='oracle') or the reference templates (which='ref').
     dot_mode=DOT_DEVICE_TREE makes the restatement sum every dot product in
     libab2's reduction tree (tree_blocks = its block cap), for bit-exact checks.
@@ -183,7 +191,7 @@ def solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8
     n = rp.size - 1
     x = np.zeros(n) if x0 is None else _c(x0, np.float64).copy()
     o = Options(SOLVER[solver], PRECOND[precond], tol, max_iter, poly_factor, poly_order, poly_factor_max_iter,
-                dot_mode, tree_blocks, int(cheb_saad), int(cheb_lanczos))
+                dot_mode, tree_blocks, int(cheb_saad), int(cheb_lanczos), filu_factor_iter, filu_solver_iter)
     r = Result()
     cap = 2 * max_iter + 8
     hist = np.zeros(cap)
@@ -192,6 +200,32 @@ def solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8
     fn(n, _ip(rp), _ip(ci), _dp(v), _dp(bb), _dp(x), C.byref(o), C.byref(r), _dp(hist), cap)
     return OracleSolve(x, r.iterations, bool(r.converged), r.error, BREAKDOWN.get(r.breakdown), r.nrm2_b, r.last_rr,
                        r.cheb_alpha, r.cheb_beta, hist[:min(r.history_len, cap)].copy())
+
+
+def filu0_apply(row_ptr, cols, vals, y, factor_iter=0, solver_iter=3, which="oracle"):
+    """One FILU0 application x = M^-1 y (FILU0Preconditioner.h, the
+    device-algebra branch) and the factor in CSR order."""
+    rp, ci, v, yy = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(y, np.float64)
+    n = rp.size - 1
+    x = np.zeros(n)
+    lu = np.zeros(rp[-1])
+    L = orc() if which == "oracle" else ref()
+    fn = L.orc_filu0_apply if which == "oracle" else L.ref_filu0_apply
+    fn(n, _ip(rp), _ip(ci), _dp(v), factor_iter, solver_iter, _dp(yy), _dp(x), _dp(lu))
+    return x, lu
+
+
+def neumann_apply(row_ptr, cols, vals, x, factor, order=3, max_iter=10, which="oracle"):
+    """One Neumann-polynomial application y = M^-1 x and the omega used
+    (factor = 0: power method; the reference seeds it from random_device)."""
+    rp, ci, v, xx = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(x, np.float64)
+    n = rp.size - 1
+    y = np.zeros(n)
+    om = np.zeros(1)
+    L = orc() if which == "oracle" else ref()
+    fn = L.orc_neumann_apply if which == "oracle" else L.ref_neumann_apply
+    fn(n, _ip(rp), _ip(ci), _dp(v), factor, order, max_iter, _dp(xx), _dp(y), _dp(om))
+    return y, float(om[0])
 
 
 def spmv(row_ptr, cols, vals, x) -> np.ndarray:
@@ -350,13 +384,15 @@ class MixedSolve:
 
 def mixed_solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8, max_outer=20,
                 inner_tol=1e-4, inner_max_iter=1000, poly_factor=0.0, poly_order=3, poly_factor_max_iter=20,
-                cheb_saad=False, cheb_lanczos=False, dot_mode=DOT_SEQUENTIAL, tree_blocks=1184) -> MixedSolve:
+                cheb_saad=False, cheb_lanczos=False, dot_mode=DOT_SEQUENTIAL, tree_blocks=1184, filu_factor_iter=0,
+                filu_solver_iter=3) -> MixedSolve:
     """FP32 inner Krylov in FP64 refinement, as libab2's ab2_mixed_solve."""
     rp, ci, v, bb = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(b, np.float64)
     n = rp.size - 1
     x = np.zeros(n) if x0 is None else _c(x0, np.float64).copy()
     o = MixedOptions(SOLVER[solver], PRECOND[precond], tol, max_outer, inner_tol, inner_max_iter, poly_factor,
-                     poly_order, poly_factor_max_iter, int(cheb_saad), int(cheb_lanczos), dot_mode, tree_blocks)
+                     poly_order, poly_factor_max_iter, int(cheb_saad), int(cheb_lanczos), dot_mode, tree_blocks,
+                     filu_factor_iter, filu_solver_iter)
     r = MixedResult()
     cap = max_outer + 2
     hist = np.zeros(cap)

@@ -4,7 +4,8 @@
 // oracle/_ref/libalien_ref.so, straight from the reference sources where they
 // lie (ALIEN_REF_SRC, default the read-only reference checkout's src/core):
 //   alien/expression/krylov/{Iteration,CG,BiCGStab,DiagPreconditioner,
-//                            ILU0Preconditioner,ChebyshevPreconditioner}.h
+//                            ILU0Preconditioner,ChebyshevPreconditioner,
+//                            FILU0Preconditioner,NeumannPolyPreconditioner}.h
 //   alien/handlers/scalar/CSRModifierViewT.h
 // Nothing of those files is copied here.  What this file supplies is the
 // minimum the templates need from the rest of Alien, which cannot be built in
@@ -17,7 +18,11 @@
 //     ILU0Preconditioner.h:51-61 and CSRModifierViewT.h:105-145 touch;
 //   * ITraceMng, MatrixDistribution and LUSendRecvTraits stand-ins (the
 //     parallel branches that use the latter are never taken: isParallel()
-//     is false on one process).
+//     is false on one process);
+//   * a second matrix type that is not host-only (DevMatrix) with an algebra
+//     carrying addLMult/addUMult (ShimDevAlgebra, SimpleCSRMatrixMultT.h:193-233),
+//     so that FILU0Preconditioner.h takes its device-algebra branch -- the
+//     branch a GPU back end runs.
 // The exported C entry points mirror oracle/ab2_oracle.cpp's, so tests can
 // check the restatement against the reference templates result for result.
 
@@ -27,6 +32,7 @@
 #include <memory>
 #include <random>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../simplecsr_kernels.h"
@@ -67,6 +73,8 @@ struct DistInfo {
   std::vector<int> m_local_row_size;
   std::vector<int> m_cols;
   int m_first_upper_ghost_index = 0;
+  int m_send_info = 0;  // FILU0's parallel branch names these; never taken here
+  int m_recv_info = 0;
   const int* dcol(const Profile&) const { return nullptr; }
 };
 
@@ -83,6 +91,9 @@ struct Matrix {
   MatrixDistribution dist;
 
   bool isParallel() const { return false; }
+  int getSendPolicy() const { return 0; }
+  int getRecvPolicy() const { return 0; }
+  void* getParallelMng() const { return nullptr; }
   std::size_t getAllocSize() const { return (std::size_t)profile->n; }
   MatrixDistribution const& distribution() const { return dist; }
   Matrix* cloneTo(void*) const { return new Matrix(*this); }
@@ -95,8 +106,19 @@ struct Matrix {
   ab2_oracle::Csr csr() const { return ab2_oracle::Csr{profile->n, profile->rp.data(), profile->ci.data(), values.data()}; }
 };
 
+// The same matrix seen by the templates as living on a device: FILU0's
+// solveL/solveU then go through the algebra (copy, addLMult/addUMult,
+// pointwiseMult) instead of their host loops.
+struct DevMatrix : Matrix {
+  static const bool on_host_only = false;
+  DevMatrix() = default;
+  explicit DevMatrix(Matrix const& m) : Matrix(m) {}
+  DevMatrix* cloneTo(void*) const { return new DevMatrix(*this); }
+};
+
 struct Vector {
   std::vector<double> v;
+  void resize(std::size_t n) { v.resize(n); }
   double* data() { return v.data(); }
   const double* data() const { return v.data(); }
   int size() const { return (int)v.size(); }
@@ -108,13 +130,23 @@ struct LUOp {
   void sendUpperNeighbLUData(double*) {}
 };
 
+// Ghost exchange of FILU0's parallel sweeps (never constructed: one process).
+struct VecOp {
+  template <typename... A>
+  explicit VecOp(A&&...) {}
+  void lowerRecv() {}
+  void upperSend() {}
+  void upperRecv() {}
+  void lowerSend() {}
+};
+
 }  // namespace shim
 
 template <>
 class LUSendRecvTraits<shim::Tag> {
  public:
   typedef shim::LUOp matrix_op_type;
-  typedef void vector_op_type;
+  typedef shim::VecOp vector_op_type;
 };
 
 // The AlgebraT concept as the Krylov templates call it.
@@ -192,6 +224,31 @@ class ShimAlgebra {
   }
 };
 
+// ShimAlgebra over DevMatrix, plus the strict-triangle products of
+// SimpleCSRMatrixMultT::_seqAddLMult/_seqAddUMult (:193-233): per row
+// tmpy += alpha * a_k * x[c_k] in CSR order.
+class ShimDevAlgebra : public ShimAlgebra {
+ public:
+  typedef shim::DevMatrix Matrix;
+  void addLMult(double alpha, Matrix const& A, Vector const& x, Vector& y) const { tri(alpha, A, x, y, true); }
+  void addUMult(double alpha, Matrix const& A, Vector const& x, Vector& y) const { tri(alpha, A, x, y, false); }
+  template <typename PrecondT>
+  void exec(PrecondT& precond, Vector const& x, Vector& y) {
+    precond.solve(*this, x, y);
+  }
+
+ private:
+  static void tri(double alpha, Matrix const& A, Vector const& x, Vector& y, bool lower) {
+    const shim::Profile& p = *A.profile;
+    for (int i = 0; i < p.n; ++i) {
+      double t = y.v[i];
+      const int kb = lower ? p.rp[i] : p.dc[i] + 1, ke = lower ? p.dc[i] : p.rp[i + 1];
+      for (int k = kb; k < ke; ++k) t += alpha * A.values[k] * x.v[p.ci[k]];
+      y.v[i] = t;
+    }
+  }
+};
+
 }  // namespace Alien
 
 #include <alien/expression/krylov/Iteration.h>
@@ -200,6 +257,8 @@ class ShimAlgebra {
 #include <alien/expression/krylov/DiagPreconditioner.h>
 #include <alien/expression/krylov/ChebyshevPreconditioner.h>
 #include <alien/expression/krylov/ILU0Preconditioner.h>
+#include <alien/expression/krylov/FILU0Preconditioner.h>
+#include <alien/expression/krylov/NeumannPolyPreconditioner.h>
 
 extern "C" {
 
@@ -218,6 +277,8 @@ typedef struct {
   int tree_blocks;
   int cheb_saad;
   int cheb_lanczos;
+  int filu_factor_iter;
+  int filu_solver_iter;
 } ref_options;
 
 typedef struct {
@@ -259,9 +320,9 @@ int breakdown_code(std::string const& w) {
   return 9;
 }
 
-template <typename SolverT, typename PrecondT>
-int run(ShimAlgebra& alg, SolverT& solver, PrecondT& pc, Alien::Iteration<ShimAlgebra>& it,
-        Alien::shim::Matrix const& A, Alien::shim::Vector const& b, Alien::shim::Vector& x, ref_result* res) {
+template <typename Alg, typename SolverT, typename PrecondT>
+int run(Alg& alg, SolverT& solver, PrecondT& pc, Alien::Iteration<Alg>& it, typename Alg::Matrix const& A,
+        Alien::shim::Vector const& b, Alien::shim::Vector& x, ref_result* res) {
   try {
     solver.solve(pc, it, A, b, x);
   } catch (ShimAlgebra::NullValueException const& e) {
@@ -271,19 +332,16 @@ int run(ShimAlgebra& alg, SolverT& solver, PrecondT& pc, Alien::Iteration<ShimAl
   return res->error;
 }
 
-}  // namespace
-
-extern "C" {
-
-int ref_solve(int n, const int* rp, const int* ci, const double* v, const double* b, double* x,
-              const ref_options* o, ref_result* res, double* hist, int hist_cap) {
+template <typename Alg>
+int solve_with(int n, const int* rp, const int* ci, const double* v, const double* b, double* x,
+               const ref_options* o, ref_result* res, double* hist, int hist_cap) {
   std::memset(res, 0, sizeof(*res));
-  ShimAlgebra alg;
-  Alien::shim::Matrix A = make_matrix(n, rp, ci, v);
+  Alg alg;
+  typename Alg::Matrix A(make_matrix(n, rp, ci, v));
   Alien::shim::Vector vb, vx;
   vb.v.assign(b, b + n);
   vx.v.assign(x, x + n);
-  Alien::Iteration<ShimAlgebra> it(alg, vb, o->tol, o->max_iter, nullptr);
+  Alien::Iteration<Alg> it(alg, vb, o->tol, o->max_iter, nullptr);
 
   auto finish = [&]() {
     for (int i = 0; i < n; ++i) x[i] = vx.v[i];
@@ -297,45 +355,76 @@ int ref_solve(int n, const int* rp, const int* ci, const double* v, const double
 
   auto with_solver = [&](auto& pc) {
     if (o->solver == 0) {
-      Alien::CG<ShimAlgebra> s(alg, nullptr);
+      Alien::CG<Alg> s(alg, nullptr);
       run(alg, s, pc, it, A, vb, vx, res);
     } else {
-      Alien::BiCGStab<ShimAlgebra> s(alg, nullptr);
+      Alien::BiCGStab<Alg> s(alg, nullptr);
       run(alg, s, pc, it, A, vb, vx, res);
     }
   };
 
+  constexpr bool dev = std::is_same<Alg, Alien::ShimDevAlgebra>::value;
+  if (dev != (o->precond == 4)) return -6;
+  if constexpr (dev) {
+    Alien::FILU0Preconditioner<Alg> pc(alg, A, nullptr);
+    pc.setParameter("nb-factor-iter", o->filu_factor_iter);
+    pc.setParameter("nb-solver-iter", o->filu_solver_iter);
+    pc.init();
+    with_solver(pc);
+    finish();
+    return res->error;
+  } else {
   switch (o->precond) {
     case 1: {
-      Alien::DiagPreconditioner<ShimAlgebra> pc(alg, A);
+      Alien::DiagPreconditioner<Alg> pc(alg, A);
       pc.init();
       with_solver(pc);
       break;
     }
     case 2: {
-      Alien::ILU0Preconditioner<ShimAlgebra> pc(alg, A, nullptr);
+      Alien::ILU0Preconditioner<Alg> pc(alg, A, nullptr);
       pc.init();
       with_solver(pc);
       break;
     }
     case 3: {
       if (o->cheb_saad) {
-        Alien::ChebyshevPreconditioner<ShimAlgebra, true> pc(alg, A, o->poly_factor, o->poly_order,
-                                                             o->poly_factor_max_iter, &g_trace);
+        Alien::ChebyshevPreconditioner<Alg, true> pc(alg, A, o->poly_factor, o->poly_order, o->poly_factor_max_iter,
+                                                     &g_trace);
         pc.init();
         with_solver(pc);
       } else {
-        Alien::ChebyshevPreconditioner<ShimAlgebra> pc(alg, A, o->poly_factor, o->poly_order,
-                                                       o->poly_factor_max_iter, nullptr);
+        Alien::ChebyshevPreconditioner<Alg> pc(alg, A, o->poly_factor, o->poly_order, o->poly_factor_max_iter,
+                                               nullptr);
         pc.init();
         with_solver(pc);
       }
+      break;
+    }
+    case 5: {
+      Alien::NeumannPolyPreconditioner<Alg> pc(alg, A, o->poly_factor, o->poly_order, o->poly_factor_max_iter,
+                                               nullptr);
+      pc.init();
+      with_solver(pc);
       break;
     }
     default: return -6;
   }
   finish();
   return res->error;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// FILU0 runs on the device-algebra shim (its GPU branch); everything else on
+// the host SimpleCSR shim.
+int ref_solve(int n, const int* rp, const int* ci, const double* v, const double* b, double* x,
+              const ref_options* o, ref_result* res, double* hist, int hist_cap) {
+  if (o->precond == 4) return solve_with<Alien::ShimDevAlgebra>(n, rp, ci, v, b, x, o, res, hist, hist_cap);
+  return solve_with<ShimAlgebra>(n, rp, ci, v, b, x, o, res, hist, hist_cap);
 }
 
 // ILU(0) factor computed by the reference's LUFactorisationAlgo.
@@ -381,6 +470,49 @@ int ref_cheb_apply(int n, const int* rp, const int* ci, const double* v, double 
     alg.exec(pc, vx, vy);
   }
   std::memcpy(yout, vy.v.data(), sizeof(double) * (size_t)n);
+  return 0;
+}
+
+// One application of the reference's FILU0Preconditioner on the
+// device-algebra shim; lu (optional) receives its factor in CSR order.
+int ref_filu0_apply(int n, const int* rp, const int* ci, const double* v, int factor_iter, int solver_iter,
+                    const double* y, double* x, double* lu) {
+  Alien::ShimDevAlgebra alg;
+  Alien::shim::DevMatrix A(make_matrix(n, rp, ci, v));
+  Alien::FILU0Preconditioner<Alien::ShimDevAlgebra> pc(alg, A, nullptr);
+  pc.setParameter("nb-factor-iter", factor_iter);
+  pc.setParameter("nb-solver-iter", solver_iter);
+  pc.init();
+  Alien::shim::Vector vy, vx;
+  vy.v.assign(y, y + n);
+  vx.v.assign((std::size_t)n, 0.0);
+  alg.exec(pc, vy, vx);
+  std::memcpy(x, vx.v.data(), sizeof(double) * (size_t)n);
+  if (lu) {
+    // the factor, by repeating the reference's own factorisation on a clone
+    Alien::FLUFactorisationAlgo<Alien::shim::DevMatrix, Alien::shim::Vector> algo;
+    algo.setParameter("nb-factor-iter", factor_iter);
+    algo.init(alg, A);
+    std::memcpy(lu, algo.getLUMatrix().values.data(), sizeof(double) * (size_t)rp[n]);
+  }
+  return 0;
+}
+
+// One application of the reference's NeumannPolyPreconditioner; factor must
+// be nonzero (factor = 0 draws from std::random_device).
+int ref_neumann_apply(int n, const int* rp, const int* ci, const double* v, double factor, int order, int max_iter,
+                      const double* x, double* y, double* omega) {
+  if (factor == 0.0) return -6;
+  ShimAlgebra alg;
+  Alien::shim::Matrix A = make_matrix(n, rp, ci, v);
+  Alien::NeumannPolyPreconditioner<ShimAlgebra> pc(alg, A, factor, order, max_iter, nullptr);
+  pc.init();
+  Alien::shim::Vector vx, vy;
+  vx.v.assign(x, x + n);
+  vy.v.assign((std::size_t)n, 0.0);
+  alg.exec(pc, vx, vy);
+  std::memcpy(y, vy.v.data(), sizeof(double) * (size_t)n);
+  if (omega) *omega = factor;
   return 0;
 }
 

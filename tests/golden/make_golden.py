@@ -3,9 +3,10 @@
     python tests/golden/make_golden.py
 
 Runs oracle/_ref/libalien_ref.so (the reference's header-only CG.h,
-BiCGStab.h, Iteration.h, DiagPreconditioner.h, ILU0Preconditioner.h and
-ChebyshevPreconditioner.h compiled over a SimpleCSR-restating CPU algebra, see
-oracle/ref/ref_driver.cpp) on small seeded systems from libab2's generators and
+BiCGStab.h, Iteration.h, DiagPreconditioner.h, ILU0Preconditioner.h,
+ChebyshevPreconditioner.h, FILU0Preconditioner.h and
+NeumannPolyPreconditioner.h compiled over a SimpleCSR-restating CPU algebra,
+see oracle/ref/ref_driver.cpp) on small seeded systems from libab2's generators and
 records, per case: iteration count, convergence flag, breakdown, the full
 residual history of the stop test, and the solution (as float64 hex, so the
 fixture is exact).  The inputs are regenerated from their seeds by the tests.
@@ -44,6 +45,16 @@ for prob in PROBLEMS:
         # ChebyshevPreconditioner<AlgebraT, true> (Saad's recurrence, _algo1)
         CASES.append(dict(problem=prob, solver=solver, precond="cheb", tol=1e-8, max_iter=300, poly_factor=0.0,
                           poly_order=3, poly_factor_max_iter=20, cheb_saad=True))
+# FILU0 (nonsymmetric sweeps: BiCGStab) and Neumann (omega = 1 / the
+# Gershgorin bound of each matrix, passed explicitly: the reference's own
+# estimate draws from std::random_device)
+GERSHGORIN = {}
+for prob in PROBLEMS:
+    for fi, si in ((0, 3), (1, 2), (0, 1)):
+        CASES.append(dict(problem=prob, solver="bicgs", precond="filu0", tol=1e-8, max_iter=300, poly_factor=0.0,
+                          poly_order=3, poly_factor_max_iter=10, filu_factor_iter=fi, filu_solver_iter=si))
+    CASES.append(dict(problem=prob, solver="cg", precond="neumann", tol=1e-8, max_iter=300, poly_factor="1/gershgorin",
+                      poly_order=3, poly_factor_max_iter=10))
 # edge cases the reference's control flow has
 CASES += [
     dict(problem="poisson16", solver="cg", precond="diag", tol=1e-8, max_iter=1, poly_factor=0.0, poly_order=3,
@@ -73,6 +84,8 @@ def main() -> int:
                                   b_sha256=hashlib.sha256(P.b.tobytes()).hexdigest())
     for c in CASES:
         P = cache[c["problem"]]
+        if c["poly_factor"] == "1/gershgorin":
+            c["poly_factor"] = 1.0 / float(np.add.reduceat(np.abs(P.vals), P.row_ptr[:-1]).max())
         kw = {k: v for k, v in c.items() if k != "problem"}
         r = O.solve(P.row_ptr, P.cols, P.vals, P.b, which="ref", **kw)
         idx = np.unique(np.linspace(0, P.n - 1, 48).astype(np.int64))

@@ -166,7 +166,8 @@ def test_golden_solves(ctx, case):
     P = problems.get(case["problem"])
     kw = dict(solver=case["solver"], precond=case["precond"], tol=case["tol"], max_iter=case["max_iter"],
               poly_factor=case["poly_factor"], poly_order=case["poly_order"],
-              poly_factor_max_iter=case["poly_factor_max_iter"], cheb_saad=case.get("cheb_saad", False))
+              poly_factor_max_iter=case["poly_factor_max_iter"], cheb_saad=case.get("cheb_saad", False),
+              filu_factor_iter=case.get("filu_factor_iter", 0), filu_solver_iter=case.get("filu_solver_iter", 3))
     st, x, hist = gpu_solve(ctx, P, **kw)
     assert st.succeeded
     tree = tree_solve(ctx, P, **kw)

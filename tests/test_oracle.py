@@ -61,6 +61,8 @@ def test_restatement_matches_reference_templates(case):
     kw = {k: case[k] for k in ("solver", "precond", "tol", "max_iter", "poly_factor", "poly_order",
                                "poly_factor_max_iter")}
     kw["cheb_saad"] = case.get("cheb_saad", False)
+    kw["filu_factor_iter"] = case.get("filu_factor_iter", 0)
+    kw["filu_solver_iter"] = case.get("filu_solver_iter", 3)
     r = O.solve(P.row_ptr, P.cols, P.vals, P.b, which="oracle", **kw)
     assert r.iterations == case["iterations"]
     assert r.converged == case["converged"]
@@ -170,3 +172,40 @@ def test_fp32_pieces_are_float_restatements():
     z32 = O.ilu0_apply32(P.row_ptr, P.cols, P.vals, x)
     z64 = O.ilu0_apply(P.row_ptr, P.cols, P.vals, x.astype(np.float64))
     assert np.max(np.abs(z32 - z64)) < 1e-5 * np.max(np.abs(z64))
+
+
+# ----------------------------------------------------------------- FILU0 and Neumann
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", ["poisson16", "diffusion12", "convdiff16", "ragged", "diffusion2d_31x9"])
+def test_filu0_and_neumann_vs_reference(name):
+    """FILU0Preconditioner.h (factor by 0, 1 or 3 fixed-point sweeps -- each
+    starting from the previous iterate, as the reference's init hands its own
+    factor matrix to factorizeMultiIter -- and 0, 1 or 3 Jacobi sweeps per
+    triangle, device-algebra branch) and NeumannPolyPreconditioner.h: factor
+    and application bit for bit."""
+    P = problems.get(name)
+    y = np.random.default_rng(5).normal(size=P.n)
+    for fi in (0, 1, 3):
+        for si in (0, 1, 3):
+            xo, luo = O.filu0_apply(P.row_ptr, P.cols, P.vals, y, fi, si, "oracle")
+            xr, lur = O.filu0_apply(P.row_ptr, P.cols, P.vals, y, fi, si, "ref")
+            np.testing.assert_array_equal(luo, lur)
+            np.testing.assert_array_equal(xo, xr)
+    if name != "ragged":
+        _, lu_ilu = O.filu0_apply(P.row_ptr, P.cols, P.vals, y, 0, 1, "oracle")
+        np.testing.assert_array_equal(lu_ilu, O.ilu0_factor(P.row_ptr, P.cols, P.vals))
+    omega = 1.0 / float(np.add.reduceat(np.abs(P.vals), P.row_ptr[:-1]).max())
+    for order in (0, 1, 3):
+        yo, wo = O.neumann_apply(P.row_ptr, P.cols, P.vals, y, omega, order, 10, "oracle")
+        yr, _ = O.neumann_apply(P.row_ptr, P.cols, P.vals, y, omega, order, 10, "ref")
+        assert wo == omega
+        np.testing.assert_array_equal(yo, yr)
+
+
+def test_neumann_power_method_estimates_the_largest_eigenvalue():
+    """computeFactor's unnormalised power iteration approaches lambda_max
+    from below (slowly: lambda_2/lambda_1 is close to 1)."""
+    P = problems.get("poisson16")
+    lam = 6 + 6 * np.cos(np.pi / 17)  # 3-D 7-point Dirichlet Laplacian, 16^3 cells
+    est = [1 / O.neumann_apply(P.row_ptr, P.cols, P.vals, np.ones(P.n), 0.0, 3, it)[1] for it in (10, 40)]
+    assert est[0] < est[1] < lam and (lam - est[1]) / lam < 0.05
