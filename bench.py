@@ -52,6 +52,18 @@ METHODS = {
                                  poly_factor_max_iter=20),
 }
 
+# The reference's other two preconditioners, measured where they converge
+# (bench `preconditioners` section): on the heterogeneous headline system
+# unscaled Neumann stalls (rows with small coefficients barely move) and
+# BiCGStab + FILU0 diverges, as the reference's own templates do.
+OTHER_METHODS = {
+    # NeumannPolyPreconditioner.h (omega = 1 / power-method estimate, 20 steps)
+    "neumann3_power20": dict(precond="neumann", poly_order=3, poly_factor_max_iter=20),
+    # FILU0Preconditioner.h: exact ILU(0) factor, 3 Jacobi sweeps per triangle
+    # (the krylov example's defaults); not symmetric, so with BiCGStab
+    "bicgstab_filu0_3": dict(solver="bicgs", precond="filu0", filu_factor_iter=0, filu_solver_iter=3),
+}
+
 
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
@@ -141,13 +153,21 @@ def iteration_bytes(method: str, n: int, nnz: int) -> int:
     """Fused-schedule lower bound of one PCG iteration (FP64), from the CSR
     SpMV bytes B = 12 nnz + 4(n+1) + 16 n: Jacobi B + 104 n; ILU0
     B + B_LU + 120 n with B_LU = 12 nnz + 4(n+1) + 8 n; Chebyshev(3)
-    4 B + 200 n."""
+    4 B + 200 n; Neumann(k) (k+1) B + (24 k + 104) n; BiCGStab + FILU0(S)
+    twice (B + S B_sweeps + 100 n), B_sweeps = 12 (nnz - n) + 56 n (the strict
+    triangles' slots and one L and one U sweep's vectors)."""
     b_spmv = 12 * nnz + 4 * (n + 1) + 16 * n
-    pc = METHODS[method]["precond"]
+    m = METHODS[method] if method in METHODS else OTHER_METHODS[method]
+    pc = m["precond"]
     if pc == "diag":
         return b_spmv + 104 * n
     if pc == "ilu0":
         return b_spmv + (12 * nnz + 4 * (n + 1) + 8 * n) + 120 * n
+    if pc == "neumann":
+        k = m["poly_order"]
+        return (k + 1) * b_spmv + (24 * k + 104) * n
+    if pc == "filu0":
+        return 2 * (b_spmv + m["filu_solver_iter"] * (12 * (nnz - n) + 56 * n) + 100 * n)
     return 4 * b_spmv + 200 * n
 
 
@@ -170,12 +190,21 @@ def reference_method(method: str) -> tuple[dict, str]:
     kw = dict(poly_factor=0.0, poly_order=3, poly_factor_max_iter=20, cheb_saad=False)
     m = METHODS[method]
     kw["precond"] = m["precond"]
+    kw["solver"] = m.get("solver", "cg")
     if m["precond"] == "cheb":
         kw["cheb_saad"] = True
         kw["poly_order"] = m["poly_order"]
         kw["poly_factor_max_iter"] = m["poly_factor_max_iter"]
+    if m["precond"] == "filu0":
+        kw["filu_factor_iter"] = m["filu_factor_iter"]
+        kw["filu_solver_iter"] = m["filu_solver_iter"]
+    if m["precond"] == "neumann":
+        kw["poly_order"] = m["poly_order"]
     label = {"ilu0": "ILU0Preconditioner.h", "diag": "DiagPreconditioner.h",
-             "cheb": "ChebyshevPreconditioner<.., true>.h (power-method bounds)"}[m["precond"]]
+             "cheb": "ChebyshevPreconditioner<.., true>.h (power-method bounds)",
+             "filu0": "BiCGStab.h + FILU0Preconditioner.h",
+             "neumann": "NeumannPolyPreconditioner.h (omega = 1/Gershgorin bound: its own estimate "
+                        "seeds from std::random_device)"}[m["precond"]]
     return kw, label
 
 
@@ -186,10 +215,12 @@ def reference_sample(P, method: str, iterations_hint: int | None, sample_iters=(
     from oracle import oracle as O
 
     kw, _ = reference_method(method)
+    if kw["precond"] == "neumann":
+        kw["poly_factor"] = 1.0 / float(np.add.reduceat(np.abs(P.vals), P.row_ptr[:-1]).max())
     times = []
     for m in sample_iters:
         t = time.perf_counter()
-        r = O.solve(P.row_ptr, P.cols, P.vals, P.b, solver="cg", tol=1e-8, max_iter=m, which="ref", **kw)
+        r = O.solve(P.row_ptr, P.cols, P.vals, P.b, tol=1e-8, max_iter=m, which="ref", **kw)
         times.append((r.iterations, time.perf_counter() - t))
     (i1, t1), (i2, t2) = times
     per_iter = (t2 - t1) / max(i2 - i1, 1)
@@ -361,6 +392,74 @@ def batch_section(abi, ctx, stream, a):
     return out
 
 
+def preconditioner_section(abi, ctx, stream, A, P, a):
+    """Every preconditioner of the path: one application at the headline size
+    (time and GB/s of its algorithmic bytes), and the two the headline system
+    does not suit solved where they converge -- BiCGStab + FILU0 against
+    BiCGStab + ILU0 on the 128^3 convection-diffusion system, CG + Neumann
+    against CG + Jacobi on the 192^3 constant-coefficient Poisson system."""
+    import torch
+
+    n, nnz = P.n, P.nnz
+    b_spmv = 12 * nnz + 4 * (n + 1) + 16 * n
+    sweeps = 12 * (nnz - n) + 56 * n
+    kinds = {"diag": (dict(kind="diag"), 24 * n),
+             "ilu0": (dict(kind="ilu0"), 8 * nnz + 16 * n),
+             "cheb3_saad": (dict(kind="cheb", cheb_saad=True, poly_order=3, poly_factor_max_iter=20),
+                            3 * b_spmv + 5 * 8 * n),
+             "filu0_3": (dict(kind="filu0", filu_factor_iter=0, filu_solver_iter=3), 3 * sweeps),
+             "neumann3": (dict(kind="neumann", poly_order=3, poly_factor_max_iter=20), 3 * (b_spmv + 16 * n))}
+    pk, pk_kind = peaks()
+    vx, vy = ctx.vector(P.b), ctx.vector(n)
+    out = {"apply": {}, "note": "algorithmic bytes per application: diag 24n; ILU0 8 nnz + 16 n; Chebyshev(3) "
+                                 "3 B_spmv + 40 n; FILU0(3 sweeps) 3 (12 (nnz - n) + 56 n); Neumann(3) 3 (B_spmv + 16 n)"}
+    for name, (kw, nbytes) in kinds.items():
+        pc = abi.Precond(ctx, A, **kw)
+        for _ in range(3):
+            pc.apply(vx, vy)
+        k0 = torch.cuda.Event(enable_timing=True)
+        k1 = torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        for _ in range(20):
+            pc.apply(vx, vy)
+        k1.record(stream)
+        k1.synchronize()
+        ms = k0.elapsed_time(k1) / 20
+        out["apply"][name] = {"ms": round(ms, 4), "algorithmic_bytes": int(nbytes),
+                              "gbs": round(nbytes / ms / 1e6, 1), "frac": round(nbytes / ms / 1e6 / pk["hbm_gbs"], 4)}
+        pc.close()
+    for v in (vx, vy):
+        v.close()
+    out["peak_source"] = pk_kind
+
+    def solve_pair(Q, label, pairs):
+        AQ = ctx.matrix(Q.row_ptr, Q.cols, Q.vals)
+        bq, xq = ctx.vector(Q.b), ctx.vector(Q.n)
+        res = {"rows": Q.n, "nnz": Q.nnz}
+
+        def run(S):
+            ctx.assign(xq, 0.0)
+            return S.solve(bq, xq)
+
+        for name, kw in pairs:
+            t, st, _ = timed_solve(torch, stream, lambda kw=kw: abi.Solver(ctx, AQ, tol=1e-8, max_iter=5000,
+                                                                            use_graph=not a.host_loop, **kw), run)
+            res[name] = {"s": round(t, 5), "iterations": st.iterations, "converged": bool(st.succeeded),
+                         "true_rel_residual": st.true_residual}
+        for o in (bq, xq, AQ):
+            o.close()
+        out[label] = res
+
+    m = 128 if a.n >= 128 else a.n
+    solve_pair(abi.convdiff(m, m, m, peclet=10.0, modes=8, seed=0), f"convdiff3d_{m}",
+               [(f"bicgstab_filu0_{k}", dict(solver="bicgs", precond="filu0", filu_factor_iter=0, filu_solver_iter=k))
+                for k in (3, 6, 10)] + [("bicgstab_ilu0", dict(solver="bicgs", precond="ilu0"))])
+    solve_pair(abi.poisson(a.n, a.n, a.n, seed=0), f"poisson3d_{a.n}",
+               [("cg_neumann3_power20", dict(solver="cg", precond="neumann", poly_order=3, poly_factor_max_iter=20)),
+                ("cg_jacobi", dict(solver="cg", precond="diag"))])
+    return out
+
+
 GNN_WEIGHTS = ROOT / "alien_b200" / "gnn_weights.npy"
 
 
@@ -509,6 +608,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-systems measurement")
     ap.add_argument("--batch-systems", type=int, default=512)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner measurement")
+    ap.add_argument("--no-precond", action="store_true", help="skip the per-preconditioner measurements")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Krylov loop from the host instead of the CUDA graph (same kernels; for "
                          "profilers that do not see kernels inside conditional graph nodes)")
@@ -519,8 +619,9 @@ def main():
 
     n1 = a.n
     P = abi.diffusion(n1, n1, n1, sigma=1.0, smooth=4.0, seed=rank)
-    workload = f"diffusion3d_{n1}^3_grf_sigma1_len4_cg_{a.method}_tol1e-8"
-    config = {"workload": workload, "rows": P.n, "nnz": P.nnz, "precision": "fp64", "solver": "cg",
+    head_solver = METHODS[a.method].get("solver", "cg")
+    workload = f"diffusion3d_{n1}^3_grf_sigma1_len4_{'cg_' if head_solver == 'cg' else ''}{a.method}_tol1e-8"
+    config = {"workload": workload, "rows": P.n, "nnz": P.nnz, "precision": "fp64", "solver": head_solver,
               "method": a.method, "tol": 1e-8, "formats": "csr+ell32", "l2": "inputs larger than L2 (no flush)",
               "parallelism": f"independent systems x{world}"}
 
@@ -534,7 +635,10 @@ def main():
         if hint is None and P.n <= 300_000:  # small enough to count the iterations with one full solve
             from oracle import oracle as O
 
-            hint = O.solve(P.row_ptr, P.cols, P.vals, P.b, solver="cg", tol=1e-8, max_iter=a.max_iter, which="ref",
+            rkw = dict(rkw)
+            if rkw["precond"] == "neumann":
+                rkw["poly_factor"] = 1.0 / float(np.add.reduceat(np.abs(P.vals), P.row_ptr[:-1]).max())
+            hint = O.solve(P.row_ptr, P.cols, P.vals, P.b, tol=1e-8, max_iter=a.max_iter, which="ref",
                            **rkw).iterations
         steps = []
         for i in range(a.warmup + a.steps):
@@ -564,8 +668,9 @@ def main():
     x = ctx.vector(P.n)
 
     def solver_kw(method):
-        return dict(solver="cg", tol=1e-8, max_iter=a.max_iter, poly_factor=0.0, use_graph=not a.host_loop,
-                    **METHODS[method])
+        kw = dict(solver="cg", tol=1e-8, max_iter=a.max_iter, poly_factor=0.0, use_graph=not a.host_loop)
+        kw.update(METHODS[method])
+        return kw
 
     kw = solver_kw(a.method)
 
@@ -626,6 +731,7 @@ def main():
     mixed = None if a.no_mixed else mixed_section(abi, ctx, stream, A, P, b, x, methods, a)
     batched = None if a.no_batch else batch_section(abi, ctx, stream, a)
     learned = None if a.no_learned else learned_section(abi, ctx, stream, a)
+    preconds = None if a.no_precond else preconditioner_section(abi, ctx, stream, A, P, a)
 
     pk, pk_kind = peaks()
     traffic = load_traffic()
@@ -712,7 +818,7 @@ def main():
                 "solver_gbs": round(st.iterations * iteration_bytes(a.method, P.n, P.nnz) / (st.solve_ms * 1e-3)
                                     / 1e9, 1),
                 "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "methods": methods, "mixed": mixed, "batched": batched,
-                "learned": learned,
+                "learned": learned, "preconditioners": preconds,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     from alien_b200 import dist
