@@ -2,15 +2,16 @@
 //
 // TEST PROGRAM.  Built by tests/cpp/Makefile from the reference sources where
 // they lie (ALIEN_REF_SRC): expression/krylov/{Iteration,CG,BiCGStab,
-// DiagPreconditioner,ChebyshevPreconditioner}.h, included unmodified.  The
+// DiagPreconditioner,ChebyshevPreconditioner,NeumannPolyPreconditioner}.h,
+// included unmodified.  The
 // algebra they are instantiated with is Alien::B200::Algebra
 // (include/alien/b200/B200Algebra.h): every vector operation, SpMV, dot
 // product and preconditioner application runs on the GPU through the C ABI.
 // ILU(0) is Alien::B200::ILU0Preconditioner (the reference's runs on host
-// arrays).  The only stand-in supplied here is the ITraceMng the templates
+// arrays), FILU0 Alien::B200::FILU0Preconditioner likewise.  The only stand-in supplied here is the ITraceMng the templates
 // take a pointer to (Arccore is not available).
 //
-//   drop_in <dir> <cg|bicgs> <diag|ilu0|cheb|cheb_saad> <tol> <max_iter> [solve2]
+//   drop_in <dir> <cg|bicgs> <diag|ilu0|cheb|cheb_saad|neumann|filu0> <tol> <max_iter> [solve2]
 //
 // reads <dir>/{rp.i32,ci.i32,v.f64,b.f64} (n = size of b), solves from x = 0,
 // writes <dir>/x.f64 and prints one JSON line with the iteration count, the
@@ -40,6 +41,7 @@ class ITraceMng {
 #include <alien/expression/krylov/BiCGStab.h>
 #include <alien/expression/krylov/DiagPreconditioner.h>
 #include <alien/expression/krylov/ChebyshevPreconditioner.h>
+#include <alien/expression/krylov/NeumannPolyPreconditioner.h>
 
 namespace {
 
@@ -117,6 +119,19 @@ int main(int argc, char** argv) {
     run(pc);
   } else if (pc_name == "cheb_saad") {
     Alien::ChebyshevPreconditioner<Algebra, true> pc(alg, A, 0.0, 3, 20, &trace);
+    pc.init();
+    run(pc);
+  } else if (pc_name == "neumann") {
+    // omega from dir/omega.txt: the template's own estimate seeds from std::random_device
+    double omega = 0.0;
+    std::ifstream(dir + "/omega.txt") >> omega;
+    Alien::NeumannPolyPreconditioner<Algebra> pc(alg, A, omega, 3, 20, nullptr);
+    pc.init();
+    run(pc);
+  } else if (pc_name == "filu0") {
+    Alien::B200::FILU0Preconditioner<Algebra> pc(alg, A);
+    pc.setParameter("nb-factor-iter", 0);
+    pc.setParameter("nb-solver-iter", 3);
     pc.init();
     run(pc);
   } else {
