@@ -215,6 +215,9 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_problem_diffusion": (_I, [_I, _I, _I, _D, _D, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_convdiff": (_I, [_I, _I, _I, _D, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_destroy": (_I, [C.POINTER(Problem)]),
+    "ab2_problem_read_matrix_market": (_I, [C.c_char_p, C.c_char_p, C.POINTER(C.POINTER(Problem))]),
+    "ab2_problem_write_matrix_market": (_I, [C.POINTER(Problem), C.c_char_p, C.c_char_p]),
+    "ab2_matrix_market_error": (C.c_char_p, []),
     "ab2_rng_u64": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
     "ab2_rng_uniform": (_D, [C.c_uint64, C.c_uint64, C.c_uint64]),
 }
@@ -811,10 +814,37 @@ def _take(p) -> CsrProblem:
         return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
 
     out = CsrProblem(n, arr(P.row_ptr, n + 1, np.int32), arr(P.cols, nnz, np.int32), arr(P.vals, nnz, np.float64),
-                     arr(P.x_true, n, np.float64), arr(P.b, n, np.float64),
+                     arr(P.x_true, n, np.float64) if bool(P.x_true) else None, arr(P.b, n, np.float64),
                      arr(P.log10_k, n, np.float64) if bool(P.log10_k) else None, (P.nx, P.ny, P.nz))
     lib().ab2_problem_destroy(p)
     return out
+
+
+def read_matrix_market(path, rhs=None) -> CsrProblem:
+    """A MatrixMarket system as Alien's reader loads it (see
+    include/ab2_problems.h); b = 1 without an rhs file; x_true is None."""
+    p = C.POINTER(Problem)()
+    rc = lib().ab2_problem_read_matrix_market(str(path).encode(), None if rhs is None else str(rhs).encode(),
+                                              C.byref(p))
+    if rc:
+        raise AB2Error(rc, lib().ab2_matrix_market_error().decode())
+    return _take(p)
+
+
+def write_matrix_market(P: CsrProblem, path, rhs=None) -> None:
+    """Writes P's matrix ("coordinate real general") and, with rhs, its b."""
+    keep = [np.ascontiguousarray(P.row_ptr, np.int32), np.ascontiguousarray(P.cols, np.int32),
+            np.ascontiguousarray(P.vals, np.float64), np.ascontiguousarray(P.b, np.float64)]
+    pr = Problem()
+    pr.n, pr.nnz, pr.nx, pr.ny, pr.nz = P.n, P.nnz, P.n, 1, 1
+    pr.row_ptr = keep[0].ctypes.data_as(_IP)
+    pr.cols = keep[1].ctypes.data_as(_IP)
+    pr.vals = keep[2].ctypes.data_as(_DP)
+    pr.b = keep[3].ctypes.data_as(_DP)
+    rc = lib().ab2_problem_write_matrix_market(C.byref(pr), str(path).encode(),
+                                               None if rhs is None else str(rhs).encode())
+    if rc:
+        raise AB2Error(rc, lib().ab2_matrix_market_error().decode())
 
 
 def poisson(nx, ny=None, nz=None, seed=0) -> CsrProblem:

@@ -59,6 +59,21 @@ int ab2_problem_convdiff(int nx, int ny, int nz, double peclet, int modes, uint6
 
 int ab2_problem_destroy(ab2_problem* p);
 
+/* MatrixMarket files (the reference reads them with
+ * src/movesemantic/alien/move/impl/MatrixMarketReader.cc:58-157 and
+ * benchmarks them through benchmark/src/alien/benchmark/MatrixMarketProblem.cpp).
+ * Matrix: "%%MatrixMarket matrix coordinate real <symmetry>" -- any symmetry
+ * but "general" is mirrored with the same value, duplicates are summed in
+ * file order, columns come out ascending per row; square only.  rhs_path: an
+ * "array real" file with one value per line, or NULL for b = 1.  x_true is
+ * NULL and nx = n, ny = nz = 1.  Errors return AB2_ERR_BAD_ARG with the text
+ * in ab2_matrix_market_error(). */
+int ab2_problem_read_matrix_market(const char* matrix_path, const char* rhs_path, ab2_problem** out);
+/* "coordinate real general" with 17 significant digits (exact round trip), and
+ * b as "array real" (rhs_path may be NULL). */
+int ab2_problem_write_matrix_market(const ab2_problem* p, const char* matrix_path, const char* rhs_path);
+const char* ab2_matrix_market_error(void);
+
 /* The generator's random streams, for tests. */
 uint64_t ab2_rng_u64(uint64_t seed, uint64_t stream, uint64_t index);
 double ab2_rng_uniform(uint64_t seed, uint64_t stream, uint64_t index); /* [-1, 1) */
