@@ -207,6 +207,110 @@ __global__ void __launch_bounds__(kCtlThreads) k_cg_update(int n, const T* __res
   }
 }
 
+// ------------------------------------------------------------------ CG with Diag or no preconditioner
+// The same iteration in two kernels instead of five (precond, r.z, p, SpMV,
+// update): the update kernel also applies the Jacobi scaling and reduces r.z
+// for the next iteration beside r.r, and the SpMV kernel forms p = z + beta p
+// on the fly, reading the previous p from the other of two buffers (a row's
+// neighbours must still see the old values).  Every element is computed with
+// the operations, operands and order of the five-kernel form and every dot in
+// the same grid and tree, so the iterates are bit-identical; the loop moves
+// 96 n instead of 128 n vector bytes and launches 2 kernels per iteration.
+// The p buffers alternate with the body count (bodies & 1).
+
+// Before the loop: z = D^-1 r (inv = nullptr: z = r), rho1 = r.z, beta = 0.
+template <class T>
+__global__ void __launch_bounds__(kCtlThreads) k_cgj_start(int n, const T* __restrict__ r, const T* __restrict__ inv,
+                                                           T* __restrict__ z, SolveStateT<T>* st, Red<T> red) {
+  T acc[1] = {T(0)};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const T rv = r[i];
+    const T zv = inv ? mul_rn(inv[i], rv) : rv;
+    z[i] = zv;
+    acc[0] = fma_rn(rv, zv, acc[0]);
+  }
+  if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) {
+    st->rho1 = red.result[0];
+    st->beta = T(0);
+  }
+}
+
+// p = first ? z : z + beta p_old (into the other buffer) ; q = A p ; den = q.p
+template <class View, class T>
+__global__ void __launch_bounds__(kCtlThreads) k_cgj_spmv(int n, View A, const T* __restrict__ z, T* p0, T* p1,
+                                                          T* __restrict__ q, SolveStateT<T>* st, Red<T> red) {
+  if (st->done) return;  // every block returns: the reduction below is skipped as a whole
+  const int par = st->bodies & 1;
+  const T* __restrict__ po = par ? p1 : p0;
+  T* __restrict__ pn = par ? p0 : p1;
+  const T beta = st->beta;
+  const int first = st->first;
+  auto pval = [&](int c) { return first ? z[c] : fma_rn(beta, po[c], z[c]); };
+  T acc[1] = {T(0)};
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    const T qv = A.row_f(row, pval);
+    const T pr = pval(row);
+    pn[row] = pr;
+    q[row] = qv;
+    acc[0] = fma_rn(qv, pr, acc[0]);
+  }
+  if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) st->den = red.result[0];
+}
+
+// alpha = rho1/den ; x += alpha p ; r -= alpha q ; z = D^-1 r ; r.r (stop test) and r.z (next rho1).
+template <class T>
+__global__ void __launch_bounds__(kCtlThreads) k_cgj_update(int n, const T* p0, const T* p1, const T* __restrict__ q,
+                                                            T* __restrict__ r, T* __restrict__ z,
+                                                            const T* __restrict__ inv, SolveStateT<T>* st, Red<T> red,
+                                                            cudaGraphConditionalHandle h, int use_graph) {
+  if (st->done) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(h, use_graph, 0);
+    return;
+  }
+  const T* __restrict__ p = (st->bodies & 1) ? p0 : p1;  // the buffer k_cgj_spmv wrote
+  const T den = st->den;
+  const bool ok = den != T(0);
+  const T alpha = ok ? st->rho1 / den : T(0);
+  T* x = st->x;
+  T acc[2] = {T(0), T(0)};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    T rv = r[i];
+    if (ok) {
+      x[i] = fma_rn(alpha, p[i], x[i]);
+      rv = fma_rn(-alpha, q[i], rv);
+      r[i] = rv;
+    }
+    acc[0] = fma_rn(rv, rv, acc[0]);
+    const T zv = inv ? mul_rn(inv[i], rv) : rv;
+    z[i] = zv;
+    acc[1] = fma_rn(rv, zv, acc[1]);
+  }
+  if (grid_reduce<2>(acc, red.partials, red.counter, red.result)) {
+    const T rr = red.result[0];
+    const T rz = red.result[1];
+    st->bodies += 1;
+    if (!ok) {
+      // CG.h:96-104 / 131-139: converged after all, or breakdown "alpha"
+      if (stop_test(st, rr)) st->iter += 1;
+      else {
+        st->error = AB2_ERR_BREAKDOWN;
+        st->breakdown = AB2_BREAKDOWN_ALPHA;
+      }
+      st->done = 1;
+    } else {
+      st->alpha = alpha;
+      st->rho = st->rho1;
+      st->iter += 1;
+      st->first = 0;
+      // the next iteration's rho1 = r.z and beta = rho1 / rho (CG.h:117-118)
+      st->rho1 = rz;
+      st->beta = rz / st->rho;
+      if (stop_test(st, rr)) st->done = 1;
+    }
+    set_loop(h, use_graph, !st->done);
+  }
+}
+
 // ------------------------------------------------------------------ BiCGStab
 // p = r (first) or p = r + beta (p - omega v)  (BiCGStab.h:273-276, three BLAS-1 calls)
 template <class T>
@@ -392,7 +496,16 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
   const int ge = grid_for(n);
   const long long before = ctx->launches;
   SolveStateT<T>* st = d_st;
-  if (solver == AB2_SOLVER_CG) {
+  if (fused_diag) {
+    T *r = w[0], *z = w[1], *p0 = w[2], *q = w[3], *p1 = w[4];
+    with_view<T>(A, variant, [&](auto view) {
+      k_cgj_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z, p0, p1, q, st, red_of<T>(ctx, 2));
+    });
+    check_launch(ctx, "cgj_spmv");
+    k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p1, q, r, z, diag_inv(), st, red_of<T>(ctx, 3), h,
+                                                     graph_loop);
+    check_launch(ctx, "cgj_update");
+  } else if (solver == AB2_SOLVER_CG) {
     T *r = w[0], *z = w[1], *p = w[2], *q = w[3];
     pc_apply_t(ctx, pc, r, z);
     k_cg_rz<<<g, kCtlThreads, 0, ctx->stream>>>(n, r, z, st, red_of<T>(ctx, 1));
@@ -426,6 +539,13 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
     check_launch(ctx, "bicg_update");
   }
   return (int)(ctx->launches - before);
+}
+
+template <class T>
+const T* Krylov<T>::diag_inv() const {
+  if (pc->kind != AB2_PC_DIAG) return nullptr;
+  if constexpr (sizeof(T) == sizeof(double)) return pc->d_inv;
+  else return pc->d_inv32;
 }
 
 template <class T>
@@ -464,7 +584,8 @@ void Krylov<T>::init(ab2_context* c, const ab2_matrix* a, const ab2_precond* p, 
   solver = solver_kind;
   variant = spmv_variant;
   use_graph = graph_loop;
-  const int nw = solver == AB2_SOLVER_CG ? 4 : 8;
+  fused_diag = solver == AB2_SOLVER_CG && pc && (pc->kind == AB2_PC_DIAG || pc->kind == AB2_PC_NONE);
+  const int nw = fused_diag ? 5 : solver == AB2_SOLVER_CG ? 4 : 8;
   for (int i = 0; i < nw; ++i) {
     w[i] = dev_alloc<T>(ctx, (size_t)A->n);
     AB2_CUDA(cudaMemsetAsync(w[i], 0, sizeof(T) * (size_t)std::max(A->n, 1), ctx->stream));
@@ -493,6 +614,10 @@ void Krylov<T>::solve(const T* b, T* x, T tol, int max_iter) {
     k_residual<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, d_st, w[0], r0, red_of<T>(ctx, 0));
   });
   check_launch(ctx, "residual");
+  if (fused_diag) {
+    k_cgj_start<<<g, kCtlThreads, 0, ctx->stream>>>(n, w[0], diag_inv(), w[1], d_st, red_of<T>(ctx, 1));
+    check_launch(ctx, "cgj_start");
+  }
   // Null right-hand side: the reference returns before any iteration.
   AB2_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(SolveStateT<T>), cudaMemcpyDeviceToHost, ctx->stream));
   AB2_CUDA(cudaStreamSynchronize(ctx->stream));

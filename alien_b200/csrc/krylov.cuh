@@ -39,7 +39,7 @@ struct Krylov {
   int solver = AB2_SOLVER_CG;
   int variant = AB2_SPMV_AUTO;
   int use_graph = 1;
-  T* w[8] = {};  // CG: r z p q ; BiCGStab: r r0 p phat v s shat t
+  T* w[8] = {};  // CG: r z p q (+ p' for the two-kernel body) ; BiCGStab: r r0 p phat v s shat t
   SolveStateT<T>* d_st = nullptr;
   SolveStateT<T>* h_st = nullptr;  // pinned copy, valid after solve()
   T* d_hist = nullptr;
@@ -48,6 +48,7 @@ struct Krylov {
   cudaGraphExec_t exec = nullptr;
   cudaGraphConditionalHandle handle = 0;
   int body_launches = 0;
+  bool fused_diag = false;  // CG with Diag or no preconditioner: the two-kernel body
 
   // Allocates the work vectors (max_iter sizes the history) and builds the graph.
   void init(ab2_context* c, const ab2_matrix* a, const ab2_precond* p, int solver_kind, int spmv_variant, int graph_loop,
@@ -61,6 +62,7 @@ struct Krylov {
  private:
   int enqueue_body(cudaGraphConditionalHandle h, int graph_loop);
   void build_graph();
+  const T* diag_inv() const;  // 1/a_ii of a Diag preconditioner in T, else null
 };
 
 }  // namespace ab2

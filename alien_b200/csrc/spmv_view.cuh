@@ -20,6 +20,14 @@ struct CsrView {
     for (int k = rp[r]; k < e; ++k) acc = mul_add_rn(__ldcs(v + k), __ldg(x + __ldcs(ci + k)), acc);
     return acc;
   }
+  // The same sum with the operand x[c] given by f(c) (computed on the fly).
+  template <class F>
+  __device__ __forceinline__ T row_f(int r, F&& f) const {
+    T acc = 0;
+    const int e = rp[r + 1];
+    for (int k = rp[r]; k < e; ++k) acc = mul_add_rn(__ldcs(v + k), f(__ldcs(ci + k)), acc);
+    return acc;
+  }
 };
 
 template <class T>
@@ -35,6 +43,33 @@ struct EllView {
     const int* cp = ci + base;
     const T* vp = v + base;
     return ell_row_sum(cp, vp, w, x);
+  }
+  template <class F>
+  __device__ __forceinline__ T row_f(int r, F&& f) const {
+    const int s = r >> 5, lane = r & 31;
+    const int o = off[s];
+    const int w = off[s + 1] - o;
+    const size_t base = (size_t)o * kEllSlice + lane;
+    const int* cp = ci + base;
+    const T* vp = v + base;
+    T acc = 0;
+    for (int j = 0; j < w; j += 8) {
+      int c[8];
+      T a[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const bool in = j + u < w;
+        c[u] = in ? __ldcs(cp + (size_t)(j + u) * kEllSlice) : -1;
+        a[u] = in ? __ldcs(vp + (size_t)(j + u) * kEllSlice) : (T)0;
+      }
+      T xv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? f(c[u]) : (T)0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (c[u] >= 0) acc = mul_add_rn(a[u], xv[u], acc);
+    }
+    return acc;
   }
 
   // Slots in groups of 8, all loads of a group issued before the first use
