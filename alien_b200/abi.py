@@ -1,4 +1,4 @@
-"""ctypes binding of libab2 (include/ab2.h, include/ab2_problems.h).
+"""ctypes binding of libab2 (include/ab2.h, include/ab2_dist.h, include/ab2_problems.h).
 
 This is the Python face of the C ABI, shaped like Alien's algebra/solver API
 (SimpleCSRInternalLinearAlgebra method names, the krylov example's solver and
@@ -123,6 +123,13 @@ class FcgStatus(C.Structure):
                 ("solve_ms", C.c_double)]
 
 
+class DistInfo(C.Structure):
+    _fields_ = [("global_rows", C.c_int), ("local_rows", C.c_int), ("ghost_rows", C.c_int),
+                ("interface_rows", C.c_int), ("recv_neighbours", C.c_int), ("send_neighbours", C.c_int),
+                ("send_count", C.c_int), ("first_upper_ghost_index", C.c_int), ("local_nnz", C.c_longlong),
+                ("ghost_nnz", C.c_longlong)]
+
+
 class Problem(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("row_ptr", C.POINTER(C.c_int)), ("cols", C.POINTER(C.c_int)), ("vals", C.POINTER(C.c_double)),
@@ -211,6 +218,28 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_gnn_destroy": (_I, [_P]),
     "ab2_fcg_options_default": (None, [C.POINTER(FcgOptions)]),
     "ab2_fcg_solve": (_I, [_P, _P, _P, _P, _P, _P, C.POINTER(FcgOptions), C.POINTER(FcgStatus)]),
+    "ab2_comm_local_group": (_I, [C.POINTER(_P), _I, _D, C.POINTER(_P)]),
+    "ab2_comm_nccl_unique_id": (_I, [C.POINTER(C.c_ubyte)]),
+    "ab2_comm_nccl_create": (_I, [_P, C.POINTER(C.c_ubyte), _I, _I, C.POINTER(_P)]),
+    "ab2_comm_rank": (_I, [_P, _IP]),
+    "ab2_comm_size": (_I, [_P, _IP]),
+    "ab2_comm_destroy": (_I, [_P]),
+    "ab2_dist_matrix_create": (_I, [_P, _P, _IP, _IP, _IP, _DP, _I, C.POINTER(_P)]),
+    "ab2_dist_matrix_get_info": (_I, [_P, C.POINTER(DistInfo)]),
+    "ab2_dist_matrix_layout": (_I, [_P, _IP, _IP, _DP, _IP, _IP, _IP]),
+    "ab2_dist_matrix_plan": (_I, [_P, _IP, _IP, _IP, _IP, _IP]),
+    "ab2_dist_matrix_local": (_I, [_P, C.POINTER(_P)]),
+    "ab2_dist_matrix_destroy": (_I, [_P]),
+    "ab2_dist_vector_create": (_I, [_P, _P, C.POINTER(_P)]),
+    "ab2_dist_mult": (_I, [_P, _P, _P, _P]),
+    "ab2_dist_dot": (_I, [_P, _P, _P, _P, _DP]),
+    "ab2_dist_norm1": (_I, [_P, _P, _P, _DP]),
+    "ab2_dist_norm2": (_I, [_P, _P, _P, _DP]),
+    "ab2_dist_precond_create": (_I, [_P, _P, C.POINTER(PrecondOptions), C.POINTER(_P)]),
+    "ab2_dist_solver_create": (_I, [_P, _P, _P, C.POINTER(SolverOptions), C.POINTER(_P)]),
+    "ab2_dist_solver_solve": (_I, [_P, _P, _P, C.POINTER(Status)]),
+    "ab2_dist_solver_history": (_I, [_P, _DP, _I, _IP]),
+    "ab2_dist_solver_destroy": (_I, [_P]),
     "ab2_problem_poisson": (_I, [_I, _I, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_diffusion": (_I, [_I, _I, _I, _D, _D, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_convdiff": (_I, [_I, _I, _I, _D, _I, C.c_uint64, C.POINTER(C.POINTER(Problem))]),
@@ -406,9 +435,12 @@ class Matrix:
 
 
 class Vector:
-    def __init__(self, ctx: Context, n: int):
+    def __init__(self, ctx: Context, n: int, handle=None):
         self.ctx = ctx
         self.n = n
+        if handle is not None:  # created elsewhere (ab2_dist_vector_create)
+            self.h = handle
+            return
         h = _P()
         ctx.check(lib().ab2_vector_create(ctx.h, n, C.byref(h)), "vector_create")
         self.h = h
@@ -550,6 +582,214 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+
+# ---------------------------------------------------------------------------- row-block distribution
+class Comm:
+    """One rank of an ab2_comm (include/ab2_dist.h).  Collective calls must be
+    made by every rank in the same order; with a local group each rank is
+    driven by its own thread (ctypes releases the GIL during the calls)."""
+
+    def __init__(self, ctx: Context, handle):
+        self.ctx, self.h = ctx, handle
+
+    @staticmethod
+    def local_group(ctxs: list[Context], timeout_s: float = 120.0) -> list["Comm"]:
+        k = len(ctxs)
+        arr = (_P * k)(*[c.h for c in ctxs])
+        out = (_P * k)()
+        ctxs[0].check(lib().ab2_comm_local_group(arr, k, timeout_s, out), "comm_local_group")
+        return [Comm(c, _P(out[i])) for i, c in enumerate(ctxs)]
+
+    @staticmethod
+    def nccl_unique_id() -> bytes:
+        buf = (C.c_ubyte * 128)()
+        rc = lib().ab2_comm_nccl_unique_id(buf)
+        if rc != AB2_OK:
+            raise AB2Error(rc, "comm_nccl_unique_id")
+        return bytes(buf)
+
+    @staticmethod
+    def nccl(ctx: Context, uid: bytes, rank: int, size: int) -> "Comm":
+        buf = (C.c_ubyte * 128).from_buffer_copy(uid)
+        h = _P()
+        ctx.check(lib().ab2_comm_nccl_create(ctx.h, buf, rank, size, C.byref(h)), "comm_nccl_create")
+        return Comm(ctx, h)
+
+    @property
+    def rank(self) -> int:
+        r = C.c_int()
+        lib().ab2_comm_rank(self.h, C.byref(r))
+        return r.value
+
+    @property
+    def size(self) -> int:
+        r = C.c_int()
+        lib().ab2_comm_size(self.h, C.byref(r))
+        return r.value
+
+    def dot(self, x: Vector, y: Vector) -> float:
+        r = C.c_double()
+        self.ctx.check(lib().ab2_dist_dot(self.ctx.h, self.h, x.h, y.h, C.byref(r)), "dist_dot")
+        return r.value
+
+    def norm1(self, x: Vector) -> float:
+        r = C.c_double()
+        self.ctx.check(lib().ab2_dist_norm1(self.ctx.h, self.h, x.h, C.byref(r)), "dist_norm1")
+        return r.value
+
+    def norm2(self, x: Vector) -> float:
+        r = C.c_double()
+        self.ctx.check(lib().ab2_dist_norm2(self.ctx.h, self.h, x.h, C.byref(r)), "dist_norm2")
+        return r.value
+
+    def close(self):
+        if self.h:
+            lib().ab2_comm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DistMatrix:
+    """This rank's rows of a row-block distributed matrix (ab2_dist_matrix);
+    cols in global numbering.  Creation is collective."""
+
+    def __init__(self, ctx: Context, comm: Comm, offsets, row_ptr, cols, vals, formats: int = FMT_CSR | FMT_ELL):
+        self.ctx, self.comm = ctx, comm
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        ci = np.ascontiguousarray(cols, dtype=np.int32)
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        h = _P()
+        ctx.check(lib().ab2_dist_matrix_create(ctx.h, comm.h, _ip(self.offsets), _ip(rp), _ip(ci), _dp(v), formats,
+                                               C.byref(h)), "dist_matrix_create")
+        self.h = h
+        self.n = int(self.offsets[comm.rank + 1] - self.offsets[comm.rank])
+
+    @classmethod
+    def from_global(cls, ctx: Context, comm: Comm, offsets, row_ptr, cols, vals, formats: int = FMT_CSR | FMT_ELL):
+        """This rank's block of a global CSR matrix."""
+        r = comm.rank
+        a, b = int(offsets[r]), int(offsets[r + 1])
+        rp = np.asarray(row_ptr)
+        lo, hi = int(rp[a]), int(rp[b])
+        return cls(ctx, comm, offsets, rp[a:b + 1] - lo, np.asarray(cols)[lo:hi], np.asarray(vals)[lo:hi], formats)
+
+    @property
+    def info(self) -> DistInfo:
+        i = DistInfo()
+        self.ctx.check(lib().ab2_dist_matrix_get_info(self.h, C.byref(i)))
+        return i
+
+    def layout(self) -> dict:
+        i = self.info
+        nnz = i.local_nnz + i.ghost_nnz
+        out = dict(row_ptr=np.empty(i.local_rows + 1, np.int32), cols=np.empty(nnz, np.int32),
+                   vals=np.empty(nnz, np.float64), local_row_size=np.empty(i.local_rows, np.int32),
+                   ghost_uids=np.empty(i.ghost_rows, np.int32), interface_rows=np.empty(i.interface_rows, np.int32))
+        self.ctx.check(lib().ab2_dist_matrix_layout(self.h, _ip(out["row_ptr"]), _ip(out["cols"]), _dp(out["vals"]),
+                                                    _ip(out["local_row_size"]), _ip(out["ghost_uids"]),
+                                                    _ip(out["interface_rows"])))
+        return out
+
+    def plan(self) -> dict:
+        i = self.info
+        out = dict(recv_ranks=np.empty(i.recv_neighbours, np.int32), recv_offsets=np.empty(i.recv_neighbours + 1, np.int32),
+                   send_ranks=np.empty(i.send_neighbours, np.int32), send_offsets=np.empty(i.send_neighbours + 1, np.int32),
+                   send_ids=np.empty(i.send_count, np.int32))
+        self.ctx.check(lib().ab2_dist_matrix_plan(self.h, _ip(out["recv_ranks"]), _ip(out["recv_offsets"]),
+                                                  _ip(out["send_ranks"]), _ip(out["send_offsets"]), _ip(out["send_ids"])))
+        return out
+
+    def vector(self, values=None) -> Vector:
+        """A vector of this rank's rows with room for the ghost values."""
+        h = _P()
+        self.ctx.check(lib().ab2_dist_vector_create(self.ctx.h, self.h, C.byref(h)), "dist_vector_create")
+        v = Vector(self.ctx, self.n, handle=h)
+        if values is not None:
+            v.upload(values)
+        return v
+
+    def mult(self, x: Vector, y: Vector):
+        self.ctx.check(lib().ab2_dist_mult(self.ctx.h, self.h, x.h, y.h), "dist_mult")
+
+    def close(self):
+        if self.h:
+            lib().ab2_dist_matrix_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DistPrecond(Precond):
+    """NONE, DIAG or block-Jacobi ILU0 over this rank's rows (ab2_dist_precond_create)."""
+
+    def __init__(self, ctx: Context, A: DistMatrix, kind: str = "ilu0", ilu_schedule: str = "auto"):
+        self.ctx, self.A = ctx, A
+        o = PrecondOptions(PRECOND[kind], 0.0, 3, 10, ILU_SCHEDULE[ilu_schedule], 0, 0, 0, 3, 0.0)
+        h = _P()
+        ctx.check(lib().ab2_dist_precond_create(ctx.h, A.h, C.byref(o), C.byref(h)), "dist_precond_create")
+        self.h = h
+
+    def ilu0_values(self) -> np.ndarray:
+        out = np.empty(self.A.info.local_nnz, dtype=np.float64)
+        self.ctx.check(lib().ab2_precond_ilu0_values(self.ctx.h, self.h, _dp(out)), "ilu0_values")
+        return out
+
+
+class DistSolver:
+    """ab2_dist_solver: CG on the distributed algebra, device-resident; solve() is collective."""
+
+    def __init__(self, ctx: Context, comm: Comm, A: DistMatrix, **opts):
+        self.ctx, self.comm, self.A = ctx, comm, A
+        self.opts = solver_options(**opts)
+        h = _P()
+        ctx.check(lib().ab2_dist_solver_create(ctx.h, comm.h, A.h, C.byref(self.opts), C.byref(h)),
+                  "dist_solver_create")
+        self.h = h
+
+    def solve(self, b: Vector, x: Vector) -> SolveResult:
+        st = Status()
+        self.ctx.check(lib().ab2_dist_solver_solve(self.h, b.h, x.h, C.byref(st)), "dist_solve")
+        return SolveResult(bool(st.succeeded), st.iterations, st.error, BREAKDOWN.get(st.breakdown), st.residual,
+                           st.true_residual, st.nrm2_b, st.setup_ms, st.solve_ms)
+
+    def history(self) -> np.ndarray:
+        n = C.c_int()
+        lib().ab2_dist_solver_history(self.h, None, 0, C.byref(n))
+        out = np.empty(max(n.value, 0), dtype=np.float64)
+        if n.value:
+            self.ctx.check(lib().ab2_dist_solver_history(self.h, _dp(out), n.value, C.byref(n)), "history")
+        return out
+
+    def close(self):
+        if self.h:
+            lib().ab2_dist_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def row_offsets(n: int, nranks: int, align: int = 1) -> np.ndarray:
+    """Contiguous row blocks of nearly equal size (multiples of align rows,
+    e.g. a grid plane, except the last block)."""
+    units = -(-n // align)
+    cuts = [min(n, (units * r // nranks) * align) for r in range(nranks)] + [n]
+    return np.asarray(cuts, dtype=np.int32)
 
 
 @dataclass

@@ -51,6 +51,7 @@ struct ab2_vector {
   ab2_context* ctx = nullptr;
   int n = 0;
   double* d = nullptr;
+  int cap = 0;  // doubles allocated (> n for distributed vectors: room for ghost values)
 };
 
 struct ab2_scalar {

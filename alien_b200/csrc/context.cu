@@ -244,6 +244,7 @@ int ab2_vector_create(ab2_context* ctx, int n, ab2_vector** out) {
   v->ctx = ctx_retain(ctx);
   int rc = guard(ctx, [&] {
     v->n = n;
+    v->cap = n;
     v->d = dev_alloc<double>(v->ctx, (size_t)n);
     AB2_CUDA(cudaMemsetAsync(v->d, 0, sizeof(double) * (size_t)std::max(n, 1), ctx->stream));
   });

@@ -459,7 +459,7 @@ int bulk_grid(ab2_context* ctx, long long n) {
 
 }  // namespace
 
-bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d) {
+bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool factored) {
   const int n = A->n;
   const int* rp = A->h_rp.data();
   const int* ci = A->h_ci.data();
@@ -495,14 +495,22 @@ bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d) {
   d.d_tile_tickets = dev_alloc<unsigned int>(ctx, 3);
   AB2_CUDA(cudaMemsetAsync(d.d_tile_tickets, 0, 3 * sizeof(unsigned int), ctx->stream));
   const Bands b = bands_of(d.d_bands, n);
-  k_stencil_extract<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, g, A->d_rp, A->d_v, b);
-  check_launch(ctx, "stencil_extract");
-  k_fill_bits<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, kSentinel, b.P);
-  check_launch(ctx, "stencil_fill");
-  k_stencil_factor<<<wave_grid(ctx, g.ntx * g.nty), kTileThreads, 0, ctx->stream>>>(g, b, d.d_tile_tickets, d.d_err);
-  check_launch(ctx, "stencil_factor");
-  k_stencil_pack<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, g, A->d_rp, b, d.d_lu);
-  check_launch(ctx, "stencil_pack");
+  if (factored) {
+    // d_lu holds the factor: its diagonal is the pivot band.
+    k_stencil_extract<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, g, A->d_rp, d.d_lu, b);
+    check_launch(ctx, "stencil_extract");
+    AB2_CUDA(cudaMemcpyAsync(b.P, b.D, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
+  } else {
+    k_stencil_extract<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, g, A->d_rp, A->d_v, b);
+    check_launch(ctx, "stencil_extract");
+    k_fill_bits<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, kSentinel, b.P);
+    check_launch(ctx, "stencil_fill");
+    k_stencil_factor<<<wave_grid(ctx, g.ntx * g.nty), kTileThreads, 0, ctx->stream>>>(g, b, d.d_tile_tickets,
+                                                                                         d.d_err);
+    check_launch(ctx, "stencil_factor");
+    k_stencil_pack<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, g, A->d_rp, b, d.d_lu);
+    check_launch(ctx, "stencil_pack");
+  }
 
   // The sweeps' arrays in walk order.
   const Walk w = walk_of(d);

@@ -313,7 +313,7 @@ int sweep_blocks(ab2_context* ctx, int len, int widest_chunks) {
 
 }  // namespace
 
-void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule) {
+void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule, const double* lu) {
   const ab2_matrix* A = pc->A;
   Ilu0Data& d = pc->ilu;
   d.d_lu = dev_alloc<double>(ctx, (size_t)A->nnz);
@@ -322,13 +322,15 @@ void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule) {
   d.d_err = dev_alloc<int>(ctx, 1);
   AB2_CUDA(cudaMemsetAsync(d.d_counters, 0, 2 * sizeof(unsigned int), ctx->stream));
   AB2_CUDA(cudaMemsetAsync(d.d_err, 0, sizeof(int), ctx->stream));
-  AB2_CUDA(cudaMemcpyAsync(d.d_lu, A->d_v, sizeof(double) * (size_t)A->nnz, cudaMemcpyDeviceToDevice, ctx->stream));
+  AB2_CUDA(cudaMemcpyAsync(d.d_lu, lu ? lu : A->d_v, sizeof(double) * (size_t)A->nnz, cudaMemcpyDeviceToDevice,
+                           ctx->stream));
   k_fill_bits<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, kSentinel, d.d_tmp);
   check_launch(ctx, "ilu_fill");
-  if (schedule != AB2_ILU_WAVEFRONT && ilu_stencil_setup(ctx, A, d)) return;
+  if (schedule != AB2_ILU_WAVEFRONT && ilu_stencil_setup(ctx, A, d, lu != nullptr)) return;
   require(schedule != AB2_ILU_STENCIL, "ILU0 tile schedule requested but the matrix is not a 3-D 7-point "
                                        "matrix in lexicographic order");
   ilu_symbolic(A, d);
+  if (lu) return;
   for (int l = 1; l < d.levels_l; ++l) {  // wavefront 0 rows have nothing left of the diagonal
     const int a = d.lev_ptr_l[l], b = d.lev_ptr_l[l + 1];
     const int cnt = b - a;

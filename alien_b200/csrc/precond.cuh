@@ -42,8 +42,9 @@ struct Ilu0Data {
 };
 
 // Detects a 3-D 7-point matrix in lexicographic order and, if found,
-// factorises it on the tile-walk schedule (bands + CSR copy in d_lu).
-bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d);
+// factorises it on the tile-walk schedule (bands + CSR copy in d_lu); with
+// factored, d_lu already holds the factor and only the walk arrays are built.
+bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool factored = false);
 void ilu_stencil_apply(ab2_context* ctx, const ab2_matrix* A, const Ilu0Data& d, const double* y, double* z);
 // Puts the sweeps' propagation arrays back to the sentinel (after a failed application).
 void ilu_stencil_reset(ab2_context* ctx, const Ilu0Data& d);
@@ -93,7 +94,9 @@ struct NeumannData {
 };
 
 // ILU(0) set-up into pc->ilu (precond.cu): factor plus the sweep schedule.
-void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule);
+// With lu (device, A's CSR profile) the factor is taken as given -- the
+// block-Jacobi factor of a distributed matrix -- and only the schedule is built.
+void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule, const double* lu = nullptr);
 void filu_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o);
 void neumann_init(ab2_context* ctx, ab2_precond* pc, const ab2_precond_options* o);
 template <class T>

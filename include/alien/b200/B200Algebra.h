@@ -116,6 +116,13 @@ class Vector {
     m_h.reset();
     m_n = 0;
   }
+  // Takes ownership of a vector made elsewhere in the C ABI (e.g. a
+  // distributed vector with room for ghost values).
+  void adopt(const Context& ctx, ab2_vector* h, int n) {
+    m_h = std::shared_ptr<ab2_vector>(h, [](ab2_vector* v) { ab2_vector_destroy(v); });
+    m_ctx = ctx.handle();
+    m_n = n;
+  }
   void upload(const double* host) { check(ab2_vector_upload(m_ctx, m_h.get(), host), "ab2_vector_upload"); }
   void download(double* host) const { check(ab2_vector_download(m_ctx, m_h.get(), host), "ab2_vector_download"); }
   std::vector<double> download() const {

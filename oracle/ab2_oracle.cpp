@@ -176,9 +176,26 @@ thread_local int g_tree_blocks = 1184;
 thread_local bool g_cheb_saad = false;
 thread_local bool g_cheb_lanczos = false;
 
+// Row-block distribution in effect (orc_dist_solve): every dot is each rank's
+// local dot over its rows, summed over the ranks left to right (CBLASMPIKernel
+// dot + mpAllReduce; MPI leaves the order of that sum open, libab2 fixes this one).
+thread_local const std::vector<int>* g_dist_off = nullptr;
+
+template <class T>
+T local_dot(int n, const T* x, const T* y) {
+  return g_dot_mode == 1 ? tree_dot(n, x, y, g_tree_blocks) : dot(n, x, y);
+}
+
 template <class T>
 T vdot(int n, const T* x, const T* y) {
-  return g_dot_mode == 1 ? tree_dot(n, x, y, g_tree_blocks) : dot(n, x, y);
+  if (!g_dist_off) return local_dot(n, x, y);
+  const std::vector<int>& off = *g_dist_off;
+  T s = 0;
+  for (size_t r = 0; r + 1 < off.size(); ++r) {
+    const T p = local_dot(off[r + 1] - off[r], x + off[r], y + off[r]);
+    s = r == 0 ? p : s + p;
+  }
+  return s;
 }
 
 // Stop test shared by CG (Iteration.h) and BiCGStab (its nested Iteration).
@@ -633,9 +650,164 @@ struct Cheb : Precond<T> {
   }
 };
 
+// ---------------------------------------------------------------- row-block distribution
+// One rank's rows in the layout of DistStructInfo::compute
+// (kernels/simple_csr/DistStructInfo.cc:44-233) after sortGhostCols
+// (SimpleCSRMatrix.h:215-258): in each row the local columns first (local id =
+// global id - base), then the ghost columns (id n + g, ghosts numbered by
+// owning rank, ascending global id inside each owner); lrs = local entries per
+// row; interface rows = rows with a ghost entry.
+struct DistLocal {
+  int n = 0, base = 0, nghost = 0;
+  std::vector<int> rp, ci, lrs, ghost_uids, iface;
+  std::vector<double> v;
+};
+
+DistLocal dist_local(const Csr& A, const std::vector<int>& off, int r) {
+  DistLocal L;
+  L.base = off[r];
+  L.n = off[r + 1] - off[r];
+  const int np = (int)off.size() - 1;
+  auto owner = [&](int c) {
+    int q = 0;
+    while (c >= off[q + 1]) ++q;
+    return q;
+  };
+  std::vector<std::vector<int>> gids(np);
+  L.rp.assign(1, 0);
+  for (int i = 0; i < L.n; ++i) {
+    const int g = L.base + i;
+    int nl = 0;
+    for (int k = A.rp[g]; k < A.rp[g + 1]; ++k)
+      if (owner(A.ci[k]) == r) {
+        L.ci.push_back(A.ci[k] - L.base);
+        L.v.push_back(A.v[k]);
+        ++nl;
+      }
+    for (int k = A.rp[g]; k < A.rp[g + 1]; ++k)
+      if (owner(A.ci[k]) != r) {
+        L.ci.push_back(-1 - A.ci[k]);  // global id, numbered below
+        L.v.push_back(A.v[k]);
+        gids[owner(A.ci[k])].push_back(A.ci[k]);
+      }
+    L.lrs.push_back(nl);
+    L.rp.push_back((int)L.ci.size());
+    if (L.rp[i + 1] - L.rp[i] > nl) L.iface.push_back(i);
+  }
+  for (auto& v : gids) {
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    L.ghost_uids.insert(L.ghost_uids.end(), v.begin(), v.end());
+  }
+  L.nghost = (int)L.ghost_uids.size();
+  for (auto& c : L.ci)
+    if (c < 0) c = L.n + (int)(std::lower_bound(L.ghost_uids.begin(), L.ghost_uids.end(), -1 - c) - L.ghost_uids.begin());
+  return L;
+}
+
+struct DistCsr {
+  int n = 0;  // global rows
+  std::vector<int> off;
+  std::vector<DistLocal> ranks;
+  DistCsr(const Csr& A, const std::vector<int>& o) : n(A.n), off(o) {
+    for (size_t r = 0; r + 1 < off.size(); ++r) ranks.push_back(dist_local(A, off, (int)r));
+  }
+};
+
+// SimpleCSRMatrixMultT::_parallelMult (:85-128): each row's local entries
+// summed (tmpy from 0, a*x rounded apart), then the interface rows add the sum
+// of their ghost entries; ghost values are the owners' entries of x.
+void spmv(const DistCsr& A, const double* x, double* y) {
+  for (const DistLocal& L : A.ranks) {
+    std::vector<double> xe(L.n + L.nghost);
+    for (int i = 0; i < L.n; ++i) xe[i] = x[L.base + i];
+    for (int g = 0; g < L.nghost; ++g) xe[L.n + g] = x[L.ghost_uids[g]];
+    for (int i = 0; i < L.n; ++i) {
+      double t = 0.;
+      for (int k = L.rp[i]; k < L.rp[i] + L.lrs[i]; ++k) t += L.v[k] * xe[L.ci[k]];
+      y[L.base + i] = t;
+    }
+    for (int i : L.iface) {
+      double t = 0.;
+      for (int k = L.rp[i] + L.lrs[i]; k < L.rp[i + 1]; ++k) t += L.v[k] * xe[L.ci[k]];
+      y[L.base + i] += t;
+    }
+  }
+}
+
+// DistStructInfo::computeUpperDiagOffset: first local position not below the row.
+std::vector<int> dist_dcol(const DistLocal& L) {
+  std::vector<int> d(L.n);
+  for (int i = 0; i < L.n; ++i) {
+    int k = L.rp[i];
+    while (k < L.rp[i] + L.lrs[i] && L.ci[k] < i) ++k;
+    d[i] = k;
+  }
+  return d;
+}
+
+// The parallel block-Jacobi factorisation of ILU0Preconditioner.h:93-119,
+// loop bounds as written there: row i is eliminated by row krow = col(k) only
+// at positions j in (k, kcol[krow] + lrs[i]), with krow's local columns marked.
+// With a single rank the matrix is not parallel (m_is_parallel = nproc > 1)
+// and the sequential branch runs: rows eliminated up to their end (:156-178).
+void bj_ilu0_factor(const DistLocal& L, const std::vector<int>& d, std::vector<double>& lu, bool parallel) {
+  std::vector<int> work(L.n + L.nghost, -1);
+  const int nnz = L.rp[L.n];
+  for (int i = 1; i < L.n; ++i)
+    for (int k = L.rp[i]; k < d[i]; ++k) {
+      const int kr = L.ci[k];
+      const double aik = lu[k] / (d[kr] < nnz ? lu[d[kr]] : 0.0);
+      lu[k] = aik;
+      for (int l = L.rp[kr]; l < L.rp[kr] + L.lrs[kr]; ++l) work[L.ci[l]] = l;
+      const int bound = parallel ? L.rp[kr] + L.lrs[i] : L.rp[i + 1];
+      for (int j = k + 1; j < bound; ++j) {
+        const int kj = work[L.ci[j]];
+        if (kj != -1) lu[j] = lu[j] - aik * lu[kj];
+      }
+      for (int l = L.rp[kr]; l < L.rp[kr] + L.lrs[kr]; ++l) work[L.ci[l]] = -1;
+    }
+}
+
+// Block-Jacobi ILU(0): every rank factorises its rows (local columns only;
+// one rank: the sequential ILU(0)) and sweeps them (solveL over local entries left of dcol, solveU over local
+// entries right of it: ILU0Preconditioner.h:181-231, parallel branches).
+struct BjIlu0 : Precond<double> {
+  const DistCsr& A;
+  std::vector<std::vector<int>> d;
+  std::vector<std::vector<double>> lu;
+  std::vector<double> t;
+  explicit BjIlu0(const DistCsr& M) : A(M), t(M.n) {
+    for (const DistLocal& L : A.ranks) {
+      d.push_back(dist_dcol(L));
+      lu.push_back(L.v);
+      bj_ilu0_factor(L, d.back(), lu.back(), A.ranks.size() > 1);
+    }
+  }
+  void apply(const double* y, double* x) override {
+    for (size_t r = 0; r < A.ranks.size(); ++r) {
+      const DistLocal& L = A.ranks[r];
+      const std::vector<int>& dc = d[r];
+      const std::vector<double>& f = lu[r];
+      double* tt = t.data() + L.base;
+      for (int i = 0; i < L.n; ++i) {
+        double v = y[L.base + i];
+        for (int k = L.rp[i]; k < dc[i]; ++k) v = v - f[k] * tt[L.ci[k]];
+        tt[i] = v;
+      }
+      double* xx = x + L.base;
+      for (int i = L.n - 1; i >= 0; --i) {
+        double v = tt[i];
+        for (int k = dc[i] + 1; k < L.rp[i] + L.lrs[i]; ++k) v = v - f[k] * xx[L.ci[k]];
+        xx[i] = v / f[dc[i]];
+      }
+    }
+  }
+};
+
 // ---------------------------------------------------------------- solvers
-template <class T>
-void cg(const CsrT<T>& A, Precond<T>& M, StopTest<T>& it, const T* b, T* x) {
+template <class T, class Mat>
+void cg(const Mat& A, Precond<T>& M, StopTest<T>& it, const T* b, T* x) {
   if (it.null_rhs()) return;
   const int n = A.n;
   std::vector<T> p(n), z(n), q(n), r(n);
@@ -679,8 +851,8 @@ void cg(const CsrT<T>& A, Precond<T>& M, StopTest<T>& it, const T* b, T* x) {
   }
 }
 
-template <class T>
-void bicgstab(const CsrT<T>& A, Precond<T>& M, StopTest<T>& it, const T* b, T* x) {
+template <class T, class Mat>
+void bicgstab(const Mat& A, Precond<T>& M, StopTest<T>& it, const T* b, T* x) {
   if (it.null_rhs()) return;
   const int n = A.n;
   std::vector<T> p(n), phat(n), s(n), shat(n), t(n), v(n), r(n), r0(n);
@@ -1243,6 +1415,116 @@ int orc_ell_layout(int n, const int* rp, const int* ci, const double* v, int S, 
     }
   }
   return ORC_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- row-block distribution (C)
+extern "C" {
+
+// One rank's layout: sizes[0..3] = local rows, ghosts, interface rows, entries;
+// the arrays (any may be null) as ab2_dist_matrix_layout fills them.
+int orc_dist_layout(int n, const int* rp, const int* ci, const double* v, int nranks, const int* offsets, int rank,
+                    int* sizes, int* out_rp, int* out_ci, double* out_v, int* lrs, int* ghost_uids, int* iface) {
+  if (nranks < 1 || rank < 0 || rank >= nranks || offsets[0] != 0 || offsets[nranks] != n) return ORC_ERR_BAD_ARG;
+  const std::vector<int> off(offsets, offsets + nranks + 1);
+  const DistLocal L = dist_local(Csr{n, rp, ci, v}, off, rank);
+  if (sizes) {
+    sizes[0] = L.n;
+    sizes[1] = L.nghost;
+    sizes[2] = (int)L.iface.size();
+    sizes[3] = L.rp[L.n];
+  }
+  if (out_rp) std::copy(L.rp.begin(), L.rp.end(), out_rp);
+  if (out_ci) std::copy(L.ci.begin(), L.ci.end(), out_ci);
+  if (out_v) std::copy(L.v.begin(), L.v.end(), out_v);
+  if (lrs) std::copy(L.lrs.begin(), L.lrs.end(), lrs);
+  if (ghost_uids) std::copy(L.ghost_uids.begin(), L.ghost_uids.end(), ghost_uids);
+  if (iface) std::copy(L.iface.begin(), L.iface.end(), iface);
+  return ORC_OK;
+}
+
+// y = A x with A distributed by offsets (each rank's _parallelMult).
+int orc_dist_spmv(int n, const int* rp, const int* ci, const double* v, int nranks, const int* offsets, const double* x,
+                  double* y) {
+  if (nranks < 1 || offsets[0] != 0 || offsets[nranks] != n) return ORC_ERR_BAD_ARG;
+  spmv(DistCsr(Csr{n, rp, ci, v}, std::vector<int>(offsets, offsets + nranks + 1)), x, y);
+  return ORC_OK;
+}
+
+// Sum over ranks of the local dots (dot_mode / tree_blocks as orc_options).
+double orc_dist_dot(int nranks, const int* offsets, const double* x, const double* y, int dot_mode, int tree_blocks) {
+  const std::vector<int> off(offsets, offsets + nranks + 1);
+  g_dot_mode = dot_mode;
+  g_tree_blocks = tree_blocks > 0 ? tree_blocks : 1184;
+  g_dist_off = &off;
+  const double s = vdot(offsets[nranks], x, y);
+  g_dist_off = nullptr;
+  return s;
+}
+
+// Block-Jacobi ILU(0): x = M^-1 y over all ranks; lu (optional) receives each
+// rank's factor on its local entries, rank after rank, in the diagonal
+// block's CSR order (what ab2_precond_ilu0_values returns on that rank).
+int orc_bj_ilu0_apply(int n, const int* rp, const int* ci, const double* v, int nranks, const int* offsets,
+                      const double* y, double* x, double* lu) {
+  if (nranks < 1 || offsets[0] != 0 || offsets[nranks] != n) return ORC_ERR_BAD_ARG;
+  const DistCsr A(Csr{n, rp, ci, v}, std::vector<int>(offsets, offsets + nranks + 1));
+  BjIlu0 M(A);
+  M.apply(y, x);
+  if (lu) {
+    size_t o = 0;
+    for (size_t r = 0; r < A.ranks.size(); ++r) {
+      const DistLocal& L = A.ranks[r];
+      for (int i = 0; i < L.n; ++i)
+        for (int p = 0; p < L.lrs[i]; ++p) lu[o++] = M.lu[r][L.rp[i] + p];
+    }
+  }
+  return ORC_OK;
+}
+
+// The solve every rank runs on the distributed algebra: CG or BiCGStab with
+// NONE, DIAG or ILU0 (block Jacobi).  Same conventions as orc_solve.
+int orc_dist_solve(int n, const int* rp, const int* ci, const double* v, int nranks, const int* offsets, const double* b,
+                   double* x, const orc_options* o, orc_result* res, double* hist, int hist_cap) {
+  if (!o || !res || nranks < 1 || offsets[0] != 0 || offsets[nranks] != n) return ORC_ERR_BAD_ARG;
+  std::memset(res, 0, sizeof(*res));
+  g_dot_mode = o->dot_mode;
+  g_tree_blocks = o->tree_blocks > 0 ? o->tree_blocks : 1184;
+  const std::vector<int> off(offsets, offsets + nranks + 1);
+  const Csr G{n, rp, ci, v};
+  const DistCsr A(G, off);
+  Identity<double> pid(n);
+  Precond<double>* M = &pid;
+  Diag<double>* pd = nullptr;
+  BjIlu0* pb = nullptr;
+  switch (o->precond) {
+    case ORC_PC_NONE: break;
+    case ORC_PC_DIAG: M = pd = new Diag<double>(G); break;
+    case ORC_PC_ILU0: M = pb = new BjIlu0(A); break;
+    default: return ORC_ERR_BAD_ARG;
+  }
+  g_dist_off = &off;
+  int rc = ORC_OK;
+  StopTest<double> it(n, b, o->tol, o->max_iter, hist, hist_cap);
+  try {
+    if (o->solver == ORC_SOLVER_CG) cg(A, *M, it, b, x);
+    else if (o->solver == ORC_SOLVER_BICGSTAB) bicgstab(A, *M, it, b, x);
+    else rc = ORC_ERR_BAD_ARG;
+  } catch (const Breakdown& e) {
+    rc = ORC_ERR_BREAKDOWN;
+    res->breakdown = e.which;
+  }
+  g_dist_off = nullptr;
+  res->iterations = it.iter;
+  res->converged = it.status ? 1 : 0;
+  res->error = rc;
+  res->nrm2_b = it.nrm2_b;
+  res->last_rr = it.last;
+  res->history_len = it.hist_len;
+  delete pd;
+  delete pb;
+  return rc;
 }
 
 }  // extern "C"

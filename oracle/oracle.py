@@ -128,6 +128,13 @@ def orc() -> C.CDLL:
                                       C.c_double, C.c_int, C.c_int, C.c_int, _IP, _IP, _IP, _DP]
         L.orc_mixed_solve.argtypes = [C.c_int, _IP, _IP, _DP, _DP, _DP, C.POINTER(MixedOptions),
                                       C.POINTER(MixedResult), _DP, C.c_int]
+        L.orc_dist_layout.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, _IP, C.c_int, _IP, _IP, _IP, _DP, _IP, _IP, _IP]
+        L.orc_dist_spmv.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, _IP, _DP, _DP]
+        L.orc_dist_dot.argtypes = [C.c_int, _IP, _DP, _DP, C.c_int, C.c_int]
+        L.orc_dist_dot.restype = C.c_double
+        L.orc_bj_ilu0_apply.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, _IP, _DP, _DP, _DP]
+        L.orc_dist_solve.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, _IP, _DP, _DP, C.POINTER(Options),
+                                     C.POINTER(Result), _DP, C.c_int]
         _orc = L
     return _orc
 
@@ -141,6 +148,7 @@ def ref() -> C.CDLL:
     if _ref is None:
         _ref = _load(REF_SO, "ref")
         _ref.ref_set_cheb_saad.argtypes = [C.c_int]
+        _ref.ref_bj_ilu0_apply.argtypes = [C.c_int, C.c_int, _IP, _IP, _DP, _IP, _DP, _DP, _DP]
     return _ref
 
 
@@ -423,3 +431,82 @@ def batch_solve(row_ptr, cols, vals, sys_offsets, b, x0=None, tol=1e-8, max_oute
     orc().orc_batch_solve(n, _ip(rp), _ip(ci), _dp(v), ns, _ip(off), _dp(bb), _dp(x), tol, max_outer, inner_tol,
                           inner_max_iter, cluster_size, threads, _ip(conv), _ip(outer), _ip(inner), _dp(res))
     return BatchSolve(x, conv.astype(bool), outer, inner, res)
+
+
+# ---------------------------------------------------------------------------- row-block distribution
+def dist_layout(row_ptr, cols, vals, offsets, rank) -> dict:
+    """One rank's rows in the reference's distributed layout (DistStructInfo)."""
+    rp, ci, v, off = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(offsets, np.int32)
+    n, k = rp.size - 1, off.size - 1
+    sz = np.zeros(4, np.int32)
+    orc().orc_dist_layout(n, _ip(rp), _ip(ci), _dp(v), k, _ip(off), rank, _ip(sz), None, None, None, None, None, None)
+    nl, ng, ni, nnz = (int(t) for t in sz)
+    out = dict(row_ptr=np.empty(nl + 1, np.int32), cols=np.empty(nnz, np.int32), vals=np.empty(nnz),
+               local_row_size=np.empty(nl, np.int32), ghost_uids=np.empty(ng, np.int32),
+               interface_rows=np.empty(ni, np.int32))
+    orc().orc_dist_layout(n, _ip(rp), _ip(ci), _dp(v), k, _ip(off), rank, _ip(sz), _ip(out["row_ptr"]),
+                          _ip(out["cols"]), _dp(out["vals"]), _ip(out["local_row_size"]), _ip(out["ghost_uids"]),
+                          _ip(out["interface_rows"]))
+    return out
+
+
+def dist_spmv(row_ptr, cols, vals, offsets, x) -> np.ndarray:
+    rp, ci, v, off, xx = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(offsets, np.int32), \
+        _c(x, np.float64)
+    y = np.empty(rp.size - 1)
+    orc().orc_dist_spmv(rp.size - 1, _ip(rp), _ip(ci), _dp(v), off.size - 1, _ip(off), _dp(xx), _dp(y))
+    return y
+
+
+def dist_dot(offsets, x, y, dot_mode=DOT_SEQUENTIAL, tree_blocks=1184) -> float:
+    off, xx, yy = _c(offsets, np.int32), _c(x, np.float64), _c(y, np.float64)
+    return orc().orc_dist_dot(off.size - 1, _ip(off), _dp(xx), _dp(yy), dot_mode, tree_blocks)
+
+
+def bj_ilu0_apply(row_ptr, cols, vals, offsets, y):
+    """Block-Jacobi ILU(0) over the row blocks: (x, per-rank factors on their local entries)."""
+    rp, ci, v, off, yy = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(offsets, np.int32), \
+        _c(y, np.float64)
+    n = rp.size - 1
+    x = np.empty(n)
+    lu = np.empty(ci.size)
+    orc().orc_bj_ilu0_apply(n, _ip(rp), _ip(ci), _dp(v), off.size - 1, _ip(off), _dp(yy), _dp(x), _dp(lu))
+    # split per rank: each rank's local entries
+    parts, o = [], 0
+    for r in range(off.size - 1):
+        L = dist_layout(rp, ci, v, off, r)
+        m = int(L["local_row_size"].sum())
+        parts.append(lu[o:o + m].copy())
+        o += m
+    return x, parts
+
+
+def ref_bj_ilu0_apply(layout: dict, y):
+    """The reference's parallel LUFactorisationAlgo on one rank's layout: (x, factor in distributed order)."""
+    rp, ci, v, lrs = (_c(layout[k], dt) for k, dt in (("row_ptr", np.int32), ("cols", np.int32),
+                                                        ("vals", np.float64), ("local_row_size", np.int32)))
+    n = rp.size - 1
+    yy = _c(y, np.float64)
+    x = np.empty(n)
+    lu = np.empty(ci.size)
+    ref().ref_bj_ilu0_apply(n, int(layout["ghost_uids"].size), _ip(rp), _ip(ci), _dp(v), _ip(lrs), _dp(yy), _dp(x),
+                            _dp(lu))
+    return x, lu
+
+
+def dist_solve(row_ptr, cols, vals, offsets, b, x0=None, solver="cg", precond="diag", tol=1e-8, max_iter=1000,
+               dot_mode=DOT_SEQUENTIAL, tree_blocks=1184) -> OracleSolve:
+    """The solve every rank runs on the distributed algebra (block-Jacobi ILU0,
+    dots summed over the ranks in rank order)."""
+    rp, ci, v, bb, off = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(b, np.float64), \
+        _c(offsets, np.int32)
+    n = rp.size - 1
+    x = np.zeros(n) if x0 is None else _c(x0, np.float64).copy()
+    o = Options(SOLVER[solver], PRECOND[precond], tol, max_iter, 0.0, 3, 10, dot_mode, tree_blocks, 0, 0, 0, 3)
+    r = Result()
+    cap = 2 * max_iter + 8
+    hist = np.zeros(cap)
+    orc().orc_dist_solve(n, _ip(rp), _ip(ci), _dp(v), off.size - 1, _ip(off), _dp(bb), _dp(x), C.byref(o), C.byref(r),
+                         _dp(hist), cap)
+    return OracleSolve(x, r.iterations, bool(r.converged), r.error, BREAKDOWN.get(r.breakdown), r.nrm2_b, r.last_rr,
+                       0.0, 0.0, hist[:min(r.history_len, cap)].copy())

@@ -69,13 +69,33 @@ struct Profile {
   const int* dcol() const { return dc.data(); }
 };
 
+// The members of DistStructInfo (kernels/simple_csr/DistStructInfo.h) the
+// parallel branches of LUFactorisationAlgo read: the rank's columns in the
+// distributed numbering (local ids, then ghost ids), the number of local
+// entries of each row, and dcol(profile) -- computeUpperDiagOffset
+// (DistStructInfo.h:77-92): per row, the first local position whose column is
+// not below the row.
 struct DistInfo {
   std::vector<int> m_local_row_size;
   std::vector<int> m_cols;
   int m_first_upper_ghost_index = 0;
   int m_send_info = 0;  // FILU0's parallel branch names these; never taken here
   int m_recv_info = 0;
-  const int* dcol(const Profile&) const { return nullptr; }
+  mutable std::vector<int> m_upper_diag_offset;
+  const int* dcol(const Profile& p) const {
+    if (m_upper_diag_offset.empty()) {
+      m_upper_diag_offset.resize((std::size_t)p.n);
+      for (int i = 0; i < p.n; ++i) {
+        int idx = p.rp[(std::size_t)i];
+        for (int k = p.rp[(std::size_t)i]; k < p.rp[(std::size_t)i] + m_local_row_size[(std::size_t)i]; ++k) {
+          if (m_cols[(std::size_t)k] < i) ++idx;
+          else break;
+        }
+        m_upper_diag_offset[(std::size_t)i] = idx;
+      }
+    }
+    return m_upper_diag_offset.data();
+  }
 };
 
 struct Matrix {
@@ -90,11 +110,13 @@ struct Matrix {
   DistInfo dist_info;
   MatrixDistribution dist;
 
-  bool isParallel() const { return false; }
+  bool parallel = false;  // one rank of a row-block distribution (dist_info filled)
+  int ghosts = 0;
+  bool isParallel() const { return parallel; }
   int getSendPolicy() const { return 0; }
   int getRecvPolicy() const { return 0; }
   void* getParallelMng() const { return nullptr; }
-  std::size_t getAllocSize() const { return (std::size_t)profile->n; }
+  std::size_t getAllocSize() const { return (std::size_t)(profile->n + ghosts); }
   MatrixDistribution const& distribution() const { return dist; }
   Matrix* cloneTo(void*) const { return new Matrix(*this); }
   Profile const& getProfile() const { return *profile; }
@@ -448,6 +470,36 @@ int ref_ilu0_apply(int n, const int* rp, const int* ci, const double* v, const d
   vy.v.assign(y, y + n);
   vx.v.assign((std::size_t)n, 0.0);
   alg.exec(pc, vy, vx);
+  std::memcpy(x, vx.v.data(), sizeof(double) * (size_t)n);
+  return 0;
+}
+
+// One rank's block-Jacobi ILU(0): the reference's LUFactorisationAlgo with
+// isParallel() true (ILU0Preconditioner.h:93-119 factorisation, :181-231
+// sweeps) on the rank's rows in the distributed layout (rp, ci with local ids
+// then ghost ids n.., lrs = local entries per row).  lu receives the factor
+// (rp[n] values, distributed order), x = (LU)^-1 y.
+int ref_bj_ilu0_apply(int n, int ghosts, const int* rp, const int* ci, const double* v, const int* lrs, const double* y,
+                      double* x, double* lu) {
+  ShimAlgebra alg;
+  Alien::shim::Matrix A;
+  A.profile = std::make_shared<Alien::shim::Profile>();
+  A.profile->n = n;
+  A.profile->rp.assign(rp, rp + n + 1);
+  A.profile->ci.assign(ci, ci + rp[n]);  // the profile's own columns are not read on this branch
+  A.values.assign(v, v + rp[n]);
+  A.parallel = true;
+  A.ghosts = ghosts;
+  A.dist_info.m_local_row_size.assign(lrs, lrs + n);
+  A.dist_info.m_cols.assign(ci, ci + rp[n]);
+  Alien::LUFactorisationAlgo<Alien::shim::Matrix, Alien::shim::Vector> algo;
+  algo.init(alg, A);
+  const Alien::shim::Matrix& LU = algo.getLUMatrix();
+  if (lu) std::memcpy(lu, LU.values.data(), sizeof(double) * (size_t)rp[n]);
+  Alien::shim::Vector vy, vx;
+  vy.v.assign(y, y + n);
+  vx.v.assign((std::size_t)n, 0.0);
+  algo.solve(alg, vy, vx);
   std::memcpy(x, vx.v.data(), sizeof(double) * (size_t)n);
   return 0;
 }
