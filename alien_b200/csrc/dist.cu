@@ -56,6 +56,7 @@ struct LocalGroup {
     const double* send[2] = {nullptr, nullptr};
     const HaloPlan* plan[2] = {nullptr, nullptr};
     double* pub[2] = {nullptr, nullptr};            // kMaxRedComps partials
+    char op[2] = {0, 0};                            // 'h' halo, 'g' gather: ranks must agree
     std::vector<int> host;
   };
   std::vector<Slot> slots;
@@ -97,6 +98,13 @@ struct LocalComm : ab2_comm {
     return all;
   }
 
+  // Every rank has to be in the same collective: a mismatch would read a
+  // peer's buffers of another kind.
+  void check_peers(int parity, char op) {
+    for (int q = 0; q < size; ++q)
+      require(g->slots[(size_t)q].op[parity] == op, "local group: ranks are in different collectives");
+  }
+
   void before_publish(int parity) override {
     for (int q = 0; q < size; ++q)
       if (q != rank) AB2_CUDA(cudaStreamWaitEvent(ctx->stream, g->slots[(size_t)q].consumed[parity], 0));
@@ -106,8 +114,10 @@ struct LocalComm : ab2_comm {
     LocalGroup::Slot& s = me();
     s.send[parity] = sendbuf;
     s.plan[parity] = &plan;
+    s.op[parity] = 'h';
     AB2_CUDA(cudaEventRecord(s.produced[parity], ctx->stream));
     g->barrier();
+    check_peers(parity, 'h');
     // The ghost room is free once this rank's earlier work is done.
     AB2_CUDA(cudaStreamWaitEvent(cs, s.produced[parity], 0));
     for (size_t i = 0; i + 1 < plan.recv_off.size(); ++i) {
@@ -131,8 +141,10 @@ struct LocalComm : ab2_comm {
   void allgather(int parity, const double* in, int k, double* out) override {
     LocalGroup::Slot& s = me();
     AB2_CUDA(cudaMemcpyAsync(s.pub[parity], in, sizeof(double) * k, cudaMemcpyDeviceToDevice, ctx->stream));
+    s.op[parity] = 'g';
     AB2_CUDA(cudaEventRecord(s.produced[parity], ctx->stream));
     g->barrier();
+    check_peers(parity, 'g');
     for (int q = 0; q < size; ++q) {
       const LocalGroup::Slot& ps = g->slots[(size_t)q];
       AB2_CUDA(cudaStreamWaitEvent(cs, ps.produced[parity], 0));
