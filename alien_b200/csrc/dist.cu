@@ -145,6 +145,9 @@ struct LocalComm : ab2_comm {
     AB2_CUDA(cudaEventRecord(s.produced[parity], ctx->stream));
     g->barrier();
     check_peers(parity, 'g');
+    // out is this rank's buffer: the copies start after this rank's earlier
+    // work, which includes the sum kernel that read out last time.
+    AB2_CUDA(cudaStreamWaitEvent(cs, s.produced[parity], 0));
     for (int q = 0; q < size; ++q) {
       const LocalGroup::Slot& ps = g->slots[(size_t)q];
       AB2_CUDA(cudaStreamWaitEvent(cs, ps.produced[parity], 0));

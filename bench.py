@@ -460,6 +460,71 @@ def preconditioner_section(abi, ctx, stream, A, P, a):
     return out
 
 
+def rowblock_section(abi, stream, P, x_single, iters_single, a):
+    """The row-block distribution (include/ab2_dist.h) on the headline system:
+    the device-resident distributed CG + ILU0 with one rank over NCCL (its
+    solution must equal the single-GPU solver's bit for bit), and 2, 4, 8
+    ranks of a local group SHARING this one GPU -- the iteration counts of
+    block-Jacobi ILU(0) as the slabs shrink and the cost of the distributed
+    machinery; their times are not a scaling measurement."""
+    import threading
+
+    out = {"note": "1 rank over NCCL, then R ranks sharing one GPU (threads of one process, host barriers): "
+                   "times of shared-GPU runs are not multi-GPU scaling"}
+    n = P.n
+    plane = a.n * a.n
+
+    def solve_rank(ctx, comm, off, r, res):
+        t0 = time.perf_counter()
+        A = abi.DistMatrix.from_global(ctx, comm, off, P.row_ptr, P.cols, P.vals)
+        S = abi.DistSolver(ctx, comm, A, solver="cg", precond="ilu0", tol=1e-8, max_iter=a.max_iter)
+        b, x = A.vector(P.b[off[r]:off[r + 1]]), A.vector()
+        t1 = time.perf_counter()
+        st = S.solve(b, x)
+        res[r] = (st, x.download() if r == 0 or len(off) == 2 else None, t1 - t0, time.perf_counter() - t1)
+        S.close(), A.close(), b.close(), x.close()
+
+    try:
+        uid = abi.Comm.nccl_unique_id()
+        ctx = abi.Context(0)
+        comm = abi.Comm.nccl(ctx, uid, 0, 1)
+        off = np.asarray([0, n], np.int32)
+        res = [None]
+        solve_rank(ctx, comm, off, 0, res)  # warm
+        solve_rank(ctx, comm, off, 0, res)
+        st, xr, setup_s, solve_s = res[0]
+        out["nccl_1"] = {"iterations": st.iterations, "converged": bool(st.succeeded), "solve_ms": round(st.solve_ms, 2),
+                         "setup_s": round(setup_s, 3), "true_rel_residual": st.true_residual,
+                         "identical_to_single_gpu_solver": bool(np.array_equal(xr, x_single)
+                                                                and st.iterations == iters_single)}
+        comm.close()
+        ctx.close()
+    except abi.AB2Error as e:
+        out["nccl_1"] = {"unavailable": str(e)}
+
+    for k in (2, 4, 8):
+        off = abi.row_offsets(n, k, plane)
+        ctxs = [abi.Context(0) for _ in range(k)]
+        comms = abi.Comm.local_group(ctxs, timeout_s=600.0)
+        res = [None] * k
+        ts = [threading.Thread(target=solve_rank, args=(ctxs[r], comms[r], off, r, res)) for r in range(k)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        if any(v is None for v in res):
+            out[f"local_{k}"] = {"error": "a rank failed"}
+            continue
+        st = res[0][0]
+        out[f"local_{k}"] = {"ranks": k, "planes_per_rank": a.n // k, "iterations": st.iterations,
+                             "converged": bool(st.succeeded), "true_rel_residual": st.true_residual,
+                             "solve_ms_max_over_ranks": round(max(v[0].solve_ms for v in res), 2),
+                             "iterations_vs_one_rank": round(st.iterations / iters_single, 3)}
+        for c in comms:
+            c.close()
+    return out
+
+
 GNN_WEIGHTS = ROOT / "alien_b200" / "gnn_weights.npy"
 
 
@@ -609,6 +674,7 @@ def main():
     ap.add_argument("--batch-systems", type=int, default=512)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner measurement")
     ap.add_argument("--no-precond", action="store_true", help="skip the per-preconditioner measurements")
+    ap.add_argument("--no-rowblock", action="store_true", help="skip the row-block distribution measurements")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Krylov loop from the host instead of the CUDA graph (same kernels; for "
                          "profilers that do not see kernels inside conditional graph nodes)")
@@ -732,6 +798,8 @@ def main():
     batched = None if a.no_batch else batch_section(abi, ctx, stream, a)
     learned = None if a.no_learned else learned_section(abi, ctx, stream, a)
     preconds = None if a.no_precond else preconditioner_section(abi, ctx, stream, A, P, a)
+    rowblock = None if (a.no_rowblock or a.method != "ilu0" or world > 1) else \
+        rowblock_section(abi, stream, P, xs, st.iterations, a)
 
     pk, pk_kind = peaks()
     traffic = load_traffic()
@@ -818,7 +886,7 @@ def main():
                 "solver_gbs": round(st.iterations * iteration_bytes(a.method, P.n, P.nnz) / (st.solve_ms * 1e-3)
                                     / 1e9, 1),
                 "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "methods": methods, "mixed": mixed, "batched": batched,
-                "learned": learned, "preconditioners": preconds,
+                "learned": learned, "preconditioners": preconds, "rowblock": rowblock,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     from alien_b200 import dist

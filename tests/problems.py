@@ -20,6 +20,8 @@ def get(name: str) -> abi.CsrProblem:
         return abi.diffusion(12, 12, 12, sigma=1.0, smooth=2.0, seed=1)
     if name == "diffusion24":
         return abi.diffusion(24, 24, 24, sigma=1.0, smooth=4.0, seed=5)
+    if name == "diffusion64":
+        return abi.diffusion(64, 64, 64, sigma=1.0, smooth=4.0, seed=0)
     if name == "diffusion2d_31x9":
         return abi.diffusion(31, 9, 1, sigma=1.5, smooth=3.0, seed=7)
     if name == "convdiff_10x11x12":
