@@ -450,8 +450,11 @@ class Vector:
         assert a.size == self.n
         self.ctx.check(lib().ab2_vector_upload(self.ctx.h, self.h, _dp(a)), "upload")
 
-    def download(self) -> np.ndarray:
-        out = np.empty(self.n, dtype=np.float64)
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The vector's values; into `out` (contiguous float64, e.g. pinned memory) when given."""
+        if out is None:
+            out = np.empty(self.n, dtype=np.float64)
+        assert out.dtype == np.float64 and out.size == self.n and out.flags.c_contiguous
         self.ctx.check(lib().ab2_vector_download(self.ctx.h, self.h, _dp(out)), "download")
         return out
 

@@ -80,8 +80,10 @@ struct ab2_matrix {
   int* d_ell_ci = nullptr;    // -1 marks padding
   double* d_ell_v = nullptr;
   float* d_ell_v32 = nullptr;
-  // host mirror of the profile, used by symbolic set-up (ILU0 wavefronts)
-  std::vector<int> h_rp, h_ci;
+  // host mirror of the profile for symbolic set-ups (ILU0 wavefronts, batch
+  // checks), downloaded on first use by host_profile()
+  mutable std::vector<int> h_rp, h_ci;
+  mutable bool h_profile = false;
 };
 
 namespace ab2 {
@@ -215,5 +217,7 @@ void op_inv_diag(ab2_context* ctx, const ab2_matrix* A, double* inv);
 void op_diagonal(ab2_context* ctx, const ab2_matrix* A, double* d);
 void op_mult_inv_diag(ab2_context* ctx, const ab2_matrix* A, double* y);
 int resolve_variant(const ab2_matrix* A, int variant);
+// Fills A->h_rp / A->h_ci from the device once (synchronises the stream).
+void host_profile(const ab2_matrix* A);
 
 }  // namespace ab2

@@ -434,6 +434,7 @@ int ab2_batch_create(ab2_context* ctx, const ab2_matrix* A, int nsys, const int*
     return AB2_ERR_BAD_ARG;
   // systems: increasing offsets from 0 to n, each a diagonal block of A
   if (sys_offsets[0] != 0 || sys_offsets[nsys] != A->n) return AB2_ERR_BAD_ARG;
+  if (const int rc = guard(ctx, [&] { host_profile(A); }); rc != AB2_OK) return rc;
   for (int s = 0; s < nsys; ++s) {
     if (sys_offsets[s + 1] <= sys_offsets[s]) return AB2_ERR_BAD_ARG;
     for (int r = sys_offsets[s]; r < sys_offsets[s + 1]; ++r)

@@ -1055,6 +1055,7 @@ int ab2_gnn_bind(ab2_gnn* G, const ab2_matrix* A) {
     dev_free(ctx, d_bad);
     if (!bad) {
       int maxlen = 0;  // off-diagonal entries of the longest row (every row has its diagonal)
+      host_profile(A);
       for (int i = 0; i < n; ++i) maxlen = std::max(maxlen, A->h_rp[i + 1] - A->h_rp[i] - 1);
       G->nbw = std::max(2, (maxlen + 1) / 2 * 2);
       if (G->nbw > kMaxNbw) {

@@ -100,6 +100,21 @@ __global__ void k_stencil_check(int n, Geom g, const int* __restrict__ rp, const
   }
 }
 
+// geo[0] = min over rows with 7 entries (starts at n); then geo[1..2] = the
+// first two columns of that row.
+__global__ void k_first_full_row(int n, const int* __restrict__ rp, int* geo) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    if (rp[r + 1] - rp[r] == 7) atomicMin(geo, r);
+}
+
+__global__ void k_full_row_cols(int n, const int* __restrict__ rp, const int* __restrict__ ci, int* geo) {
+  const int r = geo[0];
+  if (r < n) {
+    geo[1] = ci[rp[r]];
+    geo[2] = ci[rp[r] + 1];
+  }
+}
+
 __global__ void k_stencil_extract(int n, Geom g, const int* __restrict__ rp, const double* __restrict__ v, Bands b) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const int i = r % g.nx, j = (r / g.nx) % g.ny, k = (int)(r / g.nxny);
@@ -461,18 +476,22 @@ int bulk_grid(ab2_context* ctx, long long n) {
 
 bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool factored) {
   const int n = A->n;
-  const int* rp = A->h_rp.data();
-  const int* ci = A->h_ci.data();
+  if (n == 0) return false;
   // Geometry from the first full row: its columns start r - nx ny, r - nx.
-  int r7 = -1;
-  for (int r = 0; r < n; ++r)
-    if (rp[r + 1] - rp[r] == 7) {
-      r7 = r;
-      break;
-    }
-  if (r7 < 0) return false;
-  const long long nxny = (long long)r7 - ci[rp[r7]];
-  const long long nx = (long long)r7 - ci[rp[r7] + 1];
+  int* d_geo = dev_alloc<int>(ctx, 3);
+  int geo[3] = {n, 0, 0};
+  AB2_CUDA(cudaMemcpyAsync(d_geo, geo, sizeof(geo), cudaMemcpyHostToDevice, ctx->stream));
+  k_first_full_row<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, d_geo);
+  check_launch(ctx, "first_full_row");
+  k_full_row_cols<<<1, 1, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, d_geo);
+  check_launch(ctx, "full_row_cols");
+  AB2_CUDA(cudaMemcpyAsync(geo, d_geo, sizeof(geo), cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  dev_free(ctx, d_geo);
+  const int r7 = geo[0];
+  if (r7 >= n) return false;
+  const long long nxny = (long long)r7 - geo[1];
+  const long long nx = (long long)r7 - geo[2];
   if (nx < 2 || nxny <= nx || nxny % nx != 0 || n % nxny != 0) return false;
   const long long ny = nxny / nx, nz = n / nxny;
   if (ny < 2 || nz < 2) return false;

@@ -243,6 +243,7 @@ __global__ void k_pmult2(int n, const T* __restrict__ a, const T* x, T* y) {
 }
 
 void ilu_symbolic(const ab2_matrix* A, Ilu0Data& d) {
+  host_profile(A);
   const int n = A->n;
   const int* rp = A->h_rp.data();
   const int* ci = A->h_ci.data();

@@ -185,25 +185,84 @@ __global__ void k_diagonal(int n, const int* __restrict__ rp, const int* __restr
   }
 }
 
-// Greedy row blocks: at most kThreads rows and kStageCap nonzeros per block
-// (a longer row gets a block of its own).
-std::vector<int> make_row_blocks(int n, const int* rp) {
-  std::vector<int> b;
-  b.push_back(0);
-  int r = 0;
-  while (r < n) {
-    int start = r;
+// Row blocks of the staged kernel, built on the device: every 256-row chunk is
+// split greedily into blocks of at most kStageCap entries (a longer row gets a
+// block of its own).  The staged kernel sums each row in column order whatever
+// the blocking, so only the launch shape depends on it.
+__device__ int chunk_blocks(int c, int n, const int* __restrict__ rp, int* out) {
+  const int end = min(n, (c + 1) * kThreads);
+  int r = c * kThreads, m = 0;
+  while (r < end) {
+    const int start = r;
     long long nz = 0;
-    while (r < n && r - start < kThreads) {
+    while (r < end) {
       const int len = rp[r + 1] - rp[r];
       if (nz + len > kStageCap) break;
       nz += len;
       ++r;
     }
-    if (r == start) ++r;  // a single row above the cap
-    b.push_back(r);
+    if (r == start) ++r;
+    if (out) out[m] = r;
+    ++m;
   }
-  return b;
+  return m;
+}
+
+__global__ void k_rowblock_count(int n, int nc, const int* __restrict__ rp, long long* __restrict__ cnt) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+    cnt[c] = chunk_blocks(c, n, rp, nullptr);
+}
+
+__global__ void k_rowblock_emit(int n, int nc, const int* __restrict__ rp, const long long* __restrict__ off,
+                                int* __restrict__ blocks) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+    chunk_blocks(c, n, rp, blocks + 1 + off[c]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) blocks[0] = 0;
+}
+
+// Longest row of every 32-row slice.
+__global__ void k_slice_width(int n, int ns, const int* __restrict__ rp, long long* __restrict__ w) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) {
+    int m = 0;
+    for (int r = s * kEllSlice; r < min(n, (s + 1) * kEllSlice); ++r) m = max(m, rp[r + 1] - rp[r]);
+    w[s] = m;
+  }
+}
+
+// out[i] = in[0] + ... + in[i-1] for i <= m (one block of 1024 threads: each
+// sums a contiguous segment, the segment sums are scanned in shared memory).
+__global__ void __launch_bounds__(1024) k_scan_excl(int m, const long long* __restrict__ in, long long* __restrict__ out) {
+  __shared__ long long s[1024];
+  const int t = threadIdx.x;
+  const int per = (m + 1023) / 1024;
+  const int a = min(m, t * per), b = min(m, a + per);
+  long long acc = 0;
+  for (int i = a; i < b; ++i) acc += in[i];
+  s[t] = acc;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    const long long v = t >= d ? s[t - d] : 0;
+    __syncthreads();
+    s[t] += v;
+    __syncthreads();
+  }
+  long long run = s[t] - acc;
+  for (int i = a; i < b; ++i) {
+    out[i] = run;
+    run += in[i];
+  }
+  if (t == 1023) out[m] = s[1023];
+}
+
+__global__ void k_narrow(int m, const long long* __restrict__ in, int* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) out[i] = (int)in[i];
+}
+
+long long read_ll(ab2_context* ctx, const long long* d) {
+  long long v = 0;
+  AB2_CUDA(cudaMemcpyAsync(&v, d, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  return v;
 }
 
 }  // namespace
@@ -283,6 +342,23 @@ static void refresh_values(ab2_context* ctx, ab2_matrix* A) {
 
 }  // namespace ab2
 
+namespace ab2 {
+
+void host_profile(const ab2_matrix* A) {
+  if (A->h_profile) return;
+  ab2_context* ctx = A->ctx;
+  A->h_rp.resize((size_t)A->n + 1);
+  A->h_ci.resize((size_t)A->nnz);
+  AB2_CUDA(cudaMemcpyAsync(A->h_rp.data(), A->d_rp, sizeof(int) * ((size_t)A->n + 1), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  if (A->nnz)
+    AB2_CUDA(cudaMemcpyAsync(A->h_ci.data(), A->d_ci, sizeof(int) * (size_t)A->nnz, cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  A->h_profile = true;
+}
+
+}  // namespace ab2
+
 using namespace ab2;
 
 extern "C" {
@@ -303,8 +379,6 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
     A->nnz = row_ptr[n];
     A->formats = (formats | AB2_FMT_CSR);
     const size_t nnz = (size_t)A->nnz;
-    A->h_rp.assign(row_ptr, row_ptr + n + 1);
-    A->h_ci.assign(cols, cols + nnz);
     A->d_rp = dev_alloc<int>(ctx, (size_t)n + 1, &A->device_bytes);
     A->d_ci = dev_alloc<int>(ctx, nnz, &A->device_bytes);
     A->d_v = dev_alloc<double>(ctx, nnz, &A->device_bytes);
@@ -328,29 +402,45 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
       k_dcol<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, A->d_dcol);
       check_launch(ctx, "dcol");
     }
-    std::vector<int> blocks = make_row_blocks(n, row_ptr);
-    A->n_row_blocks = (int)blocks.size() - 1;
-    A->d_row_blocks = dev_alloc<int>(ctx, blocks.size(), &A->device_bytes);
-    AB2_CUDA(cudaMemcpyAsync(A->d_row_blocks, blocks.data(), sizeof(int) * blocks.size(), cudaMemcpyHostToDevice,
-                             ctx->stream));
+    // Row blocks of the staged kernel (the profile is valid from here on).
+    {
+      const int nc = (n + kThreads - 1) / kThreads;
+      long long* d_cnt = dev_alloc<long long>(ctx, (size_t)nc + 1);
+      long long* d_off = dev_alloc<long long>(ctx, (size_t)nc + 1);
+      if (nc > 0) {
+        k_rowblock_count<<<grid_for(nc), kThreads, 0, ctx->stream>>>(n, nc, A->d_rp, d_cnt);
+        check_launch(ctx, "rowblock_count");
+      }
+      k_scan_excl<<<1, 1024, 0, ctx->stream>>>(nc, d_cnt, d_off);
+      check_launch(ctx, "rowblock_scan");
+      const long long nb = read_ll(ctx, d_off + nc);
+      A->n_row_blocks = (int)nb;
+      A->d_row_blocks = dev_alloc<int>(ctx, (size_t)nb + 1, &A->device_bytes);
+      k_rowblock_emit<<<grid_for(std::max(nc, 1)), kThreads, 0, ctx->stream>>>(n, nc, A->d_rp, d_off, A->d_row_blocks);
+      check_launch(ctx, "rowblock_emit");
+      dev_free(ctx, d_cnt);
+      dev_free(ctx, d_off);
+    }
     if (A->formats & AB2_FMT_ELL) {
       const int ns = (n + kEllSlice - 1) / kEllSlice;
-      std::vector<int> off((size_t)ns + 1);
-      long long acc = 0;
-      for (int s = 0; s < ns; ++s) {
-        off[s] = (int)acc;
-        int w = 0;
-        for (int l = 0; l < kEllSlice && s * kEllSlice + l < n; ++l)
-          w = std::max(w, row_ptr[s * kEllSlice + l + 1] - row_ptr[s * kEllSlice + l]);
-        acc += w;
+      long long* d_w = dev_alloc<long long>(ctx, (size_t)ns + 1);
+      long long* d_woff = dev_alloc<long long>(ctx, (size_t)ns + 1);
+      if (ns > 0) {
+        k_slice_width<<<grid_for(ns), kThreads, 0, ctx->stream>>>(n, ns, A->d_rp, d_w);
+        check_launch(ctx, "slice_width");
       }
-      require(acc * kEllSlice < (1LL << 31) * 8, "matrix too large for the sliced-ELL layout");
-      off[ns] = (int)acc;
+      k_scan_excl<<<1, 1024, 0, ctx->stream>>>(ns, d_w, d_woff);
+      check_launch(ctx, "slice_scan");
+      const long long acc = read_ll(ctx, d_woff + ns);
+      require(acc < (1LL << 31) && acc * kEllSlice < (1LL << 31) * 8, "matrix too large for the sliced-ELL layout");
       A->ell_stored = acc * kEllSlice;
-      A->d_ell_off = dev_alloc<int>(ctx, off.size(), &A->device_bytes);
+      A->d_ell_off = dev_alloc<int>(ctx, (size_t)ns + 1, &A->device_bytes);
       A->d_ell_ci = dev_alloc<int>(ctx, (size_t)A->ell_stored, &A->device_bytes);
       A->d_ell_v = dev_alloc<double>(ctx, (size_t)A->ell_stored, &A->device_bytes);
-      AB2_CUDA(cudaMemcpyAsync(A->d_ell_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, ctx->stream));
+      k_narrow<<<grid_for(ns + 1), kThreads, 0, ctx->stream>>>(ns + 1, d_woff, A->d_ell_off);
+      check_launch(ctx, "slice_offsets");
+      dev_free(ctx, d_w);
+      dev_free(ctx, d_woff);
       const int n_pad = ns * kEllSlice;
       if (n_pad > n) {
         k_ell_pad_tail<<<1, kEllSlice, 0, ctx->stream>>>(n, n_pad, A->d_ell_off, A->d_ell_ci);
