@@ -269,16 +269,97 @@ __global__ void k_walk_gather(Walk g, const S* __restrict__ src, T* __restrict__
   }
 }
 
+// Walk order <-> natural order for every application (y in, z out), both
+// sides coalesced.  A thread keeps one grid line (li, lj) of a tile: at walk
+// step s it owns cell k = s - li - lj, so at one step a warp touches 32
+// consecutive walk entries, and at one plane k a warp touches two runs of 16
+// consecutive natural rows.  Each thread stages its own cells in a ring of
+// planes in shared memory (its own column: no barrier) and moves a plane
+// once every lane has it.  One CTA per (tile, kTrPlanes planes).
+constexpr int kTrPlanes = 64;
+constexpr int kTrBatch = 4;                          // steps (planes) per batch
+constexpr int kTrRing = 2 * (kTile - 1) + kTrBatch;  // planes live at once per thread
+
+template <class T>
+constexpr int tr_smem() {
+  return kTrRing * kTileThreads * (int)sizeof(T);
+}
+
 // dst[row(w)] = src[w], and src[w] back to the sentinel for the next walk.
 template <class T>
-__global__ void k_walk_scatter(Walk g, T* __restrict__ src, T* __restrict__ dst) {
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < g.nw; w += (long long)gridDim.x * blockDim.x) {
-    const long long r = walk_row(g, w);
-    if (r >= 0) {
-      dst[r] = src[w];
-      src[w] = sentinel_of<T>();
+__global__ void __launch_bounds__(kTileThreads) k_walk_scatter_t(Walk g, T* __restrict__ src, T* __restrict__ dst) {
+  extern __shared__ unsigned char tr_smem_raw[];
+  T* ring = reinterpret_cast<T*>(tr_smem_raw);
+  const int nch = (g.nz + kTrPlanes - 1) / kTrPlanes;
+  const int tile = blockIdx.x / nch, ch = blockIdx.x - tile * nch;
+  const int t = threadIdx.x, li = t & (kTile - 1), lj = t >> 4, d = li + lj;
+  const int i = (tile % g.ntx) * kTile + li, j = (tile / g.ntx) * kTile + lj;
+  const bool line = i < g.nx && j < g.ny;
+  const int k0 = ch * kTrPlanes, k1 = min(g.nz, k0 + kTrPlanes);
+  const long long wb = (long long)tile * g.nsteps * kTileThreads + t;
+  const long long rb = i + (long long)g.nx * j;
+  int out = k0;
+  for (int s0 = k0; s0 < k1 + 2 * (kTile - 1); s0 += kTrBatch) {
+    // the batch's loads first (all in flight together), then the stores
+    T v[kTrBatch];
+#pragma unroll
+    for (int u = 0; u < kTrBatch; ++u) {
+      const int k = s0 + u - d;
+      v[u] = (line && k >= k0 && k < k1) ? __ldcs(src + wb + (long long)(s0 + u) * kTileThreads) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kTrBatch; ++u) {
+      const int k = s0 + u - d;
+      if (line && k >= k0 && k < k1) {
+        ring[(k % kTrRing) * kTileThreads + t] = v[u];
+        src[wb + (long long)(s0 + u) * kTileThreads] = sentinel_of<T>();
+      }
+    }
+    const int last = min(k1, s0 + kTrBatch - 2 * (kTile - 1));  // planes every lane has read
+    for (; out < last; ++out)
+      if (line) dst[rb + g.nxny * out] = ring[(out % kTrRing) * kTileThreads + t];
+  }
+}
+
+// dst[w] = src[row(w)] for the cells of the grid (padding entries are left
+// as they are: zero since set-up).
+template <class T>
+__global__ void __launch_bounds__(kTileThreads) k_walk_gather_t(Walk g, const T* __restrict__ src, T* __restrict__ dst) {
+  extern __shared__ unsigned char tr_smem_raw[];
+  T* ring = reinterpret_cast<T*>(tr_smem_raw);
+  const int nch = (g.nz + kTrPlanes - 1) / kTrPlanes;
+  const int tile = blockIdx.x / nch, ch = blockIdx.x - tile * nch;
+  const int t = threadIdx.x, li = t & (kTile - 1), lj = t >> 4, d = li + lj;
+  const int i = (tile % g.ntx) * kTile + li, j = (tile / g.ntx) * kTile + lj;
+  const bool line = i < g.nx && j < g.ny;
+  const int k0 = ch * kTrPlanes, k1 = min(g.nz, k0 + kTrPlanes);
+  const long long wb = (long long)tile * g.nsteps * kTileThreads + t;
+  const long long rb = i + (long long)g.nx * j;
+  int s = k0;  // next step to write
+  for (int p0 = k0; p0 < k1 + 2 * (kTile - 1); p0 += kTrBatch) {
+    T v[kTrBatch];
+#pragma unroll
+    for (int u = 0; u < kTrBatch; ++u) {
+      const int k = p0 + u;
+      v[u] = (line && k < k1) ? __ldcs(src + rb + g.nxny * k) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kTrBatch; ++u) {
+      const int k = p0 + u;
+      if (line && k < k1) ring[(k % kTrRing) * kTileThreads + t] = v[u];
+    }
+    const int last = p0 + kTrBatch;  // steps whose cells every lane has read
+    for (; s < last; ++s) {
+      const int k = s - d;
+      if (line && k >= k0 && k < k1) dst[wb + (long long)s * kTileThreads] = ring[(k % kTrRing) * kTileThreads + t];
     }
   }
+}
+
+template <class T>
+void set_transpose_smem() {
+  AB2_CUDA(cudaFuncSetAttribute(k_walk_scatter_t<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, tr_smem<T>()));
+  AB2_CUDA(cudaFuncSetAttribute(k_walk_gather_t<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, tr_smem<T>()));
 }
 
 template <class T>
@@ -547,6 +628,8 @@ bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool 
   AB2_CUDA(cudaStreamSynchronize(ctx->stream));
   dev_free(ctx, d.d_bands);
   d.d_bands = nullptr;
+  set_transpose_smem<double>();
+  set_transpose_smem<float>();
   d.stencil = true;
   d.levels_l = d.levels_u = (int)(nx + ny + nz - 2);
   return true;
@@ -562,7 +645,8 @@ void walk_apply(ab2_context* ctx, const Ilu0Data& d, T* base, const T* y, T* z) 
   T* yw = walk_array(base, d, kWalkY);
   T* lw = walk_array(base, d, kWalkL);
   T* uw = walk_array(base, d, kWalkU);
-  k_walk_gather<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, y, yw);
+  const int tr_grid = tiles * ((w.nz + kTrPlanes - 1) / kTrPlanes);
+  k_walk_gather_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, y, yw);
   check_launch(ctx, "walk_gather");
   k_walk_sweep<false, T><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, yw, lw, d.d_tile_tickets,
                                                                                 d.d_err);
@@ -570,7 +654,7 @@ void walk_apply(ab2_context* ctx, const Ilu0Data& d, T* base, const T* y, T* z) 
   k_walk_sweep<true, T><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, lw, uw, d.d_tile_tickets,
                                                                                d.d_err);
   check_launch(ctx, "walk_usweep");
-  k_walk_scatter<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, uw, z);
+  k_walk_scatter_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, uw, z);
   check_launch(ctx, "walk_scatter");
 }
 
