@@ -834,7 +834,7 @@ def main():
     if METHODS[a.method]["precond"] == "ilu0":
         pc = abi.Precond(ctx, A, "ilu0")
         ilu_ms = timed(lambda: pc.apply(b, vy), 20)
-        roofline = roof("k_stencil_wave<kLower>+k_stencil_wave<kUpper> (ILU0 apply, tiled wavefront)",
+        roofline = roof("k_walk_gather_t + k_walk_sweep<L> + k_walk_sweep<U> + k_walk_scatter_t (ILU0 apply, tile walk)",
                         ilu_bytes(P.n, P.nnz), ilu_ms, f"ilu0_apply_{n1}")
         pc.close()
     else:
