@@ -1,0 +1,105 @@
+"""Parity at the bench's full size: the 192^3 heterogeneous diffusion system
+(7,077,888 rows, 49,324,032 entries).
+
+The oracle is sequential C++, so at this size it checks what it can finish
+in seconds, bit for bit: the SpMV (every variant), the dot product in
+libab2's tree, the ILU(0) factor and one application (tile walk and wavefront
+schedule), and the first five CG+ILU0 iterations (history and iterate).  The
+full solve is then checked through properties that do not need the oracle:
+the graph loop and the host-driven loop agree bit for bit, the true residual
+meets the tolerance, and the row-block solver with one rank reproduces the
+single-GPU solve bit for bit.
+"""
+import numpy as np
+import pytest
+
+from alien_b200 import abi
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+N = 192
+
+
+@pytest.fixture(scope="module")
+def big():
+    return abi.diffusion(N, N, N, sigma=1.0, smooth=4.0, seed=0)
+
+
+@pytest.fixture(scope="module")
+def dev(ctx, big):
+    A = ctx.matrix(big.row_ptr, big.cols, big.vals, abi.FMT_CSR | abi.FMT_ELL)
+    yield A
+    A.close()
+
+
+def test_size(big):
+    assert (big.n, big.nnz) == (7_077_888, 49_324_032)
+
+
+def test_spmv_variants_bit_exact(ctx, big, dev):
+    x = np.random.default_rng(1).uniform(-1, 1, big.n)
+    exp = O.spmv(big.row_ptr, big.cols, big.vals, x)
+    vx, vy = ctx.vector(x), ctx.vector(big.n)
+    for variant in (abi.SPMV_ELL, abi.SPMV_CSR_STAGED, abi.SPMV_CSR_SCALAR):
+        ctx.mult(dev, vx, vy, variant)
+        np.testing.assert_array_equal(vy.download(), exp)
+
+
+def test_dot_bit_exact(ctx, big):
+    rng = np.random.default_rng(2)
+    x, y = rng.standard_normal(big.n), rng.standard_normal(big.n)
+    assert ctx.dot(ctx.vector(x), ctx.vector(y)) == O.dot_tree(x, y, ctx.info.reduction_max_blocks)
+
+
+@pytest.mark.parametrize("schedule", ["stencil", "wavefront"])
+def test_ilu0_factor_and_apply_bit_exact(ctx, big, dev, schedule):
+    y = np.random.default_rng(3).standard_normal(big.n)
+    M = abi.Precond(ctx, dev, "ilu0", ilu_schedule=schedule)
+    assert M.info.ilu_schedule == (2 if schedule == "stencil" else 1)
+    np.testing.assert_array_equal(M.ilu0_values(), O.ilu0_factor(big.row_ptr, big.cols, big.vals))
+    vy, vz = ctx.vector(y), ctx.vector(big.n)
+    M.apply(vy, vz)
+    np.testing.assert_array_equal(vz.download(), O.ilu0_apply(big.row_ptr, big.cols, big.vals, y))
+    M.close()
+
+
+def test_first_cg_ilu0_iterations_bit_exact(ctx, big, dev):
+    b, x = ctx.vector(big.b), ctx.vector(big.n)
+    S = abi.Solver(ctx, dev, solver="cg", precond="ilu0", tol=1e-8, max_iter=5)
+    st = S.solve(b, x)
+    o = O.solve(big.row_ptr, big.cols, big.vals, big.b, solver="cg", precond="ilu0", tol=1e-8, max_iter=5,
+                dot_mode=O.DOT_DEVICE_TREE, tree_blocks=ctx.info.reduction_max_blocks)
+    assert (st.iterations, st.succeeded) == (o.iterations, o.converged) == (5, False)
+    np.testing.assert_array_equal(S.history(), o.history)
+    np.testing.assert_array_equal(x.download(), o.x)
+    S.close()
+
+
+def test_full_solve_properties(ctx, big, dev):
+    b = ctx.vector(big.b)
+    runs = {}
+    for graph in (True, False):
+        x = ctx.vector(big.n)
+        S = abi.Solver(ctx, dev, solver="cg", precond="ilu0", tol=1e-8, max_iter=2000, use_graph=graph)
+        st = S.solve(b, x)
+        runs[graph] = (st, x.download(), S.history())
+        S.close()
+    (sg, xg, hg), (sh, xh, hh) = runs[True], runs[False]
+    assert sg.succeeded and sg.iterations == sh.iterations
+    np.testing.assert_array_equal(hg, hh)
+    np.testing.assert_array_equal(xg, xh)
+    assert sg.true_residual <= 1.5e-8
+    r = big.b - O.spmv(big.row_ptr, big.cols, big.vals, xg)
+    assert np.linalg.norm(r) / np.linalg.norm(big.b) == pytest.approx(sg.true_residual, rel=1e-6)
+    # one rank of the row-block distribution is the same solve
+    comm = abi.Comm.local_group([ctx])[0]
+    A1 = abi.DistMatrix.from_global(ctx, comm, np.asarray([0, big.n], np.int32), big.row_ptr, big.cols, big.vals)
+    D = abi.DistSolver(ctx, comm, A1, solver="cg", precond="ilu0", tol=1e-8, max_iter=2000)
+    bd, xd = A1.vector(big.b), A1.vector()
+    sd = D.solve(bd, xd)
+    assert sd.iterations == sg.iterations
+    np.testing.assert_array_equal(D.history(), hg)
+    np.testing.assert_array_equal(xd.download(), xg)
+    for o in (D, A1, comm):
+        o.close()
