@@ -751,7 +751,7 @@ class DistPrecond(Precond):
 
 
 class DistSolver:
-    """ab2_dist_solver: CG on the distributed algebra, device-resident; solve() is collective."""
+    """ab2_dist_solver: CG or BiCGStab on the distributed algebra, device-resident; solve() is collective."""
 
     def __init__(self, ctx: Context, comm: Comm, A: DistMatrix, **opts):
         self.ctx, self.comm, self.A = ctx, comm, A

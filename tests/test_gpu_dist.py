@@ -143,33 +143,40 @@ def test_block_ilu0_bit_exact(name, k, align, schedule):
             assert o[2] == 2
 
 
-@pytest.mark.parametrize("name,k,align,precond", [("diffusion12", 1, 144, "ilu0"), ("diffusion12", 2, 144, "ilu0"),
+SOLVER_CASES = [("diffusion12", 1, 144, "ilu0"), ("diffusion12", 2, 144, "ilu0"),
                                                   ("diffusion12", 3, 144, "diag"), ("poisson16", 4, 1, "ilu0"),
                                                   ("ragged", 3, 1, "ilu0"), ("poisson16", 2, 1, "none"),
                                                   # eight ranks sharing the GPU: the transfer streams of a local
                                                   # group lag their contexts, which once let a gather overwrite
                                                   # partials before the previous sum had read them
-                                                  ("diffusion64", 8, 4096, "ilu0"), ("diffusion64", 8, 4096, "diag")])
-def test_dist_solver_cg_bit_exact(name, k, align, precond):
+                ("diffusion64", 8, 4096, "ilu0"), ("diffusion64", 8, 4096, "diag")]
+
+
+@pytest.mark.parametrize("solver,name,k,align,precond",
+                         [("cg",) + c for c in SOLVER_CASES] +
+                         [("bicgs", "convdiff_10x11x12", 1, 110, "ilu0"), ("bicgs", "convdiff_10x11x12", 3, 110, "ilu0"),
+                          ("bicgs", "ragged", 2, 1, "diag"), ("bicgs", "convdiff16", 4, 256, "ilu0"),
+                          ("bicgs", "diffusion64", 8, 4096, "ilu0"), ("bicgs", "poisson16", 2, 1, "none")])
+def test_dist_solver_bit_exact(solver, name, k, align, precond):
     P = problems.get(name)
     off = abi.row_offsets(P.n, k, align)
     tb = tree_blocks()
 
     def rank(r, ctx, comm):
         A = abi.DistMatrix.from_global(ctx, comm, off, P.row_ptr, P.cols, P.vals)
-        S = abi.DistSolver(ctx, comm, A, solver="cg", precond=precond, tol=1e-8, max_iter=400)
+        S = abi.DistSolver(ctx, comm, A, solver=solver, precond=precond, tol=1e-8, max_iter=400)
         b, x = A.vector(P.b[off[r]:off[r + 1]]), A.vector()
         st = S.solve(b, x)
         return st, x.download(), S.history()
 
     res = run_ranks(k, rank)
-    o = O.dist_solve(P.row_ptr, P.cols, P.vals, off, P.b, solver="cg", precond=precond, tol=1e-8, max_iter=400,
+    o = O.dist_solve(P.row_ptr, P.cols, P.vals, off, P.b, solver=solver, precond=precond, tol=1e-8, max_iter=400,
                      dot_mode=O.DOT_DEVICE_TREE, tree_blocks=tb)
     for st, _, h in res:
-        assert (st.iterations, st.succeeded) == (o.iterations, o.converged)
+        assert (st.iterations, st.succeeded, st.breakdown) == (o.iterations, o.converged, o.breakdown)
         np.testing.assert_array_equal(h, o.history)
     np.testing.assert_array_equal(np.concatenate([r[1] for r in res]), o.x)
-    if o.converged:
+    if o.converged and solver == "cg":
         assert res[0][0].true_residual < 1e-7
 
 
@@ -251,3 +258,28 @@ def test_rank_that_never_arrives_times_out_on_the_host():
     res = run_ranks(2, rank, timeout_s=1.0)
     assert res[1] == "left"
     assert res[0] == [abi.AB2_ERR_TIMEOUT, abi.AB2_ERR_TIMEOUT]
+
+
+@pytest.mark.parametrize("solver", ["cg", "bicgs"])
+def test_dist_breakdown_reported(solver):
+    """The zero operator on two ranks: p.Ap (CG) or v.r0 (BiCGStab) sums to 0
+    on every rank alike, the stop test fails, breakdown "alpha" (CG.h:96-104,
+    BiCGStab.h:186-187), the same on every rank and in the oracle."""
+    n = 64
+    rp = np.arange(n + 1, dtype=np.int32)
+    ci = np.arange(n, dtype=np.int32)
+    vals = np.zeros(n)
+    off = abi.row_offsets(n, 2)
+
+    def rank(r, ctx, comm):
+        A = abi.DistMatrix.from_global(ctx, comm, off, rp, ci, vals)
+        S = abi.DistSolver(ctx, comm, A, solver=solver, precond="none", tol=1e-8, max_iter=10)
+        st = S.solve(A.vector(np.ones(off[r + 1] - off[r])), A.vector())
+        return st
+
+    res = run_ranks(2, rank)
+    o = O.dist_solve(rp, ci, vals, off, np.ones(n), solver=solver, precond="none", tol=1e-8, max_iter=10)
+    assert o.error == -3 and o.breakdown == "alpha"
+    for st in res:
+        assert st.error == abi.AB2_ERR_BREAKDOWN and st.breakdown == "alpha"
+        assert st.iterations == o.iterations and not st.succeeded
