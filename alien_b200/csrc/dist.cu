@@ -358,7 +358,24 @@ void dist_build(ab2_dist_matrix* A, const int* row_ptr, const int* cols, const d
   const std::vector<int>& off = A->offsets;
   const int n = A->n_loc;
   const int base = off[(size_t)me];
-  require(row_ptr[0] == 0, "row_ptr must start at 0");
+  // Every rank reaches the exchange below, valid rows or not, so that a
+  // rejection on one rank fails the call on all of them instead of leaving
+  // the others waiting in the collective.
+  std::string bad;
+  if (row_ptr[0] != 0) bad = "row_ptr must start at 0";
+  for (int i = 0; bad.empty() && i < n; ++i) {
+    const int b = row_ptr[i], e = row_ptr[i + 1];
+    if (b > e) bad = "row_ptr must be non-decreasing";
+    else if (e > b && (!cols || !vals)) bad = "null cols or vals";
+    for (int k = b; bad.empty() && k < e; ++k) {
+      if (cols[k] < 0 || cols[k] >= A->global_n) bad = "column index out of range";
+      else if (k > b && cols[k - 1] >= cols[k]) bad = "columns must be strictly ascending inside each row";
+    }
+  }
+  if (!bad.empty()) {
+    comm->host_allgather(std::vector<int>{1});
+    throw Error{AB2_ERR_BAD_ARG, bad};
+  }
   const long long nnz = row_ptr[n];
   // sortGhostCols: local columns first, ghosts after, each in their order
   A->h_rp.assign(row_ptr, row_ptr + n + 1);
@@ -370,12 +387,9 @@ void dist_build(ab2_dist_matrix* A, const int* row_ptr, const int* cols, const d
   g_owner.assign((size_t)nnz, -1);
   for (int i = 0; i < n; ++i) {
     const int b = row_ptr[i], e = row_ptr[i + 1];
-    require(b <= e, "row_ptr must be non-decreasing");
     int nl = 0;
     for (int k = b; k < e; ++k) {
       const int c = cols[k];
-      require(c >= 0 && c < A->global_n, "column index out of range");
-      require(k == b || cols[k - 1] < c, "columns must be strictly ascending inside each row");
       if (c >= base && c < base + n) ++nl;
     }
     A->h_lrs[(size_t)i] = nl;
@@ -440,8 +454,8 @@ void dist_build(ab2_dist_matrix* A, const int* row_ptr, const int* cols, const d
       P.recv_off.push_back(P.recv_off.back() + (int)gids[(size_t)q].size());
     }
   A->first_upper_ghost = n + P.recv_off[(size_t)first_upper];
-  // requests: (owner, count, ids...) for every owner this rank needs values from
-  std::vector<int> req;
+  // requests: status 0, then (owner, count, ids...) for every owner this rank needs values from
+  std::vector<int> req(1, 0);
   for (int q = 0; q < np; ++q)
     if (!gids[(size_t)q].empty()) {
       req.push_back(q);
@@ -449,12 +463,15 @@ void dist_build(ab2_dist_matrix* A, const int* row_ptr, const int* cols, const d
       req.insert(req.end(), gids[(size_t)q].begin(), gids[(size_t)q].end());
     }
   const std::vector<std::vector<int>> all = comm->host_allgather(req);
+  for (int q = 0; q < np; ++q)
+    if (all[(size_t)q].empty() || all[(size_t)q][0] != 0)
+      throw Error{AB2_ERR_BAD_ARG, "rank " + std::to_string(q) + " rejected its rows"};
   P.send_ranks.clear();
   P.send_off.assign(1, 0);
   A->h_send_ids.clear();
   for (int q = 0; q < np; ++q) {
     const std::vector<int>& r = all[(size_t)q];
-    for (size_t t = 0; t + 1 < r.size();) {
+    for (size_t t = 1; t + 1 < r.size();) {
       const int owner = r[t], cnt = r[t + 1];
       require(cnt >= 0 && t + 2 + (size_t)cnt <= r.size(), "malformed ghost request");
       if (owner == me && q != me) {
@@ -672,10 +689,6 @@ int ab2_dist_matrix_create(ab2_context* ctx, ab2_comm* comm, const int* offsets,
   A->offsets.assign(offsets, offsets + np + 1);
   A->global_n = offsets[np];
   A->n_loc = offsets[comm->rank + 1] - offsets[comm->rank];
-  if (A->n_loc > 0 && (!cols || !vals) && row_ptr[A->n_loc] > 0) {
-    dist_free(A);
-    return AB2_ERR_BAD_ARG;
-  }
   const int rc = guard(ctx, [&] { dist_build(A, row_ptr, cols, vals, formats); });
   if (rc != AB2_OK) {
     dist_free(A);

@@ -283,3 +283,24 @@ def test_dist_breakdown_reported(solver):
     for st in res:
         assert st.error == abi.AB2_ERR_BREAKDOWN and st.breakdown == "alpha"
         assert st.iterations == o.iterations and not st.succeeded
+
+
+def test_rows_rejected_on_one_rank_fail_every_rank():
+    """A rank whose rows are invalid still takes part in the set-up exchange,
+    so every rank fails with AB2_ERR_BAD_ARG at once (no rank left waiting)."""
+    P = problems.get("poisson16")
+    off = abi.row_offsets(P.n, 2)
+
+    def rank(r, ctx, comm):
+        a, b = int(off[r]), int(off[r + 1])
+        lo, hi = int(P.row_ptr[a]), int(P.row_ptr[b])
+        cols = P.cols[lo:hi].copy()
+        if r == 1:
+            cols[3] = P.n + 5  # out of range
+        try:
+            abi.DistMatrix(ctx, comm, off, P.row_ptr[a:b + 1] - lo, cols, P.vals[lo:hi])
+        except abi.AB2Error as e:
+            return e.code
+        return None
+
+    assert run_ranks(2, rank, timeout_s=30.0) == [abi.AB2_ERR_BAD_ARG, abi.AB2_ERR_BAD_ARG]
