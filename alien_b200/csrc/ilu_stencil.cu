@@ -54,6 +54,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "ab2_internal.cuh"
 #include "precond.cuh"
@@ -269,6 +270,19 @@ __global__ void k_walk_gather(Walk g, const S* __restrict__ src, T* __restrict__
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < g.nw; w += (long long)gridDim.x * blockDim.x) {
     const long long r = walk_row(g, w);
     dst[w] = r >= 0 ? (T)__ldg(src + r) : T(0);
+  }
+}
+
+// dst[row(w)] = src[w], and src[w] back to the sentinel for the next walk
+// (element-wise; the FP32 walk's scatter).
+template <class T>
+__global__ void k_walk_scatter(Walk g, T* __restrict__ src, T* __restrict__ dst) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < g.nw; w += (long long)gridDim.x * blockDim.x) {
+    const long long r = walk_row(g, w);
+    if (r >= 0) {
+      dst[r] = src[w];
+      src[w] = sentinel_of<T>();
+    }
   }
 }
 
@@ -632,7 +646,6 @@ bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool 
   dev_free(ctx, d.d_bands);
   d.d_bands = nullptr;
   set_transpose_smem<double>();
-  set_transpose_smem<float>();
   d.stencil = true;
   d.levels_l = d.levels_u = (int)(nx + ny + nz - 2);
   return true;
@@ -648,8 +661,13 @@ void walk_apply(ab2_context* ctx, const Ilu0Data& d, T* base, const T* y, T* z) 
   T* yw = walk_array(base, d, kWalkY);
   T* lw = walk_array(base, d, kWalkL);
   T* uw = walk_array(base, d, kWalkU);
+  // FP64: shared-memory transposes; FP32 (half the bytes): element-wise
+  // kernels, which move them faster than the latency-bound transposes (both
+  // measured back to back on one GPU).
+  constexpr bool kTranspose = std::is_same<T, double>::value;
   const int tr_grid = tiles * ((w.nz + kTrPlanes - 1) / kTrPlanes);
-  k_walk_gather_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, y, yw);
+  if (kTranspose) k_walk_gather_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, y, yw);
+  else k_walk_gather<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, y, yw);
   check_launch(ctx, "walk_gather");
   k_walk_sweep<false, T><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, yw, lw, d.d_tile_tickets,
                                                                                 d.d_err);
@@ -657,7 +675,8 @@ void walk_apply(ab2_context* ctx, const Ilu0Data& d, T* base, const T* y, T* z) 
   k_walk_sweep<true, T><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, lw, uw, d.d_tile_tickets,
                                                                                d.d_err);
   check_launch(ctx, "walk_usweep");
-  k_walk_scatter_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, uw, z);
+  if (kTranspose) k_walk_scatter_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, uw, z);
+  else k_walk_scatter<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, uw, z);
   check_launch(ctx, "walk_scatter");
 }
 
