@@ -247,6 +247,7 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_problem_read_matrix_market": (_I, [C.c_char_p, C.c_char_p, C.POINTER(C.POINTER(Problem))]),
     "ab2_problem_write_matrix_market": (_I, [C.POINTER(Problem), C.c_char_p, C.c_char_p]),
     "ab2_matrix_market_error": (C.c_char_p, []),
+    "ab2_selftest_bounded_wait": (_I, [_P, _IP, _DP]),
     "ab2_rng_u64": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
     "ab2_rng_uniform": (_D, [C.c_uint64, C.c_uint64, C.c_uint64]),
 }
@@ -325,6 +326,12 @@ class Context:
         c = C.c_longlong()
         self.check(lib().ab2_context_launch_count(self.h, C.byref(c)))
         return c.value
+
+    def selftest_bounded_wait(self) -> tuple[bool, float]:
+        """(expired, seconds): a device-side wait on a word nothing writes gives up on its budget."""
+        e, t = C.c_int(), C.c_double()
+        self.check(lib().ab2_selftest_bounded_wait(self.h, C.byref(e), C.byref(t)), "selftest_bounded_wait")
+        return bool(e.value), t.value
 
     # -- objects
     def matrix(self, row_ptr, cols, vals, formats: int = FMT_CSR | FMT_ELL) -> "Matrix":

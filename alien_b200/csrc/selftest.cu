@@ -1,0 +1,45 @@
+// selftest.cu -- the failure-detection path of the bounded device-side waits,
+// exercised without a fault: one thread polls a word that holds the
+// sentinel and that nothing ever writes, as a sweep would poll a value whose
+// producer is gone.  The wait gives up after its clock budget, sets the
+// error flag and returns, the kernel ends, and the host reads the flag: the
+// same path that turns a stuck ILU(0) sweep into AB2_ERR_TIMEOUT with the
+// context still usable.
+#include <chrono>
+
+#include "ab2_internal.cuh"
+#include "sentinel.cuh"
+
+namespace ab2 {
+namespace {
+
+__global__ void k_selftest_wait(const double* word, int* err, double* out) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = wait_value(word, err);
+}
+
+}  // namespace
+}  // namespace ab2
+
+using namespace ab2;
+
+extern "C" int ab2_selftest_bounded_wait(ab2_context* ctx, int* expired, double* seconds) {
+  if (!ctx || !expired || !seconds) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    double* word = dev_alloc<double>(ctx, 2);
+    int* err = dev_alloc<int>(ctx, 1);
+    k_fill_bits<<<1, 1, 0, ctx->stream>>>(1, kSentinel, word);
+    check_launch(ctx, "selftest_fill");
+    AB2_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ctx->stream));
+    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+    const auto t0 = std::chrono::steady_clock::now();
+    k_selftest_wait<<<1, 32, 0, ctx->stream>>>(word, err, word + 1);
+    check_launch(ctx, "selftest_wait");
+    int e = 0;
+    AB2_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *expired = e;
+    dev_free(ctx, word);
+    dev_free(ctx, err);
+  });
+}

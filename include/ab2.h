@@ -449,6 +449,13 @@ void ab2_fcg_options_default(ab2_fcg_options* opts);
 int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* gnn, const ab2_precond* fallback,
                   const ab2_vector* b, ab2_vector* x, const ab2_fcg_options* opts, ab2_fcg_status* status);
 
+/* ------------------------------------------------------------------ self-test
+ * Failure detection of the bounded device-side waits, without a fault: one
+ * thread polls a sentinel word that nothing writes; the wait gives up after
+ * its clock budget (~2 s), sets the error flag (*expired = 1) and the kernel
+ * ends; *seconds is the wall time.  The context stays usable. */
+int ab2_selftest_bounded_wait(ab2_context* ctx, int* expired, double* seconds);
+
 #ifdef __cplusplus
 }
 #endif
