@@ -45,6 +45,10 @@ struct ab2_context {
   unsigned int* d_counters = nullptr; // kRedSlots
   double* d_results = nullptr;        // kRedSlots * kMaxRedComps
   double* h_pinned = nullptr;         // 64 doubles of pinned staging
+  // Host-side fault injection (ab2_context_inject_alloc_failure): the
+  // fail_alloc_at-th device allocation from the call on fails as OOM.
+  long long alloc_count = 0;
+  long long fail_alloc_at = 0;
 };
 
 struct ab2_vector {
@@ -131,6 +135,10 @@ template <class T>
 T* dev_alloc(ab2_context* ctx, size_t count, long long* accounted = nullptr) {
   T* p = nullptr;
   if (count == 0) count = 1;
+  if (ctx->fail_alloc_at > 0 && ++ctx->alloc_count == ctx->fail_alloc_at) {
+    ctx->fail_alloc_at = 0;
+    throw Error{AB2_ERR_OOM, "device allocation failed (injected)"};
+  }
   check_cuda(cudaMallocAsync((void**)&p, count * sizeof(T), ctx->stream), "cudaMallocAsync");
   check_cuda(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
   if (accounted) *accounted += (long long)(count * sizeof(T));

@@ -43,3 +43,13 @@ extern "C" int ab2_selftest_bounded_wait(ab2_context* ctx, int* expired, double*
     dev_free(ctx, err);
   });
 }
+
+// Host-side fault injection: the nth device allocation from now on fails
+// with AB2_ERR_OOM (once); nth = 0 turns it off.  Every creation path must
+// then unwind cleanly and the context stay usable.
+extern "C" int ab2_context_inject_alloc_failure(ab2_context* ctx, long long nth) {
+  if (!ctx || nth < 0) return AB2_ERR_BAD_ARG;
+  ctx->alloc_count = 0;
+  ctx->fail_alloc_at = nth;
+  return AB2_OK;
+}
