@@ -123,6 +123,10 @@ class FcgStatus(C.Structure):
                 ("solve_ms", C.c_double)]
 
 
+class PhaseTime(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("calls", C.c_longlong), ("ms", C.c_double)]
+
+
 class DistInfo(C.Structure):
     _fields_ = [("global_rows", C.c_int), ("local_rows", C.c_int), ("ghost_rows", C.c_int),
                 ("interface_rows", C.c_int), ("recv_neighbours", C.c_int), ("send_neighbours", C.c_int),
@@ -152,6 +156,8 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_synchronize": (_I, [_P]),
     "ab2_context_launch_count": (_I, [_P, C.POINTER(C.c_longlong)]),
     "ab2_context_get_info": (_I, [_P, C.POINTER(ContextInfo)]),
+    "ab2_context_set_phase_timing": (_I, [_P, _I]),
+    "ab2_context_phase_times": (_I, [_P, C.POINTER(PhaseTime), _I, _IP]),
     "ab2_matrix_create_csr": (_I, [_P, _I, _IP, _IP, _DP, _I, C.POINTER(_P)]),
     "ab2_matrix_update_values": (_I, [_P, _P, _DP]),
     "ab2_matrix_destroy": (_I, [_P]),
@@ -327,6 +333,18 @@ class Context:
         c = C.c_longlong()
         self.check(lib().ab2_context_launch_count(self.h, C.byref(c)))
         return c.value
+
+    def set_phase_timing(self, on: bool = True) -> None:
+        """Phase timers on (restarted at zero) or off: device time per ABI operation ("CSR-SPMV", ...)."""
+        self.check(lib().ab2_context_set_phase_timing(self.h, int(on)), "set_phase_timing")
+
+    def phase_times(self) -> dict:
+        """{phase: (calls, ms)} of the operations since timing was turned on (synchronises)."""
+        n = C.c_int()
+        self.check(lib().ab2_context_phase_times(self.h, None, 0, C.byref(n)), "phase_times")
+        arr = (PhaseTime * max(n.value, 1))()
+        self.check(lib().ab2_context_phase_times(self.h, arr, n.value, C.byref(n)), "phase_times")
+        return {arr[i].name.decode(): (arr[i].calls, arr[i].ms) for i in range(n.value)}
 
     def selftest_bounded_wait(self) -> tuple[bool, float]:
         """(expired, seconds): a device-side wait on a word nothing writes gives up on its budget."""

@@ -28,6 +28,8 @@ struct Error {
   std::string msg;
 };
 
+struct PhaseTimer;  // context.cu
+
 }  // namespace ab2
 
 struct ab2_context {
@@ -49,6 +51,8 @@ struct ab2_context {
   // fail_alloc_at-th device allocation from the call on fails as OOM.
   long long alloc_count = 0;
   long long fail_alloc_at = 0;
+  // Phase timers (ab2_context_set_phase_timing, or AB2_PERF_TIMER=1): null when off.
+  ab2::PhaseTimer* timer = nullptr;
 };
 
 struct ab2_vector {
@@ -168,6 +172,24 @@ inline int grid_for(long long n, int threads = kThreads, int cap = 148 * 32) {
   if (g > cap) g = cap;
   return (int)g;
 }
+
+// Phase timers: device time of each ABI operation by phase name (the
+// reference's StdTimer sentries, e.g. "CSR-SPMV"), from CUDA events recorded
+// on the context's stream around the call and resolved when read.
+void phase_begin(ab2_context* ctx, const char* name, int* token);
+void phase_end(ab2_context* ctx, int token);
+struct PhaseScope {
+  ab2_context* ctx;
+  int tok = -1;
+  PhaseScope(ab2_context* c, const char* name) : ctx(c) {
+    if (c && c->timer) phase_begin(c, name, &tok);
+  }
+  ~PhaseScope() {
+    if (tok >= 0) phase_end(ctx, tok);
+  }
+  PhaseScope(const PhaseScope&) = delete;
+  PhaseScope& operator=(const PhaseScope&) = delete;
+};
 
 // Runs f, mapping exceptions to ABI codes and recording the message on ctx.
 template <class F>

@@ -506,6 +506,7 @@ int ab2_batch_create(ab2_context* ctx, const ab2_matrix* A, int nsys, const int*
 int ab2_batch_solve(ab2_batch* B, const ab2_vector* b, ab2_vector* x, ab2_batch_status* status) {
   if (!B || !b || !x || !status || b->n != B->A->n || x->n != B->A->n) return AB2_ERR_BAD_ARG;
   ab2_context* ctx = B->ctx;
+  PhaseScope phase_scope(ctx, "BATCH-SOLVE");
   std::memset(status, 0, sizeof(*status));
   return guard(ctx, [&] {
     AB2_CUDA(cudaEventRecord(B->ev0, ctx->stream));

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "ab2_internal.cuh"
@@ -67,9 +68,109 @@ int red_grid(const ab2_context* ctx, int n) {
   return grid_for(n, kThreads, std::min(kMaxRedBlocks, ctx->num_sms * (2048 / kThreads)));
 }
 
+// ---------------------------------------------------------------- phase timers
+struct PhaseTimer {
+  struct Rec {
+    int phase;
+    cudaEvent_t a, b;
+    bool ended;
+  };
+  std::vector<std::string> names;
+  std::vector<long long> calls;
+  std::vector<double> ms;
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  bool print_at_exit = false;
+
+  cudaEvent_t event() {
+    cudaEvent_t e = nullptr;
+    if (!pool.empty()) {
+      e = pool.back();
+      pool.pop_back();
+    } else if (cudaEventCreate(&e) != cudaSuccess) {
+      e = nullptr;
+    }
+    return e;
+  }
+  int phase(const char* name) {
+    for (size_t i = 0; i < names.size(); ++i)
+      if (names[i] == name) return (int)i;
+    names.push_back(name);
+    calls.push_back(0);
+    ms.push_back(0.0);
+    return (int)names.size() - 1;
+  }
+  // Folds every finished record into the totals (waits for their events).
+  void resolve() {
+    std::vector<Rec> keep;
+    for (Rec& r : recs) {
+      if (!r.ended) {
+        keep.push_back(r);
+        continue;
+      }
+      float t = 0.f;
+      if (r.phase >= 0 && cudaEventSynchronize(r.b) == cudaSuccess &&
+          cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+        ms[(size_t)r.phase] += t;
+        calls[(size_t)r.phase] += 1;
+      }
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    recs.swap(keep);
+  }
+  ~PhaseTimer() {
+    for (Rec& r : recs) {
+      if (r.a) cudaEventDestroy(r.a);
+      if (r.b) cudaEventDestroy(r.b);
+    }
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+  }
+};
+
+void phase_begin(ab2_context* ctx, const char* name, int* token) {
+  PhaseTimer* t = ctx->timer;
+  cudaEvent_t a = t->event(), b = t->event();
+  if (!a || !b || cudaEventRecord(a, ctx->stream) != cudaSuccess) {
+    if (a) t->pool.push_back(a);
+    if (b) t->pool.push_back(b);
+    return;
+  }
+  t->recs.push_back(PhaseTimer::Rec{t->phase(name), a, b, false});
+  *token = (int)t->recs.size() - 1;
+}
+
+void phase_end(ab2_context* ctx, int token) {
+  PhaseTimer* t = ctx->timer;
+  if (!t || token >= (int)t->recs.size()) return;
+  PhaseTimer::Rec& r = t->recs[(size_t)token];
+  if (cudaEventRecord(r.b, ctx->stream) != cudaSuccess) r.phase = -1;  // dropped when resolved
+  r.ended = true;
+  // Bounded memory: fold finished records once many are pending (only when
+  // no scope is open, so the tokens of open scopes stay valid).
+  if (t->recs.size() >= 4096 && token == (int)t->recs.size() - 1) {
+    bool all_ended = true;
+    for (const PhaseTimer::Rec& x : t->recs) all_ended = all_ended && x.ended;
+    if (all_ended) t->resolve();
+  }
+}
+
 void ctx_release(ab2_context* ctx) {
   if (ctx->refs.fetch_sub(1) != 1) return;
   ctx_quiesce(ctx);
+  if (ctx->timer) {
+    if (ctx->timer->print_at_exit) {
+      // StdTimer::printInfo's format (utils/StdTimer.h): phase:seconds
+      ctx->timer->resolve();
+      std::fprintf(stderr, "================================\nPERF INFO : B200-ALGEBRA (device %d)\n", ctx->device);
+      for (size_t i = 0; i < ctx->timer->names.size(); ++i)
+        std::fprintf(stderr, "%s:%.6f (%lld calls)\n", ctx->timer->names[i].c_str(), ctx->timer->ms[i] * 1e-3,
+                     ctx->timer->calls[i]);
+      std::fprintf(stderr, "================================\n");
+    }
+    delete ctx->timer;
+    ctx->timer = nullptr;
+  }
   dev_free(ctx, ctx->d_partials);
   dev_free(ctx, ctx->d_counters);
   dev_free(ctx, ctx->d_results);
@@ -191,6 +292,13 @@ int ab2_context_create(int device, ab2_context** out) {
     ctx->d_results = dev_alloc<double>(ctx, (size_t)kRedSlots * kMaxRedComps);
     AB2_CUDA(cudaMemset(ctx->d_counters, 0, sizeof(unsigned int) * kRedSlots));
     AB2_CUDA(cudaMallocHost((void**)&ctx->h_pinned, 64 * sizeof(double)));
+    // AB2_PERF_TIMER=1: phase timers on, printed when the context goes (as
+    // the reference's ALIEN_USE_PERF_TIMER build prints its timers).
+    const char* pt = std::getenv("AB2_PERF_TIMER");
+    if (pt && pt[0] && pt[0] != '0') {
+      ctx->timer = new PhaseTimer();
+      ctx->timer->print_at_exit = true;
+    }
   });
   if (rc != AB2_OK) {
     fprintf(stderr, "ab2_context_create: %s\n", ctx->last_error.c_str());
@@ -295,34 +403,42 @@ int ab2_vector_device_ptr(const ab2_vector* v, void** dptr) {
 // ---------------------------------------------------------------- BLAS-1
 int ab2_axpy(ab2_context* ctx, double a, const ab2_vector* x, ab2_vector* y) {
   if (!ctx || !x || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-AXPY");
   return guard(ctx, [&] { op_axpy(ctx, x->n, a, x->d, y->d); });
 }
 int ab2_aypx(ab2_context* ctx, double a, ab2_vector* y, const ab2_vector* x) {
   if (!ctx || !x || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-AYPX");
   return guard(ctx, [&] { op_aypx(ctx, x->n, a, y->d, x->d); });
 }
 int ab2_copy(ab2_context* ctx, const ab2_vector* x, ab2_vector* y) {
   if (!ctx || !x || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-COPY");
   return guard(ctx, [&] { op_copy(ctx, x->n, x->d, y->d); });
 }
 int ab2_scal(ab2_context* ctx, double a, ab2_vector* x) {
   if (!ctx || !x) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-SCAL");
   return guard(ctx, [&] { op_scal(ctx, x->n, a, x->d); });
 }
 int ab2_pointwise_mult(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, ab2_vector* w) {
   if (!ctx || !x || check_vec(y, x->n) || check_vec(w, x->n)) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-PMULT");
   return guard(ctx, [&] { op_pmult(ctx, x->n, x->d, y->d, w->d); });
 }
 int ab2_assign(ab2_context* ctx, ab2_vector* x, double a) {
   if (!ctx || !x) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-ASSIGN");
   return guard(ctx, [&] { op_fill(ctx, x->n, a, x->d); });
 }
 int ab2_reciprocal(ab2_context* ctx, ab2_vector* x) {
   if (!ctx || !x) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-RECIPROCAL");
   return guard(ctx, [&] { op_reciprocal(ctx, x->n, x->d); });
 }
 int ab2_dot(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, double* result) {
   if (!ctx || !x || !result || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-DOT");
   return guard(ctx, [&] {
     RedSlot s = red_slot(ctx, 0);
     op_dot(ctx, x->n, x->d, y->d, s.result, 0);
@@ -331,6 +447,7 @@ int ab2_dot(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, double* 
 }
 int ab2_norm2(ab2_context* ctx, const ab2_vector* x, double* result) {
   if (!ctx || !x || !result) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-NORM2");
   return guard(ctx, [&] {
     RedSlot s = red_slot(ctx, 0);
     op_dot(ctx, x->n, x->d, x->d, s.result, 0);
@@ -339,6 +456,7 @@ int ab2_norm2(ab2_context* ctx, const ab2_vector* x, double* result) {
 }
 int ab2_norm1(ab2_context* ctx, const ab2_vector* x, double* result) {
   if (!ctx || !x || !result) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-NORM1");
   return guard(ctx, [&] {
     RedSlot s = red_slot(ctx, 0);
     op_norm1(ctx, x->n, x->d, s.result, 0);
@@ -347,6 +465,7 @@ int ab2_norm1(ab2_context* ctx, const ab2_vector* x, double* result) {
 }
 int ab2_norm0(ab2_context* ctx, const ab2_vector* x, double* result) {
   if (!ctx || !x || !result) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-NORM0");
   return guard(ctx, [&] {
     RedSlot s = red_slot(ctx, 0);
     op_norm0(ctx, x->n, x->d, s.result, 0);
@@ -382,11 +501,46 @@ int ab2_scalar_destroy(ab2_scalar* s) {
 }
 int ab2_dot_async(ab2_context* ctx, const ab2_vector* x, const ab2_vector* y, ab2_scalar* result) {
   if (!ctx || !x || !result || check_vec(y, x->n)) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-DOT-F");
   return guard(ctx, [&] { op_dot(ctx, x->n, x->d, y->d, result->d, 0); });
 }
 int ab2_scalar_get(ab2_context* ctx, const ab2_scalar* s, double* value) {
   if (!ctx || !s || !value) return AB2_ERR_BAD_ARG;
   return guard(ctx, [&] { *value = read_scalar(ctx, s->d); });
+}
+
+// ---------------------------------------------------------------- phase timers
+int ab2_context_set_phase_timing(ab2_context* ctx, int on) {
+  if (!ctx) return AB2_ERR_BAD_ARG;
+  return guard(ctx, [&] {
+    const bool print = ctx->timer && ctx->timer->print_at_exit;
+    if (ctx->timer) {
+      AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+      delete ctx->timer;
+      ctx->timer = nullptr;
+    }
+    if (on) {
+      ctx->timer = new PhaseTimer();
+      ctx->timer->print_at_exit = print;
+    }
+  });
+}
+
+int ab2_context_phase_times(ab2_context* ctx, ab2_phase_time* out, int cap, int* count) {
+  if (!ctx || !count || cap < 0 || (cap > 0 && !out)) return AB2_ERR_BAD_ARG;
+  *count = 0;
+  if (!ctx->timer) return AB2_OK;
+  return guard(ctx, [&] {
+    PhaseTimer* t = ctx->timer;
+    t->resolve();
+    *count = (int)t->names.size();
+    for (int i = 0; i < std::min(cap, *count); ++i) {
+      std::memset(out[i].name, 0, sizeof(out[i].name));
+      std::strncpy(out[i].name, t->names[(size_t)i].c_str(), sizeof(out[i].name) - 1);
+      out[i].calls = t->calls[(size_t)i];
+      out[i].ms = t->ms[(size_t)i];
+    }
+  });
 }
 
 }  // extern "C"

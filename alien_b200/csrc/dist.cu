@@ -759,6 +759,7 @@ int ab2_dist_vector_create(ab2_context* ctx, const ab2_dist_matrix* A, ab2_vecto
 
 int ab2_dist_mult(ab2_context* ctx, const ab2_dist_matrix* A, ab2_vector* x, ab2_vector* y) {
   if (!ctx || !A || !x || !y || x == y || x->n != A->n_loc || y->n != A->n_loc) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "DIST-SPMV");
   if (x->cap < A->n_loc + A->n_ghost) {
     ctx->last_error = "ab2_dist_mult: x has no room for the ghost values (create it with ab2_dist_vector_create)";
     return AB2_ERR_BAD_ARG;
@@ -786,14 +787,17 @@ extern "C" {
 
 int ab2_dist_dot(ab2_context* ctx, ab2_comm* c, const ab2_vector* x, const ab2_vector* y, double* result) {
   if (!y || !x || x->n != y->n) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "DIST-DOT");
   return dist_scalar(ctx, c, x, result, [&](double* out) { op_dot(ctx, x->n, x->d, y->d, out, 0); }, false);
 }
 
 int ab2_dist_norm1(ab2_context* ctx, ab2_comm* c, const ab2_vector* x, double* result) {
+  PhaseScope phase_scope(ctx, "DIST-NORM1");
   return dist_scalar(ctx, c, x, result, [&](double* out) { op_norm1(ctx, x->n, x->d, out, 0); }, false);
 }
 
 int ab2_dist_norm2(ab2_context* ctx, ab2_comm* c, const ab2_vector* x, double* result) {
+  PhaseScope phase_scope(ctx, "DIST-NORM2");
   return dist_scalar(ctx, c, x, result, [&](double* out) { op_dot(ctx, x->n, x->d, x->d, out, 0); }, true);
 }
 

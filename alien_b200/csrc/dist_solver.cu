@@ -494,6 +494,7 @@ int ab2_dist_solver_create(ab2_context* ctx, ab2_comm* comm, const ab2_dist_matr
 
 int ab2_dist_solver_solve(ab2_dist_solver* S, const ab2_vector* b, ab2_vector* x, ab2_status* status) {
   if (!S || !b || !x || !status || b->n != S->n || x->n != S->n) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(S->ctx, S->o.solver == AB2_SOLVER_CG ? "DIST-SOLVER-CG" : "DIST-SOLVER-BICGSTAB");
   *status = ab2_status{};
   return guard(S->ctx, [&] { dist_solve(S, b->d, x->d, status); });
 }

@@ -1078,6 +1078,7 @@ int ab2_gnn_bind(ab2_gnn* G, const ab2_matrix* A) {
 
 int ab2_gnn_apply(ab2_gnn* G, const ab2_vector* r, ab2_vector* z) {
   if (!G || !r || !z || !G->A || r->n != G->n || z->n != G->n || r->d == z->d) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(G->ctx, "GNN-APPLY");
   return guard(G->ctx, [&] { gnn_forward(G, r->d, z->d); });
 }
 
@@ -1143,6 +1144,7 @@ int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_p
                   const ab2_vector* b, ab2_vector* x, const ab2_fcg_options* o, ab2_fcg_status* st) {
   if (!ctx || !A || !b || !x || !o || !st || b->n != A->n || x->n != A->n) return AB2_ERR_BAD_ARG;
   if (!G && !fallback) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "FCG-SOLVE");
   if (G && (G->A != A)) return AB2_ERR_BAD_ARG;
   if (fallback && fallback->A != A) return AB2_ERR_BAD_ARG;
   std::memset(st, 0, sizeof(*st));

@@ -740,6 +740,7 @@ int ab2_solver_create(ab2_context* ctx, const ab2_matrix* A, const ab2_solver_op
 
 int ab2_solver_solve(ab2_solver* S, const ab2_vector* b, ab2_vector* x, ab2_status* status) {
   if (!S || !b || !x || !status || b->n != S->A->n || x->n != S->A->n) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(S->ctx, S->opts.solver == AB2_SOLVER_CG ? "SOLVER-CG" : "SOLVER-BICGSTAB");
   ab2_context* ctx = S->ctx;
   std::memset(status, 0, sizeof(*status));
   return guard(ctx, [&] {

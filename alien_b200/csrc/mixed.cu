@@ -157,6 +157,7 @@ int ab2_mixed_create(ab2_context* ctx, const ab2_matrix* A, const ab2_mixed_opti
 int ab2_mixed_solve(ab2_mixed* M, const ab2_vector* b, ab2_vector* x, ab2_mixed_status* status) {
   if (!M || !b || !x || !status || b->n != M->A->n || x->n != M->A->n) return AB2_ERR_BAD_ARG;
   ab2_context* ctx = M->ctx;
+  PhaseScope phase_scope(ctx, "MIXED-SOLVE");
   std::memset(status, 0, sizeof(*status));
   M->history.clear();
   return guard(ctx, [&] {

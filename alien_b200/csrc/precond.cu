@@ -698,6 +698,9 @@ int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_
 
 int ab2_precond_apply(ab2_context* ctx, const ab2_precond* pc, const ab2_vector* x, ab2_vector* y) {
   if (!ctx || !pc || !x || !y || x->n != pc->A->n || y->n != pc->A->n) return AB2_ERR_BAD_ARG;
+  static const char* const kPhase[] = {"PRECOND-NONE", "PRECOND-DIAG", "PRECOND-ILU0", "PRECOND-CHEB", "PRECOND-FILU0",
+                                       "PRECOND-NEUMANN"};
+  PhaseScope phase_scope(ctx, kPhase[pc->kind]);
   return guard(ctx, [&] { pc_apply(ctx, pc, x->d, y->d); });
 }
 

@@ -505,31 +505,37 @@ int ab2_mult(ab2_context* ctx, const ab2_matrix* A, const ab2_vector* x, ab2_vec
 
 int ab2_mult_variant(ab2_context* ctx, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y, int variant) {
   if (!ctx || !A || !x || !y || x->n != A->n || y->n != A->n || x->d == y->d) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-SPMV");
   return guard(ctx, [&] { op_spmv(ctx, A, x->d, y->d, variant); });
 }
 
 int ab2_add_lmult(ab2_context* ctx, double alpha, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y) {
   if (!ctx || !A || !x || !y || x->n != A->n || y->n != A->n || x->d == y->d) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-AddLMult");
   return guard(ctx, [&] { op_add_lu_mult(ctx, A, alpha, x->d, y->d, true); });
 }
 
 int ab2_add_umult(ab2_context* ctx, double alpha, const ab2_matrix* A, const ab2_vector* x, ab2_vector* y) {
   if (!ctx || !A || !x || !y || x->n != A->n || y->n != A->n || x->d == y->d) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-AddUMult");
   return guard(ctx, [&] { op_add_lu_mult(ctx, A, alpha, x->d, y->d, false); });
 }
 
 int ab2_compute_inv_diag(ab2_context* ctx, const ab2_matrix* A, ab2_vector* inv) {
   if (!ctx || !A || !inv || inv->n != A->n) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-INVDIAG");
   return guard(ctx, [&] { op_inv_diag(ctx, A, inv->d); });
 }
 
 int ab2_mult_inv_diag(ab2_context* ctx, const ab2_matrix* A, ab2_vector* y) {
   if (!ctx || !A || !y || y->n != A->n) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-MULTINVDIAG");
   return guard(ctx, [&] { op_mult_inv_diag(ctx, A, y->d); });
 }
 
 int ab2_diagonal(ab2_context* ctx, const ab2_matrix* A, ab2_vector* d) {
   if (!ctx || !A || !d || d->n != A->n) return AB2_ERR_BAD_ARG;
+  PhaseScope phase_scope(ctx, "CSR-DIAGONAL");
   return guard(ctx, [&] { op_diagonal(ctx, A, d->d); });
 }
 

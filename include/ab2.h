@@ -99,6 +99,23 @@ typedef struct {
 } ab2_context_info;
 int ab2_context_get_info(const ab2_context* ctx, ab2_context_info* info);
 
+/* Phase timers (the reference's StdTimer sentries under ALIEN_USE_PERF_TIMER,
+ * utils/StdTimer.h): with timing on, every ABI operation records CUDA events
+ * on the context's stream around its work and adds its device time to a
+ * phase named as the reference's ("CSR-SPMV", "CSR-DOT", "CSR-AXPY", ...,
+ * plus "PRECOND-<kind>", "SOLVER-CG", "DIST-SPMV", ...).  Nothing
+ * synchronises until the times are read.  AB2_PERF_TIMER=1 in the environment
+ * turns it on for every new context and prints the phases ("phase:seconds")
+ * when the context is destroyed. */
+typedef struct {
+  char name[32];
+  long long calls;
+  double ms;
+} ab2_phase_time;
+int ab2_context_set_phase_timing(ab2_context* ctx, int on); /* on: (re)start at zero; 0: stop */
+/* Writes up to cap phases, *count = phases recorded (synchronises on their events). */
+int ab2_context_phase_times(ab2_context* ctx, ab2_phase_time* out, int cap, int* count);
+
 /* ------------------------------------------------------------------ matrix */
 /* Copies a host CSR matrix (columns sorted ascending inside each row, as
  * Alien's profilers produce) to the device in the requested formats.

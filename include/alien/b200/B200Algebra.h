@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstddef>
 #include <memory>
+#include <ostream>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -65,6 +66,26 @@ class Context {
     if (rc != AB2_OK) throw Error(rc, std::string(what) + ": " + ab2_last_error_message(m_h.get()));
   }
   void synchronize() const { check(ab2_synchronize(m_h.get()), "ab2_synchronize"); }
+
+  // Phase timers, the reference's StdTimer under ALIEN_USE_PERF_TIMER
+  // (utils/StdTimer.h): device seconds per operation ("CSR-SPMV", "CSR-DOT",
+  // ...) since timing was turned on.
+  void setPhaseTiming(bool on) const { check(ab2_context_set_phase_timing(m_h.get(), on ? 1 : 0), "set_phase_timing"); }
+  std::vector<std::pair<std::string, double>> phaseTimes() const {
+    int n = 0;
+    check(ab2_context_phase_times(m_h.get(), nullptr, 0, &n), "phase_times");
+    std::vector<ab2_phase_time> t((std::size_t)n);
+    if (n) check(ab2_context_phase_times(m_h.get(), t.data(), n, &n), "phase_times");
+    std::vector<std::pair<std::string, double>> out;
+    for (auto const& e : t) out.emplace_back(e.name, e.ms * 1e-3);
+    return out;
+  }
+  // StdTimer::printInfo's layout: phase:seconds between rules.
+  void printInfo(std::ostream& os, const std::string& msg) const {
+    os << "================================\n" << "PERF INFO : " << msg << "\n";
+    for (auto const& p : phaseTimes()) os << p.first << ":" << p.second << "\n";
+    os << "================================" << std::endl;
+  }
 
  private:
   std::shared_ptr<ab2_context> m_h;
