@@ -6,6 +6,9 @@ Rules (src/movesemantic/alien/move/impl/MatrixMarketReader.cc): only
 the SAME value (so a skew-symmetric file comes out symmetric); duplicate
 entries are summed in file order; '%' lines are comments.  Without a
 right-hand-side file b = 1 (benchmark/src/alien/benchmark/MatrixMarketProblem.cpp)."""
+import os
+from pathlib import Path
+
 import numpy as np
 import pytest
 import scipy.io
@@ -104,3 +107,26 @@ def test_bad_files_rejected(tmp_path, text, rhs, msg):
     with pytest.raises(abi.AB2Error) as e:
         abi.read_matrix_market(f, r)
     assert e.value.code == abi.AB2_ERR_BAD_ARG and msg in str(e.value)
+
+
+# The reference's own MatrixMarket fixtures, read where they lie in the
+# reference checkout (ALIEN_REF_SRC, as oracle/Makefile; skipped when absent).
+REF_TESTS = Path(os.environ.get("ALIEN_REF_SRC", "/root/reference/src/core")).parent / "movesemantic" / "tests"
+
+
+@pytest.mark.skipif(not (REF_TESTS / "simple.mtx").exists(), reason="reference checkout absent")
+def test_reference_fixture_simple_mtx():
+    """TestMatrixMarket.cc (movesemantic/tests): simple.mtx is 25 x 25 and
+    simple_rhs.mtx holds i + 1 (floored) at row i, also per row block (the
+    MatrixVector case reads the vector on the matrix's row distribution)."""
+    P = abi.read_matrix_market(str(REF_TESTS / "simple.mtx"), str(REF_TESTS / "simple_rhs.mtx"))
+    assert P.n == 25
+    np.testing.assert_array_equal(np.floor(P.b), np.arange(1, 26))
+    for off in ([0, 25], [0, 12, 25], [0, 7, 13, 25]):
+        for a, b in zip(off[:-1], off[1:]):
+            np.testing.assert_array_equal(np.floor(P.b[a:b]), np.arange(a, b) + 1)
+    S = sp.csr_matrix(scipy.io.mmread(str(REF_TESTS / "simple.mtx")))
+    S.sort_indices()
+    np.testing.assert_array_equal(P.row_ptr, S.indptr)
+    np.testing.assert_array_equal(P.cols, S.indices)
+    np.testing.assert_array_equal(P.vals, S.data)
