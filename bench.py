@@ -460,6 +460,47 @@ def preconditioner_section(abi, ctx, stream, A, P, a):
     return out
 
 
+def small_section(abi, ctx, stream, a):
+    """The plain method at the small size: 3-D 7-point constant-coefficient
+    Poisson on 32^3 (32,768 rows), b = A x_true, Jacobi-CG to 1e-8, max 1000
+    iterations -- the case the reference runs on its CPU path.  The matrix
+    (3.3 MB) lives in L2: a latency-bound case, reported but not a roofline
+    figure.  Beside it the reference's own CG.h + DiagPreconditioner.h
+    (oracle/_ref) solving the same system on one host core."""
+    import torch
+
+    Q = abi.poisson(32, 32, 32, seed=0)
+    A = ctx.matrix(Q.row_ptr, Q.cols, Q.vals)
+    b, x = ctx.vector(Q.b), ctx.vector(Q.n)
+
+    def run(S):
+        ctx.assign(x, 0.0)
+        return S.solve(b, x)
+
+    t, st, _ = timed_solve(torch, stream, lambda: abi.Solver(ctx, A, solver="cg", precond="diag", tol=1e-8,
+                                                              max_iter=1000, use_graph=not a.host_loop), run)
+    out = {"workload": "poisson3d_32^3_cg_jacobi_tol1e-8", "rows": Q.n, "nnz": Q.nnz, "s": round(t, 6),
+           "iterations": st.iterations, "converged": bool(st.succeeded), "true_rel_residual": st.true_residual,
+           "note": "set-up + solve on the device, median of three; the matrix lives in L2 (latency-bound)"}
+    if not a.no_cpu:
+        from oracle import oracle as O
+
+        if O.ref_available():
+            runs = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                r = O.solve(Q.row_ptr, Q.cols, Q.vals, Q.b, solver="cg", precond="diag", tol=1e-8, max_iter=1000,
+                            which="ref")
+                runs.append(time.perf_counter() - t0)
+            out["cpu_reference"] = {"s": round(sorted(runs)[1], 6), "iterations": r.iterations, "cores": 1,
+                                    "kind": "reference",
+                                    "sample": "Alien CG.h + DiagPreconditioner.h (oracle/_ref), whole solve, median "
+                                              "of three"}
+    for o in (b, x, A):
+        o.close()
+    return out
+
+
 def rowblock_section(abi, stream, P, x_single, iters_single, a):
     """The row-block distribution (include/ab2_dist.h) on the headline system:
     the device-resident distributed CG + ILU0 with one rank over NCCL (its
@@ -772,6 +813,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner measurement")
     ap.add_argument("--no-precond", action="store_true", help="skip the per-preconditioner measurements")
     ap.add_argument("--no-rowblock", action="store_true", help="skip the row-block distribution measurements")
+    ap.add_argument("--no-small", action="store_true", help="skip the 32^3 Jacobi-CG case")
     ap.add_argument("--rowblock", action="store_true",
                     help="strong scaling instead: one system split across the N ranks by z-slabs (NCCL), "
                          "distributed CG")
@@ -900,6 +942,7 @@ def main():
     batched = None if a.no_batch else batch_section(abi, ctx, stream, a)
     learned = None if a.no_learned else learned_section(abi, ctx, stream, a)
     preconds = None if a.no_precond else preconditioner_section(abi, ctx, stream, A, P, a)
+    small = None if a.no_small else small_section(abi, ctx, stream, a)
     rowblock = None if (a.no_rowblock or a.method != "ilu0" or world > 1) else \
         rowblock_section(abi, stream, P, xs, st.iterations, a)
 
@@ -996,7 +1039,7 @@ def main():
                 "solver_gbs": round(st.iterations * iteration_bytes(a.method, P.n, P.nnz) / (st.solve_ms * 1e-3)
                                     / 1e9, 1),
                 "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "methods": methods, "mixed": mixed, "batched": batched,
-                "learned": learned, "preconditioners": preconds, "rowblock": rowblock,
+                "learned": learned, "preconditioners": preconds, "rowblock": rowblock, "small": small,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     from alien_b200 import dist
