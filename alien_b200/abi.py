@@ -27,7 +27,7 @@ AB2_ERR_BAD_ARG = -6
 AB2_ERR_UNSUPPORTED = -7
 
 FMT_CSR, FMT_ELL, FMT_F32 = 1, 2, 4
-SPMV_AUTO, SPMV_CSR_SCALAR, SPMV_CSR_STAGED, SPMV_ELL = 0, 1, 2, 3
+SPMV_AUTO, SPMV_CSR_SCALAR, SPMV_CSR_STAGED, SPMV_ELL, SPMV_CSR_VECTOR = 0, 1, 2, 3, 4
 SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
 PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3, "filu0": 4, "neumann": 5}
 ILU_SCHEDULE = {"auto": 0, "wavefront": 1, "stencil": 2}

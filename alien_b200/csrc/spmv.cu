@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 
 #include "ab2_internal.cuh"
@@ -132,6 +133,69 @@ __global__ void __launch_bounds__(kThreads) k_spmv_csr_staged(const int* __restr
       }
     }
   }
+}
+
+// A group of LPR lanes per row (LPR = 4, 8, 16 or 32, chosen from the mean
+// row length), for matrices whose rows are long: the lanes read the row's
+// values and columns as 16- and 8-byte pairs (2 doubles, 2 int32 columns),
+// two pairs in flight per lane per pass, and the group sums its lanes'
+// partial sums with shuffles.  The row's sum is therefore grouped, not
+// sequential: results differ from the reference's row-sequential order in
+// the last bits, which is why no solver or AUTO choice uses this kernel
+// (ab2_mult_variant only).  Pairs start at even entry offsets, so the value
+// and column arrays (whole device allocations) give aligned loads; an odd
+// first entry and an odd last entry are read singly.
+template <int LPR>
+__global__ void __launch_bounds__(kThreads) k_spmv_csr_vector(int n, const int* __restrict__ rp,
+                                                              const int* __restrict__ ci, const double* __restrict__ v,
+                                                              const double* __restrict__ x, double* __restrict__ y) {
+  constexpr int RPW = 32 / LPR;  // rows per warp per pass
+  const int lane = threadIdx.x & 31, sub = lane % LPR, grp = lane / LPR;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  // every lane of the warp runs every pass (the shuffles take the full mask);
+  // a group past the last row works on an empty row and stores nothing
+  for (long long w0 = warp * RPW; w0 < n; w0 += nwarps * RPW) {
+    const long long row = w0 + grp;
+    int b = 0, e = 0;
+    if (row < n) {
+      b = rp[row];
+      e = rp[row + 1];
+    }
+    double acc = 0;
+    const int a0 = min(e, (b + 1) & ~1);  // first even offset in the row
+    const int a1 = max(a0, e & ~1);       // end of the paired body
+    if (sub == 0 && b < a0) acc = mul_add_rn(v[b], __ldg(x + ci[b]), acc);
+    int k = a0 + 2 * sub;
+    for (; k + 2 * LPR < a1; k += 4 * LPR) {
+      const double2 v0 = *reinterpret_cast<const double2*>(v + k);
+      const int2 c0 = *reinterpret_cast<const int2*>(ci + k);
+      const double2 v1 = *reinterpret_cast<const double2*>(v + k + 2 * LPR);
+      const int2 c1 = *reinterpret_cast<const int2*>(ci + k + 2 * LPR);
+      const double x0 = __ldg(x + c0.x), x1 = __ldg(x + c0.y), x2 = __ldg(x + c1.x), x3 = __ldg(x + c1.y);
+      acc = mul_add_rn(v0.x, x0, acc);
+      acc = mul_add_rn(v0.y, x1, acc);
+      acc = mul_add_rn(v1.x, x2, acc);
+      acc = mul_add_rn(v1.y, x3, acc);
+    }
+    if (k < a1) {
+      const double2 v0 = *reinterpret_cast<const double2*>(v + k);
+      const int2 c0 = *reinterpret_cast<const int2*>(ci + k);
+      acc = mul_add_rn(v0.x, __ldg(x + c0.x), acc);
+      acc = mul_add_rn(v0.y, __ldg(x + c0.y), acc);
+    }
+    if (sub == 0 && a1 < e) acc = mul_add_rn(v[a1], __ldg(x + ci[a1]), acc);
+#pragma unroll
+    for (int off = LPR / 2; off > 0; off >>= 1) acc = add_rn(acc, __shfl_down_sync(0xffffffffu, acc, off, LPR));
+    if (sub == 0 && row < n) y[row] = acc;
+  }
+}
+
+template <int LPR>
+void launch_csr_vector(ab2_context* ctx, const ab2_matrix* A, const double* v, const double* x, double* y) {
+  const long long n = A->n, warps = std::min<long long>((n + 32 / LPR - 1) / (32 / LPR), (long long)ctx->num_sms * 64);
+  k_spmv_csr_vector<LPR><<<(int)((warps * 32 + kThreads - 1) / kThreads), kThreads, 0, ctx->stream>>>(
+      A->n, A->d_rp, A->d_ci, v, x, y);
 }
 
 template <class T>
@@ -282,6 +346,17 @@ void spmv_t(ab2_context* ctx, const ab2_matrix* A, const T* v_csr, const T* v_el
       break;
     case AB2_SPMV_CSR_STAGED:
       k_spmv_csr_staged<T><<<A->n_row_blocks, kThreads, 0, ctx->stream>>>(A->d_row_blocks, A->d_rp, A->d_ci, v_csr, x, y);
+      break;
+    case AB2_SPMV_CSR_VECTOR:
+      if constexpr (sizeof(T) == 8) {  // FP64 only: ab2_mult_variant is its one caller
+        const long long mean = A->nnz / n;
+        if (mean <= 8) launch_csr_vector<4>(ctx, A, v_csr, x, y);
+        else if (mean <= 16) launch_csr_vector<8>(ctx, A, v_csr, x, y);
+        else if (mean <= 32) launch_csr_vector<16>(ctx, A, v_csr, x, y);
+        else launch_csr_vector<32>(ctx, A, v_csr, x, y);
+      } else {
+        throw Error{AB2_ERR_UNSUPPORTED, "the grouped-lane SpMV runs in FP64 only"};
+      }
       break;
     case AB2_SPMV_ELL:
       require(v_ell != nullptr, "matrix has no sliced-ELL copy in this precision");

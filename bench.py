@@ -666,6 +666,49 @@ def rowblock_main(a, world, rank, local) -> int:
 GNN_WEIGHTS = ROOT / "alien_b200" / "gnn_weights.npy"
 
 
+def long_row_matrix(n: int, mean: int, seed: int = 0):
+    """Synthetic long-row CSR system: row i holds L_i entries (L_i uniform in
+    [mean/4, 7 mean/4]) at columns i + j (n // L_i) mod n, diagonal first,
+    sorted; values uniform in [-1, 1].  The shape on which one thread per
+    row stalls and a warp per row does not."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(mean // 4, 7 * mean // 4 + 1, n).astype(np.int64)
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    row = np.repeat(np.arange(n, dtype=np.int64), lens)
+    j = np.arange(rp[-1], dtype=np.int64) - rp[row]
+    col = (row + j * (n // lens[row])) % n
+    order = np.argsort(row * n + col, kind="stable")
+    return rp.astype(np.int32), col[order].astype(np.int32), rng.uniform(-1, 1, rp[-1])
+
+
+def spmv_variant_section(abi, ctx, timed, A, P, a):
+    """Every SpMV variant timed alone on the headline matrix and on a
+    long-row matrix; GB/s over the CSR algorithmic bytes (value + column per
+    entry, row pointers, x and y once), which the ELL variant also moves at
+    slice width 7."""
+    names = {abi.SPMV_CSR_SCALAR: "csr_scalar", abi.SPMV_CSR_STAGED: "csr_staged",
+             abi.SPMV_CSR_VECTOR: "csr_warp_per_row", abi.SPMV_ELL: "ell32"}
+
+    def table(M, n, nnz, variants):
+        x, y = ctx.vector(np.random.default_rng(5).uniform(-1, 1, n)), ctx.vector(n)
+        nbytes = 12 * nnz + 4 * (n + 1) + 16 * n
+        out = {}
+        for v in variants:
+            ms = timed(lambda v=v: ctx.mult(M, x, y, v), 30)
+            out[names[v]] = {"us": round(ms * 1e3, 1), "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1)}
+        return out
+
+    res = {"bytes": "12 nnz + 4 (n + 1) + 16 n",
+           "headline": table(A, P.n, P.nnz, list(names))}
+    rp, ci, v = long_row_matrix(a.long_rows, 256)
+    L = ctx.matrix(rp, ci, v, abi.FMT_CSR | abi.FMT_ELL)
+    res["long_rows"] = {"n": a.long_rows, "nnz": int(rp[-1]), "row_len": "uniform 64..448",
+                        **table(L, a.long_rows, int(rp[-1]), list(names))}
+    L.close()
+    return res
+
+
 def gnn_apply_bytes(n: int, nbw: int) -> int:
     """Algorithmic bytes of one network application: scale (r, 1/sqrt(a_ii)
     read, x_r written), encoder (x_r, log a_ii read, h1 written), three layers
@@ -814,6 +857,8 @@ def main():
     ap.add_argument("--no-precond", action="store_true", help="skip the per-preconditioner measurements")
     ap.add_argument("--no-rowblock", action="store_true", help="skip the row-block distribution measurements")
     ap.add_argument("--no-small", action="store_true", help="skip the 32^3 Jacobi-CG case")
+    ap.add_argument("--no-variants", action="store_true", help="skip the per-variant SpMV table")
+    ap.add_argument("--long-rows", type=int, default=262144, help="rows of the long-row SpMV matrix")
     ap.add_argument("--rowblock", action="store_true",
                     help="strong scaling instead: one system split across the N ranks by z-slabs (NCCL), "
                          "distributed CG")
@@ -973,6 +1018,7 @@ def main():
     spmv_ms = timed(lambda: ctx.mult(A, b, vy, abi.SPMV_ELL), 50)
     spmv_roof = roof("k_spmv_ell (sliced ELL-32 FP64 SpMV)", spmv_bytes(info, P.n), spmv_ms, f"spmv_ell_{n1}")
     achieved = spmv_roof["achieved"]
+    variants = None if a.no_variants else spmv_variant_section(abi, ctx, timed, A, P, a)
 
     # The headline step's dominant kernel: for ILU0 the two triangular sweeps
     # (one precond apply), else the SpMV.
@@ -1038,7 +1084,7 @@ def main():
                 "setup_ms": round(st.setup_ms, 3), "solve_ms": round(st.solve_ms, 3),
                 "solver_gbs": round(st.iterations * iteration_bytes(a.method, P.n, P.nnz) / (st.solve_ms * 1e-3)
                                     / 1e9, 1),
-                "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "methods": methods, "mixed": mixed, "batched": batched,
+                "spmv_gbs": achieved, "roofline": roofline, "spmv_roofline": spmv_roof, "spmv_variants": variants, "methods": methods, "mixed": mixed, "batched": batched,
                 "learned": learned, "preconditioners": preconds, "rowblock": rowblock, "small": small,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)

@@ -57,6 +57,10 @@ extern "C" {
 #define AB2_SPMV_CSR_SCALAR 1 /* one thread per row, values read straight from HBM */
 #define AB2_SPMV_CSR_STAGED 2 /* row blocks staged through shared memory */
 #define AB2_SPMV_ELL 3        /* sliced ELL, one thread per row, coalesced slots */
+#define AB2_SPMV_CSR_VECTOR 4 /* FP64, 4/8/16/32 lanes per row by mean row length, 16-byte loads, lanes' partial
+                                 sums combined by shuffles: for long rows; NOT the reference's row-sequential
+                                 summation order (last-bit differences), so only ab2_mult_variant uses it --
+                                 solvers and AUTO never do */
 
 /* solvers / preconditioners (same names as the krylov example's options) */
 #define AB2_SOLVER_CG 0

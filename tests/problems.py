@@ -32,6 +32,8 @@ def get(name: str) -> abi.CsrProblem:
         return ragged(1000, seed=11)
     if name == "longrow":
         return long_row_matrix()
+    if name.startswith("wide"):  # wide<mean>: rows of mean/4 .. 7 mean/4 entries
+        return wide_rows(3001, int(name[4:]), seed=17)
     raise KeyError(name)
 
 
@@ -76,6 +78,27 @@ def long_row_matrix(n: int = 4000, seed: int = 13) -> abi.CsrProblem:
     row_ptr = np.asarray(row_ptr, dtype=np.int32)
     cols = np.asarray(cols, dtype=np.int32)
     vals = np.asarray(vals)
+    x_true = rng.uniform(-1, 1, size=n)
+    from oracle import oracle as O
+
+    return abi.CsrProblem(n, row_ptr, cols, vals, x_true, O.spmv(row_ptr, cols, vals, x_true), None, (n, 1, 1))
+
+
+def wide_rows(n: int, mean: int, seed: int) -> abi.CsrProblem:
+    """Rows of uniform random length in [mean/4, 7 mean/4] (at least 1), the
+    diagonal plus columns spread at stride n / length, diagonally dominant."""
+    rng = np.random.default_rng(seed)
+    lens = np.maximum(1, rng.integers(mean // 4, 7 * mean // 4 + 1, n))
+    row_ptr = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=row_ptr[1:])
+    row = np.repeat(np.arange(n), lens)
+    j = np.arange(row_ptr[-1]) - row_ptr[row]
+    cols = (row + j * (n // lens[row])) % n
+    order = np.argsort(row * n + cols, kind="stable")
+    cols = cols[order].astype(np.int32)
+    vals = rng.uniform(-1, 1, row_ptr[-1])
+    vals[cols == row] = lens + 1.0
+    row_ptr = row_ptr.astype(np.int32)
     x_true = rng.uniform(-1, 1, size=n)
     from oracle import oracle as O
 

@@ -33,6 +33,26 @@ def test_spmv_bit_exact(ctx, name, variant):
     np.testing.assert_array_equal(vy.download(), O.spmv(P.row_ptr, P.cols, P.vals, x))
 
 
+@pytest.mark.parametrize("name", MATRICES + ["diffusion64", "wide12", "wide24", "wide200", "wide1000"])
+def test_spmv_warp_per_row(ctx, name):
+    """The grouped-lane variant splits a row across 4, 8, 16 or 32 lanes (by
+    mean row length; the wide* matrices reach every width) and adds their
+    partial sums in a shuffle tree: not the sequential order, so it is held to
+    1e-13 of sum |a_ij x_j| per row, and must be bit-reproducible."""
+    P = problems.get(name)
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals, abi.FMT_CSR)
+    x = rnd(P.n, 4)
+    vx, vy = ctx.vector(x), ctx.vector(P.n)
+    ctx.mult(A, vx, vy, abi.SPMV_CSR_VECTOR)
+    got = vy.download()
+    exp = O.spmv(P.row_ptr, P.cols, P.vals, x)
+    scale = O.spmv(P.row_ptr, P.cols, np.abs(P.vals), np.abs(x))
+    assert np.all(np.abs(got - exp) <= 1e-13 * scale)
+    ctx.mult(A, vx, vy, abi.SPMV_CSR_VECTOR)
+    np.testing.assert_array_equal(vy.download(), got)
+    A.close()
+
+
 @pytest.mark.parametrize("name", ["diffusion12", "ragged"])
 def test_lu_products_invdiag(ctx, name):
     P = problems.get(name)
