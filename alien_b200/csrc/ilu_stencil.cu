@@ -13,9 +13,10 @@
 // walks the tile's diagonals: at step s thread (li,lj) computes cell
 // k = s - li - lj.  Its k-1 input is its own previous value (a register), the
 // i-1 and j-1 inputs were computed by neighbouring threads at step s-1 (shared
-// memory, one __syncthreads per step).  Only the first line of a tile reads a
+// memory, one named barrier per step).  Only the first line of a tile reads a
 // value owned by another tile, 15 steps ahead in that tile's walk; those come
-// through global memory with the sentinel-value wait of sentinel.cuh.  Tiles
+// through global memory (the sentinel values of sentinel.cuh), fetched by a
+// ninth, polling warp that hands them over through shared memory.  Tiles
 // are claimed from an atomic ticket in dependency order (a tile waits only on
 // tiles with a smaller ticket), so no co-residency is needed.
 //
@@ -67,11 +68,12 @@ namespace {
 constexpr int kTile = 16;
 constexpr int kTileThreads = kTile * kTile;
 constexpr int kWalkPrefetch = 8;  // steps a walk loads ahead; the walk length is padded to a multiple
-// Steps ahead a walk loads its neighbouring tiles' values.  A consumer tile
-// trails its producer by this distance plus the 15-step skew and the
-// store-to-load latency; 2..7 measured within 3% of each other at 64^3-192^3
-// on B200, 4 the best.
-constexpr int kWalkPrefetchB = 4;
+// The sweeps' poll warp: steps whose neighbouring-tile values it loads per
+// round (all in flight at once), and the shared-memory ring it hands them to
+// the compute warps through.
+constexpr int kPollDepth = 8;
+constexpr int kBndRing = 16;
+static_assert(kBndRing >= kPollDepth, "a poll round fits in the ring");
 
 struct Geom {
   int nx, ny, nz, ntx, nty;
@@ -384,14 +386,26 @@ struct WalkArrays {
   const T *Lk, *Lj, *Li, *Ui, *Uj, *Uk, *P;
 };
 
-// Per-step inputs, loaded kWalkPrefetch steps ahead: the right-hand side,
-// three band values (L: -k,-j,-i ; U: +i,+j,+k), the pivot (U walk), and the
-// value owned by the neighbouring tile (bi / bj, first line of the tile only),
-// possibly still the sentinel when loaded.
+// Per-step inputs of a compute thread, loaded kWalkPrefetch steps ahead: the
+// right-hand side, three band values (L: -k,-j,-i ; U: +i,+j,+k) and the
+// pivot (U walk).
 template <class T>
 struct PreW {
-  T y, a1, a2, a3, piv, bi, bj;
+  T y, a1, a2, a3, piv;
 };
+
+__device__ __forceinline__ void compute_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kTileThreads) : "memory"); }
+
+template <class T>
+__device__ __forceinline__ T quiet_nan();
+template <>
+__device__ __forceinline__ double quiet_nan<double>() {
+  return __longlong_as_double(0x7FF8000000000000LL);
+}
+template <>
+__device__ __forceinline__ float quiet_nan<float>() {
+  return __uint_as_float(0x7FC00000u);
+}
 
 // One triangular sweep in walk layout.  UP = false: forward sweep
 // x_i = y_i - sum_{k<dcol} l_ik x_k (solveL, ILU0Preconditioner.h:181-198) from
@@ -399,20 +413,44 @@ struct PreW {
 // / u_ii (solveU, :200-231), reading `in` through the reversed index and
 // putting it back to the sentinel.  `wave` must hold the sentinel on entry.
 //
-// A step is a handful of instructions per thread, and with one 256-thread CTA
-// per SM the schedulers have two warps each, so the step time is close to
-// the instruction count: every array is reached through a per-thread pointer
-// that moves once per group of kWalkPrefetch steps, with constant offsets
-// inside the unrolled group.
-template <bool UP, class T, int kPreB = kWalkPrefetchB>
-__global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArrays<T> b, T* in, T* wave,
-                                                              unsigned int* tickets, int* err) {
+// A CTA is 8 compute warps (the 16 x 16 lines of a tile, synchronised per
+// step on named barrier 1) and one poll warp.  The 32 values a step needs
+// from the two neighbouring tiles (the first line's inputs: lane l < 16 the
+// j-side value of line (l, 0), lane 16 + l the i-side value of line (0, l))
+// are fetched by the poll warp: each round it loads the next kPollDepth
+// steps' values at once, publishes the leading steps whose values have all
+// arrived into a ring in shared memory (s_ready = last published step), and
+// reloads the rest in the next round.  A compute thread on the first line
+// spins on s_ready in shared memory, not on a global load.  Why: a tile's
+// first steps run right behind its neighbour's; a compute warp that found
+// the sentinel and polled L2 itself paid a full round trip inside every such
+// step (about 1 us against a 0.26 us step), and the next tile waits on those
+// steps -- at 192^3 that cost 16-18 us per tile boundary on the critical
+// path.  With the polls in flight beside the compute, a step waits only for
+// the value's arrival.
+//
+// Every wait is bounded (kWaitCycles without progress): the poll warp then
+// records the error and publishes quiet NaNs, so the compute warps and the
+// kernel always finish.
+//
+// Compute warps: a step is a handful of instructions per thread, and every
+// array is reached through a per-thread pointer that moves once per group of
+// kWalkPrefetch steps, with constant offsets inside the unrolled group.
+template <bool UP, class T>
+__global__ void __launch_bounds__(kTileThreads + 32, 1) k_walk_sweep(Walk g, WalkArrays<T> b, T* in, T* wave,
+                                                                   unsigned int* tickets, int* err) {
   constexpr int kPre = kWalkPrefetch;
-  static_assert(kPreB >= 1 && kPreB < kPre, "boundary values are loaded inside the band prefetch window");
   constexpr long long kStep = UP ? -kTileThreads : kTileThreads;  // element stride of one step
   __shared__ T s_val[2][kTile][kTile + 1];
+  __shared__ T s_bnd[kBndRing][2 * kTile];
   __shared__ int s_tile;
-  const int li = threadIdx.x % kTile, lj = threadIdx.x / kTile;
+  __shared__ volatile int s_ready;  // last step whose neighbouring values are in s_bnd
+  __shared__ volatile int s_done;   // last step the compute warps have finished
+  const bool poller = threadIdx.x >= kTileThreads;
+  const int lane = threadIdx.x & 31;
+  // The line this thread computes (compute warps) or feeds (poll warp).
+  const int li = poller ? (lane < kTile ? lane : 0) : threadIdx.x % kTile;
+  const int lj = poller ? (lane < kTile ? 0 : lane - kTile) : threadIdx.x / kTile;
   const int ntiles = g.ntx * g.nty;
   const int nsteps = g.nsteps;
   // Walk coordinates of the grid's first cell (the U walk's tiles are the
@@ -425,7 +463,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArra
 
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) s_tile = (int)atomicAdd(tickets + (UP ? 2 : 1), 1u);
+    if (threadIdx.x == 0) {
+      s_tile = (int)atomicAdd(tickets + (UP ? 2 : 1), 1u);
+      s_ready = -1;
+      s_done = -1;
+    }
     __syncthreads();
     const int tile = s_tile;
     if (tile >= ntiles) break;
@@ -438,11 +480,72 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArra
     const int s_lo = active ? li + lj + oz : nsteps;
     const int s_hi = active ? s_lo + g.nz : nsteps;
     const long long tbase = (long long)tile * nsteps * kTileThreads;
-    // Step-0 pointers.  Own cell: walk index tbase + thread.  Neighbouring
-    // tile's cell at the same k: 15 steps further in that tile's walk.
+
+    if (poller) {
+      // Neighbouring tile's cell at the same k: 15 steps further in that
+      // tile's walk (its last line along i, resp. j).
+      const bool need = lane < kTile ? bnd_j : bnd_i;
+      if (!__any_sync(0xffffffffu, need)) continue;  // first tile row and column: nothing to fetch
+      const long long w_nb =
+          lane < kTile ? phys(tbase - (long long)g.ntx * nsteps * kTileThreads + 15 * kTileThreads + 15 * kTile + li)
+                       : phys(tbase - (long long)nsteps * kTileThreads + 15 * kTileThreads + lj * kTile + 15);
+      const T* p_nb = wave + (need ? w_nb : 0);
+      long long t_last = clock64();
+      bool failed = false;
+      for (int t = 0; t < nsteps;) {
+        // ring space: slot (t + d) % kBndRing is free once step t + d - kBndRing is done
+        const int space = __shfl_sync(0xffffffffu, s_done, 0) + kBndRing - t + 1;
+        if (space <= 0) {
+          __nanosleep(64);
+          bool stop = (clock64() - t_last > kWaitCycles) || *(volatile int*)err;
+          if (__any_sync(0xffffffffu, stop)) {  // the compute warps stopped progressing: give up
+            if (lane == 0) atomicOr(err, 1);
+            break;
+          }
+          continue;
+        }
+        T v[kPollDepth];
+#pragma unroll
+        for (int d = 0; d < kPollDepth; ++d) {
+          const int st = t + d;
+          v[d] = (need && st >= s_lo && st < s_hi && !failed) ? ld_relaxed(p_nb + (long long)st * kStep) : T(0);
+        }
+        int first_missing = kPollDepth;
+#pragma unroll
+        for (int d = kPollDepth - 1; d >= 0; --d) {
+          const int st = t + d;
+          if (need && st >= s_lo && st < s_hi && is_sentinel(v[d]) && !failed) first_missing = d;
+        }
+        int n_pub = __reduce_min_sync(0xffffffffu, first_missing);
+        if (n_pub == 0) {
+          bool stop = (clock64() - t_last > kWaitCycles) || *(volatile int*)err;
+          if (__any_sync(0xffffffffu, stop)) {
+            // give up on the missing values: quiet NaNs from here on
+            if (lane == 0) atomicOr(err, 1);
+            failed = true;
+          }
+          continue;
+        }
+        n_pub = min(n_pub, space);
+#pragma unroll
+        for (int d = 0; d < kPollDepth; ++d) {
+          const int st = t + d;
+          if (d < n_pub && need && st >= s_lo && st < s_hi)
+            s_bnd[st % kBndRing][lane] = failed ? quiet_nan<T>() : v[d];
+        }
+        __syncwarp();
+        if (lane == 0) {
+          __threadfence_block();
+          s_ready = t + n_pub - 1;
+        }
+        t += n_pub;
+        t_last = clock64();
+      }
+      continue;
+    }
+
+    // Compute warps.  Step-0 pointers: own cell at walk index tbase + thread.
     const long long w_own = phys(tbase + threadIdx.x);
-    const long long w_bi = phys(tbase - (long long)nsteps * kTileThreads + 15 * kTileThreads + lj * kTile + 15);
-    const long long w_bj = phys(tbase - (long long)g.ntx * nsteps * kTileThreads + 15 * kTileThreads + 15 * kTile + li);
     const T* p_y = in + w_own;
     const T* p_a1 = (UP ? b.Ui : b.Lk) + w_own;
     const T* p_a2 = (UP ? b.Uj : b.Lj) + w_own;
@@ -450,15 +553,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArra
     const T* p_piv = b.P + w_own;
     T* p_in = in + w_own;
     T* p_out = wave + w_own;
-    const T* p_bi = wave + (bnd_i ? w_bi : w_own);
-    const T* p_bj = wave + (bnd_j ? w_bj : w_own);
 
     // Loads of step s (offset o = s * kStep from the step-0 pointers).
-    auto load_b = [&](int s, long long o, PreW<T>& p) {
-      if (s < s_lo || s >= s_hi) return;
-      if (bnd_j) p.bj = ld_relaxed(p_bj + o);
-      if (bnd_i) p.bi = ld_relaxed(p_bi + o);
-    };
     auto load = [&](int s, long long o, PreW<T>& p) {
       if (s < s_lo || s >= s_hi) return;
       // Read-only path: none of these is written during the walk except
@@ -469,13 +565,28 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArra
       p.a3 = __ldg(p_a3 + o);
       if (UP) p.piv = __ldg(p_piv + o);
     };
+    // The step's neighbouring-tile values, from the poll warp's ring.
+    auto boundary = [&](int s, T& vi, T& vj) {
+      if (s_ready < s) {
+        const long long t0 = clock64();
+        for (unsigned it = 1; s_ready < s; ++it) {
+          if ((it & 255) == 0 && (clock64() - t0 > kWaitCycles || *(volatile int*)err)) {
+            atomicOr(err, 1);
+            vi = vj = quiet_nan<T>();
+            return;
+          }
+        }
+      }
+      __threadfence_block();
+      if (bnd_j) vj = s_bnd[s % kBndRing][li];
+      if (bnd_i) vi = s_bnd[s % kBndRing][kTile + lj];
+    };
 
     PreW<T> pre[kPre];
 #pragma unroll
     for (int u = 0; u < kPre; ++u) {
-      pre[u] = PreW<T>{0, 0, 0, 0, 0, 0, 0};
+      pre[u] = PreW<T>{0, 0, 0, 0, 0};
       load(u, u * kStep, pre[u]);
-      if (u < kPreB) load_b(u, u * kStep, pre[u]);
     }
     T own = 0;
     for (int s0 = 0; s0 < nsteps; s0 += kPre) {  // nsteps is a multiple of kPre
@@ -486,13 +597,13 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArra
         const long long o = o0 + u * kStep;
         const PreW<T> c = pre[u];
         load(s + kPre, o + kPre * kStep, pre[u]);
-        load_b(s + kPreB, o + kPreB * kStep, pre[(u + kPreB) % kPre]);
         T val = 0;
         if (s >= s_lo && s < s_hi) {
           const T* prev = &s_val[(s + 1) & 1][0][0];
           T vi = 0, vj = 0;
-          if (has_j) vj = lj > 0 ? prev[(lj - 1) * (kTile + 1) + li] : is_sentinel(c.bj) ? wait_value(p_bj + o, err) : c.bj;
-          if (has_i) vi = li > 0 ? prev[lj * (kTile + 1) + li - 1] : is_sentinel(c.bi) ? wait_value(p_bi + o, err) : c.bi;
+          if (bnd_i || bnd_j) boundary(s, vi, vj);
+          if (has_j && lj > 0) vj = prev[(lj - 1) * (kTile + 1) + li];
+          if (has_i && li > 0) vi = prev[lj * (kTile + 1) + li - 1];
           const bool has_k = s > s_lo;
           T acc = c.y;
           if (!UP) {  // columns ascending: -k, -j, -i
@@ -511,7 +622,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_walk_sweep(Walk g, WalkArra
           own = val;
         }
         s_val[s & 1][lj][li] = val;
-        __syncthreads();
+        compute_bar();
+        if (threadIdx.x == 0) {
+          __threadfence_block();
+          s_done = s;
+        }
       }
     }
   }
@@ -669,10 +784,10 @@ void walk_apply(ab2_context* ctx, const Ilu0Data& d, T* base, const T* y, T* z) 
   if (kTranspose) k_walk_gather_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, y, yw);
   else k_walk_gather<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, y, yw);
   check_launch(ctx, "walk_gather");
-  k_walk_sweep<false, T><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, yw, lw, d.d_tile_tickets,
+  k_walk_sweep<false, T><<<wave_grid(ctx, tiles), kTileThreads + 32, 0, ctx->stream>>>(w, b, yw, lw, d.d_tile_tickets,
                                                                                 d.d_err);
   check_launch(ctx, "walk_lsweep");
-  k_walk_sweep<true, T><<<wave_grid(ctx, tiles), kTileThreads, 0, ctx->stream>>>(w, b, lw, uw, d.d_tile_tickets,
+  k_walk_sweep<true, T><<<wave_grid(ctx, tiles), kTileThreads + 32, 0, ctx->stream>>>(w, b, lw, uw, d.d_tile_tickets,
                                                                                d.d_err);
   check_launch(ctx, "walk_usweep");
   if (kTranspose) k_walk_scatter_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, uw, z);
