@@ -47,11 +47,12 @@
 // same walk (pivots propagate; in a 7-point matrix ILU(0) changes only the
 // diagonal and the L values).
 //
-// Measured on B200, one application at 192^3: 1.02 ms (gather + two walks +
-// scatter), against 1.69 ms for the same walk on natural-order arrays and
-// 3.45 ms for the wavefront schedule of precond.cu.  A lone tile steps in
-// ~0.24 us; the rest is the trail each of the 22 tile boundaries on the
-// critical path adds.
+// Measured on B200, one application at 192^3: 0.61 ms (gather + two walks +
+// scatter; 0.97 ms before the poll warp), against 1.69 ms for the same walk
+// on natural-order arrays and 3.45 ms for the wavefront schedule of
+// precond.cu.  A lone tile steps in ~0.26 us; the rest is the trail each of
+// the 22 tile boundaries on the critical path adds.  Values loaded per poll
+// round: 4 steps (2: 0.63 ms, 3: 0.60, 8: 0.63, 16: 0.70).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -71,7 +72,7 @@ constexpr int kWalkPrefetch = 8;  // steps a walk loads ahead; the walk length i
 // The sweeps' poll warp: steps whose neighbouring-tile values it loads per
 // round (all in flight at once), and the shared-memory ring it hands them to
 // the compute warps through.
-constexpr int kPollDepth = 8;
+constexpr int kPollDepth = 4;
 constexpr int kBndRing = 16;
 static_assert(kBndRing >= kPollDepth, "a poll round fits in the ring");
 
