@@ -32,6 +32,8 @@ SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
 PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3, "filu0": 4, "neumann": 5}
 ILU_SCHEDULE = {"auto": 0, "wavefront": 1, "stencil": 2}
 BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho"}
+FCG_FALLBACK = {"sticky": 0, "step": 1}
+COMM_ID_BYTES = 128
 
 
 class AB2Error(RuntimeError):
@@ -637,7 +639,7 @@ class Comm:
 
     @staticmethod
     def nccl_unique_id() -> bytes:
-        buf = (C.c_ubyte * 128)()
+        buf = (C.c_ubyte * COMM_ID_BYTES)()
         rc = lib().ab2_comm_nccl_unique_id(buf)
         if rc != AB2_OK:
             raise AB2Error(rc, "comm_nccl_unique_id")
@@ -645,7 +647,7 @@ class Comm:
 
     @staticmethod
     def nccl(ctx: Context, uid: bytes, rank: int, size: int) -> "Comm":
-        buf = (C.c_ubyte * 128).from_buffer_copy(uid)
+        buf = (C.c_ubyte * COMM_ID_BYTES).from_buffer_copy(uid)
         h = _P()
         ctx.check(lib().ab2_comm_nccl_create(ctx.h, buf, rank, size, C.byref(h)), "comm_nccl_create")
         return Comm(ctx, h)
@@ -1054,7 +1056,7 @@ def fcg_solve(ctx: Context, A: Matrix, b: Vector, x: Vector, gnn: Gnn | None = N
     if truncation is not None:
         o.truncation = truncation
     if fallback_mode is not None:
-        o.fallback_mode = {"sticky": 0, "step": 1}[fallback_mode]
+        o.fallback_mode = FCG_FALLBACK[fallback_mode]
     st = FcgStatus()
     ctx.check(lib().ab2_fcg_solve(ctx.h, A.h, gnn.h if gnn else None, fallback.h if fallback else None, b.h, x.h,
                                   C.byref(o), C.byref(st)), "fcg_solve")
