@@ -46,6 +46,17 @@ def test_spmv_variants_bit_exact(ctx, big, dev):
         np.testing.assert_array_equal(vy.download(), exp)
 
 
+def test_spmv_grouped_lanes_within_tolerance(ctx, big, dev):
+    """The explicit grouped-lane variant sums a row in a shuffle tree: within
+    1e-13 of sum |a_ij x_j| per row of the sequential result."""
+    x = np.random.default_rng(1).uniform(-1, 1, big.n)
+    exp = O.spmv(big.row_ptr, big.cols, big.vals, x)
+    scale = O.spmv(big.row_ptr, big.cols, np.abs(big.vals), np.abs(x))
+    vx, vy = ctx.vector(x), ctx.vector(big.n)
+    ctx.mult(dev, vx, vy, abi.SPMV_CSR_VECTOR)
+    assert np.all(np.abs(vy.download() - exp) <= 1e-13 * scale)
+
+
 def test_dot_bit_exact(ctx, big):
     rng = np.random.default_rng(2)
     x, y = rng.standard_normal(big.n), rng.standard_normal(big.n)
