@@ -2,7 +2,8 @@
 (7,077,888 rows, 49,324,032 entries).
 
 The oracle is sequential C++, so at this size it checks what it can finish
-in seconds, bit for bit: the SpMV (every variant), the dot product in
+in seconds, bit for bit: the SpMV (every bit-exact variant; the grouped-lane
+one within its tolerance), the dot product in
 libab2's tree, the ILU(0) factor and one application (tile walk and wavefront
 schedule), and the first five CG+ILU0 iterations (history and iterate).  The
 full solve is then checked through properties that do not need the oracle:
