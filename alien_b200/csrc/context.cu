@@ -557,11 +557,13 @@ int ab2_context_phase_times(ab2_context* ctx, ab2_phase_time* out, int cap, int*
 // context's buffers.  The array exists once per GPU that loads libab2 and stays
 // there until the process exits.
 //
-// Each block of this variant reduces a fixed chunk of kNoAllocChunk elements,
-// so the scratch it needs grows with n: kNoAllocSlots partials cover n up to
-// kNoAllocSlots * kNoAllocChunk = 16,777,216 elements; larger n is rejected.
-// (ab2_dot's grid instead follows the context's reduction rule, so the two
-// entry points may sum in different trees and agree to rounding, not bits.)
+// The grid of this variant is ceil(n / kNoAllocChunk) blocks, so it writes at
+// most kNoAllocSlots block partials for n up to kNoAllocSlots * kNoAllocChunk
+// = 16,777,216 elements; larger n is rejected.  Inside the grid k_dot is the
+// usual grid-stride loop: each thread sums the elements spaced one grid apart
+// (up to 16 of them), then the block and finally the last block sum in fixed
+// trees.  (ab2_dot's grid follows the context's reduction rule instead, so the
+// two entry points may sum in different trees and agree to rounding, not bits.)
 //
 // All calls in the process share the array and it keeps the last call's
 // contents; the counter, which must start at zero, is cleared on the caller's

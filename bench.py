@@ -19,9 +19,13 @@ so no explicit flush is needed between steps.
 
 --impl reference times the reference's own CPU path for the same workload:
 Alien's CG.h + ILU0Preconditioner.h templates over the SimpleCSR-restating
-algebra (oracle/_ref), one host core (SimpleCSR is sequential per rank), on a
-bounded sample (set-up + a few iterations) scaled to the iteration count the
-solve needs.
+algebra (oracle/_ref), one host core (SimpleCSR and its ILU(0) sweeps are
+sequential per rank).  It builds the system with the host-only build of the
+same seeded generator (oracle/_build/libab2_inputs.so) and loads no CUDA
+code.  Each warm-up step is a bounded sample (set-up + 2 and 8 iterations,
+whose per-iteration time cross-checks the complete solves); each timed step
+is one COMPLETE solve to convergence, as many of the requested K as fit in
+--ref-budget seconds (at least one); the line reports the counts that ran.
 """
 from __future__ import annotations
 
@@ -211,12 +215,11 @@ def reference_method(method: str) -> tuple[dict, str]:
 def reference_sample(P, method: str, iterations_hint: int | None, sample_iters=(2, 8)):
     """Alien's own templates (oracle/_ref) on one host core: set-up + a few
     iterations, extrapolated to `iterations_hint` (the iteration count this
-    solve takes; the templates and the GPU agree on it to +-2)."""
+    solve takes; the templates and the GPU agree on it to +-2).  A bounded
+    sample: the complete solve is timed by reference_solve."""
     from oracle import oracle as O
 
-    kw, _ = reference_method(method)
-    if kw["precond"] == "neumann":
-        kw["poly_factor"] = 1.0 / float(np.add.reduceat(np.abs(P.vals), P.row_ptr[:-1]).max())
+    kw = reference_kwargs(P, method)
     times = []
     for m in sample_iters:
         t = time.perf_counter()
@@ -227,6 +230,92 @@ def reference_sample(P, method: str, iterations_hint: int | None, sample_iters=(
     setup = max(t1 - i1 * per_iter, 0.0)
     iters = iterations_hint if iterations_hint else i2
     return setup + per_iter * iters, setup, per_iter, sum(t for _, t in times)
+
+
+def reference_kwargs(P, method: str) -> dict:
+    kw, _ = reference_method(method)
+    if kw["precond"] == "neumann":
+        kw["poly_factor"] = 1.0 / float(np.add.reduceat(np.abs(P.vals), P.row_ptr[:-1]).max())
+    return kw
+
+
+def reference_solve(P, method: str, max_iter: int):
+    """One complete solve by Alien's own templates (oracle/_ref) on one host
+    core, set-up included: (seconds, result)."""
+    from oracle import oracle as O
+
+    kw = reference_kwargs(P, method)
+    t = time.perf_counter()
+    r = O.solve(P.row_ptr, P.cols, P.vals, P.b, tol=1e-8, max_iter=max_iter, which="ref", **kw)
+    return time.perf_counter() - t, r
+
+
+def host_info() -> dict:
+    """The host the CPU legs ran on: logical cores and the CPU model."""
+    model = None
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.lower().startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "cpu_model": model}
+
+
+def solution_digest(x: np.ndarray) -> dict:
+    """Size-independent figures of a solution, printed by both arms so that
+    their solutions can be compared across processes: 2-norm, plain sum and
+    the dot with a fixed +-1 pattern."""
+    w = np.where(np.arange(x.size) % 3 == 0, 1.0, -1.0)
+    return {"norm2": float(np.linalg.norm(x)), "sum": float(np.sum(x)), "dot_pm1": float(np.dot(w, x))}
+
+
+def reference_main(a, world: int, rank: int, P, config: dict) -> int:
+    """--impl reference: Alien's templates on the host cores (rank 0 only)."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    _, label = reference_method(a.method)
+    t_start = time.perf_counter()
+    samples = []
+    for _ in range(a.warmup):  # bounded samples; their per-iteration time cross-checks the complete solves
+        samples.append(reference_sample(P, a.method, None))
+    steps, res = [], None
+    t0 = time.perf_counter()
+    while len(steps) < max(a.steps, 1):
+        dt, res = reference_solve(P, a.method, a.max_iter)
+        steps.append(dt)
+        if time.perf_counter() - t0 + dt > a.ref_budget:
+            break
+    value = float(np.median(steps))
+    r_true = P.b - O.spmv(P.row_ptr, P.cols, P.vals, res.x)
+    true_rel = float(np.linalg.norm(r_true) / np.linalg.norm(P.b))
+    cross = None
+    if samples:
+        _, setup, per_iter, _ = samples[-1]
+        cross = {"sample_setup_s": round(setup, 4), "sample_ms_per_iteration": round(per_iter * 1e3, 3),
+                 "extrapolated_s": round(setup + per_iter * res.iterations, 3),
+                 "note": "set-up + 2 and 8 iterations (a warm-up step), scaled to the complete solve's iterations"}
+    host = host_info()
+    line = {"metric": "time_to_true_rel_residual_1e-8", "value": value, "unit": "s", "n_gpus": a.gpus,
+            "steps": len(steps), "warmup": len(samples), "requested": {"steps": a.steps, "warmup": a.warmup},
+            "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded generator, host-only build)", "impl": "reference",
+            "config": config, "iterations": res.iterations, "converged": bool(res.converged),
+            "true_rel_residual": true_rel,
+            "rel_error_vs_x_true": float(np.linalg.norm(res.x - P.x_true) / np.linalg.norm(P.x_true)),
+            "solution_digest": solution_digest(res.x), "step_times_s": [round(t, 4) for t in steps],
+            "cross_check": cross,
+            "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": "reference", **host,
+                             "sample": f"Alien CG.h + {label} (oracle/_ref) on 1 host core, {len(steps)} complete "
+                                       f"solve(s) to convergence ({res.iterations} iterations), set-up included; "
+                                       f"SimpleCSR and its ILU(0) sweeps are sequential per rank"},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": round(time.perf_counter() - t_start, 2)}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def timed_solve(torch, stream, make, run, reps=3):
@@ -862,56 +951,40 @@ def main():
     ap.add_argument("--rowblock", action="store_true",
                     help="strong scaling instead: one system split across the N ranks by z-slabs (NCCL), "
                          "distributed CG")
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="--impl reference: seconds of complete solves to fit the timed steps into")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the Krylov loop from the host instead of the CUDA graph (same kernels; for "
                          "profilers that do not see kernels inside conditional graph nodes)")
     a = ap.parse_args()
 
+    n1 = a.n
+    head_solver = METHODS[a.method].get("solver", "cg")
+    workload = f"diffusion3d_{n1}^3_grf_sigma1_len4_{'cg_' if head_solver == 'cg' else ''}{a.method}_tol1e-8"
+
+    def make_config(P):
+        return {"workload": workload, "rows": P.n, "nnz": P.nnz, "precision": "fp64", "solver": head_solver,
+                "method": a.method, "tol": 1e-8, "formats": "csr+ell32", "l2": "inputs larger than L2 (no flush)",
+                "parallelism": f"independent systems x{world}"}
+
+    if a.impl == "reference":
+        # No process group, no CUDA: rank 0 alone times the host path, the others exit.
+        from alien_b200 import dist
+        from oracle import oracle as O
+
+        world, rank, local = dist.ranks()
+        if rank != 0:
+            return 0
+        P = O.problem_diffusion(n1, n1, n1, sigma=1.0, smooth=4.0, seed=rank)
+        return reference_main(a, world, rank, P, make_config(P))
+
     world, rank, local = dist_init()
-    if a.rowblock and a.impl == "ours":
+    if a.rowblock:
         return rowblock_main(a, world, rank, local)
     from alien_b200 import abi
 
-    n1 = a.n
     P = abi.diffusion(n1, n1, n1, sigma=1.0, smooth=4.0, seed=rank)
-    head_solver = METHODS[a.method].get("solver", "cg")
-    workload = f"diffusion3d_{n1}^3_grf_sigma1_len4_{'cg_' if head_solver == 'cg' else ''}{a.method}_tol1e-8"
-    config = {"workload": workload, "rows": P.n, "nnz": P.nnz, "precision": "fp64", "solver": head_solver,
-              "method": a.method, "tol": 1e-8, "formats": "csr+ell32", "l2": "inputs larger than L2 (no flush)",
-              "parallelism": f"independent systems x{world}"}
-
-    if a.impl == "reference":
-        if rank != 0:
-            return 0
-        hint_file = ROOT / "profiles" / "iterations.json"
-        hints = json.loads(hint_file.read_text()) if hint_file.exists() else {}
-        hint = hints.get(workload)
-        rkw, label = reference_method(a.method)
-        if hint is None and P.n <= 300_000:  # small enough to count the iterations with one full solve
-            from oracle import oracle as O
-
-            rkw = dict(rkw)
-            if rkw["precond"] == "neumann":
-                rkw["poly_factor"] = 1.0 / float(np.add.reduceat(np.abs(P.vals), P.row_ptr[:-1]).max())
-            hint = O.solve(P.row_ptr, P.cols, P.vals, P.b, tol=1e-8, max_iter=a.max_iter, which="ref",
-                           **rkw).iterations
-        steps = []
-        for i in range(a.warmup + a.steps):
-            v, setup, per_iter, spent = reference_sample(P, a.method, hint)
-            if i >= a.warmup:
-                steps.append(v)
-        value = float(np.median(steps))
-        line = {"metric": "time_to_true_rel_residual_1e-8", "value": value, "unit": "s", "n_gpus": a.gpus,
-                "steps": a.steps, "warmup": a.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-                "impl": "reference", "config": config,
-                "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": "reference",
-                                 "sample": f"Alien CG.h + {label} on 1 host core: set-up + 2 and 8 iterations on "
-                                           f"the full system, per-iteration time scaled to {hint or 'sampled'} "
-                                           f"iterations"},
-                "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return 0
+    config = make_config(P)
 
     import torch
 
@@ -1069,10 +1142,12 @@ def main():
         if O.ref_available():
             v, setup, per_iter, spent = reference_sample(P, a.method, st.iterations)
             _, label = reference_method(a.method)
-            cpu = {"value": round(v, 3), "unit": "s", "cores": 1, "kind": "reference",
+            cpu = {"value": round(v, 3), "unit": "s", "cores": 1, "kind": "reference", **host_info(),
+                   "extrapolated": True,
                    "sample": f"Alien CG.h + {label} (oracle/_ref) on 1 host core: set-up + 2 and 8 "
                              f"iterations of the same system ({spent:.1f} s), scaled to {st.iterations} iterations "
-                             f"(set-up {setup:.2f} s, {per_iter*1e3:.1f} ms/iteration)"}
+                             f"(set-up {setup:.2f} s, {per_iter*1e3:.1f} ms/iteration); complete solves are timed "
+                             f"by --impl reference"}
 
     if rank == 0:
         line = {"metric": "time_to_true_rel_residual_1e-8", "value": round(ms / 1e3, 5), "unit": "s",

@@ -187,7 +187,9 @@ int ab2_scalar_get(ab2_context* ctx, const ab2_scalar* s, double* value);
  * cudaMalloc/cudaFree and the device synchronisation they can cause).
  * x, y: device arrays of n doubles on the current device; result: one device
  * double, written on `stream` (a cudaStream_t, NULL for the default stream);
- * nothing is synchronised.  The block partials live in a fixed 32 KB device
+ * nothing is synchronised.  The scratch array used is that of the device that
+ * is current on the calling thread (cudaSetDevice): make the device that holds
+ * x, y and result current before the call.  The block partials live in a fixed 32 KB device
  * array inside libab2 (one per GPU, held until the process exits), which
  * limits n to 16,777,216; larger n returns AB2_ERR_BAD_ARG.  The first call on
  * each device looks that array up (cudaGetSymbolAddress): make it before any

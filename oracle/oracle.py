@@ -510,3 +510,96 @@ def dist_solve(row_ptr, cols, vals, offsets, b, x0=None, solver="cg", precond="d
                          _dp(hist), cap)
     return OracleSolve(x, r.iterations, bool(r.converged), r.error, BREAKDOWN.get(r.breakdown), r.nrm2_b, r.last_rr,
                        0.0, 0.0, hist[:min(r.history_len, cap)].copy())
+
+
+# ----------------------------------------------------------------------------- inputs without libab2
+INPUTS_SO = HERE / "_build" / "libab2_inputs.so"
+_inp = None
+
+
+class _Problem(C.Structure):
+    # struct ab2_problem (include/ab2_problems.h)
+    _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("row_ptr", _IP), ("cols", _IP), ("vals", _DP), ("x_true", _DP), ("b", _DP), ("log10_k", _DP)]
+
+
+@dataclass
+class InputProblem:
+    """A seeded system as the CPU timing legs see it (same fields as
+    alien_b200.abi.CsrProblem)."""
+    n: int
+    row_ptr: np.ndarray
+    cols: np.ndarray
+    vals: np.ndarray
+    x_true: np.ndarray | None
+    b: np.ndarray
+    log10_k: np.ndarray | None
+    shape: tuple
+
+    @property
+    def nnz(self) -> int:
+        return int(self.row_ptr[-1])
+
+
+def inputs() -> C.CDLL:
+    """libab2's input generators built for the host alone (oracle/Makefile),
+    so that a CPU-only process makes the same system without loading the
+    CUDA library."""
+    global _inp
+    if _inp is None:
+        if not INPUTS_SO.exists():
+            raise ImportError(f"{INPUTS_SO} missing: run make -f oracle/Makefile")
+        L = C.CDLL(str(INPUTS_SO))
+        PP = C.POINTER(C.POINTER(_Problem))
+        L.ab2_problem_poisson.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, PP]
+        L.ab2_problem_diffusion.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint64, PP]
+        L.ab2_problem_convdiff.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_uint64, PP]
+        L.ab2_problem_destroy.argtypes = [C.POINTER(_Problem)]
+        for f in (L.ab2_problem_poisson, L.ab2_problem_diffusion, L.ab2_problem_convdiff, L.ab2_problem_destroy):
+            f.restype = C.c_int
+        _inp = L
+    return _inp
+
+
+def _take_problem(p) -> InputProblem:
+    P = p.contents
+    n, nnz = P.n, P.nnz
+
+    def arr(ptr, count, dt):
+        return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+    out = InputProblem(n, arr(P.row_ptr, n + 1, np.int32), arr(P.cols, nnz, np.int32), arr(P.vals, nnz, np.float64),
+                       arr(P.x_true, n, np.float64) if bool(P.x_true) else None, arr(P.b, n, np.float64),
+                       arr(P.log10_k, n, np.float64) if bool(P.log10_k) else None, (P.nx, P.ny, P.nz))
+    inputs().ab2_problem_destroy(p)
+    return out
+
+
+def problem_poisson(nx, ny=None, nz=None, seed=0) -> InputProblem:
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    p = C.POINTER(_Problem)()
+    rc = inputs().ab2_problem_poisson(nx, ny, nz, seed, C.byref(p))
+    if rc:
+        raise RuntimeError(f"ab2_problem_poisson failed ({rc})")
+    return _take_problem(p)
+
+
+def problem_diffusion(nx, ny=None, nz=None, sigma=1.0, smooth=4.0, seed=0) -> InputProblem:
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    p = C.POINTER(_Problem)()
+    rc = inputs().ab2_problem_diffusion(nx, ny, nz, sigma, smooth, seed, C.byref(p))
+    if rc:
+        raise RuntimeError(f"ab2_problem_diffusion failed ({rc})")
+    return _take_problem(p)
+
+
+def problem_convdiff(nx, ny=None, nz=None, peclet=10.0, modes=8, seed=0) -> InputProblem:
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    p = C.POINTER(_Problem)()
+    rc = inputs().ab2_problem_convdiff(nx, ny, nz, peclet, modes, seed, C.byref(p))
+    if rc:
+        raise RuntimeError(f"ab2_problem_convdiff failed ({rc})")
+    return _take_problem(p)

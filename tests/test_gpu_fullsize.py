@@ -10,6 +10,11 @@ full solve is then checked through properties that do not need the oracle:
 the graph loop and the host-driven loop agree bit for bit, the true residual
 meets the tolerance, and the row-block solver with one rank reproduces the
 single-GPU solve bit for bit.
+
+One test runs the complete solve of Alien's own templates too (CG.h +
+ILU0Preconditioner.h over the SimpleCSR restatement, oracle/_ref, sequential
+dot products; about a minute on one host core) and holds the GPU solve to the
+drop-in's bar: iterations within +-2 and the solution within 1e-10 relative.
 """
 import numpy as np
 import pytest
@@ -115,3 +120,35 @@ def test_full_solve_properties(ctx, big, dev):
     np.testing.assert_array_equal(xd.download(), xg)
     for o in (D, A1, comm):
         o.close()
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+def test_full_solve_vs_reference_templates(ctx, big, dev):
+    """The complete 192^3 CG+ILU0 solve against the complete solve of Alien's
+    own templates in the reference's summation order: iterations within +-2,
+    solution within 1e-10 relative (compared at the smaller iteration count
+    when the counts differ), and both true residuals at the tolerance."""
+    kw = dict(solver="cg", precond="ilu0", tol=1e-8, max_iter=2000)
+    b, x = ctx.vector(big.b), ctx.vector(big.n)
+    S = abi.Solver(ctx, dev, **kw)
+    st = S.solve(b, x)
+    xg = x.download()
+    S.close()
+    r = O.solve(big.row_ptr, big.cols, big.vals, big.b, which="ref", **kw)
+    assert st.succeeded and r.converged
+    assert abs(st.iterations - r.iterations) <= 2, (st.iterations, r.iterations)
+    xs = r.x
+    k = min(st.iterations, r.iterations)
+    if r.iterations > k:
+        xs = O.solve(big.row_ptr, big.cols, big.vals, big.b, which="ref", **dict(kw, max_iter=k)).x
+    elif st.iterations > k:
+        S = abi.Solver(ctx, dev, **dict(kw, max_iter=k))
+        x2 = ctx.vector(big.n)
+        assert S.solve(b, x2).iterations == k
+        xg = x2.download()
+        S.close()
+    rel = np.linalg.norm(xg - xs) / np.linalg.norm(xs)
+    assert rel <= 1e-10, rel
+    for xx in (x.download(), r.x):
+        res = big.b - O.spmv(big.row_ptr, big.cols, big.vals, xx)
+        assert np.linalg.norm(res) / np.linalg.norm(big.b) <= 1.5e-8

@@ -110,8 +110,10 @@ def test_bad_files_rejected(tmp_path, text, rhs, msg):
 
 
 # The reference's own MatrixMarket fixtures, read where they lie in the
-# reference checkout (ALIEN_REF_SRC, as oracle/Makefile; skipped when absent).
-REF_TESTS = Path(os.environ.get("ALIEN_REF_SRC", "/root/reference/src/core")).parent / "movesemantic" / "tests"
+# reference checkout (ALIEN_REF_SRC, as oracle/Makefile: by default a checkout
+# of arcaneframework/alien beside this repository; skipped when absent).
+_REF_SRC = os.environ.get("ALIEN_REF_SRC") or str(Path(__file__).resolve().parents[2] / "reference" / "src" / "core")
+REF_TESTS = Path(_REF_SRC).parent / "movesemantic" / "tests"
 
 
 @pytest.mark.skipif(not (REF_TESTS / "simple.mtx").exists(), reason="reference checkout absent")
