@@ -1156,6 +1156,7 @@ def main():
                 "data": "synthetic (seeded generator, per-rank seed)", "config": config,
                 "iterations": st.iterations, "converged": bool(st.succeeded),
                 "true_rel_residual": st.true_residual, "rel_error_vs_x_true": err,
+                "solution_digest": solution_digest(xs),
                 "setup_ms": round(st.setup_ms, 3), "solve_ms": round(st.solve_ms, 3),
                 "solver_gbs": round(st.iterations * iteration_bytes(a.method, P.n, P.nnz) / (st.solve_ms * 1e-3)
                                     / 1e9, 1),
