@@ -26,13 +26,14 @@ AB2_ERR_TIMEOUT = -5
 AB2_ERR_BAD_ARG = -6
 AB2_ERR_UNSUPPORTED = -7
 
-FMT_CSR, FMT_ELL, FMT_F32 = 1, 2, 4
-SPMV_AUTO, SPMV_CSR_SCALAR, SPMV_CSR_STAGED, SPMV_ELL, SPMV_CSR_VECTOR = 0, 1, 2, 3, 4
+FMT_CSR, FMT_ELL, FMT_F32, FMT_STENCIL = 1, 2, 4, 8
+SPMV_AUTO, SPMV_CSR_SCALAR, SPMV_CSR_STAGED, SPMV_ELL, SPMV_CSR_VECTOR, SPMV_STENCIL = 0, 1, 2, 3, 4, 5
 SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
 PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3, "filu0": 4, "neumann": 5}
 ILU_SCHEDULE = {"auto": 0, "wavefront": 1, "stencil": 2}
 BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho"}
 FCG_FALLBACK = {"sticky": 0, "step": 1}
+MIXED_JACOBI = {"auto": 0, "plain": 1, "scaled": 2}
 COMM_ID_BYTES = 128
 
 
@@ -49,7 +50,8 @@ class ContextInfo(C.Structure):
 
 class MatrixInfo(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz", C.c_longlong), ("ell_stored", C.c_longlong), ("ell_slice", C.c_int),
-                ("formats", C.c_int), ("device_bytes", C.c_longlong)]
+                ("formats", C.c_int), ("device_bytes", C.c_longlong), ("stencil_bands", C.c_int),
+                ("stencil_nx", C.c_int), ("stencil_ny", C.c_int), ("stencil_nz", C.c_int)]
 
 
 class PrecondOptions(C.Structure):
@@ -85,13 +87,13 @@ class MixedOptions(C.Structure):
                 ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int), ("cheb_saad", C.c_int),
                 ("cheb_lanczos", C.c_int), ("ilu_schedule", C.c_int), ("spmv_variant", C.c_int),
                 ("use_graph", C.c_int), ("filu_factor_iter", C.c_int),
-                ("filu_solver_iter", C.c_int), ("filu_tol", C.c_double)]
+                ("filu_solver_iter", C.c_int), ("filu_tol", C.c_double), ("jacobi_form", C.c_int)]
 
 
 class MixedStatus(C.Structure):
     _fields_ = [("succeeded", C.c_int), ("outer_iterations", C.c_int), ("inner_iterations", C.c_int),
                 ("error", C.c_int), ("true_residual", C.c_double), ("setup_ms", C.c_double),
-                ("solve_ms", C.c_double)]
+                ("solve_ms", C.c_double), ("jacobi_scaled", C.c_int)]
 
 
 class BatchOptions(C.Structure):
@@ -836,12 +838,13 @@ class MixedResult:
     true_residual: float
     setup_ms: float
     solve_ms: float
+    jacobi_scaled: bool = False
 
 
 def mixed_options(solver="cg", precond="diag", tol=1e-8, max_outer=20, inner_tol=1e-4, inner_max_iter=1000,
                   poly_factor=0.0, poly_order=3, poly_factor_max_iter=20, cheb_saad=False, cheb_lanczos=False,
                   ilu_schedule="auto", spmv_variant=SPMV_AUTO, use_graph=True, filu_factor_iter=0,
-                  filu_solver_iter=3, filu_tol=0.0) -> MixedOptions:
+                  filu_solver_iter=3, filu_tol=0.0, jacobi_form="auto") -> MixedOptions:
     o = MixedOptions()
     lib().ab2_mixed_options_default(C.byref(o))
     o.solver = SOLVER[solver]
@@ -861,6 +864,7 @@ def mixed_options(solver="cg", precond="diag", tol=1e-8, max_outer=20, inner_tol
     o.filu_factor_iter = filu_factor_iter
     o.filu_solver_iter = filu_solver_iter
     o.filu_tol = filu_tol
+    o.jacobi_form = MIXED_JACOBI[jacobi_form]
     return o
 
 
@@ -879,7 +883,7 @@ class Mixed:
         st = MixedStatus()
         self.ctx.check(lib().ab2_mixed_solve(self.h, b.h, x.h, C.byref(st)), "mixed_solve")
         return MixedResult(bool(st.succeeded), st.outer_iterations, st.inner_iterations, st.error,
-                           st.true_residual, st.setup_ms, st.solve_ms)
+                           st.true_residual, st.setup_ms, st.solve_ms, bool(st.jacobi_scaled))
 
     def history(self) -> np.ndarray:
         n = C.c_int()

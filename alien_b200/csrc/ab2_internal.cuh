@@ -88,6 +88,16 @@ struct ab2_matrix {
   int* d_ell_ci = nullptr;    // -1 marks padding
   double* d_ell_v = nullptr;
   float* d_ell_v32 = nullptr;
+  // 7-point bands (AB2_FMT_STENCIL, kept when the profile is a 3-D 7-point
+  // stencil numbered i + nx (j + ny k)): no column indices, the grid fixes
+  // them.  Band-major, n values per band, 0 where a neighbour is outside the
+  // grid.  7 bands (Lz, Ly, Lx, D, Ux, Uy, Uz), or 4 (D, Ux, Uy, Uz) when every
+  // off-diagonal pair is bit-for-bit symmetric: the lower values are then read
+  // from the neighbouring rows' upper bands.
+  int st_nx = 0, st_ny = 0, st_nz = 0;
+  int st_bands = 0;            // 0 (absent), 4 or 7
+  double* d_st_v = nullptr;
+  float* d_st_v32 = nullptr;   // FP32 copy when AB2_FMT_F32
   // host mirror of the profile for symbolic set-ups (ILU0 wavefronts, batch
   // checks), downloaded on first use by host_profile()
   mutable std::vector<int> h_rp, h_ci;
@@ -165,6 +175,27 @@ inline void ctx_quiesce(ab2_context* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
 }
+
+// Unsigned division by a divisor fixed at set-up, as a multiply-high and a
+// shift (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, the round-up multiplier): with l = ceil(log2 d)
+// and m = floor(2^32 (2^l - d) / d) + 1, n / d = (umulhi(n, m) + n) >> l for
+// every n < 2^31 (the sum then stays below 2^32).
+struct FastDiv {
+  unsigned d = 1, m = 1, l = 0;
+  FastDiv() = default;
+  explicit FastDiv(unsigned div) : d(div) {
+    while ((1ull << l) < (unsigned long long)div) ++l;
+    m = (unsigned)(((1ull << 32) * ((1ull << l) - div)) / div + 1);
+  }
+  __host__ __device__ __forceinline__ unsigned div(unsigned n) const {
+#ifdef __CUDA_ARCH__
+    return (__umulhi(n, m) + n) >> l;
+#else
+    return (unsigned)((((unsigned long long)n * m) >> 32) + n) >> l;
+#endif
+  }
+};
 
 inline int grid_for(long long n, int threads = kThreads, int cap = 148 * 32) {
   long long g = (n + threads - 1) / threads;
@@ -247,6 +278,10 @@ void op_inv_diag(ab2_context* ctx, const ab2_matrix* A, double* inv);
 void op_diagonal(ab2_context* ctx, const ab2_matrix* A, double* d);
 void op_mult_inv_diag(ab2_context* ctx, const ab2_matrix* A, double* y);
 int resolve_variant(const ab2_matrix* A, int variant);
+// The 3-D 7-point geometry of A's profile (rows i + nx (j + ny k) holding
+// exactly their in-grid neighbours in ascending columns): true and nx, ny, nz
+// when it has one (nx, ny, nz >= 2).  Device-side check; synchronises.
+bool stencil_geometry(ab2_context* ctx, const ab2_matrix* A, int* nx, int* ny, int* nz);
 // Fills A->h_rp / A->h_ci from the device once (synchronises the stream).
 void host_profile(const ab2_matrix* A);
 

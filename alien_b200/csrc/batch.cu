@@ -314,8 +314,8 @@ bool launch_batch(ab2_batch* B, V64 a64, V32 a32, int csize, int threads, const 
 bool run_batch(ab2_batch* B, int variant, int csize, int threads, const double* b, double* x, int max_outer,
                int inner_max_iter, int nsys_run) {
   bool ok = false;
-  with_view<double>(B->A, variant, [&](auto v64) {
-    with_view<float>(B->A, variant, [&](auto v32) {
+  with_view<double, false>(B->A, variant, [&](auto v64) {
+    with_view<float, false>(B->A, variant, [&](auto v32) {
       // both views in the same format (decltype of a captured parameter may be a reference)
       using V64 = std::remove_cv_t<std::remove_reference_t<decltype(v64)>>;
       using V32 = std::remove_cv_t<std::remove_reference_t<decltype(v32)>>;

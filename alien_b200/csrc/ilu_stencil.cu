@@ -85,43 +85,6 @@ struct Bands {
   double *Lk, *Lj, *Li, *Ui, *Uj, *Uk, *P, *D;
 };
 
-// Rows must hold exactly the in-grid 7-point neighbours, in ascending columns.
-__global__ void k_stencil_check(int n, Geom g, const int* __restrict__ rp, const int* __restrict__ ci, int* bad) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    const int i = r % g.nx, j = (r / g.nx) % g.ny, k = (int)(r / g.nxny);
-    int e = rp[r];
-    const int end = rp[r + 1];
-    bool ok = true;
-    auto expect = [&](long long c) {
-      ok = ok && e < end && ci[e] == c;
-      ++e;
-    };
-    if (k > 0) expect(r - g.nxny);
-    if (j > 0) expect(r - g.nx);
-    if (i > 0) expect(r - 1);
-    expect(r);
-    if (i < g.nx - 1) expect(r + 1);
-    if (j < g.ny - 1) expect(r + g.nx);
-    if (k < g.nz - 1) expect(r + g.nxny);
-    if (!ok || e != end) atomicOr(bad, 1);
-  }
-}
-
-// geo[0] = min over rows with 7 entries (starts at n); then geo[1..2] = the
-// first two columns of that row.
-__global__ void k_first_full_row(int n, const int* __restrict__ rp, int* geo) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
-    if (rp[r + 1] - rp[r] == 7) atomicMin(geo, r);
-}
-
-__global__ void k_full_row_cols(int n, const int* __restrict__ rp, const int* __restrict__ ci, int* geo) {
-  const int r = geo[0];
-  if (r < n) {
-    geo[1] = ci[rp[r]];
-    geo[2] = ci[rp[r] + 1];
-  }
-}
-
 __global__ void k_stencil_extract(int n, Geom g, const int* __restrict__ rp, const double* __restrict__ v, Bands b) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const int i = r % g.nx, j = (r / g.nx) % g.ny, k = (int)(r / g.nxny);
@@ -691,37 +654,13 @@ int bulk_grid(ab2_context* ctx, long long n) {
 bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool factored) {
   const int n = A->n;
   if (n == 0) return false;
-  // Geometry from the first full row: its columns start r - nx ny, r - nx.
-  int* d_geo = dev_alloc<int>(ctx, 3);
-  int geo[3] = {n, 0, 0};
-  AB2_CUDA(cudaMemcpyAsync(d_geo, geo, sizeof(geo), cudaMemcpyHostToDevice, ctx->stream));
-  k_first_full_row<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, d_geo);
-  check_launch(ctx, "first_full_row");
-  k_full_row_cols<<<1, 1, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, d_geo);
-  check_launch(ctx, "full_row_cols");
-  AB2_CUDA(cudaMemcpyAsync(geo, d_geo, sizeof(geo), cudaMemcpyDeviceToHost, ctx->stream));
-  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
-  dev_free(ctx, d_geo);
-  const int r7 = geo[0];
-  if (r7 >= n) return false;
-  const long long nxny = (long long)r7 - geo[1];
-  const long long nx = (long long)r7 - geo[2];
-  if (nx < 2 || nxny <= nx || nxny % nx != 0 || n % nxny != 0) return false;
-  const long long ny = nxny / nx, nz = n / nxny;
-  if (ny < 2 || nz < 2) return false;
-  d.st_nx = (int)nx;
-  d.st_ny = (int)ny;
-  d.st_nz = (int)nz;
+  // The 7-point geometry: kept by the matrix (AB2_FMT_STENCIL) or checked here.
+  int nx = A->st_nx, ny = A->st_ny, nz = A->st_nz;
+  if (nx == 0 && !stencil_geometry(ctx, A, &nx, &ny, &nz)) return false;
+  d.st_nx = nx;
+  d.st_ny = ny;
+  d.st_nz = nz;
   const Geom g = geom_of(d);
-  int* d_bad = dev_alloc<int>(ctx, 1);
-  AB2_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), ctx->stream));
-  k_stencil_check<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, g, A->d_rp, A->d_ci, d_bad);
-  check_launch(ctx, "stencil_check");
-  int bad = 0;
-  AB2_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
-  dev_free(ctx, d_bad);
-  if (bad) return false;
 
   // Factorisation on natural-order bands.
   d.d_bands = dev_alloc<double>(ctx, (size_t)n * 8);

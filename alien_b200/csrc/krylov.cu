@@ -218,7 +218,8 @@ __global__ void __launch_bounds__(kCtlThreads) k_cg_update(int n, const T* __res
 // 96 n instead of 128 n vector bytes and launches 2 kernels per iteration.
 // The p buffers alternate with the body count (bodies & 1).
 
-// Before the loop: z = D^-1 r (inv = nullptr: z = r), rho1 = r.z, beta = 0.
+// Before the loop: z = D^-1 r (inv = nullptr: z = r, and z is not stored:
+// the other kernels then read r in its place), rho1 = r.z, beta = 0.
 template <class T>
 __global__ void __launch_bounds__(kCtlThreads) k_cgj_start(int n, const T* __restrict__ r, const T* __restrict__ inv,
                                                            T* __restrict__ z, SolveStateT<T>* st, Red<T> red) {
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_start(int n, const T* __res
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const T rv = r[i];
     const T zv = inv ? mul_rn(inv[i], rv) : rv;
-    z[i] = zv;
+    if (inv) z[i] = zv;
     acc[0] = fma_rn(rv, zv, acc[0]);
   }
   if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) {
@@ -258,6 +259,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_spmv(int n, View A, const T
 }
 
 // alpha = rho1/den ; x += alpha p ; r -= alpha q ; z = D^-1 r ; r.r (stop test) and r.z (next rho1).
+// inv = nullptr: z = r, not stored (z may be null).
 template <class T>
 __global__ void __launch_bounds__(kCtlThreads) k_cgj_update(int n, const T* p0, const T* p1, const T* __restrict__ q,
                                                             T* __restrict__ r, T* __restrict__ z,
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_update(int n, const T* p0, 
     }
     acc[0] = fma_rn(rv, rv, acc[0]);
     const T zv = inv ? mul_rn(inv[i], rv) : rv;
-    z[i] = zv;
+    if (inv) z[i] = zv;
     acc[1] = fma_rn(rv, zv, acc[1]);
   }
   if (grid_reduce<2>(acc, red.partials, red.counter, red.result)) {
@@ -488,6 +490,18 @@ void pc_apply_t(ab2_context* ctx, const ab2_precond* pc, const T* x, T* y) {
 
 }  // namespace
 
+template <class T>
+template <class F>
+void Krylov<T>::with_op(F&& f) const {
+  if constexpr (sizeof(T) == sizeof(float)) {
+    if (unit_bands) {
+      f(stencil_view<T, true, true>(A, unit_bands));
+      return;
+    }
+  }
+  with_view<T>(A, variant, f);
+}
+
 // Enqueues one loop iteration.  Returns the number of kernels it launched.
 template <class T>
 int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
@@ -497,12 +511,14 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
   const long long before = ctx->launches;
   SolveStateT<T>* st = d_st;
   if (fused_diag) {
-    T *r = w[0], *z = w[1], *p0 = w[2], *q = w[3], *p1 = w[4];
-    with_view<T>(A, variant, [&](auto view) {
-      k_cgj_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z, p0, p1, q, st, red_of<T>(ctx, 2));
+    // without a Jacobi scaling z is r itself: read r, store no z
+    const T* inv = diag_inv();
+    T *r = w[0], *z = inv ? w[1] : nullptr, *p0 = w[2], *q = w[3], *p1 = w[4];
+    with_op([&](auto view) {
+      k_cgj_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z ? z : r, p0, p1, q, st, red_of<T>(ctx, 2));
     });
     check_launch(ctx, "cgj_spmv");
-    k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p1, q, r, z, diag_inv(), st, red_of<T>(ctx, 3), h,
+    k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p1, q, r, z, inv, st, red_of<T>(ctx, 3), h,
                                                      graph_loop);
     check_launch(ctx, "cgj_update");
   } else if (solver == AB2_SOLVER_CG) {
@@ -512,7 +528,7 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
     check_launch(ctx, "cg_rz");
     k_cg_p<<<ge, kThreads, 0, ctx->stream>>>(n, z, p, st);
     check_launch(ctx, "cg_p");
-    with_view<T>(A, variant, [&](auto view) {
+    with_op([&](auto view) {
       k_cg_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red_of<T>(ctx, 2));
     });
     check_launch(ctx, "cg_spmv");
@@ -523,14 +539,14 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
     k_bicg_p<<<ge, kThreads, 0, ctx->stream>>>(n, r, v, p, st);
     check_launch(ctx, "bicg_p");
     pc_apply_t(ctx, pc, p, phat);
-    with_view<T>(A, variant, [&](auto view) {
+    with_op([&](auto view) {
       k_bicg_v<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, phat, r0, v, st, red_of<T>(ctx, 1));
     });
     check_launch(ctx, "bicg_v");
     k_bicg_s<<<g, kCtlThreads, 0, ctx->stream>>>(n, r, v, s, st, red_of<T>(ctx, 2));
     check_launch(ctx, "bicg_s");
     pc_apply_t(ctx, pc, s, shat);
-    with_view<T>(A, variant, [&](auto view) {
+    with_op([&](auto view) {
       k_bicg_t<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, shat, s, t, st, red_of<T>(ctx, 3));
     });
     check_launch(ctx, "bicg_t");
@@ -610,12 +626,13 @@ void Krylov<T>::solve(const T* b, T* x, T tol, int max_iter) {
   check_launch(ctx, "state_init");
   // r = b - A x (and r0, rho1 for BiCGStab)
   T* r0 = solver == AB2_SOLVER_BICGSTAB ? w[1] : nullptr;
-  with_view<T>(A, variant, [&](auto view) {
+  with_op([&](auto view) {
     k_residual<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, d_st, w[0], r0, red_of<T>(ctx, 0));
   });
   check_launch(ctx, "residual");
   if (fused_diag) {
-    k_cgj_start<<<g, kCtlThreads, 0, ctx->stream>>>(n, w[0], diag_inv(), w[1], d_st, red_of<T>(ctx, 1));
+    const T* inv = diag_inv();
+    k_cgj_start<<<g, kCtlThreads, 0, ctx->stream>>>(n, w[0], inv, inv ? w[1] : nullptr, d_st, red_of<T>(ctx, 1));
     check_launch(ctx, "cgj_start");
   }
   // Null right-hand side: the reference returns before any iteration.

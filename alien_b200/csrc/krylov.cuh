@@ -49,6 +49,10 @@ struct Krylov {
   cudaGraphConditionalHandle handle = 0;
   int body_launches = 0;
   bool fused_diag = false;  // CG with Diag or no preconditioner: the two-kernel body
+  // Operator override (set before init): the symmetric unit-diagonal 7-point
+  // operator kept as three upper bands on A's grid (the mixed solver's
+  // symmetrically scaled Jacobi form), used in place of A's own values.
+  const T* unit_bands = nullptr;
 
   // Allocates the work vectors (max_iter sizes the history) and builds the graph.
   void init(ab2_context* c, const ab2_matrix* a, const ab2_precond* p, int solver_kind, int spmv_variant, int graph_loop,
@@ -61,6 +65,8 @@ struct Krylov {
 
  private:
   int enqueue_body(cudaGraphConditionalHandle h, int graph_loop);
+  template <class F>
+  void with_op(F&& f) const;  // f(view of the operator): unit_bands or A in `variant`
   void build_graph();
   const T* diag_inv() const;  // 1/a_ii of a Diag preconditioner in T, else null
 };

@@ -14,6 +14,16 @@
 // preconditioner is the FP64 set-up rounded (the ILU(0) factor is computed in
 // FP64, bit-identical to the reference's, then rounded).
 //
+// CG + Diag has a second, scaled form (AB2_MIXED_JACOBI_SCALED): Jacobi-PCG
+// on A is plain CG on S A S with S = diag(1/sqrt(a_ii)), so the inner solve
+// runs on that unit-diagonal operator -- three FP32 bands on A's 7-point
+// grid, s_r = 1/sqrt(a_rr) and each upper value (a_rc s_r) s_c rounded once,
+// the lower values read from the neighbours' upper bands -- with no
+// preconditioner vector and no z: r32 = float((r / ||r||) s) on the way in,
+// x += ||r|| (s d) on the way out.  Per inner iteration it moves 3 bands and
+// 10 vectors of 4 bytes (52 bytes per row) against 7 slots of 8 bytes (ELL)
+// or 7 bands of 4 and 12 vectors for the plain FP32 form.
+//
 // Stops without success when max_outer steps are used or a step fails to
 // reduce the true residual (the FP32 inner solve can no longer help).
 #include <cuda_runtime.h>
@@ -46,19 +56,48 @@ __global__ void __launch_bounds__(kThreads) k_refine_residual(int n, View A, con
   grid_reduce<1>(acc, red.partials, red.counter, red.result);
 }
 
-// r32 = float(r / ||r||), ||r||^2 read from the device.
+// r32 = float(r / ||r||), ||r||^2 read from the device; with sc (the scaled
+// Jacobi form) r32 = float((r / ||r||) sc).
 __global__ void k_refine_scale(int n, const double* __restrict__ r, const double* __restrict__ rr,
-                               float* __restrict__ r32) {
+                               const double* __restrict__ sc, float* __restrict__ r32) {
   const double s = 1.0 / sqrt(*rr);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) r32[i] = (float)(r[i] * s);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    r32[i] = sc ? (float)((r[i] * s) * sc[i]) : (float)(r[i] * s);
 }
 
-// x += ||r|| d.
+// x += ||r|| d; with sc, x += ||r|| (sc d).
 __global__ void k_refine_update(int n, const float* __restrict__ d, const double* __restrict__ rr,
-                                double* __restrict__ x) {
+                                const double* __restrict__ sc, double* __restrict__ x) {
   const double s = sqrt(*rr);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    x[i] = fma(s, (double)d[i], x[i]);
+    x[i] = fma(s, sc ? (double)d[i] * sc[i] : (double)d[i], x[i]);
+}
+
+// The scaled Jacobi operator from A's symmetric bands (D, Ux, Uy, Uz):
+// sc_r = 1/sqrt(a_rr); hat_b[r] = float((u_b[r] sc_r) sc_{r+s_b}) for the three
+// upper neighbours inside the grid, 0 outside.  bad |= 1 where a_rr is not
+// positive and finite (the form does not apply).
+__global__ void k_scaled_bands(int n, int nx, int ny, int nz, const double* __restrict__ bands,
+                               double* __restrict__ sc, float* __restrict__ hat, int* bad) {
+  const size_t N = (size_t)n;
+  const long long sz = (long long)nx * ny;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int i = r % nx, j = (r / nx) % ny, k = (int)(r / sz);
+    const double d = bands[r];
+    if (!(d > 0.0) || !isfinite(d)) atomicOr(bad, 1);
+    const double sr = 1.0 / sqrt(d);
+    sc[r] = sr;
+    const bool in[3] = {i < nx - 1, j < ny - 1, k < nz - 1};
+    const long long off[3] = {1, nx, sz};
+    for (int b = 0; b < 3; ++b) {
+      float h = 0.0f;
+      if (in[b]) {
+        const double sn = 1.0 / sqrt(bands[r + off[b]]);
+        h = (float)((bands[(size_t)(b + 1) * N + r] * sr) * sn);
+      }
+      hat[(size_t)b * N + r] = h;
+    }
+  }
 }
 
 }  // namespace
@@ -76,6 +115,10 @@ struct ab2_mixed {
   float* d_r32 = nullptr;  // scaled FP32 right-hand side of the inner solve
   float* d_d32 = nullptr;  // FP32 correction
   double* d_rr = nullptr;  // ||r||^2 of the current step (device)
+  // scaled Jacobi form: sc = 1/sqrt(a_ii) (FP64), the operator's three FP32 upper bands
+  bool scaled = false;
+  double* d_sc = nullptr;
+  float* d_hat = nullptr;
   std::vector<double> history;
   double setup_ms = 0, solve_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -98,6 +141,7 @@ void ab2_mixed_options_default(ab2_mixed_options* o) {
   o->spmv_variant = AB2_SPMV_AUTO;
   o->use_graph = 1;
   o->filu_solver_iter = 3;
+  o->jacobi_form = AB2_MIXED_JACOBI_AUTO;
 }
 
 int ab2_mixed_create(ab2_context* ctx, const ab2_matrix* A, const ab2_mixed_options* o, ab2_mixed** out) {
@@ -105,6 +149,7 @@ int ab2_mixed_create(ab2_context* ctx, const ab2_matrix* A, const ab2_mixed_opti
   if (o->solver != AB2_SOLVER_CG && o->solver != AB2_SOLVER_BICGSTAB) return AB2_ERR_BAD_ARG;
   if (o->max_outer < 0 || o->inner_max_iter < 0 || !(o->tol >= 0) || !(o->inner_tol > 0 && o->inner_tol < 1))
     return AB2_ERR_BAD_ARG;
+  if (o->jacobi_form < AB2_MIXED_JACOBI_AUTO || o->jacobi_form > AB2_MIXED_JACOBI_SCALED) return AB2_ERR_BAD_ARG;
   *out = nullptr;
   if (!A->d_v32) {
     ctx->last_error = "mixed-precision solver needs the matrix's FP32 values (create it with AB2_FMT_F32)";
@@ -119,8 +164,37 @@ int ab2_mixed_create(ab2_context* ctx, const ab2_matrix* A, const ab2_mixed_opti
     AB2_CUDA(cudaEventCreate(&M->ev0));
     AB2_CUDA(cudaEventCreate(&M->ev1));
     AB2_CUDA(cudaEventRecord(M->ev0, ctx->stream));
+    // The scaled Jacobi form where asked for or (AUTO) where the matrix allows it.
+    const bool jacobi = o->solver == AB2_SOLVER_CG && o->precond == AB2_PC_DIAG;
+    const bool bands_ok = A->st_bands == 4 && A->d_st_v != nullptr;
+    if (jacobi && o->jacobi_form == AB2_MIXED_JACOBI_SCALED && !bands_ok)
+      throw Error{AB2_ERR_BAD_ARG, "scaled Jacobi form: needs a bit-symmetric 7-point matrix kept as bands "
+                                   "(AB2_FMT_STENCIL)"};
+    if (jacobi && bands_ok && o->jacobi_form != AB2_MIXED_JACOBI_PLAIN) {
+      const size_t n = (size_t)A->n;
+      M->d_sc = dev_alloc<double>(ctx, n);
+      M->d_hat = dev_alloc<float>(ctx, 3 * n);
+      int* d_bad = dev_alloc<int>(ctx, 1);
+      AB2_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), ctx->stream));
+      k_scaled_bands<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, A->st_nx, A->st_ny, A->st_nz, A->d_st_v,
+                                                                   M->d_sc, M->d_hat, d_bad);
+      check_launch(ctx, "scaled_bands");
+      int bad = 0;
+      AB2_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+      AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+      dev_free(ctx, d_bad);
+      if (bad && o->jacobi_form == AB2_MIXED_JACOBI_SCALED)
+        throw Error{AB2_ERR_BAD_ARG, "scaled Jacobi form: the diagonal must be positive"};
+      M->scaled = !bad;
+      if (!M->scaled) {
+        dev_free(ctx, M->d_sc);
+        dev_free(ctx, M->d_hat);
+        M->d_sc = nullptr;
+        M->d_hat = nullptr;
+      }
+    }
     ab2_precond_options po;
-    po.kind = o->precond;
+    po.kind = M->scaled ? AB2_PC_NONE : o->precond;
     po.poly_factor = o->poly_factor;
     po.poly_order = o->poly_order;
     po.poly_factor_max_iter = o->poly_factor_max_iter;
@@ -134,6 +208,7 @@ int ab2_mixed_create(ab2_context* ctx, const ab2_matrix* A, const ab2_mixed_opti
     if (prc != AB2_OK) throw Error{prc, ctx->last_error};
     M->pc->variant = o->spmv_variant;
     pc_enable_f32(ctx, M->pc);
+    if (M->scaled) M->eng.unit_bands = M->d_hat;
     M->eng.init(ctx, A, M->pc, o->solver, o->spmv_variant, o->use_graph, o->inner_max_iter);
     const size_t n = (size_t)A->n;
     M->d_r = dev_alloc<double>(ctx, n);
@@ -196,7 +271,7 @@ int ab2_mixed_solve(ab2_mixed* M, const ab2_vector* b, ab2_vector* x, ab2_mixed_
           break;
         }
         prev = res;
-        k_refine_scale<<<ge, kThreads, 0, ctx->stream>>>(n, M->d_r, M->d_rr, M->d_r32);
+        k_refine_scale<<<ge, kThreads, 0, ctx->stream>>>(n, M->d_r, M->d_rr, M->d_sc, M->d_r32);
         check_launch(ctx, "refine_scale");
         AB2_CUDA(cudaMemsetAsync(M->d_d32, 0, sizeof(float) * (size_t)n, ctx->stream));
         M->eng.solve(M->d_r32, M->d_d32, (float)o.inner_tol, o.inner_max_iter);
@@ -211,7 +286,7 @@ int ab2_mixed_solve(ab2_mixed* M, const ab2_vector* b, ab2_vector* x, ab2_mixed_
           error = st.error;
           break;
         }
-        k_refine_update<<<ge, kThreads, 0, ctx->stream>>>(n, M->d_d32, M->d_rr, x->d);
+        k_refine_update<<<ge, kThreads, 0, ctx->stream>>>(n, M->d_d32, M->d_rr, M->d_sc, x->d);
         check_launch(ctx, "refine_update");
         ++outer;
       }
@@ -228,6 +303,7 @@ int ab2_mixed_solve(ab2_mixed* M, const ab2_vector* b, ab2_vector* x, ab2_mixed_
     status->true_residual = res;
     status->setup_ms = M->setup_ms;
     status->solve_ms = M->solve_ms;
+    status->jacobi_scaled = M->scaled ? 1 : 0;
   });
 }
 
@@ -249,6 +325,8 @@ int ab2_mixed_destroy(ab2_mixed* M) {
     dev_free(M->ctx, M->d_r32);
     dev_free(M->ctx, M->d_d32);
     dev_free(M->ctx, M->d_rr);
+    dev_free(M->ctx, M->d_sc);
+    dev_free(M->ctx, M->d_hat);
   }
   if (M->ev0) cudaEventDestroy(M->ev0);
   if (M->ev1) cudaEventDestroy(M->ev1);

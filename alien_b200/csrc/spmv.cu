@@ -11,7 +11,10 @@
 //
 // Every variant sums a row's products in column order, rounding each product
 // and each partial sum (mul_add_rn) exactly as the reference loop does, so all
-// variants give bit-identical y.  The
+// variants give bit-identical y (the grouped-lane variant excepted, see
+// ab2.h).  For 3-D 7-point profiles the values may also be kept as bands
+// without column indices (AB2_FMT_STENCIL): 7 bands, or 4 when the matrix is
+// bit-for-bit symmetric, read by StencilView (spmv_view.cuh).  The
 // sliced-ELL layout keeps 32-row slices (not the reference's 1024) and stores
 // slot j of the slice's rows contiguously, so the 32 lanes of a warp read 256
 // contiguous bytes of values and 128 of column indices per slot.  Padding slots
@@ -211,6 +214,82 @@ __global__ void __launch_bounds__(kThreads) k_spmv_ell(int n, const int* __restr
   y[row] = EllView<T>::ell_row_sum(eci + base, ev + base, w, x);
 }
 
+// y = A x through a row view (the 7-point bands).
+template <class View, class T>
+__global__ void __launch_bounds__(kThreads) k_spmv_view(int n, View A, const T* __restrict__ x, T* __restrict__ y) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) y[row] = A.row(row, x);
+}
+
+// ----------------------------------------------------------------- 7-point bands
+// geo[0] = min over rows with 7 entries (starts at n); then geo[1..2] = the
+// first two columns of that row: r - nx ny and r - nx.
+__global__ void k_first_full_row7(int n, const int* __restrict__ rp, int* geo) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    if (rp[r + 1] - rp[r] == 7) atomicMin(geo, r);
+}
+
+__global__ void k_full_row7_cols(int n, const int* __restrict__ rp, const int* __restrict__ ci, int* geo) {
+  const int r = geo[0];
+  if (r < n) {
+    geo[1] = ci[rp[r]];
+    geo[2] = ci[rp[r] + 1];
+  }
+}
+
+// Rows must hold exactly their in-grid 7-point neighbours, in ascending columns.
+__global__ void k_stencil7_check(int n, int nx, int ny, int nz, const int* __restrict__ rp, const int* __restrict__ ci,
+                                 int* bad) {
+  const long long nxny = (long long)nx * ny;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int i = r % nx, j = (r / nx) % ny, k = (int)(r / nxny);
+    int e = rp[r];
+    const int end = rp[r + 1];
+    bool ok = true;
+    auto expect = [&](long long c) {
+      ok = ok && e < end && ci[e] == c;
+      ++e;
+    };
+    if (k > 0) expect(r - nxny);
+    if (j > 0) expect(r - nx);
+    if (i > 0) expect(r - 1);
+    expect(r);
+    if (i < nx - 1) expect(r + 1);
+    if (j < ny - 1) expect(r + nx);
+    if (k < nz - 1) expect(r + nxny);
+    if (!ok || e != end) atomicOr(bad, 1);
+  }
+}
+
+// The 7 bands (Lz, Ly, Lx, D, Ux, Uy, Uz; band-major) from a checked 7-point
+// CSR profile; 0 where the neighbour is outside the grid.
+__global__ void k_stencil7_fill(int n, int nx, int ny, int nz, const int* __restrict__ rp, const double* __restrict__ v,
+                                double* __restrict__ bands) {
+  const long long nxny = (long long)nx * ny;
+  const size_t N = (size_t)n;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int i = r % nx, j = (r / nx) % ny, k = (int)(r / nxny);
+    const bool in[7] = {k > 0, j > 0, i > 0, true, i < nx - 1, j < ny - 1, k < nz - 1};
+    int e = rp[r];
+    for (int b = 0; b < 7; ++b) bands[(size_t)b * N + r] = in[b] ? v[e++] : 0.0;
+  }
+}
+
+// bad |= 1 unless every off-diagonal pair is equal bit for bit: the upper
+// value of row r toward r + s against the lower value of row r + s toward r.
+__global__ void k_stencil7_symmetric(int n, int nx, int ny, int nz, const double* __restrict__ bands, int* bad) {
+  const long long nxny = (long long)nx * ny;
+  const size_t N = (size_t)n;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int i = r % nx, j = (r / nx) % ny, k = (int)(r / nxny);
+    bool ok = true;
+    auto same = [](double a, double b) { return __double_as_longlong(a) == __double_as_longlong(b); };
+    if (i < nx - 1) ok = ok && same(bands[4 * N + r], bands[2 * N + r + 1]);
+    if (j < ny - 1) ok = ok && same(bands[5 * N + r], bands[1 * N + r + nx]);
+    if (k < nz - 1) ok = ok && same(bands[6 * N + r], bands[0 * N + r + nxny]);
+    if (!ok) atomicOr(bad, 1);
+  }
+}
+
 __global__ void k_add_lu(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
                          const int* __restrict__ dcol, double alpha, const double* __restrict__ x, double* __restrict__ y,
                          bool lower) {
@@ -332,8 +411,53 @@ long long read_ll(ab2_context* ctx, const long long* d) {
 }  // namespace
 
 int resolve_variant(const ab2_matrix* A, int variant) {
-  if (variant == AB2_SPMV_AUTO) return (A->formats & AB2_FMT_ELL) ? AB2_SPMV_ELL : AB2_SPMV_CSR_STAGED;
+  if (variant == AB2_SPMV_AUTO)
+    return A->st_bands ? AB2_SPMV_STENCIL : (A->formats & AB2_FMT_ELL) ? AB2_SPMV_ELL : AB2_SPMV_CSR_STAGED;
   return variant;
+}
+
+bool stencil_geometry(ab2_context* ctx, const ab2_matrix* A, int* nx_out, int* ny_out, int* nz_out) {
+  const int n = A->n;
+  if (n == 0) return false;
+  // Geometry from the first full row: its columns start r - nx ny, r - nx.
+  int* d_geo = dev_alloc<int>(ctx, 4);
+  int geo[4] = {n, 0, 0, 0};
+  AB2_CUDA(cudaMemcpyAsync(d_geo, geo, sizeof(geo), cudaMemcpyHostToDevice, ctx->stream));
+  k_first_full_row7<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, d_geo);
+  check_launch(ctx, "first_full_row");
+  k_full_row7_cols<<<1, 1, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, d_geo);
+  check_launch(ctx, "full_row_cols");
+  AB2_CUDA(cudaMemcpyAsync(geo, d_geo, sizeof(geo), cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  const int r7 = geo[0];
+  bool ok = r7 < n;
+  long long nx = 0, ny = 0, nz = 0;
+  if (ok) {
+    const long long nxny = (long long)r7 - geo[1];
+    nx = (long long)r7 - geo[2];
+    ok = nx >= 2 && nxny > nx && nxny % nx == 0 && n % nxny == 0;
+    if (ok) {
+      ny = nxny / nx;
+      nz = n / nxny;
+      ok = ny >= 2 && nz >= 2;
+    }
+  }
+  if (ok) {
+    AB2_CUDA(cudaMemsetAsync(d_geo + 3, 0, sizeof(int), ctx->stream));
+    k_stencil7_check<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, (int)nx, (int)ny, (int)nz, A->d_rp, A->d_ci,
+                                                                d_geo + 3);
+    check_launch(ctx, "stencil_check");
+    int bad = 0;
+    AB2_CUDA(cudaMemcpyAsync(&bad, d_geo + 3, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+    ok = bad == 0;
+  }
+  dev_free(ctx, d_geo);
+  if (!ok) return false;
+  *nx_out = (int)nx;
+  *ny_out = (int)ny;
+  *nz_out = (int)nz;
+  return true;
 }
 
 template <class T>
@@ -357,6 +481,12 @@ void spmv_t(ab2_context* ctx, const ab2_matrix* A, const T* v_csr, const T* v_el
       } else {
         throw Error{AB2_ERR_UNSUPPORTED, "the grouped-lane SpMV runs in FP64 only"};
       }
+      break;
+    case AB2_SPMV_STENCIL:
+      require(A->st_bands != 0, "matrix has no 7-point bands (AB2_FMT_STENCIL on a 7-point profile)");
+      with_view<T>(A, AB2_SPMV_STENCIL, [&](auto view) {
+        k_spmv_view<<<grid_for(n, kThreads, 1 << 30), kThreads, 0, ctx->stream>>>(n, view, x, y);
+      });
       break;
     case AB2_SPMV_ELL:
       require(v_ell != nullptr, "matrix has no sliced-ELL copy in this precision");
@@ -396,9 +526,50 @@ void op_diagonal(ab2_context* ctx, const ab2_matrix* A, double* d) {
   check_launch(ctx, "diagonal");
 }
 
-// Fills the value arrays (CSR, ELL and the FP32 copies) from the device CSR values.
+// The 7-point bands from the device CSR values: 7 bands, or 4 when the
+// values are bit-for-bit symmetric (re-decided on every value update).
+static void refresh_stencil(ab2_context* ctx, ab2_matrix* A) {
+  const int n = A->n;
+  const size_t N = (size_t)n;
+  double* b7 = dev_alloc<double>(ctx, 7 * N);
+  k_stencil7_fill<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->st_nx, A->st_ny, A->st_nz, A->d_rp, A->d_v, b7);
+  check_launch(ctx, "stencil_fill");
+  int* d_bad = dev_alloc<int>(ctx, 1);
+  AB2_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), ctx->stream));
+  k_stencil7_symmetric<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->st_nx, A->st_ny, A->st_nz, b7, d_bad);
+  check_launch(ctx, "stencil_symmetric");
+  int bad = 0;
+  AB2_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  dev_free(ctx, d_bad);
+  const int nb = bad ? 7 : 4;
+  if (nb != A->st_bands) {
+    if (A->d_st_v) A->device_bytes -= (long long)(A->st_bands * N * sizeof(double));
+    if (A->d_st_v32) A->device_bytes -= (long long)(A->st_bands * N * sizeof(float));
+    dev_free(ctx, A->d_st_v);
+    dev_free(ctx, A->d_st_v32);
+    A->d_st_v = nullptr;
+    A->d_st_v32 = nullptr;
+    A->st_bands = 0;
+    A->d_st_v = dev_alloc<double>(ctx, nb * N, &A->device_bytes);
+    if (A->formats & AB2_FMT_F32) A->d_st_v32 = dev_alloc<float>(ctx, nb * N, &A->device_bytes);
+    A->st_bands = nb;
+  }
+  // symmetric: D, Ux, Uy, Uz are the last four of the seven bands
+  AB2_CUDA(cudaMemcpyAsync(A->d_st_v, b7 + (7 - nb) * N, sizeof(double) * nb * N, cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+  dev_free(ctx, b7);
+  if (A->d_st_v32) {
+    k_to_f32<<<grid_for((long long)nb * n), kThreads, 0, ctx->stream>>>((long long)nb * n, A->d_st_v, A->d_st_v32);
+    check_launch(ctx, "stencil_to_f32");
+  }
+}
+
+// Fills the value arrays (CSR, ELL, the 7-point bands and the FP32 copies)
+// from the device CSR values.
 static void refresh_values(ab2_context* ctx, ab2_matrix* A) {
   const int n = A->n;
+  if (A->st_nx > 0) refresh_stencil(ctx, A);
   if (A->formats & AB2_FMT_ELL) {
     k_ell_fill<double><<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, A->d_v, A->d_ell_off, A->d_ell_ci,
                                                                   A->d_ell_v);
@@ -526,6 +697,17 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
       A->d_v32 = dev_alloc<float>(ctx, nnz, &A->device_bytes);
       if (A->formats & AB2_FMT_ELL) A->d_ell_v32 = dev_alloc<float>(ctx, (size_t)A->ell_stored, &A->device_bytes);
     }
+    if (A->formats & AB2_FMT_STENCIL) {
+      // kept only for a 7-point profile; the flag reports what is present
+      int nx = 0, ny = 0, nz = 0;
+      if (stencil_geometry(ctx, A, &nx, &ny, &nz)) {
+        A->st_nx = nx;
+        A->st_ny = ny;
+        A->st_nz = nz;
+      } else {
+        A->formats &= ~AB2_FMT_STENCIL;
+      }
+    }
     refresh_values(ctx, A);
     AB2_CUDA(cudaStreamSynchronize(ctx->stream));
   });
@@ -558,6 +740,8 @@ int ab2_matrix_destroy(ab2_matrix* A) {
   dev_free(A->ctx, A->d_ell_ci);
   dev_free(A->ctx, A->d_ell_v);
   dev_free(A->ctx, A->d_ell_v32);
+  dev_free(A->ctx, A->d_st_v);
+  dev_free(A->ctx, A->d_st_v32);
   if (A->ctx) ctx_release(A->ctx);
   delete A;
   return AB2_OK;
@@ -571,6 +755,10 @@ int ab2_matrix_get_info(const ab2_matrix* A, ab2_matrix_info* info) {
   info->ell_slice = kEllSlice;
   info->formats = A->formats;
   info->device_bytes = A->device_bytes;
+  info->stencil_bands = A->st_bands;
+  info->stencil_nx = A->st_nx;
+  info->stencil_ny = A->st_ny;
+  info->stencil_nz = A->st_nz;
   return AB2_OK;
 }
 

@@ -96,14 +96,83 @@ struct EllView {
   }
 };
 
-// Calls f(view) with the view the variant selects (ELL when present, else CSR).
-template <class T, class F>
+// 7-point bands (ab2_matrix::d_st_v): row r = i + nx (j + ny k) holds its
+// in-grid neighbours in ascending column order -nx ny, -nx, -1, 0, +1, +nx,
+// +nx ny, so the sum runs over the same terms in the same order as the CSR
+// row and rounds identically; neighbours outside the grid are skipped, not
+// added as zeros.  The coordinates come from two invariant divisions.  SYM: 4
+// bands (D, Ux, Uy, Uz) and the lower values read from the neighbouring
+// rows' upper bands (bit-for-bit the same numbers in a symmetric matrix).
+// UNIT (with SYM): a unit diagonal that is not stored, 3 bands (Ux, Uy, Uz);
+// the diagonal term is 1 * x_r, as a stored 1 would give.
+template <class T, bool SYM, bool UNIT = false>
+struct StencilView {
+  static_assert(SYM || !UNIT, "a unit-diagonal operator is kept in its symmetric form");
+  static constexpr int kUx = UNIT ? 0 : 1;  // band index of Ux (then Uy, Uz)
+  const T* __restrict__ v;
+  int n, nx, ny, nz;
+  FastDiv fx, fy;
+  template <class F>
+  __device__ __forceinline__ T row_f(int r, F&& f) const {
+    const unsigned q = fx.div((unsigned)r);
+    const int i = r - (int)q * nx;
+    const int k = (int)fy.div(q);
+    const int j = (int)q - k * ny;
+    const int sx = 1, sy = nx, sz = nx * ny;
+    const bool in[7] = {k > 0, j > 0, i > 0, true, i < nx - 1, j < ny - 1, k < nz - 1};
+    const int off[7] = {-sz, -sy, -sx, 0, sx, sy, sz};
+    const size_t N = (size_t)n;
+    T a[7];
+    if constexpr (SYM) {
+      // lower value of row r toward r - s = upper value of row r - s toward r
+      a[0] = in[0] ? __ldg(v + (kUx + 2) * N + (r - sz)) : T(0);
+      a[1] = in[1] ? __ldg(v + (kUx + 1) * N + (r - sy)) : T(0);
+      a[2] = in[2] ? __ldg(v + kUx * N + (r - sx)) : T(0);
+      a[3] = UNIT ? T(1) : __ldg(v + r);
+      a[4] = in[4] ? __ldg(v + kUx * N + r) : T(0);
+      a[5] = in[5] ? __ldg(v + (kUx + 1) * N + r) : T(0);
+      a[6] = in[6] ? __ldg(v + (kUx + 2) * N + r) : T(0);
+    } else {
+#pragma unroll
+      for (int b = 0; b < 7; ++b) a[b] = in[b] ? __ldcs(v + (size_t)b * N + r) : T(0);
+    }
+    T xv[7];
+#pragma unroll
+    for (int b = 0; b < 7; ++b) xv[b] = in[b] ? f(r + off[b]) : T(0);
+    T acc = 0;
+#pragma unroll
+    for (int b = 0; b < 7; ++b)
+      if (in[b]) acc = mul_add_rn(a[b], xv[b], acc);
+    return acc;
+  }
+  __device__ __forceinline__ T row(int r, const T* __restrict__ x) const {
+    return row_f(r, [x](int c) { return __ldg(x + c); });
+  }
+};
+
+template <class T, bool SYM, bool UNIT = false>
+StencilView<T, SYM, UNIT> stencil_view(const ab2_matrix* A, const T* bands) {
+  return StencilView<T, SYM, UNIT>{bands, A->n, A->st_nx, A->st_ny, A->st_nz, FastDiv((unsigned)A->st_nx),
+                                   FastDiv((unsigned)A->st_ny)};
+}
+
+// Calls f(view) with the view the variant selects: the 7-point bands when
+// chosen and present in T, ELL when chosen and present, else CSR.
+// kStencil = false leaves the band views out (callers whose kernels are never
+// given a 7-point matrix, so that they are not instantiated for it).
+template <class T, bool kStencil = true, class F>
 void with_view(const ab2_matrix* A, int variant, F&& f) {
   const bool f32 = sizeof(T) == 4;
   const int v = resolve_variant(A, variant);
   const T* ev = (const T*)(f32 ? (const void*)A->d_ell_v32 : (const void*)A->d_ell_v);
   const T* cv = (const T*)(f32 ? (const void*)A->d_v32 : (const void*)A->d_v);
-  if (v == AB2_SPMV_ELL && ev) {
+  const T* sv = (const T*)(f32 ? (const void*)A->d_st_v32 : (const void*)A->d_st_v);
+  if (kStencil && v == AB2_SPMV_STENCIL && sv) {
+    if constexpr (kStencil) {
+      if (A->st_bands == 4) f(stencil_view<T, true>(A, sv));
+      else f(stencil_view<T, false>(A, sv));
+    }
+  } else if ((v == AB2_SPMV_ELL || v == AB2_SPMV_STENCIL) && ev) {
     f(EllView<T>{A->d_ell_off, A->d_ell_ci, ev});
   } else {
     require(cv != nullptr, "matrix values missing in the requested precision");

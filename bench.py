@@ -342,7 +342,8 @@ def timed_solve(torch, stream, make, run, reps=3):
 
 MIXED_METHODS = {  # mixed-precision forms of the FP64 methods, same system, same 1e-8 true residual
     "ilu0": dict(precond="ilu0"),
-    "jacobi": dict(precond="diag"),
+    "jacobi": dict(precond="diag"),  # AUTO: the scaled Jacobi form on the 7-point bands
+    "jacobi_plain": dict(precond="diag", jacobi_form="plain"),
     "cheb3_saad_lanczos20": dict(precond="cheb", cheb_saad=True, cheb_lanczos=True, poly_order=3,
                                  poly_factor_max_iter=20),
 }
@@ -382,8 +383,13 @@ def mixed_section(abi, ctx, stream, A, P, b, x, methods, a):
                  "setup_ms": round(st.setup_ms, 3), "solve_ms": round(st.solve_ms, 3),
                  "rel_error_vs_fp64_1e-12": float(np.linalg.norm(xs - x_ref) / np.linalg.norm(x_ref)),
                  "residual_history": [float(h) for h in hist]}
-        if m in methods:
-            entry["speedup_vs_fp64_same_precond"] = round(methods[m]["s"] / t, 3)
+        entry["jacobi_scaled"] = bool(st.jacobi_scaled)
+        if st.jacobi_scaled and st.inner_iterations:
+            # FP32 inner CG on the scaled operator: 3 bands + 10 vectors of 4 bytes per row and iteration
+            entry["inner_bytes_per_iteration"] = 52 * P.n
+        base = m if m in methods else m.split("_")[0]
+        if base in methods:
+            entry["speedup_vs_fp64_same_precond"] = round(methods[base]["s"] / t, 3)
         if "ilu0" in methods:
             entry["speedup_vs_fp64_cg_ilu0"] = round(methods["ilu0"]["s"] / t, 3)
         if fp64_best:
@@ -394,7 +400,7 @@ def mixed_section(abi, ctx, stream, A, P, b, x, methods, a):
     # 128^3 convection-diffusion, nonsymmetric: mixed BiCGStab + ILU0 to 1e-10 vs FP64 BiCGStab + ILU0.
     n3 = 128 if a.n >= 128 else a.n
     Q = abi.convdiff(n3, n3, n3, peclet=10.0, modes=8, seed=0)
-    AQ = ctx.matrix(Q.row_ptr, Q.cols, Q.vals, abi.FMT_CSR | abi.FMT_ELL | abi.FMT_F32)
+    AQ = ctx.matrix(Q.row_ptr, Q.cols, Q.vals, abi.FMT_CSR | abi.FMT_ELL | abi.FMT_F32 | abi.FMT_STENCIL)
     bq, xq = ctx.vector(Q.b), ctx.vector(Q.n)
 
     def run_q(S):
@@ -777,7 +783,8 @@ def spmv_variant_section(abi, ctx, timed, A, P, a):
     entry, row pointers, x and y once), which the ELL variant also moves at
     slice width 7."""
     names = {abi.SPMV_CSR_SCALAR: "csr_scalar", abi.SPMV_CSR_STAGED: "csr_staged",
-             abi.SPMV_CSR_VECTOR: "csr_warp_per_row", abi.SPMV_ELL: "ell32"}
+             abi.SPMV_CSR_VECTOR: "csr_warp_per_row", abi.SPMV_ELL: "ell32", abi.SPMV_STENCIL: "stencil_bands"}
+    pk, _ = peaks()
 
     def table(M, n, nnz, variants):
         x, y = ctx.vector(np.random.default_rng(5).uniform(-1, 1, n)), ctx.vector(n)
@@ -786,10 +793,17 @@ def spmv_variant_section(abi, ctx, timed, A, P, a):
         for v in variants:
             ms = timed(lambda v=v: ctx.mult(M, x, y, v), 30)
             out[names[v]] = {"us": round(ms * 1e3, 1), "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1)}
+            if v == abi.SPMV_STENCIL:
+                own = M.info.stencil_bands * 8 * n + 16 * n  # the bands, x once, y once
+                out[names[v]].update({"own_bytes": own, "own_gbs": round(own / (ms * 1e-3) / 1e9, 1),
+                                      "own_frac": round(own / (ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4),
+                                      "bands": M.info.stencil_bands})
         return out
 
-    res = {"bytes": "12 nnz + 4 (n + 1) + 16 n",
-           "headline": table(A, P.n, P.nnz, list(names))}
+    head = list(names) if A.info.stencil_bands else [v for v in names if v != abi.SPMV_STENCIL]
+    res = {"bytes": "12 nnz + 4 (n + 1) + 16 n (CSR); stencil_bands also by its own bytes: bands x 8 n + 16 n",
+           "headline": table(A, P.n, P.nnz, head)}
+    names.pop(abi.SPMV_STENCIL)
     rp, ci, v = long_row_matrix(a.long_rows, 256)
     L = ctx.matrix(rp, ci, v, abi.FMT_CSR | abi.FMT_ELL)
     res["long_rows"] = {"n": a.long_rows, "nnz": int(rp[-1]), "row_len": "uniform 64..448",
@@ -991,7 +1005,9 @@ def main():
     torch.cuda.set_device(local)
     ctx = abi.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
-    A = ctx.matrix(P.row_ptr, P.cols, P.vals, abi.FMT_CSR | abi.FMT_ELL | abi.FMT_F32)
+    # CSR + BEllPack-32 as the configuration names them, the FP32 copies for the
+    # mixed forms, and the 7-point bands that AUTO then picks for every SpMV
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals, abi.FMT_CSR | abi.FMT_ELL | abi.FMT_F32 | abi.FMT_STENCIL)
     b = ctx.vector(P.b)
     x = ctx.vector(P.n)
 
@@ -1122,7 +1138,7 @@ def main():
         for i in range(2):
             torch.cuda.synchronize()
             t = time.perf_counter()
-            A2 = ctx.matrix(rp, ci, vv, abi.FMT_CSR | abi.FMT_ELL)
+            A2 = ctx.matrix(rp, ci, vv, abi.FMT_CSR | abi.FMT_ELL | abi.FMT_STENCIL)
             b2 = ctx.vector(bh)
             x2 = ctx.vector(P.n)
             S2 = abi.Solver(ctx, A2, **kw)

@@ -51,6 +51,11 @@ extern "C" {
 #define AB2_FMT_CSR 1   /* CSR, int32 columns, as SimpleCSR */
 #define AB2_FMT_ELL 2   /* sliced ELL (BEllPack) with 32-row slices */
 #define AB2_FMT_F32 4   /* additionally keep an FP32 copy of the values */
+#define AB2_FMT_STENCIL 8 /* when the profile is a 3-D 7-point stencil in lexicographic order
+                             (row i + nx (j + ny k) holds exactly its in-grid neighbours), also keep
+                             the values as 7 bands without column indices -- 4 bands when the matrix
+                             is bit-for-bit symmetric; silently absent for other profiles (see
+                             ab2_matrix_info.stencil_bands) */
 
 /* SpMV variants (ab2_mult_variant) */
 #define AB2_SPMV_AUTO 0
@@ -61,6 +66,9 @@ extern "C" {
                                  sums combined by shuffles: for long rows; NOT the reference's row-sequential
                                  summation order (last-bit differences), so only ab2_mult_variant uses it --
                                  solvers and AUTO never do */
+#define AB2_SPMV_STENCIL 5    /* the 7-point bands (AB2_FMT_STENCIL): one thread per row, no column indices,
+                                 the row's terms in ascending column order as the CSR sum; AUTO's choice when
+                                 present (falls back to ELL, then CSR, where the bands are absent) */
 
 /* solvers / preconditioners (same names as the krylov example's options) */
 #define AB2_SOLVER_CG 0
@@ -137,6 +145,8 @@ typedef struct {
   int ell_slice;        /* rows per slice (32) */
   int formats;          /* AB2_FMT_* present */
   long long device_bytes;
+  int stencil_bands;    /* 0 (no 7-point bands), 7, or 4 (bit-symmetric values) */
+  int stencil_nx, stencil_ny, stencil_nz; /* grid of the 7-point profile, 0 when absent */
 } ab2_matrix_info;
 int ab2_matrix_get_info(const ab2_matrix* mat, ab2_matrix_info* info);
 
@@ -317,7 +327,21 @@ typedef struct {
   int filu_factor_iter; /* see ab2_precond_options */
   int filu_solver_iter;
   double filu_tol;
+  int jacobi_form;     /* CG + Diag only: AB2_MIXED_JACOBI_* */
 } ab2_mixed_options;
+
+/* How the mixed solver runs CG + Diag.  PLAIN: the FP32 Jacobi-PCG on A32.
+ * SCALED: the same method in its symmetrically scaled form -- plain CG on
+ * S A S (S = diag(1/sqrt(a_ii)), computed in FP64 then rounded: a unit
+ * diagonal and three FP32 bands), with r32 = float(S r / ||r||) and
+ * x += ||r|| S d; it needs a bit-symmetric 7-point matrix kept as bands
+ * (AB2_FMT_STENCIL, ab2_matrix_info.stencil_bands == 4) with a positive
+ * diagonal, and moves about half the bytes per inner iteration.  AUTO: SCALED
+ * when the matrix allows it, else PLAIN.  ab2_mixed_status.jacobi_scaled
+ * tells which ran. */
+#define AB2_MIXED_JACOBI_AUTO 0
+#define AB2_MIXED_JACOBI_PLAIN 1
+#define AB2_MIXED_JACOBI_SCALED 2
 
 typedef struct {
   int succeeded;          /* final true relative residual < tol */
@@ -329,6 +353,7 @@ typedef struct {
   double true_residual;   /* final ||b - A x|| / ||b||, FP64 */
   double setup_ms;        /* FP64 preconditioner set-up + FP32 copies + graph build */
   double solve_ms;        /* device time of the last solve */
+  int jacobi_scaled;      /* 1 when CG + Diag ran in the scaled form (AB2_MIXED_JACOBI_SCALED) */
 } ab2_mixed_status;
 
 void ab2_mixed_options_default(ab2_mixed_options* opts);

@@ -107,6 +107,7 @@ typedef struct {
   int tree_blocks;
   int filu_factor_iter;
   int filu_solver_iter;
+  int jacobi_scaled;        // CG + Diag in the scaled form (mixed.cu's AB2_MIXED_JACOBI_SCALED)
 } orc_mixed_options;
 
 typedef struct {
@@ -1186,6 +1187,33 @@ int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const 
       break;
     default: return ORC_ERR_BAD_ARG;
   }
+  // The scaled Jacobi form: plain CG on S A S, S = diag(1/sqrt(a_ii)), unit
+  // diagonal, each off-diagonal value (a_rc s_r) s_c rounded once from the
+  // upper triangle's entry (the lower one mirrors it), as mixed.cu builds it.
+  const bool scaled = o->jacobi_scaled && o->solver == ORC_SOLVER_CG && o->precond == ORC_PC_DIAG;
+  std::vector<double> sc;
+  std::vector<float> vhat;
+  CsrT<float> Ahat{n, rp, ci, nullptr};
+  if (scaled) {
+    sc.assign(n, 0.0);
+    for (int r = 0; r < n; ++r)
+      for (int k = rp[r]; k < rp[r + 1]; ++k)
+        if (ci[k] == r) sc[r] = 1.0 / std::sqrt(v[k]);
+    auto entry = [&](int row, int col) {
+      for (int k = rp[row]; k < rp[row + 1]; ++k)
+        if (ci[k] == col) return v[k];
+      return 0.0;
+    };
+    vhat.assign(v32.size(), 0.0f);
+    for (int r = 0; r < n; ++r)
+      for (int k = rp[r]; k < rp[r + 1]; ++k) {
+        const int c = ci[k];
+        vhat[k] = c == r ? 1.0f : c > r ? (float)((v[k] * sc[r]) * sc[c]) : (float)((entry(c, r) * sc[c]) * sc[r]);
+      }
+    Ahat.v = vhat.data();
+    M = &pid;
+  }
+  const CsrT<float>& Ain = scaled ? Ahat : A32;
   std::vector<double> r(n), ax(n);
   std::vector<float> r32(n), d32(n);
   const double bb = vdot(n, b, b);
@@ -1216,13 +1244,13 @@ int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const 
         break;
       }
       prev = resid;
-      const double sc = 1.0 / std::sqrt(rr);
-      for (int i = 0; i < n; ++i) r32[i] = (float)(r[i] * sc);
+      const double scn = 1.0 / std::sqrt(rr);
+      for (int i = 0; i < n; ++i) r32[i] = scaled ? (float)((r[i] * scn) * sc[i]) : (float)(r[i] * scn);
       std::fill(d32.begin(), d32.end(), 0.0f);
       StopTest<float> it(n, r32.data(), (float)o->inner_tol, o->inner_max_iter, nullptr, 0);
       try {
-        if (o->solver == ORC_SOLVER_CG) cg(A32, *M, it, r32.data(), d32.data());
-        else bicgstab(A32, *M, it, r32.data(), d32.data());
+        if (o->solver == ORC_SOLVER_CG) cg(Ain, *M, it, r32.data(), d32.data());
+        else bicgstab(Ain, *M, it, r32.data(), d32.data());
       } catch (const Breakdown&) {
         if (it.iter == 0) {
           inner += it.iter;
@@ -1232,7 +1260,7 @@ int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const 
       }
       inner += it.iter;
       const double s = std::sqrt(rr);
-      for (int i = 0; i < n; ++i) x[i] = std::fma(s, (double)d32[i], x[i]);
+      for (int i = 0; i < n; ++i) x[i] = std::fma(s, scaled ? (double)d32[i] * sc[i] : (double)d32[i], x[i]);
       ++outer;
     }
   }

@@ -51,7 +51,7 @@ class MixedOptions(C.Structure):
                 ("inner_tol", C.c_double), ("inner_max_iter", C.c_int), ("poly_factor", C.c_double),
                 ("poly_order", C.c_int), ("poly_factor_max_iter", C.c_int), ("cheb_saad", C.c_int),
                 ("cheb_lanczos", C.c_int), ("dot_mode", C.c_int), ("tree_blocks", C.c_int),
-                ("filu_factor_iter", C.c_int), ("filu_solver_iter", C.c_int)]
+                ("filu_factor_iter", C.c_int), ("filu_solver_iter", C.c_int), ("jacobi_scaled", C.c_int)]
 
 
 class MixedResult(C.Structure):
@@ -393,14 +393,15 @@ class MixedSolve:
 def mixed_solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8, max_outer=20,
                 inner_tol=1e-4, inner_max_iter=1000, poly_factor=0.0, poly_order=3, poly_factor_max_iter=20,
                 cheb_saad=False, cheb_lanczos=False, dot_mode=DOT_SEQUENTIAL, tree_blocks=1184, filu_factor_iter=0,
-                filu_solver_iter=3) -> MixedSolve:
-    """FP32 inner Krylov in FP64 refinement, as libab2's ab2_mixed_solve."""
+                filu_solver_iter=3, jacobi_scaled=False) -> MixedSolve:
+    """FP32 inner Krylov in FP64 refinement, as libab2's ab2_mixed_solve
+    (jacobi_scaled: CG + Diag in its symmetrically scaled form)."""
     rp, ci, v, bb = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(b, np.float64)
     n = rp.size - 1
     x = np.zeros(n) if x0 is None else _c(x0, np.float64).copy()
     o = MixedOptions(SOLVER[solver], PRECOND[precond], tol, max_outer, inner_tol, inner_max_iter, poly_factor,
                      poly_order, poly_factor_max_iter, int(cheb_saad), int(cheb_lanczos), dot_mode, tree_blocks,
-                     filu_factor_iter, filu_solver_iter)
+                     filu_factor_iter, filu_solver_iter, int(jacobi_scaled))
     r = MixedResult()
     cap = max_outer + 2
     hist = np.zeros(cap)
