@@ -77,11 +77,14 @@ Red<T> red_of(ab2_context* ctx, int slot) {
   return Red<T>{reinterpret_cast<T*>(s.partials), s.counter, reinterpret_cast<T*>(s.result)};
 }
 
-// b.b into st->nrm2_b: the same tree as op_dot.
+// b.b into st->nrm2_b: the same tree as op_dot.  With a weight w (the mixed
+// solver's scaled Jacobi form): sum (b_i w_i) b_i.
 template <class T>
-__global__ void __launch_bounds__(kCtlThreads) k_bb(int n, const T* __restrict__ b, SolveStateT<T>* st, Red<T> red) {
+__global__ void __launch_bounds__(kCtlThreads) k_bb(int n, const T* __restrict__ b, const T* __restrict__ w,
+                                                    SolveStateT<T>* st, Red<T> red) {
   T acc[1] = {T(0)};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] = fma_rn(b[i], b[i], acc[0]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    acc[0] = fma_rn(w ? mul_rn(b[i], w[i]) : b[i], b[i], acc[0]);
   if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) st->nrm2_b = red.result[0];
 }
 
@@ -259,11 +262,13 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_spmv(int n, View A, const T
 }
 
 // alpha = rho1/den ; x += alpha p ; r -= alpha q ; z = D^-1 r ; r.r (stop test) and r.z (next rho1).
-// inv = nullptr: z = r, not stored (z may be null).
+// inv = nullptr: z = r, not stored (z may be null).  w: the stop test sums
+// (r_i w_i) r_i instead (the scaled Jacobi form's unscaled residual norm).
 template <class T>
 __global__ void __launch_bounds__(kCtlThreads) k_cgj_update(int n, const T* p0, const T* p1, const T* __restrict__ q,
                                                             T* __restrict__ r, T* __restrict__ z,
-                                                            const T* __restrict__ inv, SolveStateT<T>* st, Red<T> red,
+                                                            const T* __restrict__ inv, const T* __restrict__ w,
+                                                            SolveStateT<T>* st, Red<T> red,
                                                             cudaGraphConditionalHandle h, int use_graph) {
   if (st->done) {
     if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(h, use_graph, 0);
@@ -282,7 +287,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_update(int n, const T* p0, 
       rv = fma_rn(-alpha, q[i], rv);
       r[i] = rv;
     }
-    acc[0] = fma_rn(rv, rv, acc[0]);
+    acc[0] = fma_rn(w ? mul_rn(rv, w[i]) : rv, rv, acc[0]);
     const T zv = inv ? mul_rn(inv[i], rv) : rv;
     if (inv) z[i] = zv;
     acc[1] = fma_rn(rv, zv, acc[1]);
@@ -518,7 +523,7 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
       k_cgj_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z ? z : r, p0, p1, q, st, red_of<T>(ctx, 2));
     });
     check_launch(ctx, "cgj_spmv");
-    k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p1, q, r, z, inv, st, red_of<T>(ctx, 3), h,
+    k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p1, q, r, z, inv, stop_weight, st, red_of<T>(ctx, 3), h,
                                                      graph_loop);
     check_launch(ctx, "cgj_update");
   } else if (solver == AB2_SOLVER_CG) {
@@ -620,7 +625,7 @@ void Krylov<T>::solve(const T* b, T* x, T tol, int max_iter) {
   const int n = A->n;
   const int g = red_grid(ctx, n);
   // Iteration ctor: b.b and the criterion (Iteration.h:44-68)
-  k_bb<<<g, kCtlThreads, 0, ctx->stream>>>(n, b, d_st, red_of<T>(ctx, 0));
+  k_bb<<<g, kCtlThreads, 0, ctx->stream>>>(n, b, stop_weight, d_st, red_of<T>(ctx, 0));
   check_launch(ctx, "dot");
   k_state_init<<<1, 1, 0, ctx->stream>>>(d_st, tol, max_iter, x, b, d_hist, hist_cap);
   check_launch(ctx, "state_init");

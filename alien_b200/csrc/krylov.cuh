@@ -53,6 +53,10 @@ struct Krylov {
   // operator kept as three upper bands on A's grid (the mixed solver's
   // symmetrically scaled Jacobi form), used in place of A's own values.
   const T* unit_bands = nullptr;
+  // Stop-test weight (CG with no preconditioner only): the stop test and b.b
+  // sum (v_i w_i) v_i -- with w = the diagonal, the norm of the residual
+  // before the symmetric scaling.
+  const T* stop_weight = nullptr;
 
   // Allocates the work vectors (max_iter sizes the history) and builds the graph.
   void init(ab2_context* c, const ab2_matrix* a, const ab2_precond* p, int solver_kind, int spmv_variant, int graph_loop,

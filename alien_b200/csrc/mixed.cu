@@ -20,9 +20,13 @@
 // grid, s_r = 1/sqrt(a_rr) and each upper value (a_rc s_r) s_c rounded once,
 // the lower values read from the neighbours' upper bands -- with no
 // preconditioner vector and no z: r32 = float((r / ||r||) s) on the way in,
-// x += ||r|| (s d) on the way out.  Per inner iteration it moves 3 bands and
-// 10 vectors of 4 bytes (52 bytes per row) against 7 slots of 8 bytes (ELL)
-// or 7 bands of 4 and 12 vectors for the plain FP32 form.
+// x += ||r|| (s d) on the way out.  The inner stop test keeps measuring the
+// unscaled residual: it sums (r_i float(a_ii)) r_i, which is ||r||^2 before the
+// scaling (with the scaled residual's own norm the inner solves would stop
+// elsewhere: on the 192^3 heterogeneous system that took twice the
+// iterations).  Per inner iteration it moves 3 bands and 11 vectors of 4
+// bytes (56 bytes per row) against 4 bands and 12 vectors (64 bytes) for the
+// plain FP32 form on the same bands.
 //
 // Stops without success when max_outer steps are used or a step fails to
 // reduce the true residual (the FP32 inner solve can no longer help).
@@ -75,10 +79,11 @@ __global__ void k_refine_update(int n, const float* __restrict__ d, const double
 
 // The scaled Jacobi operator from A's symmetric bands (D, Ux, Uy, Uz):
 // sc_r = 1/sqrt(a_rr); hat_b[r] = float((u_b[r] sc_r) sc_{r+s_b}) for the three
-// upper neighbours inside the grid, 0 outside.  bad |= 1 where a_rr is not
-// positive and finite (the form does not apply).
+// upper neighbours inside the grid, 0 outside; w32 = float(a_rr), the inner
+// stop test's weight.  bad |= 1 where a_rr is not positive and finite (the
+// form does not apply).
 __global__ void k_scaled_bands(int n, int nx, int ny, int nz, const double* __restrict__ bands,
-                               double* __restrict__ sc, float* __restrict__ hat, int* bad) {
+                               double* __restrict__ sc, float* __restrict__ hat, float* __restrict__ w32, int* bad) {
   const size_t N = (size_t)n;
   const long long sz = (long long)nx * ny;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
@@ -87,6 +92,7 @@ __global__ void k_scaled_bands(int n, int nx, int ny, int nz, const double* __re
     if (!(d > 0.0) || !isfinite(d)) atomicOr(bad, 1);
     const double sr = 1.0 / sqrt(d);
     sc[r] = sr;
+    w32[r] = (float)d;
     const bool in[3] = {i < nx - 1, j < ny - 1, k < nz - 1};
     const long long off[3] = {1, nx, sz};
     for (int b = 0; b < 3; ++b) {
@@ -119,6 +125,7 @@ struct ab2_mixed {
   bool scaled = false;
   double* d_sc = nullptr;
   float* d_hat = nullptr;
+  float* d_w32 = nullptr;  // float(a_ii): the inner stop test measures the unscaled residual
   std::vector<double> history;
   double setup_ms = 0, solve_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -174,10 +181,11 @@ int ab2_mixed_create(ab2_context* ctx, const ab2_matrix* A, const ab2_mixed_opti
       const size_t n = (size_t)A->n;
       M->d_sc = dev_alloc<double>(ctx, n);
       M->d_hat = dev_alloc<float>(ctx, 3 * n);
+      M->d_w32 = dev_alloc<float>(ctx, n);
       int* d_bad = dev_alloc<int>(ctx, 1);
       AB2_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), ctx->stream));
       k_scaled_bands<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, A->st_nx, A->st_ny, A->st_nz, A->d_st_v,
-                                                                   M->d_sc, M->d_hat, d_bad);
+                                                                   M->d_sc, M->d_hat, M->d_w32, d_bad);
       check_launch(ctx, "scaled_bands");
       int bad = 0;
       AB2_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -189,8 +197,10 @@ int ab2_mixed_create(ab2_context* ctx, const ab2_matrix* A, const ab2_mixed_opti
       if (!M->scaled) {
         dev_free(ctx, M->d_sc);
         dev_free(ctx, M->d_hat);
+        dev_free(ctx, M->d_w32);
         M->d_sc = nullptr;
         M->d_hat = nullptr;
+        M->d_w32 = nullptr;
       }
     }
     ab2_precond_options po;
@@ -208,7 +218,10 @@ int ab2_mixed_create(ab2_context* ctx, const ab2_matrix* A, const ab2_mixed_opti
     if (prc != AB2_OK) throw Error{prc, ctx->last_error};
     M->pc->variant = o->spmv_variant;
     pc_enable_f32(ctx, M->pc);
-    if (M->scaled) M->eng.unit_bands = M->d_hat;
+    if (M->scaled) {
+      M->eng.unit_bands = M->d_hat;
+      M->eng.stop_weight = M->d_w32;
+    }
     M->eng.init(ctx, A, M->pc, o->solver, o->spmv_variant, o->use_graph, o->inner_max_iter);
     const size_t n = (size_t)A->n;
     M->d_r = dev_alloc<double>(ctx, n);
@@ -327,6 +340,7 @@ int ab2_mixed_destroy(ab2_mixed* M) {
     dev_free(M->ctx, M->d_rr);
     dev_free(M->ctx, M->d_sc);
     dev_free(M->ctx, M->d_hat);
+    dev_free(M->ctx, M->d_w32);
   }
   if (M->ev0) cudaEventDestroy(M->ev0);
   if (M->ev1) cudaEventDestroy(M->ev1);

@@ -385,8 +385,8 @@ def mixed_section(abi, ctx, stream, A, P, b, x, methods, a):
                  "residual_history": [float(h) for h in hist]}
         entry["jacobi_scaled"] = bool(st.jacobi_scaled)
         if st.jacobi_scaled and st.inner_iterations:
-            # FP32 inner CG on the scaled operator: 3 bands + 10 vectors of 4 bytes per row and iteration
-            entry["inner_bytes_per_iteration"] = 52 * P.n
+            # FP32 inner CG on the scaled operator: 3 bands + 11 vectors of 4 bytes per row and iteration
+            entry["inner_bytes_per_iteration"] = 56 * P.n
         base = m if m in methods else m.split("_")[0]
         if base in methods:
             entry["speedup_vs_fp64_same_precond"] = round(methods[base]["s"] / t, 3)
@@ -941,6 +941,38 @@ def learned_field(abi, ctx, stream, a, P, workload):
     return out
 
 
+def profile_case(a) -> int:
+    """--profile-case: one piece of the workload on the --n system, run twice
+    (the second run is the steady one), for ncu launch lists and captures."""
+    from alien_b200 import abi
+
+    n1 = a.n
+    P = abi.diffusion(n1, n1, n1, sigma=1.0, smooth=4.0, seed=0)
+    ctx = abi.Context(0)
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals, abi.FMT_CSR | abi.FMT_ELL | abi.FMT_F32 | abi.FMT_STENCIL)
+    b, x = ctx.vector(P.b), ctx.vector(P.n)
+    graph = not a.host_loop
+    for _ in range(2):
+        ctx.assign(x, 0.0)
+        if a.profile_case == "spmv_bands":
+            ctx.mult(A, b, x, abi.SPMV_STENCIL)
+            st = None
+        elif a.profile_case.startswith("mixed"):
+            form = "plain" if a.profile_case.endswith("plain") else "auto"
+            M = abi.Mixed(ctx, A, solver="cg", precond="diag", tol=1e-8, max_outer=20, inner_tol=1e-4,
+                          inner_max_iter=5000, use_graph=graph, jacobi_form=form)
+            st = M.solve(b, x)
+            M.close()
+        else:
+            pc = "diag" if a.profile_case == "fp64_jacobi" else "ilu0"
+            S = abi.Solver(ctx, A, solver="cg", precond=pc, tol=1e-8, max_iter=a.max_iter, use_graph=graph)
+            st = S.solve(b, x)
+            S.close()
+        ctx.synchronize()
+    print(f"profile case {a.profile_case} at {n1}^3 done: {st}", flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -965,6 +997,10 @@ def main():
     ap.add_argument("--rowblock", action="store_true",
                     help="strong scaling instead: one system split across the N ranks by z-slabs (NCCL), "
                          "distributed CG")
+    ap.add_argument("--profile-case", choices=["mixed_jacobi", "mixed_jacobi_plain", "fp64_jacobi", "fp64_ilu0",
+                                               "spmv_bands"],
+                    help="run one small piece of the workload and exit (for profilers): the solve or the SpMV, "
+                         "twice, on the --n system, no timing or JSON line")
     ap.add_argument("--ref-budget", type=float, default=150.0,
                     help="--impl reference: seconds of complete solves to fit the timed steps into")
     ap.add_argument("--host-loop", action="store_true",
@@ -992,6 +1028,8 @@ def main():
         P = O.problem_diffusion(n1, n1, n1, sigma=1.0, smooth=4.0, seed=rank)
         return reference_main(a, world, rank, P, make_config(P))
 
+    if a.profile_case:
+        return profile_case(a)
     world, rank, local = dist_init()
     if a.rowblock:
         return rowblock_main(a, world, rank, local)

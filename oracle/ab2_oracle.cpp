@@ -213,15 +213,27 @@ struct StopTest {
   int hist_cap;
   int hist_len = 0;
 
-  StopTest(int n_, const T* b, T tol, int max_it, T* h, int cap) : n(n_), max_iter(max_it), hist(h), hist_cap(cap) {
-    nrm2_b = vdot(n, b, b);
+  // weight (the mixed solver's scaled Jacobi form): the stop test and b.b
+  // become sum (v_i w_i) v_i, the residual's norm before the scaling.
+  const T* weight = nullptr;
+  std::vector<T> vw;
+
+  StopTest(int n_, const T* b, T tol, int max_it, T* h, int cap, const T* w = nullptr)
+      : n(n_), max_iter(max_it), hist(h), hist_cap(cap), weight(w) {
+    nrm2_b = wdot(b);
     criteria = tol * tol * nrm2_b;
     status = (nrm2_b == 0);
+  }
+  T wdot(const T* v) {
+    if (!weight) return vdot(n, v, v);
+    vw.resize((size_t)n);
+    for (int i = 0; i < n; ++i) vw[(size_t)i] = v[i] * weight[i];
+    return vdot(n, vw.data(), v);
   }
   bool null_rhs() const { return nrm2_b == 0; }
   bool stop(const T* r) {
     if (iter >= max_iter) return true;
-    last = vdot(n, r, r);
+    last = wdot(r);
     if (hist && hist_len < hist_cap) hist[hist_len] = last;
     ++hist_len;
     status = last < criteria;
@@ -1189,16 +1201,22 @@ int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const 
   }
   // The scaled Jacobi form: plain CG on S A S, S = diag(1/sqrt(a_ii)), unit
   // diagonal, each off-diagonal value (a_rc s_r) s_c rounded once from the
-  // upper triangle's entry (the lower one mirrors it), as mixed.cu builds it.
+  // upper triangle's entry (the lower one mirrors it), as mixed.cu builds it;
+  // its stop test weighs r^2 by float(a_ii), the unscaled residual's norm.
   const bool scaled = o->jacobi_scaled && o->solver == ORC_SOLVER_CG && o->precond == ORC_PC_DIAG;
   std::vector<double> sc;
   std::vector<float> vhat;
+  std::vector<float> w32;  // the stop test's weight: float(a_ii)
   CsrT<float> Ahat{n, rp, ci, nullptr};
   if (scaled) {
     sc.assign(n, 0.0);
+    w32.assign(n, 0.0f);
     for (int r = 0; r < n; ++r)
       for (int k = rp[r]; k < rp[r + 1]; ++k)
-        if (ci[k] == r) sc[r] = 1.0 / std::sqrt(v[k]);
+        if (ci[k] == r) {
+          sc[r] = 1.0 / std::sqrt(v[k]);
+          w32[r] = (float)v[k];
+        }
     auto entry = [&](int row, int col) {
       for (int k = rp[row]; k < rp[row + 1]; ++k)
         if (ci[k] == col) return v[k];
@@ -1247,7 +1265,8 @@ int orc_mixed_solve(int n, const int* rp, const int* ci, const double* v, const 
       const double scn = 1.0 / std::sqrt(rr);
       for (int i = 0; i < n; ++i) r32[i] = scaled ? (float)((r[i] * scn) * sc[i]) : (float)(r[i] * scn);
       std::fill(d32.begin(), d32.end(), 0.0f);
-      StopTest<float> it(n, r32.data(), (float)o->inner_tol, o->inner_max_iter, nullptr, 0);
+      StopTest<float> it(n, r32.data(), (float)o->inner_tol, o->inner_max_iter, nullptr, 0,
+                         scaled ? w32.data() : nullptr);
       try {
         if (o->solver == ORC_SOLVER_CG) cg(Ain, *M, it, r32.data(), d32.data());
         else bicgstab(Ain, *M, it, r32.data(), d32.data());

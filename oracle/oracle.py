@@ -22,6 +22,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libab2_oracle.so"
+THREADS_SO = HERE / "_build" / "libab2_oracle_threads.so"  # the same restatement on all host threads
 REF_SO = HERE / "_ref" / "libalien_ref.so"
 
 SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
@@ -139,6 +140,20 @@ def orc() -> C.CDLL:
     return _orc
 
 
+_thr = None
+
+
+def threads() -> C.CDLL:
+    """The restatement built with its SpMV and BLAS-1 loops on all host
+    threads (AB2_CPU_THREADS, default all): the all-cores CPU timing
+    baseline -- a restatement, not the reference (its dots sum per-thread
+    partials)."""
+    global _thr
+    if _thr is None:
+        _thr = _load(THREADS_SO, "orc")
+    return _thr
+
+
 def ref_available() -> bool:
     return REF_SO.exists()
 
@@ -190,7 +205,9 @@ def solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8
           poly_order=3, poly_factor_max_iter=10, which="oracle", dot_mode=DOT_SEQUENTIAL,
           tree_blocks=1184, cheb_saad=False, cheb_lanczos=False, filu_factor_iter=0,
           filu_solver_iter=3) -> OracleSolve:
-    """Runs the restatement (which='oracle') or the reference templates (which='ref').
+    """Runs the restatement (which='oracle'), the reference templates
+    (which='ref') or the restatement on all host threads (which='threads',
+    timing only).
     dot_mode=DOT_DEVICE_TREE makes the restatement sum every dot product in
     libab2's reduction tree (tree_blocks = its block cap), for bit-exact checks.
     cheb_saad selects ChebyshevPreconditioner<.., true>; cheb_lanczos (oracle
@@ -203,8 +220,8 @@ def solve(row_ptr, cols, vals, b, x0=None, solver="cg", precond="diag", tol=1e-8
     r = Result()
     cap = 2 * max_iter + 8
     hist = np.zeros(cap)
-    L = orc() if which == "oracle" else ref()
-    fn = L.orc_solve if which == "oracle" else L.ref_solve
+    L = {"oracle": orc, "ref": ref, "threads": threads}[which]()
+    fn = L.ref_solve if which == "ref" else L.orc_solve
     fn(n, _ip(rp), _ip(ci), _dp(v), _dp(bb), _dp(x), C.byref(o), C.byref(r), _dp(hist), cap)
     return OracleSolve(x, r.iterations, bool(r.converged), r.error, BREAKDOWN.get(r.breakdown), r.nrm2_b, r.last_rr,
                        r.cheb_alpha, r.cheb_beta, hist[:min(r.history_len, cap)].copy())

@@ -11,6 +11,9 @@
 #include <cmath>
 #include <cstring>
 #include <vector>
+#ifdef ORC_THREADS
+#include "host_threads.h"
+#endif
 
 namespace ab2_oracle {
 
@@ -37,13 +40,29 @@ inline std::vector<int> diag_offsets(const CsrT<T>& A) {
   return d;
 }
 
+// ORC_THREADS (the all-cores CPU baseline build, oracle/Makefile): the row
+// loop of the SpMV and the BLAS-1 loops run on the host threads of
+// host_threads.h -- each element computed as in the sequential form -- and
+// the dot sums per-thread partials (contiguous blocks, each summed
+// sequentially) in thread order.  A restatement for timing, not the
+// reference: its dot order differs.
+#ifdef ORC_THREADS
+#define ORC_FOR(n, i, body)                                                        \
+  HostPool::get().run((n), [&](int, long long lo_, long long hi_) {                \
+    for (long long i = lo_; i < hi_; ++i) body;                                     \
+  })
+#else
+#define ORC_FOR(n, i, body) \
+  for (long long i = 0; i < (long long)(n); ++i) body
+#endif
+
 template <class T>
 inline void spmv(const CsrT<T>& A, const T* x, T* y) {
-  for (int i = 0; i < A.n; ++i) {
+  ORC_FOR(A.n, i, {
     T acc = 0;
     for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) acc = acc + A.v[k] * x[A.ci[k]];
     y[i] = acc;
-  }
+  });
 }
 
 // BLAS-1 as CBLAS kernels compute it on FMA hardware: axpy is one fma per
@@ -51,17 +70,29 @@ inline void spmv(const CsrT<T>& A, const T* x, T* y) {
 // defined; the GPU sums the same products in a fixed tree).
 template <class T>
 inline T dot(int n, const T* x, const T* y) {
+#ifdef ORC_THREADS
+  std::vector<T> part((size_t)HostPool::get().size(), T(0));
+  HostPool::get().run(n, [&](int t, long long lo, long long hi) {
+    T s = 0;
+    for (long long i = lo; i < hi; ++i) s = std::fma(x[i], y[i], s);
+    part[(size_t)t] = s;
+  });
+  T s = 0;
+  for (const T p : part) s = s + p;
+  return s;
+#else
   T s = 0;
   for (int i = 0; i < n; ++i) s = std::fma(x[i], y[i], s);
   return s;
+#endif
 }
 template <class T>
 inline void axpy(int n, T a, const T* x, T* y) {
-  for (int i = 0; i < n; ++i) y[i] = std::fma(a, x[i], y[i]);
+  ORC_FOR(n, i, y[i] = std::fma(a, x[i], y[i]));
 }
 template <class T>
 inline void scal(int n, T a, T* x) {
-  for (int i = 0; i < n; ++i) x[i] = a * x[i];
+  ORC_FOR(n, i, x[i] = a * x[i]);
 }
 template <class T>
 inline void copy(int n, const T* x, T* y) {
@@ -69,7 +100,7 @@ inline void copy(int n, const T* x, T* y) {
 }
 template <class T>
 inline void pmult(int n, const T* x, const T* y, T* w) {
-  for (int i = 0; i < n; ++i) w[i] = x[i] * y[i];
+  ORC_FOR(n, i, w[i] = x[i] * y[i]);
 }
 
 }  // namespace ab2_oracle

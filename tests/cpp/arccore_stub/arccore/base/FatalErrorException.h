@@ -1,0 +1,3 @@
+// Stand-in for Arccore's <arccore/base/FatalErrorException.h>: see arccore_min.h.
+#pragma once
+#include "../../arccore_min.h"
