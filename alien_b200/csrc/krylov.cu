@@ -519,12 +519,31 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
     // without a Jacobi scaling z is r itself: read r, store no z
     const T* inv = diag_inv();
     T *r = w[0], *z = inv ? w[1] : nullptr, *p0 = w[2], *q = w[3], *p1 = w[4];
-    with_op([&](auto view) {
-      k_cgj_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z ? z : r, p0, p1, q, st, red_of<T>(ctx, 2));
-    });
-    check_launch(ctx, "cgj_spmv");
-    k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p1, q, r, z, inv, stop_weight, st, red_of<T>(ctx, 3), h,
-                                                     graph_loop);
+    if constexpr (sizeof(T) == sizeof(double)) {
+      // FP64: p formed on the fly inside the SpMV (two p buffers)
+      with_op([&](auto view) {
+        k_cgj_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z ? z : r, p0, p1, q, st, red_of<T>(ctx, 2));
+      });
+      check_launch(ctx, "cgj_spmv");
+      k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p1, q, r, z, inv, stop_weight, st, red_of<T>(ctx, 3), h,
+                                                       graph_loop);
+    } else {
+      // FP32: p = z + beta p in place by its own streaming kernel, then the
+      // plain SpMV; the same values, the same p.q tree, one launch more.  In
+      // FP32 the fused SpMV's per-row work (7 neighbours' p formed from z and
+      // the old p: 20 loads) left it latency-bound at 2.8 TB/s; split, the
+      // mixed 192^3 Jacobi solve took 70.5 ms against 83.8 ms.  In FP64 the
+      // split was slower (165.7 against 142.5 ms), so FP64 keeps the fused form.
+      (void)p1;
+      k_cg_p<<<ge, kThreads, 0, ctx->stream>>>(n, z ? z : r, p0, st);
+      check_launch(ctx, "cg_p");
+      with_op([&](auto view) {
+        k_cg_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, p0, q, st, red_of<T>(ctx, 2));
+      });
+      check_launch(ctx, "cg_spmv");
+      k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p0, q, r, z, inv, stop_weight, st, red_of<T>(ctx, 3), h,
+                                                       graph_loop);
+    }
     check_launch(ctx, "cgj_update");
   } else if (solver == AB2_SOLVER_CG) {
     T *r = w[0], *z = w[1], *p = w[2], *q = w[3];
