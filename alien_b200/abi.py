@@ -98,17 +98,19 @@ class MixedStatus(C.Structure):
 
 class BatchOptions(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_outer", C.c_int), ("inner_tol", C.c_double), ("inner_max_iter", C.c_int),
-                ("spmv_variant", C.c_int), ("cluster_size", C.c_int), ("threads", C.c_int), ("tune_iters", C.c_int)]
+                ("spmv_variant", C.c_int), ("cluster_size", C.c_int), ("threads", C.c_int), ("tune_iters", C.c_int),
+                ("ell_slice", C.c_int), ("lanes_per_row", C.c_int)]
 
 
 class BatchTrial(C.Structure):
-    _fields_ = [("spmv_variant", C.c_int), ("cluster_size", C.c_int), ("threads", C.c_int), ("ms", C.c_float)]
+    _fields_ = [("spmv_variant", C.c_int), ("cluster_size", C.c_int), ("threads", C.c_int), ("ms", C.c_float),
+                ("ell_slice", C.c_int), ("lanes_per_row", C.c_int)]
 
 
 class BatchInfo(C.Structure):
     _fields_ = [("nsys", C.c_int), ("rows", C.c_longlong), ("spmv_variant", C.c_int), ("cluster_size", C.c_int),
                 ("threads", C.c_int), ("tuned", C.c_int), ("tune_ms", C.c_double), ("setup_ms", C.c_double),
-                ("trials", C.c_int)]
+                ("trials", C.c_int), ("ell_slice", C.c_int), ("lanes_per_row", C.c_int)]
 
 
 class BatchStatus(C.Structure):
@@ -918,11 +920,12 @@ class BatchResult:
 class Batch:
     """ab2_batch: independent systems (diagonal blocks of A, rows
     sys_offsets[s]..sys_offsets[s+1]-1) solved in one persistent launch; A
-    needs FMT_F32.  cluster_size / threads / spmv_variant = 0 / 0 / SPMV_AUTO
-    let the autotuner pick."""
+    needs FMT_F32.  cluster_size / threads / spmv_variant / ell_slice /
+    lanes_per_row = 0 / 0 / SPMV_AUTO / 0 / 0 let the autotuner pick."""
 
     def __init__(self, ctx: Context, A: Matrix, sys_offsets, tol=1e-8, max_outer=20, inner_tol=1e-4,
-                 inner_max_iter=5000, spmv_variant=SPMV_AUTO, cluster_size=0, threads=0, tune_iters=8):
+                 inner_max_iter=5000, spmv_variant=SPMV_AUTO, cluster_size=0, threads=0, tune_iters=8, ell_slice=0,
+                 lanes_per_row=0):
         self.ctx, self.A = ctx, A
         self.offsets = np.ascontiguousarray(sys_offsets, dtype=np.int32)
         self.nsys = self.offsets.size - 1
@@ -930,6 +933,7 @@ class Batch:
         lib().ab2_batch_options_default(C.byref(o))
         o.tol, o.max_outer, o.inner_tol, o.inner_max_iter = tol, max_outer, inner_tol, inner_max_iter
         o.spmv_variant, o.cluster_size, o.threads, o.tune_iters = spmv_variant, cluster_size, threads, tune_iters
+        o.ell_slice, o.lanes_per_row = ell_slice, lanes_per_row
         h = _P()
         ctx.check(lib().ab2_batch_create(ctx.h, A.h, self.nsys, _ip(self.offsets), C.byref(o), C.byref(h)),
                   "batch_create")
@@ -955,11 +959,12 @@ class Batch:
         self.ctx.check(lib().ab2_batch_get_info(self.h, C.byref(i)), "batch_info")
         return i
 
-    def trials(self) -> list[tuple[int, int, int, float]]:
+    def trials(self) -> list[tuple[int, int, int, float, int, int]]:
+        """(spmv_variant, cluster_size, threads, ms, ell_slice, lanes_per_row) per autotuning trial."""
         n = self.info.trials
         arr = (BatchTrial * max(n, 1))()
         self.ctx.check(lib().ab2_batch_trials(self.h, arr, n), "batch_trials")
-        return [(t.spmv_variant, t.cluster_size, t.threads, t.ms) for t in arr[:n]]
+        return [(t.spmv_variant, t.cluster_size, t.threads, t.ms, t.ell_slice, t.lanes_per_row) for t in arr[:n]]
 
     def close(self):
         if self.h:

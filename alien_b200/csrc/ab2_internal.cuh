@@ -284,5 +284,16 @@ int resolve_variant(const ab2_matrix* A, int variant);
 bool stencil_geometry(ab2_context* ctx, const ab2_matrix* A, int* nx, int* ny, int* nz);
 // Fills A->h_rp / A->h_ci from the device once (synchronises the stream).
 void host_profile(const ab2_matrix* A);
+// A sliced-ELL copy of A's values in FP32 with S-row slices (S = 16, 32 or
+// 64), kept by the caller (the batched solver's autotuner); free_ell frees it.
+struct EllLayout {
+  int S = 0;
+  int* off = nullptr;  // n_slices + 1
+  int* ci = nullptr;   // -1 marks padding
+  float* v = nullptr;
+  long long stored = 0;
+};
+EllLayout build_ell_f32(ab2_context* ctx, const ab2_matrix* A, int S);
+void free_ell(ab2_context* ctx, EllLayout& e);
 
 }  // namespace ab2

@@ -176,10 +176,24 @@ __global__ void k_batch_cg(BatchArgs<V64, V32> a) {
         // q = A32 p ; alpha = rho / (p.q)   (p of every CTA written: the barrier in cluster_sum above
         // or the explicit one at the end of the previous iteration)
         float pq[1] = {0.f};
-        for (int i = lo + threadIdx.x; i < hi; i += T) {
-          const float qv = a.A32.row(i, a.p);
-          a.q[i] = qv;
-          pq[0] = __fmaf_rn(a.p[i], qv, pq[0]);
+        if constexpr (lanes_per_row<V32>::value > 1) {
+          // LPR lanes per row: the group's rows first, then p.q with one row per thread
+          constexpr int LPR = lanes_per_row<V32>::value;
+          const int g = threadIdx.x % LPR;
+          for (int base = lo; base < hi; base += T / LPR) {
+            const int i = base + (int)threadIdx.x / LPR;
+            const bool in = i < hi;
+            const float qv = a.A32.row_group(in ? i : lo, in, g, a.p);
+            if (in && g == 0) a.q[i] = qv;
+          }
+          __syncthreads();
+          for (int i = lo + threadIdx.x; i < hi; i += T) pq[0] = __fmaf_rn(a.p[i], a.q[i], pq[0]);
+        } else {
+          for (int i = lo + threadIdx.x; i < hi; i += T) {
+            const float qv = a.A32.row(i, a.p);
+            a.q[i] = qv;
+            pq[0] = __fmaf_rn(a.p[i], qv, pq[0]);
+          }
         }
         cluster_sum<1>(pq, s_part32, s_warp32, slot, cluster);
         slot ^= 1;
@@ -244,7 +258,9 @@ struct ab2_batch {
   float* d_inv32 = nullptr;
   int *d_conv = nullptr, *d_outer = nullptr, *d_inner = nullptr;
   double* d_res = nullptr;
-  int variant = AB2_SPMV_ELL, csize = 4, threads = 256;
+  int variant = AB2_SPMV_ELL, csize = 4, threads = 256, slice = 32, lpr = 1;
+  // FP32 sliced-ELL copies with 16 and 64 rows per slice (32: the matrix's own)
+  ab2::EllLayout ell16, ell64;
   int tuned = 0;
   double tune_ms = 0, setup_ms = 0, solve_ms = 0;
   std::vector<ab2_batch_trial> trials;
@@ -311,81 +327,100 @@ bool launch_batch(ab2_batch* B, V64 a64, V32 a32, int csize, int threads, const 
   return true;
 }
 
-bool run_batch(ab2_batch* B, int variant, int csize, int threads, const double* b, double* x, int max_outer,
-               int inner_max_iter, int nsys_run) {
-  bool ok = false;
-  with_view<double, false>(B->A, variant, [&](auto v64) {
-    with_view<float, false>(B->A, variant, [&](auto v32) {
-      // both views in the same format (decltype of a captured parameter may be a reference)
-      using V64 = std::remove_cv_t<std::remove_reference_t<decltype(v64)>>;
-      using V32 = std::remove_cv_t<std::remove_reference_t<decltype(v32)>>;
-      if constexpr (std::is_same_v<V64, EllView<double>> == std::is_same_v<V32, EllView<float>>) {
-        ok = launch_batch(B, v64, v32, csize, threads, b, x, max_outer, inner_max_iter, nsys_run);
-      } else {
-        throw Error{AB2_ERR_UNSUPPORTED, "batched solver: FP64 and FP32 values in different formats"};
-      }
-    });
-  });
-  return ok;
+// The FP64 residual reads the CSR values (any format gives the same bits);
+// the FP32 inner SpMV runs in the format under trial.
+bool run_batch(ab2_batch* B, int variant, int slice, int lpr, int csize, int threads, const double* b, double* x,
+               int max_outer, int inner_max_iter, int nsys_run) {
+  const ab2_matrix* A = B->A;
+  const CsrView<double> v64{A->d_rp, A->d_ci, A->d_v};
+  auto go = [&](auto v32) { return launch_batch(B, v64, v32, csize, threads, b, x, max_outer, inner_max_iter, nsys_run); };
+  if (variant == AB2_SPMV_ELL) {
+    if (slice == 16) return go(EllViewS<float, 16>{B->ell16.off, B->ell16.ci, B->ell16.v});
+    if (slice == 64) return go(EllViewS<float, 64>{B->ell64.off, B->ell64.ci, B->ell64.v});
+    require(A->d_ell_v32 != nullptr, "batched solver: the matrix has no FP32 sliced-ELL copy");
+    return go(EllViewS<float, 32>{A->d_ell_off, A->d_ell_ci, A->d_ell_v32});
+  }
+  switch (lpr) {
+    case 2: return go(CsrGroupView<float, 2>{A->d_rp, A->d_ci, A->d_v32});
+    case 4: return go(CsrGroupView<float, 4>{A->d_rp, A->d_ci, A->d_v32});
+    case 8: return go(CsrGroupView<float, 8>{A->d_rp, A->d_ci, A->d_v32});
+    default: return go(CsrView<float>{A->d_rp, A->d_ci, A->d_v32});
+  }
 }
 
-// Times every candidate (SpMV format x CTAs per system x threads per CTA) on
-// the batch itself, from b = 1, and keeps the one with the smallest score =
-// (one refinement step of `tune_iters` FP32 iterations for every system: the
-// throughput of the launch) + (4 x tune_iters iterations of the largest system
-// alone: the latency of the long pole, which bounds a batch whose hardest
-// system needs many iterations).  Shapes that do not fit are skipped.
+// A shape of the inner SpMV: sliced ELL (slice rows) or CSR (lanes per row).
+struct Fmt {
+  int variant, slice, lpr;
+};
+
+// Scores candidates on the batch itself, from b = 1: score = (one refinement
+// step of `tune_iters` FP32 iterations for every system: the throughput of the
+// launch) + (4 x tune_iters iterations of the largest system alone: the
+// latency of the long pole, which bounds a batch whose hardest system needs
+// many iterations).  Two rounds: every SpMV format (ELL with 16 / 32 / 64
+// rows per slice, CSR with 1 / 2 / 4 / 8 lanes per row) at 8 CTAs x 512
+// threads (or the fixed shape), then the best format at every CTA count x
+// width.  Shapes that do not fit are skipped.
 void autotune(ab2_batch* B) {
   ab2_context* ctx = B->ctx;
   const int N = B->A->n;
   double* b = dev_alloc<double>(ctx, (size_t)N);
   double* x = dev_alloc<double>(ctx, (size_t)N);
   op_fill(ctx, N, 1.0, b);
-  std::vector<int> variants;
-  if (B->opts.spmv_variant == AB2_SPMV_AUTO) {
-    if (B->A->d_ell_v32) variants.push_back(AB2_SPMV_ELL);
-    variants.push_back(AB2_SPMV_CSR_SCALAR);
-  } else {
-    variants.push_back(B->opts.spmv_variant);
+  const ab2_batch_options& o = B->opts;
+  std::vector<Fmt> fmts;
+  const bool ell_ok = B->A->d_ell_v32 != nullptr;
+  if (o.spmv_variant == AB2_SPMV_AUTO || o.spmv_variant == AB2_SPMV_ELL) {
+    for (int sl : {16, 32, 64})
+      if ((o.ell_slice == 0 || o.ell_slice == sl) && (sl != 32 || ell_ok)) fmts.push_back(Fmt{AB2_SPMV_ELL, sl, 0});
   }
-  std::vector<int> csizes =
-      B->opts.cluster_size ? std::vector<int>{B->opts.cluster_size} : std::vector<int>{1, 2, 4, 8, 16};
-  std::vector<int> widths = B->opts.threads ? std::vector<int>{B->opts.threads} : std::vector<int>{256, 512};
-  const int iters = B->opts.tune_iters > 0 ? B->opts.tune_iters : 8;
-  float best = 1e30f;
+  if (o.spmv_variant == AB2_SPMV_AUTO || o.spmv_variant == AB2_SPMV_CSR_SCALAR) {
+    for (int l : {1, 2, 4, 8})
+      if (o.lanes_per_row == 0 || o.lanes_per_row == l) fmts.push_back(Fmt{AB2_SPMV_CSR_SCALAR, 0, l});
+  }
+  const std::vector<int> csizes = o.cluster_size ? std::vector<int>{o.cluster_size} : std::vector<int>{1, 2, 4, 8, 16};
+  const std::vector<int> widths = o.threads ? std::vector<int>{o.threads} : std::vector<int>{256, 512};
+  const int iters = o.tune_iters > 0 ? o.tune_iters : 8;
   cudaEvent_t e0, e1;
   AB2_CUDA(cudaEventCreate(&e0));
   AB2_CUDA(cudaEventCreate(&e1));
   AB2_CUDA(cudaEventRecord(B->ev0, ctx->stream));
-  for (int v : variants)
-    for (int c : csizes)
-      for (int t : widths) {
-        float ms = 0;
-        bool fits = true;
-        for (int part = 0; part < 2 && fits; ++part) {
-          const int nrun = part == 0 ? B->nsys : 1;
-          const int it = part == 0 ? iters : 4 * iters;
-          op_fill(ctx, N, 0.0, x);
-          fits = run_batch(B, v, c, t, b, x, 1, it, nrun);  // warm
-          if (!fits) break;
-          op_fill(ctx, N, 0.0, x);
-          AB2_CUDA(cudaEventRecord(e0, ctx->stream));
-          run_batch(B, v, c, t, b, x, 1, it, nrun);
-          AB2_CUDA(cudaEventRecord(e1, ctx->stream));
-          AB2_CUDA(cudaEventSynchronize(e1));
-          float part_ms = 0;
-          AB2_CUDA(cudaEventElapsedTime(&part_ms, e0, e1));
-          ms += part_ms;
-        }
-        if (!fits) continue;
-        B->trials.push_back(ab2_batch_trial{v, c, t, ms});
-        if (ms < best) {
-          best = ms;
-          B->variant = v;
-          B->csize = c;
-          B->threads = t;
-        }
-      }
+  float best = 1e30f;
+  Fmt best_fmt = fmts.empty() ? Fmt{AB2_SPMV_CSR_SCALAR, 0, 1} : fmts[0];
+  auto trial = [&](const Fmt& f, int c, int t) {
+    float ms = 0;
+    for (int part = 0; part < 2; ++part) {
+      const int nrun = part == 0 ? B->nsys : 1;
+      const int it = part == 0 ? iters : 4 * iters;
+      op_fill(ctx, N, 0.0, x);
+      if (!run_batch(B, f.variant, f.slice, f.lpr, c, t, b, x, 1, it, nrun)) return;  // warm; does not fit
+      op_fill(ctx, N, 0.0, x);
+      AB2_CUDA(cudaEventRecord(e0, ctx->stream));
+      run_batch(B, f.variant, f.slice, f.lpr, c, t, b, x, 1, it, nrun);
+      AB2_CUDA(cudaEventRecord(e1, ctx->stream));
+      AB2_CUDA(cudaEventSynchronize(e1));
+      float part_ms = 0;
+      AB2_CUDA(cudaEventElapsedTime(&part_ms, e0, e1));
+      ms += part_ms;
+    }
+    B->trials.push_back(ab2_batch_trial{f.variant, c, t, ms, f.slice, f.lpr});
+    if (ms < best) {
+      best = ms;
+      best_fmt = f;
+      B->variant = f.variant;
+      B->slice = f.slice;
+      B->lpr = f.lpr;
+      B->csize = c;
+      B->threads = t;
+    }
+  };
+  // round 1: the format, at the reference shape
+  const int c0 = o.cluster_size ? o.cluster_size : 8, t0 = o.threads ? o.threads : 512;
+  for (const Fmt& f : fmts) trial(f, c0, t0);
+  // round 2: the shape, for the best format
+  for (int c : csizes)
+    for (int t : widths)
+      if (!(c == c0 && t == t0)) trial(best_fmt, c, t);
   AB2_CUDA(cudaEventRecord(B->ev1, ctx->stream));
   AB2_CUDA(cudaEventSynchronize(B->ev1));
   float ms = 0;
@@ -430,6 +465,10 @@ int ab2_batch_create(ab2_context* ctx, const ab2_matrix* A, int nsys, const int*
         o->cluster_size == 8 || o->cluster_size == 16))
     return AB2_ERR_BAD_ARG;
   if (o->threads != 0 && (o->threads < 64 || o->threads > 1024 || o->threads % 32 != 0)) return AB2_ERR_BAD_ARG;
+  if (!(o->ell_slice == 0 || o->ell_slice == 16 || o->ell_slice == 32 || o->ell_slice == 64)) return AB2_ERR_BAD_ARG;
+  if (!(o->lanes_per_row == 0 || o->lanes_per_row == 1 || o->lanes_per_row == 2 || o->lanes_per_row == 4 ||
+        o->lanes_per_row == 8))
+    return AB2_ERR_BAD_ARG;
   if (!(o->tol >= 0) || !(o->inner_tol > 0 && o->inner_tol < 1) || o->max_outer < 0 || o->inner_max_iter < 1)
     return AB2_ERR_BAD_ARG;
   // systems: increasing offsets from 0 to n, each a diagonal block of A
@@ -484,9 +523,24 @@ int ab2_batch_create(ab2_context* ctx, const ab2_matrix* A, int nsys, const int*
     B->d_res = dev_alloc<double>(ctx, (size_t)nsys);
     B->variant = o->spmv_variant == AB2_SPMV_AUTO ? (A->d_ell_v32 ? AB2_SPMV_ELL : AB2_SPMV_CSR_SCALAR)
                                                   : o->spmv_variant;
+    B->slice = o->ell_slice ? o->ell_slice : 32;
+    B->lpr = o->lanes_per_row ? o->lanes_per_row : 1;
     B->csize = o->cluster_size ? o->cluster_size : 4;
     B->threads = o->threads ? o->threads : 256;
-    if (o->spmv_variant == AB2_SPMV_AUTO || o->cluster_size == 0 || o->threads == 0) autotune(B);
+    const bool tune_fmt = o->spmv_variant == AB2_SPMV_AUTO ||
+                          (o->spmv_variant == AB2_SPMV_ELL && o->ell_slice == 0) ||
+                          (o->spmv_variant == AB2_SPMV_CSR_SCALAR && o->lanes_per_row == 0);
+    // the 16- and 64-row ELL copies, where ELL may be used with those widths
+    if (o->spmv_variant != AB2_SPMV_CSR_SCALAR) {
+      if (o->ell_slice == 16 || (o->ell_slice == 0 && tune_fmt)) B->ell16 = build_ell_f32(ctx, A, 16);
+      if (o->ell_slice == 64 || (o->ell_slice == 0 && tune_fmt)) B->ell64 = build_ell_f32(ctx, A, 64);
+    }
+    if (B->variant == AB2_SPMV_ELL && B->slice == 32 && !A->d_ell_v32 && !tune_fmt)
+      throw Error{AB2_ERR_BAD_ARG, "batched solver: 32-row ELL needs the matrix's ELL copy (AB2_FMT_ELL)"};
+    if (tune_fmt || o->cluster_size == 0 || o->threads == 0) autotune(B);
+    // the ELL copies the chosen format does not use are not kept
+    if (!(B->variant == AB2_SPMV_ELL && B->slice == 16)) free_ell(ctx, B->ell16);
+    if (!(B->variant == AB2_SPMV_ELL && B->slice == 64)) free_ell(ctx, B->ell64);
     AB2_CUDA(cudaEventRecord(s1, ctx->stream));
     AB2_CUDA(cudaEventSynchronize(s1));
     float ms = 0;
@@ -510,8 +564,8 @@ int ab2_batch_solve(ab2_batch* B, const ab2_vector* b, ab2_vector* x, ab2_batch_
   std::memset(status, 0, sizeof(*status));
   return guard(ctx, [&] {
     AB2_CUDA(cudaEventRecord(B->ev0, ctx->stream));
-    if (!run_batch(B, B->variant, B->csize, B->threads, b->d, x->d, B->opts.max_outer, B->opts.inner_max_iter,
-                   B->nsys))
+    if (!run_batch(B, B->variant, B->slice, B->lpr, B->csize, B->threads, b->d, x->d, B->opts.max_outer,
+                   B->opts.inner_max_iter, B->nsys))
       throw Error{AB2_ERR_UNSUPPORTED, "batched solver: no cluster of the configured shape fits on this GPU"};
     AB2_CUDA(cudaEventRecord(B->ev1, ctx->stream));
     AB2_CUDA(cudaEventSynchronize(B->ev1));
@@ -560,6 +614,8 @@ int ab2_batch_get_info(const ab2_batch* B, ab2_batch_info* info) {
   info->tune_ms = B->tune_ms;
   info->setup_ms = B->setup_ms;
   info->trials = (int)B->trials.size();
+  info->ell_slice = B->variant == AB2_SPMV_ELL ? B->slice : 0;
+  info->lanes_per_row = B->variant == AB2_SPMV_CSR_SCALAR ? B->lpr : 0;
   return AB2_OK;
 }
 
@@ -577,6 +633,8 @@ int ab2_batch_destroy(ab2_batch* B) {
     for (void* p : {(void*)B->d_off, (void*)B->d_order, (void*)B->d_ticket, (void*)B->d_r64, (void*)B->d_vec32,
                     (void*)B->d_inv32, (void*)B->d_conv, (void*)B->d_outer, (void*)B->d_inner, (void*)B->d_res})
       dev_free(B->ctx, p);
+    free_ell(B->ctx, B->ell16);
+    free_ell(B->ctx, B->ell64);
   }
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);

@@ -59,16 +59,18 @@ __global__ void k_dcol(int n, const int* __restrict__ rp, const int* __restrict_
   }
 }
 
+// Sliced ELL with S-row slices (S = kEllSlice for the matrix's own copy).
 template <class T>
-__global__ void k_ell_fill(int n, const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
-                           const int* __restrict__ off, int* __restrict__ eci, T* __restrict__ ev) {
+__global__ void k_ell_fill(int n, int S, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const double* __restrict__ v, const int* __restrict__ off, int* __restrict__ eci,
+                           T* __restrict__ ev) {
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-    const int s = row / kEllSlice, lane = row % kEllSlice;
+    const int s = row / S, lane = row % S;
     const int w = off[s + 1] - off[s];
-    const size_t base = (size_t)off[s] * kEllSlice + lane;
+    const size_t base = (size_t)off[s] * S + lane;
     const int a = rp[row], len = rp[row + 1] - a;
     for (int j = 0; j < w; ++j) {
-      const size_t at = base + (size_t)j * kEllSlice;
+      const size_t at = base + (size_t)j * S;
       eci[at] = j < len ? ci[a + j] : -1;
       ev[at] = j < len ? (T)v[a + j] : (T)0;
     }
@@ -76,12 +78,12 @@ __global__ void k_ell_fill(int n, const int* __restrict__ rp, const int* __restr
 }
 
 // Padding rows past n in the last slice.
-__global__ void k_ell_pad_tail(int n, int n_pad, const int* __restrict__ off, int* __restrict__ eci) {
+__global__ void k_ell_pad_tail(int n, int n_pad, int S, const int* __restrict__ off, int* __restrict__ eci) {
   const int row = n + blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= n_pad) return;
-  const int s = row / kEllSlice, lane = row % kEllSlice;
+  const int s = row / S, lane = row % S;
   const int w = off[s + 1] - off[s];
-  for (int j = 0; j < w; ++j) eci[(size_t)off[s] * kEllSlice + lane + (size_t)j * kEllSlice] = -1;
+  for (int j = 0; j < w; ++j) eci[(size_t)off[s] * S + lane + (size_t)j * S] = -1;
 }
 
 __global__ void k_to_f32(long long m, const double* __restrict__ a, float* __restrict__ b) {
@@ -364,10 +366,10 @@ __global__ void k_rowblock_emit(int n, int nc, const int* __restrict__ rp, const
 }
 
 // Longest row of every 32-row slice.
-__global__ void k_slice_width(int n, int ns, const int* __restrict__ rp, long long* __restrict__ w) {
+__global__ void k_slice_width(int n, int ns, int S, const int* __restrict__ rp, long long* __restrict__ w) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) {
     int m = 0;
-    for (int r = s * kEllSlice; r < min(n, (s + 1) * kEllSlice); ++r) m = max(m, rp[r + 1] - rp[r]);
+    for (int r = s * S; r < min(n, (s + 1) * S); ++r) m = max(m, rp[r + 1] - rp[r]);
     w[s] = m;
   }
 }
@@ -571,7 +573,7 @@ static void refresh_values(ab2_context* ctx, ab2_matrix* A) {
   const int n = A->n;
   if (A->st_nx > 0) refresh_stencil(ctx, A);
   if (A->formats & AB2_FMT_ELL) {
-    k_ell_fill<double><<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, A->d_v, A->d_ell_off, A->d_ell_ci,
+    k_ell_fill<double><<<grid_for(n), kThreads, 0, ctx->stream>>>(n, kEllSlice, A->d_rp, A->d_ci, A->d_v, A->d_ell_off, A->d_ell_ci,
                                                                   A->d_ell_v);
     check_launch(ctx, "ell_fill");
   }
@@ -579,7 +581,7 @@ static void refresh_values(ab2_context* ctx, ab2_matrix* A) {
     k_to_f32<<<grid_for(A->nnz), kThreads, 0, ctx->stream>>>(A->nnz, A->d_v, A->d_v32);
     check_launch(ctx, "to_f32");
     if (A->formats & AB2_FMT_ELL) {
-      k_ell_fill<float><<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, A->d_v, A->d_ell_off, A->d_ell_ci,
+      k_ell_fill<float><<<grid_for(n), kThreads, 0, ctx->stream>>>(n, kEllSlice, A->d_rp, A->d_ci, A->d_v, A->d_ell_off, A->d_ell_ci,
                                                                   A->d_ell_v32);
       check_launch(ctx, "ell_fill_f32");
     }
@@ -589,6 +591,47 @@ static void refresh_values(ab2_context* ctx, ab2_matrix* A) {
 }  // namespace ab2
 
 namespace ab2 {
+
+EllLayout build_ell_f32(ab2_context* ctx, const ab2_matrix* A, int S) {
+  require(S == 16 || S == 32 || S == 64, "ELL slice width must be 16, 32 or 64");
+  EllLayout e;
+  e.S = S;
+  const int n = A->n;
+  const int ns = (n + S - 1) / S;
+  long long* d_w = dev_alloc<long long>(ctx, (size_t)ns + 1);
+  long long* d_woff = dev_alloc<long long>(ctx, (size_t)ns + 1);
+  if (ns > 0) {
+    k_slice_width<<<grid_for(ns), kThreads, 0, ctx->stream>>>(n, ns, S, A->d_rp, d_w);
+    check_launch(ctx, "slice_width");
+  }
+  k_scan_excl<<<1, 1024, 0, ctx->stream>>>(ns, d_w, d_woff);
+  check_launch(ctx, "slice_scan");
+  const long long acc = read_ll(ctx, d_woff + ns);
+  require(acc < (1LL << 31) && acc * S < (1LL << 31) * 8, "matrix too large for the sliced-ELL layout");
+  e.stored = acc * S;
+  e.off = dev_alloc<int>(ctx, (size_t)ns + 1);
+  e.ci = dev_alloc<int>(ctx, (size_t)e.stored);
+  e.v = dev_alloc<float>(ctx, (size_t)e.stored);
+  k_narrow<<<grid_for(ns + 1), kThreads, 0, ctx->stream>>>(ns + 1, d_woff, e.off);
+  check_launch(ctx, "slice_offsets");
+  dev_free(ctx, d_w);
+  dev_free(ctx, d_woff);
+  const int n_pad = ns * S;
+  if (n_pad > n) {
+    k_ell_pad_tail<<<1, S, 0, ctx->stream>>>(n, n_pad, S, e.off, e.ci);
+    check_launch(ctx, "ell_pad_tail");
+  }
+  k_ell_fill<float><<<grid_for(n), kThreads, 0, ctx->stream>>>(n, S, A->d_rp, A->d_ci, A->d_v, e.off, e.ci, e.v);
+  check_launch(ctx, "ell_fill_f32");
+  return e;
+}
+
+void free_ell(ab2_context* ctx, EllLayout& e) {
+  dev_free(ctx, e.off);
+  dev_free(ctx, e.ci);
+  dev_free(ctx, e.v);
+  e = EllLayout{};
+}
 
 void host_profile(const ab2_matrix* A) {
   if (A->h_profile) return;
@@ -672,7 +715,7 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
       long long* d_w = dev_alloc<long long>(ctx, (size_t)ns + 1);
       long long* d_woff = dev_alloc<long long>(ctx, (size_t)ns + 1);
       if (ns > 0) {
-        k_slice_width<<<grid_for(ns), kThreads, 0, ctx->stream>>>(n, ns, A->d_rp, d_w);
+        k_slice_width<<<grid_for(ns), kThreads, 0, ctx->stream>>>(n, ns, kEllSlice, A->d_rp, d_w);
         check_launch(ctx, "slice_width");
       }
       k_scan_excl<<<1, 1024, 0, ctx->stream>>>(ns, d_w, d_woff);
@@ -689,7 +732,7 @@ int ab2_matrix_create_csr(ab2_context* ctx, int n, const int* row_ptr, const int
       dev_free(ctx, d_woff);
       const int n_pad = ns * kEllSlice;
       if (n_pad > n) {
-        k_ell_pad_tail<<<1, kEllSlice, 0, ctx->stream>>>(n, n_pad, A->d_ell_off, A->d_ell_ci);
+        k_ell_pad_tail<<<1, kEllSlice, 0, ctx->stream>>>(n, n_pad, kEllSlice, A->d_ell_off, A->d_ell_ci);
         check_launch(ctx, "ell_pad_tail");
       }
     }

@@ -96,6 +96,75 @@ struct EllView {
   }
 };
 
+// Sliced ELL with S-row slices (the batched solver's autotuned layouts,
+// build_ell_f32): the same slot-major layout and column-order sum as EllView.
+template <class T, int S>
+struct EllViewS {
+  const int* __restrict__ off;
+  const int* __restrict__ ci;
+  const T* __restrict__ v;
+  __device__ __forceinline__ T row(int r, const T* __restrict__ x) const {
+    const int s = r / S, lane = r % S;
+    const int o = off[s];
+    const int w = off[s + 1] - o;
+    const size_t base = (size_t)o * S + lane;
+    const int* cp = ci + base;
+    const T* vp = v + base;
+    T acc = 0;
+    for (int j = 0; j < w; j += 8) {
+      int c[8];
+      T a[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const bool in = j + u < w;
+        c[u] = in ? __ldcs(cp + (size_t)(j + u) * S) : -1;
+        a[u] = in ? __ldcs(vp + (size_t)(j + u) * S) : T(0);
+      }
+      T xv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : T(0);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (c[u] >= 0) acc = mul_add_rn(a[u], xv[u], acc);
+    }
+    return acc;
+  }
+};
+
+// CSR with LPR consecutive lanes per row (the batched solver's "rows per
+// warp" = 32 / LPR): lane g of the group sums the row's entries g, g + LPR,
+// ... in order (product and sum rounded apart), then the group adds its
+// partials by an xor butterfly (offsets LPR/2 .. 1), so every lane of the
+// group holds the same total.  Not the row-sequential order: only the
+// batched solver uses it, and its oracle restates this tree.
+template <class T, int LPR>
+struct CsrGroupView {
+  static_assert(LPR == 2 || LPR == 4 || LPR == 8 || LPR == 16 || LPR == 32, "lanes per row: a power of two <= 32");
+  const int* __restrict__ rp;
+  const int* __restrict__ ci;
+  const T* __restrict__ v;
+  // Every lane of the warp must call it (the shuffles); g = lane's index in its group.
+  __device__ __forceinline__ T row_group(int r, bool valid, int g, const T* __restrict__ x) const {
+    T acc = 0;
+    if (valid) {
+      const int e = rp[r + 1];
+      for (int k = rp[r] + g; k < e; k += LPR) acc = mul_add_rn(__ldcs(v + k), __ldg(x + __ldcs(ci + k)), acc);
+    }
+#pragma unroll
+    for (int off = LPR / 2; off > 0; off >>= 1) acc = acc + __shfl_xor_sync(0xffffffffu, acc, off);
+    return acc;
+  }
+};
+
+template <class V>
+struct lanes_per_row {
+  static constexpr int value = 1;
+};
+template <class T, int LPR>
+struct lanes_per_row<CsrGroupView<T, LPR>> {
+  static constexpr int value = LPR;
+};
+
 // 7-point bands (ab2_matrix::d_st_v): row r = i + nx (j + ny k) holds its
 // in-grid neighbours in ascending column order -nx ny, -nx, -1, 0, +1, +nx,
 // +nx ny, so the sum runs over the same terms in the same order as the CSR

@@ -473,6 +473,11 @@ def mixed_section(abi, ctx, stream, A, P, b, x, methods, a):
     return out
 
 
+def fmt_name(variant: int, slice_rows: int, lanes: int) -> str:
+    """The batched solver's inner SpMV format: ell<rows per slice> or csr_l<lanes per row>."""
+    return f"ell{slice_rows}" if variant == 3 else f"csr_l{lanes}" if variant == 1 else str(variant)
+
+
 def batch_section(abi, ctx, stream, a):
     """The batched form: 512 independent SPD systems (2-D 5-point or 3-D
     7-point heterogeneous diffusion, log10 k ~ smoothed N(0,1), per-system
@@ -515,11 +520,11 @@ def batch_section(abi, ctx, stream, a):
            "inner_iterations_total": int(inner.sum()), "inner_iterations_max": int(inner.max()),
            "outer_steps_max": int(outer.max()),
            "rows_per_s": round(Q.n / min(times), 1),
-           "config": {"spmv_variant": {1: "csr_scalar", 3: "ell32"}.get(info.spmv_variant, info.spmv_variant),
+           "config": {"spmv_variant": fmt_name(info.spmv_variant, info.ell_slice, info.lanes_per_row),
                       "cluster_size": info.cluster_size, "threads": info.threads, "autotuned": bool(info.tuned)},
            "autotune_ms": round(info.tune_ms, 2), "setup_ms": round(info.setup_ms, 2),
-           "trials": [{"spmv": {1: "csr_scalar", 3: "ell32"}.get(v, v), "cluster": c, "threads": th, "ms": round(ms, 3)}
-                      for v, c, th, ms in S.trials()],
+           "trials": [{"spmv": fmt_name(v, sl, lpr), "cluster": c, "threads": th, "ms": round(ms, 3)}
+                      for v, c, th, ms, sl, lpr in S.trials()],
            "rel_error_vs_x_true_sample": err, "generate_s": round(gen_s, 2)}
     S.close()
     for o in (bq, xq, A):

@@ -374,9 +374,10 @@ int ab2_mixed_destroy(ab2_mixed* m);
  * values (AB2_FMT_F32).  A grid of thread-block clusters, as many as fit on
  * the GPU at once, takes systems largest first from a ticket; a cluster
  * solves its system to the per-system true relative residual tol, then takes
- * the next.  The SpMV format, the CTAs per system (cluster size) and the
- * threads per CTA are picked by timing every candidate on the batch at
- * creation (the autotuner) unless fixed in the options. */
+ * the next.  The inner SpMV format -- sliced ELL with 16, 32 or 64 rows per
+ * slice, or CSR with 1, 2, 4 or 8 lanes per row -- the CTAs per system
+ * (cluster size) and the threads per CTA are picked by timing candidates on
+ * the batch at creation (the autotuner) unless fixed in the options. */
 typedef struct ab2_batch ab2_batch;
 
 typedef struct {
@@ -388,12 +389,16 @@ typedef struct {
   int cluster_size;    /* CTAs per system: 0 (autotune), 1, 2, 4, 8 or 16 (16: where the GPU places it) */
   int threads;         /* threads per CTA: 0 (autotune) or 64..1024, a multiple of 32 */
   int tune_iters;      /* FP32 iterations per system in each autotuning trial (0: 8) */
+  int ell_slice;       /* AB2_SPMV_ELL: rows per slice, 0 (autotune), 16, 32 or 64 */
+  int lanes_per_row;   /* AB2_SPMV_CSR_SCALAR: lanes per row (rows per warp = 32 / it), 0 (autotune), 1, 2,
+                          4 or 8; more than one sums a row in an xor-butterfly tree of per-lane partials */
 } ab2_batch_options;
 
 typedef struct {
   int spmv_variant, cluster_size, threads;
   float ms;            /* one trial's score: tune_iters FP32 iterations of every system plus
                           4 x tune_iters of the largest system alone (throughput + long pole) */
+  int ell_slice, lanes_per_row;  /* the format's shape (0 where it does not apply) */
 } ab2_batch_trial;
 
 typedef struct {
@@ -404,6 +409,7 @@ typedef struct {
   double tune_ms;       /* time spent autotuning */
   double setup_ms;      /* creation, autotuning included */
   int trials;           /* number of autotuning trials (ab2_batch_trials) */
+  int ell_slice, lanes_per_row;  /* the format's shape in use (0 where it does not apply) */
 } ab2_batch_info;
 
 typedef struct {

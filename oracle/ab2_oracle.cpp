@@ -1341,8 +1341,10 @@ extern "C" {
 
 int orc_batch_solve(int n, const int* rp, const int* ci, const double* v, int nsys, const int* off, const double* b,
                     double* x, double tol, int max_outer, double inner_tol, int inner_max_iter, int csize, int threads,
-                    int* conv_out, int* outer_out, int* inner_out, double* res_out) {
+                    int lanes_per_row, int* conv_out, int* outer_out, int* inner_out, double* res_out) {
   if (n < 0 || nsys < 0 || csize < 1 || threads < 32) return ORC_ERR_BAD_ARG;
+  const int lpr = lanes_per_row > 1 ? lanes_per_row : 1;
+  if (lpr > 32 || (lpr & (lpr - 1)) != 0) return ORC_ERR_BAD_ARG;
   const Csr A{n, rp, ci, v};
   std::vector<float> v32(v, v + (n > 0 ? rp[n] : 0));
   std::vector<int> d = diag_offsets(A);
@@ -1355,10 +1357,26 @@ int orc_batch_solve(int n, const int* rp, const int* ci, const double* v, int ns
     for (int k = rp[i]; k < rp[i + 1]; ++k) acc = acc + v[k] * x[ci[k]];
     return acc;
   };
+  // FP32 row sum: in column order, or (lpr > 1, batch.cu's CsrGroupView)
+  // lane g of lpr summing entries g, g + lpr, ... in order, then the xor
+  // butterfly over the lanes (offsets lpr/2 .. 1); lane 0's value.
   auto row32 = [&](int i, const float* y) {
-    float acc = 0.f;
-    for (int k = rp[i]; k < rp[i + 1]; ++k) acc = acc + v32[k] * y[ci[k]];
-    return acc;
+    if (lpr == 1) {
+      float acc = 0.f;
+      for (int k = rp[i]; k < rp[i + 1]; ++k) acc = acc + v32[k] * y[ci[k]];
+      return acc;
+    }
+    float part[32], nxt[32];
+    for (int g = 0; g < lpr; ++g) {
+      float acc = 0.f;
+      for (int k = rp[i] + g; k < rp[i + 1]; k += lpr) acc = acc + v32[k] * y[ci[k]];
+      part[g] = acc;
+    }
+    for (int o = lpr / 2; o > 0; o >>= 1) {
+      for (int g = 0; g < lpr; ++g) nxt[g] = part[g] + part[g ^ o];
+      for (int g = 0; g < lpr; ++g) part[g] = nxt[g];
+    }
+    return part[0];
   };
   const float itol = (float)inner_tol;
   for (int s = 0; s < nsys; ++s) {

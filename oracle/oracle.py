@@ -126,7 +126,7 @@ def orc() -> C.CDLL:
         L.orc_ilu0_apply32.argtypes = [C.c_int, _IP, _IP, _DP, _FP, _FP]
         L.orc_cheb_apply32.argtypes = [C.c_int, _IP, _IP, _DP, _FP, C.c_double, C.c_int, C.c_int, _FP, _FP]
         L.orc_batch_solve.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, _IP, _DP, _DP, C.c_double, C.c_int,
-                                      C.c_double, C.c_int, C.c_int, C.c_int, _IP, _IP, _IP, _DP]
+                                      C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, _IP, _IP, _IP, _DP]
         L.orc_mixed_solve.argtypes = [C.c_int, _IP, _IP, _DP, _DP, _DP, C.POINTER(MixedOptions),
                                       C.POINTER(MixedResult), _DP, C.c_int]
         L.orc_dist_layout.argtypes = [C.c_int, _IP, _IP, _DP, C.c_int, _IP, C.c_int, _IP, _IP, _IP, _DP, _IP, _IP, _IP]
@@ -437,9 +437,10 @@ class BatchSolve:
 
 
 def batch_solve(row_ptr, cols, vals, sys_offsets, b, x0=None, tol=1e-8, max_outer=20, inner_tol=1e-4,
-                inner_max_iter=5000, cluster_size=4, threads=256) -> BatchSolve:
-    """libab2's batched solver restated for a given cluster size and CTA width
-    (each fixes the reduction trees, hence the rounding)."""
+                inner_max_iter=5000, cluster_size=4, threads=256, lanes_per_row=1) -> BatchSolve:
+    """libab2's batched solver restated for a given cluster size, CTA width
+    and (CSR) lanes per row: each fixes a reduction tree, hence the rounding.
+    The ELL slice width changes nothing (the row sum keeps column order)."""
     rp, ci, v, bb = _c(row_ptr, np.int32), _c(cols, np.int32), _c(vals, np.float64), _c(b, np.float64)
     off = _c(sys_offsets, np.int32)
     n, ns = rp.size - 1, off.size - 1
@@ -447,7 +448,8 @@ def batch_solve(row_ptr, cols, vals, sys_offsets, b, x0=None, tol=1e-8, max_oute
     conv, outer, inner = (np.zeros(ns, dtype=np.int32) for _ in range(3))
     res = np.zeros(ns)
     orc().orc_batch_solve(n, _ip(rp), _ip(ci), _dp(v), ns, _ip(off), _dp(bb), _dp(x), tol, max_outer, inner_tol,
-                          inner_max_iter, cluster_size, threads, _ip(conv), _ip(outer), _ip(inner), _dp(res))
+                          inner_max_iter, cluster_size, threads, lanes_per_row, _ip(conv), _ip(outer), _ip(inner),
+                          _dp(res))
     return BatchSolve(x, conv.astype(bool), outer, inner, res)
 
 

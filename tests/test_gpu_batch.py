@@ -32,15 +32,26 @@ def run(ctx, B, **kw):
     return S, st, x.download()
 
 
-@pytest.mark.parametrize("variant,cluster,threads", [(abi.SPMV_ELL, 4, 256), (abi.SPMV_ELL, 1, 128),
-                                                     (abi.SPMV_ELL, 8, 512), (abi.SPMV_CSR_SCALAR, 2, 256),
-                                                     (abi.SPMV_CSR_SCALAR, 8, 1024)])
-def test_batch_bit_exact(ctx, batch, variant, cluster, threads):
-    S, st, x = run(ctx, batch, tol=1e-8, spmv_variant=variant, cluster_size=cluster, threads=threads)
-    assert not S.info.tuned and (S.info.cluster_size, S.info.threads) == (cluster, threads)
+@pytest.mark.parametrize("variant,cluster,threads,shape", [(abi.SPMV_ELL, 4, 256, 32), (abi.SPMV_ELL, 1, 128, 32),
+                                                           (abi.SPMV_ELL, 8, 512, 32), (abi.SPMV_ELL, 4, 256, 16),
+                                                           (abi.SPMV_ELL, 2, 512, 64),
+                                                           (abi.SPMV_CSR_SCALAR, 2, 256, 1),
+                                                           (abi.SPMV_CSR_SCALAR, 8, 1024, 1),
+                                                           (abi.SPMV_CSR_SCALAR, 4, 256, 2),
+                                                           (abi.SPMV_CSR_SCALAR, 2, 512, 4),
+                                                           (abi.SPMV_CSR_SCALAR, 8, 256, 8)])
+def test_batch_bit_exact(ctx, batch, variant, cluster, threads, shape):
+    """shape: rows per ELL slice, or CSR lanes per row (the latter sums a row
+    in a lane tree: the oracle restates it)."""
+    ell = variant == abi.SPMV_ELL
+    S, st, x = run(ctx, batch, tol=1e-8, spmv_variant=variant, cluster_size=cluster, threads=threads,
+                   ell_slice=shape if ell else 0, lanes_per_row=0 if ell else shape)
+    info = S.info
+    assert not info.tuned and (info.cluster_size, info.threads) == (cluster, threads)
+    assert (info.ell_slice, info.lanes_per_row) == ((shape, 0) if ell else (0, shape))
     P = batch.problem
     o = O.batch_solve(P.row_ptr, P.cols, P.vals, batch.sys_offsets, P.b, tol=1e-8, cluster_size=cluster,
-                      threads=threads)
+                      threads=threads, lanes_per_row=1 if ell else shape)
     conv, outer, inner, res = S.results()
     np.testing.assert_array_equal(conv, o.converged)
     np.testing.assert_array_equal(outer, o.outer)
@@ -52,16 +63,24 @@ def test_batch_bit_exact(ctx, batch, variant, cluster, threads):
 
 
 def test_batch_autotuner_picks_the_fastest_trial(ctx, batch):
+    """Round 1: the seven inner SpMV formats (ELL with 16 / 32 / 64 rows per
+    slice, CSR with 1 / 2 / 4 / 8 lanes per row) at 8 CTAs x 512 threads;
+    round 2: the best of them at every placeable cluster size (1, 2, 4, 8
+    always, 16 where the GPU places it) x width (256, 512)."""
     S, st, x = run(ctx, batch, tol=1e-8)
     info = S.info
     trials = S.trials()
-    # formats x cluster sizes (1, 2, 4, 8 always fit; 16 where the GPU places it) x widths
-    assert info.tuned and len(trials) == info.trials and 2 * 4 * 2 <= len(trials) <= 2 * 5 * 2
+    assert info.tuned and len(trials) == info.trials and 7 + 4 * 2 - 1 <= len(trials) <= 7 + 5 * 2 - 1
+    fmts = {(t[0], t[4], t[5]) for t in trials[:7]}
+    assert fmts == {(abi.SPMV_ELL, 16, 0), (abi.SPMV_ELL, 32, 0), (abi.SPMV_ELL, 64, 0),
+                    (abi.SPMV_CSR_SCALAR, 0, 1), (abi.SPMV_CSR_SCALAR, 0, 2), (abi.SPMV_CSR_SCALAR, 0, 4),
+                    (abi.SPMV_CSR_SCALAR, 0, 8)}
     best = min(trials, key=lambda t: t[3])
     assert (info.spmv_variant, info.cluster_size, info.threads) == best[:3]
+    assert (info.ell_slice, info.lanes_per_row) == best[4:]
     P = batch.problem
     o = O.batch_solve(P.row_ptr, P.cols, P.vals, batch.sys_offsets, P.b, tol=1e-8, cluster_size=info.cluster_size,
-                      threads=info.threads)
+                      threads=info.threads, lanes_per_row=info.lanes_per_row if info.lanes_per_row else 1)
     np.testing.assert_array_equal(x, o.x)
     assert st.systems_converged == batch.nsys
 
@@ -98,7 +117,9 @@ def test_batch_rejects_bad_input(ctx, batch):
                      ((A32, np.array([0, P.n // 2, P.n // 2, P.n])), {}),  # empty system
                      ((A32, np.array([0, batch.sys_offsets[1] + 1, P.n])), {}),  # cuts through a block
                      ((A32, batch.sys_offsets), dict(cluster_size=3)),
-                     ((A32, batch.sys_offsets), dict(threads=100))]:
+                     ((A32, batch.sys_offsets), dict(threads=100)),
+                     ((A32, batch.sys_offsets), dict(ell_slice=8)),
+                     ((A32, batch.sys_offsets), dict(lanes_per_row=3))]:
         with pytest.raises(abi.AB2Error) as e:
             abi.Batch(ctx, *args, **kw)
         assert e.value.code == abi.AB2_ERR_BAD_ARG
