@@ -31,9 +31,10 @@
 // y in (one bulk kernel), runs the two walks, and scatters z out (one bulk
 // kernel) -- bulk kernels have the whole GPU to hide latency, a wavefront
 // step does not.  Those two are transposes through shared memory
-// (k_walk_gather_t / k_walk_scatter_t), contiguous on both sides: 1.00 ms per
-// application at 192^3 against 1.03 ms with element-wise gather/scatter, and
-// 14 ms less per CG+ILU0 solve (286 applications).
+// (k_walk_gather_t / k_walk_scatter_t), contiguous on both sides; against
+// element-wise gather/scatter they saved ~30 us per application at 192^3
+// (14 ms per CG+ILU0 solve of 286 applications, measured before the poll
+// warp below).
 //
 // The backward sweep is the forward walk run backwards: the U walk's thread
 // (li,lj) of tile T at step s handles the cell the L walk handles at the
