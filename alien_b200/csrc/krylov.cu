@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "ab2_internal.cuh"
 #include "krylov.cuh"
@@ -143,13 +144,31 @@ __global__ void __launch_bounds__(kCtlThreads) k_cg_rz(int n, const T* __restric
   }
 }
 
-// p = z (first step, CG.h:89) or z += beta p ; p = z (CG.h:119-120)
+// p = z (first step, CG.h:89) or z += beta p ; p = z (CG.h:119-120).
+// Element-wise, so the thread that computes an element does not matter: 16
+// bytes (4 floats, 2 doubles) per thread and access, then the tail.
 template <class T>
 __global__ void k_cg_p(int n, const T* __restrict__ z, T* __restrict__ p, const SolveStateT<T>* st) {
   const T beta = st->beta;
   const int first = st->first;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    p[i] = first ? z[i] : fma_rn(beta, p[i], z[i]);
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  constexpr int W = 16 / (int)sizeof(T);
+  const int nv = n / W;
+  const V* __restrict__ zv = reinterpret_cast<const V*>(z);
+  V* __restrict__ pv = reinterpret_cast<V*>(p);
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int i = t0; i < nv; i += stride) {
+    V a = zv[i];
+    if (!first) {
+      const V b = pv[i];
+      T* pa = reinterpret_cast<T*>(&a);
+      const T* pb = reinterpret_cast<const T*>(&b);
+#pragma unroll
+      for (int u = 0; u < W; ++u) pa[u] = fma_rn(beta, pb[u], pa[u]);
+    }
+    pv[i] = a;
+  }
+  for (int i = nv * W + t0; i < n; i += stride) p[i] = first ? z[i] : fma_rn(beta, p[i], z[i]);
 }
 
 // q = A p ; den = q.p

@@ -1195,7 +1195,15 @@ def main():
     info = A.info
     vy = ctx.vector(P.n)
     spmv_ms = timed(lambda: ctx.mult(A, b, vy, abi.SPMV_ELL), 50)
-    spmv_roof = roof("k_spmv_ell (sliced ELL-32 FP64 SpMV)", spmv_bytes(info, P.n), spmv_ms, f"spmv_ell_{n1}")
+    ell_roof = roof("k_spmv_ell (sliced ELL-32 FP64 SpMV)", spmv_bytes(info, P.n), spmv_ms, f"spmv_ell_{n1}")
+    # the SpMV every solver on this matrix runs (AUTO: the 7-point bands), by its own bytes
+    if info.stencil_bands:
+        band_ms = timed(lambda: ctx.mult(A, b, vy, abi.SPMV_STENCIL), 50)
+        spmv_roof = roof(f"k_spmv_view<StencilView> (7-point bands x{info.stencil_bands}, FP64 SpMV)",
+                         info.stencil_bands * 8 * P.n + 16 * P.n, band_ms, f"spmv_bands_{n1}")
+        spmv_roof["ell32"] = ell_roof
+    else:
+        spmv_roof = ell_roof
     achieved = spmv_roof["achieved"]
     variants = None if a.no_variants else spmv_variant_section(abi, ctx, timed, A, P, a)
 
