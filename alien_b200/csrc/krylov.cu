@@ -185,14 +185,18 @@ __global__ void __launch_bounds__(kCtlThreads) k_cg_spmv(int n, View A, const T*
 }
 
 // alpha = rho1/den ; x += alpha p ; r -= alpha q ; then the loop's stop test on r.
+// p1 != nullptr: p is double-buffered (k_cgj_spmv formed it), and the buffer
+// it wrote is p0 or p1 by the body count's parity.
 template <class T>
-__global__ void __launch_bounds__(kCtlThreads) k_cg_update(int n, const T* __restrict__ p, const T* __restrict__ q,
-                                                           T* __restrict__ r, SolveStateT<T>* st, Red<T> red,
+__global__ void __launch_bounds__(kCtlThreads) k_cg_update(int n, const T* __restrict__ p0, const T* __restrict__ p1,
+                                                           const T* __restrict__ q, T* __restrict__ r,
+                                                           SolveStateT<T>* st, Red<T> red,
                                                            cudaGraphConditionalHandle h, int use_graph) {
   if (st->done) {
     if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(h, use_graph, 0);
     return;
   }
+  const T* __restrict__ p = (p1 && !(st->bodies & 1)) ? p1 : p0;
   const T den = st->den;
   const bool ok = den != T(0);
   const T alpha = ok ? st->rho1 / den : T(0);
@@ -569,13 +573,25 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
     pc_apply_t(ctx, pc, r, z);
     k_cg_rz<<<g, kCtlThreads, 0, ctx->stream>>>(n, r, z, st, red_of<T>(ctx, 1));
     check_launch(ctx, "cg_rz");
-    k_cg_p<<<ge, kThreads, 0, ctx->stream>>>(n, z, p, st);
-    check_launch(ctx, "cg_p");
-    with_op([&](auto view) {
-      k_cg_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red_of<T>(ctx, 2));
-    });
-    check_launch(ctx, "cg_spmv");
-    k_cg_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p, q, r, st, red_of<T>(ctx, 3), h, graph_loop);
+    if constexpr (sizeof(T) == sizeof(double)) {
+      // FP64: p = z + beta p formed inside the SpMV (two p buffers), as the
+      // Diag body does; the same values and trees
+      T* p1 = w[4];
+      with_op([&](auto view) {
+        k_cgj_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z, p, p1, q, st, red_of<T>(ctx, 2));
+      });
+      check_launch(ctx, "cgj_spmv");
+      k_cg_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p, p1, q, r, st, red_of<T>(ctx, 3), h, graph_loop);
+    } else {
+      k_cg_p<<<ge, kThreads, 0, ctx->stream>>>(n, z, p, st);
+      check_launch(ctx, "cg_p");
+      with_op([&](auto view) {
+        k_cg_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red_of<T>(ctx, 2));
+      });
+      check_launch(ctx, "cg_spmv");
+      k_cg_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p, (const T*)nullptr, q, r, st, red_of<T>(ctx, 3), h,
+                                                      graph_loop);
+    }
     check_launch(ctx, "cg_update");
   } else {
     T *r = w[0], *r0 = w[1], *p = w[2], *phat = w[3], *v = w[4], *s = w[5], *shat = w[6], *t = w[7];
@@ -644,7 +660,7 @@ void Krylov<T>::init(ab2_context* c, const ab2_matrix* a, const ab2_precond* p, 
   variant = spmv_variant;
   use_graph = graph_loop;
   fused_diag = solver == AB2_SOLVER_CG && pc && (pc->kind == AB2_PC_DIAG || pc->kind == AB2_PC_NONE);
-  const int nw = fused_diag ? 5 : solver == AB2_SOLVER_CG ? 4 : 8;
+  const int nw = fused_diag ? 5 : solver == AB2_SOLVER_CG ? (sizeof(T) == sizeof(double) ? 5 : 4) : 8;
   for (int i = 0; i < nw; ++i) {
     w[i] = dev_alloc<T>(ctx, (size_t)A->n);
     AB2_CUDA(cudaMemsetAsync(w[i], 0, sizeof(T) * (size_t)std::max(A->n, 1), ctx->stream));

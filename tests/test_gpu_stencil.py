@@ -157,3 +157,27 @@ def test_scaled_form_needs_symmetric_bands(ctx):
             abi.Mixed(ctx, A, solver="cg", precond="diag", jacobi_form="scaled")
         assert e.value.code == abi.AB2_ERR_BAD_ARG
         A.close()
+
+
+def test_explicit_zeros_in_the_profile_stay_terms(ctx):
+    """Entries stored with the value 0 are part of the row (as in the CSR
+    sum): 0 * inf gives NaN in the band SpMV exactly where the row-sequential
+    sum gives it."""
+    P = problems.get("poisson16")
+    v = P.vals.copy()
+    rows = [100, 777, 2048]
+    for r in rows:  # zero the (r, r+1) / (r+1, r) pair: still symmetric
+        a = P.row_ptr[r] + int(np.nonzero(P.cols[P.row_ptr[r]:P.row_ptr[r + 1]] == r + 1)[0][0])
+        b = P.row_ptr[r + 1] + int(np.nonzero(P.cols[P.row_ptr[r + 1]:P.row_ptr[r + 2]] == r)[0][0])
+        v[a] = v[b] = 0.0
+    A = ctx.matrix(P.row_ptr, P.cols, v, BANDS)
+    assert A.info.stencil_bands == 4
+    x = rnd(P.n, 9)
+    x[[r + 1 for r in rows]] = np.inf
+    vx, vy = ctx.vector(x), ctx.vector(P.n)
+    ctx.mult(A, vx, vy, abi.SPMV_STENCIL)
+    got = vy.download()
+    exp = O.spmv(P.row_ptr, P.cols, v, x)
+    np.testing.assert_array_equal(got, exp)
+    assert np.all(np.isnan(got[rows]))
+    A.close()
