@@ -30,7 +30,7 @@ FMT_CSR, FMT_ELL, FMT_F32, FMT_STENCIL = 1, 2, 4, 8
 SPMV_AUTO, SPMV_CSR_SCALAR, SPMV_CSR_STAGED, SPMV_ELL, SPMV_CSR_VECTOR, SPMV_STENCIL = 0, 1, 2, 3, 4, 5
 SOLVER = {"cg": 0, "bicgs": 1, "bicgstab": 1}
 PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3, "filu0": 4, "neumann": 5}
-ILU_SCHEDULE = {"auto": 0, "wavefront": 1, "stencil": 2}
+ILU_SCHEDULE = {"auto": 0, "wavefront": 1, "stencil": 2, "stencil_cluster": 3}
 BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho"}
 FCG_FALLBACK = {"sticky": 0, "step": 1}
 MIXED_JACOBI = {"auto": 0, "plain": 1, "scaled": 2}

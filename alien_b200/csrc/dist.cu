@@ -882,7 +882,7 @@ extern "C" int ab2_dist_precond_create(ab2_context* ctx, const ab2_dist_matrix* 
     ctx->last_error = "distributed preconditioners: NONE, DIAG and ILU0 (block Jacobi)";
     return AB2_ERR_UNSUPPORTED;
   }
-  if (o->ilu_schedule < AB2_ILU_AUTO || o->ilu_schedule > AB2_ILU_STENCIL) return AB2_ERR_BAD_ARG;
+  if (o->ilu_schedule < AB2_ILU_AUTO || o->ilu_schedule > AB2_ILU_STENCIL_CLUSTER) return AB2_ERR_BAD_ARG;
   ab2_precond* pc = new (std::nothrow) ab2_precond();
   if (!pc) return AB2_ERR_OOM;
   pc->ctx = ctx_retain(ctx);

@@ -51,12 +51,22 @@
 // Measured on B200, one application at 192^3: 0.61 ms (gather + two walks +
 // scatter; 0.97 ms before the poll warp), against 1.69 ms for the same walk
 // on natural-order arrays and 3.45 ms for the wavefront schedule of
-// precond.cu.  A lone tile steps in ~0.26 us; the rest is the trail each of
-// the 22 tile boundaries on the critical path adds.  Values loaded per poll
-// round: 4 steps (2: 0.63 ms, 3: 0.60, 8: 0.63, 16: 0.70).
+// precond.cu.  Values loaded per poll round: 4 steps (2: 0.63 ms, 3: 0.60,
+// 8: 0.63, 16: 0.70).  The cluster walk further down (2 x 2 tiles a cluster,
+// hand-offs inside a cluster through distributed shared memory): 0.58 ms.
+//
+// Where the time goes (per-tile timestamps of one L walk at 192^3, 144
+// tiles): a tile without upstream tiles steps in 0.265 us; tiles downstream
+// step in 0.34-0.42 us, since every step waits for a value its neighbour
+// produced 15 steps earlier plus the hand-off; a tile starts its walk ~8.5 us
+// (16 neighbour steps + hand-off) after its upstream tile.  The critical path
+// is 22 such lags plus one tile's walk: ~263 us.  The dependency depth
+// (nx + ny + nz - 2 = 574 steps) at the lone tile's step time would be 152 us.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 #include "ab2_internal.cuh"
@@ -64,6 +74,8 @@
 #include "sentinel.cuh"
 
 namespace ab2 {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -599,6 +611,325 @@ __global__ void __launch_bounds__(kTileThreads + 32, 1) k_walk_sweep(Walk g, Wal
   if (blockIdx.x == 0 && threadIdx.x == 0) tickets[UP ? 1 : 2] = 0u;
 }
 
+// ------------------------------------------------------------------ cluster walk
+// The same sweep with the tiles grouped into thread-block clusters of CX x CY
+// tiles, one tile per CTA.  Inside a cluster a tile's boundary values are
+// pushed by the producing threads (the last line along i, resp. j) straight
+// into the consuming CTA's shared memory, so a hand-off costs one store to a
+// neighbouring SM instead of a store to L2 followed by a poll of L2.
+// Hand-offs between clusters keep the poll warp's path through global memory.
+//
+// Every boundary value reaches the consuming compute thread through a buffer
+// of one slot per walk step (nsteps x 32 words of dynamic shared memory: the
+// j-side values of lines (l, 0) in lanes 0-15, the i-side values of lines
+// (0, l) in lanes 16-31).  Each slot is written once per launch and holds the
+// sentinel until its value arrives -- the value is the flag, as in global
+// memory -- so neither side waits for space and nothing is reset.  The poll
+// warp fills the slots of the sides whose upstream tile is in another
+// cluster; the producers in the cluster fill the others.
+//
+// Clusters take super-tiles from a ticket in row-major order, so a cluster
+// waits only on clusters that run or are done; the CTAs of one cluster run
+// together by construction.  Every wait is bounded as in the single-CTA walk.
+// A cluster barrier at the start makes every buffer valid before a peer
+// writes to it, and one at the end keeps each CTA's shared memory alive until
+// no peer can write to it any more.
+
+// Shared-memory words by 32-bit address: this CTA's (shared::cta) and a
+// peer's (shared::cluster, from mapa).
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned peer_addr(unsigned a, int rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+// No "memory" clobber: the value is its own flag, so no other access needs
+// ordering against the store, and a clobber would pin the walk's prefetched
+// loads in place (register spills in the FP64 backward sweep).
+__device__ __forceinline__ void st_peer(unsigned a, double v) {
+  asm volatile("st.relaxed.cluster.shared::cluster.b64 [%0], %1;" ::"r"(a),
+               "l"((unsigned long long)__double_as_longlong(v)));
+}
+__device__ __forceinline__ void st_peer(unsigned a, float v) {
+  asm volatile("st.relaxed.cluster.shared::cluster.b32 [%0], %1;" ::"r"(a), "r"(__float_as_uint(v)));
+}
+__device__ __forceinline__ double ld_slot(unsigned a, double) {
+  unsigned long long v;
+  asm volatile("ld.volatile.shared.b64 %0, [%1];" : "=l"(v) : "r"(a));
+  return __longlong_as_double((long long)v);
+}
+__device__ __forceinline__ float ld_slot(unsigned a, float) {
+  unsigned v;
+  asm volatile("ld.volatile.shared.b32 %0, [%1];" : "=r"(v) : "r"(a));
+  return __uint_as_float(v);
+}
+
+template <class T>
+__device__ __forceinline__ void cp_async(T* dst, const T* src) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte words");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst)), "l"(src), "n"((int)sizeof(T))
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// A slot of this CTA's buffer: its value, waited for (bounded) if it has not
+// arrived yet.
+template <class T>
+__device__ __noinline__ T wait_slot(unsigned a, int* err) {
+  const long long t0 = clock64();
+  for (unsigned it = 1;; ++it) {
+    const T v = ld_slot(a, T());
+    if (!is_sentinel(v)) return v;
+    if ((it & 255) == 0 && (clock64() - t0 > kWaitCycles || *(volatile int*)err)) {
+      atomicOr(err, 1);
+      return quiet_nan<T>();
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ T take_slot(unsigned a, int* err) {
+  const T v = ld_slot(a, T());
+  return is_sentinel(v) ? wait_slot<T>(a, err) : v;
+}
+
+// Whether a cluster sweep takes its step inputs through shared memory (the
+// FP64 backward sweep) rather than registers.
+template <bool UP, class T>
+constexpr bool walk_cl_async() {
+  return UP && sizeof(T) == 8;
+}
+
+// Dynamic shared memory of the cluster walk: the boundary buffer (nsteps x
+// 32 words) and, for the sweep that takes its inputs through shared memory,
+// the step-input ring (kWalkPrefetch + 1 slots of 5 x 256 words).
+template <bool UP, class T>
+constexpr size_t walk_cl_smem(int nsteps) {
+  return ((size_t)nsteps * 2 * kTile + (walk_cl_async<UP, T>() ? (size_t)(kWalkPrefetch + 1) * 5 * kTileThreads : 0)) *
+         sizeof(T);
+}
+
+template <bool UP, class T, int CX, int CY>
+__global__ void __launch_bounds__(kTileThreads + 32, 1)
+    k_walk_sweep_cl(Walk g, WalkArrays<T> b, T* in, T* wave, unsigned int* tickets, int* err) {
+  constexpr int kPre = kWalkPrefetch;
+  constexpr long long kStep = UP ? -kTileThreads : kTileThreads;
+  constexpr int kLanes = 2 * kTile;
+  constexpr bool kAsyncInputs = walk_cl_async<UP, T>();
+  __shared__ T s_val[2][kTile][kTile + 1];
+  __shared__ int s_tile;
+  extern __shared__ unsigned char walk_cl_raw[];
+  T* s_bnd = reinterpret_cast<T*>(walk_cl_raw);  // [step][lane]
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int cx = rank % CX, cy = rank / CX;
+  const int nsteps = g.nsteps;
+  for (int q = threadIdx.x; q < nsteps * kLanes; q += blockDim.x) s_bnd[q] = sentinel_of<T>();
+  if (threadIdx.x == 0 && rank == 0) s_tile = (int)atomicAdd(tickets + (UP ? 2 : 1), 1u);
+  cl.sync();
+  const int super = *cl.map_shared_rank(&s_tile, 0);
+  const int nsx = (g.ntx + CX - 1) / CX;
+  const int tx = (super % nsx) * CX + cx, ty = (super / nsx) * CY + cy;
+
+  if (tx < g.ntx && ty < g.nty) {
+    const int tile = ty * g.ntx + tx;
+    const bool poller = threadIdx.x >= kTileThreads;
+    const int lane = threadIdx.x & 31;
+    const int li = poller ? (lane < kTile ? lane : 0) : threadIdx.x % kTile;
+    const int lj = poller ? (lane < kTile ? 0 : lane - kTile) : threadIdx.x / kTile;
+    const int ox = UP ? g.ntx * kTile - g.nx : 0;
+    const int oy = UP ? g.nty * kTile - g.ny : 0;
+    const int oz = UP ? nsteps - g.nz - 2 * (kTile - 1) : 0;
+    auto phys = [&](long long w) { return UP ? g.nw - 1 - w : w; };
+    const int ai = tx * kTile + li;
+    const int aj = ty * kTile + lj;
+    const bool active = ai >= ox && ai < ox + g.nx && aj >= oy && aj < oy + g.ny;
+    const bool has_i = ai > ox, has_j = aj > oy;
+    const bool bnd_i = li == 0 && has_i, bnd_j = lj == 0 && has_j;
+    const int s_lo = active ? li + lj + oz : nsteps;
+    const int s_hi = active ? s_lo + g.nz : nsteps;
+    const long long tbase = (long long)tile * nsteps * kTileThreads;
+
+    if (poller) {
+      // The sides whose upstream tile is in another cluster: global memory.
+      const bool need = lane < kTile ? (bnd_j && cy == 0) : (bnd_i && cx == 0);
+      if (__any_sync(0xffffffffu, need)) {
+        const long long w_nb =
+            lane < kTile ? phys(tbase - (long long)g.ntx * nsteps * kTileThreads + 15 * kTileThreads + 15 * kTile + li)
+                         : phys(tbase - (long long)nsteps * kTileThreads + 15 * kTileThreads + lj * kTile + 15);
+        const T* p_nb = wave + (need ? w_nb : 0);
+        volatile T* slots = s_bnd + lane;
+        int t = need ? s_lo : s_hi;  // next step this lane hands over
+        long long t_last = clock64();
+        bool failed = false;
+        while (__any_sync(0xffffffffu, t < s_hi)) {
+          T v[kPollDepth];
+#pragma unroll
+          for (int d = 0; d < kPollDepth; ++d) {
+            const int st = t + d;
+            v[d] = (st < s_hi && !failed) ? ld_relaxed(p_nb + (long long)st * kStep) : sentinel_of<T>();
+          }
+          int adv = 0;  // leading steps whose values arrived
+#pragma unroll
+          for (int d = 0; d < kPollDepth; ++d) {
+            const int st = t + d;
+            if (adv == d && st < s_hi && (failed || !is_sentinel(v[d]))) {
+              slots[st * kLanes] = failed ? quiet_nan<T>() : v[d];
+              ++adv;
+            }
+          }
+          t += adv;
+          if (__any_sync(0xffffffffu, adv > 0)) {
+            t_last = clock64();
+          } else {  // (warp-uniform) give up after the bound: quiet NaNs from here on
+            const bool stop = __any_sync(0xffffffffu, clock64() - t_last > kWaitCycles || *(volatile int*)err != 0);
+            if (stop && !failed) {
+              if (lane == 0) atomicOr(err, 1);
+              failed = true;
+            }
+          }
+        }
+      }
+    } else {
+      // In-cluster consumers of this tile's last lines.
+      const bool feed_i = active && li == kTile - 1 && cx < CX - 1 && tx + 1 < g.ntx;
+      const bool feed_j = active && lj == kTile - 1 && cy < CY - 1 && ty + 1 < g.nty;
+      // 32-bit shared addresses of this thread's slots at step 0: own (read)
+      // and the consumers' (written); a step is kLanes words further.
+      const unsigned a_j = smem_addr(s_bnd + li), a_i = smem_addr(s_bnd + kTile + lj);
+      const unsigned r_i = feed_i ? peer_addr(a_i, rank + 1) : 0u;  // consumer line (0, lj)
+      const unsigned r_j = feed_j ? peer_addr(a_j, rank + CX) : 0u;  // consumer line (li, 0)
+      constexpr unsigned kSlotStep = kLanes * sizeof(T);
+
+      const long long w_own = phys(tbase + threadIdx.x);
+      const T* p_y = in + w_own;
+      const T* p_a1 = (UP ? b.Ui : b.Lk) + w_own;
+      const T* p_a2 = (UP ? b.Uj : b.Lj) + w_own;
+      const T* p_a3 = (UP ? b.Uk : b.Li) + w_own;
+      const T* p_piv = b.P + w_own;
+      T* p_in = in + w_own;
+      T* p_out = wave + w_own;
+
+      // One step of the walk from its inputs c.
+      T own = 0;
+      auto step = [&](int s, const PreW<T>& c) {
+        const long long o = (long long)s * kStep;
+        T val = 0;
+        if (s >= s_lo && s < s_hi) {
+          const T* prev = &s_val[(s + 1) & 1][0][0];
+          T vi = 0, vj = 0;
+          if (bnd_j) vj = take_slot<T>(a_j + s * kSlotStep, err);
+          if (bnd_i) vi = take_slot<T>(a_i + s * kSlotStep, err);
+          if (has_j && lj > 0) vj = prev[(lj - 1) * (kTile + 1) + li];
+          if (has_i && li > 0) vi = prev[lj * (kTile + 1) + li - 1];
+          const bool has_k = s > s_lo;
+          T acc = c.y;
+          if (!UP) {  // columns ascending: -k, -j, -i
+            if (has_k) acc = mul_sub_rn(c.a1, own, acc);
+            if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
+            if (has_i) acc = mul_sub_rn(c.a3, vi, acc);
+            val = acc;
+          } else {  // columns ascending: +i, +j, +k
+            if (has_i) acc = mul_sub_rn(c.a1, vi, acc);
+            if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
+            if (has_k) acc = mul_sub_rn(c.a3, own, acc);
+            p_in[o] = sentinel_of<T>();
+            val = acc / c.piv;
+          }
+          const T out = not_sentinel(val);
+          st_relaxed(p_out + o, out);
+          // the consumer's step: this one less the 15 lines between
+          const int cs = s - (kTile - 1);
+          if (feed_i) st_peer(r_i + cs * kSlotStep, out);
+          if (feed_j) st_peer(r_j + cs * kSlotStep, out);
+          own = val;
+        }
+        s_val[s & 1][lj][li] = val;
+      };
+
+      if constexpr (kAsyncInputs) {
+        // The FP64 backward sweep: its kPre steps of five inputs do not fit
+        // in registers beside the cluster hand-off (at most 168 a thread with
+        // nine warps), so they arrive by cp.async into a ring of kPre + 1
+        // slots in shared memory (this thread's column of each slot: no
+        // barrier), and the registers hold one step's inputs.
+        T* ring = s_bnd + (size_t)nsteps * kLanes + threadIdx.x;  // slot r, field f: ring[(r * 5 + f) * 256]
+        auto issue = [&](int s, int slot) {
+          if (s < nsteps) {
+            const long long o = (long long)s * kStep;
+            T* d = ring + slot * 5 * kTileThreads;
+            cp_async(d, p_y + o);
+            cp_async(d + kTileThreads, p_a1 + o);
+            cp_async(d + 2 * kTileThreads, p_a2 + o);
+            cp_async(d + 3 * kTileThreads, p_a3 + o);
+            cp_async(d + 4 * kTileThreads, p_piv + o);
+          }
+          cp_commit();
+        };
+        auto fetch = [&](int slot, PreW<T>& c) {
+          const T* d = ring + slot * 5 * kTileThreads;
+          c.y = d[0];
+          c.a1 = d[kTileThreads];
+          c.a2 = d[2 * kTileThreads];
+          c.a3 = d[3 * kTileThreads];
+          c.piv = d[4 * kTileThreads];
+        };
+        constexpr int kSlots = kPre + 1;
+#pragma unroll
+        for (int u = 0; u < kPre; ++u) issue(u, u);
+        int slot_next = 0, slot_issue = kPre;  // slots of step s + 1 and of step s + kPre
+        PreW<T> nxt{0, 0, 0, 0, 0};
+        cp_wait<kPre - 1>();
+        fetch(0, nxt);
+        for (int s = 0; s < nsteps; ++s) {
+          const PreW<T> c = nxt;
+          issue(s + kPre, slot_issue);
+          slot_issue = slot_issue + 1 == kSlots ? 0 : slot_issue + 1;
+          step(s, c);
+          // the next step's inputs, before the barrier
+          slot_next = slot_next + 1 == kSlots ? 0 : slot_next + 1;
+          cp_wait<kPre - 1>();
+          fetch(slot_next, nxt);
+          compute_bar();
+        }
+      } else {
+        // Inputs kPre steps ahead in registers, as in the single-CTA walk.
+        auto load = [&](int s, long long o, PreW<T>& p) {
+          if (s < s_lo || s >= s_hi) return;
+          p.y = __ldg(p_y + o);
+          p.a1 = __ldg(p_a1 + o);
+          p.a2 = __ldg(p_a2 + o);
+          p.a3 = __ldg(p_a3 + o);
+          if (UP) p.piv = __ldg(p_piv + o);
+        };
+        PreW<T> pre[kPre];
+#pragma unroll
+        for (int u = 0; u < kPre; ++u) {
+          pre[u] = PreW<T>{0, 0, 0, 0, 0};
+          load(u, u * kStep, pre[u]);
+        }
+        for (int s0 = 0; s0 < nsteps; s0 += kPre) {
+          const long long o0 = (long long)s0 * kStep;
+#pragma unroll
+          for (int u = 0; u < kPre; ++u) {
+            const PreW<T> c = pre[u];
+            load(s0 + u + kPre, o0 + (u + kPre) * kStep, pre[u]);
+            step(s0 + u, c);
+            compute_bar();
+          }
+        }
+      }
+    }
+  }
+  // Hand the other sweep its ticket back (it does not run concurrently).
+  if (blockIdx.x == 0 && threadIdx.x == 0) tickets[UP ? 1 : 2] = 0u;
+  cl.sync();
+}
+
 Geom geom_of(const Ilu0Data& d) {
   Geom g;
   g.nx = d.st_nx;
@@ -646,13 +977,95 @@ WalkArrays<T> walk_bands(T* base, const Ilu0Data& d) {
 
 int wave_grid(ab2_context* ctx, int ntiles) { return std::max(1, std::min(ntiles, ctx->num_sms * 2)); }
 
+// The cluster walk: 2 x 2 tiles per cluster.  Measured at 192^3 (one ILU(0)
+// application, B200): 2 x 2 0.581 ms, 2 x 4 0.588, 4 x 2 0.646, 4 x 4 0.642,
+// against 0.609 for the single-CTA walk.  With one CTA an SM (the walk's
+// shared memory), a GPC holds fewer large clusters than its SMs allow CTAs,
+// and the remaining clusters start late.
+constexpr int kClX = 2, kClY = 2;
+// Its buffers live in shared memory: up to this many bytes (nz up to ~470 in
+// FP64, ~1000 in FP32); longer walks take the single-CTA walk.
+constexpr size_t kWalkClSmemMax = 216 * 1024;
+
+template <bool UP, class T>
+cudaLaunchConfig_t walk_cl_config(cudaStream_t stream, const Walk& w, cudaLaunchAttribute* attr) {
+  const int nsx = (w.ntx + kClX - 1) / kClX, nsy = (w.nty + kClY - 1) / kClY;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kClX * kClY;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nsx * nsy * kClX * kClY));
+  cfg.blockDim = dim3(kTileThreads + 32);
+  cfg.dynamicSmemBytes = walk_cl_smem<UP, T>(w.nsteps);
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+// Whether the device runs the cluster walk at all: both sweeps, at the
+// shared-memory cap, asked once per device and word size (the kernels'
+// shared-memory limit is raised to the cap on the way, so that no set-up can
+// lower it under another factor's walk).
+template <class T>
+bool walk_cl_device_ok(ab2_context* ctx) {
+  static std::atomic<int> ok[64];  // 0: not asked, 1: yes, 2: no
+  const int dev = ctx->device;
+  if (dev >= 0 && dev < 64 && ok[dev].load() != 0) return ok[dev].load() == 1;
+  bool fits = true;
+  Walk w{};
+  w.ntx = w.nty = kClX * kClY;
+  cudaLaunchAttribute attr[1];
+  for (int up = 0; up < 2 && fits; ++up) {
+    const void* k = up ? (const void*)k_walk_sweep_cl<true, T, kClX, kClY> : (const void*)k_walk_sweep_cl<false, T, kClX, kClY>;
+    AB2_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWalkClSmemMax));
+    cudaLaunchConfig_t cfg = up ? walk_cl_config<true, T>(nullptr, w, attr) : walk_cl_config<false, T>(nullptr, w, attr);
+    cfg.dynamicSmemBytes = kWalkClSmemMax;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess || n < 1) {
+      (void)cudaGetLastError();
+      fits = false;
+    }
+  }
+  if (dev >= 0 && dev < 64) ok[dev].store(fits ? 1 : 2);
+  return fits;
+}
+
+// Whether this factor's walk can take the cluster walk (both word sizes: the
+// mixed-precision solvers run the FP32 copy on the same schedule).
+bool walk_cl_possible(ab2_context* ctx, const Walk& w) {
+  const bool size_ok = walk_cl_smem<true, double>(w.nsteps) <= kWalkClSmemMax &&
+                       walk_cl_smem<false, double>(w.nsteps) <= kWalkClSmemMax;
+  return size_ok && walk_cl_device_ok<double>(ctx) && walk_cl_device_ok<float>(ctx);
+}
+
+template <bool UP, class T>
+void launch_walk_cl(ab2_context* ctx, const Walk& w, const WalkArrays<T>& b, T* in, T* wave, unsigned int* tickets,
+                    int* err) {
+  cudaLaunchAttribute attr[1];
+  const cudaLaunchConfig_t cfg = walk_cl_config<UP, T>(ctx->stream, w, attr);
+  AB2_CUDA(cudaLaunchKernelEx(&cfg, k_walk_sweep_cl<UP, T, kClX, kClY>, w, b, in, wave, tickets, err));
+}
+
+// One sweep (UP: the backward one) on the factor's walk.
+template <bool UP, class T>
+void walk_sweep(ab2_context* ctx, const Ilu0Data& d, const Walk& w, const WalkArrays<T>& b, T* in, T* wave) {
+  if (d.walk_cluster)
+    launch_walk_cl<UP, T>(ctx, w, b, in, wave, d.d_tile_tickets, d.d_err);
+  else
+    k_walk_sweep<UP, T><<<wave_grid(ctx, w.ntx * w.nty), kTileThreads + 32, 0, ctx->stream>>>(
+        w, b, in, wave, d.d_tile_tickets, d.d_err);
+  check_launch(ctx, UP ? "walk_usweep" : "walk_lsweep");
+}
+
 int bulk_grid(ab2_context* ctx, long long n) {
   return (int)std::max(1LL, std::min((n + kThreads - 1) / kThreads, (long long)ctx->num_sms * 16));
 }
 
 }  // namespace
 
-bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool factored) {
+bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool factored, int schedule) {
   const int n = A->n;
   if (n == 0) return false;
   // The 7-point geometry: kept by the matrix (AB2_FMT_STENCIL) or checked here.
@@ -702,6 +1115,9 @@ bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool 
   dev_free(ctx, d.d_bands);
   d.d_bands = nullptr;
   set_transpose_smem<double>();
+  d.walk_cluster = schedule != AB2_ILU_STENCIL && walk_cl_possible(ctx, w);
+  require(schedule != AB2_ILU_STENCIL_CLUSTER || d.walk_cluster,
+          "ILU0 cluster schedule requested but its buffers do not fit shared memory (too many planes along z)");
   d.stencil = true;
   d.levels_l = d.levels_u = (int)(nx + ny + nz - 2);
   return true;
@@ -725,12 +1141,8 @@ void walk_apply(ab2_context* ctx, const Ilu0Data& d, T* base, const T* y, T* z) 
   if (kTranspose) k_walk_gather_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, y, yw);
   else k_walk_gather<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, y, yw);
   check_launch(ctx, "walk_gather");
-  k_walk_sweep<false, T><<<wave_grid(ctx, tiles), kTileThreads + 32, 0, ctx->stream>>>(w, b, yw, lw, d.d_tile_tickets,
-                                                                                d.d_err);
-  check_launch(ctx, "walk_lsweep");
-  k_walk_sweep<true, T><<<wave_grid(ctx, tiles), kTileThreads + 32, 0, ctx->stream>>>(w, b, lw, uw, d.d_tile_tickets,
-                                                                               d.d_err);
-  check_launch(ctx, "walk_usweep");
+  walk_sweep<false, T>(ctx, d, w, b, yw, lw);
+  walk_sweep<true, T>(ctx, d, w, b, lw, uw);
   if (kTranspose) k_walk_scatter_t<T><<<tr_grid, kTileThreads, tr_smem<T>(), ctx->stream>>>(w, uw, z);
   else k_walk_scatter<<<bulk_grid(ctx, w.nw), kThreads, 0, ctx->stream>>>(w, uw, z);
   check_launch(ctx, "walk_scatter");

@@ -327,9 +327,9 @@ void ilu_init(ab2_context* ctx, ab2_precond* pc, int schedule, const double* lu)
                            ctx->stream));
   k_fill_bits<<<grid_for(A->n), kThreads, 0, ctx->stream>>>(A->n, kSentinel, d.d_tmp);
   check_launch(ctx, "ilu_fill");
-  if (schedule != AB2_ILU_WAVEFRONT && ilu_stencil_setup(ctx, A, d, lu != nullptr)) return;
-  require(schedule != AB2_ILU_STENCIL, "ILU0 tile schedule requested but the matrix is not a 3-D 7-point "
-                                       "matrix in lexicographic order");
+  if (schedule != AB2_ILU_WAVEFRONT && ilu_stencil_setup(ctx, A, d, lu != nullptr, schedule)) return;
+  require(schedule != AB2_ILU_STENCIL && schedule != AB2_ILU_STENCIL_CLUSTER,
+          "ILU0 tile schedule requested but the matrix is not a 3-D 7-point matrix in lexicographic order");
   ilu_symbolic(A, d);
   if (lu) return;
   for (int l = 1; l < d.levels_l; ++l) {  // wavefront 0 rows have nothing left of the diagonal
@@ -677,7 +677,7 @@ int ab2_precond_create(ab2_context* ctx, const ab2_matrix* A, const ab2_precond_
       op_inv_diag(ctx, A, pc->d_inv);
     }
     if (o->kind == AB2_PC_ILU0) {
-      require(o->ilu_schedule >= AB2_ILU_AUTO && o->ilu_schedule <= AB2_ILU_STENCIL, "unknown ILU0 schedule");
+      require(o->ilu_schedule >= AB2_ILU_AUTO && o->ilu_schedule <= AB2_ILU_STENCIL_CLUSTER, "unknown ILU0 schedule");
       ilu_init(ctx, pc, o->ilu_schedule);
     }
     if (o->kind == AB2_PC_CHEB) {
@@ -739,7 +739,9 @@ int ab2_precond_get_info(const ab2_precond* pc, ab2_precond_info* info) {
   info->cheb_beta = pc->cheb.beta;
   info->ilu_levels_lower = pc->ilu.levels_l;
   info->ilu_levels_upper = pc->ilu.levels_u;
-  info->ilu_schedule = pc->kind != AB2_PC_ILU0 ? 0 : pc->ilu.stencil ? AB2_ILU_STENCIL : AB2_ILU_WAVEFRONT;
+  info->ilu_schedule = pc->kind != AB2_PC_ILU0 ? 0
+                      : pc->ilu.stencil ? (pc->ilu.walk_cluster ? AB2_ILU_STENCIL_CLUSTER : AB2_ILU_STENCIL)
+                                        : AB2_ILU_WAVEFRONT;
   info->neumann_factor = pc->neu.omega;
   return AB2_OK;
 }

@@ -39,12 +39,16 @@ struct Ilu0Data {
   long long walk_n = 0;
   double* d_walk = nullptr;
   float* d_walk32 = nullptr;  // the same arrays in FP32 (mixed-precision inner solves), built on demand
+  bool walk_cluster = false;  // sweeps in 2 x 2-tile clusters (else one tile per CTA)
 };
 
 // Detects a 3-D 7-point matrix in lexicographic order and, if found,
 // factorises it on the tile-walk schedule (bands + CSR copy in d_lu); with
 // factored, d_lu already holds the factor and only the walk arrays are built.
-bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool factored = false);
+// schedule (AB2_ILU_*): AB2_ILU_STENCIL keeps one tile per CTA; AUTO and
+// AB2_ILU_STENCIL_CLUSTER take the cluster walk when it fits (the latter
+// fails otherwise).
+bool ilu_stencil_setup(ab2_context* ctx, const ab2_matrix* A, Ilu0Data& d, bool factored, int schedule);
 void ilu_stencil_apply(ab2_context* ctx, const ab2_matrix* A, const Ilu0Data& d, const double* y, double* z);
 // Puts the sweeps' propagation arrays back to the sentinel (after a failed application).
 void ilu_stencil_reset(ab2_context* ctx, const Ilu0Data& d);

@@ -208,15 +208,22 @@ int ab2_scalar_get(ab2_context* ctx, const ab2_scalar* s, double* value);
 int ab2_dot_noalloc(const double* x, const double* y, int n, double* result, void* stream);
 
 /* ------------------------------------------------------------------ preconditioners */
-/* ILU(0) schedules; both give the same factor and applications bit for bit.
+/* ILU(0) schedules; all give the same factor and applications bit for bit.
  * WAVEFRONT: any CSR matrix; rows grouped by wavefront of the triangular
  *   graphs, one warp per 32 rows, cross-warp waits through global memory.
  * STENCIL: 3-D 7-point matrices in lexicographic order; 16x16 tiles of
- *   grid lines per CTA walk their diagonals through shared memory.
- * AUTO: STENCIL when the matrix has that structure, else WAVEFRONT. */
+ *   grid lines per CTA walk their diagonals through shared memory; values
+ *   between tiles through global memory.
+ * STENCIL_CLUSTER: the STENCIL walk with 2x2 tiles per thread-block cluster;
+ *   values between the tiles of a cluster go straight into the neighbour's
+ *   shared memory.  Its buffers must fit shared memory: up to ~470 planes
+ *   along z in FP64 (a request beyond that is refused).
+ * AUTO: STENCIL_CLUSTER, else STENCIL when the matrix has that structure,
+ *   else WAVEFRONT. */
 #define AB2_ILU_AUTO 0
 #define AB2_ILU_WAVEFRONT 1
 #define AB2_ILU_STENCIL 2
+#define AB2_ILU_STENCIL_CLUSTER 3
 
 typedef struct {
   int kind;                 /* AB2_PC_* */
@@ -252,7 +259,7 @@ typedef struct {
   double cheb_beta;  /* upper bound used by Chebyshev */
   int ilu_levels_lower; /* wavefronts of the L sweep */
   int ilu_levels_upper; /* wavefronts of the U sweep */
-  int ilu_schedule;     /* AB2_ILU_WAVEFRONT or AB2_ILU_STENCIL as chosen */
+  int ilu_schedule;     /* AB2_ILU_WAVEFRONT, AB2_ILU_STENCIL or AB2_ILU_STENCIL_CLUSTER as chosen */
   double neumann_factor; /* omega used by Neumann */
 } ab2_precond_info;
 int ab2_precond_get_info(const ab2_precond* pc, ab2_precond_info* info);

@@ -69,11 +69,11 @@ def test_dot_bit_exact(ctx, big):
     assert ctx.dot(ctx.vector(x), ctx.vector(y)) == O.dot_tree(x, y, ctx.info.reduction_max_blocks)
 
 
-@pytest.mark.parametrize("schedule", ["stencil", "wavefront"])
+@pytest.mark.parametrize("schedule", ["stencil_cluster", "stencil", "wavefront"])
 def test_ilu0_factor_and_apply_bit_exact(ctx, big, dev, schedule):
     y = np.random.default_rng(3).standard_normal(big.n)
     M = abi.Precond(ctx, dev, "ilu0", ilu_schedule=schedule)
-    assert M.info.ilu_schedule == (2 if schedule == "stencil" else 1)
+    assert M.info.ilu_schedule == abi.ILU_SCHEDULE[schedule]
     np.testing.assert_array_equal(M.ilu0_values(), O.ilu0_factor(big.row_ptr, big.cols, big.vals))
     vy, vz = ctx.vector(y), ctx.vector(big.n)
     M.apply(vy, vz)

@@ -29,7 +29,7 @@ def test_ilu0_factor_and_apply_bit_exact(ctx, name, schedule):
     P = abi.diffusion(37, 21, 5, sigma=1.0, smooth=2.0, seed=9) if name == "grid_37x21x5" else problems.get(name)
     A = ctx.matrix(P.row_ptr, P.cols, P.vals)
     pc = abi.Precond(ctx, A, "ilu0", ilu_schedule=schedule)
-    expect = abi.ILU_SCHEDULE["stencil" if schedule == "auto" and name in STENCIL_SHAPED else "wavefront"]
+    expect = abi.ILU_SCHEDULE["stencil_cluster" if schedule == "auto" and name in STENCIL_SHAPED else "wavefront"]
     assert pc.info.ilu_schedule == expect
     np.testing.assert_array_equal(pc.ilu0_values(), O.ilu0_factor(P.row_ptr, P.cols, P.vals))
     for seed in range(3):  # repeated applications (sweep state must reset itself)
@@ -48,11 +48,28 @@ def test_ilu0_factor_and_apply_bit_exact(ctx, name, schedule):
         assert info.ilu_levels_lower == 3 * 16 - 2
 
 
-def test_ilu0_stencil_schedule_refused_for_other_matrices(ctx):
+@pytest.mark.parametrize("schedule", ["stencil", "stencil_cluster"])
+def test_ilu0_stencil_schedule_refused_for_other_matrices(ctx, schedule):
     P = problems.get("ragged")
     A = ctx.matrix(P.row_ptr, P.cols, P.vals)
     with pytest.raises(abi.AB2Error) as e:
-        abi.Precond(ctx, A, "ilu0", ilu_schedule="stencil")
+        abi.Precond(ctx, A, "ilu0", ilu_schedule=schedule)
+    assert e.value.code == abi.AB2_ERR_BAD_ARG
+
+
+def test_ilu0_cluster_schedule_needs_its_buffers_in_shared_memory(ctx):
+    """600 planes along z: the cluster walk's buffers exceed shared memory,
+    so AUTO takes the single-CTA walk and an explicit request is refused."""
+    P = abi.diffusion(20, 18, 600, sigma=1.0, smooth=2.0, seed=3)
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals)
+    pc = abi.Precond(ctx, A, "ilu0")
+    assert pc.info.ilu_schedule == abi.ILU_SCHEDULE["stencil"]
+    y = rnd(P.n, 4)
+    vy, vx = ctx.vector(y), ctx.vector(P.n)
+    pc.apply(vy, vx)
+    np.testing.assert_array_equal(vx.download(), O.ilu0_apply(P.row_ptr, P.cols, P.vals, y))
+    with pytest.raises(abi.AB2Error) as e:
+        abi.Precond(ctx, A, "ilu0", ilu_schedule="stencil_cluster")
     assert e.value.code == abi.AB2_ERR_BAD_ARG
 
 
@@ -109,3 +126,22 @@ def test_chebyshev_bounds_and_apply(ctx, name, factor):
     np.testing.assert_allclose(vy.download(), ref, rtol=0, atol=1e-11 * np.max(np.abs(ref)))
     pc.apply(vx, vx)  # aliasing input/output
     np.testing.assert_array_equal(vx.download(), exact)
+
+
+# The stencil sweeps one tile per CTA and in 2 x 2-tile thread-block clusters
+# (tiles handing boundary values to their cluster neighbours through
+# distributed shared memory), on grids whose tiles fill several clusters,
+# partly filled clusters and partial tiles included.  Same bits as the
+# sequential sweeps.
+@pytest.mark.parametrize("schedule", ["stencil", "stencil_cluster"])
+@pytest.mark.parametrize("dims", [(130, 75, 7), (40, 40, 6), (16, 100, 3), (100, 16, 3)])
+def test_ilu0_stencil_walks_bit_exact(ctx, schedule, dims):
+    P = abi.diffusion(*dims, sigma=1.0, smooth=2.0, seed=5)
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals)
+    pc = abi.Precond(ctx, A, "ilu0", ilu_schedule=schedule)
+    assert pc.info.ilu_schedule == abi.ILU_SCHEDULE[schedule]
+    for seed in range(2):
+        y = rnd(P.n, 20 + seed)
+        vy, vx = ctx.vector(y), ctx.vector(P.n)
+        pc.apply(vy, vx)
+        np.testing.assert_array_equal(vx.download(), O.ilu0_apply(P.row_ptr, P.cols, P.vals, y))
