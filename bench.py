@@ -1212,7 +1212,7 @@ def main():
     if METHODS[a.method]["precond"] == "ilu0":
         pc = abi.Precond(ctx, A, "ilu0")
         ilu_ms = timed(lambda: pc.apply(b, vy), 20)
-        roofline = roof("k_walk_gather_t + k_walk_sweep<L> + k_walk_sweep<U> + k_walk_scatter_t (ILU0 apply, tile walk)",
+        roofline = roof("k_walk_gather_t + k_walk_sweep_cl<L> + k_walk_sweep_cl<U> + k_walk_scatter_t (ILU0 apply, tile walk in 2x2-tile clusters)",
                         ilu_bytes(P.n, P.nnz), ilu_ms, f"ilu0_apply_{n1}")
         pc.close()
     else:
