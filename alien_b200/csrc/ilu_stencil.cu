@@ -859,7 +859,7 @@ __global__ void __launch_bounds__(kTileThreads + 32, 1)
         // barrier), and the registers hold one step's inputs.
         T* ring = s_bnd + (size_t)nsteps * kLanes + threadIdx.x;  // slot r, field f: ring[(r * 5 + f) * 256]
         auto issue = [&](int s, int slot) {
-          if (s < nsteps) {
+          if (s >= s_lo && s < s_hi) {  // (the walk's padding cells are never read)
             const long long o = (long long)s * kStep;
             T* d = ring + slot * 5 * kTileThreads;
             cp_async(d, p_y + o);
