@@ -147,9 +147,15 @@ def spmv_bytes(info, n: int) -> int:
 
 
 def ilu_bytes(n: int, nnz: int) -> int:
-    """ILU0 apply (both sweeps), algorithmic minimum for the stencil layout:
-    every factor value read once (no column indices: the stencil fixes
-    them), y read once, x written once."""
+    """ILU0 apply (both sweeps), B_LU: the LU factor's values and column
+    indices, its row pointers and one n-vector of 8-byte values."""
+    return int(12 * nnz + 4 * (n + 1) + 8 * n)
+
+
+def ilu_stencil_min_bytes(n: int, nnz: int) -> int:
+    """ILU0 apply (both sweeps), the least any schedule on a 7-point matrix
+    must move: every factor value read once (no column indices: the stencil
+    fixes them), y read once, x written once."""
     return int(8 * nnz + 16 * n)
 
 
@@ -544,14 +550,14 @@ def preconditioner_section(abi, ctx, stream, A, P, a):
     b_spmv = 12 * nnz + 4 * (n + 1) + 16 * n
     sweeps = 12 * (nnz - n) + 56 * n
     kinds = {"diag": (dict(kind="diag"), 24 * n),
-             "ilu0": (dict(kind="ilu0"), 8 * nnz + 16 * n),
+             "ilu0": (dict(kind="ilu0"), ilu_bytes(n, nnz)),
              "cheb3_saad": (dict(kind="cheb", cheb_saad=True, poly_order=3, poly_factor_max_iter=20),
                             3 * b_spmv + 5 * 8 * n),
              "filu0_3": (dict(kind="filu0", filu_factor_iter=0, filu_solver_iter=3), 3 * sweeps),
              "neumann3": (dict(kind="neumann", poly_order=3, poly_factor_max_iter=20), 3 * (b_spmv + 16 * n))}
     pk, pk_kind = peaks()
     vx, vy = ctx.vector(P.b), ctx.vector(n)
-    out = {"apply": {}, "note": "algorithmic bytes per application: diag 24n; ILU0 8 nnz + 16 n; Chebyshev(3) "
+    out = {"apply": {}, "note": "algorithmic bytes per application: diag 24n; ILU0 B_LU = 12 nnz + 4 (n + 1) + 8 n; Chebyshev(3) "
                                  "3 B_spmv + 40 n; FILU0(3 sweeps) 3 (12 (nnz - n) + 56 n); Neumann(3) 3 (B_spmv + 16 n)"}
     for name, (kw, nbytes) in kinds.items():
         pc = abi.Precond(ctx, A, **kw)
@@ -1214,6 +1220,10 @@ def main():
         ilu_ms = timed(lambda: pc.apply(b, vy), 20)
         roofline = roof("k_walk_gather_t + k_walk_sweep_cl<L> + k_walk_sweep_cl<U> + k_walk_scatter_t (ILU0 apply, tile walk in 2x2-tile clusters)",
                         ilu_bytes(P.n, P.nnz), ilu_ms, f"ilu0_apply_{n1}")
+        roofline["bytes_formula"] = "B_LU = 12 nnz + 4 (n + 1) + 8 n"
+        smin = ilu_stencil_min_bytes(P.n, P.nnz)
+        roofline["stencil_min"] = {"bytes": smin, "formula": "8 nnz + 16 n",
+                                   "frac": round(smin / (ilu_ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4)}
         pc.close()
     else:
         roofline = spmv_roof
