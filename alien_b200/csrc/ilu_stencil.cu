@@ -53,7 +53,8 @@
 // on natural-order arrays and 3.45 ms for the wavefront schedule of
 // precond.cu.  Values loaded per poll round: 4 steps (2: 0.63 ms, 3: 0.60,
 // 8: 0.63, 16: 0.70).  The cluster walk further down (2 x 2 tiles a cluster,
-// hand-offs inside a cluster through distributed shared memory): 0.58 ms.
+// hand-offs inside a cluster through distributed shared memory, step inputs
+// by bulk copy): 0.566 ms.
 //
 // Where the time goes (per-tile timestamps of one L walk at 192^3, 144
 // tiles): a tile without upstream tiles steps in 0.265 us; tiles downstream
@@ -628,12 +629,23 @@ __global__ void __launch_bounds__(kTileThreads + 32, 1) k_walk_sweep(Walk g, Wal
 // warp fills the slots of the sides whose upstream tile is in another
 // cluster; the producers in the cluster fill the others.
 //
+// The step inputs (y and the three bands, plus the pivot in the backward
+// sweep: 256 consecutive words per array and step in walk order) come by bulk
+// copy (cp.async.bulk, no multicast) into a ring of kInRing steps in shared
+// memory, issued by a tenth warp as soon as the compute warps free a slot and
+// completed on one mbarrier per slot; every compute thread waits on the slot
+// (bounded) and reads its words.  Against the single-CTA walk's register
+// prefetch this frees the compute warps' registers and load instructions; the
+// issuing warp is separate from the poll warp, whose rounds through L2 would
+// otherwise hold the copies back.
+//
 // Clusters take super-tiles from a ticket in row-major order, so a cluster
 // waits only on clusters that run or are done; the CTAs of one cluster run
 // together by construction.  Every wait is bounded as in the single-CTA walk.
 // A cluster barrier at the start makes every buffer valid before a peer
 // writes to it, and one at the end keeps each CTA's shared memory alive until
-// no peer can write to it any more.
+// no peer can write to it any more; before it the issuing warp waits
+// (bounded) for its copies still in flight.
 
 // Shared-memory words by 32-bit address: this CTA's (shared::cta) and a
 // peer's (shared::cluster, from mapa).
@@ -664,18 +676,6 @@ __device__ __forceinline__ float ld_slot(unsigned a, float) {
   return __uint_as_float(v);
 }
 
-template <class T>
-__device__ __forceinline__ void cp_async(T* dst, const T* src) {
-  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte words");
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst)), "l"(src), "n"((int)sizeof(T))
-               : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // A slot of this CTA's buffer: its value, waited for (bounded) if it has not
 // arrived yet.
 template <class T>
@@ -697,50 +697,113 @@ __device__ __forceinline__ T take_slot(unsigned a, int* err) {
   return is_sentinel(v) ? wait_slot<T>(a, err) : v;
 }
 
-// Whether a cluster sweep takes its step inputs through shared memory (the
-// FP64 backward sweep) rather than registers.
-template <bool UP, class T>
-constexpr bool walk_cl_async() {
-  return UP && sizeof(T) == 8;
+// Step inputs by bulk copy: each step's rows of the walk arrays (256
+// consecutive words per array, in walk order) land in a ring of kInRing steps
+// in shared memory, each slot completed on its own mbarrier.
+constexpr int kInRing = 12;
+template <bool UP>
+constexpr int walk_in_fields() {
+  return UP ? 5 : 4;  // y, three bands (and the pivot)
+}
+
+__device__ __forceinline__ void mbar_init(unsigned a, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned a, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned a, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Global -> this CTA's shared memory, completing on the mbarrier (no
+// multicast: the destination is this CTA's own window).
+__device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigned bytes, unsigned mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+// A word of the input ring (after the mbarrier wait, whose "memory" clobber
+// keeps the load behind it).
+__device__ __forceinline__ double ld_in(unsigned a, double) {
+  unsigned long long v;
+  asm("ld.shared.b64 %0, [%1];" : "=l"(v) : "r"(a) : "memory");
+  return __longlong_as_double((long long)v);
+}
+__device__ __forceinline__ float ld_in(unsigned a, float) {
+  unsigned v;
+  asm("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+  return __uint_as_float(v);
+}
+
+// Waits (bounded) for the phase of the given parity; false if it gave up.
+__device__ __noinline__ bool mbar_wait(unsigned a, unsigned parity, int* err) {
+  const long long t0 = clock64();
+  for (unsigned it = 1;; ++it) {
+    if (mbar_try_wait(a, parity)) return true;
+    if ((it & 15) == 0 && (clock64() - t0 > kWaitCycles || *(volatile int*)err)) {
+      atomicOr(err, 1);
+      return false;
+    }
+  }
 }
 
 // Dynamic shared memory of the cluster walk: the boundary buffer (nsteps x
-// 32 words) and, for the sweep that takes its inputs through shared memory,
-// the step-input ring (kWalkPrefetch + 1 slots of 5 x 256 words).
+// 32 words), the input ring (kInRing x fields x 256 words) and its mbarriers.
 template <bool UP, class T>
 constexpr size_t walk_cl_smem(int nsteps) {
-  return ((size_t)nsteps * 2 * kTile + (walk_cl_async<UP, T>() ? (size_t)(kWalkPrefetch + 1) * 5 * kTileThreads : 0)) *
-         sizeof(T);
+  return ((size_t)nsteps * 2 * kTile + (size_t)kInRing * walk_in_fields<UP>() * kTileThreads) * sizeof(T) +
+         kInRing * sizeof(unsigned long long);
 }
 
 template <bool UP, class T, int CX, int CY>
-__global__ void __launch_bounds__(kTileThreads + 32, 1)
+__global__ void __launch_bounds__(kTileThreads + 64, 1)
     k_walk_sweep_cl(Walk g, WalkArrays<T> b, T* in, T* wave, unsigned int* tickets, int* err) {
   constexpr int kPre = kWalkPrefetch;
   constexpr long long kStep = UP ? -kTileThreads : kTileThreads;
   constexpr int kLanes = 2 * kTile;
-  constexpr bool kAsyncInputs = walk_cl_async<UP, T>();
+  constexpr int kF = walk_in_fields<UP>();
+  constexpr unsigned kRowBytes = kTileThreads * sizeof(T);
   __shared__ T s_val[2][kTile][kTile + 1];
   __shared__ int s_tile;
-  extern __shared__ unsigned char walk_cl_raw[];
-  T* s_bnd = reinterpret_cast<T*>(walk_cl_raw);  // [step][lane]
+  __shared__ volatile int s_done;  // last step the compute warps finished (the input ring's producer)
+  extern __shared__ __align__(128) unsigned char walk_cl_raw[];
+  T* s_bnd = reinterpret_cast<T*>(walk_cl_raw);                   // [step][lane]
+  T* s_in = s_bnd + (size_t)g.nsteps * kLanes;                    // [slot][field][256]
+  unsigned long long* s_mbar = reinterpret_cast<unsigned long long*>(s_in + (size_t)kInRing * kF * kTileThreads);
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   const int cx = rank % CX, cy = rank / CX;
   const int nsteps = g.nsteps;
   for (int q = threadIdx.x; q < nsteps * kLanes; q += blockDim.x) s_bnd[q] = sentinel_of<T>();
-  if (threadIdx.x == 0 && rank == 0) s_tile = (int)atomicAdd(tickets + (UP ? 2 : 1), 1u);
+  if (threadIdx.x == 0) {
+    s_done = -1;
+    if (rank == 0) s_tile = (int)atomicAdd(tickets + (UP ? 2 : 1), 1u);
+  }
+  if (threadIdx.x == kTileThreads + 32) {
+    for (int q = 0; q < kInRing; ++q) mbar_init(smem_addr(s_mbar + q), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
   cl.sync();
   const int super = *cl.map_shared_rank(&s_tile, 0);
   const int nsx = (g.ntx + CX - 1) / CX;
   const int tx = (super % nsx) * CX + cx, ty = (super / nsx) * CY + cy;
+  const unsigned mbar0 = smem_addr(s_mbar);
 
   if (tx < g.ntx && ty < g.nty) {
     const int tile = ty * g.ntx + tx;
-    const bool poller = threadIdx.x >= kTileThreads;
+    const bool copier = threadIdx.x >= kTileThreads + 32;
+    const bool poller = !copier && threadIdx.x >= kTileThreads;
     const int lane = threadIdx.x & 31;
     const int li = poller ? (lane < kTile ? lane : 0) : threadIdx.x % kTile;
-    const int lj = poller ? (lane < kTile ? 0 : lane - kTile) : threadIdx.x / kTile;
+    const int lj = poller ? (lane < kTile ? 0 : lane - kTile) : (threadIdx.x / kTile) % kTile;
     const int ox = UP ? g.ntx * kTile - g.nx : 0;
     const int oy = UP ? g.nty * kTile - g.ny : 0;
     const int oz = UP ? nsteps - g.nz - 2 * (kTile - 1) : 0;
@@ -754,7 +817,46 @@ __global__ void __launch_bounds__(kTileThreads + 32, 1)
     const int s_hi = active ? s_lo + g.nz : nsteps;
     const long long tbase = (long long)tile * nsteps * kTileThreads;
 
-    if (poller) {
+    if (copier) {
+      // Lane 0 issues each step's bulk copies once its slot is free.
+      if (lane == 0) {
+        const T* src[kF];
+        src[0] = in;
+        src[1] = UP ? b.Ui : b.Lk;
+        src[2] = UP ? b.Uj : b.Lj;
+        src[3] = UP ? b.Uk : b.Li;
+        if constexpr (kF == 5) src[4] = b.P;
+        // first word of step t's 256 in the arrays (the U walk reads its block reversed)
+        auto row0 = [&](int t) { return UP ? g.nw - kTileThreads - tbase - (long long)t * kTileThreads
+                                           : tbase + (long long)t * kTileThreads; };
+        const unsigned in0 = smem_addr(s_in);
+        int t_issue = 0;  // next step whose inputs are copied
+        long long t_last = clock64();
+        while (t_issue < nsteps) {
+          const int lim = min(nsteps, s_done + kInRing + 1);
+          if (t_issue < lim) {
+            for (; t_issue < lim; ++t_issue) {
+              const int q = t_issue % kInRing;
+              const unsigned mb = mbar0 + q * 8;
+              mbar_expect_tx(mb, kF * kRowBytes);
+              const long long w0 = row0(t_issue);
+#pragma unroll
+              for (int f = 0; f < kF; ++f) bulk_load(in0 + (q * kF + f) * kRowBytes, src[f] + w0, kRowBytes, mb);
+            }
+            t_last = clock64();
+          } else {
+            __nanosleep(100);  // waiting for the compute warps to free a slot
+            if (clock64() - t_last > kWaitCycles || *(volatile int*)err) {
+              atomicOr(err, 1);
+              break;
+            }
+          }
+        }
+        // Copies still in flight land before the CTA may leave (bounded).
+        for (int x = max(0, t_issue - kInRing); x < t_issue; ++x)
+          if (!mbar_wait(mbar0 + (x % kInRing) * 8, (x / kInRing) & 1, err)) break;
+      }
+    } else if (poller) {
       // The sides whose upstream tile is in another cluster: global memory.
       const bool need = lane < kTile ? (bnd_j && cy == 0) : (bnd_i && cx == 0);
       if (__any_sync(0xffffffffu, need)) {
@@ -806,120 +908,71 @@ __global__ void __launch_bounds__(kTileThreads + 32, 1)
       constexpr unsigned kSlotStep = kLanes * sizeof(T);
 
       const long long w_own = phys(tbase + threadIdx.x);
-      const T* p_y = in + w_own;
-      const T* p_a1 = (UP ? b.Ui : b.Lk) + w_own;
-      const T* p_a2 = (UP ? b.Uj : b.Lj) + w_own;
-      const T* p_a3 = (UP ? b.Uk : b.Li) + w_own;
-      const T* p_piv = b.P + w_own;
       T* p_in = in + w_own;
       T* p_out = wave + w_own;
+      // this thread's word of each input row in the ring (the U walk's rows are reversed)
+      const unsigned a_in = smem_addr(s_in) + (UP ? kTileThreads - 1 - threadIdx.x : threadIdx.x) * sizeof(T);
 
-      // One step of the walk from its inputs c.
-      T own = 0;
-      auto step = [&](int s, const PreW<T>& c) {
-        const long long o = (long long)s * kStep;
-        T val = 0;
-        if (s >= s_lo && s < s_hi) {
-          const T* prev = &s_val[(s + 1) & 1][0][0];
-          T vi = 0, vj = 0;
-          if (bnd_j) vj = take_slot<T>(a_j + s * kSlotStep, err);
-          if (bnd_i) vi = take_slot<T>(a_i + s * kSlotStep, err);
-          if (has_j && lj > 0) vj = prev[(lj - 1) * (kTile + 1) + li];
-          if (has_i && li > 0) vi = prev[lj * (kTile + 1) + li - 1];
-          const bool has_k = s > s_lo;
-          T acc = c.y;
-          if (!UP) {  // columns ascending: -k, -j, -i
-            if (has_k) acc = mul_sub_rn(c.a1, own, acc);
-            if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
-            if (has_i) acc = mul_sub_rn(c.a3, vi, acc);
-            val = acc;
-          } else {  // columns ascending: +i, +j, +k
-            if (has_i) acc = mul_sub_rn(c.a1, vi, acc);
-            if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
-            if (has_k) acc = mul_sub_rn(c.a3, own, acc);
-            p_in[o] = sentinel_of<T>();
-            val = acc / c.piv;
-          }
-          const T out = not_sentinel(val);
-          st_relaxed(p_out + o, out);
-          // the consumer's step: this one less the 15 lines between
-          const int cs = s - (kTile - 1);
-          if (feed_i) st_peer(r_i + cs * kSlotStep, out);
-          if (feed_j) st_peer(r_j + cs * kSlotStep, out);
-          own = val;
-        }
-        s_val[s & 1][lj][li] = val;
+      // Step s's inputs, once their slot's copies have landed.
+      auto fetch = [&](int s, PreW<T>& c) {
+        const int q = s % kInRing;
+        const unsigned mb = mbar0 + q * 8, par = (s / kInRing) & 1;
+        if (!mbar_try_wait(mb, par)) mbar_wait(mb, par, err);
+        const unsigned a = a_in + q * kF * kRowBytes;
+        c.y = ld_in(a, T());
+        c.a1 = ld_in(a + kRowBytes, T());
+        c.a2 = ld_in(a + 2 * kRowBytes, T());
+        c.a3 = ld_in(a + 3 * kRowBytes, T());
+        if constexpr (kF == 5) c.piv = ld_in(a + 4 * kRowBytes, T());
       };
 
-      if constexpr (kAsyncInputs) {
-        // The FP64 backward sweep: its kPre steps of five inputs do not fit
-        // in registers beside the cluster hand-off (at most 168 a thread with
-        // nine warps), so they arrive by cp.async into a ring of kPre + 1
-        // slots in shared memory (this thread's column of each slot: no
-        // barrier), and the registers hold one step's inputs.
-        T* ring = s_bnd + (size_t)nsteps * kLanes + threadIdx.x;  // slot r, field f: ring[(r * 5 + f) * 256]
-        auto issue = [&](int s, int slot) {
-          if (s >= s_lo && s < s_hi) {  // (the walk's padding cells are never read)
-            const long long o = (long long)s * kStep;
-            T* d = ring + slot * 5 * kTileThreads;
-            cp_async(d, p_y + o);
-            cp_async(d + kTileThreads, p_a1 + o);
-            cp_async(d + 2 * kTileThreads, p_a2 + o);
-            cp_async(d + 3 * kTileThreads, p_a3 + o);
-            cp_async(d + 4 * kTileThreads, p_piv + o);
-          }
-          cp_commit();
-        };
-        auto fetch = [&](int slot, PreW<T>& c) {
-          const T* d = ring + slot * 5 * kTileThreads;
-          c.y = d[0];
-          c.a1 = d[kTileThreads];
-          c.a2 = d[2 * kTileThreads];
-          c.a3 = d[3 * kTileThreads];
-          c.piv = d[4 * kTileThreads];
-        };
-        constexpr int kSlots = kPre + 1;
-#pragma unroll
-        for (int u = 0; u < kPre; ++u) issue(u, u);
-        int slot_next = 0, slot_issue = kPre;  // slots of step s + 1 and of step s + kPre
-        PreW<T> nxt{0, 0, 0, 0, 0};
-        cp_wait<kPre - 1>();
-        fetch(0, nxt);
-        for (int s = 0; s < nsteps; ++s) {
-          const PreW<T> c = nxt;
-          issue(s + kPre, slot_issue);
-          slot_issue = slot_issue + 1 == kSlots ? 0 : slot_issue + 1;
-          step(s, c);
-          // the next step's inputs, before the barrier
-          slot_next = slot_next + 1 == kSlots ? 0 : slot_next + 1;
-          cp_wait<kPre - 1>();
-          fetch(slot_next, nxt);
-          compute_bar();
-        }
-      } else {
-        // Inputs kPre steps ahead in registers, as in the single-CTA walk.
-        auto load = [&](int s, long long o, PreW<T>& p) {
-          if (s < s_lo || s >= s_hi) return;
-          p.y = __ldg(p_y + o);
-          p.a1 = __ldg(p_a1 + o);
-          p.a2 = __ldg(p_a2 + o);
-          p.a3 = __ldg(p_a3 + o);
-          if (UP) p.piv = __ldg(p_piv + o);
-        };
-        PreW<T> pre[kPre];
+      T own = 0;
+      PreW<T> nxt{0, 0, 0, 0, 0};
+      fetch(0, nxt);
+      for (int s0 = 0; s0 < nsteps; s0 += kPre) {
 #pragma unroll
         for (int u = 0; u < kPre; ++u) {
-          pre[u] = PreW<T>{0, 0, 0, 0, 0};
-          load(u, u * kStep, pre[u]);
-        }
-        for (int s0 = 0; s0 < nsteps; s0 += kPre) {
-          const long long o0 = (long long)s0 * kStep;
-#pragma unroll
-          for (int u = 0; u < kPre; ++u) {
-            const PreW<T> c = pre[u];
-            load(s0 + u + kPre, o0 + (u + kPre) * kStep, pre[u]);
-            step(s0 + u, c);
-            compute_bar();
+          const int s = s0 + u;
+          const long long o = (long long)s * kStep;
+          const PreW<T> c = nxt;
+          T val = 0;
+          if (s >= s_lo && s < s_hi) {
+            const T* prev = &s_val[(s + 1) & 1][0][0];
+            T vi = 0, vj = 0;
+            if (bnd_j) vj = take_slot<T>(a_j + s * kSlotStep, err);
+            if (bnd_i) vi = take_slot<T>(a_i + s * kSlotStep, err);
+            if (has_j && lj > 0) vj = prev[(lj - 1) * (kTile + 1) + li];
+            if (has_i && li > 0) vi = prev[lj * (kTile + 1) + li - 1];
+            const bool has_k = s > s_lo;
+            T acc = c.y;
+            if (!UP) {  // columns ascending: -k, -j, -i
+              if (has_k) acc = mul_sub_rn(c.a1, own, acc);
+              if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
+              if (has_i) acc = mul_sub_rn(c.a3, vi, acc);
+              val = acc;
+            } else {  // columns ascending: +i, +j, +k
+              if (has_i) acc = mul_sub_rn(c.a1, vi, acc);
+              if (has_j) acc = mul_sub_rn(c.a2, vj, acc);
+              if (has_k) acc = mul_sub_rn(c.a3, own, acc);
+              p_in[o] = sentinel_of<T>();
+              val = acc / c.piv;
+            }
+            const T out = not_sentinel(val);
+            st_relaxed(p_out + o, out);
+            // the consumer's step: this one less the 15 lines between
+            const int cs = s - (kTile - 1);
+            if (feed_i) st_peer(r_i + cs * kSlotStep, out);
+            if (feed_j) st_peer(r_j + cs * kSlotStep, out);
+            own = val;
+          }
+          s_val[s & 1][lj][li] = val;
+          // the next step's inputs, before the barrier (this step's slot is
+          // handed back to the producer once s_done passes it)
+          if (s + 1 < nsteps) fetch(s + 1, nxt);
+          compute_bar();
+          if (threadIdx.x == 0) {
+            __threadfence_block();
+            s_done = s;
           }
         }
       }
@@ -983,8 +1036,8 @@ int wave_grid(ab2_context* ctx, int ntiles) { return std::max(1, std::min(ntiles
 // shared memory), a GPC holds fewer large clusters than its SMs allow CTAs,
 // and the remaining clusters start late.
 constexpr int kClX = 2, kClY = 2;
-// Its buffers live in shared memory: up to this many bytes (nz up to ~470 in
-// FP64, ~1000 in FP32); longer walks take the single-CTA walk.
+// Its buffers live in shared memory: up to this many bytes (nz up to ~350 in
+// FP64); longer walks take the single-CTA walk.
 constexpr size_t kWalkClSmemMax = 216 * 1024;
 
 template <bool UP, class T>
@@ -996,7 +1049,7 @@ cudaLaunchConfig_t walk_cl_config(cudaStream_t stream, const Walk& w, cudaLaunch
   attr[0].val.clusterDim.z = 1;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(nsx * nsy * kClX * kClY));
-  cfg.blockDim = dim3(kTileThreads + 32);
+  cfg.blockDim = dim3(kTileThreads + 64);
   cfg.dynamicSmemBytes = walk_cl_smem<UP, T>(w.nsteps);
   cfg.stream = stream;
   cfg.attrs = attr;

@@ -216,8 +216,8 @@ int ab2_dot_noalloc(const double* x, const double* y, int n, double* result, voi
  *   between tiles through global memory.
  * STENCIL_CLUSTER: the STENCIL walk with 2x2 tiles per thread-block cluster;
  *   values between the tiles of a cluster go straight into the neighbour's
- *   shared memory.  Its buffers must fit shared memory: up to ~470 planes
- *   along z in FP64 (a request beyond that is refused).
+ *   shared memory.  Its buffers must fit shared memory: up to ~350 planes
+ *   along z (a request beyond that is refused).
  * AUTO: STENCIL_CLUSTER, else STENCIL when the matrix has that structure,
  *   else WAVEFRONT. */
 #define AB2_ILU_AUTO 0
