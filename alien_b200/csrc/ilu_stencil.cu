@@ -54,7 +54,7 @@
 // precond.cu.  Values loaded per poll round: 4 steps (2: 0.63 ms, 3: 0.60,
 // 8: 0.63, 16: 0.70).  The cluster walk further down (2 x 2 tiles a cluster,
 // hand-offs inside a cluster through distributed shared memory, step inputs
-// by bulk copy): 0.566 ms.
+// by bulk copy): 0.551 ms.
 //
 // Where the time goes (per-tile timestamps of one L walk at 192^3, 144
 // tiles): a tile without upstream tiles steps in 0.265 us; tiles downstream
@@ -970,10 +970,10 @@ __global__ void __launch_bounds__(kTileThreads + 64, 1)
           // handed back to the producer once s_done passes it)
           if (s + 1 < nsteps) fetch(s + 1, nxt);
           compute_bar();
-          if (threadIdx.x == 0) {
-            __threadfence_block();
-            s_done = s;
-          }
+          // (no fence: the only reader, the copy warp, reuses the slot of a
+          // step whose words every thread read into registers before the
+          // barrier; a fence here cost ~13 us per application at 192^3)
+          if (threadIdx.x == 0) s_done = s;
         }
       }
     }
