@@ -730,6 +730,15 @@ __device__ __forceinline__ void bulk_load(unsigned dst, const void* src, unsigne
                "l"(src), "r"(bytes), "r"(mbar)
                : "memory");
 }
+// The walk's output word, its own flag for the next tiles (no "memory"
+// clobber: no other access needs ordering against it).
+__device__ __forceinline__ void st_flag(double* p, double x) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(x)));
+}
+__device__ __forceinline__ void st_flag(float* p, float x) {
+  asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(__float_as_uint(x)));
+}
+
 // A word of the input ring (after the mbarrier wait, whose "memory" clobber
 // keeps the load behind it).
 __device__ __forceinline__ double ld_in(unsigned a, double) {
@@ -914,9 +923,16 @@ __global__ void __launch_bounds__(kTileThreads + 64, 1)
       const unsigned a_in = smem_addr(s_in) + (UP ? kTileThreads - 1 - threadIdx.x : threadIdx.x) * sizeof(T);
 
       // Step s's inputs, once their slot's copies have landed.
+      int f_slot = 0;
+      unsigned f_par = 0;  // slot and phase parity of the next step to fetch
       auto fetch = [&](int s, PreW<T>& c) {
-        const int q = s % kInRing;
-        const unsigned mb = mbar0 + q * 8, par = (s / kInRing) & 1;
+        (void)s;
+        const int q = f_slot;
+        const unsigned mb = mbar0 + q * 8, par = f_par;
+        if (++f_slot == kInRing) {
+          f_slot = 0;
+          f_par ^= 1u;
+        }
         if (!mbar_try_wait(mb, par)) mbar_wait(mb, par, err);
         const unsigned a = a_in + q * kF * kRowBytes;
         c.y = ld_in(a, T());
@@ -958,7 +974,7 @@ __global__ void __launch_bounds__(kTileThreads + 64, 1)
               val = acc / c.piv;
             }
             const T out = not_sentinel(val);
-            st_relaxed(p_out + o, out);
+            st_flag(p_out + o, out);
             // the consumer's step: this one less the 15 lines between
             const int cs = s - (kTile - 1);
             if (feed_i) st_peer(r_i + cs * kSlotStep, out);
