@@ -273,8 +273,11 @@ __global__ void k_walk_scatter(Walk g, T* __restrict__ src, T* __restrict__ dst)
 // consecutive natural rows.  Each thread stages its own cells in a ring of
 // planes in shared memory (its own column: no barrier) and moves a plane
 // once every lane has it.  One CTA per (tile, kTrPlanes planes).
-constexpr int kTrPlanes = 64;
-constexpr int kTrBatch = 4;                          // steps (planes) per batch
+// Measured per application at 192^3 (planes a CTA / batch): 64/4 550 us,
+// 64/8 598, 64/16 555, 96/8 583, 96/12 542, 96/16 542, 96/20 551, 96/24 553,
+// 96/32 561, 128/16 551, 128/24 564, 192/16 560.
+constexpr int kTrPlanes = 96;
+constexpr int kTrBatch = 12;                         // steps (planes) per batch
 constexpr int kTrRing = 2 * (kTile - 1) + kTrBatch;  // planes live at once per thread
 
 template <class T>
