@@ -755,6 +755,15 @@ __device__ __forceinline__ float ld_in(unsigned a, float) {
   return __uint_as_float(v);
 }
 
+// Waits for the phase of the given parity within the time bound only (the
+// end-of-kernel drain of copies in flight); false if it gave up.
+__device__ __noinline__ bool mbar_drain(unsigned a, unsigned parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(a, parity))
+    if (clock64() - t0 > kWaitCycles) return false;
+  return true;
+}
+
 // Waits (bounded) for the phase of the given parity; false if it gave up.
 __device__ __noinline__ bool mbar_wait(unsigned a, unsigned parity, int* err) {
   const long long t0 = clock64();
@@ -864,9 +873,10 @@ __global__ void __launch_bounds__(kTileThreads + 64, 1)
             }
           }
         }
-        // Copies still in flight land before the CTA may leave (bounded).
+        // Copies still in flight land before the CTA may leave (bounded by
+        // time only: also after a failure, whatever the error flag says).
         for (int x = max(0, t_issue - kInRing); x < t_issue; ++x)
-          if (!mbar_wait(mbar0 + (x % kInRing) * 8, (x / kInRing) & 1, err)) break;
+          if (!mbar_drain(mbar0 + (x % kInRing) * 8, (x / kInRing) & 1)) break;
       }
     } else if (poller) {
       // The sides whose upstream tile is in another cluster: global memory.
