@@ -134,7 +134,7 @@ def test_chebyshev_bounds_and_apply(ctx, name, factor):
 # partly filled clusters and partial tiles included.  Same bits as the
 # sequential sweeps.
 @pytest.mark.parametrize("schedule", ["stencil", "stencil_cluster"])
-@pytest.mark.parametrize("dims", [(130, 75, 7), (40, 40, 6), (16, 100, 3), (100, 16, 3)])
+@pytest.mark.parametrize("dims", [(130, 75, 7), (40, 40, 6), (16, 100, 3), (100, 16, 3), (20, 18, 340)])
 def test_ilu0_stencil_walks_bit_exact(ctx, schedule, dims):
     P = abi.diffusion(*dims, sigma=1.0, smooth=2.0, seed=5)
     A = ctx.matrix(P.row_ptr, P.cols, P.vals)
