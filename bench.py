@@ -517,6 +517,12 @@ def batch_section(abi, ctx, stream, a):
         lo, hi = B.sys_offsets[s_], B.sys_offsets[s_ + 1]
         err.append(float(np.linalg.norm(xs[lo:hi] - Q.x_true[lo:hi]) / np.linalg.norm(Q.x_true[lo:hi])))
     sizes = np.diff(B.sys_offsets)
+    # Inner FP32 Jacobi-PCG bytes per iteration of each system, the fused-schedule
+    # lower bound B_SpMV + 52 n with 4-byte values (B_SpMV = 8 nnz + 4 (n + 1) + 8 n).
+    nnz_s = np.diff(Q.row_ptr[B.sys_offsets]).astype(np.float64)
+    bytes_it = 8 * nnz_s + 4 * (sizes + 1) + 8 * sizes + 52 * sizes
+    inner_bytes = float(np.sum(inner.astype(np.float64) * bytes_it))
+    pk, pk_kind = peaks()
     out = {"workload": f"{B.nsys} systems, 2-D 5-pt / 3-D 7-pt heterogeneous diffusion, rows log-uniform 2k-200k, "
                        f"cg_jacobi fp32 inner + fp64 refinement, per-system tol 1e-8",
            "systems": B.nsys, "rows": int(Q.n), "nnz": int(Q.nnz), "rows_min_max": [int(sizes.min()), int(sizes.max())],
@@ -526,6 +532,11 @@ def batch_section(abi, ctx, stream, a):
            "inner_iterations_total": int(inner.sum()), "inner_iterations_max": int(inner.max()),
            "outer_steps_max": int(outer.max()),
            "rows_per_s": round(Q.n / min(times), 1),
+           "inner_bytes": inner_bytes,
+           "inner_gbs": round(inner_bytes / min(times) / 1e9, 1),
+           "inner_frac": round(inner_bytes / min(times) / 1e9 / pk["hbm_gbs"], 4), "peak_source": pk_kind,
+           "inner_bytes_note": "sum over systems of inner iterations x (8 nnz + 4 (n + 1) + 60 n): the FP32 "
+                               "Jacobi-PCG fused-schedule lower bound; systems of up to ~20 MB run from L2",
            "config": {"spmv_variant": fmt_name(info.spmv_variant, info.ell_slice, info.lanes_per_row),
                       "cluster_size": info.cluster_size, "threads": info.threads, "autotuned": bool(info.tuned)},
            "autotune_ms": round(info.tune_ms, 2), "setup_ms": round(info.setup_ms, 2),
