@@ -29,7 +29,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
+#include <unordered_map>
 
 #include "ab2_internal.cuh"
 #include "krylov.cuh"
@@ -106,6 +108,7 @@ __global__ void k_state_init(SolveStateT<T>* st, T tol, int max_iter, T* x, cons
   st->error = 0;
   st->breakdown = 0;
   st->exit_fixup = 0;
+  st->x_pending = 0;
   st->bodies = 0;
   st->rho = st->rho1 = st->den = st->alpha = st->beta = st->omega = st->rr_r = 0;
 }
@@ -171,17 +174,77 @@ __global__ void k_cg_p(int n, const T* __restrict__ z, T* __restrict__ p, const 
   for (int i = nv * W + t0; i < n; i += stride) p[i] = first ? z[i] : fma_rn(beta, p[i], z[i]);
 }
 
-// q = A p ; den = q.p
-template <class View, class T>
+// k_cg_p with the owed x update of the previous iteration in the same pass
+// (x += alpha p_old with the p about to be replaced: the same values and the
+// same rounding as updating x in k_cgj_update, one read of p less).  Nothing
+// once the solve is done (the host-driven loop queues bodies past the end).
+template <class T>
+__global__ void k_cg_px(int n, const T* __restrict__ z, T* __restrict__ p, const SolveStateT<T>* st) {
+  if (st->done) return;
+  const T beta = st->beta, alpha = st->alpha;
+  const int first = st->first, owed = st->x_pending;
+  T* __restrict__ x = st->x;
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  constexpr int W = 16 / (int)sizeof(T);
+  const int nv = n / W;
+  const V* __restrict__ zv = reinterpret_cast<const V*>(z);
+  V* __restrict__ pv = reinterpret_cast<V*>(p);
+  V* __restrict__ xv = reinterpret_cast<V*>(x);
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int i = t0; i < nv; i += stride) {
+    V a = zv[i];
+    if (!first) {
+      const V b = pv[i];
+      T* pa = reinterpret_cast<T*>(&a);
+      const T* pb = reinterpret_cast<const T*>(&b);
+      if (owed) {
+        V c = xv[i];
+        T* pc = reinterpret_cast<T*>(&c);
+#pragma unroll
+        for (int u = 0; u < W; ++u) pc[u] = fma_rn(alpha, pb[u], pc[u]);
+        xv[i] = c;
+      }
+#pragma unroll
+      for (int u = 0; u < W; ++u) pa[u] = fma_rn(beta, pb[u], pa[u]);
+    }
+    pv[i] = a;
+  }
+  for (int i = nv * W + t0; i < n; i += stride) {
+    if (!first && owed) x[i] = fma_rn(alpha, p[i], x[i]);
+    p[i] = first ? z[i] : fma_rn(beta, p[i], z[i]);
+  }
+}
+
+// After the loop: the last iteration's owed x += alpha p.
+template <class T>
+__global__ void k_cg_xfix(int n, const T* __restrict__ p, const SolveStateT<T>* st) {
+  if (!st->x_pending) return;
+  const T alpha = st->alpha;
+  T* __restrict__ x = st->x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = fma_rn(alpha, p[i], x[i]);
+}
+
+// q = A p ; den = q.p.  VB logical blocks of the reduction grid per block
+// (grid_reduce_v): a thread walks its VB logical threads' rows side by side,
+// so at any time the GPU works on one contiguous stretch of rows.
+template <class View, class T, int VB = 1>
 __global__ void __launch_bounds__(kCtlThreads) k_cg_spmv(int n, View A, const T* __restrict__ p, T* __restrict__ q,
                                                          SolveStateT<T>* st, Red<T> red) {
-  T acc[1] = {T(0)};
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-    const T qv = A.row(row, p);
-    q[row] = qv;
-    acc[0] = fma_rn(qv, p[row], acc[0]);
+  T acc[VB][1] = {};
+  const int lstride = gridDim.x * blockDim.x;  // between a thread's logical threads
+  for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += VB * lstride) {
+#pragma unroll
+    for (int v = 0; v < VB; ++v) {
+      const int row = base + v * lstride;
+      if (row < n) {
+        const T qv = A.row(row, p);
+        q[row] = qv;
+        acc[v][0] = fma_rn(qv, p[row], acc[v][0]);
+      }
+    }
   }
-  if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) st->den = red.result[0];
+  if (grid_reduce_v<1, VB>(acc, red.partials, red.counter, red.result)) st->den = red.result[0];
 }
 
 // alpha = rho1/den ; x += alpha p ; r -= alpha q ; then the loop's stop test on r.
@@ -263,7 +326,8 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_start(int n, const T* __res
 }
 
 // p = first ? z : z + beta p_old (into the other buffer) ; q = A p ; den = q.p
-template <class View, class T>
+// (VB: as k_cg_spmv)
+template <class View, class T, int VB = 1>
 __global__ void __launch_bounds__(kCtlThreads) k_cgj_spmv(int n, View A, const T* __restrict__ z, T* p0, T* p1,
                                                           T* __restrict__ q, SolveStateT<T>* st, Red<T> red) {
   if (st->done) return;  // every block returns: the reduction below is skipped as a whole
@@ -273,22 +337,31 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_spmv(int n, View A, const T
   const T beta = st->beta;
   const int first = st->first;
   auto pval = [&](int c) { return first ? z[c] : fma_rn(beta, po[c], z[c]); };
-  T acc[1] = {T(0)};
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-    const T qv = A.row_f(row, pval);
-    const T pr = pval(row);
-    pn[row] = pr;
-    q[row] = qv;
-    acc[0] = fma_rn(qv, pr, acc[0]);
+  T acc[VB][1] = {};
+  const int lstride = gridDim.x * blockDim.x;  // between a thread's logical threads
+  for (int base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += VB * lstride) {
+#pragma unroll
+    for (int v = 0; v < VB; ++v) {
+      const int row = base + v * lstride;
+      if (row < n) {
+        const T qv = A.row_f(row, pval);
+        const T pr = pval(row);
+        pn[row] = pr;
+        q[row] = qv;
+        acc[v][0] = fma_rn(qv, pr, acc[v][0]);
+      }
+    }
   }
-  if (grid_reduce<1>(acc, red.partials, red.counter, red.result)) st->den = red.result[0];
+  if (grid_reduce_v<1, VB>(acc, red.partials, red.counter, red.result)) st->den = red.result[0];
 }
 
 // alpha = rho1/den ; x += alpha p ; r -= alpha q ; z = D^-1 r ; r.r (stop test) and r.z (next rho1).
 // inv = nullptr: z = r, not stored (z may be null).  w: the stop test sums
 // (r_i w_i) r_i instead (the scaled Jacobi form's unscaled residual norm).
-template <class T>
-__global__ void __launch_bounds__(kCtlThreads) k_cgj_update(int n, const T* p0, const T* p1, const T* __restrict__ q,
+// DEFER_X: x is not touched here; x += alpha p is owed (x_pending) and paid
+// by the next k_cg_px, which reads p anyway, or by k_cg_xfix after the loop.
+template <class T, bool DEFER_X = false>
+__global__ void __launch_bounds__(kCtlThreads, 8) k_cgj_update(int n, const T* p0, const T* p1, const T* __restrict__ q,
                                                             T* __restrict__ r, T* __restrict__ z,
                                                             const T* __restrict__ inv, const T* __restrict__ w,
                                                             SolveStateT<T>* st, Red<T> red,
@@ -302,11 +375,12 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_update(int n, const T* p0, 
   const bool ok = den != T(0);
   const T alpha = ok ? st->rho1 / den : T(0);
   T* x = st->x;
+  (void)x;
   T acc[2] = {T(0), T(0)};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     T rv = r[i];
     if (ok) {
-      x[i] = fma_rn(alpha, p[i], x[i]);
+      if constexpr (!DEFER_X) x[i] = fma_rn(alpha, p[i], x[i]);
       rv = fma_rn(-alpha, q[i], rv);
       r[i] = rv;
     }
@@ -319,6 +393,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_update(int n, const T* p0, 
     const T rr = red.result[0];
     const T rz = red.result[1];
     st->bodies += 1;
+    if constexpr (DEFER_X) st->x_pending = ok ? 1 : 0;
     if (!ok) {
       // CG.h:96-104 / 131-139: converged after all, or breakdown "alpha"
       if (stop_test(st, rr)) st->iter += 1;
@@ -516,6 +591,49 @@ void pc_apply_t(ab2_context* ctx, const ab2_precond* pc, const T* x, T* y) {
   else pc_apply_f32(ctx, pc, x, y);
 }
 
+
+// Logical reduction blocks per launched block for a fused-reduction kernel
+// on a reduction grid of g blocks: 2 when the grid does not fit the GPU in
+// one wave (and halves evenly), else 1.  Asked of the runtime once per kernel.
+int red_blocks_per_sm(const void* kernel) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kCtlThreads, 0) != cudaSuccess) {
+    (void)cudaGetLastError();
+    b = 0;
+  }
+  cache[kernel] = b;
+  return b;
+}
+
+int red_virtual(const ab2_context* ctx, const void* kernel, int g) {
+  const int per_sm = red_blocks_per_sm(kernel);
+  return (per_sm > 0 && g > per_sm * ctx->num_sms && g % 2 == 0) ? 2 : 1;
+}
+
+// q = A p (and p formed) with the p.q reduction, one wave where the
+// reduction grid allows it.
+template <class View, class T>
+void launch_cgj_spmv(ab2_context* ctx, int g, int n, View view, const T* z, T* p0, T* p1, T* q, SolveStateT<T>* st,
+                     Red<T> red) {
+  if (red_virtual(ctx, (const void*)k_cgj_spmv<View, T, 1>, g) == 2)
+    k_cgj_spmv<View, T, 2><<<g / 2, kCtlThreads, 0, ctx->stream>>>(n, view, z, p0, p1, q, st, red);
+  else
+    k_cgj_spmv<View, T, 1><<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z, p0, p1, q, st, red);
+}
+
+template <class View, class T>
+void launch_cg_spmv(ab2_context* ctx, int g, int n, View view, const T* p, T* q, SolveStateT<T>* st, Red<T> red) {
+  if (red_virtual(ctx, (const void*)k_cg_spmv<View, T, 1>, g) == 2)
+    k_cg_spmv<View, T, 2><<<g / 2, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red);
+  else
+    k_cg_spmv<View, T, 1><<<g, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red);
+}
+
 }  // namespace
 
 template <class T>
@@ -545,7 +663,7 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
     if constexpr (sizeof(T) == sizeof(double)) {
       // FP64: p formed on the fly inside the SpMV (two p buffers)
       with_op([&](auto view) {
-        k_cgj_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z ? z : r, p0, p1, q, st, red_of<T>(ctx, 2));
+        launch_cgj_spmv<decltype(view), T>(ctx, g, n, view, z ? z : r, p0, p1, q, st, red_of<T>(ctx, 2));
       });
       check_launch(ctx, "cgj_spmv");
       k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p1, q, r, z, inv, stop_weight, st, red_of<T>(ctx, 3), h,
@@ -558,14 +676,14 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
       // mixed 192^3 Jacobi solve took 70.5 ms against 83.8 ms.  In FP64 the
       // split was slower (165.7 against 142.5 ms), so FP64 keeps the fused form.
       (void)p1;
-      k_cg_p<<<ge, kThreads, 0, ctx->stream>>>(n, z ? z : r, p0, st);
-      check_launch(ctx, "cg_p");
+      k_cg_px<<<ge, kThreads, 0, ctx->stream>>>(n, z ? z : r, p0, st);
+      check_launch(ctx, "cg_px");
       with_op([&](auto view) {
-        k_cg_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, p0, q, st, red_of<T>(ctx, 2));
+        launch_cg_spmv<decltype(view), T>(ctx, g, n, view, p0, q, st, red_of<T>(ctx, 2));
       });
       check_launch(ctx, "cg_spmv");
-      k_cgj_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p0, q, r, z, inv, stop_weight, st, red_of<T>(ctx, 3), h,
-                                                       graph_loop);
+      k_cgj_update<T, true><<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p0, q, r, z, inv, stop_weight, st,
+                                                                red_of<T>(ctx, 3), h, graph_loop);
     }
     check_launch(ctx, "cgj_update");
   } else if (solver == AB2_SOLVER_CG) {
@@ -578,7 +696,7 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
       // Diag body does; the same values and trees
       T* p1 = w[4];
       with_op([&](auto view) {
-        k_cgj_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z, p, p1, q, st, red_of<T>(ctx, 2));
+        launch_cgj_spmv<decltype(view), T>(ctx, g, n, view, z, p, p1, q, st, red_of<T>(ctx, 2));
       });
       check_launch(ctx, "cgj_spmv");
       k_cg_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p, p1, q, r, st, red_of<T>(ctx, 3), h, graph_loop);
@@ -586,7 +704,7 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
       k_cg_p<<<ge, kThreads, 0, ctx->stream>>>(n, z, p, st);
       check_launch(ctx, "cg_p");
       with_op([&](auto view) {
-        k_cg_spmv<<<g, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red_of<T>(ctx, 2));
+        launch_cg_spmv<decltype(view), T>(ctx, g, n, view, p, q, st, red_of<T>(ctx, 2));
       });
       check_launch(ctx, "cg_spmv");
       k_cg_update<<<g, kCtlThreads, 0, ctx->stream>>>(n, p, (const T*)nullptr, q, r, st, red_of<T>(ctx, 3), h,
@@ -709,6 +827,12 @@ void Krylov<T>::solve(const T* b, T* x, T tol, int max_iter) {
         AB2_CUDA(cudaStreamSynchronize(ctx->stream));
         if (h_st->done) break;
       }
+    }
+  }
+  if constexpr (sizeof(T) == sizeof(float)) {
+    if (fused_diag) {  // the FP32 body defers x += alpha p to the next pass: the last one is owed
+      k_cg_xfix<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, w[2], d_st);
+      check_launch(ctx, "cg_xfix");
     }
   }
   AB2_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(SolveStateT<T>), cudaMemcpyDeviceToHost, ctx->stream));

@@ -24,6 +24,7 @@ struct SolveStateT {
   int iter, max_iter;
   int first, done, converged, error, breakdown;
   int exit_fixup;  // BiCGStab exits on ||s||: x += alpha phat still to do
+  int x_pending;   // CG with the deferred x update: x += alpha p still owed
   int bodies;      // loop bodies executed (for launch accounting)
 };
 

@@ -86,4 +86,67 @@ __device__ __forceinline__ bool grid_reduce(T (&acc)[NC], T* partials, unsigned 
   return writer;
 }
 
+// The same reduction for a kernel whose logical grid of V * gridDim.x blocks
+// runs on gridDim.x blocks: block b stands for logical blocks
+// v * gridDim.x + b (v < V), reduces acc[v] exactly as that logical block
+// would (the same shuffle tree over its 256 threads) and writes its partial
+// at that logical position; the last block to arrive sums all V * gridDim.x
+// partials in logical order.  So the summation tree -- and the rounding --
+// is grid_reduce's on the logical grid, while a logical grid that does not
+// fit the GPU at once runs in one wave.
+template <int NC, int V, Combine C = Combine::Sum, class T>
+__device__ __forceinline__ bool grid_reduce_v(T (&acc)[V][NC], T* partials, unsigned int* counter, T* out) {
+  if constexpr (V == 1) {
+    return grid_reduce<NC, C, T>(acc[0], partials, counter, out);
+  } else {
+    __shared__ T s_warp[V][NC][32];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+    const int G = (int)gridDim.x * V;
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        T x = warp_reduce<C, T>(acc[v][c]);
+        if (lane == 0) s_warp[v][c][warp] = x;
+      }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          T x = lane < nwarps ? s_warp[v][c][lane] : reduce_identity<C, T>();
+          x = warp_reduce<C, T>(x);
+          if (lane == 0) partials[(size_t)c * G + v * gridDim.x + blockIdx.x] = x;
+        }
+      if (lane == 0) {
+        __threadfence();
+        unsigned int ticket = atomicAdd(counter, 1u);
+        s_last = (ticket == gridDim.x - 1);
+      }
+    }
+    __syncthreads();
+    bool writer = false;
+    if (s_last && warp == 0) {
+      __threadfence();
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        T x = reduce_identity<C, T>();
+        for (int b = lane; b < G; b += 32) x = combine<C, T>(x, __ldcg(partials + (size_t)c * G + b));
+        x = warp_reduce<C, T>(x);
+        if (lane == 0) out[c] = x;
+      }
+      if (lane == 0) {
+        *counter = 0u;
+        __threadfence();
+        writer = true;
+      }
+    }
+    return writer;
+  }
+}
+
 }  // namespace ab2

@@ -194,13 +194,17 @@ struct StencilView {
     T a[7];
     if constexpr (SYM) {
       // lower value of row r toward r - s = upper value of row r - s toward r
-      a[0] = in[0] ? __ldg(v + (kUx + 2) * N + (r - sz)) : T(0);
-      a[1] = in[1] ? __ldg(v + (kUx + 1) * N + (r - sy)) : T(0);
-      a[2] = in[2] ? __ldg(v + kUx * N + (r - sx)) : T(0);
+      // (band rows addressed as base + 32-bit row index)
+      const T* __restrict__ ux = v + kUx * N;
+      const T* __restrict__ uy = ux + N;
+      const T* __restrict__ uz = uy + N;
+      a[0] = in[0] ? __ldg(uz + (r - sz)) : T(0);
+      a[1] = in[1] ? __ldg(uy + (r - sy)) : T(0);
+      a[2] = in[2] ? __ldg(ux + (r - sx)) : T(0);
       a[3] = UNIT ? T(1) : __ldg(v + r);
-      a[4] = in[4] ? __ldg(v + kUx * N + r) : T(0);
-      a[5] = in[5] ? __ldg(v + (kUx + 1) * N + r) : T(0);
-      a[6] = in[6] ? __ldg(v + (kUx + 2) * N + r) : T(0);
+      a[4] = in[4] ? __ldg(ux + r) : T(0);
+      a[5] = in[5] ? __ldg(uy + r) : T(0);
+      a[6] = in[6] ? __ldg(uz + r) : T(0);
     } else {
 #pragma unroll
       for (int b = 0; b < 7; ++b) a[b] = in[b] ? __ldcs(v + (size_t)b * N + r) : T(0);
