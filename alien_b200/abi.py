@@ -33,6 +33,7 @@ PRECOND = {"none": 0, "diag": 1, "ilu0": 2, "cheb": 3, "filu0": 4, "neumann": 5}
 ILU_SCHEDULE = {"auto": 0, "wavefront": 1, "stencil": 2, "stencil_cluster": 3}
 BREAKDOWN = {0: None, 1: "alpha", 2: "beta", 3: "rho"}
 FCG_FALLBACK = {"sticky": 0, "step": 1}
+GNN_LAYER = {"auto": 0, "gather": 1, "grid": 2}
 MIXED_JACOBI = {"auto": 0, "plain": 1, "scaled": 2}
 COMM_ID_BYTES = 128
 
@@ -223,6 +224,8 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_gnn_create": (_I, [_P, C.POINTER(C.c_float), C.c_ulonglong, C.POINTER(_P)]),
     "ab2_gnn_get_params": (_I, [_P, C.POINTER(C.c_float)]),
     "ab2_gnn_set_params": (_I, [_P, C.POINTER(C.c_float)]),
+    "ab2_gnn_set_layer": (_I, [_P, _I]),
+    "ab2_gnn_get_layer": (_I, [_P, C.POINTER(C.c_int)]),
     "ab2_gnn_bind": (_I, [_P, _P]),
     "ab2_gnn_apply": (_I, [_P, _P, _P]),
     "ab2_gnn_loss_grad": (_I, [_P, _P, _P, _DP, C.POINTER(C.c_float)]),
@@ -1010,6 +1013,16 @@ class Gnn:
     def params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)
         self.ctx.check(lib().ab2_gnn_set_params(self.h, _fp32(p)), "gnn_set_params")
+
+    def set_layer(self, layer: str):
+        """'auto', 'gather' or 'grid' (takes effect at the next bind)."""
+        self.ctx.check(lib().ab2_gnn_set_layer(self.h, GNN_LAYER[layer]), "gnn_set_layer")
+
+    @property
+    def layer(self) -> str:
+        v = C.c_int()
+        self.ctx.check(lib().ab2_gnn_get_layer(self.h, C.byref(v)), "gnn_get_layer")
+        return next(k for k, c in GNN_LAYER.items() if c == v.value)
 
     def bind(self, A: Matrix):
         self.ctx.check(lib().ab2_gnn_bind(self.h, A.h), "gnn_bind")

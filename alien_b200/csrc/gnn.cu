@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <random>
 #include <vector>
@@ -30,7 +31,9 @@
 #include "ab2_internal.cuh"
 #include "precond.cuh"
 #include "reduce.cuh"
+#include "sentinel.cuh"
 #include "spmv_view.cuh"
+#include "tcgen05.cuh"
 
 namespace ab2 {
 namespace {
@@ -143,6 +146,27 @@ __global__ void k_gnn_nbr(int n, const int* __restrict__ rp, const int* __restri
       nb_idx[(size_t)i * nbw + w] = -1;
       nb_ef[(size_t)i * nbw + w] = 0.f;
     }
+  }
+}
+
+// The grid layer's edge features: per node (rows padded to whole 128-node
+// tiles) the feature of each direction -nx ny, -nx, -1, +1, +nx, +nx ny (the
+// CSR column order), NaN where the row has no entry there.
+__global__ void k_gnn_dir_table(int n, long long rows, int nx, int sxy, const int* __restrict__ rp,
+                                const int* __restrict__ ci, const float* __restrict__ efeat, float* __restrict__ tab) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < rows; i += (long long)gridDim.x * blockDim.x) {
+    float e[6];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) e[d] = __int_as_float(0x7fc00000);
+    if (i < n) {
+      for (int k = rp[i]; k < rp[i + 1]; ++k) {
+        const long long off = (long long)ci[k] - i;
+        const int d = off == -sxy ? 0 : off == -nx ? 1 : off == -1 ? 2 : off == 1 ? 3 : off == nx ? 4 : off == sxy ? 5 : -1;
+        if (d >= 0) e[d] = efeat[k];
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 6; ++d) tab[i * 6 + d] = e[d];
   }
 }
 
@@ -421,6 +445,277 @@ __global__ void __launch_bounds__(kLayerWarps * 32) k_gnn_layer(const LayerArgs 
     }
     __syncwarp();  // the staging rows are refilled by the next tile's copies
   }
+}
+
+// ------------------------------------------------------------------ layer on a 3-D grid (tcgen05)
+// The same layer for a matrix whose graph is a 3-D 7-point grid in
+// lexicographic order (row i + nx (j + ny k), off-diagonal columns at -nx ny,
+// -nx, -1, +1, +nx, +nx ny where inside the grid): 128 consecutive nodes a
+// tile, so each direction's neighbour rows form one contiguous block of h and
+// nothing is gathered by index.  A persistent CTA (one an SM, 512 threads)
+// walks tiles; per tile:
+//   - its inputs arrive by bulk copy (cp.async.bulk, no multicast), issued
+//     two tiles ahead into a two-stage ring: the tile's own rows with one row
+//     either side (the +-1 neighbours), the four +-nx / +-nx ny blocks, and
+//     the edge features in direction order (NaN where no neighbour);
+//   - every thread computes m = sum_d g_d h_nbr(d) for one node and two
+//     8-feature chunks (FP32, in the CSR column order, rounded to BF16 as the
+//     tensor-core aggregation of k_gnn_layer is) and writes [h ; m] as the
+//     MMA's A operand (128 x 128 BF16, 128-byte swizzle);
+//   - one thread issues eight tcgen05.mma (M = 128, N = 64, K = 16) into a
+//     128 x 64 FP32 accumulator in tensor memory; B is W (64 x 128 BF16),
+//     staged once per CTA;
+//   - the 16 warps read the accumulator (tcgen05.ld: a lane quarter x 16
+//     columns each), add the bias, relu, round to BF16 and stage the rows in
+//     shared memory (swizzled: no bank conflicts), then all threads store
+//     them with coalesced 16-byte writes; LAST applies the decoder.
+// Every wait is bounded: on expiry the kernel sets *err, takes no further
+// tile, waits (bounded) for the copies and the MMA it issued, frees its
+// tensor memory and returns.
+constexpr int kTcThreads = 512;
+constexpr int kTcTile = 128;
+constexpr unsigned kTcRowB = kH * 2;                         // bytes of one h row
+constexpr unsigned kTcW = 0;                                 // B: 2 regions x 64 rows x 128 B
+constexpr unsigned kTcA = kTcW + 2 * kH * kTcRowB;           // A: 2 regions x 128 rows x 128 B
+constexpr unsigned kTcARegion = kTcTile * kTcRowB;
+constexpr unsigned kTcStage0 = kTcA + 2 * kTcARegion;
+constexpr unsigned kTcXOff = 0;                              // rows b-1 .. b+128
+constexpr unsigned kTcYmOff = kTcXOff + (kTcTile + 2) * kTcRowB;
+constexpr unsigned kTcYpOff = kTcYmOff + kTcARegion;
+constexpr unsigned kTcZmOff = kTcYpOff + kTcARegion;
+constexpr unsigned kTcZpOff = kTcZmOff + kTcARegion;
+constexpr unsigned kTcEfOff = kTcZpOff + kTcARegion;         // 128 x 6 floats
+constexpr unsigned kTcEfBytes = kTcTile * 6 * 4;
+constexpr unsigned kTcStageB = kTcEfOff + kTcEfBytes;
+constexpr unsigned kTcStage1 = kTcStage0 + kTcStageB;
+constexpr unsigned kTcY = kTcStage1 + kTcStageB;             // decoder partials, 4 x 128 floats
+constexpr unsigned kTcBias = kTcY + 4 * kTcTile * 4;         // bias, wd: 2 x 64 floats
+constexpr unsigned kTcBar = kTcBias + 2 * kH * 4;            // 3 mbarriers, tensor-memory address, abort flag
+constexpr unsigned kTcSmem = kTcBar + 32 + 1024;             // + slack to align the base to 1024 bytes
+static_assert(kTcSmem <= 227 * 1024, "grid layer: shared memory");
+static_assert(kTcStage0 % 1024 == 0 && kTcA % 1024 == 0 && kTcStageB % 16 == 0, "grid layer: alignment");
+
+struct GridLayerArgs {
+  LayerArgs a;
+  int nx, sxy;           // grid strides along j and k
+  const float* dir_ef;   // [ceil(n/128) * 128][6] edge features by direction, NaN = none
+  int* err;              // set when a bounded wait gives up
+};
+
+template <bool LAST>
+__global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLayerArgs ga) {
+  const LayerArgs& a = ga.a;
+  extern __shared__ unsigned char tc_smem_raw[];
+  unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) &
+                                                       ~static_cast<uintptr_t>(1023));
+  const unsigned sb = tc::smem_u32(sm);
+  float* s_y = reinterpret_cast<float*>(sm + kTcY);
+  float* s_bias = reinterpret_cast<float*>(sm + kTcBias);
+  float* s_wd = s_bias + kH;
+  volatile unsigned* s_tmem = reinterpret_cast<volatile unsigned*>(sm + kTcBar + 24);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kTcBar + 28);
+  const unsigned bar_in0 = sb + kTcBar, bar_mma = sb + kTcBar + 16;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n = a.n;
+  const int ntiles = (n + kTcTile - 1) / kTcTile;
+  const int count = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+  // W as the B operand (row o = output feature, K-major, 128-byte swizzle)
+  for (int t = tid; t < kH * kIn / 8; t += kTcThreads) {
+    const int o = t >> 4, reg = (t >> 3) & 1, c = t & 7;
+    *reinterpret_cast<uint4*>(sm + kTcW + reg * (kH * kTcRowB) + o * kTcRowB + ((c ^ (o & 7)) << 4)) =
+        reinterpret_cast<const uint4*>(a.W)[t];
+  }
+  for (int t = tid; t < kH; t += kTcThreads) {
+    s_bias[t] = a.P[kOffB + a.layer * kH + t];
+    s_wd[t] = a.P[kOffWd + t];
+  }
+  if (tid == 0) {
+    tc::mbar_init(bar_in0, 1);
+    tc::mbar_init(bar_in0 + 8, 1);
+    tc::mbar_init(bar_mma, 1);
+    *s_abort = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(sb + kTcBar + 24, 64);
+    tc::tmem_relinquish();
+  }
+  tc::fence_proxy_async_smem();  // W (generic stores) is read by the tensor core
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const unsigned tmem = *s_tmem;
+
+  // thread 0: the inputs of the c-th tile of this CTA into stage s
+  auto issue = [&](int c, int s) {
+    const long long b = (long long)((int)blockIdx.x + c * (int)gridDim.x) * kTcTile;
+    const unsigned st = sb + (s ? kTcStage1 : kTcStage0);
+    const long long first[5] = {b - 1, b - ga.nx, b + ga.nx, b - ga.sxy, b + ga.sxy};
+    const int rows[5] = {kTcTile + 2, kTcTile, kTcTile, kTcTile, kTcTile};
+    const unsigned dst[5] = {kTcXOff, kTcYmOff, kTcYpOff, kTcZmOff, kTcZpOff};
+    long long lo[5], hi[5];
+    unsigned bytes = kTcEfBytes;
+    for (int q = 0; q < 5; ++q) {
+      lo[q] = first[q] < 0 ? 0 : first[q];
+      hi[q] = first[q] + rows[q] > n ? n : first[q] + rows[q];
+      if (hi[q] > lo[q]) bytes += (unsigned)(hi[q] - lo[q]) * kTcRowB;
+    }
+    tc::mbar_expect_tx(bar_in0 + 8 * s, bytes);
+    for (int q = 0; q < 5; ++q)
+      if (hi[q] > lo[q])
+        tc::bulk_g2s(st + dst[q] + (unsigned)(lo[q] - first[q]) * kTcRowB, a.h_in + lo[q] * kH,
+                     (unsigned)(hi[q] - lo[q]) * kTcRowB, bar_in0 + 8 * s);
+    tc::bulk_g2s(st + kTcEfOff, ga.dir_ef + b * 6, kTcEfBytes, bar_in0 + 8 * s);
+  };
+  // thread 0's record of what is in flight: the parity of stage s's
+  // unawaited phase (-1: none), and of the MMA's
+  int pend[2] = {-1, -1};
+  int mma_pend = -1;
+  if (tid == 0) {
+    for (int c = 0; c < 2 && c < count; ++c) {
+      issue(c, c);
+      pend[c] = 0;
+    }
+  }
+
+  const float u = a.P[kOffU + a.layer], cg = a.P[kOffC + a.layer];
+  const int ln = tid >> 2, qq = tid & 3;        // aggregation: node ln, chunks qq and qq + 4
+  const int eq = warp & 3, ecg = warp >> 2;     // epilogue: lanes 32 eq .., columns 16 ecg ..
+  const int erow = 32 * eq + lane;
+  for (int c = 0; c < count; ++c) {
+    const int s = c & 1;
+    const long long b = (long long)((int)blockIdx.x + c * (int)gridDim.x) * kTcTile;
+    const unsigned char* stg = sm + (s ? kTcStage1 : kTcStage0);
+    int failed = 0;  // this thread's bounded wait gave up (the barriers OR it over the CTA)
+    if (!tc::mbar_wait(bar_in0 + 8 * s, (unsigned)(c >> 1) & 1u, kWaitCycles, s_abort)) {
+      failed = 1;
+      *s_abort = 1;
+      atomicOr(ga.err, 1);
+    } else if (tid == 0) {
+      pend[s] = -1;
+    }
+    // ---- aggregation: m for node ln, chunks qq and qq + 4; [h ; m] into A
+    {
+      const long long gi = b + ln;
+      const float* efr = reinterpret_cast<const float*>(stg + kTcEfOff) + ln * 6;
+      float g[6];
+      bool pr[6];
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        const float e = efr[d];
+        pr[d] = e == e;
+        g[d] = pr[d] ? bf16r(sigmoidf(fmaf(u, e, cg))) : 0.f;
+      }
+      const unsigned char* src[6] = {stg + kTcZmOff + ln * kTcRowB, stg + kTcYmOff + ln * kTcRowB,
+                                     stg + kTcXOff + ln * kTcRowB, stg + kTcXOff + (ln + 2) * kTcRowB,
+                                     stg + kTcYpOff + ln * kTcRowB, stg + kTcZpOff + ln * kTcRowB};
+      const unsigned char* own = stg + kTcXOff + (ln + 1) * kTcRowB;
+#pragma unroll
+      for (int jj = 0; jj < 2; ++jj) {
+        const int ch = 4 * ((ln & 1) ^ jj) + qq;  // the 8 threads of a quarter-warp touch 8 distinct banks
+        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int d = 0; d < 6; ++d) {
+          if (pr[d]) {
+            const uint4 w = *reinterpret_cast<const uint4*>(src[d] + ch * 16);
+            const unsigned wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              acc[2 * e] = fmaf(g[d], __uint_as_float(wv[e] << 16), acc[2 * e]);
+              acc[2 * e + 1] = fmaf(g[d], __uint_as_float(wv[e] & 0xffff0000u), acc[2 * e + 1]);
+            }
+          }
+        }
+        const uint4 hv = gi < n ? *reinterpret_cast<const uint4*>(own + ch * 16) : make_uint4(0u, 0u, 0u, 0u);
+        const unsigned pos = ln * kTcRowB + ((ch ^ (ln & 7)) << 4);
+        *reinterpret_cast<uint4*>(sm + kTcA + pos) = hv;
+        *reinterpret_cast<uint4*>(sm + kTcA + kTcARegion + pos) = pack8(acc);
+      }
+    }
+    tc::fence_proxy_async_smem();
+    if (__syncthreads_or(failed)) break;  // (1) A complete; the stage's inputs consumed
+    if (tid == 0) {
+      if (c + 2 < count) {
+        issue(c + 2, s);
+        pend[s] = ((c + 2) >> 1) & 1;
+      }
+      tc::fence_after_sync();
+      constexpr uint32_t idesc = tc::idesc_bf16_f32(kTcTile, kH);
+#pragma unroll
+      for (int k = 0; k < kIn / 16; ++k) {
+        const unsigned aoff = (k >> 2) * kTcARegion + (k & 3) * 32, boff = (k >> 2) * (kH * kTcRowB) + (k & 3) * 32;
+        tc::mma_bf16_ss(tmem, tc::sdesc_sw128(sb + kTcA + aoff), tc::sdesc_sw128(sb + kTcW + boff), idesc, k > 0);
+      }
+      tc::mma_commit(bar_mma);
+      mma_pend = c & 1;
+    }
+    if (!tc::mbar_wait(bar_mma, (unsigned)c & 1u, kWaitCycles, s_abort)) {
+      failed = 1;
+      *s_abort = 1;
+      atomicOr(ga.err, 1);
+    } else if (tid == 0) {
+      mma_pend = -1;
+    }
+    tc::fence_after_sync();
+    // ---- epilogue: bias, relu, BF16; rows staged in A's first region (the
+    // MMA has read it), swizzled
+    {
+      float v[16];
+      tc::tmem_ld16(tmem + ((unsigned)(32 * eq) << 16) + 16 * ecg, v);
+      float hb[16];
+      float y = 0.f;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        hb[j] = bf16r(fmaxf(v[j] + s_bias[16 * ecg + j], 0.f));
+        if constexpr (LAST) y = fmaf(s_wd[16 * ecg + j], hb[j], y);
+      }
+      if (a.h_out) {
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+          const int ch = 2 * ecg + h2;
+          float f8[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) f8[e] = hb[8 * h2 + e];
+          *reinterpret_cast<uint4*>(sm + kTcA + erow * kTcRowB + ((ch ^ (erow & 7)) << 4)) = pack8(f8);
+        }
+      }
+      if constexpr (LAST) s_y[ecg * kTcTile + erow] = y;
+    }
+    tc::fence_before_sync();
+    __syncthreads();  // (2) staged rows, decoder partials
+    // ---- coalesced stores: 16 bytes a thread, 8 threads a row
+    for (int idx = tid; idx < kTcTile * 8; idx += kTcThreads) {
+      const int row = idx >> 3, ch = idx & 7;
+      const long long gi = b + row;
+      if (gi < n) {
+        const unsigned pos = row * kTcRowB + ((ch ^ (row & 7)) << 4);
+        if (a.h_out) reinterpret_cast<uint4*>(a.h_out + gi * kH)[ch] = *reinterpret_cast<const uint4*>(sm + kTcA + pos);
+        if (a.m_out)
+          reinterpret_cast<uint4*>(a.m_out + gi * kH)[ch] =
+              *reinterpret_cast<const uint4*>(sm + kTcA + kTcARegion + pos);
+      }
+    }
+    if constexpr (LAST) {
+      if (tid < kTcTile && b + tid < n) {
+        const long long gi = b + tid;
+        const float y = ((s_y[tid] + s_y[kTcTile + tid]) + s_y[2 * kTcTile + tid]) + s_y[3 * kTcTile + tid];
+        const double s = a.s2[0], is = a.s2[1];
+        const float bd = a.P[kOffBd], ws = a.P[kOffWs];
+        a.z[gi] = s * (double)(y + bd + ws * (float)(a.xr[gi] * is)) * (double)a.isd[gi];
+      }
+    }
+    if (__syncthreads_or(failed)) break;  // (3) A and the partials free for the next tile
+  }
+  // ---- drain: no copy or MMA of this CTA may still be in flight at exit
+  if (tid == 0) {
+    for (int s = 0; s < 2; ++s)
+      if (pend[s] >= 0) tc::mbar_wait(bar_in0 + 8 * s, (unsigned)pend[s], kWaitCycles, nullptr);
+    if (mma_pend >= 0) tc::mbar_wait(bar_mma, (unsigned)mma_pend, kWaitCycles, nullptr);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 64);
 }
 
 // h1 = relu(W0 x0 + b0), x0 = [xr / s, log(a_ii)/10]: 8 lanes per node, 8 features a lane.
@@ -806,6 +1101,13 @@ struct ab2_gnn {
   float* d_part = nullptr;
   float* d_red = nullptr;    // reduced partials scratch (64 x 128 + 64)
   long long part_cap = 0;
+  // the layer kernel: AB2_GNN_LAYER_* requested, and whether the bound
+  // matrix's graph is a 3-D 7-point grid (then the grid layer's inputs)
+  int layout = AB2_GNN_LAYER_AUTO;
+  bool grid = false;
+  int gnx = 0, gny = 0, gnz = 0;
+  float* d_dir_ef = nullptr;  // [ceil(n/128) 128][6] edge features by direction
+  int* d_err = nullptr;       // set by the grid layer when a bounded wait gives up
 };
 
 namespace ab2 {
@@ -825,8 +1127,12 @@ void release_binding(ab2_gnn* G) {
   for (void* p : {(void*)G->d_isd, (void*)G->d_logd10, (void*)G->d_efeat, (void*)G->d_tidx, (void*)G->d_h,
                   (void*)G->d_m, (void*)G->d_xr, (void*)G->d_s2, (void*)G->d_dh, (void*)G->d_dh2, (void*)G->d_dm,
                   (void*)G->d_z, (void*)G->d_d, (void*)G->d_Ad, (void*)G->d_Ae, (void*)G->d_part, (void*)G->d_red,
-                  (void*)G->d_nb_idx, (void*)G->d_nb_ef})
+                  (void*)G->d_nb_idx, (void*)G->d_nb_ef, (void*)G->d_dir_ef, (void*)G->d_err})
     dev_free(ctx, p);
+  G->d_dir_ef = nullptr;
+  G->d_err = nullptr;
+  G->grid = false;
+  G->gnx = G->gny = G->gnz = 0;
   G->d_nb_idx = nullptr;
   G->d_nb_ef = nullptr;
   G->nbw = 0;
@@ -862,6 +1168,35 @@ void launch_layer(ab2_context* ctx, const LayerArgs& la) {
   check_launch(ctx, "gnn_layer");
 }
 
+template <bool LAST>
+void launch_layer_grid(ab2_context* ctx, const GridLayerArgs& ga) {
+  static thread_local int configured_device = -1;
+  if (configured_device != ctx->device) {
+    AB2_CUDA(cudaFuncSetAttribute(k_gnn_layer_grid<LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    configured_device = ctx->device;
+  }
+  const int ntiles = (ga.a.n + kTcTile - 1) / kTcTile;
+  const int grid = std::max(1, std::min(ntiles, ctx->num_sms));
+  k_gnn_layer_grid<LAST><<<grid, kTcThreads, kTcSmem, ctx->stream>>>(ga);
+  check_launch(ctx, "gnn_layer_grid");
+}
+
+bool use_grid_layer(const ab2_gnn* G) { return G->grid && G->layout != AB2_GNN_LAYER_GATHER; }
+
+// A bounded wait of the grid layer gave up (its outputs are then garbage):
+// AB2_ERR_TIMEOUT, the flag cleared for the next call.  Synchronises.
+void check_grid_wait(ab2_gnn* G) {
+  if (!G->d_err) return;
+  ab2_context* ctx = G->ctx;
+  int e = 0;
+  AB2_CUDA(cudaMemcpyAsync(&e, G->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  AB2_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (e) {
+    AB2_CUDA(cudaMemsetAsync(G->d_err, 0, sizeof(int), ctx->stream));
+    throw Error{AB2_ERR_TIMEOUT, "learned preconditioner: a bounded wait of the grid layer gave up"};
+  }
+}
+
 // z = network(r) (FP64 in and out).  training: keep m1..m4 and h5 for the
 // backward pass (h1..h4 are always written).
 void gnn_forward(ab2_gnn* G, const double* r, double* z, bool training = false) {
@@ -890,8 +1225,15 @@ void gnn_forward(ab2_gnn* G, const double* r, double* z, bool training = false) 
     la.m_out = training ? mbuf(G, l) : nullptr;
     la.h_out = (training || l + 1 < kLayers) ? hbuf(G, l + 1) : nullptr;
     la.z = l + 1 == kLayers ? z : nullptr;
-    if (l + 1 < kLayers) launch_layer<false>(ctx, la);
-    else launch_layer<true>(ctx, la);
+    if (use_grid_layer(G)) {
+      const GridLayerArgs ga{la, G->gnx, G->gnx * G->gny, G->d_dir_ef, G->d_err};
+      if (l + 1 < kLayers) launch_layer_grid<false>(ctx, ga);
+      else launch_layer_grid<true>(ctx, ga);
+    } else if (l + 1 < kLayers) {
+      launch_layer<false>(ctx, la);
+    } else {
+      launch_layer<true>(ctx, la);
+    }
   }
 }
 
@@ -947,6 +1289,7 @@ double gnn_loss_grad(ab2_gnn* G, const double* r, const double* e) {
   k_gnn_encode_bwd<<<wg, 256, 0, ctx->stream>>>(n, G->d_xr, G->d_s2, G->d_logd10, hbuf(G, 0), dh, G->d_part);
   check_launch(ctx, "gnn_encode_bwd");
   reduce_into(G, wg, 3 * kH, G->d_grad + kOffW0);
+  check_grid_wait(G);
   return dAd / eAe;
 }
 
@@ -1067,6 +1410,23 @@ int ab2_gnn_bind(ab2_gnn* G, const ab2_matrix* A) {
       k_gnn_nbr<<<grid_for(n), kThreads, 0, ctx->stream>>>(n, A->d_rp, A->d_ci, G->d_efeat, G->nbw, G->d_nb_idx,
                                                            G->d_nb_ef);
       check_launch(ctx, "gnn_nbr");
+      int nx = 0, ny = 0, nz = 0;
+      G->grid = stencil_geometry(ctx, A, &nx, &ny, &nz);
+      if (G->grid) {
+        G->gnx = nx;
+        G->gny = ny;
+        G->gnz = nz;
+        const long long rows = ((long long)n + kTcTile - 1) / kTcTile * kTcTile;
+        G->d_dir_ef = dev_alloc<float>(ctx, (size_t)rows * 6);
+        G->d_err = dev_alloc<int>(ctx, 1);
+        AB2_CUDA(cudaMemsetAsync(G->d_err, 0, sizeof(int), ctx->stream));
+        k_gnn_dir_table<<<grid_for(rows), kThreads, 0, ctx->stream>>>(n, rows, nx, nx * ny, A->d_rp, A->d_ci,
+                                                                      G->d_efeat, G->d_dir_ef);
+        check_launch(ctx, "gnn_dir_table");
+      } else if (G->layout == AB2_GNN_LAYER_GRID) {
+        release_binding(G);
+        throw Error{AB2_ERR_UNSUPPORTED, "learned preconditioner: the grid layer needs a 3-D 7-point matrix"};
+      }
     }
     if (bad) {
       release_binding(G);
@@ -1076,10 +1436,25 @@ int ab2_gnn_bind(ab2_gnn* G, const ab2_matrix* A) {
   });
 }
 
+int ab2_gnn_set_layer(ab2_gnn* G, int layer) {
+  if (!G || layer < AB2_GNN_LAYER_AUTO || layer > AB2_GNN_LAYER_GRID) return AB2_ERR_BAD_ARG;
+  G->layout = layer;
+  return AB2_OK;
+}
+
+int ab2_gnn_get_layer(const ab2_gnn* G, int* layer) {
+  if (!G || !layer) return AB2_ERR_BAD_ARG;
+  *layer = !G->A ? AB2_GNN_LAYER_AUTO : use_grid_layer(G) ? AB2_GNN_LAYER_GRID : AB2_GNN_LAYER_GATHER;
+  return AB2_OK;
+}
+
 int ab2_gnn_apply(ab2_gnn* G, const ab2_vector* r, ab2_vector* z) {
   if (!G || !r || !z || !G->A || r->n != G->n || z->n != G->n || r->d == z->d) return AB2_ERR_BAD_ARG;
   PhaseScope phase_scope(G->ctx, "GNN-APPLY");
-  return guard(G->ctx, [&] { gnn_forward(G, r->d, z->d); });
+  return guard(G->ctx, [&] {
+    gnn_forward(G, r->d, z->d);
+    check_grid_wait(G);
+  });
 }
 
 int ab2_gnn_loss_grad(ab2_gnn* G, const ab2_vector* r, const ab2_vector* e, double* loss, float* grad) {
@@ -1264,6 +1639,7 @@ int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* G, const ab2_p
     dev_free(ctx, zq_counter);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (G) check_grid_wait(G);
   });
 }
 

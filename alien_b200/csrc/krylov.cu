@@ -247,6 +247,111 @@ __global__ void __launch_bounds__(kCtlThreads) k_cg_spmv(int n, View A, const T*
   if (grid_reduce_v<1, VB>(acc, red.partials, red.counter, red.result)) st->den = red.result[0];
 }
 
+// k_cg_spmv for FP32 7-point bands in their symmetric form (StencilView<float,
+// true, UNIT>), four consecutive rows of one grid line a thread: 16-byte loads
+// of p, the bands and q, the row coordinates divided out once per four rows,
+// and two sweeps' loads in flight before either is used (one row a thread,
+// FP32 moves half the bytes of FP64 per load and the kernel waited on memory
+// latency at 0.56 of HBM bandwidth).  Needs nx % 4 == 0 (so the four rows
+// share j and k, and p +- nx, +- nx ny stay 16-byte aligned).  Each row sums
+// the terms of StencilView::row_f in the same order, so q is bit-identical;
+// the rows of logical thread g of the G-block reduction grid are k_cg_spmv's
+// (g, g + 256 G, ...), thread t carries logical threads 4t .. 4t + 3 (their
+// sweeps in order), and grid_reduce_r reduces their p.q partials with
+// k_cg_spmv's tree.
+struct BandRows4 {  // one sweep of a thread: four rows' operands
+  float4 pc, uxc, pym, uym, pyp, uyc, pzm, uzm, pzp, uzc, dg;
+  float pl, uxl, pr;
+  int r0;
+  bool xl, xr, ym, yp, zm, zp;
+};
+
+template <bool UNIT>
+__device__ __forceinline__ BandRows4 band_rows4_load(const StencilView<float, true, UNIT>& A, const float* __restrict__ p,
+                                                     const float* __restrict__ ux, const float* __restrict__ uy,
+                                                     const float* __restrict__ uz, int r0) {
+  auto ld4 = [](const float* a) { return __ldg(reinterpret_cast<const float4*>(a)); };
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int nx = A.nx, ny = A.ny, nz = A.nz, sy = nx, sz = nx * ny;
+  BandRows4 o;
+  o.r0 = r0;
+  const unsigned qq = A.fx.div((unsigned)r0);
+  const int i0 = r0 - (int)qq * nx;
+  const int k = (int)A.fy.div(qq);
+  const int j = (int)qq - k * ny;
+  o.xl = i0 > 0;
+  o.xr = i0 + 4 < nx;
+  o.ym = j > 0;
+  o.yp = j < ny - 1;
+  o.zm = k > 0;
+  o.zp = k < nz - 1;
+  o.pc = ld4(p + r0);
+  o.uxc = ld4(ux + r0);
+  o.pl = o.xl ? __ldg(p + r0 - 1) : 0.f;
+  o.uxl = o.xl ? __ldg(ux + r0 - 1) : 0.f;
+  o.pr = o.xr ? __ldg(p + r0 + 4) : 0.f;
+  o.pym = o.ym ? ld4(p + r0 - sy) : z4;
+  o.uym = o.ym ? ld4(uy + r0 - sy) : z4;
+  o.pyp = o.yp ? ld4(p + r0 + sy) : z4;
+  o.uyc = o.yp ? ld4(uy + r0) : z4;
+  o.pzm = o.zm ? ld4(p + r0 - sz) : z4;
+  o.uzm = o.zm ? ld4(uz + r0 - sz) : z4;
+  o.pzp = o.zp ? ld4(p + r0 + sz) : z4;
+  o.uzc = o.zp ? ld4(uz + r0) : z4;
+  o.dg = UNIT ? make_float4(1.f, 1.f, 1.f, 1.f) : ld4(A.v + r0);
+  return o;
+}
+
+// q for the four rows (stored) and their p.q terms added to acc[u][0].
+__device__ __forceinline__ void band_rows4_sum(const BandRows4& o, float* __restrict__ q, float (&acc)[4][1]) {
+  const float P[6] = {o.pl, o.pc.x, o.pc.y, o.pc.z, o.pc.w, o.pr};  // p at i0 - 1 .. i0 + 4
+  const float UX[5] = {o.uxl, o.uxc.x, o.uxc.y, o.uxc.z, o.uxc.w};  // ux at r0 - 1 .. r0 + 3
+  const float PYM[4] = {o.pym.x, o.pym.y, o.pym.z, o.pym.w}, UYM[4] = {o.uym.x, o.uym.y, o.uym.z, o.uym.w};
+  const float PYP[4] = {o.pyp.x, o.pyp.y, o.pyp.z, o.pyp.w}, UYC[4] = {o.uyc.x, o.uyc.y, o.uyc.z, o.uyc.w};
+  const float PZM[4] = {o.pzm.x, o.pzm.y, o.pzm.z, o.pzm.w}, UZM[4] = {o.uzm.x, o.uzm.y, o.uzm.z, o.uzm.w};
+  const float PZP[4] = {o.pzp.x, o.pzp.y, o.pzp.z, o.pzp.w}, UZC[4] = {o.uzc.x, o.uzc.y, o.uzc.z, o.uzc.w};
+  const float DG[4] = {o.dg.x, o.dg.y, o.dg.z, o.dg.w};
+  float qv[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    float a = 0.f;
+    if (o.zm) a = mul_add_rn(UZM[u], PZM[u], a);
+    if (o.ym) a = mul_add_rn(UYM[u], PYM[u], a);
+    if (u > 0 || o.xl) a = mul_add_rn(UX[u], P[u], a);
+    a = mul_add_rn(DG[u], P[u + 1], a);
+    if (u < 3 || o.xr) a = mul_add_rn(UX[u + 1], P[u + 2], a);
+    if (o.yp) a = mul_add_rn(UYC[u], PYP[u], a);
+    if (o.zp) a = mul_add_rn(UZC[u], PZP[u], a);
+    qv[u] = a;
+    acc[u][0] = fma_rn(a, P[u + 1], acc[u][0]);
+  }
+  *reinterpret_cast<float4*>(q + o.r0) = make_float4(qv[0], qv[1], qv[2], qv[3]);
+}
+
+template <bool UNIT>
+__global__ void __launch_bounds__(kCtlThreads) k_cg_spmv_x4(int n, StencilView<float, true, UNIT> A,
+                                                            const float* __restrict__ p, float* __restrict__ q,
+                                                            SolveStateT<float>* st, Red<float> red, int G) {
+  const int S = G * kCtlThreads;  // rows per sweep of the logical grid
+  const int t4 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const size_t N = (size_t)n;
+  const float* __restrict__ ux = A.v + (UNIT ? 0 : N);
+  const float* __restrict__ uy = ux + N;
+  const float* __restrict__ uz = uy + N;
+  float acc[4][1] = {{0.f}, {0.f}, {0.f}, {0.f}};
+  if (t4 < S) {
+    for (int r0 = t4; r0 < n; r0 += 2 * S) {
+      const bool two = r0 + S < n;
+      const BandRows4 a = band_rows4_load(A, p, ux, uy, uz, r0);
+      BandRows4 b;
+      if (two) b = band_rows4_load(A, p, ux, uy, uz, r0 + S);
+      band_rows4_sum(a, q, acc);
+      if (two) band_rows4_sum(b, q, acc);
+    }
+  }
+  if (grid_reduce_r<1, 4>(acc, G, red.partials, red.counter, red.result)) st->den = red.result[0];
+}
+
 // alpha = rho1/den ; x += alpha p ; r -= alpha q ; then the loop's stop test on r.
 // p1 != nullptr: p is double-buffered (k_cgj_spmv formed it), and the buffer
 // it wrote is p0 or p1 by the body count's parity.
@@ -355,6 +460,34 @@ __global__ void __launch_bounds__(kCtlThreads) k_cgj_spmv(int n, View A, const T
   if (grid_reduce_v<1, VB>(acc, red.partials, red.counter, red.result)) st->den = red.result[0];
 }
 
+// The scalar part of a Jacobi-CG update, in the last block: the state after
+// r.r = rr and r.z = rz (CG.h:96-139).
+template <class T, bool DEFER_X>
+__device__ __forceinline__ void cgj_update_scalars(SolveStateT<T>* st, T rr, T rz, bool ok, T alpha,
+                                                   cudaGraphConditionalHandle h, int use_graph) {
+  st->bodies += 1;
+  if constexpr (DEFER_X) st->x_pending = ok ? 1 : 0;
+  if (!ok) {
+    // CG.h:96-104 / 131-139: converged after all, or breakdown "alpha"
+    if (stop_test(st, rr)) st->iter += 1;
+    else {
+      st->error = AB2_ERR_BREAKDOWN;
+      st->breakdown = AB2_BREAKDOWN_ALPHA;
+    }
+    st->done = 1;
+  } else {
+    st->alpha = alpha;
+    st->rho = st->rho1;
+    st->iter += 1;
+    st->first = 0;
+    // the next iteration's rho1 = r.z and beta = rho1 / rho (CG.h:117-118)
+    st->rho1 = rz;
+    st->beta = rz / st->rho;
+    if (stop_test(st, rr)) st->done = 1;
+  }
+  set_loop(h, use_graph, !st->done);
+}
+
 // alpha = rho1/den ; x += alpha p ; r -= alpha q ; z = D^-1 r ; r.r (stop test) and r.z (next rho1).
 // inv = nullptr: z = r, not stored (z may be null).  w: the stop test sums
 // (r_i w_i) r_i instead (the scaled Jacobi form's unscaled residual norm).
@@ -389,31 +522,91 @@ __global__ void __launch_bounds__(kCtlThreads, 8) k_cgj_update(int n, const T* p
     if (inv) z[i] = zv;
     acc[1] = fma_rn(rv, zv, acc[1]);
   }
-  if (grid_reduce<2>(acc, red.partials, red.counter, red.result)) {
-    const T rr = red.result[0];
-    const T rz = red.result[1];
-    st->bodies += 1;
-    if constexpr (DEFER_X) st->x_pending = ok ? 1 : 0;
-    if (!ok) {
-      // CG.h:96-104 / 131-139: converged after all, or breakdown "alpha"
-      if (stop_test(st, rr)) st->iter += 1;
-      else {
-        st->error = AB2_ERR_BREAKDOWN;
-        st->breakdown = AB2_BREAKDOWN_ALPHA;
-      }
-      st->done = 1;
-    } else {
-      st->alpha = alpha;
-      st->rho = st->rho1;
-      st->iter += 1;
-      st->first = 0;
-      // the next iteration's rho1 = r.z and beta = rho1 / rho (CG.h:117-118)
-      st->rho1 = rz;
-      st->beta = rz / st->rho;
-      if (stop_test(st, rr)) st->done = 1;
-    }
-    set_loop(h, use_graph, !st->done);
+  if (grid_reduce<2>(acc, red.partials, red.counter, red.result))
+    cgj_update_scalars<T, DEFER_X>(st, red.result[0], red.result[1], ok, alpha, h, use_graph);
+}
+
+// k_cgj_update<float> for n % 4 == 0: four consecutive elements a thread
+// (16-byte accesses).  Logical thread g of the G-block reduction grid owns
+// elements g, g + 256 G, ... as in k_cgj_update; thread t carries logical
+// threads 4t .. 4t + 3, and grid_reduce_r sums their r.r and r.z partials
+// with k_cgj_update's tree, so every value and scalar is bit-identical.
+template <bool DEFER_X>
+__global__ void __launch_bounds__(kCtlThreads) k_cgj_update_x4(int n, const float* p0, const float* p1,
+                                                               const float* __restrict__ q, float* __restrict__ r,
+                                                               float* __restrict__ z, const float* __restrict__ inv,
+                                                               const float* __restrict__ w, SolveStateT<float>* st,
+                                                               Red<float> red, cudaGraphConditionalHandle h,
+                                                               int use_graph, int G) {
+  if (st->done) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(h, use_graph, 0);
+    return;
   }
+  const float* __restrict__ p = (st->bodies & 1) ? p0 : p1;
+  const float den = st->den;
+  const bool ok = den != 0.f;
+  const float alpha = ok ? st->rho1 / den : 0.f;
+  float* x = st->x;
+  (void)x;
+  (void)p;
+  const int S = G * kCtlThreads;
+  const int t4 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  float acc[4][2] = {};
+  auto ld4 = [](const float* a) { return *reinterpret_cast<const float4*>(a); };
+  if (t4 < S) {
+    for (int i = t4; i < n; i += 2 * S) {
+      const bool two = i + S < n;
+      const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 rv[2] = {z4, z4}, qv[2] = {z4, z4}, wv[2] = {z4, z4}, iv[2] = {z4, z4}, pv[2] = {z4, z4},
+             xv[2] = {z4, z4};
+#pragma unroll
+      for (int h2 = 0; h2 < 2; ++h2) {
+        if (h2 == 1 && !two) break;
+        const int e = i + h2 * S;
+        rv[h2] = ld4(r + e);
+        if (ok) {
+          qv[h2] = ld4(q + e);
+          if constexpr (!DEFER_X) {
+            pv[h2] = ld4(p + e);
+            xv[h2] = ld4(x + e);
+          }
+        }
+        if (w) wv[h2] = ld4(w + e);
+        if (inv) iv[h2] = ld4(inv + e);
+      }
+#pragma unroll
+      for (int h2 = 0; h2 < 2; ++h2) {
+        if (h2 == 1 && !two) break;
+        const int e = i + h2 * S;
+        float R[4] = {rv[h2].x, rv[h2].y, rv[h2].z, rv[h2].w};
+        const float Q[4] = {qv[h2].x, qv[h2].y, qv[h2].z, qv[h2].w};
+        const float W4[4] = {wv[h2].x, wv[h2].y, wv[h2].z, wv[h2].w};
+        const float I4[4] = {iv[h2].x, iv[h2].y, iv[h2].z, iv[h2].w};
+        float Z[4];
+        if (ok) {
+          if constexpr (!DEFER_X) {
+            const float P4[4] = {pv[h2].x, pv[h2].y, pv[h2].z, pv[h2].w};
+            float X[4] = {xv[h2].x, xv[h2].y, xv[h2].z, xv[h2].w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) X[u] = fma_rn(alpha, P4[u], X[u]);
+            *reinterpret_cast<float4*>(x + e) = make_float4(X[0], X[1], X[2], X[3]);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) R[u] = fma_rn(-alpha, Q[u], R[u]);
+          *reinterpret_cast<float4*>(r + e) = make_float4(R[0], R[1], R[2], R[3]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          acc[u][0] = fma_rn(w ? mul_rn(R[u], W4[u]) : R[u], R[u], acc[u][0]);
+          Z[u] = inv ? mul_rn(I4[u], R[u]) : R[u];
+          acc[u][1] = fma_rn(R[u], Z[u], acc[u][1]);
+        }
+        if (inv) *reinterpret_cast<float4*>(z + e) = make_float4(Z[0], Z[1], Z[2], Z[3]);
+      }
+    }
+  }
+  if (grid_reduce_r<2, 4>(acc, G, red.partials, red.counter, red.result))
+    cgj_update_scalars<float, DEFER_X>(st, red.result[0], red.result[1], ok, alpha, h, use_graph);
 }
 
 // ------------------------------------------------------------------ BiCGStab
@@ -626,8 +819,21 @@ void launch_cgj_spmv(ab2_context* ctx, int g, int n, View view, const T* z, T* p
     k_cgj_spmv<View, T, 1><<<g, kCtlThreads, 0, ctx->stream>>>(n, view, z, p0, p1, q, st, red);
 }
 
+template <class View>
+struct sym_bands_f32 : std::false_type {};
+template <bool UNIT>
+struct sym_bands_f32<StencilView<float, true, UNIT>> : std::true_type {
+  static constexpr bool unit = UNIT;
+};
+
 template <class View, class T>
 void launch_cg_spmv(ab2_context* ctx, int g, int n, View view, const T* p, T* q, SolveStateT<T>* st, Red<T> red) {
+  if constexpr (sym_bands_f32<View>::value) {
+    if (view.nx % 4 == 0) {  // four rows a thread, the same q and the same p.q tree
+      k_cg_spmv_x4<sym_bands_f32<View>::unit><<<(g + 3) / 4, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red, g);
+      return;
+    }
+  }
   if (red_virtual(ctx, (const void*)k_cg_spmv<View, T, 1>, g) == 2)
     k_cg_spmv<View, T, 2><<<g / 2, kCtlThreads, 0, ctx->stream>>>(n, view, p, q, st, red);
   else
@@ -682,8 +888,12 @@ int Krylov<T>::enqueue_body(cudaGraphConditionalHandle h, int graph_loop) {
         launch_cg_spmv<decltype(view), T>(ctx, g, n, view, p0, q, st, red_of<T>(ctx, 2));
       });
       check_launch(ctx, "cg_spmv");
-      k_cgj_update<T, true><<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p0, q, r, z, inv, stop_weight, st,
-                                                                red_of<T>(ctx, 3), h, graph_loop);
+      if (n % 4 == 0)  // four elements a thread, the same values and trees
+        k_cgj_update_x4<true><<<(g + 3) / 4, kCtlThreads, 0, ctx->stream>>>(n, p0, p0, q, r, z, inv, stop_weight, st,
+                                                                           red_of<T>(ctx, 3), h, graph_loop, g);
+      else
+        k_cgj_update<T, true><<<g, kCtlThreads, 0, ctx->stream>>>(n, p0, p0, q, r, z, inv, stop_weight, st,
+                                                                  red_of<T>(ctx, 3), h, graph_loop);
     }
     check_launch(ctx, "cgj_update");
   } else if (solver == AB2_SOLVER_CG) {

@@ -149,4 +149,72 @@ __device__ __forceinline__ bool grid_reduce_v(T (&acc)[V][NC], T* partials, unsi
   }
 }
 
+// The same reduction for a kernel whose threads each carry R consecutive
+// logical threads of a logical grid of G blocks of 256 threads: thread t of
+// the launch (256-thread blocks) holds the NC running values of logical
+// threads R t .. R t + R - 1 (acc[u][c]), so launched block b holds logical
+// blocks R b .. R b + R - 1.  The values are staged in shared memory by
+// logical thread; every logical warp is reduced by the same shuffle tree on
+// the same values, every logical block's eight warp sums likewise, and the
+// last launched block sums the G partials of each component in logical
+// order: the rounding of grid_reduce on a G-block grid.
+template <int NC, int R, class T>
+__device__ __forceinline__ bool grid_reduce_r(const T (&acc)[R][NC], int G, T* partials, unsigned int* counter,
+                                              T* out) {
+  constexpr int kB = 256;  // blockDim.x of the launch and of the logical grid
+  constexpr int kW = kB / 32;
+  __shared__ T s_val[NC][R * kB];
+  __shared__ T s_warp[NC][R][kW];
+  __shared__ bool s_last;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int u = 0; u < R; ++u) s_val[c][R * threadIdx.x + u] = acc[u][c];
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int m = 0; m < R; ++m) {  // logical block m of this block, its warp `warp`
+      T x = warp_reduce<Combine::Sum, T>(s_val[c][(m * kW + warp) * 32 + lane]);
+      if (lane == 0) s_warp[c][m][warp] = x;
+    }
+  __syncthreads();
+  if (warp < R) {  // warp m finishes logical block m
+    const int L = R * (int)blockIdx.x + warp;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      T x = lane < kW ? s_warp[c][warp][lane] : T(0);
+      x = warp_reduce<Combine::Sum, T>(x);
+      if (lane == 0 && L < G) partials[(size_t)c * G + L] = x;
+    }
+    if (lane == 0) __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned int ticket = atomicAdd(counter, 1u);
+    s_last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  bool writer = false;
+  if (s_last && warp == 0) {
+    __threadfence();
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      T x = T(0);
+      for (int b = lane; b < G; b += 32) x = x + __ldcg(partials + (size_t)c * G + b);
+      x = warp_reduce<Combine::Sum, T>(x);
+      if (lane == 0) out[c] = x;
+    }
+    if (lane == 0) {
+      *counter = 0u;
+      __threadfence();
+      writer = true;
+    }
+  }
+  return writer;
+}
+
 }  // namespace ab2

@@ -464,6 +464,23 @@ int ab2_gnn_param_count(void);
 int ab2_gnn_create(ab2_context* ctx, const float* params, unsigned long long seed, ab2_gnn** gnn);
 int ab2_gnn_get_params(const ab2_gnn* gnn, float* params);
 int ab2_gnn_set_params(ab2_gnn* gnn, const float* params);
+/* Layer kernels.  GATHER: any graph; a warp takes 16 nodes, copies their
+ * neighbours' rows by index (cp.async) and runs both products on mma.sync.
+ * GRID: a 3-D 7-point matrix in lexicographic order (rows i + nx (j + ny k));
+ * 128 consecutive nodes a tile, each direction's neighbour rows one contiguous
+ * block (bulk copies, no gather), the aggregation on the CUDA cores and the
+ * dense layer on tcgen05 tensor cores with the accumulator in tensor memory.
+ * AUTO (the default): GRID when the bound matrix has the 3-D 7-point profile,
+ * else GATHER.  The two give the same network up to the order of the FP32
+ * aggregation sums. */
+#define AB2_GNN_LAYER_AUTO 0
+#define AB2_GNN_LAYER_GATHER 1
+#define AB2_GNN_LAYER_GRID 2
+/* Takes effect at the next bind; GRID then fails with AB2_ERR_UNSUPPORTED on
+ * a matrix without the 3-D 7-point profile. */
+int ab2_gnn_set_layer(ab2_gnn* gnn, int layer);
+/* The kernel the current binding uses (GATHER or GRID; AUTO when unbound). */
+int ab2_gnn_get_layer(const ab2_gnn* gnn, int* layer);
 /* Reads the graph features of A and sizes the activation buffers (A must outlive the binding). */
 int ab2_gnn_bind(ab2_gnn* gnn, const ab2_matrix* A);
 int ab2_gnn_apply(ab2_gnn* gnn, const ab2_vector* r, ab2_vector* z);   /* z = network(r), r != z */

@@ -22,6 +22,12 @@ def get(name: str) -> abi.CsrProblem:
         return abi.diffusion(24, 24, 24, sigma=1.0, smooth=4.0, seed=5)
     if name == "diffusion64":
         return abi.diffusion(64, 64, 64, sigma=1.0, smooth=4.0, seed=0)
+    if name == "diffusion_10x11x12":  # nx not a multiple of 4
+        return abi.diffusion(10, 11, 12, sigma=1.0, smooth=2.0, seed=8)
+    if name == "diffusion_20x6x9":
+        return abi.diffusion(20, 6, 9, sigma=1.0, smooth=2.0, seed=9)
+    if name == "diffusion_80x72x64":  # more rows than one sweep of the largest reduction grid
+        return abi.diffusion(80, 72, 64, sigma=1.0, smooth=4.0, seed=10)
     if name == "diffusion2d_31x9":
         return abi.diffusion(31, 9, 1, sigma=1.5, smooth=3.0, seed=7)
     if name == "convdiff_10x11x12":

@@ -29,7 +29,7 @@ def binding_value(name: str):
     if short == "COMM_ID_BYTES":
         return abi.COMM_ID_BYTES
     tables = {"SOLVER_": abi.SOLVER, "PC_": abi.PRECOND, "ILU_": abi.ILU_SCHEDULE, "FCG_FALLBACK_": abi.FCG_FALLBACK,
-              "MIXED_JACOBI_": abi.MIXED_JACOBI}
+              "MIXED_JACOBI_": abi.MIXED_JACOBI, "GNN_LAYER_": abi.GNN_LAYER}
     for prefix, table in tables.items():
         if short.startswith(prefix):
             return table[short[len(prefix):].lower()]

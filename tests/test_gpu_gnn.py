@@ -30,12 +30,15 @@ def system():
     return P, rng.normal(size=P.n), rng.normal(size=P.n)
 
 
-def test_forward_matches_oracle(ctx, system):
+@pytest.mark.parametrize("layer", ["grid", "gather"])
+def test_forward_matches_oracle(ctx, system, layer):
     P, r, _ = system
     p = G.init_params(2)
     net = abi.Gnn(ctx, p.flat().astype(np.float32))
+    net.set_layer(layer)
     A = ctx.matrix(P.row_ptr, P.cols, P.vals)
     net.bind(A)
+    assert net.layer == layer
     vr, vz = ctx.vector(r), ctx.vector(P.n)
     net.apply(vr, vz)
     z = vz.download()
@@ -60,10 +63,12 @@ def test_jacobi_skip_alone_is_jacobi(ctx, system):
     np.testing.assert_allclose(vz.download(), r / d, rtol=1e-6, atol=0)
 
 
-def test_gradient_matches_oracle(ctx, system):
+@pytest.mark.parametrize("layer", ["grid", "gather"])
+def test_gradient_matches_oracle(ctx, system, layer):
     P, r, e = system
     p = G.init_params(3)
     net = abi.Gnn(ctx, p.flat().astype(np.float32))
+    net.set_layer(layer)
     A = ctx.matrix(P.row_ptr, P.cols, P.vals)
     net.bind(A)
     L, g = net.loss_grad(ctx.vector(r), ctx.vector(e))
@@ -75,6 +80,53 @@ def test_gradient_matches_oracle(ctx, system):
         err = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
         cos = a @ b / max(np.linalg.norm(a) * np.linalg.norm(b), 1e-30)
         assert err < 5e-2 and cos > 0.998, (name, err, cos)
+
+
+@pytest.mark.parametrize("shape", [(12, 11, 10), (40, 36, 30), (128, 3, 3), (3, 3, 257)])
+def test_layer_kernels_agree(ctx, shape):
+    """The grid layer (bulk-copied neighbour blocks, tcgen05 dense layer) and
+    the gather layer (indexed neighbour rows, mma.sync) compute the same
+    network: outputs within BF16 rounding of each other on grids with a
+    ragged last tile, several tiles a CTA, and neighbour blocks that start
+    before the first or end after the last node; on a 2-D grid (no 3-D
+    profile) AUTO takes the gather layer and an explicit grid request is
+    refused."""
+    nx, ny, nz = shape
+    P = abi.diffusion(nx, ny, nz, sigma=1.5, smooth=2.0, seed=6)
+    rng = np.random.default_rng(3)
+    r = rng.normal(size=P.n)
+    p = G.init_params(4, wd_scale=4.0).flat().astype(np.float32)
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals)
+    out = {}
+    for layer in ("grid", "gather"):
+        net = abi.Gnn(ctx, p)
+        net.set_layer(layer)
+        net.bind(A)
+        assert net.layer == layer
+        vr, vz = ctx.vector(r), ctx.vector(P.n)
+        net.apply(vr, vz)
+        out[layer] = vz.download()
+        net.close()
+    assert np.all(np.isfinite(out["grid"]))
+    rel = np.linalg.norm(out["grid"] - out["gather"]) / np.linalg.norm(out["gather"])
+    assert rel < 1e-2, rel
+    if P.n <= 2000:
+        zo, _ = G.forward(G.Params.unflat(p.astype(np.float64)), G.Graph.from_csr(P.row_ptr, P.cols, P.vals), r,
+                          bf16_round=True)
+        assert np.linalg.norm(out["grid"] - zo) / np.linalg.norm(zo) < 2e-2
+
+
+def test_grid_layer_needs_a_3d_grid(ctx):
+    P = abi.diffusion(31, 9, 1, sigma=1.5, smooth=3.0, seed=7)
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals)
+    net = abi.Gnn(ctx, G.init_params(1).flat().astype(np.float32))
+    net.bind(A)
+    assert net.layer == "gather"
+    net.set_layer("grid")
+    with pytest.raises(abi.AB2Error) as e:
+        net.bind(A)
+    assert e.value.code == abi.AB2_ERR_UNSUPPORTED
+    net.close()
 
 
 def test_training_reduces_loss_and_fcg_converges(ctx):

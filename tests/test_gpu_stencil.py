@@ -122,6 +122,10 @@ MIXED = [
     ("diffusion24", "cg", "diag", "auto", True),
     ("diffusion24", "cg", "diag", "plain", False),
     ("poisson16", "cg", "diag", "scaled", True),
+    ("diffusion_10x11x12", "cg", "diag", "auto", True),
+    ("diffusion_20x6x9", "cg", "diag", "scaled", True),
+    ("diffusion_20x6x9", "cg", "diag", "plain", False),
+    ("diffusion_80x72x64", "cg", "diag", "auto", True),
     ("diffusion12", "cg", "ilu0", "auto", False),
     ("convdiff16", "bicgs", "ilu0", "auto", False),
     ("convdiff_10x11x12", "bicgs", "diag", "auto", False),
