@@ -248,6 +248,15 @@ __device__ __forceinline__ void ldsm_x4_t(unsigned (&r)[4], const void* p) {
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(smem_u32(p)));
 }
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+// acc0 += g * lo(w), acc1 += g * hi(w): BF16 operands (g and the two halves
+// of w), the exact products added to FP32 accumulators with one rounding.
+__device__ __forceinline__ void fma_bf16_pair(float& acc0, float& acc1, unsigned short g, unsigned w) {
+  asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
+      "fma.rn.f32.bf16 %0, %3, lo, %0;\n\t"
+      "fma.rn.f32.bf16 %1, %3, hi, %1;\n\t}"
+      : "+f"(acc0), "+f"(acc1)
+      : "r"(w), "h"(g));
+}
 __device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
   return make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
 }
@@ -490,7 +499,10 @@ constexpr unsigned kTcStageB = kTcEfOff + kTcEfBytes;
 constexpr unsigned kTcStage1 = kTcStage0 + kTcStageB;
 constexpr unsigned kTcY = kTcStage1 + kTcStageB;             // decoder partials, 4 x 128 floats
 constexpr unsigned kTcBias = kTcY + 4 * kTcTile * 4;         // bias, wd: 2 x 64 floats
-constexpr unsigned kTcBar = kTcBias + 2 * kH * 4;            // 3 mbarriers, tensor-memory address, abort flag
+constexpr unsigned kTcGate = kTcBias + 2 * kH * 4;           // gates, BF16: 2 tiles x 128 x 6
+constexpr unsigned kTcGateB = kTcTile * 6 * 2;
+constexpr unsigned kTcZero = kTcGate + 2 * kTcGateB;         // one row of zeros (absent neighbours)
+constexpr unsigned kTcBar = kTcZero + kTcRowB;               // 3 mbarriers, tensor-memory address, abort flag
 constexpr unsigned kTcSmem = kTcBar + 32 + 1024;             // + slack to align the base to 1024 bytes
 static_assert(kTcSmem <= 227 * 1024, "grid layer: shared memory");
 static_assert(kTcStage0 % 1024 == 0 && kTcA % 1024 == 0 && kTcStageB % 16 == 0, "grid layer: alignment");
@@ -580,6 +592,28 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
   }
 
   const float u = a.P[kOffU + a.layer], cg = a.P[kOffC + a.layer];
+  // gates of the c-th tile (its stage complete): 768 (node, direction) pairs,
+  // one or two a thread, as BF16 bits (0 where the neighbour is absent)
+  auto gates = [&](int c) {
+    const float* ef = reinterpret_cast<const float*>(sm + ((c & 1) ? kTcStage1 : kTcStage0) + kTcEfOff);
+    unsigned short* gt = reinterpret_cast<unsigned short*>(sm + kTcGate + (c & 1) * kTcGateB);
+    for (int q = tid; q < kTcTile * 6; q += kTcThreads) {
+      const float e = ef[q];
+      gt[q] = e == e ? __bfloat16_as_ushort(__float2bfloat16_rn(sigmoidf(fmaf(u, e, cg)))) : (unsigned short)0;
+    }
+  };
+  if (tid < (int)kTcRowB / 16) reinterpret_cast<uint4*>(sm + kTcZero)[tid] = make_uint4(0u, 0u, 0u, 0u);
+  int failed = 0;  // this thread's bounded wait gave up (the barriers OR it over the CTA)
+  if (count > 0) {
+    if (!tc::mbar_wait(bar_in0, 0u, kWaitCycles, s_abort)) {
+      failed = 1;
+      *s_abort = 1;
+      atomicOr(ga.err, 1);
+    } else if (tid == 0) {
+      pend[0] = -1;
+    }
+    gates(0);
+  }
   const int ln = tid >> 2, qq = tid & 3;        // aggregation: node ln, chunks qq and qq + 4
   const int eq = warp & 3, ecg = warp >> 2;     // epilogue: lanes 32 eq .., columns 16 ecg ..
   const int erow = 32 * eq + lane;
@@ -587,29 +621,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
     const int s = c & 1;
     const long long b = (long long)((int)blockIdx.x + c * (int)gridDim.x) * kTcTile;
     const unsigned char* stg = sm + (s ? kTcStage1 : kTcStage0);
-    int failed = 0;  // this thread's bounded wait gave up (the barriers OR it over the CTA)
-    if (!tc::mbar_wait(bar_in0 + 8 * s, (unsigned)(c >> 1) & 1u, kWaitCycles, s_abort)) {
-      failed = 1;
-      *s_abort = 1;
-      atomicOr(ga.err, 1);
-    } else if (tid == 0) {
-      pend[s] = -1;
-    }
-    // ---- aggregation: m for node ln, chunks qq and qq + 4; [h ; m] into A
+    if (__syncthreads_or(failed)) break;  // (0) this tile's inputs landed and its gates are in the table
+    // ---- aggregation: m for node ln, chunks qq and qq + 4 (FP32 sums of BF16
+    // products in the CSR column order; absent neighbours read a zero row);
+    // [h ; m] into A
     {
       const long long gi = b + ln;
-      const float* efr = reinterpret_cast<const float*>(stg + kTcEfOff) + ln * 6;
-      float g[6];
-      bool pr[6];
+      const unsigned short* gt = reinterpret_cast<const unsigned short*>(sm + kTcGate + s * kTcGateB) + ln * 6;
+      const float* efr = reinterpret_cast<const float*>(stg + kTcEfOff) + ln * 6;  // NaN: no neighbour
+      const unsigned char* zero = sm + kTcZero;
+      const unsigned char* row[6] = {stg + kTcZmOff + ln * kTcRowB, stg + kTcYmOff + ln * kTcRowB,
+                                     stg + kTcXOff + ln * kTcRowB, stg + kTcXOff + (ln + 2) * kTcRowB,
+                                     stg + kTcYpOff + ln * kTcRowB, stg + kTcZpOff + ln * kTcRowB};
+      unsigned short g[6];
+      const unsigned char* src[6];
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
         const float e = efr[d];
-        pr[d] = e == e;
-        g[d] = pr[d] ? bf16r(sigmoidf(fmaf(u, e, cg))) : 0.f;
+        g[d] = gt[d];
+        src[d] = e == e ? row[d] : zero;
       }
-      const unsigned char* src[6] = {stg + kTcZmOff + ln * kTcRowB, stg + kTcYmOff + ln * kTcRowB,
-                                     stg + kTcXOff + ln * kTcRowB, stg + kTcXOff + (ln + 2) * kTcRowB,
-                                     stg + kTcYpOff + ln * kTcRowB, stg + kTcZpOff + ln * kTcRowB};
       const unsigned char* own = stg + kTcXOff + (ln + 1) * kTcRowB;
 #pragma unroll
       for (int jj = 0; jj < 2; ++jj) {
@@ -617,15 +648,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
         float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int d = 0; d < 6; ++d) {
-          if (pr[d]) {
-            const uint4 w = *reinterpret_cast<const uint4*>(src[d] + ch * 16);
-            const unsigned wv[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              acc[2 * e] = fmaf(g[d], __uint_as_float(wv[e] << 16), acc[2 * e]);
-              acc[2 * e + 1] = fmaf(g[d], __uint_as_float(wv[e] & 0xffff0000u), acc[2 * e + 1]);
-            }
-          }
+          const uint4 w = *reinterpret_cast<const uint4*>(src[d] + ch * 16);
+          fma_bf16_pair(acc[0], acc[1], g[d], w.x);
+          fma_bf16_pair(acc[2], acc[3], g[d], w.y);
+          fma_bf16_pair(acc[4], acc[5], g[d], w.z);
+          fma_bf16_pair(acc[6], acc[7], g[d], w.w);
         }
         const uint4 hv = gi < n ? *reinterpret_cast<const uint4*>(own + ch * 16) : make_uint4(0u, 0u, 0u, 0u);
         const unsigned pos = ln * kTcRowB + ((ch ^ (ln & 7)) << 4);
@@ -634,7 +661,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
       }
     }
     tc::fence_proxy_async_smem();
-    if (__syncthreads_or(failed)) break;  // (1) A complete; the stage's inputs consumed
+    __syncthreads();  // (1) A complete; the stage's inputs consumed
     if (tid == 0) {
       if (c + 2 < count) {
         issue(c + 2, s);
@@ -650,25 +677,40 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
       tc::mma_commit(bar_mma);
       mma_pend = c & 1;
     }
-    if (!tc::mbar_wait(bar_mma, (unsigned)c & 1u, kWaitCycles, s_abort)) {
-      failed = 1;
-      *s_abort = 1;
-      atomicOr(ga.err, 1);
-    } else if (tid == 0) {
-      mma_pend = -1;
+    // while the tensor core runs: the next tile's inputs and gates
+    if (c + 1 < count) {
+      if (!tc::mbar_wait(bar_in0 + 8 * (s ^ 1), (unsigned)((c + 1) >> 1) & 1u, kWaitCycles, s_abort)) {
+        failed = 1;
+        *s_abort = 1;
+        atomicOr(ga.err, 1);
+      } else if (tid == 0) {
+        pend[s ^ 1] = -1;
+      }
+      gates(c + 1);
     }
+    if (tid == 0) {
+      if (!tc::mbar_wait(bar_mma, (unsigned)c & 1u, kWaitCycles, s_abort)) {
+        failed = 1;
+        *s_abort = 1;
+        atomicOr(ga.err, 1);
+      } else {
+        mma_pend = -1;
+      }
+    }
+    __syncthreads();  // (1b) the accumulator is complete
     tc::fence_after_sync();
     // ---- epilogue: bias, relu, BF16; rows staged in A's first region (the
     // MMA has read it), swizzled
     {
       float v[16];
       tc::tmem_ld16(tmem + ((unsigned)(32 * eq) << 16) + 16 * ecg, v);
-      float hb[16];
-      float y = 0.f;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        hb[j] = bf16r(fmaxf(v[j] + s_bias[16 * ecg + j], 0.f));
-        if constexpr (LAST) y = fmaf(s_wd[16 * ecg + j], hb[j], y);
+      for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + s_bias[16 * ecg + j], 0.f);
+      if constexpr (LAST) {
+        float y = 0.f;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) y = fmaf(s_wd[16 * ecg + j], bf16r(v[j]), y);
+        s_y[ecg * kTcTile + erow] = y;
       }
       if (a.h_out) {
 #pragma unroll
@@ -676,11 +718,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
           const int ch = 2 * ecg + h2;
           float f8[8];
 #pragma unroll
-          for (int e = 0; e < 8; ++e) f8[e] = hb[8 * h2 + e];
+          for (int e = 0; e < 8; ++e) f8[e] = v[8 * h2 + e];
           *reinterpret_cast<uint4*>(sm + kTcA + erow * kTcRowB + ((ch ^ (erow & 7)) << 4)) = pack8(f8);
         }
       }
-      if constexpr (LAST) s_y[ecg * kTcTile + erow] = y;
     }
     tc::fence_before_sync();
     __syncthreads();  // (2) staged rows, decoder partials
@@ -700,12 +741,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
       if (tid < kTcTile && b + tid < n) {
         const long long gi = b + tid;
         const float y = ((s_y[tid] + s_y[kTcTile + tid]) + s_y[2 * kTcTile + tid]) + s_y[3 * kTcTile + tid];
-        const double s = a.s2[0], is = a.s2[1];
+        const double s2 = a.s2[0], is = a.s2[1];
         const float bd = a.P[kOffBd], ws = a.P[kOffWs];
-        a.z[gi] = s * (double)(y + bd + ws * (float)(a.xr[gi] * is)) * (double)a.isd[gi];
+        a.z[gi] = s2 * (double)(y + bd + ws * (float)(a.xr[gi] * is)) * (double)a.isd[gi];
       }
     }
-    if (__syncthreads_or(failed)) break;  // (3) A and the partials free for the next tile
+    // the loop head's barrier (0) frees A and the partials for the next tile
   }
   // ---- drain: no copy or MMA of this CTA may still be in flight at exit
   if (tid == 0) {

@@ -1038,6 +1038,14 @@ def profile_case(a) -> int:
         if a.profile_case == "spmv_bands":
             ctx.mult(A, b, x, abi.SPMV_STENCIL)
             st = None
+        elif a.profile_case.startswith("gnn"):
+            # one application of the committed network, grid or gather layer kernel
+            net = abi.Gnn(ctx, np.load(GNN_WEIGHTS))
+            net.set_layer(a.profile_case[4:])
+            net.bind(A)
+            net.apply(b, x)
+            st = net.layer
+            net.close()
         elif a.profile_case.startswith("mixed"):
             form = "plain" if a.profile_case.endswith("plain") else "auto"
             M = abi.Mixed(ctx, A, solver="cg", precond="diag", tol=1e-8, max_outer=20, inner_tol=1e-4,
@@ -1079,9 +1087,9 @@ def main():
                     help="strong scaling instead: one system split across the N ranks by z-slabs (NCCL), "
                          "distributed CG")
     ap.add_argument("--profile-case", choices=["mixed_jacobi", "mixed_jacobi_plain", "fp64_jacobi", "fp64_ilu0",
-                                               "spmv_bands"],
-                    help="run one small piece of the workload and exit (for profilers): the solve or the SpMV, "
-                         "twice, on the --n system, no timing or JSON line")
+                                               "gnn_grid", "gnn_gather", "spmv_bands"],
+                    help="run one small piece of the workload and exit (for profilers): the solve, the SpMV or "
+                         "one network application, twice, on the --n system, no timing or JSON line")
     ap.add_argument("--ref-budget", type=float, default=150.0,
                     help="--impl reference: seconds of complete solves to fit the timed steps into")
     ap.add_argument("--host-loop", action="store_true",
