@@ -248,14 +248,25 @@ __device__ __forceinline__ void ldsm_x4_t(unsigned (&r)[4], const void* p) {
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(smem_u32(p)));
 }
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-// acc0 += g * lo(w), acc1 += g * hi(w): BF16 operands (g and the two halves
-// of w), the exact products added to FP32 accumulators with one rounding.
-__device__ __forceinline__ void fma_bf16_pair(float& acc0, float& acc1, unsigned short g, unsigned w) {
-  asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
-      "fma.rn.f32.bf16 %0, %3, lo, %0;\n\t"
-      "fma.rn.f32.bf16 %1, %3, hi, %1;\n\t}"
+// (acc0, acc1) += g * (lo(w), hi(w)) as one packed FP32 FMA (fma.rn.f32x2):
+// a BF16 value is the high half of its FP32 value, so the halves of w unpack
+// with a shift and a mask; each product is exact and each sum rounds once.
+__device__ __forceinline__ void fma2_bf16_pair(float& acc0, float& acc1, float g, unsigned w) {
+  const float lo = __uint_as_float(w << 16), hi = __uint_as_float(w & 0xffff0000u);
+  asm("{\n\t.reg .b64 a, x, y;\n\t"
+      "mov.b64 a, {%0, %1};\n\t"
+      "mov.b64 x, {%2, %3};\n\t"
+      "mov.b64 y, {%4, %4};\n\t"
+      "fma.rn.f32x2 a, y, x, a;\n\t"
+      "mov.b64 {%0, %1}, a;\n\t}"
       : "+f"(acc0), "+f"(acc1)
-      : "r"(w), "h"(g));
+      : "f"(lo), "f"(hi), "f"(g));
+}
+// 16 bytes of shared memory at a 32-bit shared address.
+__device__ __forceinline__ uint4 lds128(unsigned a) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+  return v;
 }
 __device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
   return make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
@@ -461,27 +472,34 @@ __global__ void __launch_bounds__(kLayerWarps * 32) k_gnn_layer(const LayerArgs 
 // lexicographic order (row i + nx (j + ny k), off-diagonal columns at -nx ny,
 // -nx, -1, +1, +nx, +nx ny where inside the grid): 128 consecutive nodes a
 // tile, so each direction's neighbour rows form one contiguous block of h and
-// nothing is gathered by index.  A persistent CTA (one an SM, 512 threads)
-// walks tiles; per tile:
-//   - its inputs arrive by bulk copy (cp.async.bulk, no multicast), issued
-//     two tiles ahead into a two-stage ring: the tile's own rows with one row
-//     either side (the +-1 neighbours), the four +-nx / +-nx ny blocks, and
-//     the edge features in direction order (NaN where no neighbour);
-//   - every thread computes m = sum_d g_d h_nbr(d) for one node and two
-//     8-feature chunks (FP32, in the CSR column order, rounded to BF16 as the
-//     tensor-core aggregation of k_gnn_layer is) and writes [h ; m] as the
-//     MMA's A operand (128 x 128 BF16, 128-byte swizzle);
-//   - one thread issues eight tcgen05.mma (M = 128, N = 64, K = 16) into a
-//     128 x 64 FP32 accumulator in tensor memory; B is W (64 x 128 BF16),
-//     staged once per CTA;
-//   - the 16 warps read the accumulator (tcgen05.ld: a lane quarter x 16
-//     columns each), add the bias, relu, round to BF16 and stage the rows in
-//     shared memory (swizzled: no bank conflicts), then all threads store
-//     them with coalesced 16-byte writes; LAST applies the decoder.
-// Every wait is bounded: on expiry the kernel sets *err, takes no further
-// tile, waits (bounded) for the copies and the MMA it issued, frees its
-// tensor memory and returns.
-constexpr int kTcThreads = 512;
+// nothing is gathered by index.  A persistent CTA (one an SM) walks tiles with
+// its warps in three roles that hand tiles on through mbarriers, so one
+// tile's MMA and epilogue overlap the next tile's aggregation:
+//   - control (one thread): issues each tile's inputs by bulk copy
+//     (cp.async.bulk, no multicast) two tiles ahead into a two-stage ring --
+//     the tile's own rows with one row either side (the +-1 neighbours), the
+//     four +-nx / +-nx ny blocks, and the edge features in direction order
+//     (NaN where no neighbour) -- and, once a tile's A operand is complete and
+//     an accumulator buffer is free, eight tcgen05.mma (M = 128, N = 64,
+//     K = 16) into that buffer (two 128 x 64 FP32 accumulators in tensor
+//     memory); B is W (64 x 128 BF16), staged once per CTA;
+//   - aggregation (16 warps): the gates sigmoid(u e + c) once per (node,
+//     direction), then m = sum_d g_d h_nbr(d), four threads a node and two
+//     8-feature chunks a thread
+//     (BF16 x BF16 products, FP32 sums in the CSR column order, rounded to
+//     BF16 as the tensor-core aggregation of k_gnn_layer is; absent neighbours
+//     read a row of zeros), held in registers until the tensor core has
+//     released A, then [h ; m] written as A (128 x 128 BF16, 128-byte swizzle);
+//   - epilogue (4 warps, one a tensor-memory lane quarter): a row a thread,
+//     bias, relu, BF16, stored to h (LAST: the decoder's z instead).
+// Every wait is bounded: on expiry the kernel sets *err, every role stops at
+// its next tile, and the CTA waits (bounded) for the copies and the MMA it
+// issued and frees its tensor memory before it returns.
+constexpr int kTcAggWarps = 16;
+constexpr int kTcEpiWarps = 4;
+constexpr int kTcAggThreads = kTcAggWarps * 32;
+constexpr int kTcEpiThreads = kTcEpiWarps * 32;
+constexpr int kTcThreads = kTcAggThreads + kTcEpiThreads + 32;  // + the control warp
 constexpr int kTcTile = 128;
 constexpr unsigned kTcRowB = kH * 2;                         // bytes of one h row
 constexpr unsigned kTcW = 0;                                 // B: 2 regions x 64 rows x 128 B
@@ -497,15 +515,16 @@ constexpr unsigned kTcEfOff = kTcZpOff + kTcARegion;         // 128 x 6 floats
 constexpr unsigned kTcEfBytes = kTcTile * 6 * 4;
 constexpr unsigned kTcStageB = kTcEfOff + kTcEfBytes;
 constexpr unsigned kTcStage1 = kTcStage0 + kTcStageB;
-constexpr unsigned kTcY = kTcStage1 + kTcStageB;             // decoder partials, 4 x 128 floats
-constexpr unsigned kTcBias = kTcY + 4 * kTcTile * 4;         // bias, wd: 2 x 64 floats
+constexpr unsigned kTcBias = kTcStage1 + kTcStageB;          // bias, wd: 2 x 64 floats
 constexpr unsigned kTcGate = kTcBias + 2 * kH * 4;           // gates, BF16: 2 tiles x 128 x 6
 constexpr unsigned kTcGateB = kTcTile * 6 * 2;
 constexpr unsigned kTcZero = kTcGate + 2 * kTcGateB;         // one row of zeros (absent neighbours)
-constexpr unsigned kTcBar = kTcZero + kTcRowB;               // 3 mbarriers, tensor-memory address, abort flag
-constexpr unsigned kTcSmem = kTcBar + 32 + 1024;             // + slack to align the base to 1024 bytes
+constexpr unsigned kTcBar = kTcZero + kTcRowB;               // 8 mbarriers, tensor-memory address, abort flag
+constexpr unsigned kTcSmem = kTcBar + 80 + 1024;             // + slack to align the base to 1024 bytes
+constexpr unsigned kTcCols = 2 * kH;                         // tensor-memory columns: two accumulators
 static_assert(kTcSmem <= 227 * 1024, "grid layer: shared memory");
 static_assert(kTcStage0 % 1024 == 0 && kTcA % 1024 == 0 && kTcStageB % 16 == 0, "grid layer: alignment");
+static_assert(kTcAggThreads == kTcTile * 4, "grid layer: four aggregation threads a node");
 
 struct GridLayerArgs {
   LayerArgs a;
@@ -514,6 +533,20 @@ struct GridLayerArgs {
   int* err;              // set when a bounded wait gives up
 };
 
+// Named barrier `id` over `count` threads that ORs a flag across them.
+__device__ __forceinline__ int bar_or(int id, int count, int v) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.s32 p, %1, 0;\n\t"
+      "barrier.cta.red.or.pred q, %2, %3, p;\n\t"
+      "selp.s32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"(v), "r"(id), "r"(count)
+      : "memory");
+  return r;
+}
+
 template <bool LAST>
 __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLayerArgs ga) {
   const LayerArgs& a = ga.a;
@@ -521,16 +554,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
   unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) &
                                                        ~static_cast<uintptr_t>(1023));
   const unsigned sb = tc::smem_u32(sm);
-  float* s_y = reinterpret_cast<float*>(sm + kTcY);
   float* s_bias = reinterpret_cast<float*>(sm + kTcBias);
   float* s_wd = s_bias + kH;
-  volatile unsigned* s_tmem = reinterpret_cast<volatile unsigned*>(sm + kTcBar + 24);
-  volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kTcBar + 28);
-  const unsigned bar_in0 = sb + kTcBar, bar_mma = sb + kTcBar + 16;
+  // mbarriers: inputs of stage 0/1 landed; A written; A released by the
+  // tensor core; accumulator 0/1 complete; accumulator 0/1 read
+  const unsigned bar_full = sb + kTcBar, bar_afull = bar_full + 16, bar_aempty = bar_full + 24;
+  const unsigned bar_accf = bar_full + 32, bar_acce = bar_full + 48;
+  volatile unsigned* s_tmem = reinterpret_cast<volatile unsigned*>(sm + kTcBar + 64);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(sm + kTcBar + 68);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int n = a.n;
   const int ntiles = (n + kTcTile - 1) / kTcTile;
   const int count = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  auto tile_base = [&](int c) { return (long long)((int)blockIdx.x + c * (int)gridDim.x) * kTcTile; };
+  auto give_up = [&]() {
+    *s_abort = 1;
+    atomicOr(ga.err, 1);
+  };
 
   // W as the B operand (row o = output feature, K-major, 128-byte swizzle)
   for (int t = tid; t < kH * kIn / 8; t += kTcThreads) {
@@ -542,15 +582,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
     s_bias[t] = a.P[kOffB + a.layer * kH + t];
     s_wd[t] = a.P[kOffWd + t];
   }
+  if (tid < (int)kTcRowB / 16) reinterpret_cast<uint4*>(sm + kTcZero)[tid] = make_uint4(0u, 0u, 0u, 0u);
   if (tid == 0) {
-    tc::mbar_init(bar_in0, 1);
-    tc::mbar_init(bar_in0 + 8, 1);
-    tc::mbar_init(bar_mma, 1);
+    tc::mbar_init(bar_full, 1);
+    tc::mbar_init(bar_full + 8, 1);
+    tc::mbar_init(bar_afull, kTcAggThreads);
+    tc::mbar_init(bar_aempty, 1);
+    tc::mbar_init(bar_accf, 1);
+    tc::mbar_init(bar_accf + 8, 1);
+    tc::mbar_init(bar_acce, kTcEpiThreads);
+    tc::mbar_init(bar_acce + 8, kTcEpiThreads);
     *s_abort = 0;
     tc::fence_mbar_init();
   }
   if (warp == 0) {
-    tc::tmem_alloc(sb + kTcBar + 24, 64);
+    tc::tmem_alloc(sb + kTcBar + 64, kTcCols);
     tc::tmem_relinquish();
   }
   tc::fence_proxy_async_smem();  // W (generic stores) is read by the tensor core
@@ -559,204 +605,193 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
   tc::fence_after_sync();
   const unsigned tmem = *s_tmem;
 
-  // thread 0: the inputs of the c-th tile of this CTA into stage s
-  auto issue = [&](int c, int s) {
-    const long long b = (long long)((int)blockIdx.x + c * (int)gridDim.x) * kTcTile;
-    const unsigned st = sb + (s ? kTcStage1 : kTcStage0);
-    const long long first[5] = {b - 1, b - ga.nx, b + ga.nx, b - ga.sxy, b + ga.sxy};
-    const int rows[5] = {kTcTile + 2, kTcTile, kTcTile, kTcTile, kTcTile};
-    const unsigned dst[5] = {kTcXOff, kTcYmOff, kTcYpOff, kTcZmOff, kTcZpOff};
-    long long lo[5], hi[5];
-    unsigned bytes = kTcEfBytes;
-    for (int q = 0; q < 5; ++q) {
-      lo[q] = first[q] < 0 ? 0 : first[q];
-      hi[q] = first[q] + rows[q] > n ? n : first[q] + rows[q];
-      if (hi[q] > lo[q]) bytes += (unsigned)(hi[q] - lo[q]) * kTcRowB;
-    }
-    tc::mbar_expect_tx(bar_in0 + 8 * s, bytes);
-    for (int q = 0; q < 5; ++q)
-      if (hi[q] > lo[q])
-        tc::bulk_g2s(st + dst[q] + (unsigned)(lo[q] - first[q]) * kTcRowB, a.h_in + lo[q] * kH,
-                     (unsigned)(hi[q] - lo[q]) * kTcRowB, bar_in0 + 8 * s);
-    tc::bulk_g2s(st + kTcEfOff, ga.dir_ef + b * 6, kTcEfBytes, bar_in0 + 8 * s);
-  };
-  // thread 0's record of what is in flight: the parity of stage s's
-  // unawaited phase (-1: none), and of the MMA's
-  int pend[2] = {-1, -1};
-  int mma_pend = -1;
-  if (tid == 0) {
-    for (int c = 0; c < 2 && c < count; ++c) {
-      issue(c, c);
-      pend[c] = 0;
-    }
-  }
-
-  const float u = a.P[kOffU + a.layer], cg = a.P[kOffC + a.layer];
-  // gates of the c-th tile (its stage complete): 768 (node, direction) pairs,
-  // one or two a thread, as BF16 bits (0 where the neighbour is absent)
-  auto gates = [&](int c) {
-    const float* ef = reinterpret_cast<const float*>(sm + ((c & 1) ? kTcStage1 : kTcStage0) + kTcEfOff);
-    unsigned short* gt = reinterpret_cast<unsigned short*>(sm + kTcGate + (c & 1) * kTcGateB);
-    for (int q = tid; q < kTcTile * 6; q += kTcThreads) {
-      const float e = ef[q];
-      gt[q] = e == e ? __bfloat16_as_ushort(__float2bfloat16_rn(sigmoidf(fmaf(u, e, cg)))) : (unsigned short)0;
-    }
-  };
-  if (tid < (int)kTcRowB / 16) reinterpret_cast<uint4*>(sm + kTcZero)[tid] = make_uint4(0u, 0u, 0u, 0u);
-  int failed = 0;  // this thread's bounded wait gave up (the barriers OR it over the CTA)
-  if (count > 0) {
-    if (!tc::mbar_wait(bar_in0, 0u, kWaitCycles, s_abort)) {
-      failed = 1;
-      *s_abort = 1;
-      atomicOr(ga.err, 1);
-    } else if (tid == 0) {
-      pend[0] = -1;
-    }
-    gates(0);
-  }
-  const int ln = tid >> 2, qq = tid & 3;        // aggregation: node ln, chunks qq and qq + 4
-  const int eq = warp & 3, ecg = warp >> 2;     // epilogue: lanes 32 eq .., columns 16 ecg ..
-  const int erow = 32 * eq + lane;
-  for (int c = 0; c < count; ++c) {
-    const int s = c & 1;
-    const long long b = (long long)((int)blockIdx.x + c * (int)gridDim.x) * kTcTile;
-    const unsigned char* stg = sm + (s ? kTcStage1 : kTcStage0);
-    if (__syncthreads_or(failed)) break;  // (0) this tile's inputs landed and its gates are in the table
-    // ---- aggregation: m for node ln, chunks qq and qq + 4 (FP32 sums of BF16
-    // products in the CSR column order; absent neighbours read a zero row);
-    // [h ; m] into A
-    {
-      const long long gi = b + ln;
+  if (warp < kTcAggWarps) {
+    // ================================================================ aggregation
+    const float u = a.P[kOffU + a.layer], cg = a.P[kOffC + a.layer];
+    int failed = 0;
+    for (int c = 0; c < count; ++c) {
+      const int s = c & 1;
+      const long long b = tile_base(c);
+      const unsigned char* stg = sm + (s ? kTcStage1 : kTcStage0);
+      if (!tc::mbar_wait(bar_full + 8 * s, (unsigned)(c >> 1) & 1u, kWaitCycles, s_abort)) {
+        failed = 1;
+        give_up();
+      }
+      // gates, once per (node, direction), BF16 bits (0 where no neighbour)
+      {
+        const float* ef = reinterpret_cast<const float*>(stg + kTcEfOff);
+        unsigned short* gt = reinterpret_cast<unsigned short*>(sm + kTcGate + s * kTcGateB);
+        for (int q = tid; q < kTcTile * 6; q += kTcAggThreads) {
+          const float e = ef[q];
+          gt[q] = e == e ? __bfloat16_as_ushort(__float2bfloat16_rn(sigmoidf(fmaf(u, e, cg)))) : (unsigned short)0;
+        }
+      }
+      if (bar_or(1, kTcAggThreads, failed)) break;
+      const int ln = tid >> 2, qq = tid & 3;  // node, and its chunks qq and qq + 4
       const unsigned short* gt = reinterpret_cast<const unsigned short*>(sm + kTcGate + s * kTcGateB) + ln * 6;
-      const float* efr = reinterpret_cast<const float*>(stg + kTcEfOff) + ln * 6;  // NaN: no neighbour
-      const unsigned char* zero = sm + kTcZero;
-      const unsigned char* row[6] = {stg + kTcZmOff + ln * kTcRowB, stg + kTcYmOff + ln * kTcRowB,
-                                     stg + kTcXOff + ln * kTcRowB, stg + kTcXOff + (ln + 2) * kTcRowB,
-                                     stg + kTcYpOff + ln * kTcRowB, stg + kTcZpOff + ln * kTcRowB};
-      unsigned short g[6];
-      const unsigned char* src[6];
+      const float* efr = reinterpret_cast<const float*>(stg + kTcEfOff) + ln * 6;
+      const unsigned sst = sb + (s ? kTcStage1 : kTcStage0) + ln * kTcRowB;  // this node's row of each block
+      unsigned src[6] = {sst + kTcZmOff, sst + kTcYmOff, sst + kTcXOff, sst + kTcXOff + 2 * kTcRowB, sst + kTcYpOff,
+                         sst + kTcZpOff};
+      float g[6];
 #pragma unroll
       for (int d = 0; d < 6; ++d) {
         const float e = efr[d];
-        g[d] = gt[d];
-        src[d] = e == e ? row[d] : zero;
+        src[d] = e == e ? src[d] : sb + kTcZero;
+        g[d] = __uint_as_float((unsigned)gt[d] << 16);
       }
-      const unsigned char* own = stg + kTcXOff + (ln + 1) * kTcRowB;
+      uint4 hv[2], mv[2];
 #pragma unroll
       for (int jj = 0; jj < 2; ++jj) {
         const int ch = 4 * ((ln & 1) ^ jj) + qq;  // the 8 threads of a quarter-warp touch 8 distinct banks
         float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int d = 0; d < 6; ++d) {
-          const uint4 w = *reinterpret_cast<const uint4*>(src[d] + ch * 16);
-          fma_bf16_pair(acc[0], acc[1], g[d], w.x);
-          fma_bf16_pair(acc[2], acc[3], g[d], w.y);
-          fma_bf16_pair(acc[4], acc[5], g[d], w.z);
-          fma_bf16_pair(acc[6], acc[7], g[d], w.w);
+          const uint4 w = lds128(src[d] + ch * 16);
+          fma2_bf16_pair(acc[0], acc[1], g[d], w.x);
+          fma2_bf16_pair(acc[2], acc[3], g[d], w.y);
+          fma2_bf16_pair(acc[4], acc[5], g[d], w.z);
+          fma2_bf16_pair(acc[6], acc[7], g[d], w.w);
         }
-        const uint4 hv = gi < n ? *reinterpret_cast<const uint4*>(own + ch * 16) : make_uint4(0u, 0u, 0u, 0u);
+        mv[jj] = pack8(acc);
+        hv[jj] = b + ln < n ? lds128(sst + kTcXOff + kTcRowB + ch * 16) : make_uint4(0u, 0u, 0u, 0u);
+      }
+      // A is free once the tensor core has read the previous tile's
+      if (c > 0 && !tc::mbar_wait(bar_aempty, (unsigned)(c - 1) & 1u, kWaitCycles, s_abort)) {
+        failed = 1;
+        give_up();
+      }
+#pragma unroll
+      for (int jj = 0; jj < 2; ++jj) {
+        const int ch = 4 * ((ln & 1) ^ jj) + qq;
         const unsigned pos = ln * kTcRowB + ((ch ^ (ln & 7)) << 4);
-        *reinterpret_cast<uint4*>(sm + kTcA + pos) = hv;
-        *reinterpret_cast<uint4*>(sm + kTcA + kTcARegion + pos) = pack8(acc);
+        *reinterpret_cast<uint4*>(sm + kTcA + pos) = hv[jj];
+        *reinterpret_cast<uint4*>(sm + kTcA + kTcARegion + pos) = mv[jj];
+        if (a.m_out && b + ln < n) reinterpret_cast<uint4*>(a.m_out + (b + ln) * kH)[ch] = mv[jj];
+      }
+      tc::fence_proxy_async_smem();
+      tc::mbar_arrive(bar_afull);
+    }
+  } else if (warp < kTcAggWarps + kTcEpiWarps) {
+    // ================================================================ epilogue
+    const int q = warp & 3;  // the tensor-memory lane quarter this warp may read
+    const int row = 32 * q + lane;
+    for (int c = 0; c < count; ++c) {
+      const int bsel = c & 1;
+      const long long gi = tile_base(c) + row;
+      int failed = !tc::mbar_wait(bar_accf + 8 * bsel, (unsigned)(c >> 1) & 1u, kWaitCycles, s_abort);
+      if (__any_sync(0xffffffffu, failed)) {
+        give_up();
+        break;
+      }
+      tc::fence_after_sync();
+      const unsigned ta = tmem + ((unsigned)(32 * q) << 16) + bsel * kH;
+      float y = 0.f;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {  // 32 columns at a time
+        float v[32];
+        tc::tmem_ld32(ta + 32 * h, v);
+        if (h == 1) {
+          tc::fence_before_sync();
+          tc::mbar_arrive(bar_acce + 8 * bsel);  // the accumulator is read
+        }
+        if (gi < n) {
+#pragma unroll
+          for (int j4 = 0; j4 < 8; ++j4) {
+            const float4 bb = reinterpret_cast<const float4*>(s_bias)[8 * h + j4];
+            const float bv[4] = {bb.x, bb.y, bb.z, bb.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) v[4 * j4 + e] = fmaxf(v[4 * j4 + e] + bv[e], 0.f);
+            if constexpr (LAST) {
+              const float4 ww = reinterpret_cast<const float4*>(s_wd)[8 * h + j4];
+              const float wv[4] = {ww.x, ww.y, ww.z, ww.w};
+#pragma unroll
+              for (int e = 0; e < 4; ++e) y = fmaf(wv[e], bf16r(v[4 * j4 + e]), y);
+            }
+          }
+          if (a.h_out) {
+#pragma unroll
+            for (int c8 = 0; c8 < 4; ++c8) {
+              float f8[8];
+#pragma unroll
+              for (int e = 0; e < 8; ++e) f8[e] = v[8 * c8 + e];
+              reinterpret_cast<uint4*>(a.h_out + gi * kH)[4 * h + c8] = pack8(f8);
+            }
+          }
+        }
+      }
+      if constexpr (LAST) {
+        if (gi < n) {
+          const double s2 = a.s2[0], is = a.s2[1];
+          const float bd = a.P[kOffBd], ws = a.P[kOffWs];
+          a.z[gi] = s2 * (double)(y + bd + ws * (float)(a.xr[gi] * is)) * (double)a.isd[gi];
+        }
       }
     }
-    tc::fence_proxy_async_smem();
-    __syncthreads();  // (1) A complete; the stage's inputs consumed
-    if (tid == 0) {
-      if (c + 2 < count) {
-        issue(c + 2, s);
-        pend[s] = ((c + 2) >> 1) & 1;
+  } else if (lane == 0) {
+    // ================================================================ control
+    // in flight, for the drain after a failure: the parity of each stage's
+    // last issued phase and of the last MMA commit (-1: none)
+    int last_in[2] = {-1, -1}, last_mma = -1;
+    auto issue = [&](int c) {
+      const int s = c & 1;
+      const long long b = tile_base(c);
+      const unsigned st = sb + (s ? kTcStage1 : kTcStage0);
+      const long long first[5] = {b - 1, b - ga.nx, b + ga.nx, b - ga.sxy, b + ga.sxy};
+      const int rows[5] = {kTcTile + 2, kTcTile, kTcTile, kTcTile, kTcTile};
+      const unsigned dst[5] = {kTcXOff, kTcYmOff, kTcYpOff, kTcZmOff, kTcZpOff};
+      long long lo[5], hi[5];
+      unsigned bytes = kTcEfBytes;
+      for (int k = 0; k < 5; ++k) {
+        lo[k] = first[k] < 0 ? 0 : first[k];
+        hi[k] = first[k] + rows[k] > n ? n : first[k] + rows[k];
+        if (hi[k] > lo[k]) bytes += (unsigned)(hi[k] - lo[k]) * kTcRowB;
+      }
+      tc::mbar_expect_tx(bar_full + 8 * s, bytes);
+      for (int k = 0; k < 5; ++k)
+        if (hi[k] > lo[k])
+          tc::bulk_g2s(st + dst[k] + (unsigned)(lo[k] - first[k]) * kTcRowB, a.h_in + lo[k] * kH,
+                       (unsigned)(hi[k] - lo[k]) * kTcRowB, bar_full + 8 * s);
+      tc::bulk_g2s(st + kTcEfOff, ga.dir_ef + b * 6, kTcEfBytes, bar_full + 8 * s);
+      last_in[s] = (c >> 1) & 1;
+    };
+    for (int c = 0; c < 2 && c < count; ++c) issue(c);
+    bool ok = true;
+    for (int c = 0; c < count && ok; ++c) {
+      const int bsel = c & 1;
+      ok = tc::mbar_wait(bar_afull, (unsigned)c & 1u, kWaitCycles, s_abort);  // A of tile c written
+      if (ok && c + 2 < count) issue(c + 2);  // stage c & 1 read by every aggregation thread
+      if (ok && c >= 2)  // the epilogue has read this accumulator's previous tile
+        ok = tc::mbar_wait(bar_acce + 8 * bsel, (unsigned)((c >> 1) - 1) & 1u, kWaitCycles, s_abort);
+      if (!ok) {
+        give_up();
+        break;
       }
       tc::fence_after_sync();
       constexpr uint32_t idesc = tc::idesc_bf16_f32(kTcTile, kH);
 #pragma unroll
       for (int k = 0; k < kIn / 16; ++k) {
         const unsigned aoff = (k >> 2) * kTcARegion + (k & 3) * 32, boff = (k >> 2) * (kH * kTcRowB) + (k & 3) * 32;
-        tc::mma_bf16_ss(tmem, tc::sdesc_sw128(sb + kTcA + aoff), tc::sdesc_sw128(sb + kTcW + boff), idesc, k > 0);
+        tc::mma_bf16_ss(tmem + bsel * kH, tc::sdesc_sw128(sb + kTcA + aoff), tc::sdesc_sw128(sb + kTcW + boff), idesc,
+                        k > 0);
       }
-      tc::mma_commit(bar_mma);
-      mma_pend = c & 1;
+      tc::mma_commit(bar_aempty);
+      tc::mma_commit(bar_accf + 8 * bsel);
+      last_mma = c & 1;
     }
-    // while the tensor core runs: the next tile's inputs and gates
-    if (c + 1 < count) {
-      if (!tc::mbar_wait(bar_in0 + 8 * (s ^ 1), (unsigned)((c + 1) >> 1) & 1u, kWaitCycles, s_abort)) {
-        failed = 1;
-        *s_abort = 1;
-        atomicOr(ga.err, 1);
-      } else if (tid == 0) {
-        pend[s ^ 1] = -1;
-      }
-      gates(c + 1);
+    if (!ok) {  // drain: nothing of this CTA's may still write its shared or tensor memory at exit
+      for (int s = 0; s < 2; ++s)
+        if (last_in[s] >= 0) tc::mbar_wait(bar_full + 8 * s, (unsigned)last_in[s], kWaitCycles, nullptr);
+      if (last_mma >= 0) tc::mbar_wait(bar_aempty, (unsigned)last_mma, kWaitCycles, nullptr);
     }
-    if (tid == 0) {
-      if (!tc::mbar_wait(bar_mma, (unsigned)c & 1u, kWaitCycles, s_abort)) {
-        failed = 1;
-        *s_abort = 1;
-        atomicOr(ga.err, 1);
-      } else {
-        mma_pend = -1;
-      }
-    }
-    __syncthreads();  // (1b) the accumulator is complete
-    tc::fence_after_sync();
-    // ---- epilogue: bias, relu, BF16; rows staged in A's first region (the
-    // MMA has read it), swizzled
-    {
-      float v[16];
-      tc::tmem_ld16(tmem + ((unsigned)(32 * eq) << 16) + 16 * ecg, v);
-#pragma unroll
-      for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + s_bias[16 * ecg + j], 0.f);
-      if constexpr (LAST) {
-        float y = 0.f;
-#pragma unroll
-        for (int j = 0; j < 16; ++j) y = fmaf(s_wd[16 * ecg + j], bf16r(v[j]), y);
-        s_y[ecg * kTcTile + erow] = y;
-      }
-      if (a.h_out) {
-#pragma unroll
-        for (int h2 = 0; h2 < 2; ++h2) {
-          const int ch = 2 * ecg + h2;
-          float f8[8];
-#pragma unroll
-          for (int e = 0; e < 8; ++e) f8[e] = v[8 * h2 + e];
-          *reinterpret_cast<uint4*>(sm + kTcA + erow * kTcRowB + ((ch ^ (erow & 7)) << 4)) = pack8(f8);
-        }
-      }
-    }
-    tc::fence_before_sync();
-    __syncthreads();  // (2) staged rows, decoder partials
-    // ---- coalesced stores: 16 bytes a thread, 8 threads a row
-    for (int idx = tid; idx < kTcTile * 8; idx += kTcThreads) {
-      const int row = idx >> 3, ch = idx & 7;
-      const long long gi = b + row;
-      if (gi < n) {
-        const unsigned pos = row * kTcRowB + ((ch ^ (row & 7)) << 4);
-        if (a.h_out) reinterpret_cast<uint4*>(a.h_out + gi * kH)[ch] = *reinterpret_cast<const uint4*>(sm + kTcA + pos);
-        if (a.m_out)
-          reinterpret_cast<uint4*>(a.m_out + gi * kH)[ch] =
-              *reinterpret_cast<const uint4*>(sm + kTcA + kTcARegion + pos);
-      }
-    }
-    if constexpr (LAST) {
-      if (tid < kTcTile && b + tid < n) {
-        const long long gi = b + tid;
-        const float y = ((s_y[tid] + s_y[kTcTile + tid]) + s_y[2 * kTcTile + tid]) + s_y[3 * kTcTile + tid];
-        const double s2 = a.s2[0], is = a.s2[1];
-        const float bd = a.P[kOffBd], ws = a.P[kOffWs];
-        a.z[gi] = s2 * (double)(y + bd + ws * (float)(a.xr[gi] * is)) * (double)a.isd[gi];
-      }
-    }
-    // the loop head's barrier (0) frees A and the partials for the next tile
   }
-  // ---- drain: no copy or MMA of this CTA may still be in flight at exit
-  if (tid == 0) {
-    for (int s = 0; s < 2; ++s)
-      if (pend[s] >= 0) tc::mbar_wait(bar_in0 + 8 * s, (unsigned)pend[s], kWaitCycles, nullptr);
-    if (mma_pend >= 0) tc::mbar_wait(bar_mma, (unsigned)mma_pend, kWaitCycles, nullptr);
-  }
+  __syncwarp();  // the control warp reconverges before the CTA barrier
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 64);
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, kTcCols);
+  }
 }
 
 // h1 = relu(W0 x0 + b0), x0 = [xr / s, log(a_ii)/10]: 8 lanes per node, 8 features a lane.

@@ -29,6 +29,11 @@ __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void mbar_expect_tx(unsigned a, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
 }
+// One arrival (release at CTA scope: this thread's earlier writes are
+// visible to threads that observe the phase complete).
+__device__ __forceinline__ void mbar_arrive(unsigned a) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(unsigned a, unsigned parity) {
   unsigned done;
   asm volatile(
@@ -40,14 +45,27 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned a, unsigned parity) {
       : "memory");
   return done != 0;
 }
+// The same test, suspending the thread until the phase completes or about
+// `ns` nanoseconds have passed: a waiting warp takes no issue slots.
+__device__ __forceinline__ bool mbar_try_wait_sleep(unsigned a, unsigned parity, unsigned ns) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(a), "r"(parity), "r"(ns)
+      : "memory");
+  return done != 0;
+}
 // Waits for the phase of the given parity for at most `budget` clock cycles;
 // false if it gave up (or, with an abort flag, when the flag became nonzero).
 __device__ __noinline__ bool mbar_wait(unsigned a, unsigned parity, long long budget, const volatile int* abort) {
   if (mbar_try_wait(a, parity)) return true;
   const long long t0 = clock64();
-  for (unsigned it = 1;; ++it) {
-    if (mbar_try_wait(a, parity)) return true;
-    if ((it & 15) == 0 && (clock64() - t0 > budget || (abort && *abort))) return false;
+  for (;;) {
+    if (mbar_try_wait_sleep(a, parity, 20000u)) return true;
+    if (clock64() - t0 > budget || (abort && *abort)) return false;
   }
 }
 
@@ -131,6 +149,23 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
       : "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 32 lanes x 32 columns (as tmem_ld16).
+__device__ __forceinline__ void tmem_ld32(unsigned taddr, float (&v)[32]) {
+  unsigned r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 }  // namespace tc

@@ -82,15 +82,14 @@ def test_gradient_matches_oracle(ctx, system, layer):
         assert err < 5e-2 and cos > 0.998, (name, err, cos)
 
 
-@pytest.mark.parametrize("shape", [(12, 11, 10), (40, 36, 30), (128, 3, 3), (3, 3, 257)])
+@pytest.mark.parametrize("shape", [(12, 11, 10), (40, 36, 30), (128, 3, 3), (3, 3, 257), (5, 4, 3)])
 def test_layer_kernels_agree(ctx, shape):
     """The grid layer (bulk-copied neighbour blocks, tcgen05 dense layer) and
     the gather layer (indexed neighbour rows, mma.sync) compute the same
     network: outputs within BF16 rounding of each other on grids with a
-    ragged last tile, several tiles a CTA, and neighbour blocks that start
-    before the first or end after the last node; on a 2-D grid (no 3-D
-    profile) AUTO takes the gather layer and an explicit grid request is
-    refused."""
+    ragged last tile, several tiles a CTA, fewer nodes than one tile, and
+    neighbour blocks that start before the first or end after the last
+    node."""
     nx, ny, nz = shape
     P = abi.diffusion(nx, ny, nz, sigma=1.5, smooth=2.0, seed=6)
     rng = np.random.default_rng(3)
@@ -117,6 +116,8 @@ def test_layer_kernels_agree(ctx, shape):
 
 
 def test_grid_layer_needs_a_3d_grid(ctx):
+    """On a 2-D grid (no 3-D 7-point profile) AUTO takes the gather layer and
+    an explicit grid request is refused."""
     P = abi.diffusion(31, 9, 1, sigma=1.5, smooth=3.0, seed=7)
     A = ctx.matrix(P.row_ptr, P.cols, P.vals)
     net = abi.Gnn(ctx, G.init_params(1).flat().astype(np.float32))
