@@ -262,6 +262,18 @@ __device__ __forceinline__ void fma2_bf16_pair(float& acc0, float& acc1, float g
       : "+f"(acc0), "+f"(acc1)
       : "f"(lo), "f"(hi), "f"(g));
 }
+// Shared-memory words at 32-bit shared addresses.
+__device__ __forceinline__ float lds_f32(unsigned a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ void lds_f32x2(unsigned a, float& x, float& y) {
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(x), "=f"(y) : "r"(a));
+}
+__device__ __forceinline__ void sts_f32(unsigned a, float v) {
+  asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
 // 16 bytes of shared memory at a 32-bit shared address.
 __device__ __forceinline__ uint4 lds128(unsigned a) {
   uint4 v;
@@ -516,8 +528,8 @@ constexpr unsigned kTcEfBytes = kTcTile * 6 * 4;
 constexpr unsigned kTcStageB = kTcEfOff + kTcEfBytes;
 constexpr unsigned kTcStage1 = kTcStage0 + kTcStageB;
 constexpr unsigned kTcBias = kTcStage1 + kTcStageB;          // bias, wd: 2 x 64 floats
-constexpr unsigned kTcGate = kTcBias + 2 * kH * 4;           // gates, BF16: 2 tiles x 128 x 6
-constexpr unsigned kTcGateB = kTcTile * 6 * 2;
+constexpr unsigned kTcGate = kTcBias + 2 * kH * 4;           // gates (BF16 values as FP32): 2 tiles x 128 x 6
+constexpr unsigned kTcGateB = kTcTile * 6 * 4;
 constexpr unsigned kTcZero = kTcGate + 2 * kTcGateB;         // one row of zeros (absent neighbours)
 constexpr unsigned kTcBar = kTcZero + kTcRowB;               // 8 mbarriers, tensor-memory address, abort flag
 constexpr unsigned kTcSmem = kTcBar + 80 + 1024;             // + slack to align the base to 1024 bytes
@@ -617,29 +629,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
         failed = 1;
         give_up();
       }
-      // gates, once per (node, direction), BF16 bits (0 where no neighbour)
+      // gates, once per (node, direction), rounded to BF16 (0 where no neighbour)
       {
-        const float* ef = reinterpret_cast<const float*>(stg + kTcEfOff);
-        unsigned short* gt = reinterpret_cast<unsigned short*>(sm + kTcGate + s * kTcGateB);
+        const unsigned ef = sb + (s ? kTcStage1 : kTcStage0) + kTcEfOff, gt = sb + kTcGate + s * kTcGateB;
         for (int q = tid; q < kTcTile * 6; q += kTcAggThreads) {
-          const float e = ef[q];
-          gt[q] = e == e ? __bfloat16_as_ushort(__float2bfloat16_rn(sigmoidf(fmaf(u, e, cg)))) : (unsigned short)0;
+          const float e = lds_f32(ef + 4 * q);
+          sts_f32(gt + 4 * q, e == e ? bf16r(sigmoidf(fmaf(u, e, cg))) : 0.f);
         }
       }
       if (bar_or(1, kTcAggThreads, failed)) break;
       const int ln = tid >> 2, qq = tid & 3;  // node, and its chunks qq and qq + 4
-      const unsigned short* gt = reinterpret_cast<const unsigned short*>(sm + kTcGate + s * kTcGateB) + ln * 6;
-      const float* efr = reinterpret_cast<const float*>(stg + kTcEfOff) + ln * 6;
       const unsigned sst = sb + (s ? kTcStage1 : kTcStage0) + ln * kTcRowB;  // this node's row of each block
       unsigned src[6] = {sst + kTcZmOff, sst + kTcYmOff, sst + kTcXOff, sst + kTcXOff + 2 * kTcRowB, sst + kTcYpOff,
                          sst + kTcZpOff};
-      float g[6];
+      float g[6], e[6];
+      {
+        const unsigned efa = sb + (s ? kTcStage1 : kTcStage0) + kTcEfOff + ln * 24;
+        const unsigned gta = sb + kTcGate + s * kTcGateB + ln * 24;
 #pragma unroll
-      for (int d = 0; d < 6; ++d) {
-        const float e = efr[d];
-        src[d] = e == e ? src[d] : sb + kTcZero;
-        g[d] = __uint_as_float((unsigned)gt[d] << 16);
+        for (int d = 0; d < 6; d += 2) {
+          lds_f32x2(efa + 4 * d, e[d], e[d + 1]);
+          lds_f32x2(gta + 4 * d, g[d], g[d + 1]);
+        }
       }
+#pragma unroll
+      for (int d = 0; d < 6; ++d) src[d] = e[d] == e[d] ? src[d] : sb + kTcZero;
       uint4 hv[2], mv[2];
 #pragma unroll
       for (int jj = 0; jj < 2; ++jj) {
