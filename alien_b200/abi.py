@@ -263,6 +263,7 @@ SIGNATURES: dict[str, tuple] = {
     "ab2_problem_write_matrix_market": (_I, [C.POINTER(Problem), C.c_char_p, C.c_char_p]),
     "ab2_matrix_market_error": (C.c_char_p, []),
     "ab2_selftest_bounded_wait": (_I, [_P, _IP, _DP]),
+    "ab2_selftest_mbarrier_wait": (_I, [_P, _IP, _DP]),
     "ab2_context_inject_alloc_failure": (_I, [_P, C.c_longlong]),
     "ab2_rng_u64": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64]),
     "ab2_rng_uniform": (_D, [C.c_uint64, C.c_uint64, C.c_uint64]),
@@ -359,6 +360,12 @@ class Context:
         """(expired, seconds): a device-side wait on a word nothing writes gives up on its budget."""
         e, t = C.c_int(), C.c_double()
         self.check(lib().ab2_selftest_bounded_wait(self.h, C.byref(e), C.byref(t)), "selftest_bounded_wait")
+        return bool(e.value), t.value
+
+    def selftest_mbarrier_wait(self) -> tuple[bool, float]:
+        """(expired, seconds): a wait on an mbarrier phase nothing completes gives up on its budget."""
+        e, t = C.c_int(), C.c_double()
+        self.check(lib().ab2_selftest_mbarrier_wait(self.h, C.byref(e), C.byref(t)), "selftest_mbarrier_wait")
         return bool(e.value), t.value
 
     def inject_alloc_failure(self, nth: int) -> None:

@@ -624,7 +624,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gnn_layer_grid(const GridLaye
     for (int c = 0; c < count; ++c) {
       const int s = c & 1;
       const long long b = tile_base(c);
-      const unsigned char* stg = sm + (s ? kTcStage1 : kTcStage0);
       if (!tc::mbar_wait(bar_full + 8 * s, (unsigned)(c >> 1) & 1u, kWaitCycles, s_abort)) {
         failed = 1;
         give_up();

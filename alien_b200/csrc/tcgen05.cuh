@@ -60,7 +60,8 @@ __device__ __forceinline__ bool mbar_try_wait_sleep(unsigned a, unsigned parity,
 }
 // Waits for the phase of the given parity for at most `budget` clock cycles;
 // false if it gave up (or, with an abort flag, when the flag became nonzero).
-__device__ __noinline__ bool mbar_wait(unsigned a, unsigned parity, long long budget, const volatile int* abort) {
+static __device__ __noinline__ bool mbar_wait(unsigned a, unsigned parity, long long budget,
+                                             const volatile int* abort) {
   if (mbar_try_wait(a, parity)) return true;
   const long long t0 = clock64();
   for (;;) {

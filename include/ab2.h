@@ -533,6 +533,10 @@ int ab2_fcg_solve(ab2_context* ctx, const ab2_matrix* A, ab2_gnn* gnn, const ab2
  * its clock budget (~2 s), sets the error flag (*expired = 1) and the kernel
  * ends; *seconds is the wall time.  The context stays usable. */
 int ab2_selftest_bounded_wait(ab2_context* ctx, int* expired, double* seconds);
+/* The same for the mbarrier waits of the learned preconditioner's grid layer:
+ * a wait on a barrier phase that nothing completes gives up after its clock
+ * budget; *expired = 1 when it did. */
+int ab2_selftest_mbarrier_wait(ab2_context* ctx, int* expired, double* seconds);
 /* Host-side fault injection: the nth device allocation on ctx from now on
  * fails as AB2_ERR_OOM (once); 0 turns it off. */
 int ab2_context_inject_alloc_failure(ab2_context* ctx, long long nth);

@@ -1,9 +1,11 @@
 """Failure detection on the GPU without a fault.
 
-Every device-side wait in libab2 (the sentinel polling of the ILU(0) sweeps)
-is bounded by a clock budget and an error flag.  Here one thread waits on a
-word that nothing writes -- a producer that is gone: the wait must give up by
-itself, set the flag the host reads, and leave the context usable.  (Host-side
+Every device-side wait in libab2 (the sentinel polling of the ILU(0) sweeps,
+the mbarrier waits of the learned preconditioner's grid layer) is bounded by
+a clock budget and an error flag.  Here one thread waits on a word that
+nothing writes -- a producer that is gone -- or on an mbarrier phase that
+nothing completes: the wait must give up by itself, set the flag the host
+reads, and leave the context usable.  (Host-side
 failures -- a rank that never reaches a collective -- are covered in
 test_gpu_dist.py and test_dist.py.)
 """
@@ -27,6 +29,25 @@ def test_bounded_wait_gives_up_and_context_stays_usable(ctx):
     st = S.solve(ctx.vector(P.b), ctx.vector(P.n))
     assert st.succeeded and st.error == 0
     S.close()
+    A.close()
+
+
+def test_mbarrier_wait_gives_up_and_context_stays_usable(ctx):
+    expired, seconds = ctx.selftest_mbarrier_wait()
+    assert expired
+    assert 0.5 < seconds < 30.0
+    # the grid layer of the learned preconditioner still runs on this context
+    from oracle import gnn_oracle as G
+
+    P = abi.diffusion(12, 11, 10, sigma=1.5, smooth=2.0, seed=4)
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals)
+    net = abi.Gnn(ctx, G.init_params(2).flat().astype(np.float32))
+    net.bind(A)
+    assert net.layer == "grid"
+    z = ctx.vector(P.n)
+    net.apply(ctx.vector(np.ones(P.n)), z)
+    assert np.all(np.isfinite(z.download()))
+    net.close()
     A.close()
 
 
