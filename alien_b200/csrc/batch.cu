@@ -13,8 +13,11 @@
 // rows; a dot product is a block tree per CTA plus the csize partials summed
 // in rank order through distributed shared memory, so every CTA gets the same
 // scalar; the CTAs of a cluster synchronise on the hardware cluster barrier
-// (three per CG iteration: after each of the two reductions, and after p is
-// written, because the SpMV of one CTA reads p of the others).  Clusters never
+// (two per CG iteration, after each of the two reductions: the SpMV forms
+// p = z + beta p itself at every row it reads -- from z and the previous p,
+// written before the last barrier -- and stores its own rows' p in the other
+// of two buffers; with the grouped-lane CSR variants a separate p pass and a
+// third barrier).  Clusters never
 // wait for each other, and no code spins on memory, so nothing can hang.
 //
 // Each system converges on its own: its cluster stops iterating when the
@@ -53,6 +56,7 @@ struct BatchArgs {
   double* x;
   double* r64;           // FP64 residual scratch (N)
   float *r, *z, *p, *q, *d;  // FP32 inner CG vectors (N)
+  float* p2;             // the second p buffer of the fused body (N)
   const float* inv32;    // Jacobi: 1/a_ii rounded to FP32
   double tol;
   float inner_tol;
@@ -172,6 +176,45 @@ __global__ void k_batch_cg(BatchArgs<V64, V32> a) {
       const float crit = a.inner_tol * a.inner_tol * acc[1];
       float rho = acc[0];
       int it = 0;
+      if constexpr (lanes_per_row<V32>::value == 1) {
+        // p = z + beta p formed inside the SpMV: the same fma as the p pass of
+        // the loop below, so q, p.q and every scalar are the same numbers
+        float beta = 0.f;
+        for (;;) {
+          const float* __restrict__ pold = (it & 1) ? a.p : a.p2;
+          float* __restrict__ pcur = (it & 1) ? a.p2 : a.p;
+          const bool first = it == 0;
+          auto pval = [&](int c) { return first ? a.z[c] : __fmaf_rn(beta, pold[c], a.z[c]); };
+          float pq[1] = {0.f};
+          for (int i = lo + threadIdx.x; i < hi; i += T) {
+            const float qv = a.A32.row_f(i, pval);
+            const float pv = pval(i);
+            pcur[i] = pv;
+            a.q[i] = qv;
+            pq[0] = __fmaf_rn(pv, qv, pq[0]);
+          }
+          cluster_sum<1>(pq, s_part32, s_warp32, slot, cluster);
+          slot ^= 1;
+          if (pq[0] == 0.f) break;  // breakdown "alpha": keep the correction so far
+          const float alpha = rho / pq[0];
+          float rz[2] = {0.f, 0.f};
+          for (int i = lo + threadIdx.x; i < hi; i += T) {
+            a.d[i] = __fmaf_rn(alpha, pcur[i], a.d[i]);
+            const float rv = __fmaf_rn(-alpha, a.q[i], a.r[i]);
+            a.r[i] = rv;
+            const float zv = __fmul_rn(a.inv32[i], rv);
+            a.z[i] = zv;
+            rz[0] = __fmaf_rn(rv, zv, rz[0]);
+            rz[1] = __fmaf_rn(rv, rv, rz[1]);
+          }
+          cluster_sum<2>(rz, s_part32, s_warp32, slot, cluster);
+          slot ^= 1;
+          ++it;
+          if (rz[1] < crit || it >= a.inner_max_iter) break;
+          beta = rz[0] / rho;
+          rho = rz[0];
+        }
+      } else
       for (;;) {
         // q = A32 p ; alpha = rho / (p.q)   (p of every CTA written: the barrier in cluster_sum above
         // or the explicit one at the end of the previous iteration)
@@ -254,7 +297,7 @@ struct ab2_batch {
   int* d_order = nullptr;
   unsigned int* d_ticket = nullptr;
   double* d_r64 = nullptr;
-  float* d_vec32 = nullptr;  // r z p q d
+  float* d_vec32 = nullptr;  // r z p q d p2
   float* d_inv32 = nullptr;
   int *d_conv = nullptr, *d_outer = nullptr, *d_inner = nullptr;
   double* d_res = nullptr;
@@ -293,6 +336,7 @@ bool launch_batch(ab2_batch* B, V64 a64, V32 a32, int csize, int threads, const 
   args.p = B->d_vec32 + 2 * N;
   args.q = B->d_vec32 + 3 * N;
   args.d = B->d_vec32 + 4 * N;
+  args.p2 = B->d_vec32 + 5 * N;
   args.inv32 = B->d_inv32;
   args.tol = B->opts.tol;
   args.inner_tol = (float)B->opts.inner_tol;
@@ -510,7 +554,7 @@ int ab2_batch_create(ab2_context* ctx, const ab2_matrix* A, int nsys, const int*
                              ctx->stream));
     B->d_ticket = dev_alloc<unsigned int>(ctx, 1);
     B->d_r64 = dev_alloc<double>(ctx, N);
-    B->d_vec32 = dev_alloc<float>(ctx, 5 * N);
+    B->d_vec32 = dev_alloc<float>(ctx, 6 * N);
     B->d_inv32 = dev_alloc<float>(ctx, N);
     double* inv = dev_alloc<double>(ctx, N);
     op_inv_diag(ctx, A, inv);

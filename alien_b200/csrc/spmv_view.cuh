@@ -129,6 +129,34 @@ struct EllViewS {
     }
     return acc;
   }
+  // The same sum with the operand x[c] given by f(c) (computed on the fly).
+  template <class F>
+  __device__ __forceinline__ T row_f(int r, F&& f) const {
+    const int s = r / S, lane = r % S;
+    const int o = off[s];
+    const int w = off[s + 1] - o;
+    const size_t base = (size_t)o * S + lane;
+    const int* cp = ci + base;
+    const T* vp = v + base;
+    T acc = 0;
+    for (int j = 0; j < w; j += 8) {
+      int c[8];
+      T a[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const bool in = j + u < w;
+        c[u] = in ? __ldcs(cp + (size_t)(j + u) * S) : -1;
+        a[u] = in ? __ldcs(vp + (size_t)(j + u) * S) : T(0);
+      }
+      T xv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? f(c[u]) : T(0);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (c[u] >= 0) acc = mul_add_rn(a[u], xv[u], acc);
+    }
+    return acc;
+  }
 };
 
 // CSR with LPR consecutive lanes per row (the batched solver's "rows per
