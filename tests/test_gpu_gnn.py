@@ -115,6 +115,30 @@ def test_layer_kernels_agree(ctx, shape):
         assert np.linalg.norm(out["grid"] - zo) / np.linalg.norm(zo) < 2e-2
 
 
+def test_layer_kernels_agree_on_gradients(ctx):
+    """Training on the grid layer: its forward pass also stores m1..m4 and h5
+    for the backward kernels.  On 43,200 nodes (several tiles a CTA) the loss
+    and every gradient block agree with the gather layer's to BF16 accuracy."""
+    P = abi.diffusion(40, 36, 30, sigma=1.5, smooth=2.0, seed=6)
+    rng = np.random.default_rng(9)
+    r, e = rng.normal(size=P.n), rng.normal(size=P.n)
+    p = G.init_params(5).flat().astype(np.float32)
+    A = ctx.matrix(P.row_ptr, P.cols, P.vals)
+    out = {}
+    for layer in ("grid", "gather"):
+        net = abi.Gnn(ctx, p)
+        net.set_layer(layer)
+        net.bind(A)
+        out[layer] = net.loss_grad(ctx.vector(r), ctx.vector(e))
+        net.close()
+    (Lg, gg), (La, ga) = out["grid"], out["gather"]
+    assert np.isfinite(Lg) and abs(Lg - La) <= 1e-2 * abs(La), (Lg, La)
+    bg, ba = blocks(gg.astype(np.float64)), blocks(ga.astype(np.float64))
+    for name in bg:
+        err = np.linalg.norm(bg[name] - ba[name]) / max(np.linalg.norm(ba[name]), 1e-30)
+        assert err < 5e-2, (name, err)
+
+
 def test_grid_layer_needs_a_3d_grid(ctx):
     """On a 2-D grid (no 3-D 7-point profile) AUTO takes the gather layer and
     an explicit grid request is refused."""
